@@ -1,0 +1,352 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 image-formation engine; prints ONE JSON line (rank 0).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload smlm]
+
+Workload `smlm` (the plain dSTORM SMLM render): one step renders a 200-frame 128 x 128 sCMOS movie -- every frame's
+background, ~160 Catmull-Rom PSF splats and the sCMOS noise chain -- from emitter records resident in HBM
+(`value`), and end to end from host blink events to host ADU frames through the C ABI (`e2e`: emitter collection,
+host->device copy, render, device->host copy). Frames shard across ranks (weak scaling: each rank renders its own
+200 frames; no collective on the data path). L2 is flushed (a 256 MB write) before every timed step.
+
+--impl reference: the reference's own CPU renderer (RenderPhotonImage + ApplyNoiseChain under its ParallelFor,
+compiled from its sources: oracle/_ref) on all host cores, same workload and metric; rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+# ----------------------------------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        for l in self.lines:
+            p = [x.strip() for x in l.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"), p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+# ----------------------------------------------------------------------------------------------------- dist
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ----------------------------------------------------------------------------------------------------- SMLM
+class SmlmWorkload:
+    name = "smlm-dstorm sCMOS 128x128 px, 200 frames, 4000 sites, ~160 ON/frame, 129^2x49 cubic PSF"
+    metric = "frames/s"
+
+    def __init__(self, rank: int):
+        from insiliscope_b200.workloads import smlm_dstorm
+        self.mv = smlm_dstorm(seed=42, frame0=rank * 200)
+        self.frame0 = rank * 200
+
+    # -------------------------------------------------- ours
+    def setup(self, device: int):
+        import torch
+        from insiliscope_b200 import CZT_FP32, Engine, generate_camera_maps
+        mv = self.mv
+        self.eng = eng = Engine(device)
+        t0 = time.perf_counter()
+        eng.kernel_build(0, mv.psf, CZT_FP32)
+        eng.synchronize()
+        self.psf_build_ms = (time.perf_counter() - t0) * 1e3
+        off, gain, rn = generate_camera_maps(mv.width, mv.height, mv.map_seed, mv.offset_mean, mv.offset_std,
+                                             mv.gain_nominal, mv.gain_std_fraction, mv.read_noise_nominal,
+                                             mv.read_noise_std_fraction)
+        eng.set_static(mv.width, mv.height, offset=off, gain=gain, read_noise=rn, flat_bg=mv.background)
+        self.ems, self.frames, _ = eng.collect_emitters(0, mv.events, mv.bucket_start, self.frame0, mv.width,
+                                                        mv.height, mv.pixel_nm, mv.photons_per_blink)
+        self.ems = self.ems.copy()
+        self.d_em = torch.from_numpy(self.ems.view(np.uint8)).to(f"cuda:{device}")
+        self.d_fr = torch.from_numpy(self.frames.view(np.uint8)).to(f"cuda:{device}")
+        self.d_adu = torch.empty((mv.frames, mv.height, mv.width), dtype=torch.uint16, device=f"cuda:{device}")
+        self.h_adu = np.empty((mv.frames, mv.height, mv.width), np.uint16)
+        self.stream = eng.torch_stream()
+        self.frames_per_step = mv.frames
+        self.n_emitters = len(self.ems)
+
+    def device_step(self):
+        self.eng.render_frames_dev(self.d_em, self.d_fr, self.mv.frames, self.mv.camera, self.mv.noise_seed,
+                                   None, self.d_adu)
+
+    def e2e_step(self):
+        """Host blink events -> host ADU: emitter collection, H2D, render, D2H, all through the C ABI."""
+        mv = self.mv
+        ems, frames, _ = self.eng.collect_emitters(0, mv.events, mv.bucket_start, self.frame0, mv.width, mv.height,
+                                                   mv.pixel_nm, mv.photons_per_blink, out=self._e2e_buf(),
+                                                   frames_out=self._e2e_frames())
+        _, adu = self.eng.render_frames(ems, frames, mv.camera, mv.noise_seed, want_photons=False)
+        return adu
+
+    def _e2e_buf(self):
+        from insiliscope_b200 import EMITTER_DTYPE
+        if not hasattr(self, "_eb"):
+            self._eb = np.empty(len(self.mv.events), EMITTER_DTYPE)
+        return self._eb
+
+    def _e2e_frames(self):
+        from insiliscope_b200 import FRAME_DTYPE
+        if not hasattr(self, "_ef"):
+            self._ef = np.empty(self.mv.frames, FRAME_DTYPE)
+        return self._ef
+
+    def e2e_bytes(self):
+        return self.n_emitters * 32 + self.mv.frames * 24, self.mv.frames * self.mv.width * self.mv.height * 2
+
+    def alg_bytes_per_launch(self):
+        # Per frame: the ADU written (2 B/px) and the three float camera maps read (12 B/px); per emitter its 32-byte
+        # record; the frame table. The PSF block sums (3.4 MB) stay in L2 across the launch and count once.
+        mv = self.mv
+        px = mv.width * mv.height
+        _, nz, _, bw = self.eng.kernel_info(0)
+        return mv.frames * (px * 14 + 24) + self.n_emitters * 32 + nz * bw * bw * 4
+
+    def kernel_name(self):
+        return "RenderFramesKernel"
+
+    # -------------------------------------------------- the reference on the host cores
+    def reference_setup(self, threads=0):
+        from oracle.oracle import Reference
+        from insiliscope_b200 import generate_camera_maps
+        mv = self.mv
+        self.ref = Reference()
+        self.ref.set_threads(threads)
+        self.rk = self.ref.kernel(req=mv.psf)
+        self.maps = generate_camera_maps(mv.width, mv.height, mv.map_seed, mv.offset_mean, mv.offset_std,
+                                         mv.gain_nominal, mv.gain_std_fraction, mv.read_noise_nominal,
+                                         mv.read_noise_std_fraction)
+
+    def reference_step(self):
+        mv = self.mv
+        t, _, adu = self.rk.render_movie(mv.events, self.frame0, mv.frames, mv.width, mv.height, mv.pixel_nm,
+                                         mv.photons_per_blink, mv.background, mv.camera, *self.maps, mv.noise_seed)
+        return t
+
+
+WORKLOADS = {"smlm": SmlmWorkload}
+
+
+# ----------------------------------------------------------------------------------------------------- arms
+def run_reference(args):
+    world, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return 0
+    from oracle.oracle import Reference
+    if not Reference.available():
+        print(json.dumps({"impl": "reference", "unavailable": "the reference harness oracle/_ref/libiscref.so is not "
+                                                               "built (needs the reference tree at build time)"}))
+        return 0
+    w = WORKLOADS[args.workload](0)
+    w.reference_setup(threads=0)
+    cores = w.ref.threads()
+    for _ in range(args.warmup):
+        w.reference_step()
+    times = [w.reference_step() for _ in range(args.steps)]
+    ms = 1e3 * statistics.mean(times)
+    value = w.mv.frames / (ms / 1e3)
+    line = {"metric": w.metric, "value": value, "unit": w.metric, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": w.name, "frames_per_step": w.mv.frames},
+            "cpu_baseline": {"value": value, "unit": w.metric, "cores": cores, "kind": "reference",
+                             "sample": f"the whole {w.mv.frames}-frame movie per step (RenderPhotonImage + "
+                                       "ApplyNoiseChain per frame, frames in parallel on the reference's pool; "
+                                       "PSF kernel built once before timing, as the reference memoizes it)"},
+            "e2e": {"value": value, "unit": w.metric, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def cpu_baseline(w):
+    """The reference's CPU renderer on this box's host cores, a bounded sample: one whole movie, best of 3."""
+    from oracle.oracle import Reference
+    if Reference.available():
+        w.reference_setup(threads=0)
+        w.reference_step()
+        best = min(w.reference_step() for _ in range(3))
+        return {"value": w.mv.frames / best, "unit": w.metric, "cores": w.ref.threads(), "kind": "reference",
+                "sample": f"one {w.mv.frames}-frame movie, best of 3 (reference RenderPhotonImage + ApplyNoiseChain "
+                          "on its thread pool, kernel memoized)"}
+    return None
+
+
+def run_ours(args):
+    import torch
+    world, rank, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    from insiliscope_b200.build import build_library
+    build_library()
+    w = WORKLOADS[args.workload](rank)
+    w.setup(local)
+    eng = w.eng
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")   # 256 MB > L2 (126 MB)
+    start = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stop = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with torch.cuda.stream(w.stream):
+        for i in range(args.warmup):
+            flush.fill_(float(i))
+            w.device_step()
+    eng.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    launches0 = eng.launch_count
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        barrier(world)
+        with torch.cuda.stream(w.stream):
+            for i in range(args.steps):
+                flush.fill_(float(i + 1))
+                start[i].record(w.stream)
+                w.device_step()
+                stop[i].record(w.stream)
+        eng.synchronize()
+        torch.cuda.synchronize()
+        barrier(world)
+    launches = eng.launch_count - launches0
+    step_ms = [s.elapsed_time(e) for s, e in zip(start, stop)]
+    ms = max_over_ranks(statistics.mean(step_ms), world)
+    value = world * w.frames_per_step / (ms / 1e3)
+    # end to end through the C ABI with host buffers
+    for _ in range(max(1, args.warmup)):
+        w.e2e_step()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        w.e2e_step()
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps, world)
+    h2d, d2h = w.e2e_bytes()
+    hbm, _, peak_kind = measured_peaks()
+    achieved = w.alg_bytes_per_launch() / (statistics.mean(step_ms) / 1e3) / 1e9
+    line = {"metric": w.metric, "value": value, "unit": w.metric, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": w.name, "frames_per_step": w.frames_per_step, "emitters_per_step": w.n_emitters,
+                       "l2": "flushed before every timed step (256 MB write)", "parallelism": f"frames x{world}",
+                       "psf_build_ms": round(w.psf_build_ms, 3)},
+            "e2e": {"value": world * w.frames_per_step / (e2e_ms / 1e3), "unit": w.metric, "ms_per_step": e2e_ms,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "timing": "host wall clock per step (blocking C-ABI calls), max over ranks"},
+            "roofline": {"bound": "hbm", "kernel": w.kernel_name(), "achieved": achieved, "peak": hbm,
+                         "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
+                         "traffic": None, "alg_bytes_per_launch": w.alg_bytes_per_launch()},
+            "gpu_launches": launches, "clocks": clk.summary()}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(w)
+    if rank == 0:
+        print(json.dumps(line))
+    eng.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="smlm")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    return run_reference(args) if args.impl == "reference" else run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,270 @@
+/*
+ * iscu.h -- C ABI of the B200 image-formation engine (libiscu.so).
+ *
+ * The engine replaces, on an NVIDIA B200 (sm_100a), the fluorescence image-formation path of inSiliScope's render
+ * engine: the Gibson-Lanni/Zernike chirp-Z PSF stack, the blink splat, the camera noise chain with its counter-based
+ * pcg4d stream, and the widefield mean-field FFT convolution. Every entry point is extern "C" with plain pointers and
+ * sizes, so a C++ host (the engine's GpuSimulator / SplatGpuHost / WidefieldAccelerator seams), a ctypes caller or a
+ * JNI/cgo stub binds it alike.
+ *
+ * Conventions
+ *  - Every function returns ISCU_OK (0) or an ISCU_ERR_* code; iscu_last_error() gives the calling thread's message.
+ *    No C++ exception crosses this boundary (the reference seam's `bool` + `std::string& err`,
+ *    adapter/inSiliScope/Simulation/GpuSimD3D11.h:61-111).
+ *  - A context (iscu_ctx) owns one device, one CUDA stream and the resident buffers (kernel stacks, camera maps),
+ *    the way one GpuSimulator owns its D3D11 device (GpuSimD3D11.h:28-30: one instance per thread). Calls on one
+ *    context are serialized by its mutex (WidefieldGpuHost.h:74-75's GpuBackend::mu).
+ *  - Functions whose pointer arguments end in `_dev` take device pointers and enqueue work on the context's stream
+ *    without synchronizing; the others take host pointers and return when the results are in host memory.
+ *  - Images are row-major (x fastest). Photon images are float32, camera frames uint16 ADU.
+ */
+#ifndef ISCU_H
+#define ISCU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ISCU_ABI_VERSION 1
+
+enum iscu_status {
+   ISCU_OK = 0,
+   ISCU_ERR_ARG = 1,     /* an argument is out of range or inconsistent */
+   ISCU_ERR_CUDA = 2,    /* a CUDA runtime or launch error (the message names the call) */
+   ISCU_ERR_STATE = 3,   /* the context lacks what the call needs (no kernel in the slot, no camera maps) */
+   ISCU_ERR_LIMIT = 4,   /* a size beyond a documented maximum */
+   ISCU_ERR_TIMEOUT = 5, /* a bounded device-side wait ran out (the context stays usable) */
+   ISCU_ERR_NODEV = 6    /* no CUDA device, or not an sm_100 device */
+};
+
+/* Interpolation of the splat's sub-pixel read (sim::PsfInterpMode, PsfGeneratorBridge.h:68-74). Fft has no GPU path
+ * in the reference and none here. */
+enum iscu_interp { ISCU_INTERP_NEAREST = 0, ISCU_INTERP_LINEAR = 1, ISCU_INTERP_CUBIC = 2 };
+
+/* Which chirp-Z product a PSF build uses. */
+enum iscu_czt_method {
+   ISCU_CZT_FP32 = 0,   /* the plain FP32 form: SIMT complex matmuls in shared memory */
+   ISCU_CZT_TF32X3 = 1  /* split precision on the tensor cores: hi/lo TF32 operands, three tcgen05 MMAs per product,
+                           FP32 accumulation in tensor memory */
+};
+
+typedef struct iscu_ctx iscu_ctx;
+
+/* ---------------------------------------------------------------- context ------------------------------------- */
+
+/* The calling thread's last error message ("" after a success). */
+const char* iscu_last_error(void);
+int iscu_abi_version(void);
+/* A context on CUDA device `device`; ISCU_ERR_NODEV when it is not an sm_100 device. */
+int iscu_create(int device, iscu_ctx** out);
+void iscu_destroy(iscu_ctx* ctx);
+/* Waits for the context's stream. Returns the first asynchronous error, if any. */
+int iscu_synchronize(iscu_ctx* ctx);
+/* The context's cudaStream_t (as void*), for callers that order their own work with it. */
+void* iscu_stream(iscu_ctx* ctx);
+/* Number of kernel launches this context has issued (all entry points), for launch accounting. */
+uint64_t iscu_launch_count(iscu_ctx* ctx);
+
+/* ---------------------------------------------------------------- counter RNG --------------------------------- */
+/* pcg4d (adapter/inSiliScope/Simulation/SMLMCounterRng.h:37-56, core/src/rng.h:18-33): in4_dev[4i..4i+3] = (a, b, c,
+ * d) -> out4_dev[4i..4i+3], for i < n. */
+int iscu_pcg4d_dev(iscu_ctx* ctx, const uint32_t* in4_dev, uint32_t* out4_dev, size_t n);
+/* sim::CounterRng (SMLMCounterRng.h:60-91): the first `per_pixel` uniforms of pixel p's stream, p = pixel0 + i,
+ * into out_dev[i * per_pixel + j] (float64). */
+int iscu_counter_uniforms_dev(iscu_ctx* ctx, uint32_t seed, uint32_t frame, uint32_t pixel0, uint32_t npix,
+                              uint32_t per_pixel, double* out_dev);
+
+/* ---------------------------------------------------------------- camera --------------------------------------- */
+
+/* sim::CameraNoiseParams (SMLMNoise.h:35-50). gain is photons (electrons) per ADU. */
+typedef struct iscu_camera {
+   double quantum_efficiency;
+   double dark_electrons;
+   double gain;              /* used where no gain map is set */
+   double read_noise_e;      /* used where no read-noise map is set */
+   int32_t emccd;
+   int32_t bit_depth;        /* EMCCD: ADU clipped to [0, 2^bit_depth - 1] */
+   double em_gain;           /* EMCCD: divides the read noise only */
+   double cic_electrons;     /* EMCCD: clock-induced charge per pixel and frame */
+} iscu_camera;
+
+/* Static per-pixel inputs of a width x height frame (sim::GpuSimulator::SetStatic, GpuSimD3D11.h:88-90; the window
+ * offset of SplatGpuHost::SetStatic, SplatGpu.h:51-55). offset (ADU), gain (photons/ADU), read_noise (e-) are host
+ * arrays of width*height floats or NULL (offset 0, the camera's scalar gain / read noise: ApplyNoiseChain's rule,
+ * SMLMNoise.cpp:148-153). background: width*height photons/pixel/frame before the per-frame scale, or NULL for the
+ * flat value flat_bg. illum: the illumination field (peak 1), or NULL for flat; it multiplies the background
+ * (RenderPhotonImage, SMLMSimulation.cpp:129-136) -- emitters carry their own illumination factor already.
+ * pixel_base: the frame's first pixel's index on the sensor (the noise stream is the sensor's). */
+int iscu_set_static(iscu_ctx* ctx, uint32_t width, uint32_t height, uint32_t pixel_base, const float* offset,
+                    const float* gain, const float* read_noise, const float* background, const float* illum,
+                    double flat_bg);
+
+/* sim::PixelOffsetMap / PixelGainMap / PixelReadNoiseMap::Generate (SMLMNoise.cpp:89-140) on the host, from one
+ * std::mt19937_64(seed) in the order offset, gain, read noise (SplatGpu.cpp:500-502). Any output may be NULL (its
+ * draws are still taken). keep_y0/keep_rows: a window's rows (0 rows: all). */
+int iscu_generate_camera_maps(uint32_t width, uint32_t height, uint64_t seed, double offset_mean_adu,
+                              double offset_std_adu, double gain_nominal, double gain_std_fraction,
+                              double read_noise_nominal, double read_noise_std_fraction, uint32_t keep_y0,
+                              uint32_t keep_rows, float* offset, float* gain, float* read_noise);
+
+/* ApplyNoiseChain (SMLMNoise.cpp:142-216) on n_frames photon images: photons_dev[k*w*h ..] -> adu_dev[k*w*h ..],
+ * noise keyed by (seed, frames_dev[k], pixel_base + pixel). Needs iscu_set_static for the maps. */
+int iscu_noise_frames_dev(iscu_ctx* ctx, const float* photons_dev, uint32_t n_frames, const uint32_t* frames_dev,
+                          const iscu_camera* cam, uint32_t seed, uint16_t* adu_dev);
+
+/* ---------------------------------------------------------------- PSF ------------------------------------------ */
+
+/* sim::PsfGeneratorRequest for the GibsonLanniZernike model (PsfGeneratorBridge.h:91-158) with the Zernike string
+ * parsed (ParseZernikeCoefficients, SMLMZernike.h:50-51): OSA/ANSI 0-27, waves, unnormalized. */
+typedef struct iscu_psf_request {
+   double wavelength_nm;
+   double na;
+   double immersion_index;
+   double sample_index;
+   double working_distance_um;
+   double sample_depth_nm;
+   double pixel_size_nm;
+   double zernike[28];
+   int32_t mask_double_helix;
+   int32_t mask_modes;
+   double mask_waist;
+   int32_t oversampling;
+   int32_t kernel_half_width_px;
+   int32_t nz;               /* made odd and >= 3, as GeometryFor does (ZernikePsf.cpp:118-129) */
+   int32_t pupil_samples;    /* 0: ZernikePupilSamples' automatic choice (ZernikePsf.cpp:139-158) */
+   double z_step_nm;
+   int32_t interp;           /* iscu_interp */
+   int32_t reserved;
+} iscu_psf_request;
+
+/* A request's plane geometry (GeometryFor + ZernikePupilSamples): plane size, planes, pupil samples M. */
+int iscu_psf_geometry(const iscu_psf_request* req, int32_t* size, int32_t* nz, int32_t* pupil_samples);
+
+/* One PSF library: n_psf planes of size x size float32 into out_dev (device), each the squared modulus of the
+ * chirp-Z image of a Gibson-Lanni + Zernike (+ double-helix) pupil (ComputeZernikePsfPlanes, ZernikePsf.cpp:160-337).
+ * PSF i uses request set_of_psf[i] (host array) of the `sets` requests (host array) at defocus defocus_nm[i]
+ * (host array; the reference's plane k sits at (k - (nz-1)/2) * z_step_nm). size overrides the request's
+ * 2*half*os+1 (0: keep it); the pupil samples M come from the request. normalize != 0 divides each plane by its sum
+ * (BuildZernikePsfKernelCache, ZernikePsf.cpp:400-410). method: iscu_czt_method. All sets must share M and size. */
+int iscu_psf_library_dev(iscu_ctx* ctx, const iscu_psf_request* sets, uint32_t n_sets, const uint32_t* set_of_psf,
+                         const double* defocus_nm, uint32_t n_psf, int32_t size, int32_t normalize, int32_t method,
+                         float* out_dev);
+
+/* ---------------------------------------------------------------- kernel slots -------------------------------- */
+/* At most this many kernel stacks per context (GpuSimulator::kMaxKernels, GpuSimD3D11.h:70). */
+#define ISCU_MAX_KERNELS 4
+
+/* Builds a kernel stack on the device from a request (BuildZernikePsfKernelCache, ZernikePsf.cpp:382-415: sum-1
+ * planes, then the block sums, PsfGeneratorBridge.cpp:1021-1088) into slot 0..3. */
+int iscu_kernel_build(iscu_ctx* ctx, int32_t slot, const iscu_psf_request* req, int32_t method);
+/* Uploads a kernel stack made elsewhere (the engine's PsfKernelCache planes, already sum-1): nz planes of size x size
+ * (host). The block sums are built on the device (GpuSimulator::SetKernels, GpuSimD3D11.h:72-77). */
+int iscu_kernel_set_planes(iscu_ctx* ctx, int32_t slot, const float* planes, int32_t size, int32_t nz,
+                           int32_t oversampling, double z_step_nm, int32_t interp);
+/* The halo cut (WithHaloCut, PsfGeneratorBridge.cpp:1137-1243) for a slot's stack; threshold <= 0 removes it. */
+int iscu_kernel_set_halo(iscu_ctx* ctx, int32_t slot, double threshold);
+/* Geometry of a slot: size, nz, oversampling, block-sum width. */
+int iscu_kernel_info(iscu_ctx* ctx, int32_t slot, int32_t* size, int32_t* nz, int32_t* oversampling,
+                     int32_t* block_sum_width);
+/* Reads a slot's planes (nz*size*size floats) or block sums (nz*bw*bw floats, row-major) back to the host. */
+int iscu_kernel_get_planes(iscu_ctx* ctx, int32_t slot, float* out);
+int iscu_kernel_get_block_sums(iscu_ctx* ctx, int32_t slot, float* out);
+
+/* ---------------------------------------------------------------- splat + noise ------------------------------- */
+
+/* One emitter of one frame as the splat places it (sim::FrameEmitter, SMLMSimulation.h:158-173): camera-pixel
+ * position (drift included), photons (overlap x brightness x excitation x illumination), and its kernel plane
+ * (z index | kernel slot << 16). 32 bytes. The device derives SplatSetup (PsfGeneratorBridge.cpp:1382-1422) from
+ * it in float64, so the splat is bit for bit the CPU's. */
+typedef struct iscu_emitter {
+   double x_px;
+   double y_px;
+   double photons;
+   int32_t plane;
+   int32_t reserved;
+} iscu_emitter;
+
+/* sim::GpuSplatEmitter (GpuSimD3D11.h:50-59): the reference's 64-byte device record (float weights). */
+typedef struct iscu_gpu_splat_emitter {
+   int32_t x0, y0, bx, by;
+   int32_t plane;
+   int32_t n_taps;
+   float photons;
+   int32_t cut_radius2;
+   float wx[4];
+   float wy[4];
+} iscu_gpu_splat_emitter;
+
+/* One frame of a batch: its emitters are [em_start, em_start + em_count) of the batch's array; frame is the noise
+ * stream's frame index; bg_scale multiplies the background (BackgroundFadeScale). */
+typedef struct iscu_frame {
+   uint32_t em_start;
+   uint32_t em_count;
+   uint32_t frame;
+   uint32_t reserved;
+   double bg_scale;
+} iscu_frame;
+
+/* Frames k < n_frames: the background, then every emitter of the frame splatted in list order
+ * (RenderPhotonImage, SMLMSimulation.cpp:103-160: the same float additions in the same order), then, unless
+ * cam is NULL, the noise chain (ApplyNoiseChain). photons_dev (nullable) receives the noise-free images,
+ * adu_dev (nullable) the frames; both n_frames*w*h. Needs iscu_set_static and the kernels the emitters name. */
+int iscu_render_frames_dev(iscu_ctx* ctx, const iscu_emitter* emitters_dev, const iscu_frame* frames_dev,
+                           uint32_t n_frames, const iscu_camera* cam, uint32_t seed, float* photons_dev,
+                           uint16_t* adu_dev);
+/* The same with host arrays (emitters: sum of em_count records; frames: n_frames; outputs host, nullable): the
+ * copies in and out are part of the call. */
+int iscu_render_frames(iscu_ctx* ctx, const iscu_emitter* emitters, uint32_t n_emitters, const iscu_frame* frames,
+                       uint32_t n_frames, const iscu_camera* cam, uint32_t seed, float* photons, uint16_t* adu);
+
+/* GpuSimulator::RenderFrames / SplatGpuHost::RenderFrames (GpuSimD3D11.h:98-107, SplatGpu.h:57-62) over the
+ * reference's 64-byte records: the D3D11/WGSL shader's semantics (GpuSimD3D11.cpp:169-248) -- the record's float
+ * weights, the halo radius test, an optional extra photon image per frame (extras: n_frames*w*h host floats, or NULL;
+ * the blinks are splatted onto background + extra, as SplatGpuHost does) -- with the taps summed in float64. Host
+ * arrays. */
+int iscu_render_gpu_records(iscu_ctx* ctx, const iscu_gpu_splat_emitter* emitters, uint32_t n_emitters,
+                            const iscu_frame* frames, uint32_t n_frames, const float* extras,
+                            const iscu_camera* cam, uint32_t seed, uint16_t* adu);
+
+/* ---------------------------------------------------------------- host-side emitter collection ---------------- */
+
+/* sim::BlinkEvent (SMLMSimulation.h:82-102), the fields the render reads. */
+typedef struct iscu_blink_event {
+   double x_um, y_um, z_nm;
+   double t_start, t_end;
+   double brightness;
+   double excite;
+   double reserved;
+} iscu_blink_event;
+
+/* CollectFrameEmitters (SMLMSimulation.cpp:55-101) for one frame: the events overlapping [frame, frame+1), in order,
+ * as iscu_emitter records (kernel slot `slot`, z plane from the slot's stack by NearestZIndex,
+ * PsfGeneratorBridge.cpp:40-61), min_photons applied (RenderPhotonImage's blink-min-photons). illum: the
+ * illumination field (w*h host floats) or NULL. Writes at most max_out records; *n_out gets the count. Returns
+ * ISCU_ERR_LIMIT when max_out is too small. *n_clamped (nullable) += emitters whose z was clamped. */
+int iscu_collect_frame_emitters(iscu_ctx* ctx, int32_t slot, const iscu_blink_event* events, uint32_t n_events,
+                                int64_t frame, uint32_t width, uint32_t height, double pixel_size_nm,
+                                double photons_per_blink, double drift_x_px, double drift_y_px,
+                                double global_z_offset_um, const float* illum, double min_photons,
+                                iscu_emitter* out, uint32_t max_out, uint32_t* n_out, int64_t* n_clamped);
+
+/* The same for the frames frame0 .. frame0 + n_frames - 1 of a batch, into one emitter array and its frame table
+ * (the batch a render call takes). Frame k's candidate events are bucket k: events[bucket_index[j]] for j in
+ * [bucket_start[k], bucket_start[k+1]) (BucketEventsByFrame's index lists, SMLMSimulation.cpp:203-217, in event
+ * order), or events[j] itself when bucket_index is NULL. drift_x_px / drift_y_px / global_z_offset_um / bg_scale:
+ * per-frame arrays or NULL (0, 0, 0, 1). frames_out[k]: the frame's emitter run, frame0 + k, its bg scale. */
+int iscu_collect_emitters(iscu_ctx* ctx, int32_t slot, const iscu_blink_event* events, const uint32_t* bucket_index,
+                          const uint32_t* bucket_start, int64_t frame0, uint32_t n_frames, uint32_t width,
+                          uint32_t height, double pixel_size_nm, double photons_per_blink, const double* drift_x_px,
+                          const double* drift_y_px, const double* global_z_offset_um, const double* bg_scale,
+                          const float* illum, double min_photons, iscu_emitter* out, uint32_t max_out,
+                          iscu_frame* frames_out, uint32_t* n_out, int64_t* n_clamped);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ISCU_H */

@@ -1,0 +1,157 @@
+"""ctypes declarations of include/iscu.h (libiscu.so).
+
+Loading fails loudly when the library is missing: there is no CPU fallback in this package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libiscu.so")
+
+ISCU_OK = 0
+ISCU_ERR_ARG = 1
+ISCU_ERR_CUDA = 2
+ISCU_ERR_STATE = 3
+ISCU_ERR_LIMIT = 4
+ISCU_ERR_TIMEOUT = 5
+ISCU_ERR_NODEV = 6
+
+INTERP_NEAREST, INTERP_LINEAR, INTERP_CUBIC = 0, 1, 2
+CZT_FP32, CZT_TF32X3 = 0, 1
+MAX_KERNELS = 4
+
+u8p = C.POINTER(C.c_uint8)
+u16p = C.POINTER(C.c_uint16)
+u32p = C.POINTER(C.c_uint32)
+i32p = C.POINTER(C.c_int32)
+i64p = C.POINTER(C.c_int64)
+f32p = C.POINTER(C.c_float)
+f64p = C.POINTER(C.c_double)
+vp = C.c_void_p
+
+
+class Camera(C.Structure):
+    _fields_ = [
+        ("quantum_efficiency", C.c_double),
+        ("dark_electrons", C.c_double),
+        ("gain", C.c_double),
+        ("read_noise_e", C.c_double),
+        ("emccd", C.c_int32),
+        ("bit_depth", C.c_int32),
+        ("em_gain", C.c_double),
+        ("cic_electrons", C.c_double),
+    ]
+
+
+class PsfRequest(C.Structure):
+    _fields_ = [
+        ("wavelength_nm", C.c_double),
+        ("na", C.c_double),
+        ("immersion_index", C.c_double),
+        ("sample_index", C.c_double),
+        ("working_distance_um", C.c_double),
+        ("sample_depth_nm", C.c_double),
+        ("pixel_size_nm", C.c_double),
+        ("zernike", C.c_double * 28),
+        ("mask_double_helix", C.c_int32),
+        ("mask_modes", C.c_int32),
+        ("mask_waist", C.c_double),
+        ("oversampling", C.c_int32),
+        ("kernel_half_width_px", C.c_int32),
+        ("nz", C.c_int32),
+        ("pupil_samples", C.c_int32),
+        ("z_step_nm", C.c_double),
+        ("interp", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+class Emitter(C.Structure):
+    _fields_ = [("x_px", C.c_double), ("y_px", C.c_double), ("photons", C.c_double), ("plane", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+class GpuSplatEmitter(C.Structure):
+    _fields_ = [("x0", C.c_int32), ("y0", C.c_int32), ("bx", C.c_int32), ("by", C.c_int32), ("plane", C.c_int32),
+                ("n_taps", C.c_int32), ("photons", C.c_float), ("cut_radius2", C.c_int32),
+                ("wx", C.c_float * 4), ("wy", C.c_float * 4)]
+
+
+class Frame(C.Structure):
+    _fields_ = [("em_start", C.c_uint32), ("em_count", C.c_uint32), ("frame", C.c_uint32), ("reserved", C.c_uint32),
+                ("bg_scale", C.c_double)]
+
+
+class BlinkEvent(C.Structure):
+    _fields_ = [("x_um", C.c_double), ("y_um", C.c_double), ("z_nm", C.c_double), ("t_start", C.c_double),
+                ("t_end", C.c_double), ("brightness", C.c_double), ("excite", C.c_double),
+                ("reserved", C.c_double)]
+
+
+# name -> (restype, argtypes); every function include/iscu.h declares.
+SIGNATURES = {
+    "iscu_last_error": (C.c_char_p, []),
+    "iscu_abi_version": (C.c_int, []),
+    "iscu_create": (C.c_int, [C.c_int, C.POINTER(vp)]),
+    "iscu_destroy": (None, [vp]),
+    "iscu_synchronize": (C.c_int, [vp]),
+    "iscu_stream": (vp, [vp]),
+    "iscu_launch_count": (C.c_uint64, [vp]),
+    "iscu_pcg4d_dev": (C.c_int, [vp, vp, vp, C.c_size_t]),
+    "iscu_counter_uniforms_dev": (C.c_int, [vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, vp]),
+    "iscu_set_static": (C.c_int, [vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, vp, vp, vp, C.c_double]),
+    "iscu_generate_camera_maps": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint64, C.c_double, C.c_double, C.c_double,
+                                            C.c_double, C.c_double, C.c_double, C.c_uint32, C.c_uint32, vp, vp,
+                                            vp]),
+    "iscu_noise_frames_dev": (C.c_int, [vp, vp, C.c_uint32, vp, C.POINTER(Camera), C.c_uint32, vp]),
+    "iscu_psf_geometry": (C.c_int, [C.POINTER(PsfRequest), i32p, i32p, i32p]),
+    "iscu_psf_library_dev": (C.c_int, [vp, C.POINTER(PsfRequest), C.c_uint32, vp, vp, C.c_uint32, C.c_int32,
+                                       C.c_int32, C.c_int32, vp]),
+    "iscu_kernel_build": (C.c_int, [vp, C.c_int32, C.POINTER(PsfRequest), C.c_int32]),
+    "iscu_kernel_set_planes": (C.c_int, [vp, C.c_int32, vp, C.c_int32, C.c_int32, C.c_int32, C.c_double,
+                                         C.c_int32]),
+    "iscu_kernel_set_halo": (C.c_int, [vp, C.c_int32, C.c_double]),
+    "iscu_kernel_info": (C.c_int, [vp, C.c_int32, i32p, i32p, i32p, i32p]),
+    "iscu_kernel_get_planes": (C.c_int, [vp, C.c_int32, vp]),
+    "iscu_kernel_get_block_sums": (C.c_int, [vp, C.c_int32, vp]),
+    "iscu_render_frames_dev": (C.c_int, [vp, vp, vp, C.c_uint32, C.POINTER(Camera), C.c_uint32, vp, vp]),
+    "iscu_render_frames": (C.c_int, [vp, vp, C.c_uint32, vp, C.c_uint32, C.POINTER(Camera), C.c_uint32, vp, vp]),
+    "iscu_render_gpu_records": (C.c_int, [vp, vp, C.c_uint32, vp, C.c_uint32, vp, C.POINTER(Camera), C.c_uint32,
+                                          vp]),
+    "iscu_collect_frame_emitters": (C.c_int, [vp, C.c_int32, vp, C.c_uint32, C.c_int64, C.c_uint32, C.c_uint32,
+                                              C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, vp,
+                                              C.c_double, vp, C.c_uint32, u32p, i64p]),
+    "iscu_collect_emitters": (C.c_int, [vp, C.c_int32, vp, vp, vp, C.c_int64, C.c_uint32, C.c_uint32, C.c_uint32,
+                                        C.c_double, C.c_double, vp, vp, vp, vp, vp, C.c_double, vp, C.c_uint32, vp,
+                                        u32p, i64p]),
+}
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """The loaded libiscu.so, with argtypes set. Raises if it is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"libiscu.so is not built ({LIB_PATH}); run insiliscope_b200.build.build_library()")
+        lib = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+class IscuError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"iscu error {code}: {msg}")
+        self.code = code
+
+
+def check(rc: int) -> None:
+    if rc != ISCU_OK:
+        raise IscuError(rc, load().iscu_last_error().decode())

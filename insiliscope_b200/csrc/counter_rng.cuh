@@ -1,0 +1,126 @@
+// Device restatement of the engine's counter-based noise stream and its draws.
+//
+//  - Pcg4d: adapter/inSiliScope/Simulation/SMLMCounterRng.h:37-56 (= core/src/rng.h:18-33), pure uint32 arithmetic.
+//  - CounterRng: SMLMCounterRng.h:60-91. A pixel's stream is (seed, frame, pixel, counter): one pcg4d per 4
+//    uniforms, consumed a, b, c, d; uniform = ((x >> 9) + 0.5) * 2^-23, exact in float64.
+//  - Gauss / Poisson / Gamma: SMLMCounterRng.h:95-138, in float64 with the same operations in the same order.
+//
+// Bit-exactness with the CPU path rests on (1) no floating-point contraction: every translation unit that includes
+// this header is compiled with --fmad=false, as the reference is with -ffp-contract=off (core/CMakeLists.txt:41);
+// (2) IEEE float64 sqrt and division (always correctly rounded in CUDA); (3) CUDA's float64 log/exp/cos, which, like
+// glibc's, are within an ulp: an integer draw can differ only when its argument sits within ~1e-16 of a count
+// boundary.
+#pragma once
+
+#include <cstdint>
+
+namespace iscu {
+
+__device__ __forceinline__ void Pcg4d(uint32_t& a, uint32_t& b, uint32_t& c, uint32_t& d)
+{
+   a = a * 1664525u + 1013904223u;
+   b = b * 1664525u + 1013904223u;
+   c = c * 1664525u + 1013904223u;
+   d = d * 1664525u + 1013904223u;
+   a += b * d;
+   b += c * a;
+   c += a * b;
+   d += b * c;
+   a ^= a >> 16;
+   b ^= b >> 16;
+   c ^= c >> 16;
+   d ^= d >> 16;
+   a += b * d;
+   b += c * a;
+   c += a * b;
+   d += b * c;
+}
+
+// One frame's uniform source; Pixel(p) rewinds it to pixel p's stream. The four words of the current hash are
+// consumed in order by shifting, which keeps them in registers.
+struct CounterRng
+{
+   uint32_t seed, frame, pix, ctr;
+   uint32_t q0, q1, q2, q3;
+   int k;
+
+   __device__ __forceinline__ CounterRng(uint32_t s, uint32_t f) : seed(s), frame(f), pix(0), ctr(0), k(4)
+   {
+      q0 = q1 = q2 = q3 = 0u;
+   }
+   __device__ __forceinline__ void Pixel(uint32_t p)
+   {
+      pix = p;
+      ctr = 0;
+      k = 4;
+   }
+   __device__ __forceinline__ double Uniform()
+   {
+      if (k == 4)
+      {
+         uint32_t a = seed, b = frame, c = pix, d = ctr;
+         Pcg4d(a, b, c, d);
+         q0 = a;
+         q1 = b;
+         q2 = c;
+         q3 = d;
+         ++ctr;
+         k = 0;
+      }
+      const uint32_t x = q0;
+      q0 = q1;
+      q1 = q2;
+      q2 = q3;
+      ++k;
+      return (static_cast<double>(x >> 9) + 0.5) * 1.1920928955078125e-7;
+   }
+};
+
+// Box-Muller, radius first, angle second (SMLMCounterRng.h:95-100).
+__device__ __forceinline__ double CounterGauss(CounterRng& u)
+{
+   const double r = sqrt(-2.0 * log(u.Uniform()));
+   return r * cos(6.283185307179586 * u.Uniform());
+}
+
+// Knuth inversion up to mean 60, the rounded normal beyond; 1000-iteration cap (SMLMCounterRng.h:102-118).
+__device__ __forceinline__ double CounterPoisson(double l, CounterRng& u)
+{
+   if (l > 60.0)
+   {
+      const double s = sqrt(l);
+      const double g = CounterGauss(u);
+      return fmax(0.0, floor(l + s * g + 0.5));
+   }
+   if (!(l > 0.0))
+      return 0.0;
+   const double L = exp(-l);
+   int k = 0;
+   double p = 1.0;
+   do
+   {
+      ++k;
+      p *= u.Uniform();
+   } while (p > L && k < 1000);
+   return static_cast<double>(k - 1);
+}
+
+// Marsaglia-Tsang Gamma(k, 1), 1000-iteration cap (SMLMCounterRng.h:120-136).
+__device__ __forceinline__ double CounterGamma(double k, CounterRng& u)
+{
+   const double d = k - 1.0 / 3.0, c = 1.0 / sqrt(9.0 * d);
+   for (int it = 0; it < 1000; ++it)
+   {
+      const double x = CounterGauss(u), t = 1.0 + c * x;
+      if (t <= 0.0)
+         continue;
+      const double v = t * t * t, w = u.Uniform();
+      if (w < 1.0 - 0.0331 * x * x * x * x)
+         return d * v;
+      if (log(w) < 0.5 * x * x + d * (1.0 - v + log(v)))
+         return d * v;
+   }
+   return d;
+}
+
+} // namespace iscu

@@ -1,0 +1,230 @@
+// Internal declarations shared by the translation units of libiscu.so (not part of the ABI).
+#pragma once
+
+#include "../../include/iscu.h"
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace iscu {
+
+// ------------------------------------------------------------------ errors
+void SetError(const std::string& msg);
+void ClearError();
+int Fail(int code, const std::string& msg);
+int CudaFail(cudaError_t e, const char* what);
+
+#define ISCU_CK(call)                                                                                                 \
+   do                                                                                                                 \
+   {                                                                                                                  \
+      cudaError_t e_ = (call);                                                                                        \
+      if (e_ != cudaSuccess)                                                                                          \
+         return ::iscu::CudaFail(e_, #call);                                                                          \
+   } while (0)
+
+// Checks a launch just issued (configuration errors show at once; faults at the next synchronization).
+#define ISCU_CK_LAUNCH(ctx, what)                                                                                     \
+   do                                                                                                                 \
+   {                                                                                                                  \
+      (ctx)->launches.fetch_add(1, std::memory_order_relaxed);                                                        \
+      cudaError_t e_ = cudaGetLastError();                                                                            \
+      if (e_ != cudaSuccess)                                                                                          \
+         return ::iscu::CudaFail(e_, what);                                                                           \
+   } while (0)
+
+// ------------------------------------------------------------------ device buffers
+// A device allocation owned by the context (freed with it).
+struct DevBuf
+{
+   void* p = nullptr;
+   size_t bytes = 0;
+   DevBuf() = default;
+   DevBuf(const DevBuf&) = delete;
+   DevBuf& operator=(const DevBuf&) = delete;
+   ~DevBuf() { Free(); }
+   void Free()
+   {
+      if (p)
+         cudaFree(p);
+      p = nullptr;
+      bytes = 0;
+   }
+   // Grows to at least n bytes (contents not kept).
+   cudaError_t Reserve(size_t n)
+   {
+      if (n <= bytes && p)
+         return cudaSuccess;
+      Free();
+      cudaError_t e = cudaMalloc(&p, n ? n : 16);
+      if (e == cudaSuccess)
+         bytes = n;
+      return e;
+   }
+   template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+// Page-locked host staging (grows; contents not kept).
+struct PinnedBuf
+{
+   void* p = nullptr;
+   size_t bytes = 0;
+   PinnedBuf() = default;
+   PinnedBuf(const PinnedBuf&) = delete;
+   PinnedBuf& operator=(const PinnedBuf&) = delete;
+   ~PinnedBuf()
+   {
+      if (p)
+         cudaFreeHost(p);
+   }
+   cudaError_t Reserve(size_t n)
+   {
+      if (n <= bytes && p)
+         return cudaSuccess;
+      if (p)
+         cudaFreeHost(p);
+      p = nullptr;
+      bytes = 0;
+      cudaError_t e = cudaHostAlloc(&p, n ? n : 16, cudaHostAllocDefault);
+      if (e == cudaSuccess)
+         bytes = n;
+      return e;
+   }
+   template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+// ------------------------------------------------------------------ kernel stacks (device view)
+// What the splat reads of one kernel stack. Passed by value to the kernels.
+struct KernelView
+{
+   const float* sums = nullptr;     // nz planes of bw x bw block sums, row-major
+   const int16_t* spanLo = nullptr; // halo cut: [z * (2 camRad + 1) + dy + camRad]; nullptr: the whole square
+   const int16_t* spanHi = nullptr;
+   const int32_t* radius2 = nullptr;
+   int os = 1, size = 0, nz = 0, bw = 0, camRad = 0, interp = 2;
+   double kc = 0.0;                 // (size - 1) / 2
+};
+
+struct KernelSlot
+{
+   bool valid = false;
+   int size = 0, nz = 0, os = 1, bw = 0, halfOv = 0, interp = 2;
+   double zStepNm = 0.0;
+   DevBuf planes;    // nz * size * size
+   DevBuf sums;      // nz * bw * bw
+   DevBuf spanLo, spanHi, radius2;
+   bool halo = false;
+   double haloThreshold = 0.0;
+   std::vector<int32_t> radius2Host;
+   KernelView View() const
+   {
+      KernelView v;
+      v.sums = sums.as<float>();
+      v.spanLo = halo ? spanLo.as<int16_t>() : nullptr;
+      v.spanHi = halo ? spanHi.as<int16_t>() : nullptr;
+      v.radius2 = halo ? radius2.as<int32_t>() : nullptr;
+      v.os = os;
+      v.size = size;
+      v.nz = nz;
+      v.bw = bw;
+      v.camRad = halfOv / os;
+      v.interp = interp;
+      v.kc = (size - 1) / 2.0;
+      return v;
+   }
+   // sim::PsfKernelCache::NearestZIndex (PsfGeneratorBridge.cpp:40-61).
+   int NearestZIndex(double zUm, bool* clamped) const;
+};
+
+// ------------------------------------------------------------------ camera (device view)
+struct CameraView
+{
+   double qe = 1.0, dark = 0.0, gain = 1.0, readNoise = 0.0;
+   int emccd = 0;
+   double maxAdu = 65535.0, emGain = 1.0, cic = 0.0;
+};
+CameraView MakeCameraView(const iscu_camera& c);
+
+struct StaticView
+{
+   const float* offset = nullptr;
+   const float* gain = nullptr;
+   const float* readNoise = nullptr;
+   const float* background = nullptr;
+   const float* illum = nullptr;
+   double flatBg = 0.0;
+   uint32_t width = 0, height = 0, pixelBase = 0;
+};
+
+} // namespace iscu
+
+// ------------------------------------------------------------------ the context
+struct iscu_ctx
+{
+   int device = 0;
+   cudaStream_t stream = nullptr;
+   std::recursive_mutex mu;
+   std::atomic<uint64_t> launches{0};
+   int smCount = 0;
+   iscu::KernelSlot kernels[ISCU_MAX_KERNELS];
+   // camera statics
+   bool haveStatic = false;
+   uint32_t width = 0, height = 0, pixelBase = 0;
+   double flatBg = 0.0;
+   iscu::DevBuf offset, gain, readNoise, background, illum;
+   bool haveOffset = false, haveGain = false, haveReadNoise = false, haveBackground = false, haveIllum = false;
+   std::vector<float> illumHost;   // the illumination field, for host-side emitter collection
+   // staging for the host-pointer entry points
+   iscu::DevBuf dEmitters, dFrames, dPhotons, dAdu, dExtras, dScratch;
+   iscu::PinnedBuf hIn, hOut;
+   iscu::StaticView Static() const
+   {
+      iscu::StaticView s;
+      s.offset = haveOffset ? offset.as<float>() : nullptr;
+      s.gain = haveGain ? gain.as<float>() : nullptr;
+      s.readNoise = haveReadNoise ? readNoise.as<float>() : nullptr;
+      s.background = haveBackground ? background.as<float>() : nullptr;
+      s.illum = haveIllum ? illum.as<float>() : nullptr;
+      s.flatBg = flatBg;
+      s.width = width;
+      s.height = height;
+      s.pixelBase = pixelBase;
+      return s;
+   }
+};
+
+namespace iscu {
+
+// Launchers implemented in the .cu files (ctx->mu held by the caller).
+int LaunchPcg4d(iscu_ctx* ctx, const uint32_t* in, uint32_t* out, size_t n);
+int LaunchCounterUniforms(iscu_ctx* ctx, uint32_t seed, uint32_t frame, uint32_t pixel0, uint32_t npix,
+                          uint32_t perPixel, double* out);
+int LaunchNoiseFrames(iscu_ctx* ctx, const float* photons, uint32_t nFrames, const uint32_t* frames,
+                      const CameraView& cam, uint32_t seed, uint16_t* adu);
+int LaunchRenderFrames(iscu_ctx* ctx, const iscu_emitter* ems, const iscu_frame* frames, uint32_t nFrames,
+                       const CameraView* cam, uint32_t seed, float* photons, uint16_t* adu);
+int LaunchRenderGpuRecords(iscu_ctx* ctx, const iscu_gpu_splat_emitter* ems, const iscu_frame* frames,
+                           uint32_t nFrames, const float* extras, const CameraView* cam, uint32_t seed,
+                           uint16_t* adu);
+int LaunchBlockSums(iscu_ctx* ctx, const float* planes, int n, int os, int nz, float* sums);
+int LaunchNormalizePlanes(iscu_ctx* ctx, float* planes, int planeElems, int nPlanes);
+// defocusM: each PSF's defocus in metres (the reference's resAxialM * (z - (nz - 1) / 2) for a stack's plane z).
+int BuildPsfLibrary(iscu_ctx* ctx, const iscu_psf_request* sets, uint32_t nSets, const uint32_t* setOfPsf,
+                    const double* defocusM, uint32_t nPsf, int32_t size, int32_t normalize, int32_t method,
+                    float* out);
+int BuildHalo(iscu_ctx* ctx, KernelSlot& k, double threshold);
+
+// PSF geometry helpers (ZernikePsf.cpp:118-158).
+struct PsfGeometry
+{
+   int size = 0, nz = 0, os = 1, halfOv = 0, M = 0;
+   double resLateralNm = 0.0;
+};
+bool GeometryFor(const iscu_psf_request& r, PsfGeometry& g, std::string& err);
+
+} // namespace iscu

@@ -1,0 +1,345 @@
+"""Python host side of the engine: the reference's GPU seam (sim::GpuSimulator, GpuSimD3D11.h:61-111) and the PSF
+entry (ComputePsfKernelCache, PsfGeneratorBridge.h:317) over the C ABI of libiscu.so.
+
+Host arrays are numpy; device arrays are torch CUDA tensors (torch is the device-memory plumbing, the work runs in
+libiscu.so's kernels). Errors raise IscuError with the library's message -- the reference seam's `bool` + `err`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi
+from ._abi import (CZT_FP32, CZT_TF32X3, INTERP_CUBIC, INTERP_LINEAR, INTERP_NEAREST, Camera, IscuError, PsfRequest,
+                   check, load)
+
+EMITTER_DTYPE = np.dtype([("x_px", "<f8"), ("y_px", "<f8"), ("photons", "<f8"), ("plane", "<i4"),
+                          ("reserved", "<i4")])
+FRAME_DTYPE = np.dtype([("em_start", "<u4"), ("em_count", "<u4"), ("frame", "<u4"), ("reserved", "<u4"),
+                        ("bg_scale", "<f8")])
+GPU_SPLAT_EMITTER_DTYPE = np.dtype([("x0", "<i4"), ("y0", "<i4"), ("bx", "<i4"), ("by", "<i4"), ("plane", "<i4"),
+                                    ("n_taps", "<i4"), ("photons", "<f4"), ("cut_radius2", "<i4"),
+                                    ("wx", "<f4", (4,)), ("wy", "<f4", (4,))])
+BLINK_EVENT_DTYPE = np.dtype([("x_um", "<f8"), ("y_um", "<f8"), ("z_nm", "<f8"), ("t_start", "<f8"),
+                              ("t_end", "<f8"), ("brightness", "<f8"), ("excite", "<f8"), ("reserved", "<f8")])
+assert EMITTER_DTYPE.itemsize == C.sizeof(_abi.Emitter) == 32
+assert FRAME_DTYPE.itemsize == C.sizeof(_abi.Frame) == 24
+assert GPU_SPLAT_EMITTER_DTYPE.itemsize == C.sizeof(_abi.GpuSplatEmitter) == 64
+assert BLINK_EVENT_DTYPE.itemsize == C.sizeof(_abi.BlinkEvent) == 64
+
+
+@dataclass
+class CameraParams:
+    """sim::CameraNoiseParams (SMLMNoise.h:35-50)."""
+    quantum_efficiency: float = 1.0
+    dark_electrons: float = 0.0
+    gain: float = 1.0
+    read_noise_e: float = 1.5
+    emccd: bool = False
+    bit_depth: int = 16
+    em_gain: float = 300.0
+    cic_electrons: float = 0.002
+
+    def c(self) -> Camera:
+        return Camera(self.quantum_efficiency, self.dark_electrons, self.gain, self.read_noise_e, int(self.emccd),
+                      int(self.bit_depth), self.em_gain, self.cic_electrons)
+
+
+@dataclass
+class PsfParams:
+    """sim::PsfGeneratorRequest, GibsonLanniZernike (PsfGeneratorBridge.h:91-158); zernike: OSA 0-27, waves."""
+    wavelength_nm: float = 660.0
+    na: float = 1.4
+    immersion_index: float = 1.518
+    sample_index: float = 1.518
+    working_distance_um: float = 150.0
+    sample_depth_nm: float = 0.0
+    pixel_size_nm: float = 100.0
+    zernike: list = field(default_factory=lambda: [0.0] * 28)
+    double_helix: bool = False
+    mask_modes: int = 5
+    mask_waist: float = 1.0
+    oversampling: int = 4
+    kernel_half_width_px: int = 8
+    nz: int = 1
+    pupil_samples: int = 0
+    z_step_nm: float = 100.0
+    interp: int = INTERP_NEAREST
+
+    def c(self) -> PsfRequest:
+        r = PsfRequest()
+        r.wavelength_nm = self.wavelength_nm
+        r.na = self.na
+        r.immersion_index = self.immersion_index
+        r.sample_index = self.sample_index
+        r.working_distance_um = self.working_distance_um
+        r.sample_depth_nm = self.sample_depth_nm
+        r.pixel_size_nm = self.pixel_size_nm
+        z = list(self.zernike) + [0.0] * (28 - len(self.zernike))
+        for j in range(28):
+            r.zernike[j] = float(z[j])
+        r.mask_double_helix = int(self.double_helix)
+        r.mask_modes = int(self.mask_modes)
+        r.mask_waist = float(self.mask_waist)
+        r.oversampling = int(self.oversampling)
+        r.kernel_half_width_px = int(self.kernel_half_width_px)
+        r.nz = int(self.nz)
+        r.pupil_samples = int(self.pupil_samples)
+        r.z_step_nm = float(self.z_step_nm)
+        r.interp = int(self.interp)
+        return r
+
+    def geometry(self) -> tuple[int, int, int]:
+        """(plane size, planes, pupil samples) as the reference derives them (ZernikePsf.cpp:118-158)."""
+        s, nz, m = C.c_int32(), C.c_int32(), C.c_int32()
+        req = self.c()
+        check(load().iscu_psf_geometry(C.byref(req), C.byref(s), C.byref(nz), C.byref(m)))
+        return s.value, nz.value, m.value
+
+
+def _ptr(a) -> C.c_void_p:
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        assert a.flags.c_contiguous
+        return C.c_void_p(a.ctypes.data)
+    return C.c_void_p(a.data_ptr())   # torch tensor
+
+
+def _f32(a, n=None):
+    if a is None:
+        return None
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    if n is not None and a.size != n:
+        raise ValueError(f"expected {n} values, got {a.size}")
+    return a
+
+
+def generate_camera_maps(width, height, seed, offset_mean=100.0, offset_std=2.0, gain=1.0, gain_std_fraction=0.0,
+                         read_noise=1.5, read_noise_std_fraction=0.0, keep_y0=0, keep_rows=0):
+    """PixelOffsetMap/GainMap/ReadNoiseMap::Generate from one mt19937_64(seed), offset then gain then read noise."""
+    rows = keep_rows if keep_rows else height
+    rows = min(rows, max(0, height - keep_y0)) if keep_rows else height
+    off = np.empty(width * rows, np.float32)
+    g = np.empty_like(off)
+    rn = np.empty_like(off)
+    check(load().iscu_generate_camera_maps(width, height, seed, offset_mean, offset_std, gain, gain_std_fraction,
+                                            read_noise, read_noise_std_fraction, keep_y0, keep_rows, _ptr(off),
+                                            _ptr(g), _ptr(rn)))
+    return off, g, rn
+
+
+class Engine:
+    """One libiscu context: a device, a stream, up to four resident kernel stacks and the camera statics."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        h = C.c_void_p()
+        check(self.lib.iscu_create(device, C.byref(h)))
+        self.h = h
+        self.device = device
+        self.width = self.height = 0
+
+    def close(self):
+        if self.h:
+            self.lib.iscu_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -------------------------------------------------------------------------------------------- plumbing
+    def synchronize(self):
+        check(self.lib.iscu_synchronize(self.h))
+
+    @property
+    def launch_count(self) -> int:
+        return int(self.lib.iscu_launch_count(self.h))
+
+    @property
+    def stream_handle(self) -> int:
+        return int(self.lib.iscu_stream(self.h) or 0)
+
+    def torch_stream(self):
+        import torch
+        return torch.cuda.ExternalStream(self.stream_handle, device=f"cuda:{self.device}")
+
+    # -------------------------------------------------------------------------------------------- RNG
+    def pcg4d(self, words):
+        """pcg4d of each row of an (n, 4) uint32 CUDA tensor (SMLMCounterRng.h:37-56)."""
+        import torch
+        words = words.contiguous()
+        out = torch.empty_like(words)
+        check(self.lib.iscu_pcg4d_dev(self.h, _ptr(words), _ptr(out), words.shape[0]))
+        self.synchronize()
+        return out
+
+    def counter_uniforms(self, seed, frame, pixel0, npix, per_pixel):
+        """The first per_pixel uniforms of each pixel's CounterRng stream (SMLMCounterRng.h:60-91), float64."""
+        import torch
+        out = torch.empty((npix, per_pixel), dtype=torch.float64, device=f"cuda:{self.device}")
+        check(self.lib.iscu_counter_uniforms_dev(self.h, seed, frame, pixel0, npix, per_pixel, _ptr(out)))
+        self.synchronize()
+        return out
+
+    # -------------------------------------------------------------------------------------------- camera
+    def set_static(self, width, height, pixel_base=0, offset=None, gain=None, read_noise=None, background=None,
+                   illum=None, flat_bg=0.0):
+        n = width * height
+        arrs = [_f32(a, n) for a in (offset, gain, read_noise, background, illum)]
+        check(self.lib.iscu_set_static(self.h, width, height, pixel_base, *[_ptr(a) for a in arrs], float(flat_bg)))
+        self.width, self.height = width, height
+
+    def noise_frames_dev(self, photons, frames, camera: CameraParams, seed):
+        """ApplyNoiseChain on (n, h, w) float32 CUDA photons; frames: the frame index of each. Returns uint16."""
+        import torch
+        photons = photons.contiguous()
+        fr = torch.as_tensor(np.asarray(frames, dtype=np.int64).astype(np.uint32).view(np.int32),
+                             device=photons.device)
+        out = torch.empty(photons.shape, dtype=torch.uint16, device=photons.device)
+        cam = camera.c()
+        check(self.lib.iscu_noise_frames_dev(self.h, _ptr(photons), photons.shape[0], _ptr(fr), C.byref(cam), seed,
+                                             _ptr(out)))
+        self.synchronize()
+        return out
+
+    # -------------------------------------------------------------------------------------------- PSF
+    def psf_library_dev(self, sets, set_of_psf, defocus_nm, size=0, normalize=True, method=CZT_FP32, out=None):
+        """A PSF library (n, P, P) float32 CUDA tensor; see iscu_psf_library_dev."""
+        import torch
+        reqs = (PsfRequest * len(sets))(*[s.c() for s in sets])
+        so = np.ascontiguousarray(set_of_psf, dtype=np.uint32)
+        dz = np.ascontiguousarray(defocus_nm, dtype=np.float64)
+        P = size if size > 0 else sets[0].geometry()[0]
+        if out is None:
+            out = torch.empty((len(so), P, P), dtype=torch.float32, device=f"cuda:{self.device}")
+        check(self.lib.iscu_psf_library_dev(self.h, reqs, len(sets), _ptr(so), _ptr(dz), len(so), size,
+                                            int(normalize), method, _ptr(out)))
+        return out
+
+    def kernel_build(self, slot, req: PsfParams, method=CZT_FP32):
+        r = req.c()
+        check(self.lib.iscu_kernel_build(self.h, slot, C.byref(r), method))
+
+    def kernel_set_planes(self, slot, planes, oversampling, z_step_nm, interp=INTERP_CUBIC):
+        planes = np.ascontiguousarray(planes, dtype=np.float32)
+        nz, s, s2 = planes.shape
+        assert s == s2
+        check(self.lib.iscu_kernel_set_planes(self.h, slot, _ptr(planes), s, nz, oversampling, z_step_nm, interp))
+
+    def kernel_set_halo(self, slot, threshold):
+        check(self.lib.iscu_kernel_set_halo(self.h, slot, float(threshold)))
+
+    def kernel_info(self, slot):
+        v = [C.c_int32() for _ in range(4)]
+        check(self.lib.iscu_kernel_info(self.h, slot, *[C.byref(x) for x in v]))
+        return tuple(x.value for x in v)   # size, nz, os, bw
+
+    def kernel_planes(self, slot):
+        size, nz, _, _ = self.kernel_info(slot)
+        out = np.empty((nz, size, size), np.float32)
+        check(self.lib.iscu_kernel_get_planes(self.h, slot, _ptr(out)))
+        return out
+
+    def kernel_block_sums(self, slot):
+        _, nz, _, bw = self.kernel_info(slot)
+        out = np.empty((nz, bw, bw), np.float32)
+        check(self.lib.iscu_kernel_get_block_sums(self.h, slot, _ptr(out)))
+        return out
+
+    # -------------------------------------------------------------------------------------------- splat + noise
+    def render_frames(self, emitters, frames, camera: CameraParams | None, seed, want_photons=True, want_adu=True):
+        """Host path: emitters (EMITTER_DTYPE), frames (FRAME_DTYPE) -> (photons (n,h,w) f32 | None, adu | None)."""
+        emitters = np.ascontiguousarray(emitters, dtype=EMITTER_DTYPE)
+        frames = np.ascontiguousarray(frames, dtype=FRAME_DTYPE)
+        n = len(frames)
+        ph = np.empty((n, self.height, self.width), np.float32) if want_photons else None
+        adu = np.empty((n, self.height, self.width), np.uint16) if (want_adu and camera is not None) else None
+        cam = camera.c() if camera is not None else None
+        check(self.lib.iscu_render_frames(self.h, _ptr(emitters), len(emitters), _ptr(frames), n,
+                                          C.byref(cam) if cam is not None else None, seed, _ptr(ph), _ptr(adu)))
+        return ph, adu
+
+    def render_frames_dev(self, emitters_dev, frames_dev, n_frames, camera: CameraParams | None, seed,
+                          photons_dev=None, adu_dev=None):
+        """Device path on torch CUDA buffers (emitters: uint8 view of EMITTER_DTYPE records, frames likewise)."""
+        cam = camera.c() if camera is not None else None
+        check(self.lib.iscu_render_frames_dev(self.h, _ptr(emitters_dev), _ptr(frames_dev), n_frames,
+                                              C.byref(cam) if cam is not None else None, seed, _ptr(photons_dev),
+                                              _ptr(adu_dev)))
+
+    def render_gpu_records(self, records, frames, camera: CameraParams, seed, extras=None):
+        """GpuSimulator::RenderFrames over the reference's 64-byte records (GPU_SPLAT_EMITTER_DTYPE)."""
+        records = np.ascontiguousarray(records, dtype=GPU_SPLAT_EMITTER_DTYPE)
+        frames = np.ascontiguousarray(frames, dtype=FRAME_DTYPE)
+        n = len(frames)
+        adu = np.empty((n, self.height, self.width), np.uint16)
+        ex = _f32(extras, n * self.width * self.height) if extras is not None else None
+        cam = camera.c()
+        check(self.lib.iscu_render_gpu_records(self.h, _ptr(records), len(records), _ptr(frames), n, _ptr(ex),
+                                               C.byref(cam), seed, _ptr(adu)))
+        return adu
+
+    def collect_frame_emitters(self, slot, events, frame, width, height, pixel_size_nm, photons_per_blink,
+                               drift_x_px=0.0, drift_y_px=0.0, global_z_offset_um=0.0, illum=None, min_photons=0.0):
+        """CollectFrameEmitters (SMLMSimulation.cpp:55-101) -> EMITTER_DTYPE records of one frame."""
+        events = np.ascontiguousarray(events, dtype=BLINK_EVENT_DTYPE)
+        out = np.empty(len(events), EMITTER_DTYPE)
+        n = C.c_uint32()
+        clamped = C.c_int64(0)
+        il = _f32(illum, width * height) if illum is not None else None
+        check(self.lib.iscu_collect_frame_emitters(self.h, slot, _ptr(events), len(events), int(frame), width, height,
+                                                   pixel_size_nm, photons_per_blink, drift_x_px, drift_y_px,
+                                                   global_z_offset_um, _ptr(il), min_photons, _ptr(out), len(out),
+                                                   C.byref(n), C.byref(clamped)))
+        return out[: n.value].copy(), clamped.value
+
+    def collect_emitters(self, slot, events, bucket_start, frame0, width, height, pixel_size_nm, photons_per_blink,
+                         bucket_index=None, drift_x_px=None, drift_y_px=None, global_z_offset_um=None, bg_scale=None,
+                         illum=None, min_photons=0.0, max_out=None, out=None, frames_out=None):
+        """A batch's emitters and frame table (iscu_collect_emitters). Returns (emitters, frames, n_clamped)."""
+        events = np.ascontiguousarray(events, dtype=BLINK_EVENT_DTYPE)
+        bs = np.ascontiguousarray(bucket_start, dtype=np.uint32)
+        nf = len(bs) - 1
+        bi = None if bucket_index is None else np.ascontiguousarray(bucket_index, dtype=np.uint32)
+        if out is None:
+            out = np.empty(max_out if max_out is not None else max(1, int(bs[-1] - bs[0])), EMITTER_DTYPE)
+        if frames_out is None:
+            frames_out = np.empty(nf, FRAME_DTYPE)
+        f64 = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+        dx, dy, gz, sc = f64(drift_x_px), f64(drift_y_px), f64(global_z_offset_um), f64(bg_scale)
+        il = _f32(illum, width * height) if illum is not None else None
+        n = C.c_uint32()
+        clamped = C.c_int64(0)
+        check(self.lib.iscu_collect_emitters(self.h, slot, _ptr(events), _ptr(bi), _ptr(bs), int(frame0), nf, width,
+                                             height, pixel_size_nm, photons_per_blink, _ptr(dx), _ptr(dy), _ptr(gz),
+                                             _ptr(sc), _ptr(il), min_photons, _ptr(out), len(out), _ptr(frames_out),
+                                             C.byref(n), C.byref(clamped)))
+        return out[: n.value], frames_out, clamped.value
+
+
+def frames_table(counts, frame_ids=None, bg_scales=None):
+    """A FRAME_DTYPE table for frames whose emitters are consecutive runs of `counts` records."""
+    counts = np.asarray(counts, dtype=np.int64)
+    t = np.zeros(len(counts), FRAME_DTYPE)
+    t["em_count"] = counts
+    t["em_start"] = np.concatenate([[0], np.cumsum(counts)[:-1]]) if len(counts) else []
+    t["frame"] = np.arange(len(counts)) if frame_ids is None else frame_ids
+    t["bg_scale"] = 1.0 if bg_scales is None else bg_scales
+    return t
+
+
+__all__ = ["Engine", "CameraParams", "PsfParams", "IscuError", "generate_camera_maps", "frames_table",
+           "EMITTER_DTYPE", "FRAME_DTYPE", "GPU_SPLAT_EMITTER_DTYPE", "BLINK_EVENT_DTYPE", "CZT_FP32", "CZT_TF32X3",
+           "INTERP_NEAREST", "INTERP_LINEAR", "INTERP_CUBIC"]

@@ -1,0 +1,114 @@
+"""Seeded synthetic workloads with the shapes of the engine's benchmark configurations.
+
+Every random property is a pure function of (seed, address) through the engine's own pcg4d hash
+(core/src/rng.h:37-41 HashUnit): static site properties at pcg4d(seed ^ salt, site, 0, purpose), per-frame properties
+at pcg4d(seed, site, frame, purpose) -- the DYE_CH-style channel scheme of the reference's world core
+(core/src/dyes.h:33-57). Camera maps come from std::mt19937_64(seed) in the order offset, gain, read noise and the
+noise stream from seed ^ 0x9E3779B9, as the reference's movie setup does (ScopeMovie.cpp:980-988).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from .engine import BLINK_EVENT_DTYPE, INTERP_CUBIC, CameraParams, PsfParams
+
+SITE_SALT = 0x5157E5
+M32 = np.uint64(0xFFFFFFFF)
+
+
+def pcg4d(a, b, c, d):
+    """Vectorized pcg4d (SMLMCounterRng.h:37-56) on uint32 arrays."""
+    a, b, c, d = (np.asarray(x, dtype=np.uint64) & M32 for x in np.broadcast_arrays(a, b, c, d))
+    mul, inc = np.uint64(1664525), np.uint64(1013904223)
+    a = (a * mul + inc) & M32
+    b = (b * mul + inc) & M32
+    c = (c * mul + inc) & M32
+    d = (d * mul + inc) & M32
+    for rnd in range(2):
+        a = (a + b * d) & M32
+        b = (b + c * a) & M32
+        c = (c + a * b) & M32
+        d = (d + b * c) & M32
+        if rnd == 0:
+            a ^= a >> np.uint64(16)
+            b ^= b >> np.uint64(16)
+            c ^= c >> np.uint64(16)
+            d ^= d >> np.uint64(16)
+    return a, b, c, d
+
+
+def hash_unit(seed, cx, cy, k):
+    """HashUnit (core/src/rng.h:37-41): ((pcg4d(...).a >> 9) + 0.5) * 2^-23."""
+    a = pcg4d(seed, cx, cy, k)[0]
+    return ((a >> np.uint64(9)).astype(np.float64) + 0.5) * 1.1920928955078125e-7
+
+
+def hash_normal(seed, cx, cy, k0):
+    u1 = hash_unit(seed, cx, cy, k0)
+    u2 = hash_unit(seed, cx, cy, k0 + 1)
+    return np.sqrt(-2.0 * np.log(u1)) * np.cos(2.0 * np.pi * u2)
+
+
+@dataclass
+class SmlmMovie:
+    """A blink movie: events in frame order with per-frame buckets, and what renders it."""
+    width: int
+    height: int
+    frames: int
+    pixel_nm: float
+    photons_per_blink: float
+    background: float
+    events: np.ndarray          # BLINK_EVENT_DTYPE, frame-major
+    bucket_start: np.ndarray    # frames + 1 offsets into events
+    psf: PsfParams
+    camera: CameraParams
+    map_seed: int
+    offset_mean: float
+    offset_std: float
+    gain_nominal: float
+    gain_std_fraction: float
+    read_noise_nominal: float
+    read_noise_std_fraction: float
+    noise_seed: int
+
+    @property
+    def n_events(self) -> int:
+        return len(self.events)
+
+
+def smlm_dstorm(seed: int = 42, sites: int = 4000, frames: int = 200, size: int = 128, pixel_nm: float = 108.0,
+                p_on: float = 0.04, median_photons: float = 2000.0, sigma_log: float = 0.5, z_half_nm: float = 600.0,
+                frame0: int = 0) -> SmlmMovie:
+    """The plain dSTORM movie: 128 x 128 px sCMOS at 108 nm, 200 frames, 4,000 sites uniform over the field with
+    z uniform in [-600, 600] nm, each ON in a frame with probability 0.04 (about 160 per frame), photons lognormal
+    (median 2000, sigma_log 0.5); background 20 photons/px; Gibson-Lanni PSF, NA 1.45 oil, 670 nm, 64 x 64 pupil,
+    chirp-Z to a 4x-oversampled 32 x 32 px kernel (129^2 samples), 49 planes 25 nm apart, Catmull-Rom splat; offset
+    N(100, 2) ADU, gain N(2.2, 0.1) e-/ADU, read noise N(1.5, 0.3) e-; QE 1."""
+    s = np.arange(sites, dtype=np.uint64)
+    st = np.uint64((seed ^ SITE_SALT) & 0xFFFFFFFF)
+    x_px = size * hash_unit(st, s, 0, 0)
+    y_px = size * hash_unit(st, s, 0, 1)
+    z_nm = -z_half_nm + 2.0 * z_half_nm * hash_unit(st, s, 0, 2)
+    f = np.arange(frame0, frame0 + frames, dtype=np.uint64)
+    F, S = np.meshgrid(f, s, indexing="ij")
+    on = hash_unit(seed, S, F, 0) < p_on
+    photons = median_photons * np.exp(sigma_log * hash_normal(seed, S, F, 1))
+    fi, si = np.nonzero(on)                     # frame-major, site order within a frame
+    ev = np.zeros(len(fi), BLINK_EVENT_DTYPE)
+    ev["x_um"] = x_px[si] * (pixel_nm / 1000.0)
+    ev["y_um"] = y_px[si] * (pixel_nm / 1000.0)
+    ev["z_nm"] = z_nm[si]
+    ev["t_start"] = (frame0 + fi).astype(np.float64)
+    ev["t_end"] = ev["t_start"] + 1.0
+    ev["brightness"] = photons[fi, si] / median_photons
+    ev["excite"] = 1.0
+    counts = np.bincount(fi, minlength=frames)
+    bucket = np.concatenate([[0], np.cumsum(counts)]).astype(np.uint32)
+    psf = PsfParams(wavelength_nm=670.0, na=1.45, immersion_index=1.518, sample_index=1.518,
+                    working_distance_um=150.0, sample_depth_nm=0.0, pixel_size_nm=pixel_nm, oversampling=4,
+                    kernel_half_width_px=16, nz=49, z_step_nm=25.0, pupil_samples=64, interp=INTERP_CUBIC)
+    cam = CameraParams(quantum_efficiency=1.0, dark_electrons=0.0, gain=2.2, read_noise_e=1.5, emccd=False)
+    return SmlmMovie(size, size, frames, pixel_nm, median_photons, 20.0, ev, bucket, psf, cam, seed, 100.0, 2.0, 2.2,
+                     0.1 / 2.2, 1.5, 0.2, (seed ^ 0x9E3779B9) & 0xFFFFFFFF)

@@ -1,0 +1,356 @@
+"""TEST INFRASTRUCTURE -- the oracle's Python face. Used only by tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline leg, as the checker; the product never imports it.
+
+Two checkers over the same C ABI types (include/iscu.h):
+  Oracle     liboracle.so: the CPU restatement of the reference's algorithms (iscoracle.cpp), always available.
+  Reference  _ref/libiscref.so: the reference's own hot-path sources compiled here (Makefile), when built.
+Plus the float64 FFT convolution that checks the widefield path (numpy).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libiscref.so")
+REF_TREE = "/root/reference"
+
+vp = C.c_void_p
+
+
+def build(reference: bool = True) -> None:
+    """Builds liboracle.so, and _ref/libiscref.so when the reference tree is present."""
+    targets = ["oracle"] + (["ref"] if reference and os.path.isdir(REF_TREE) else [])
+    subprocess.run(["make", "-s", "-C", HERE, "-j8", *targets], check=True)
+
+
+def _p(a):
+    if a is None:
+        return None
+    assert isinstance(a, np.ndarray) and a.flags.c_contiguous
+    return C.c_void_p(a.ctypes.data)
+
+
+def _struct_ptr(s):
+    return C.byref(s) if s is not None else None
+
+
+class Oracle:
+    """The CPU restatement (liboracle.so)."""
+
+    def __init__(self):
+        if not os.path.exists(ORACLE_SO):
+            build(reference=False)
+        L = C.CDLL(ORACLE_SO)
+        u32, i32, f64, i64 = C.c_uint32, C.c_int32, C.c_double, C.c_int64
+        L.or_pcg4d.argtypes = [u32, u32, u32, u32, vp]
+        L.or_hash_unit.argtypes = [u32, i32, i32, u32]
+        L.or_hash_unit.restype = f64
+        L.or_hash_stream.argtypes = [u32, i32, i32, u32, u32, vp]
+        L.or_counter_uniforms.argtypes = [u32, u32, u32, u32, u32, vp]
+        L.or_camera_maps.argtypes = [u32, u32, C.c_uint64, f64, f64, f64, f64, f64, f64, u32, u32, vp, vp, vp]
+        L.or_noise_chain.argtypes = [vp, u32, u32, vp, vp, vp, vp, u32, u32, u32, vp]
+        L.or_psf_geometry.argtypes = [vp, vp, vp, vp]
+        L.or_psf_planes.argtypes = [vp, C.c_int, vp, C.c_int, C.c_int, vp]
+        L.or_block_sums.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp]
+        L.or_render_frame.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp, u32, u32, u32,
+                                      f64, vp, vp, f64, vp]
+        L.or_collect_frame_emitters.argtypes = [vp, u32, i64, f64, f64, f64, f64, f64, C.c_int, f64, C.c_int, f64,
+                                                vp]
+        L.or_collect_frame_emitters.restype = u32
+        self.L = L
+
+    def pcg4d(self, a, b, c, d):
+        out = np.zeros(4, np.uint32)
+        self.L.or_pcg4d(a, b, c, d, _p(out))
+        return out
+
+    def hash_unit(self, seed, cx, cy, k):
+        return self.L.or_hash_unit(seed, cx, cy, k)
+
+    def hash_stream(self, seed, cx, cy, base, n):
+        out = np.zeros(n, np.float64)
+        self.L.or_hash_stream(seed, cx, cy, base, n, _p(out))
+        return out
+
+    def counter_uniforms(self, seed, frame, pixel0, npix, per):
+        out = np.zeros((npix, per), np.float64)
+        self.L.or_counter_uniforms(seed, frame, pixel0, npix, per, _p(out))
+        return out
+
+    def camera_maps(self, w, h, seed, off_mean, off_std, gain, gain_frac, rn, rn_frac, keep_y0=0, keep_rows=0):
+        rows = min(keep_rows, max(0, h - keep_y0)) if keep_rows else h
+        o, g, r = (np.zeros(w * rows, np.float32) for _ in range(3))
+        self.L.or_camera_maps(w, h, seed, off_mean, off_std, gain, gain_frac, rn, rn_frac, keep_y0, keep_rows, _p(o),
+                              _p(g), _p(r))
+        return o, g, r
+
+    def noise_chain(self, photons, camera, offset, gain, read_noise, seed, frame, pixel_base=0):
+        photons = np.ascontiguousarray(photons, np.float32)
+        h, w = photons.shape
+        out = np.zeros((h, w), np.uint16)
+        cam = camera.c()
+        f = lambda a: None if a is None else np.ascontiguousarray(a, np.float32)
+        o, g, r = f(offset), f(gain), f(read_noise)
+        self.L.or_noise_chain(_p(photons), w, h, C.byref(cam), _p(o), _p(g), _p(r), seed, frame, pixel_base, _p(out))
+        return out
+
+    def psf_geometry(self, req):
+        r = req.c()
+        s, nz, m = C.c_int(), C.c_int(), C.c_int()
+        self.L.or_psf_geometry(C.byref(r), C.byref(s), C.byref(nz), C.byref(m))
+        return s.value, nz.value, m.value
+
+    def psf_planes(self, req, defocus_m, size=0, normalize=False):
+        r = req.c()
+        P = size if size > 0 else self.psf_geometry(req)[0]
+        dz = np.ascontiguousarray(defocus_m, np.float64)
+        out = np.zeros((len(dz), P, P), np.float64)
+        self.L.or_psf_planes(C.byref(r), size, _p(dz), len(dz), int(normalize), _p(out))
+        return out
+
+    def stack_defocus_m(self, req):
+        """The reference's plane defocus: zStep * 1e-9 * (z - (nz-1)/2)."""
+        _, nz, _ = self.psf_geometry(req)
+        return np.array([req.z_step_nm * 1e-9 * (z - (nz - 1) / 2.0) for z in range(nz)])
+
+    def block_sums(self, planes, os_):
+        planes = np.ascontiguousarray(planes, np.float32)
+        nz, n, _ = planes.shape
+        bw = n + os_ - 1
+        out = np.zeros((nz, bw, bw), np.float32)
+        self.L.or_block_sums(_p(planes), n, os_, nz, _p(out))
+        return out
+
+    def render_frame(self, sums, os_, size, interp, emitters, w, h, flat_bg, bg_map=None, illum=None, bg_scale=1.0,
+                     span_lo=None, span_hi=None):
+        sums = np.ascontiguousarray(sums, np.float32)
+        nz, bw, _ = sums.shape
+        emitters = np.ascontiguousarray(emitters)
+        out = np.zeros((h, w), np.float32)
+        f = lambda a, t: None if a is None else np.ascontiguousarray(a, t)
+        self.L.or_render_frame(_p(sums), nz, bw, os_, size, interp, _p(f(span_lo, np.int16)), _p(f(span_hi, np.int16)),
+                               _p(emitters), len(emitters), w, h, flat_bg, _p(f(bg_map, np.float32)),
+                               _p(f(illum, np.float32)), bg_scale, _p(out))
+        return out
+
+    def collect_frame_emitters(self, events, frame, pixel_nm, per_blink, nz, z_step_nm, drift_x=0.0, drift_y=0.0,
+                               global_z_um=0.0, slot=0, min_photons=0.0):
+        from insiliscope_b200.engine import EMITTER_DTYPE
+        events = np.ascontiguousarray(events)
+        out = np.zeros(len(events), EMITTER_DTYPE)
+        n = self.L.or_collect_frame_emitters(_p(events), len(events), frame, pixel_nm, per_blink, drift_x, drift_y,
+                                             global_z_um, nz, z_step_nm, slot, min_photons, _p(out))
+        return out[:n].copy()
+
+
+class Reference:
+    """The reference's own functions, compiled from its sources (oracle/Makefile -> _ref/libiscref.so)."""
+
+    @staticmethod
+    def available() -> bool:
+        return os.path.exists(REF_SO)
+
+    def __init__(self):
+        if not os.path.exists(REF_SO):
+            raise RuntimeError("the reference harness is not built (oracle/_ref/libiscref.so)")
+        L = C.CDLL(REF_SO)
+        u32, i32, f64, i64 = C.c_uint32, C.c_int32, C.c_double, C.c_int64
+        L.ref_last_error.restype = C.c_char_p
+        L.ref_set_threads.argtypes = [C.c_uint]
+        L.ref_threads.restype = C.c_uint
+        L.ref_pcg4d.argtypes = [u32, u32, u32, u32, vp]
+        L.ref_hash_unit.argtypes = [u32, i32, i32, u32]
+        L.ref_hash_unit.restype = f64
+        L.ref_hash_stream.argtypes = [u32, i32, i32, u32, u32, vp]
+        L.ref_counter_uniforms.argtypes = [u32, u32, u32, u32, u32, vp]
+        L.ref_counter_poisson.argtypes = [u32, u32, u32, f64]
+        L.ref_counter_poisson.restype = f64
+        L.ref_counter_gamma.argtypes = [u32, u32, u32, f64]
+        L.ref_counter_gamma.restype = f64
+        L.ref_camera_maps.argtypes = [u32, u32, C.c_uint64, f64, f64, f64, f64, f64, f64, u32, u32, vp, vp, vp]
+        L.ref_noise_chain.argtypes = [vp, u32, u32, vp, vp, vp, vp, u32, u32, u32, C.c_int, vp]
+        L.ref_psf_geometry.argtypes = [vp, vp]
+        L.ref_zernike_planes.argtypes = [vp, vp]
+        L.ref_kernel_build.argtypes = [vp]
+        L.ref_kernel_build.restype = vp
+        L.ref_kernel_from_planes.argtypes = [vp, C.c_int, C.c_int, C.c_int, f64, C.c_int]
+        L.ref_kernel_from_planes.restype = vp
+        L.ref_kernel_halo.argtypes = [vp, f64]
+        L.ref_kernel_halo.restype = vp
+        L.ref_kernel_free.argtypes = [vp]
+        L.ref_kernel_info.argtypes = [vp, vp, vp, vp, vp]
+        L.ref_kernel_planes.argtypes = [vp, vp]
+        L.ref_kernel_block_sums.argtypes = [vp, vp]
+        L.ref_kernel_spans.argtypes = [vp, vp, vp, vp]
+        L.ref_nearest_z.argtypes = [vp, f64]
+        L.ref_render_photon_image.argtypes = [vp, vp, u32, i64, u32, u32, f64, f64, f64, f64, f64, f64, vp, vp, f64,
+                                              f64, C.c_int, vp]
+        L.ref_collect_gpu_emitters.argtypes = [vp, vp, u32, i64, u32, u32, f64, f64, f64, f64, f64, C.c_int, f64, vp,
+                                               u32]
+        L.ref_collect_gpu_emitters.restype = u32
+        L.ref_render_movie.argtypes = [vp, vp, u32, u32, u32, u32, u32, f64, f64, f64, vp, vp, vp, vp, u32, vp, vp]
+        L.ref_render_movie.restype = f64
+        self.L = L
+
+    def set_threads(self, n):
+        self.L.ref_set_threads(n)
+
+    def threads(self):
+        return self.L.ref_threads()
+
+    def pcg4d(self, a, b, c, d):
+        out = np.zeros(4, np.uint32)
+        self.L.ref_pcg4d(a, b, c, d, _p(out))
+        return out
+
+    def hash_unit(self, seed, cx, cy, k):
+        return self.L.ref_hash_unit(seed, cx, cy, k)
+
+    def hash_stream(self, seed, cx, cy, base, n):
+        out = np.zeros(n, np.float64)
+        self.L.ref_hash_stream(seed, cx, cy, base, n, _p(out))
+        return out
+
+    def counter_uniforms(self, seed, frame, pixel0, npix, per):
+        out = np.zeros((npix, per), np.float64)
+        self.L.ref_counter_uniforms(seed, frame, pixel0, npix, per, _p(out))
+        return out
+
+    def camera_maps(self, w, h, seed, off_mean, off_std, gain, gain_frac, rn, rn_frac, keep_y0=0, keep_rows=0):
+        rows = min(keep_rows, max(0, h - keep_y0)) if keep_rows else h
+        o, g, r = (np.zeros(w * rows, np.float32) for _ in range(3))
+        self.L.ref_camera_maps(w, h, seed, off_mean, off_std, gain, gain_frac, rn, rn_frac, keep_y0, keep_rows, _p(o),
+                               _p(g), _p(r))
+        return o, g, r
+
+    def noise_chain(self, photons, camera, offset, gain, read_noise, seed, frame, pixel_base=0, parallel=False):
+        photons = np.ascontiguousarray(photons, np.float32)
+        h, w = photons.shape
+        out = np.zeros((h, w), np.uint16)
+        cam = camera.c()
+        f = lambda a: None if a is None else np.ascontiguousarray(a, np.float32)
+        o, g, r = f(offset), f(gain), f(read_noise)
+        self.L.ref_noise_chain(_p(photons), w, h, C.byref(cam), _p(o), _p(g), _p(r), seed, frame, pixel_base,
+                               int(parallel), _p(out))
+        return out
+
+    def zernike_planes(self, req):
+        r = req.c()
+        size, nz, _ = _geometry(req)
+        out = np.zeros((nz, size, size), np.float32)
+        if self.L.ref_zernike_planes(C.byref(r), _p(out)) != 0:
+            raise RuntimeError(self.L.ref_last_error().decode())
+        return out
+
+    def kernel(self, req=None, planes=None, os_=4, z_step_nm=25.0, interp=2):
+        return RefKernel(self, req, planes, os_, z_step_nm, interp)
+
+
+def _geometry(req):
+    return Oracle().psf_geometry(req)
+
+
+class RefKernel:
+    """A sim::PsfKernelCache in the reference harness."""
+
+    def __init__(self, ref: Reference, req=None, planes=None, os_=4, z_step_nm=25.0, interp=2, handle=None):
+        self.ref = ref
+        L = ref.L
+        if handle is not None:
+            self.h = handle
+        elif req is not None:
+            r = req.c()
+            self.h = L.ref_kernel_build(C.byref(r))
+            if not self.h:
+                raise RuntimeError(L.ref_last_error().decode())
+        else:
+            planes = np.ascontiguousarray(planes, np.float32)
+            nz, s, _ = planes.shape
+            self.h = L.ref_kernel_from_planes(_p(planes), s, nz, os_, z_step_nm, interp)
+
+    def __del__(self):
+        try:
+            self.ref.L.ref_kernel_free(self.h)
+        except Exception:
+            pass
+
+    def info(self):
+        v = [C.c_int() for _ in range(4)]
+        self.ref.L.ref_kernel_info(self.h, *[C.byref(x) for x in v])
+        return tuple(x.value for x in v)
+
+    def planes(self):
+        size, nz, _, _ = self.info()
+        out = np.zeros((nz, size, size), np.float32)
+        self.ref.L.ref_kernel_planes(self.h, _p(out))
+        return out
+
+    def block_sums(self):
+        _, nz, _, bw = self.info()
+        out = np.zeros((nz, bw, bw), np.float32)
+        self.ref.L.ref_kernel_block_sums(self.h, _p(out))
+        return out
+
+    def halo(self, threshold):
+        return RefKernel(self.ref, handle=self.ref.L.ref_kernel_halo(self.h, threshold))
+
+    def spans(self):
+        size, nz, os_, _ = self.info()
+        cam = ((size - 1) // 2) // os_
+        lo = np.zeros(nz * (2 * cam + 1), np.int16)
+        hi = np.zeros_like(lo)
+        r2 = np.zeros(nz, np.int32)
+        rc = self.ref.L.ref_kernel_spans(self.h, _p(lo), _p(hi), _p(r2))
+        return None if rc < 0 else (lo, hi, r2)
+
+    def nearest_z(self, z_um):
+        return self.ref.L.ref_nearest_z(self.h, z_um)
+
+    def render_photon_image(self, events, frame, w, h, pixel_nm, per_blink, bg, drift_x=0.0, drift_y=0.0,
+                            global_z=0.0, illum=None, bg_map=None, bg_scale=1.0, min_photons=0.0, parallel=False):
+        events = np.ascontiguousarray(events)
+        out = np.zeros((h, w), np.float32)
+        f = lambda a: None if a is None else np.ascontiguousarray(a, np.float32)
+        self.ref.L.ref_render_photon_image(self.h, _p(events), len(events), frame, w, h, pixel_nm, per_blink, bg,
+                                           drift_x, drift_y, global_z, _p(f(illum)), _p(f(bg_map)), bg_scale,
+                                           min_photons, int(parallel), _p(out))
+        return out
+
+    def collect_gpu_emitters(self, events, frame, w, h, pixel_nm, per_blink, drift_x=0.0, drift_y=0.0, global_z=0.0,
+                             kernel=0, min_photons=0.0):
+        from insiliscope_b200.engine import GPU_SPLAT_EMITTER_DTYPE
+        events = np.ascontiguousarray(events)
+        out = np.zeros(len(events), GPU_SPLAT_EMITTER_DTYPE)
+        n = self.ref.L.ref_collect_gpu_emitters(self.h, _p(events), len(events), frame, w, h, pixel_nm, per_blink,
+                                                drift_x, drift_y, global_z, kernel, min_photons, _p(out), len(out))
+        return out[:n].copy()
+
+    def render_movie(self, events, frame0, n_frames, w, h, pixel_nm, per_blink, bg, camera, offset, gain,
+                     read_noise, seed, want_photons=False, want_adu=True):
+        """The reference's frame loop (frames in parallel on its pool). Returns (seconds, photons, adu)."""
+        events = np.ascontiguousarray(events)
+        ph = np.zeros((n_frames, h, w), np.float32) if want_photons else None
+        adu = np.zeros((n_frames, h, w), np.uint16) if want_adu else None
+        cam = camera.c()
+        f = lambda a: None if a is None else np.ascontiguousarray(a, np.float32)
+        t = self.ref.L.ref_render_movie(self.h, _p(events), len(events), frame0, n_frames, w, h, pixel_nm, per_blink,
+                                        bg, C.byref(cam), _p(f(offset)), _p(f(gain)), _p(f(read_noise)), seed,
+                                        _p(ph), _p(adu))
+        return t, ph, adu
+
+
+def fft_convolve_same_f64(volume: np.ndarray, psf: np.ndarray) -> np.ndarray:
+    """Linear 3D convolution of volume (nz, ny, nx) with psf (kz, ky, kx) centred on (kz//2, ky//2, kx//2), cropped
+    to the volume, in float64 (the widefield mean-field focus series' oracle)."""
+    v = np.asarray(volume, np.float64)
+    k = np.asarray(psf, np.float64)
+    shape = [a + b - 1 for a, b in zip(v.shape, k.shape)]
+    F = np.fft.rfftn(v, shape) * np.fft.rfftn(k, shape)
+    full = np.fft.irfftn(F, shape)
+    sl = tuple(slice(kk // 2, kk // 2 + n) for kk, n in zip(k.shape, v.shape))
+    return full[sl]

@@ -1,0 +1,414 @@
+// TEST INFRASTRUCTURE -- the reference itself, as a checker and as the timed CPU baseline. Never part of the product.
+//
+// A C-ABI harness over inSiliScope's own C++ render engine, compiled together with the reference's source files
+// where they lie (oracle/Makefile; output oracle/_ref/libiscref.so). It drives the hot-path functions directly with
+// plain arrays, the way the reference's GPU self-check does (adapter/inSiliScope/Simulation/SplatGpu.cpp:464-540):
+//   ComputeZernikePsfPlanes / BuildZernikePsfKernelCache (ZernikePsf.cpp:160, :382), block sums
+//   (PsfGeneratorBridge.cpp:1069), WithHaloCut (:1186), RenderPhotonImage (SMLMSimulation.cpp:103),
+//   CollectGpuEmitters (:219), ApplyNoiseChain (SMLMNoise.cpp:142), the camera maps (SMLMNoise.cpp:89-140), the
+//   counter RNG (SMLMCounterRng.h, core/src/rng.h), and a movie loop shaped like FluorescenceMovie::Render's
+//   (ScopeMovie.cpp:7267, :7649: frames in parallel on the reference's own thread pool, ParallelFor).
+#include "PsfGeneratorBridge.h"
+#include "Parallel.h"
+#include "SMLMCounterRng.h"
+#include "SMLMNoise.h"
+#include "SMLMSimulation.h"
+#include "SMLMZernike.h"
+#include "ZernikePsf.h"
+#include "rng.h"
+
+#include "../include/iscu.h"
+
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_err;
+
+std::string FullPrecisionZernike(const double* z)
+{
+   std::string s;
+   char buf[64];
+   for (int j = 0; j < 28; ++j)
+   {
+      std::snprintf(buf, sizeof(buf), "%s%.17g", j ? "," : "", z[j]);
+      s += buf;
+   }
+   return s;
+}
+
+sim::PsfGeneratorRequest ToRequest(const iscu_psf_request& r)
+{
+   sim::PsfGeneratorRequest q;
+   q.model = sim::PsfModelKind::GibsonLanniZernike;
+   q.wavelengthNm = r.wavelength_nm;
+   q.na = r.na;
+   q.immersionIndex = r.immersion_index;
+   q.sampleIndex = r.sample_index;
+   q.workingDistanceUm = r.working_distance_um;
+   q.sampleDepthNm = r.sample_depth_nm;
+   q.pixelSizeNm = r.pixel_size_nm;
+   q.zernikeCoefficients = FullPrecisionZernike(r.zernike);
+   q.maskType = r.mask_double_helix ? sim::PsfMaskType::DoubleHelix : sim::PsfMaskType::None;
+   q.maskModes = r.mask_modes;
+   q.maskWaist = r.mask_waist;
+   q.oversampling = r.oversampling;
+   q.kernelHalfWidthPx = r.kernel_half_width_px;
+   q.nz = r.nz;
+   q.zStepNm = r.z_step_nm;
+   q.pupilSamples = r.pupil_samples;
+   q.interpMode = static_cast<sim::PsfInterpMode>(r.interp);
+   return q;
+}
+
+sim::CameraNoiseParams ToCamera(const iscu_camera& c)
+{
+   sim::CameraNoiseParams p;
+   p.quantumEfficiency = c.quantum_efficiency;
+   p.darkCurrentElectrons = c.dark_electrons;
+   p.gainPhotonsPerAdu = c.gain;
+   p.readNoiseElectrons = c.read_noise_e;
+   p.emccd = c.emccd != 0;
+   p.bitDepth = c.bit_depth;
+   p.emGain = c.em_gain;
+   p.cicElectrons = c.cic_electrons;
+   return p;
+}
+
+std::vector<sim::BlinkEvent> ToEvents(const iscu_blink_event* ev, uint32_t n)
+{
+   std::vector<sim::BlinkEvent> out(n);
+   for (uint32_t i = 0; i < n; ++i)
+   {
+      out[i].xUm = ev[i].x_um;
+      out[i].yUm = ev[i].y_um;
+      out[i].zNm = ev[i].z_nm;
+      out[i].tStart = ev[i].t_start;
+      out[i].tEnd = ev[i].t_end;
+      out[i].brightness = ev[i].brightness;
+      out[i].excite = ev[i].excite;
+   }
+   return out;
+}
+
+struct Maps
+{
+   sim::PixelOffsetMap off;
+   sim::PixelGainMap gain;
+   sim::PixelReadNoiseMap rn;
+};
+
+void FillMaps(Maps& m, unsigned w, unsigned h, const float* off, const float* gain, const float* rn)
+{
+   const size_t n = static_cast<size_t>(w) * h;
+   if (off)
+   {
+      m.off.width = w;
+      m.off.height = h;
+      m.off.offset.assign(off, off + n);
+   }
+   if (gain)
+   {
+      m.gain.width = w;
+      m.gain.height = h;
+      m.gain.gainPhotonsPerAdu.assign(gain, gain + n);
+   }
+   if (rn)
+   {
+      m.rn.width = w;
+      m.rn.height = h;
+      m.rn.readNoiseElectrons.assign(rn, rn + n);
+   }
+}
+
+} // namespace
+
+extern "C" {
+
+const char* ref_last_error(void) { return g_err.c_str(); }
+
+void ref_set_threads(unsigned n) { sim::ParallelThreadCap().store(n); }
+unsigned ref_threads(void) { return sim::HardwareThreads(); }
+
+// ------------------------------------------------------------------------------------------- RNG
+void ref_pcg4d(uint32_t a, uint32_t b, uint32_t c, uint32_t d, uint32_t* out)
+{
+   sim::Pcg4d(a, b, c, d);
+   out[0] = a;
+   out[1] = b;
+   out[2] = c;
+   out[3] = d;
+}
+
+double ref_hash_unit(uint32_t seed, int32_t cx, int32_t cy, uint32_t k) { return isc::HashUnit(seed, cx, cy, k); }
+
+void ref_hash_stream(uint32_t seed, int32_t cx, int32_t cy, uint32_t base, uint32_t n, double* out)
+{
+   isc::HashStream hs(seed, cx, cy, base);
+   for (uint32_t i = 0; i < n; ++i)
+      out[i] = hs.Next();
+}
+
+void ref_counter_uniforms(uint32_t seed, uint32_t frame, uint32_t pixel0, uint32_t npix, uint32_t per, double* out)
+{
+   sim::CounterRng u(seed, frame);
+   for (uint32_t i = 0; i < npix; ++i)
+   {
+      u.Pixel(pixel0 + i);
+      for (uint32_t j = 0; j < per; ++j)
+         out[static_cast<size_t>(i) * per + j] = u.Uniform();
+   }
+}
+
+double ref_counter_poisson(uint32_t seed, uint32_t frame, uint32_t pixel, double l)
+{
+   sim::CounterRng u(seed, frame);
+   u.Pixel(pixel);
+   return sim::CounterPoisson(l, u);
+}
+
+double ref_counter_gamma(uint32_t seed, uint32_t frame, uint32_t pixel, double k)
+{
+   sim::CounterRng u(seed, frame);
+   u.Pixel(pixel);
+   return sim::CounterGamma(k, u);
+}
+
+// ------------------------------------------------------------------------------------------- camera
+void ref_camera_maps(uint32_t w, uint32_t h, uint64_t seed, double offMean, double offStd, double gainNom,
+                     double gainFrac, double rnNom, double rnFrac, uint32_t keepY0, uint32_t keepRows, float* off,
+                     float* gain, float* rn)
+{
+   std::mt19937_64 rng(seed);
+   sim::PixelOffsetMap o;
+   sim::PixelGainMap g;
+   sim::PixelReadNoiseMap r;
+   o.Generate(w, h, offMean, offStd, rng, keepY0, keepRows);
+   g.Generate(w, h, gainNom, gainFrac, rng, keepY0, keepRows);
+   r.Generate(w, h, rnNom, rnFrac, rng, keepY0, keepRows);
+   std::memcpy(off, o.offset.data(), o.offset.size() * sizeof(float));
+   std::memcpy(gain, g.gainPhotonsPerAdu.data(), g.gainPhotonsPerAdu.size() * sizeof(float));
+   std::memcpy(rn, r.readNoiseElectrons.data(), r.readNoiseElectrons.size() * sizeof(float));
+}
+
+// ApplyNoiseChain on one frame. off/gain/rn: w*h or NULL.
+void ref_noise_chain(const float* photons, uint32_t w, uint32_t h, const iscu_camera* cam, const float* off,
+                     const float* gain, const float* rn, uint32_t seed, uint32_t frame, uint32_t pixelBase,
+                     int parallel, uint16_t* out)
+{
+   Maps m;
+   FillMaps(m, w, h, off, gain, rn);
+   const std::vector<float> img(photons, photons + static_cast<size_t>(w) * h);
+   std::vector<uint16_t> adu;
+   sim::ApplyNoiseChain(img, adu, w, h, ToCamera(*cam), m.off, m.gain, m.rn, seed, frame, parallel != 0, pixelBase);
+   std::memcpy(out, adu.data(), adu.size() * sizeof(uint16_t));
+}
+
+// ------------------------------------------------------------------------------------------- PSF
+int ref_psf_geometry(const iscu_psf_request* r, int* M)
+{
+   *M = sim::ZernikePupilSamples(ToRequest(*r));
+   return 0;
+}
+
+// ComputeZernikePsfPlanes: raw |E|^2 planes (nz * size * size floats).
+int ref_zernike_planes(const iscu_psf_request* r, float* out)
+{
+   std::vector<std::vector<float>> planes;
+   if (!sim::ComputeZernikePsfPlanes(ToRequest(*r), planes, g_err))
+      return 1;
+   size_t o = 0;
+   for (const auto& p : planes)
+   {
+      std::memcpy(out + o, p.data(), p.size() * sizeof(float));
+      o += p.size();
+   }
+   return 0;
+}
+
+void* ref_kernel_build(const iscu_psf_request* r)
+{
+   auto* c = new sim::PsfKernelCache();
+   if (!sim::BuildZernikePsfKernelCache(ToRequest(*r), *c, g_err))
+   {
+      delete c;
+      return nullptr;
+   }
+   c->PrepareSplat();
+   return c;
+}
+
+// A kernel cache from planes made elsewhere (sum-1 expected), as ComputePsfKernelCache fills one.
+void* ref_kernel_from_planes(const float* planes, int size, int nz, int os, double zStepNm, int interp)
+{
+   auto* c = new sim::PsfKernelCache();
+   c->oversampling = os;
+   c->halfWidthOversampled = (size - 1) / 2;
+   c->sizeOversampled = size;
+   c->nz = nz;
+   c->zStepNm = zStepNm;
+   c->interpMode = static_cast<sim::PsfInterpMode>(interp);
+   c->blockSumWidth = size + os - 1;
+   sim::PsfKernelPlanes d;
+   d.planes.resize(static_cast<size_t>(nz));
+   for (int z = 0; z < nz; ++z)
+      d.planes[static_cast<size_t>(z)].assign(planes + static_cast<size_t>(z) * size * size,
+                                              planes + static_cast<size_t>(z + 1) * size * size);
+   c->SetData(std::move(d));
+   c->valid = true;
+   c->PrepareSplat();
+   return c;
+}
+
+void* ref_kernel_halo(void* h, double threshold)
+{
+   auto* c = new sim::PsfKernelCache(sim::WithHaloCut(*static_cast<sim::PsfKernelCache*>(h), threshold));
+   return c;
+}
+
+void ref_kernel_free(void* h) { delete static_cast<sim::PsfKernelCache*>(h); }
+
+void ref_kernel_info(void* h, int* size, int* nz, int* os, int* bw)
+{
+   const auto* c = static_cast<sim::PsfKernelCache*>(h);
+   *size = c->sizeOversampled;
+   *nz = c->nz;
+   *os = c->oversampling;
+   *bw = c->blockSumWidth;
+}
+
+void ref_kernel_planes(void* h, float* out)
+{
+   const auto* c = static_cast<sim::PsfKernelCache*>(h);
+   size_t o = 0;
+   for (const auto& p : c->Planes())
+   {
+      std::memcpy(out + o, p.data(), p.size() * sizeof(float));
+      o += p.size();
+   }
+}
+
+void ref_kernel_block_sums(void* h, float* out)
+{
+   const auto* c = static_cast<sim::PsfKernelCache*>(h);
+   size_t o = 0;
+   for (int z = 0; z < c->nz; ++z)
+   {
+      const std::vector<float> b = c->BlockSums(z).RowMajor();
+      std::memcpy(out + o, b.data(), b.size() * sizeof(float));
+      o += b.size();
+   }
+}
+
+// PsfHaloSpans of a halo-cut cache: lo/hi (nz * (2 camRad + 1)), radius2 (nz). Returns camRad, or -1 without a cut.
+int ref_kernel_spans(void* h, int16_t* lo, int16_t* hi, int32_t* radius2)
+{
+   const auto* c = static_cast<sim::PsfKernelCache*>(h);
+   if (!c->halo)
+      return -1;
+   std::memcpy(lo, c->halo->lo.data(), c->halo->lo.size() * sizeof(int16_t));
+   std::memcpy(hi, c->halo->hi.data(), c->halo->hi.size() * sizeof(int16_t));
+   std::memcpy(radius2, c->halo->radius2.data(), c->halo->radius2.size() * sizeof(int32_t));
+   return c->halo->camRad;
+}
+
+int ref_nearest_z(void* h, double zUm)
+{
+   return static_cast<sim::PsfKernelCache*>(h)->NearestZIndex(zUm);
+}
+
+// ------------------------------------------------------------------------------------------- render
+// RenderPhotonImage for one frame (background + splats), the camera-independent part.
+void ref_render_photon_image(void* h, const iscu_blink_event* ev, uint32_t nEv, int64_t frame, uint32_t w, uint32_t hgt,
+                             double pixelNm, double photonsPerBlink, double bg, double driftX, double driftY,
+                             double globalZ, const float* illum, const float* bgMap, double bgScale,
+                             double minPhotons, int parallel, float* out)
+{
+   const auto* c = static_cast<sim::PsfKernelCache*>(h);
+   const std::vector<sim::BlinkEvent> events = ToEvents(ev, nEv);
+   std::vector<float> il, bm;
+   sim::RenderExtras ex;
+   const size_t n = static_cast<size_t>(w) * hgt;
+   if (illum)
+   {
+      il.assign(illum, illum + n);
+      ex.illumField = &il;
+   }
+   if (bgMap)
+   {
+      bm.assign(bgMap, bgMap + n);
+      ex.backgroundMap = &bm;
+   }
+   ex.backgroundScale = bgScale;
+   ex.minPhotons = minPhotons;
+   ex.parallel = parallel != 0;
+   std::vector<float> img;
+   sim::RenderPhotonImage(img, w, hgt, events, frame, pixelNm, 1.3, photonsPerBlink, bg, driftX, driftY, c, globalZ,
+                          nullptr, nullptr, &ex);
+   std::memcpy(out, img.data(), n * sizeof(float));
+}
+
+// CollectGpuEmitters for one frame: the reference's 64-byte records. Returns the count (<= maxOut).
+uint32_t ref_collect_gpu_emitters(void* h, const iscu_blink_event* ev, uint32_t nEv, int64_t frame, uint32_t w,
+                                  uint32_t hgt, double pixelNm, double photonsPerBlink, double driftX, double driftY,
+                                  double globalZ, int kernel, double minPhotons, iscu_gpu_splat_emitter* out,
+                                  uint32_t maxOut)
+{
+   static_assert(sizeof(sim::GpuSplatEmitter) == sizeof(iscu_gpu_splat_emitter), "record layout");
+   const auto* c = static_cast<sim::PsfKernelCache*>(h);
+   const std::vector<sim::BlinkEvent> events = ToEvents(ev, nEv);
+   std::vector<sim::GpuSplatEmitter> rec;
+   sim::CollectGpuEmitters(events, frame, w, hgt, pixelNm, photonsPerBlink, driftX, driftY, *c, globalZ, nullptr, rec,
+                           nullptr, nullptr, kernel, minPhotons);
+   const uint32_t n = static_cast<uint32_t>(std::min<size_t>(rec.size(), maxOut));
+   std::memcpy(out, rec.data(), n * sizeof(iscu_gpu_splat_emitter));
+   return static_cast<uint32_t>(rec.size());
+}
+
+// The movie loop of one blink group: per frame RenderPhotonImage (serial) then ApplyNoiseChain (serial), frames in
+// parallel on the reference's pool (FluorescenceMovie::Render, ScopeMovie.cpp:7267 and :7649). Events are bucketed
+// per frame first (BucketEventsByFrame, SMLMSimulation.cpp:203). Returns the seconds spent in the frame loop.
+double ref_render_movie(void* h, const iscu_blink_event* ev, uint32_t nEv, uint32_t frame0, uint32_t nFrames,
+                        uint32_t w, uint32_t hgt, double pixelNm, double photonsPerBlink, double bg,
+                        const iscu_camera* cam, const float* off, const float* gain, const float* rn, uint32_t seed,
+                        float* outPhotons, uint16_t* outAdu)
+{
+   const auto* c = static_cast<sim::PsfKernelCache*>(h);
+   const std::vector<sim::BlinkEvent> events = ToEvents(ev, nEv);
+   Maps m;
+   FillMaps(m, w, hgt, off, gain, rn);
+   const sim::CameraNoiseParams cp = ToCamera(*cam);
+   const size_t n = static_cast<size_t>(w) * hgt;
+   const auto t0 = std::chrono::steady_clock::now();
+   // Buckets over [frame0, frame0 + nFrames): events shifted so the bucket index is the batch frame.
+   std::vector<sim::BlinkEvent> shifted = events;
+   for (auto& e : shifted)
+   {
+      e.tStart -= frame0;
+      e.tEnd -= frame0;
+   }
+   const auto buckets = sim::BucketEventsByFrame(shifted, nFrames);
+   sim::ParallelFor(nFrames, [&](unsigned k) {
+      std::vector<sim::BlinkEvent> fe;
+      fe.reserve(buckets[k].size());
+      for (uint32_t i : buckets[k])
+         fe.push_back(events[i]);
+      std::vector<float> img;
+      sim::RenderPhotonImage(img, w, hgt, fe, static_cast<long>(frame0 + k), pixelNm, 1.3, photonsPerBlink, bg, 0.0,
+                             0.0, c, 0.0);
+      std::vector<uint16_t> adu;
+      sim::ApplyNoiseChain(img, adu, w, hgt, cp, m.off, m.gain, m.rn, seed, frame0 + k, false, 0);
+      if (outPhotons)
+         std::memcpy(outPhotons + k * n, img.data(), n * sizeof(float));
+      if (outAdu)
+         std::memcpy(outAdu + k * n, adu.data(), n * sizeof(uint16_t));
+   });
+   return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+} // extern "C"

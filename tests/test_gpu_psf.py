@@ -1,0 +1,74 @@
+"""PSF planes on the B200 (pupil with float64 phases, chirp-Z as DFT matrix products) against the float64 oracle,
+the reference's ComputeZernikePsfPlanes / BuildZernikePsfKernelCache, and the reference's PSF fixture.
+Tolerance: max |I - I64| <= 1e-5 x max I64 per plane (the north-star bar for the PSF path)."""
+import os
+
+import numpy as np
+import pytest
+
+from insiliscope_b200 import CZT_FP32, CZT_TF32X3, INTERP_CUBIC, PsfParams
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+METHODS = [CZT_FP32]
+
+
+def _max_rel(got, want):
+    return max(np.abs(got[z] - want[z]).max() / want[z].max() for z in range(want.shape[0]))
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_fixture_planes(engine, golden_dir, method):
+    f = np.load(os.path.join(golden_dir, "zernike_ref.npz"))
+    for c in range(4):
+        req = PsfParams(wavelength_nm=660.0, na=1.4, sample_index=float(f["sample_index"][c]),
+                        sample_depth_nm=float(f["sample_depth_nm"][c]), pixel_size_nm=100.0,
+                        zernike=list(f["zernike"][c]), double_helix=bool(f["double_helix"][c]), oversampling=4,
+                        kernel_half_width_px=8, nz=3, z_step_nm=100.0, pupil_samples=64)
+        got = engine.psf_library_dev([req], [0, 0, 0], [-100.0, 0.0, 100.0], normalize=False,
+                                     method=method).cpu().numpy()
+        want = f["planes"][c].astype(np.float64)
+        assert _max_rel(got, want) <= TOL, c
+        for z in range(3):
+            assert np.argmax(got[z]) == np.argmax(want[z])
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_library_vs_oracle(engine, oracle, method):
+    """The library config's shape (M = 128 pupil -> 64 x 64 at 4x oversampling) with Noll 4-15 aberrations, four
+    wavelengths, defocus across +-800 nm, plus a double-helix and a deep, index-mismatched set."""
+    rng = np.random.default_rng(5)
+    sets = []
+    for wl in (520.0, 580.0, 670.0, 750.0):
+        z = np.zeros(28)
+        z[3:15] = rng.normal(0.0, 0.05 * 2.0, 12)
+        sets.append(PsfParams(wavelength_nm=wl, na=1.45, pixel_size_nm=100.0, oversampling=4, kernel_half_width_px=8,
+                              nz=3, z_step_nm=25.0, pupil_samples=128, zernike=list(z)))
+    sets.append(PsfParams(wavelength_nm=670.0, na=1.45, pixel_size_nm=100.0, oversampling=4, kernel_half_width_px=8,
+                          nz=3, z_step_nm=25.0, pupil_samples=128, double_helix=True))
+    sets.append(PsfParams(wavelength_nm=580.0, na=1.45, sample_index=1.33, sample_depth_nm=3000.0,
+                          pixel_size_nm=100.0, oversampling=4, kernel_half_width_px=8, nz=3, z_step_nm=25.0,
+                          pupil_samples=128))
+    set_of = np.repeat(np.arange(len(sets)), 3)
+    dz = np.tile([-800.0, 0.0, 637.5], len(sets))
+    got = engine.psf_library_dev(sets, set_of, dz, size=64, normalize=True, method=method).cpu().numpy()
+    for i in range(len(set_of)):
+        want = oracle.psf_planes(sets[set_of[i]], [dz[i] * 1e-9], size=64, normalize=True)
+        assert _max_rel(got[i:i + 1], want) <= TOL, i
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_kernel_build_vs_reference(engine, reference, method):
+    """iscu_kernel_build (planes, sum-1 normalization, block sums) against BuildZernikePsfKernelCache."""
+    req = PsfParams(wavelength_nm=670.0, na=1.45, pixel_size_nm=108.0, oversampling=4, kernel_half_width_px=16,
+                    nz=49, z_step_nm=25.0, pupil_samples=64, interp=INTERP_CUBIC)
+    k = reference.kernel(req=req)
+    engine.kernel_build(3, req, method)
+    got = engine.kernel_planes(3)
+    want = k.planes().astype(np.float64)
+    assert got.shape == want.shape == (49, 129, 129)
+    assert _max_rel(got, want) <= TOL
+    assert np.allclose(got.sum(axis=(1, 2)), 1.0, atol=1e-5)
+    sums = engine.kernel_block_sums(3)
+    assert np.abs(sums.sum(axis=(1, 2)) - 16.0).max() < 1e-3
+    assert np.abs(sums - k.block_sums()).max() <= TOL * k.block_sums().max()
