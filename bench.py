@@ -45,10 +45,14 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.time()
+            while len(self.lines) < 2 and time.time() - t0 < 5.0 and self.proc.poll() is None:
+                time.sleep(0.02)
+            self.skip = len(self.lines)   # samples from before the timed region
         except Exception:
             self.proc = None
         return self
@@ -67,7 +71,8 @@ class ClockSampler:
 
     def summary(self):
         sm, mx, reasons = [], [], set()
-        for l in self.lines:
+        lines = self.lines[getattr(self, "skip", 0):] or self.lines[-1:]
+        for l in lines:
             p = [x.strip() for x in l.split(",")]
             if len(p) < 9:
                 continue

@@ -77,7 +77,7 @@ def test_render_extras_bit_exact(engine, reference, oracle):
     ev = _events(rng, 150, W, H, F)
     all_e, counts = [], []
     for f in range(F):
-        e, _ = engine.collect_frame_emitters(1, ev, f, W, H, 108.0, 2000.0, drift_x=0.37 * f, drift_y=-0.21 * f,
+        e, _ = engine.collect_frame_emitters(1, ev, f, W, H, 108.0, 2000.0, drift_x_px=0.37 * f, drift_y_px=-0.21 * f,
                                              global_z_offset_um=0.04, illum=illum, min_photons=250.0)
         all_e.append(e)
         counts.append(len(e))
