@@ -153,6 +153,24 @@ int iscu_psf_library_dev(iscu_ctx* ctx, const iscu_psf_request* sets, uint32_t n
                          const double* defocus_nm, uint32_t n_psf, int32_t size, int32_t normalize, int32_t method,
                          float* out_dev);
 
+/* No counterpart in the reference. iscu_psf_library_dev with the plain FP32 method, for callers that must not
+ * allocate GPU memory: a host whose device memory belongs to someone else (a framework's caching allocator that has
+ * reserved the free memory, a fixed budget shared with other plug-ins), or a loop that cannot afford the device-wide
+ * synchronization a cudaFree implies. Its temporaries (set parameters, PSF items, pupil tables, DFT matrices) live in
+ * one statically sized device array of ISCU_NOALLOC_SCRATCH_BYTES that every GPU loading libiscu.so holds until exit;
+ * the call itself allocates nothing on the device. Limits: at most ISCU_NOALLOC_MAX_SETS sets and
+ * ISCU_NOALLOC_MAX_PSF PSFs, pupil samples M <= 128, plane size <= 129, and the layout within the array (sets,
+ * items, M*M*24 bytes of tables and 2*P*M*8 bytes of DFT matrices per set) must fit; beyond: ISCU_ERR_LIMIT.
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress), so make that first call
+ * before any stream capture. All calls share the array: calls whose work overlaps on the GPU (other threads or
+ * contexts) race. Returns when the planes are in out_dev. */
+#define ISCU_NOALLOC_SCRATCH_BYTES (4u << 20)
+#define ISCU_NOALLOC_MAX_SETS 4
+#define ISCU_NOALLOC_MAX_PSF 4096
+int iscu_psf_library_noalloc_dev(iscu_ctx* ctx, const iscu_psf_request* sets, uint32_t n_sets,
+                                 const uint32_t* set_of_psf, const double* defocus_nm, uint32_t n_psf, int32_t size,
+                                 int32_t normalize, float* out_dev);
+
 /* ---------------------------------------------------------------- kernel slots -------------------------------- */
 /* At most this many kernel stacks per context (GpuSimulator::kMaxKernels, GpuSimD3D11.h:70). */
 #define ISCU_MAX_KERNELS 4

@@ -109,6 +109,8 @@ SIGNATURES = {
     "iscu_psf_geometry": (C.c_int, [C.POINTER(PsfRequest), i32p, i32p, i32p]),
     "iscu_psf_library_dev": (C.c_int, [vp, C.POINTER(PsfRequest), C.c_uint32, vp, vp, C.c_uint32, C.c_int32,
                                        C.c_int32, C.c_int32, vp]),
+    "iscu_psf_library_noalloc_dev": (C.c_int, [vp, C.POINTER(PsfRequest), C.c_uint32, vp, vp, C.c_uint32,
+                                               C.c_int32, C.c_int32, vp]),
     "iscu_kernel_build": (C.c_int, [vp, C.c_int32, C.POINTER(PsfRequest), C.c_int32]),
     "iscu_kernel_set_planes": (C.c_int, [vp, C.c_int32, vp, C.c_int32, C.c_int32, C.c_int32, C.c_double,
                                          C.c_int32]),

@@ -26,6 +26,7 @@ UNITS = {
     "splat_noise.cu": ["--fmad=false"],
     "psf.cu": [],
     "psf_tc.cu": [],
+    "psf_noalloc.cu": [],
     "widefield.cu": ["--fmad=false"],
     "capi.cpp": [],
 }

@@ -395,4 +395,46 @@ int BuildPsfLibrary(iscu_ctx* ctx, const iscu_psf_request* sets, uint32_t nSets,
    return ISCU_OK;
 }
 
+// The set parameters of up to maxSets requests into caller memory (no heap): the pupil samples M and plane size P
+// they share. Used by the allocation-free entry point (psf_noalloc.cu).
+int PrepareSetParams(const iscu_psf_request* sets, uint32_t nSets, int32_t size, uint32_t maxSets, SetParams* out,
+                     int* M, int* P)
+{
+   if (nSets == 0 || nSets > maxSets)
+      return Fail(ISCU_ERR_LIMIT, "psf library: 1.." + std::to_string(maxSets) + " request sets");
+   std::string err;
+   PsfGeometry g0;
+   if (!GeometryFor(sets[0], g0, err))
+      return Fail(ISCU_ERR_ARG, err);
+   *M = g0.M;
+   *P = size > 0 ? size : g0.size;
+   for (uint32_t s = 0; s < nSets; ++s)
+   {
+      PsfGeometry g;
+      if (!GeometryFor(sets[s], g, err))
+         return Fail(ISCU_ERR_ARG, err);
+      if (g.M != *M)
+         return Fail(ISCU_ERR_ARG, "psf library: every set must have the same pupil samples");
+      MakeSetParams(sets[s], *M, *P, g.resLateralNm, out[s]);
+   }
+   return ISCU_OK;
+}
+
+// The plain FP32 pipeline (tables, DFT matrices, chirp-Z) on buffers the caller provides.
+int LaunchPsfPipelineFp32(iscu_ctx* ctx, const SetParams* dSets, const PsfItem* dItems, double3* dTab, float2* dA,
+                          float2* dAt, uint32_t nSets, uint32_t nPsf, int M, int P, int normalize, float* out)
+{
+   PupilTablesKernel<<<dim3((M * M + 127) / 128, nSets), 128, 0, ctx->stream>>>(dSets, M, dTab);
+   ISCU_CK_LAUNCH(ctx, "PupilTablesKernel");
+   DftMatrixKernel<<<dim3((P * M + 255) / 256, nSets), 256, 0, ctx->stream>>>(dSets, M, P, dA, dAt);
+   ISCU_CK_LAUNCH(ctx, "DftMatrixKernel");
+   const size_t smem = (static_cast<size_t>(M) * M + static_cast<size_t>(P) * M) * sizeof(float2);
+   if (smem > 227 * 1024)
+      return Fail(ISCU_ERR_LIMIT, "psf library (fp32): pupil and row pass exceed shared memory");
+   ISCU_CK(cudaFuncSetAttribute(CztFp32Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+   CztFp32Kernel<<<nPsf, kCztThreads, smem, ctx->stream>>>(dSets, dTab, dA, dAt, dItems, M, P, normalize, out);
+   ISCU_CK_LAUNCH(ctx, "CztFp32Kernel");
+   return ISCU_OK;
+}
+
 } // namespace iscu

@@ -67,4 +67,9 @@ __device__ __forceinline__ double BlockSumDouble(double v, double* red)
 int LaunchCztTf32x3(iscu_ctx* ctx, const SetParams* sets, const double3* tables, const float2* A, const float2* At,
                     const PsfItem* items, uint32_t nPsf, int M, int P, int normalize, float* out);
 
+int PrepareSetParams(const iscu_psf_request* sets, uint32_t nSets, int32_t size, uint32_t maxSets, SetParams* out,
+                     int* M, int* P);
+int LaunchPsfPipelineFp32(iscu_ctx* ctx, const SetParams* dSets, const PsfItem* dItems, double3* dTab, float2* dA,
+                          float2* dAt, uint32_t nSets, uint32_t nPsf, int M, int P, int normalize, float* out);
+
 } // namespace iscu

@@ -228,6 +228,16 @@ class Engine:
                                             int(normalize), method, _ptr(out)))
         return out
 
+    def psf_library_noalloc_dev(self, sets, set_of_psf, defocus_nm, out, size=0, normalize=True):
+        """iscu_psf_library_noalloc_dev: the FP32 PSF library with no device allocation in the call (its
+        temporaries in the library's static device array); out: a caller-owned (n, P, P) float32 CUDA tensor."""
+        reqs = (PsfRequest * len(sets))(*[s.c() for s in sets])
+        so = np.ascontiguousarray(set_of_psf, dtype=np.uint32)
+        dz = np.ascontiguousarray(defocus_nm, dtype=np.float64)
+        check(self.lib.iscu_psf_library_noalloc_dev(self.h, reqs, len(sets), _ptr(so), _ptr(dz), len(so), size,
+                                                    int(normalize), _ptr(out)))
+        return out
+
     def kernel_build(self, slot, req: PsfParams, method=CZT_FP32):
         r = req.c()
         check(self.lib.iscu_kernel_build(self.h, slot, C.byref(r), method))

@@ -126,10 +126,11 @@ def test_noise_vs_reference(oracle, reference, emccd):
     W, H = 64, 48
     photons = rng.gamma(1.5, 40.0, size=(H, W)).astype(np.float32)
     photons[::7, ::5] *= 30.0
-    off, gain, rn = reference.camera_maps(W, H, 17, 100.0, 2.0, 2.2, 0.05, 1.5, 0.2, keep_y0=3, keep_rows=H)
+    # a window: rows [3, 3 + H) of a sensor H + 7 rows tall
+    off, gain, rn = reference.camera_maps(W, H + 7, 17, 100.0, 2.0, 2.2, 0.05, 1.5, 0.2, keep_y0=3, keep_rows=H)
     cam = CameraParams(quantum_efficiency=0.85, dark_electrons=0.1, gain=2.2, read_noise_e=1.5, emccd=emccd,
                        em_gain=150.0, bit_depth=14)
-    maps = [a.reshape(-1, W)[:H] for a in (off, gain, rn)]
+    maps = [a.reshape(H, W) for a in (off, gain, rn)]
     want = reference.noise_chain(photons, cam, *maps, 555, 9, pixel_base=3 * W)
     got = oracle.noise_chain(photons, cam, *maps, 555, 9, pixel_base=3 * W)
     assert np.array_equal(got, want)
