@@ -165,7 +165,7 @@ class SmlmWorkload:
 
     def device_step(self):
         self.eng.render_frames_dev(self.d_em, self.d_fr, self.mv.frames, self.mv.camera, self.mv.noise_seed,
-                                   None, self.d_adu)
+                                   None, self.d_adu, sync=False)
 
     def e2e_step(self):
         """Host blink events -> host ADU: emitter collection, H2D, render, D2H, all through the C ABI."""
@@ -203,10 +203,23 @@ class SmlmWorkload:
         return "RenderFramesKernel"
 
     # -------------------------------------------------- the reference on the host cores
+    dtype = "f64"
+    cpu_kind = "reference"
+    cpu_sample = ("the whole 200-frame movie per step: the reference's RenderPhotonImage + ApplyNoiseChain per frame, "
+                  "frames in parallel on its own thread pool (ParallelFor), PSF kernel built once before timing as the "
+                  "reference memoizes it")
+    frames_per_step_cpu = 200
+
+    def cpu_cores(self):
+        return self.ref.threads()
+
     def reference_setup(self, threads=0):
         from oracle.oracle import Reference
         from insiliscope_b200 import generate_camera_maps
         mv = self.mv
+        if not Reference.available():
+            raise RuntimeError("the reference harness oracle/_ref/libiscref.so is not built (it needs the reference "
+                               "tree at build time)")
         self.ref = Reference()
         self.ref.set_threads(threads)
         self.rk = self.ref.kernel(req=mv.psf)
@@ -221,51 +234,164 @@ class SmlmWorkload:
         return t
 
 
-WORKLOADS = {"smlm": SmlmWorkload}
+class WidefieldWorkload:
+    """The widefield mean-field focus series: a 512 x 512 x 64 dye volume convolved with a 512 x 512 x 64 3D PSF
+    (1024 x 1024 x 128 FFT grid), max(0, .) + 5 photons/px background, EMCCD chain; one step = 64 frames."""
+    name = ("widefield 3D FFT convolution 512x512x64 volume (50 cells, nuclei, 200 filaments each) x 512x512x64 "
+            "Gibson-Lanni PSF (NA 1.4, 520 nm), EMCCD gain 300, 5 photons/px background")
+    metric = "frames/s"
+
+    # pass names and their algorithmic bytes (computed in setup)
+    PASSES = ("XForwardKernel", "YForwardKernel", "ZKernel<convolve>", "YInverseKernel", "XInverseKernel")
+
+    def __init__(self, rank: int):
+        from insiliscope_b200.workloads import widefield_cells
+        self.rank = rank
+        self.wv = widefield_cells(seed=42 + rank)
+        self.frame0 = rank * 64
+
+    def setup(self, device: int):
+        import torch
+        from insiliscope_b200 import Engine, WidefieldPlan, generate_camera_maps
+        wv = self.wv
+        nz, ny, nx = wv.density.shape
+        self.eng = eng = Engine(device)
+        t0 = time.perf_counter()
+        kz, ky, kx = wv.psf_shape
+        psf = eng.psf_library_dev([wv.psf], np.zeros(kz, np.uint32), wv.psf_defocus_nm, size=kx,
+                                  normalize=True).cpu().numpy()
+        eng.synchronize()
+        self.psf_build_ms = (time.perf_counter() - t0) * 1e3
+        t0 = time.perf_counter()
+        self.plan = WidefieldPlan(eng, (nz, ny, nx), psf)
+        self.plan_ms = (time.perf_counter() - t0) * 1e3
+        off, _, _ = generate_camera_maps(nx, ny, wv.map_seed, wv.offset_mean, wv.offset_std, 1.0, 0.0, 50.0, 0.0)
+        eng.set_static(nx, ny, offset=off)
+        self.d_vol = torch.from_numpy(wv.density).to(f"cuda:{device}")
+        self.d_adu = torch.empty((nz, ny, nx), dtype=torch.uint16, device=f"cuda:{device}")
+        self.h_vol = torch.from_numpy(wv.density).pin_memory().numpy()
+        self.h_adu = torch.empty((nz, ny, nx), dtype=torch.uint16).pin_memory().numpy()
+        self.stream = eng.torch_stream()
+        self.frames_per_step = nz
+        self.n_emitters = 0
+        G = self.plan.grid()
+        NK = G[0] // 2 + 1
+        vox = nx * ny * nz
+        self.pass_bytes = [vox * 4 + NK * ny * nz * 8,                    # x forward: reals in, half spectra out
+                           NK * ny * nz * 8 + NK * G[1] * nz * 8,          # y forward
+                           2 * NK * G[1] * nz * 8 + NK * G[1] * G[2] * 8,  # z: spectra in/out + the PSF spectrum
+                           NK * G[1] * nz * 8 + NK * ny * nz * 8,          # y inverse
+                           NK * ny * nz * 8 + vox * 2 + nx * ny * 4]       # x inverse: ADU out + offset map
+
+    def device_step(self):
+        wv = self.wv
+        self.plan.render_dev(self.d_vol, wv.background, wv.camera, wv.noise_seed, self.frame0, None, self.d_adu,
+                             sync=False)
+
+    def e2e_step(self):
+        wv = self.wv
+        self.plan.render(self.h_vol, wv.background, wv.camera, wv.noise_seed, self.frame0, adu=self.h_adu)
+        return self.h_adu
+
+    def e2e_bytes(self):
+        return self.h_vol.nbytes, self.h_adu.nbytes
+
+    def dominant(self):
+        """Pass times over 3 steps (CUDA events inside the plan); the slowest pass with its algorithmic bytes."""
+        self.plan.set_timing(True)
+        times = []
+        for _ in range(3):
+            self.device_step()
+            times.append(self.plan.pass_times())
+        self.plan.set_timing(False)
+        mean = [statistics.mean(t[i] for t in times) for i in range(5)]
+        i = int(np.argmax(mean))
+        return self.PASSES[i], self.pass_bytes[i], mean[i], dict(zip(self.PASSES, [round(m, 4) for m in mean]))
+
+    def alg_bytes_per_launch(self):
+        return sum(self.pass_bytes)
+
+    def kernel_name(self):
+        return "widefield step (5 passes)"
+
+    # -------------------------------------------------- CPU: the float64 FFT convolution port (scipy, all cores)
+    dtype = "f32"
+    frames_per_step_cpu = 64
+    cpu_kind = "port"
+    cpu_sample = ("the whole 64-frame focus series per step: float64 3D FFT convolution on the same padded grid "
+                  "(scipy.fft, all cores; the PSF spectrum precomputed, as the plan keeps it) + max(0, .) + background "
+                  "+ the oracle's EMCCD chain (frames in parallel)")
+
+    def reference_setup(self, threads=0):
+        import scipy.fft as sf
+        from oracle.oracle import Oracle
+        self.orc = Oracle()
+        kz, ky, kx = self.wv.psf_shape
+        k = np.zeros((kz, ky, kx))
+        k[kz // 2, ky // 2, kx // 2] = 1.0   # the timing does not depend on the PSF's values
+        self.shape = [1 << int(np.ceil(np.log2(a + b - 1))) for a, b in zip(self.wv.density.shape, k.shape)]
+        self.Kf = sf.rfftn(k, self.shape, workers=-1)
+        self.kshape = k.shape
+
+    def cpu_cores(self):
+        return os.cpu_count() or 1
+
+    def reference_step(self):
+        import scipy.fft as sf
+        from concurrent.futures import ThreadPoolExecutor
+        wv = self.wv
+        t0 = time.perf_counter()
+        F = sf.rfftn(wv.density.astype(np.float64), self.shape, workers=-1) * self.Kf
+        full = sf.irfftn(F, self.shape, workers=-1)
+        (kz, ky, kx), (nz, ny, nx) = self.kshape, wv.density.shape
+        img = (np.maximum(full[kz // 2: kz // 2 + nz, ky // 2: ky // 2 + ny, kx // 2: kx // 2 + nx], 0.0) +
+               wv.background).astype(np.float32)
+        with ThreadPoolExecutor(self.cpu_cores()) as ex:
+            list(ex.map(lambda f: self.orc.noise_chain(img[f], wv.camera, None, None, None, wv.noise_seed,
+                                                       self.frame0 + f), range(nz)))
+        return time.perf_counter() - t0
+
+
+WORKLOADS = {"smlm": SmlmWorkload, "widefield": WidefieldWorkload}
 
 
 # ----------------------------------------------------------------------------------------------------- arms
 def run_reference(args):
-    world, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    from oracle.oracle import Reference
-    if not Reference.available():
-        print(json.dumps({"impl": "reference", "unavailable": "the reference harness oracle/_ref/libiscref.so is not "
-                                                               "built (needs the reference tree at build time)"}))
-        return 0
     w = WORKLOADS[args.workload](0)
-    w.reference_setup(threads=0)
-    cores = w.ref.threads()
+    try:
+        w.reference_setup(threads=0)
+    except RuntimeError as e:
+        print(json.dumps({"impl": "reference", "unavailable": str(e)}))
+        return 0
     for _ in range(args.warmup):
         w.reference_step()
     times = [w.reference_step() for _ in range(args.steps)]
     ms = 1e3 * statistics.mean(times)
-    value = w.mv.frames / (ms / 1e3)
+    value = w.frames_per_step_cpu / (ms / 1e3)
     line = {"metric": w.metric, "value": value, "unit": w.metric, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": w.name, "frames_per_step": w.mv.frames},
-            "cpu_baseline": {"value": value, "unit": w.metric, "cores": cores, "kind": "reference",
-                             "sample": f"the whole {w.mv.frames}-frame movie per step (RenderPhotonImage + "
-                                       "ApplyNoiseChain per frame, frames in parallel on the reference's pool; "
-                                       "PSF kernel built once before timing, as the reference memoizes it)"},
+            "vs_baseline": None, "dtype": w.dtype, "data": "synthetic", "impl": "reference",
+            "config": {"workload": w.name, "frames_per_step": w.frames_per_step_cpu},
+            "cpu_baseline": {"value": value, "unit": w.metric, "cores": w.cpu_cores(), "kind": w.cpu_kind,
+                             "sample": w.cpu_sample},
             "e2e": {"value": value, "unit": w.metric, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
 
 
 def cpu_baseline(w):
-    """The reference's CPU renderer on this box's host cores, a bounded sample: one whole movie, best of 3."""
-    from oracle.oracle import Reference
-    if Reference.available():
+    """The CPU path on this box's host cores, a bounded sample (the workload's own), best of 3 after one warm-up."""
+    try:
         w.reference_setup(threads=0)
-        w.reference_step()
-        best = min(w.reference_step() for _ in range(3))
-        return {"value": w.mv.frames / best, "unit": w.metric, "cores": w.ref.threads(), "kind": "reference",
-                "sample": f"one {w.mv.frames}-frame movie, best of 3 (reference RenderPhotonImage + ApplyNoiseChain "
-                          "on its thread pool, kernel memoized)"}
-    return None
+    except RuntimeError:
+        return None
+    w.reference_step()
+    best = min(w.reference_step() for _ in range(3))
+    return {"value": w.frames_per_step_cpu / best, "unit": w.metric, "cores": w.cpu_cores(), "kind": w.cpu_kind,
+            "sample": w.cpu_sample + "; best of 3"}
 
 
 def run_ours(args):
@@ -314,20 +440,28 @@ def run_ours(args):
     e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps, world)
     h2d, d2h = w.e2e_bytes()
     hbm, _, peak_kind = measured_peaks()
-    achieved = w.alg_bytes_per_launch() / (statistics.mean(step_ms) / 1e3) / 1e9
+    if hasattr(w, "dominant"):
+        kname, kbytes, kms, breakdown = w.dominant()
+    else:
+        kname, kbytes, kms, breakdown = w.kernel_name(), w.alg_bytes_per_launch(), statistics.mean(step_ms), None
+    achieved = kbytes / (kms / 1e3) / 1e9
     line = {"metric": w.metric, "value": value, "unit": w.metric, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "vs_baseline": None, "dtype": w.dtype, "data": "synthetic",
             "config": {"workload": w.name, "frames_per_step": w.frames_per_step, "emitters_per_step": w.n_emitters,
                        "l2": "flushed before every timed step (256 MB write)", "parallelism": f"frames x{world}",
                        "psf_build_ms": round(w.psf_build_ms, 3)},
             "e2e": {"value": world * w.frames_per_step / (e2e_ms / 1e3), "unit": w.metric, "ms_per_step": e2e_ms,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "timing": "host wall clock per step (blocking C-ABI calls), max over ranks"},
-            "roofline": {"bound": "hbm", "kernel": w.kernel_name(), "achieved": achieved, "peak": hbm,
-                         "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
-                         "traffic": None, "alg_bytes_per_launch": w.alg_bytes_per_launch()},
+            "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": None,
+                         "alg_bytes_per_launch": kbytes, "launch_ms": kms},
             "gpu_launches": launches, "clocks": clk.summary()}
+    if breakdown:
+        line["roofline"]["pass_ms"] = breakdown
+        line["roofline"]["step_alg_bytes"] = w.alg_bytes_per_launch()
+        line["roofline"]["step_achieved"] = w.alg_bytes_per_launch() / (statistics.mean(step_ms) / 1e3) / 1e9
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(w)
     if rank == 0:

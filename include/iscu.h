@@ -281,6 +281,36 @@ int iscu_collect_emitters(iscu_ctx* ctx, int32_t slot, const iscu_blink_event* e
                           const float* illum, double min_photons, iscu_emitter* out, uint32_t max_out,
                           iscu_frame* frames_out, uint32_t* n_out, int64_t* n_clamped);
 
+/* ---------------------------------------------------------------- widefield ----------------------------------- */
+
+/* Widefield mean-field 3D convolution: the dye density volume (nx x ny x nz float32, x fastest, photons per voxel
+ * at focus) convolved with a 3D PSF (kx x ky x kz float32, centred on voxel (kx/2, ky/2, kz/2)), linear (zero-padded)
+ * and cropped to the volume ("same"), so image plane f is sum_k dye plane k (x) PSF plane f - k + kz/2 -- the focus
+ * series of WidefieldScene (WidefieldRender.h:588, one image per focus at every dye plane). A plan holds the PSF's
+ * spectrum resident (the reference caches kernel spectra, WidefieldRender.cpp:1408). */
+typedef struct iscu_wf_plan iscu_wf_plan;
+int iscu_wf_plan_create(iscu_ctx* ctx, uint32_t nx, uint32_t ny, uint32_t nz, const float* psf, uint32_t kx,
+                        uint32_t ky, uint32_t kz, iscu_wf_plan** out);
+void iscu_wf_plan_destroy(iscu_wf_plan* plan);
+/* The padded FFT grid of a plan (each axis a power of two >= the linear-convolution length). */
+int iscu_wf_plan_grid(iscu_wf_plan* plan, uint32_t* gx, uint32_t* gy, uint32_t* gz);
+/* density_dev (nx*ny*nz) -> image_dev (nx*ny*nz): the convolution, max(0, .) per voxel (WidefieldImages::Render's
+ * clamp, WidefieldRender.cpp:547). */
+int iscu_wf_convolve_dev(iscu_wf_plan* plan, const float* density_dev, float* image_dev);
+/* Convolution, max(0, .) + background, then the noise chain per image plane (frame f = frame0 + plane; cam NULL: no
+ * noise), host buffers: the widefield movie of one focus series. adu: nx*ny*nz uint16 (needed with cam). image
+ * (nullable): the noise-free expected frames. */
+int iscu_wf_render(iscu_wf_plan* plan, const float* density, double background, const iscu_camera* cam,
+                   uint32_t seed, uint32_t frame0, float* image, uint16_t* adu);
+/* Phase timing of a plan's renders (the reference's ISC_TIMING phases, Timing.h:123): with it on, every render
+ * records CUDA events around its five passes; iscu_wf_pass_times gives the last render's pass durations in ms
+ * (x forward, y forward, z convolve, y inverse, x inverse + noise), waiting for it. */
+int iscu_wf_set_timing(iscu_wf_plan* plan, int32_t on);
+int iscu_wf_pass_times(iscu_wf_plan* plan, float* ms5);
+/* The same on device buffers (the camera maps of iscu_set_static apply when their size is nx x ny). */
+int iscu_wf_render_dev(iscu_wf_plan* plan, const float* density_dev, double background, const iscu_camera* cam,
+                       uint32_t seed, uint32_t frame0, float* image_dev, uint16_t* adu_dev);
+
 #ifdef __cplusplus
 }
 #endif

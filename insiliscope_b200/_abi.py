@@ -125,6 +125,15 @@ SIGNATURES = {
     "iscu_collect_frame_emitters": (C.c_int, [vp, C.c_int32, vp, C.c_uint32, C.c_int64, C.c_uint32, C.c_uint32,
                                               C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, vp,
                                               C.c_double, vp, C.c_uint32, u32p, i64p]),
+    "iscu_wf_plan_create": (C.c_int, [vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, C.c_uint32, C.c_uint32,
+                                      C.c_uint32, C.POINTER(vp)]),
+    "iscu_wf_plan_destroy": (None, [vp]),
+    "iscu_wf_plan_grid": (C.c_int, [vp, u32p, u32p, u32p]),
+    "iscu_wf_convolve_dev": (C.c_int, [vp, vp, vp]),
+    "iscu_wf_set_timing": (C.c_int, [vp, C.c_int32]),
+    "iscu_wf_pass_times": (C.c_int, [vp, f32p]),
+    "iscu_wf_render": (C.c_int, [vp, vp, C.c_double, C.POINTER(Camera), C.c_uint32, C.c_uint32, vp, vp]),
+    "iscu_wf_render_dev": (C.c_int, [vp, vp, C.c_double, C.POINTER(Camera), C.c_uint32, C.c_uint32, vp, vp]),
     "iscu_collect_emitters": (C.c_int, [vp, C.c_int32, vp, vp, vp, C.c_int64, C.c_uint32, C.c_uint32, C.c_uint32,
                                         C.c_double, C.c_double, vp, vp, vp, vp, vp, C.c_double, vp, C.c_uint32, vp,
                                         u32p, i64p]),

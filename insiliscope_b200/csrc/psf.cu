@@ -244,7 +244,156 @@ __global__ void __launch_bounds__(kCztThreads) CztFp32Kernel(const SetParams* __
          plane[idx] = static_cast<float>(static_cast<double>(plane[idx]) / sum);
 }
 
+// ------------------------------------------------------------------------------------------ large pupils
+// When the pupil and the row pass do not fit shared memory (M beyond ~128: a widefield kernel's 512-sample pupil),
+// the same products go through global memory: the pupil phasors U (nPsf x M x M), then two batched complex GEMMs
+// with 64 x 64 output tiles staged 16 deep in shared memory -- T = A U, E = T A^T -- the second one ending in |E|^2
+// and the plane's float64 sum.
+__global__ void PupilKernel(const SetParams* __restrict__ sets, const double3* __restrict__ tables,
+                            const PsfItem* __restrict__ items, int M, float2* __restrict__ U)
+{
+   const int b = blockIdx.y;
+   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+   if (idx >= M * M)
+      return;
+   const PsfItem it = items[b];
+   U[static_cast<size_t>(b) * M * M + idx] =
+      PupilPhasor(tables[static_cast<size_t>(it.set) * M * M + idx], sets[it.set], it.dtiM);
+}
+
+// C[b] (rows x cols) = L (rows x K) R (K x cols), L = L0 + set * lSet + b * lBatch, R likewise. kIntensity: writes
+// |C|^2 as float and adds the tile's float64 sum to sums[b].
+template <bool kIntensity>
+__global__ void __launch_bounds__(256) CGemmTiledKernel(const PsfItem* __restrict__ items, const float2* __restrict__ L0,
+                                                       size_t lSet, size_t lBatch, const float2* __restrict__ R0,
+                                                       size_t rSet, size_t rBatch, int rows, int cols, int K,
+                                                       float2* __restrict__ C, float* __restrict__ I,
+                                                       double* __restrict__ sums)
+{
+   __shared__ float2 sL[16][65];
+   __shared__ float2 sR[16][64];
+   __shared__ double sRed[8];
+   const int b = blockIdx.z, set = items[b].set;
+   const float2* L = L0 + set * lSet + b * lBatch;
+   const float2* R = R0 + set * rSet + b * rBatch;
+   const int rb = blockIdx.y * 64, cb = blockIdx.x * 64;
+   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+   float2 acc[4][4];
+#pragma unroll
+   for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+         acc[i][j] = make_float2(0.f, 0.f);
+   for (int k0 = 0; k0 < K; k0 += 16)
+   {
+#pragma unroll
+      for (int e4 = 0; e4 < 4; ++e4)
+      {
+         const int e = threadIdx.x + 256 * e4;
+         const int r = e >> 4, kk = e & 15, kr = e >> 6, c = e & 63;
+         sL[kk][r] = (rb + r < rows && k0 + kk < K) ? L[static_cast<size_t>(rb + r) * K + k0 + kk]
+                                                    : make_float2(0.f, 0.f);
+         sR[kr][c] = (k0 + kr < K && cb + c < cols) ? R[static_cast<size_t>(k0 + kr) * cols + cb + c]
+                                                    : make_float2(0.f, 0.f);
+      }
+      __syncthreads();
+#pragma unroll
+      for (int kk = 0; kk < 16; ++kk)
+      {
+         float2 l[4], r[4];
+#pragma unroll
+         for (int i = 0; i < 4; ++i)
+         {
+            l[i] = sL[kk][ty + 16 * i];
+            r[i] = sR[kk][tx + 16 * i];
+         }
+#pragma unroll
+         for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+               Cmac(acc[i][j], l[i], r[j]);
+      }
+      __syncthreads();
+   }
+   double local = 0.0;
+#pragma unroll
+   for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+      {
+         const int r = rb + ty + 16 * i, c = cb + tx + 16 * j;
+         if (r >= rows || c >= cols)
+            continue;
+         const size_t o = static_cast<size_t>(b) * rows * cols + static_cast<size_t>(r) * cols + c;
+         if (kIntensity)
+         {
+            const float v = acc[i][j].x * acc[i][j].x + acc[i][j].y * acc[i][j].y;
+            I[o] = v;
+            local += static_cast<double>(v);
+         }
+         else
+            C[o] = acc[i][j];
+      }
+   if (kIntensity)
+   {
+      const double t = BlockSumDouble(local, sRed);
+      if (threadIdx.x == 0)
+         atomicAdd(sums + b, t);
+   }
+}
+
+__global__ void NormalizeKernel(float* __restrict__ planes, const double* __restrict__ sums, int planeElems)
+{
+   const int b = blockIdx.y;
+   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= planeElems)
+      return;
+   const double s = sums[b];
+   if (s > 0.0)
+   {
+      float* p = planes + static_cast<size_t>(b) * planeElems;
+      p[i] = static_cast<float>(static_cast<double>(p[i]) / s);
+   }
+}
+
 } // namespace
+
+// The large-pupil FP32 path (global-memory products); temporaries allocated here.
+static int LaunchCztGlobalFp32(iscu_ctx* ctx, const SetParams* dSets, const double3* dTab, const float2* dA,
+                               const float2* dAt, const PsfItem* dItems, uint32_t nPsf, int M, int P, int normalize,
+                               float* out)
+{
+   DevBuf U, T, S;
+   // in batches bounded to ~2 GB of temporaries
+   const size_t perPsf = (static_cast<size_t>(M) * M + static_cast<size_t>(P) * M) * sizeof(float2);
+   const uint32_t batch = static_cast<uint32_t>(std::max<size_t>(1, std::min<size_t>(nPsf, (2ull << 30) / perPsf)));
+   ISCU_CK(U.Reserve(static_cast<size_t>(batch) * M * M * sizeof(float2)));
+   ISCU_CK(T.Reserve(static_cast<size_t>(batch) * P * M * sizeof(float2)));
+   ISCU_CK(S.Reserve(static_cast<size_t>(nPsf) * sizeof(double)));
+   ISCU_CK(cudaMemsetAsync(S.p, 0, static_cast<size_t>(nPsf) * sizeof(double), ctx->stream));
+   for (uint32_t b0 = 0; b0 < nPsf; b0 += batch)
+   {
+      const uint32_t nb = std::min(batch, nPsf - b0);
+      PupilKernel<<<dim3((M * M + 255) / 256, nb), 256, 0, ctx->stream>>>(dSets, dTab, dItems + b0, M,
+                                                                          U.as<float2>());
+      ISCU_CK_LAUNCH(ctx, "PupilKernel");
+      CGemmTiledKernel<false><<<dim3((M + 63) / 64, (P + 63) / 64, nb), 256, 0, ctx->stream>>>(
+         dItems + b0, dA, static_cast<size_t>(P) * M, 0, U.as<float2>(), 0, static_cast<size_t>(M) * M, P, M, M,
+         T.as<float2>(), nullptr, nullptr);
+      ISCU_CK_LAUNCH(ctx, "CGemmTiledKernel<product>");
+      CGemmTiledKernel<true><<<dim3((P + 63) / 64, (P + 63) / 64, nb), 256, 0, ctx->stream>>>(
+         dItems + b0, T.as<float2>(), 0, static_cast<size_t>(P) * M, dAt, static_cast<size_t>(P) * M, 0, P, P, M,
+         nullptr, out + static_cast<size_t>(b0) * P * P, S.as<double>() + b0);
+      ISCU_CK_LAUNCH(ctx, "CGemmTiledKernel<intensity>");
+   }
+   if (normalize)
+   {
+      NormalizeKernel<<<dim3((P * P + 255) / 256, nPsf), 256, 0, ctx->stream>>>(out, S.as<double>(), P * P);
+      ISCU_CK_LAUNCH(ctx, "NormalizeKernel");
+   }
+   ISCU_CK(cudaStreamSynchronize(ctx->stream));
+   return ISCU_OK;
+}
 
 // ------------------------------------------------------------------------------------------ host side
 
@@ -382,7 +531,8 @@ int BuildPsfLibrary(iscu_ctx* ctx, const iscu_psf_request* sets, uint32_t nSets,
    {
       const size_t smem = (static_cast<size_t>(M) * M + static_cast<size_t>(P) * M) * sizeof(float2);
       if (smem > 227 * 1024)
-         return Fail(ISCU_ERR_LIMIT, "psf library (fp32): pupil and row pass exceed shared memory");
+         return LaunchCztGlobalFp32(ctx, dSets.as<SetParams>(), dTab.as<double3>(), dA.as<float2>(),
+                                    dAt.as<float2>(), dItems.as<PsfItem>(), nPsf, M, P, normalize, out);
       ISCU_CK(cudaFuncSetAttribute(CztFp32Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(smem)));
       CztFp32Kernel<<<nPsf, kCztThreads, smem, ctx->stream>>>(dSets.as<SetParams>(), dTab.as<double3>(),

@@ -15,6 +15,7 @@
 
 #include "counter_rng.cuh"
 #include "iscu_internal.h"
+#include "noise_chain.cuh"
 
 #include <cstdint>
 
@@ -23,34 +24,6 @@ namespace iscu {
 namespace {
 
 constexpr int kTileX = 16, kTileY = 16, kThreads = kTileX * kTileY, kChunk = kThreads;
-
-// ---------------------------------------------------------------------------------------------------------- noise
-__device__ __forceinline__ uint16_t NoisePixel(float photonValue, uint32_t i, const CameraView& cam,
-                                               const StaticView& st, CounterRng& u)
-{
-   u.Pixel(i + st.pixelBase);
-   const double pv = static_cast<double>(photonValue);
-   const double photons = pv > 0.0 ? pv : 0.0;   // std::max(0.0, v)
-   if (cam.emccd)
-   {
-      const double ne = CounterPoisson(photons * cam.qe + cam.dark + cam.cic, u);
-      const double out = ne > 0.0 ? CounterGamma(ne, u) : 0.0;
-      const double readE = (st.readNoise ? static_cast<double>(st.readNoise[i]) : cam.readNoise) / cam.emGain;
-      const double gain = st.gain ? static_cast<double>(st.gain[i]) : cam.gain;
-      const double offset = st.offset ? static_cast<double>(st.offset[i]) : 0.0;
-      const double g = CounterGauss(u);
-      const double adu = floor(offset + (out + readE * g) / gain + 0.5);
-      return static_cast<uint16_t>(adu < 0.0 ? 0.0 : (adu > cam.maxAdu ? cam.maxAdu : adu));
-   }
-   const double ne = CounterPoisson(photons * cam.qe + cam.dark, u);
-   const double readNoise = st.readNoise ? static_cast<double>(st.readNoise[i]) : cam.readNoise;
-   const double gain = st.gain ? static_cast<double>(st.gain[i]) : cam.gain;
-   const double offset = st.offset ? static_cast<double>(st.offset[i]) : 0.0;
-   const double g = CounterGauss(u);
-   double adu = offset + (ne + readNoise * g) / gain;
-   adu = adu < 0.0 ? 0.0 : (adu > 65535.0 ? 65535.0 : adu);
-   return static_cast<uint16_t>(floor(adu + 0.5));
-}
 
 // The background of pixel i for a frame (RenderPhotonImage's background lambda, SMLMSimulation.cpp:124-137).
 __device__ __forceinline__ float Background(const StaticView& st, uint32_t i, double bgScale)

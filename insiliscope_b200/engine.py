@@ -132,20 +132,39 @@ def generate_camera_maps(width, height, seed, offset_mean=100.0, offset_std=2.0,
 
 
 class Engine:
-    """One libiscu context: a device, a stream, up to four resident kernel stacks and the camera statics."""
+    """One libiscu context: a device, a stream, up to four resident kernel stacks and the camera statics.
+
+    The `*_dev` methods take torch CUDA tensors. The library works on its own (non-blocking) stream; by default these
+    methods wait for torch's current stream before they enqueue and for the library's stream before they return
+    (sync=True). Callers that order the two streams themselves -- e.g. work issued under
+    `torch.cuda.stream(engine.torch_stream())` -- pass sync=False."""
 
     def __init__(self, device: int = 0):
+        import weakref
         self.lib = load()
         h = C.c_void_p()
         check(self.lib.iscu_create(device, C.byref(h)))
         self.h = h
         self.device = device
         self.width = self.height = 0
+        self._plans = weakref.WeakSet()
 
     def close(self):
+        """Destroys the context, after the plans made on it (a plan must not outlive its context)."""
         if self.h:
+            for p in list(self._plans):
+                p.close()
             self.lib.iscu_destroy(self.h)
             self.h = None
+
+    def _before(self, sync):
+        if sync:
+            import torch
+            torch.cuda.current_stream(self.device).synchronize()
+
+    def _after(self, sync):
+        if sync:
+            self.synchronize()
 
     def __enter__(self):
         return self
@@ -181,6 +200,7 @@ class Engine:
         import torch
         words = words.contiguous()
         out = torch.empty_like(words)
+        self._before(True)
         check(self.lib.iscu_pcg4d_dev(self.h, _ptr(words), _ptr(out), words.shape[0]))
         self.synchronize()
         return out
@@ -209,6 +229,7 @@ class Engine:
                              device=photons.device)
         out = torch.empty(photons.shape, dtype=torch.uint16, device=photons.device)
         cam = camera.c()
+        self._before(True)
         check(self.lib.iscu_noise_frames_dev(self.h, _ptr(photons), photons.shape[0], _ptr(fr), C.byref(cam), seed,
                                              _ptr(out)))
         self.synchronize()
@@ -282,12 +303,14 @@ class Engine:
         return ph, adu
 
     def render_frames_dev(self, emitters_dev, frames_dev, n_frames, camera: CameraParams | None, seed,
-                          photons_dev=None, adu_dev=None):
+                          photons_dev=None, adu_dev=None, sync=True):
         """Device path on torch CUDA buffers (emitters: uint8 view of EMITTER_DTYPE records, frames likewise)."""
         cam = camera.c() if camera is not None else None
+        self._before(sync)
         check(self.lib.iscu_render_frames_dev(self.h, _ptr(emitters_dev), _ptr(frames_dev), n_frames,
                                               C.byref(cam) if cam is not None else None, seed, _ptr(photons_dev),
                                               _ptr(adu_dev)))
+        self._after(sync)
 
     def render_gpu_records(self, records, frames, camera: CameraParams, seed, extras=None):
         """GpuSimulator::RenderFrames over the reference's 64-byte records (GPU_SPLAT_EMITTER_DTYPE)."""
@@ -337,6 +360,80 @@ class Engine:
                                              _ptr(sc), _ptr(il), min_photons, _ptr(out), len(out), _ptr(frames_out),
                                              C.byref(n), C.byref(clamped)))
         return out[: n.value], frames_out, clamped.value
+
+
+class WidefieldPlan:
+    """iscu_wf_plan: the focus series of a dye volume (nz, ny, nx) under a 3D PSF (kz, ky, kx), PSF spectrum resident."""
+
+    def __init__(self, engine: Engine, shape, psf):
+        psf = np.ascontiguousarray(psf, dtype=np.float32)
+        self.engine = engine
+        self.lib = engine.lib
+        self.shape = tuple(int(v) for v in shape)   # (nz, ny, nx)
+        nz, ny, nx = self.shape
+        kz, ky, kx = psf.shape
+        h = C.c_void_p()
+        check(self.lib.iscu_wf_plan_create(engine.h, nx, ny, nz, _ptr(psf), kx, ky, kz, C.byref(h)))
+        self.h = h
+        engine._plans.add(self)
+
+    def close(self):
+        if self.h:
+            if self.engine.h:   # the context is still alive (Engine.close destroys its plans first)
+                self.lib.iscu_wf_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def grid(self):
+        g = [C.c_uint32() for _ in range(3)]
+        check(self.lib.iscu_wf_plan_grid(self.h, *[C.byref(x) for x in g]))
+        return tuple(x.value for x in g)
+
+    def set_timing(self, on=True):
+        check(self.lib.iscu_wf_set_timing(self.h, int(on)))
+
+    def pass_times(self):
+        """The last render's pass durations (ms): x forward, y forward, z convolve, y inverse, x inverse + noise."""
+        ms = (C.c_float * 5)()
+        check(self.lib.iscu_wf_pass_times(self.h, ms))
+        return list(ms)
+
+    def convolve_dev(self, density_dev, image_dev=None, sync=True):
+        import torch
+        if image_dev is None:
+            image_dev = torch.empty(self.shape, dtype=torch.float32, device=density_dev.device)
+        self.engine._before(sync)
+        check(self.lib.iscu_wf_convolve_dev(self.h, _ptr(density_dev), _ptr(image_dev)))
+        self.engine._after(sync)
+        return image_dev
+
+    def render_dev(self, density_dev, background, camera: CameraParams | None, seed, frame0=0, image_dev=None,
+                   adu_dev=None, sync=True):
+        cam = camera.c() if camera is not None else None
+        self.engine._before(sync)
+        check(self.lib.iscu_wf_render_dev(self.h, _ptr(density_dev), float(background),
+                                          C.byref(cam) if cam is not None else None, seed, frame0, _ptr(image_dev),
+                                          _ptr(adu_dev)))
+        self.engine._after(sync)
+
+    def render(self, density, background, camera: CameraParams | None, seed, frame0=0, want_image=False, adu=None,
+               image=None):
+        """Host path: density (nz, ny, nx) float32 -> (image | None, adu | None)."""
+        density = np.ascontiguousarray(density, dtype=np.float32)
+        if want_image and image is None:
+            image = np.empty(self.shape, np.float32)
+        if camera is not None and adu is None:
+            adu = np.empty(self.shape, np.uint16)
+        cam = camera.c() if camera is not None else None
+        check(self.lib.iscu_wf_render(self.h, _ptr(density), float(background),
+                                      C.byref(cam) if cam is not None else None, seed, frame0,
+                                      _ptr(image) if want_image else None, _ptr(adu) if cam is not None else None))
+        return (image if want_image else None), (adu if camera is not None else None)
 
 
 def frames_table(counts, frame_ids=None, bg_scales=None):

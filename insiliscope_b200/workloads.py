@@ -112,3 +112,87 @@ def smlm_dstorm(seed: int = 42, sites: int = 4000, frames: int = 200, size: int 
     cam = CameraParams(quantum_efficiency=1.0, dark_electrons=0.0, gain=2.2, read_noise_e=1.5, emccd=False)
     return SmlmMovie(size, size, frames, pixel_nm, median_photons, 20.0, ev, bucket, psf, cam, seed, 100.0, 2.0, 2.2,
                      0.1 / 2.2, 1.5, 0.2, (seed ^ 0x9E3779B9) & 0xFFFFFFFF)
+
+
+@dataclass
+class WidefieldVolume:
+    """A dye volume and what renders its focus series."""
+    density: np.ndarray         # (nz, ny, nx) float32, photons per voxel per frame at focus
+    voxel_nm: tuple
+    psf: PsfParams              # the 3D PSF's request (planes at voxel z pitch)
+    psf_shape: tuple            # (kz, ky, kx)
+    psf_defocus_nm: np.ndarray  # the kz planes' defocus
+    camera: CameraParams
+    background: float
+    map_seed: int
+    offset_mean: float
+    offset_std: float
+    noise_seed: int
+
+
+def widefield_cells(seed: int = 42, nx: int = 512, ny: int = 512, nz: int = 64, voxel_nm=(100.0, 100.0, 200.0),
+                    cells: int = 50, filaments: int = 200, steps: int = 60, photons_per_dye: float = 0.4,
+                    kernel_shape=None) -> WidefieldVolume:
+    """The widefield mean-field volume: nx x ny x nz voxels of 100 x 100 x 200 nm holding `cells` random ellipsoidal
+    cells (axes 5-15 um, random orientation) with nuclei (0.4 of the axes, 3x the dye density) and `filaments`
+    persistent random walks per cell (4 dyes per voxel step). The PSF: 3D Gibson-Lanni, NA 1.4, 520 nm, oil,
+    nx x ny x nz samples at the voxel pitch (pupil samples from the reference's automatic choice). EMCCD: EM gain
+    300, 5 photons/px background, CIC 0.002, read noise 50 e-, offset N(100, 2) ADU, 1 photon/ADU, QE 1."""
+    rng = np.random.default_rng(seed)
+    vx, vy, vz = (v / 1000.0 for v in voxel_nm)
+    d = np.zeros((nz, ny, nx), np.float32)
+    X, Y, Z = nx * vx, ny * vy, nz * vz
+    for _ in range(cells):
+        c = np.array([rng.uniform(0, X), rng.uniform(0, Y), rng.uniform(0.3, 0.7) * Z])
+        ax = rng.uniform(2.5, 7.5, 3)
+        th = rng.uniform(0, 2 * np.pi)
+        ct, st = np.cos(th), np.sin(th)
+        r = ax.max()
+        i0, i1 = max(0, int((c[0] - r) / vx)), min(nx, int((c[0] + r) / vx) + 1)
+        j0, j1 = max(0, int((c[1] - r) / vy)), min(ny, int((c[1] + r) / vy) + 1)
+        k0, k1 = max(0, int((c[2] - ax[2]) / vz)), min(nz, int((c[2] + ax[2]) / vz) + 1)
+        if i0 >= i1 or j0 >= j1 or k0 >= k1:
+            continue
+        zz, yy, xx = np.meshgrid((np.arange(k0, k1) + 0.5) * vz - c[2], (np.arange(j0, j1) + 0.5) * vy - c[1],
+                                 (np.arange(i0, i1) + 0.5) * vx - c[0], indexing="ij")
+        u = (xx * ct + yy * st) / ax[0]
+        v = (-xx * st + yy * ct) / ax[1]
+        w = zz / ax[2]
+        q = u * u + v * v + w * w
+        d[k0:k1, j0:j1, i0:i1] += (q <= 1.0).astype(np.float32) + 2.0 * (q <= 0.16).astype(np.float32)
+        # filaments: persistent walks from inside the cell, ending where they leave it
+        start = c + (rng.uniform(-0.7, 0.7, (filaments, 3)) * ax[None, :] *
+                     np.array([[1.0, 1.0, 0.5]]))
+        phi = rng.uniform(0, 2 * np.pi, filaments)
+        tilt = rng.normal(0.0, 0.15, filaments)
+        pts = []
+        p = start.copy()
+        alive = np.ones(filaments, bool)
+        for _s in range(steps):
+            phi += rng.normal(0.0, 0.3, filaments)
+            step = 0.15 * np.stack([np.cos(phi), np.sin(phi), tilt], axis=1)
+            p = p + step
+            rel = p - c
+            uu = (rel[:, 0] * ct + rel[:, 1] * st) / ax[0]
+            vv = (-rel[:, 0] * st + rel[:, 1] * ct) / ax[1]
+            ww = rel[:, 2] / ax[2]
+            alive &= (uu * uu + vv * vv + ww * ww) <= 1.0
+            pts.append(p[alive])
+        pts = np.concatenate(pts) if pts else np.zeros((0, 3))
+        ii = (pts[:, 0] / vx).astype(np.int64)
+        jj = (pts[:, 1] / vy).astype(np.int64)
+        kk = (pts[:, 2] / vz).astype(np.int64)
+        ok = (ii >= 0) & (ii < nx) & (jj >= 0) & (jj < ny) & (kk >= 0) & (kk < nz)
+        np.add.at(d, (kk[ok], jj[ok], ii[ok]), 4.0)
+    d *= photons_per_dye
+    kz, ky, kx = kernel_shape if kernel_shape is not None else (nz, ny, nx)
+    psf = PsfParams(wavelength_nm=520.0, na=1.4, immersion_index=1.518, sample_index=1.518,
+                    working_distance_um=150.0, pixel_size_nm=voxel_nm[0], oversampling=1,
+                    kernel_half_width_px=max(kx, ky) // 2, nz=kz, z_step_nm=voxel_nm[2], pupil_samples=0)
+    # Convolution orientation: image plane f gets dye plane k through PSF plane f - k + kz/2, whose defocus is the
+    # dye's height above the focal plane, (k - f) dz = (kz/2 - j) dz for PSF plane j.
+    defocus = (kz // 2 - np.arange(kz)) * voxel_nm[2]
+    cam = CameraParams(quantum_efficiency=1.0, dark_electrons=0.0, gain=1.0, read_noise_e=50.0, emccd=True,
+                       bit_depth=16, em_gain=300.0, cic_electrons=0.002)
+    return WidefieldVolume(d, tuple(voxel_nm), psf, (kz, ky, kx), defocus, cam, 5.0, seed, 100.0, 2.0,
+                           (seed ^ 0x9E3779B9) & 0xFFFFFFFF)

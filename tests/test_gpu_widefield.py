@@ -1,0 +1,105 @@
+"""Widefield mean-field focus series on the B200 (3D FFT convolution + max(0, .) + background + EMCCD chain) against
+the float64 FFT convolution oracle; at full size (512 x 512 x 64 volume and PSF, the widefield config's shape)
+through size-independent properties: the impulse response is the PSF itself, and the convolution is linear.
+Tolerance: max |I - I64| <= 1e-5 x max |I64| (the north-star bar for noise-free images)."""
+import numpy as np
+import pytest
+
+from insiliscope_b200 import CameraParams, PsfParams, WidefieldPlan
+from oracle.oracle import fft_convolve_same_f64
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+def _rel(got, want):
+    return float(np.abs(got - want).max() / np.abs(want).max())
+
+
+@pytest.mark.parametrize("vol_shape,psf_shape", [((10, 24, 30), (7, 9, 11)), ((16, 40, 64), (16, 40, 64)),
+                                                 ((5, 33, 20), (2, 4, 6)), ((1, 8, 8), (1, 3, 3))])
+def test_convolution_vs_oracle(engine, vol_shape, psf_shape):
+    import torch
+    rng = np.random.default_rng(sum(vol_shape) + sum(psf_shape))
+    vol = rng.random(vol_shape).astype(np.float32)
+    vol[vol < 0.6] = 0.0
+    psf = rng.random(psf_shape).astype(np.float32)
+    psf -= 0.2   # some negative taps, so the max(0, .) clamp is exercised
+    plan = WidefieldPlan(engine, vol_shape, psf)
+    got = plan.convolve_dev(torch.from_numpy(vol).cuda()).cpu().numpy()
+    want = np.maximum(fft_convolve_same_f64(vol, psf), 0.0)
+    assert _rel(got, want) <= TOL
+    plan.close()
+
+
+def test_render_noise_bit_exact_on_image(engine, oracle):
+    """The frames' ADU are ApplyNoiseChain (EMCCD) of the expected image, frame = frame0 + plane, with the camera
+    offset map: bit for bit the oracle's chain on the GPU's own expected image."""
+    rng = np.random.default_rng(4)
+    nz, ny, nx = 6, 36, 50
+    vol = (rng.random((nz, ny, nx)) * 30).astype(np.float32)
+    psf = rng.random((5, 7, 9)).astype(np.float32)
+    psf /= psf.sum(axis=(1, 2), keepdims=True)
+    off, _, _ = oracle.camera_maps(nx, ny, 42, 100.0, 2.0, 1.0, 0.0, 50.0, 0.0)
+    engine.set_static(nx, ny, offset=off)
+    cam = CameraParams(quantum_efficiency=1.0, gain=1.0, read_noise_e=50.0, emccd=True, em_gain=300.0,
+                       cic_electrons=0.002, bit_depth=16)
+    plan = WidefieldPlan(engine, (nz, ny, nx), psf)
+    image, adu = plan.render(vol, 5.0, cam, 777, frame0=100, want_image=True)
+    want_img = np.maximum(fft_convolve_same_f64(vol, psf), 0.0) + 5.0
+    assert _rel(image, want_img) <= TOL
+    for f in range(nz):
+        want = oracle.noise_chain(image[f], cam, off.reshape(ny, nx), None, None, 777, 100 + f)
+        assert np.array_equal(adu[f], want), f
+    plan.close()
+
+
+def _full_plan(engine):
+    rng = np.random.default_rng(9)
+    psf = rng.random((64, 512, 512)).astype(np.float32) * np.float32(1e-4)
+    psf[32, 256, 256] += 1.0
+    return psf, WidefieldPlan(engine, (64, 512, 512), psf)
+
+
+def test_full_size_impulse_response(engine):
+    """512 x 512 x 64 on the 1024 x 1024 x 128 grid: a unit dye at (z0, y0, x0) images to the PSF shifted there."""
+    import torch
+    psf, plan = _full_plan(engine)
+    assert plan.grid() == (1024, 1024, 128)
+    for (z0, y0, x0) in ((32, 256, 256), (3, 17, 500), (60, 490, 9)):
+        vol = torch.zeros((64, 512, 512), dtype=torch.float32, device="cuda")
+        vol[z0, y0, x0] = 1.0
+        got = plan.convolve_dev(vol).cpu().numpy()
+        want = np.zeros((64, 512, 512), np.float32)
+        zs, ys, xs = slice(max(0, z0 - 32), min(64, z0 + 32)), slice(max(0, y0 - 256), min(512, y0 + 256)), \
+            slice(max(0, x0 - 256), min(512, x0 + 256))
+        want[zs, ys, xs] = psf[zs.start - z0 + 32: zs.stop - z0 + 32, ys.start - y0 + 256: ys.stop - y0 + 256,
+                               xs.start - x0 + 256: xs.stop - x0 + 256]
+        assert _rel(got, want) <= TOL, (z0, y0, x0)
+    plan.close()
+
+
+def test_full_size_linearity(engine):
+    import torch
+    psf, plan = _full_plan(engine)
+    rng = np.random.default_rng(10)
+    a = torch.from_numpy(rng.random((64, 512, 512), dtype=np.float32)).cuda()
+    b = torch.from_numpy((rng.random((64, 512, 512), dtype=np.float32) < 0.01).astype(np.float32) * 50).cuda()
+    ia = plan.convolve_dev(a).double()
+    ib = plan.convolve_dev(b).double()
+    iab = plan.convolve_dev(2.5 * a + b).double()
+    assert float((iab - (2.5 * ia + ib)).abs().max() / iab.abs().max()) <= TOL
+    plan.close()
+
+
+def test_large_pupil_psf_vs_oracle(engine, oracle):
+    """The PSF path for pupils beyond shared memory (global-memory products), as the widefield PSF (M = 512) uses,
+    checked at M = 256 -> 96 x 96 planes against the float64 oracle."""
+    req = PsfParams(wavelength_nm=520.0, na=1.4, pixel_size_nm=100.0, oversampling=1, kernel_half_width_px=48,
+                    nz=3, z_step_nm=200.0, pupil_samples=256)
+    req.zernike[4] = 0.05
+    dz = np.array([-600.0, 0.0, 400.0])
+    got = engine.psf_library_dev([req], [0, 0, 0], dz, size=96, normalize=True).cpu().numpy()
+    want = oracle.psf_planes(req, dz * 1e-9, size=96, normalize=True)
+    for i in range(3):
+        assert np.abs(got[i] - want[i]).max() <= TOL * want[i].max(), i
