@@ -153,6 +153,26 @@ int iscu_psf_library_dev(iscu_ctx* ctx, const iscu_psf_request* sets, uint32_t n
                          const double* defocus_nm, uint32_t n_psf, int32_t size, int32_t normalize, int32_t method,
                          float* out_dev);
 
+/* A PSF library plan: the per-set work of ComputeZernikePsfPlanes (pupil tables, DFT matrices, and for
+ * ISCU_CZT_TF32X3 the split stacked operand) done once for `sets` at plane size `size` (0: the first request's), then
+ * runs of any number of PSFs (set index + defocus each). The memo of ComputePsfKernelCache
+ * (PsfGeneratorBridge.h:317-364) keeps kernel stacks the same way. ISCU_CZT_TF32X3 needs M <= 128 (a multiple of 16)
+ * and planes of at most 64 x 64. */
+typedef struct iscu_psf_plan iscu_psf_plan;
+int iscu_psf_plan_create(iscu_ctx* ctx, const iscu_psf_request* sets, uint32_t n_sets, int32_t size, int32_t method,
+                         iscu_psf_plan** out);
+void iscu_psf_plan_destroy(iscu_psf_plan* plan);
+/* The plan's plane size P and pupil samples M. */
+int iscu_psf_plan_info(iscu_psf_plan* plan, int32_t* size, int32_t* pupil_samples);
+/* n_psf planes (P x P floats each) into out_dev from device arrays of set indices and defocus (nm); enqueued on the
+ * context's stream. iscu_psf_plan_check waits and reports a bad set index or a tensor-core wait that ran out. */
+int iscu_psf_plan_run_dev(iscu_psf_plan* plan, const uint32_t* set_of_psf_dev, const double* defocus_nm_dev,
+                          uint32_t n_psf, int32_t normalize, float* out_dev);
+int iscu_psf_plan_check(iscu_psf_plan* plan);
+/* The same from host arrays into host memory (the copies are part of the call). */
+int iscu_psf_plan_run(iscu_psf_plan* plan, const uint32_t* set_of_psf, const double* defocus_nm, uint32_t n_psf,
+                      int32_t normalize, float* out);
+
 /* No counterpart in the reference. iscu_psf_library_dev with the plain FP32 method, for callers that must not
  * allocate GPU memory: a host whose device memory belongs to someone else (a framework's caching allocator that has
  * reserved the free memory, a fixed budget shared with other plug-ins), or a loop that cannot afford the device-wide

@@ -111,6 +111,13 @@ SIGNATURES = {
                                        C.c_int32, C.c_int32, vp]),
     "iscu_psf_library_noalloc_dev": (C.c_int, [vp, C.POINTER(PsfRequest), C.c_uint32, vp, vp, C.c_uint32,
                                                C.c_int32, C.c_int32, vp]),
+    "iscu_psf_plan_create": (C.c_int, [vp, C.POINTER(PsfRequest), C.c_uint32, C.c_int32, C.c_int32,
+                                       C.POINTER(vp)]),
+    "iscu_psf_plan_destroy": (None, [vp]),
+    "iscu_psf_plan_info": (C.c_int, [vp, i32p, i32p]),
+    "iscu_psf_plan_run_dev": (C.c_int, [vp, vp, vp, C.c_uint32, C.c_int32, vp]),
+    "iscu_psf_plan_check": (C.c_int, [vp]),
+    "iscu_psf_plan_run": (C.c_int, [vp, vp, vp, C.c_uint32, C.c_int32, vp]),
     "iscu_kernel_build": (C.c_int, [vp, C.c_int32, C.POINTER(PsfRequest), C.c_int32]),
     "iscu_kernel_set_planes": (C.c_int, [vp, C.c_int32, vp, C.c_int32, C.c_int32, C.c_int32, C.c_double,
                                          C.c_int32]),

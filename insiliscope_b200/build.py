@@ -27,6 +27,7 @@ UNITS = {
     "psf.cu": [],
     "psf_tc.cu": [],
     "psf_noalloc.cu": [],
+    "psf_plan.cu": [],
     "widefield.cu": ["--fmad=false"],
     "capi.cpp": [],
 }

@@ -101,9 +101,11 @@ __global__ void PupilTablesKernel(const SetParams* __restrict__ sets, int M, dou
    const SetParams& sp = sets[s];
    const int iy = idx / M, ix = idx % M, c0 = M / 2;
    const double ky = (iy - c0) * sp.dk, kx = (ix - c0) * sp.dk;
-   const double kr2 = kx * kx + ky * ky;
+   // The aperture test decides samples that sit exactly on the circle (M = 64: (30, 0), (18, 24), ...): rounded
+   // product by product, as the reference's uncontracted float64 does, so the same samples are in.
+   const double kr2 = __dadd_rn(__dmul_rn(kx, kx), __dmul_rn(ky, ky));
    double3 out = make_double3(0.0, -1.0, 0.0);
-   if (!(kr2 > sp.kMax * sp.kMax))
+   if (!(kr2 > __dmul_rn(sp.kMax, sp.kMax)))
    {
       const double kr = sqrt(kr2);
       const double rho = kr / (sp.k0 * sp.na);
@@ -522,8 +524,8 @@ int BuildPsfLibrary(iscu_ctx* ctx, const iscu_psf_request* sets, uint32_t nSets,
    ISCU_CK_LAUNCH(ctx, "DftMatrixKernel");
    if (method == ISCU_CZT_TF32X3)
    {
-      const int rc = LaunchCztTf32x3(ctx, dSets.as<SetParams>(), dTab.as<double3>(), dA.as<float2>(),
-                                     dAt.as<float2>(), dItems.as<PsfItem>(), nPsf, M, P, normalize, out);
+      const int rc = LaunchCztTf32x3(ctx, dSets.as<SetParams>(), dTab.as<double3>(), dA.as<float2>(), nSets,
+                                     dItems.as<PsfItem>(), nPsf, M, P, normalize, out);
       if (rc != ISCU_OK)
          return rc;
    }
@@ -567,6 +569,31 @@ int PrepareSetParams(const iscu_psf_request* sets, uint32_t nSets, int32_t size,
          return Fail(ISCU_ERR_ARG, "psf library: every set must have the same pupil samples");
       MakeSetParams(sets[s], *M, *P, g.resLateralNm, out[s]);
    }
+   return ISCU_OK;
+}
+
+// The per-set tables and DFT matrices (once per set; a PSF plan keeps them).
+int LaunchPsfTables(iscu_ctx* ctx, const SetParams* dSets, uint32_t nSets, int M, int P, double3* dTab, float2* dA,
+                    float2* dAt)
+{
+   PupilTablesKernel<<<dim3((M * M + 127) / 128, nSets), 128, 0, ctx->stream>>>(dSets, M, dTab);
+   ISCU_CK_LAUNCH(ctx, "PupilTablesKernel");
+   DftMatrixKernel<<<dim3((P * M + 255) / 256, nSets), 256, 0, ctx->stream>>>(dSets, M, P, dA, dAt);
+   ISCU_CK_LAUNCH(ctx, "DftMatrixKernel");
+   return ISCU_OK;
+}
+
+// The plain FP32 chirp-Z of nPsf items over prepared tables (shared-memory form, or the global-memory form for
+// pupils beyond shared memory).
+int LaunchCztFp32(iscu_ctx* ctx, const SetParams* dSets, const double3* dTab, const float2* dA, const float2* dAt,
+                  const PsfItem* dItems, uint32_t nPsf, int M, int P, int normalize, float* out)
+{
+   const size_t smem = (static_cast<size_t>(M) * M + static_cast<size_t>(P) * M) * sizeof(float2);
+   if (smem > 227 * 1024)
+      return LaunchCztGlobalFp32(ctx, dSets, dTab, dA, dAt, dItems, nPsf, M, P, normalize, out);
+   ISCU_CK(cudaFuncSetAttribute(CztFp32Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+   CztFp32Kernel<<<nPsf, kCztThreads, smem, ctx->stream>>>(dSets, dTab, dA, dAt, dItems, M, P, normalize, out);
+   ISCU_CK_LAUNCH(ctx, "CztFp32Kernel");
    return ISCU_OK;
 }
 

@@ -64,8 +64,17 @@ __device__ __forceinline__ double BlockSumDouble(double v, double* red)
    return t;
 }
 
-int LaunchCztTf32x3(iscu_ctx* ctx, const SetParams* sets, const double3* tables, const float2* A, const float2* At,
+int LaunchCztTf32x3(iscu_ctx* ctx, const SetParams* sets, const double3* tables, const float2* A, uint32_t nSets,
                     const PsfItem* items, uint32_t nPsf, int M, int P, int normalize, float* out);
+bool Tf32x3Supports(int M, int P);
+int BuildAhat(iscu_ctx* ctx, const float2* A, int nSets, int M, int P, DevBuf& ahat);
+int LaunchCztTf32x3Core(iscu_ctx* ctx, const SetParams* sets, const double3* tables, const float* ahat,
+                        const PsfItem* items, uint32_t nPsf, int M, int P, int normalize, float* out, int* dErr);
+
+int LaunchPsfTables(iscu_ctx* ctx, const SetParams* dSets, uint32_t nSets, int M, int P, double3* dTab, float2* dA,
+                    float2* dAt);
+int LaunchCztFp32(iscu_ctx* ctx, const SetParams* dSets, const double3* dTab, const float2* dA, const float2* dAt,
+                  const PsfItem* dItems, uint32_t nPsf, int M, int P, int normalize, float* out);
 
 int PrepareSetParams(const iscu_psf_request* sets, uint32_t nSets, int32_t size, uint32_t maxSets, SetParams* out,
                      int* M, int* P);

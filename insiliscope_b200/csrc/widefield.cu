@@ -64,10 +64,11 @@ __device__ __forceinline__ float2 Cmul(float2 a, float2 b)
 }
 __device__ __forceinline__ float2 Conj(float2 a) { return make_float2(a.x, -a.y); }
 
-// W_M^j = exp(-2 pi i j / M) from the G-point table (M divides G); conjugated for inverse transforms.
-__device__ __forceinline__ float2 Tw(const float2* __restrict__ tw, int G, int M, int j, bool inv)
+// W_M^j = exp(-2 pi i j / M) from the G-point table, M = 2^logM dividing G = 2^logG; conjugated for inverse
+// transforms. Every size here is a power of two, so index arithmetic is shifts and masks.
+__device__ __forceinline__ float2 Tw(const float2* __restrict__ tw, int logG, int logM, int j, bool inv)
 {
-   const float2 w = __ldg(tw + static_cast<size_t>(j) * (G / M));
+   const float2 w = __ldg(tw + (j << (logG - logM)));
    return inv ? Conj(w) : w;
 }
 
@@ -76,40 +77,41 @@ __device__ __forceinline__ int Rev(int n, int logN) { return static_cast<int>(__
 // Lines in shared memory: element n of line b at s[b * ls + n * es]. kColumns: es > 1, ls = 1 (threads walk the
 // lines fastest); else rows (es = 1, threads walk the elements fastest).
 template <bool kColumns>
-__device__ __forceinline__ void TupleOf(int t, int tuples, int nl, int& b, int& u)
+__device__ __forceinline__ void TupleOf(int t, int logTuples, int logNl, int& b, int& u)
 {
    if (kColumns)
    {
-      b = t % nl;
-      u = t / nl;
+      b = t & ((1 << logNl) - 1);
+      u = t >> logNl;
    }
    else
    {
-      b = t / tuples;
-      u = t % tuples;
+      b = t >> logTuples;
+      u = t & ((1 << logTuples) - 1);
    }
 }
 
-// Decimation-in-frequency FFT of nl lines of N = 2^logN points: natural order in, bit-reversed order out.
+// Decimation-in-frequency FFT of nl = 2^logNl lines of N = 2^logN points: natural order in, bit-reversed order out.
 template <bool kColumns>
-__device__ void DifLines(float2* s, int logN, int nl, int ls, int es, const float2* __restrict__ tw, int G, bool inv)
+__device__ void DifLines(float2* s, int logN, int logNl, int ls, int es, const float2* __restrict__ tw, int logG,
+                         bool inv)
 {
-   const int N = 1 << logN, tuples = N >> 2;
-   int h = N >> 1;
-   for (; h >= 2; h >>= 2)
+   const int N = 1 << logN, total4 = (N >> 2) << logNl, total2 = (N >> 1) << logNl;
+   int logQ = logN - 2;
+   for (; logQ >= 0; logQ -= 2)
    {
-      const int q = h >> 1;
-      for (int t = threadIdx.x; t < tuples * nl; t += blockDim.x)
+      const int q = 1 << logQ;
+      for (int t = threadIdx.x; t < total4; t += blockDim.x)
       {
          int b, u;
-         TupleOf<kColumns>(t, tuples, nl, b, u);
-         const int j = u % q, i = (u / q) * 4 * q + j;
+         TupleOf<kColumns>(t, logN - 2, logNl, b, u);
+         const int j = u & (q - 1), i = ((u >> logQ) << (logQ + 2)) | j;
          float2* L = s + b * ls;
          const float2 e0 = L[i * es], e1 = L[(i + q) * es], e2 = L[(i + 2 * q) * es], e3 = L[(i + 3 * q) * es];
          const float2 a0 = Cadd(e0, e2), a1 = Cadd(e1, e3);
-         const float2 a2 = Cmul(Csub(e0, e2), Tw(tw, G, 4 * q, j, inv));
-         const float2 a3 = Cmul(Csub(e1, e3), Tw(tw, G, 4 * q, j + q, inv));
-         const float2 w = Tw(tw, G, 2 * q, j, inv);
+         const float2 a2 = Cmul(Csub(e0, e2), Tw(tw, logG, logQ + 2, j, inv));
+         const float2 a3 = Cmul(Csub(e1, e3), Tw(tw, logG, logQ + 2, j + q, inv));
+         const float2 w = Tw(tw, logG, logQ + 1, j, inv);
          L[i * es] = Cadd(a0, a1);
          L[(i + q) * es] = Cmul(Csub(a0, a1), w);
          L[(i + 2 * q) * es] = Cadd(a2, a3);
@@ -117,12 +119,12 @@ __device__ void DifLines(float2* s, int logN, int nl, int ls, int es, const floa
       }
       __syncthreads();
    }
-   if (h == 1)
+   if (logQ == -1)   // logN odd: the last stage, span 1
    {
-      for (int t = threadIdx.x; t < (N >> 1) * nl; t += blockDim.x)
+      for (int t = threadIdx.x; t < total2; t += blockDim.x)
       {
          int b, u;
-         TupleOf<kColumns>(t, N >> 1, nl, b, u);
+         TupleOf<kColumns>(t, logN - 1, logNl, b, u);
          float2* L = s + b * ls;
          const float2 a = L[2 * u * es], c = L[(2 * u + 1) * es];
          L[2 * u * es] = Cadd(a, c);
@@ -134,37 +136,39 @@ __device__ void DifLines(float2* s, int logN, int nl, int ls, int es, const floa
 
 // Decimation-in-time FFT: bit-reversed order in, natural order out.
 template <bool kColumns>
-__device__ void DitLines(float2* s, int logN, int nl, int ls, int es, const float2* __restrict__ tw, int G, bool inv)
+__device__ void DitLines(float2* s, int logN, int logNl, int ls, int es, const float2* __restrict__ tw, int logG,
+                         bool inv)
 {
-   const int N = 1 << logN, tuples = N >> 2;
-   int q = 1;
-   if (logN & 1)
+   const int N = 1 << logN, total4 = (N >> 2) << logNl, total2 = (N >> 1) << logNl;
+   int logQ = 0;
+   if (logN & 1)   // the first stage, span 1
    {
-      for (int t = threadIdx.x; t < (N >> 1) * nl; t += blockDim.x)
+      for (int t = threadIdx.x; t < total2; t += blockDim.x)
       {
          int b, u;
-         TupleOf<kColumns>(t, N >> 1, nl, b, u);
+         TupleOf<kColumns>(t, logN - 1, logNl, b, u);
          float2* L = s + b * ls;
          const float2 a = L[2 * u * es], c = L[(2 * u + 1) * es];
          L[2 * u * es] = Cadd(a, c);
          L[(2 * u + 1) * es] = Csub(a, c);
       }
       __syncthreads();
-      q = 2;
+      logQ = 1;
    }
-   for (; q < N; q <<= 2)
+   for (; logQ < logN; logQ += 2)
    {
-      for (int t = threadIdx.x; t < tuples * nl; t += blockDim.x)
+      const int q = 1 << logQ;
+      for (int t = threadIdx.x; t < total4; t += blockDim.x)
       {
          int b, u;
-         TupleOf<kColumns>(t, tuples, nl, b, u);
-         const int j = u % q, i = (u / q) * 4 * q + j;
+         TupleOf<kColumns>(t, logN - 2, logNl, b, u);
+         const int j = u & (q - 1), i = ((u >> logQ) << (logQ + 2)) | j;
          float2* L = s + b * ls;
-         const float2 w = Tw(tw, G, 2 * q, j, inv);
+         const float2 w = Tw(tw, logG, logQ + 1, j, inv);
          const float2 e0 = L[i * es], e1 = Cmul(L[(i + q) * es], w);
          const float2 e2 = L[(i + 2 * q) * es], e3 = Cmul(L[(i + 3 * q) * es], w);
          const float2 a0 = Cadd(e0, e1), a1 = Csub(e0, e1), a2 = Cadd(e2, e3), a3 = Csub(e2, e3);
-         const float2 b2 = Cmul(a2, Tw(tw, G, 4 * q, j, inv)), b3 = Cmul(a3, Tw(tw, G, 4 * q, j + q, inv));
+         const float2 b2 = Cmul(a2, Tw(tw, logG, logQ + 2, j, inv)), b3 = Cmul(a3, Tw(tw, logG, logQ + 2, j + q, inv));
          L[i * es] = Cadd(a0, b2);
          L[(i + 2 * q) * es] = Csub(a0, b2);
          L[(i + q) * es] = Cadd(a1, b3);
@@ -178,7 +182,7 @@ __device__ void DitLines(float2* s, int logN, int nl, int ls, int es, const floa
 struct Dims
 {
    int nxv, nyv, nzv;   // valid extent of the input (volume or PSF)
-   int GX, GY, GZ, H, NK, G, logH, logGY, logGZ;
+   int GX, GY, GZ, H, NK, G, logH, logGY, logGZ, logG, logGX;
 };
 
 // Rows of `in` (nzv x nyv x nxv) -> A[z][k][y], k <= H, y < nyv. grid (ceil(nyv / BY), nzv); smem BY * H float2.
@@ -205,7 +209,7 @@ __global__ void __launch_bounds__(kThreads) XForwardKernel(const float* __restri
       s[b * H + n] = v;
    }
    __syncthreads();
-   DifLines<false>(s, d.logH, BY, H, 1, tw, d.G, false);
+   DifLines<false>(s, d.logH, __ffs(BY) - 1, H, 1, tw, d.logG, false);
    // X[k] = ((Z[k] + conj Z[H-k]) - i W_GX^k (Z[k] - conj Z[H-k])) / 2, Z in bit-reversed order
    for (int t = threadIdx.x; t < (H + 1) * BY; t += blockDim.x)
    {
@@ -215,7 +219,7 @@ __global__ void __launch_bounds__(kThreads) XForwardKernel(const float* __restri
       const float2 zk = s[b * H + Rev(k & (H - 1), d.logH)];
       const float2 zm = Conj(s[b * H + Rev((H - k) & (H - 1), d.logH)]);
       const float2 e = Cadd(zk, zm), o = Csub(zk, zm);
-      const float2 w = Tw(tw, d.G, d.GX, k, false);
+      const float2 w = Tw(tw, d.logG, d.logGX, k, false);
       const float2 wo = Cmul(w, o);   // then times -i: (x, y) -> (y, -x)
       const float2 X = make_float2(0.5f * (e.x + wo.y), 0.5f * (e.y - wo.x));
       A[(static_cast<size_t>(z) * d.NK + k) * d.nyv + y0 + b] = X;
@@ -237,7 +241,7 @@ __global__ void __launch_bounds__(kThreads) YForwardKernel(const float2* __restr
       s[b * N + n] = v;
    }
    __syncthreads();
-   DifLines<false>(s, d.logGY, BK, N, 1, tw, d.G, false);
+   DifLines<false>(s, d.logGY, __ffs(BK) - 1, N, 1, tw, d.logG, false);
    for (int t = threadIdx.x; t < nb * N; t += blockDim.x)
    {
       const int b = t / N, p = t % N;
@@ -265,7 +269,7 @@ __global__ void __launch_bounds__(kThreads) ZKernel(float2* __restrict__ B, Dims
       s[n * BZ + b] = v;
    }
    __syncthreads();
-   DifLines<true>(s, d.logGZ, BZ, 1, BZ, tw, d.G, false);
+   DifLines<true>(s, d.logGZ, __ffs(BZ) - 1, 1, BZ, tw, d.logG, false);
    if (!kConvolve)
    {
       for (int t = threadIdx.x; t < N * BZ; t += blockDim.x)
@@ -283,7 +287,7 @@ __global__ void __launch_bounds__(kThreads) ZKernel(float2* __restrict__ B, Dims
          s[n * BZ + b] = Cmul(s[n * BZ + b], Kh[n * plane + col + b]);
    }
    __syncthreads();
-   DitLines<true>(s, d.logGZ, BZ, 1, BZ, tw, d.G, true);
+   DitLines<true>(s, d.logGZ, __ffs(BZ) - 1, 1, BZ, tw, d.logG, true);
    for (int t = threadIdx.x; t < d.nzv * BZ; t += blockDim.x)
    {
       const int n = t / BZ, b = t % BZ;
@@ -304,7 +308,7 @@ __global__ void __launch_bounds__(kThreads) YInverseKernel(const float2* __restr
       s[b * N + p] = b < nb ? B[(static_cast<size_t>(z) * d.NK + k0 + b) * N + p] : make_float2(0.f, 0.f);
    }
    __syncthreads();
-   DitLines<false>(s, d.logGY, BK, N, 1, tw, d.G, true);
+   DitLines<false>(s, d.logGY, __ffs(BK) - 1, N, 1, tw, d.logG, true);
    for (int t = threadIdx.x; t < nb * d.nyv; t += blockDim.x)
    {
       const int b = t / d.nyv, y = t % d.nyv;
@@ -331,13 +335,13 @@ __global__ void __launch_bounds__(kThreads) XInverseKernel(const float2* __restr
       {
          const float2 xk = A[(static_cast<size_t>(z) * d.NK + k) * d.nyv + y0 + b];
          const float2 xm = Conj(A[(static_cast<size_t>(z) * d.NK + (H - k)) * d.nyv + y0 + b]);
-         const float2 e = Cadd(xk, xm), o = Cmul(Csub(xk, xm), Tw(tw, d.G, d.GX, k, true));
+         const float2 e = Cadd(xk, xm), o = Cmul(Csub(xk, xm), Tw(tw, d.logG, d.logGX, k, true));
          v = make_float2(e.x - o.y, e.y + o.x);   // e + i o
       }
       s[b * H + Rev(k, d.logH)] = v;
    }
    __syncthreads();
-   DitLines<false>(s, d.logH, BY, H, 1, tw, d.G, true);
+   DitLines<false>(s, d.logH, __ffs(BY) - 1, H, 1, tw, d.logG, true);
    const uint32_t W = static_cast<uint32_t>(d.nxv);
    CounterRng u(seed, frame0 + static_cast<uint32_t>(z));
    for (int t = threadIdx.x; t < nb * d.nxv; t += blockDim.x)
@@ -421,6 +425,8 @@ Dims MakeDims(const iscu_wf_plan* p, uint32_t nxv, uint32_t nyv, uint32_t nzv)
    d.logH = p->logH;
    d.logGY = p->logGY;
    d.logGZ = p->logGZ;
+   d.logG = Log2(p->G);
+   d.logGX = Log2(p->GX);
    return d;
 }
 
@@ -474,7 +480,8 @@ static int FinishX(iscu_wf_plan* p, double background, const iscu_camera* cam, u
    st.height = p->ny;
    const CameraView cv = cam ? MakeCameraView(*cam) : CameraView();
    const float scale = static_cast<float>(1.0 / (static_cast<double>(p->GX) * p->GY * p->GZ));
-   const int BY = LinesPerCta(d.H, 16);
+   // Few rows per CTA: the float64 noise chain that ends this pass wants occupancy more than row batching.
+   const int BY = LinesPerCta(d.H, 4);
    XInverseKernel<<<dim3((d.nyv + BY - 1) / BY, d.nzv), kThreads, BY * d.H * sizeof(float2), ctx->stream>>>(
       p->A.as<float2>(), d, BY, static_cast<int>(p->kx / 2), scale, static_cast<float>(background),
       p->tw.as<float2>(), st, cv, cam ? 1 : 0, seed, frame0, image, adu);

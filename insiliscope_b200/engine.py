@@ -362,6 +362,55 @@ class Engine:
         return out[: n.value], frames_out, clamped.value
 
 
+class PsfPlan:
+    """iscu_psf_plan: the per-set PSF work done once; runs over (set index, defocus nm) lists."""
+
+    def __init__(self, engine: Engine, sets, size=0, method=CZT_FP32):
+        self.engine = engine
+        self.lib = engine.lib
+        reqs = (PsfRequest * len(sets))(*[s.c() for s in sets])
+        h = C.c_void_p()
+        check(self.lib.iscu_psf_plan_create(engine.h, reqs, len(sets), size, method, C.byref(h)))
+        self.h = h
+        P, M = C.c_int32(), C.c_int32()
+        check(self.lib.iscu_psf_plan_info(h, C.byref(P), C.byref(M)))
+        self.P, self.M = P.value, M.value
+        engine._plans.add(self)
+
+    def close(self):
+        if self.h:
+            if self.engine.h:
+                self.lib.iscu_psf_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run_dev(self, set_of_dev, defocus_nm_dev, out_dev, normalize=True, sync=True):
+        """set_of_dev: int32/uint32 CUDA tensor, defocus_nm_dev: float64 CUDA tensor, out_dev: (n, P, P) float32."""
+        n = int(set_of_dev.numel())
+        self.engine._before(sync)
+        check(self.lib.iscu_psf_plan_run_dev(self.h, _ptr(set_of_dev), _ptr(defocus_nm_dev), n, int(normalize),
+                                             _ptr(out_dev)))
+        if sync:
+            check(self.lib.iscu_psf_plan_check(self.h))
+        return out_dev
+
+    def check(self):
+        check(self.lib.iscu_psf_plan_check(self.h))
+
+    def run(self, set_of, defocus_nm, normalize=True, out=None):
+        so = np.ascontiguousarray(set_of, dtype=np.uint32)
+        dz = np.ascontiguousarray(defocus_nm, dtype=np.float64)
+        if out is None:
+            out = np.empty((len(so), self.P, self.P), np.float32)
+        check(self.lib.iscu_psf_plan_run(self.h, _ptr(so), _ptr(dz), len(so), int(normalize), _ptr(out)))
+        return out
+
+
 class WidefieldPlan:
     """iscu_wf_plan: the focus series of a dye volume (nz, ny, nx) under a 3D PSF (kz, ky, kx), PSF spectrum resident."""
 

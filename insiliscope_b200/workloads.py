@@ -196,3 +196,55 @@ def widefield_cells(seed: int = 42, nx: int = 512, ny: int = 512, nz: int = 64, 
                        bit_depth=16, em_gain=300.0, cic_electrons=0.002)
     return WidefieldVolume(d, tuple(voxel_nm), psf, (kz, ky, kx), defocus, cam, 5.0, seed, 100.0, 2.0,
                            (seed ^ 0x9E3779B9) & 0xFFFFFFFF)
+
+
+def noll_to_nm(j: int) -> tuple[int, int]:
+    """Noll's single index j >= 1 -> (n, m), m < 0 for the sine modes (Noll 1976 ordering)."""
+    n, j1 = 0, j - 1
+    while j1 > n:
+        n += 1
+        j1 -= n
+    m = (-1) ** j * ((n % 2) + 2 * ((j1 + ((n + 1) % 2)) // 2))
+    return n, m
+
+
+def noll_rms_to_osa_waves(noll: dict) -> list:
+    """Noll-indexed rms-normalized coefficients (waves) -> the reference's 28 OSA/ANSI unnormalized coefficients
+    (waves; ZernikePsf.cpp:58-78 evaluates R_n^m cos/sin without normalization): x sqrt(2 (n + 1)) for m != 0,
+    x sqrt(n + 1) for m = 0; OSA index (n (n + 2) + m) / 2."""
+    out = [0.0] * 28
+    for j, c in noll.items():
+        n, m = noll_to_nm(j)
+        osa = (n * (n + 2) + m) // 2
+        if osa >= 28:
+            raise ValueError(f"Noll {j} (n = {n}) is beyond OSA 27")
+        out[osa] += c * (np.sqrt(2.0 * (n + 1)) if m != 0 else np.sqrt(n + 1.0))
+    return out
+
+
+@dataclass
+class PsfLibrary:
+    """A batched PSF library: request sets and, per PSF, its set and defocus."""
+    sets: list
+    set_of_psf: np.ndarray
+    defocus_nm: np.ndarray
+    size: int
+
+
+def psf_library(seed: int = 42, n_z: int = 64, wavelengths=(520.0, 580.0, 670.0, 750.0), n_aberr: int = 16,
+                pupil: int = 128, size: int = 64, z_step_nm: float = 25.0, rms_waves: float = 0.05) -> PsfLibrary:
+    """The precision config's library: 64 z-planes x 4 wavelengths x 16 Zernike sets = 4,096 PSFs, each a 128 x 128
+    pupil chirp-Z'd to 64 x 64 samples at 4x oversampling of 100 nm pixels; Noll 4-15 ~ N(0, 0.05 lambda rms)
+    (converted to the reference's OSA coefficients); NA 1.45, oil (ni = ns = 1.518); planes 25 nm apart."""
+    rng = np.random.default_rng(seed)
+    aberr = [noll_rms_to_osa_waves({j: rng.normal(0.0, rms_waves) for j in range(4, 16)}) for _ in range(n_aberr)]
+    sets = []
+    for wl in wavelengths:
+        for a in aberr:
+            sets.append(PsfParams(wavelength_nm=wl, na=1.45, immersion_index=1.518, sample_index=1.518,
+                                  pixel_size_nm=100.0, oversampling=4, kernel_half_width_px=8, nz=3,
+                                  z_step_nm=z_step_nm, pupil_samples=pupil, zernike=list(a)))
+    z = (np.arange(n_z) - n_z // 2) * z_step_nm
+    set_of = np.repeat(np.arange(len(sets), dtype=np.uint32), n_z)
+    defocus = np.tile(z, len(sets)).astype(np.float64)
+    return PsfLibrary(sets, set_of, defocus, size)

@@ -33,7 +33,7 @@ def test_fixture_planes(engine, golden_dir, method):
             assert np.argmax(got[z]) == np.argmax(want[z])
 
 
-@pytest.mark.parametrize("method", METHODS)
+@pytest.mark.parametrize("method", [CZT_FP32, CZT_TF32X3])
 def test_library_vs_oracle(engine, oracle, method):
     """The library config's shape (M = 128 pupil -> 64 x 64 at 4x oversampling) with Noll 4-15 aberrations, four
     wavelengths, defocus across +-800 nm, plus a double-helix and a deep, index-mismatched set."""
@@ -72,3 +72,57 @@ def test_kernel_build_vs_reference(engine, reference, method):
     sums = engine.kernel_block_sums(3)
     assert np.abs(sums.sum(axis=(1, 2)) - 16.0).max() < 1e-3
     assert np.abs(sums - k.block_sums()).max() <= TOL * k.block_sums().max()
+
+
+@pytest.mark.parametrize("M,P,nz", [(96, 48, 5), (128, 64, 40), (64, 33, 3), (112, 64, 300)])
+def test_tf32x3_shapes_vs_oracle(engine, oracle, M, P, nz):
+    """The tensor-core path on padded shapes (2P < 128 rows, 2M < 256 K) and more PSFs than SMs (the persistent
+    loop), against the float64 oracle, plane by plane."""
+    rng = np.random.default_rng(M + P)
+    z = np.zeros(28)
+    z[3:15] = rng.normal(0.0, 0.08, 12)
+    req = PsfParams(wavelength_nm=600.0, na=1.4, pixel_size_nm=100.0, oversampling=4, kernel_half_width_px=8,
+                    nz=3, z_step_nm=25.0, pupil_samples=M, zernike=list(z))
+    dz = rng.uniform(-700.0, 700.0, nz)
+    got = engine.psf_library_dev([req], np.zeros(nz, np.uint32), dz, size=P, normalize=True,
+                                 method=CZT_TF32X3).cpu().numpy()
+    idx = list(range(0, nz, max(1, nz // 6)))
+    want = oracle.psf_planes(req, dz[idx] * 1e-9, size=P, normalize=True)
+    for j, i in enumerate(idx):
+        assert np.abs(got[i] - want[j]).max() <= TOL * want[j].max(), i
+
+
+def test_tf32x3_matches_fp32(engine):
+    """The two chirp-Z forms agree (both within 1e-5 of float64) on a library of 4 sets, two of them double helix."""
+    rng = np.random.default_rng(77)
+    sets = [PsfParams(wavelength_nm=wl, na=1.45, pixel_size_nm=100.0, oversampling=4, kernel_half_width_px=8, nz=3,
+                      pupil_samples=128, double_helix=dh) for wl, dh in ((520.0, False), (580.0, True),
+                                                                           (670.0, False), (750.0, True))]
+    set_of = rng.integers(0, 4, 512).astype(np.uint32)
+    dz = rng.uniform(-800.0, 800.0, 512)
+    a = engine.psf_library_dev(sets, set_of, dz, size=64, method=CZT_FP32).cpu().numpy()
+    b = engine.psf_library_dev(sets, set_of, dz, size=64, method=CZT_TF32X3).cpu().numpy()
+    assert np.abs(a - b).max() <= 2 * TOL * a.max()
+
+
+@pytest.mark.parametrize("method", [CZT_FP32, CZT_TF32X3])
+def test_plan_matches_library(engine, method):
+    """A PSF plan (per-set work once, device-resident runs) gives the one-shot library call's planes, bit for bit."""
+    import torch
+    from insiliscope_b200 import PsfPlan
+    from insiliscope_b200.workloads import psf_library
+    L = psf_library(seed=3, n_z=8, n_aberr=3)
+    plan = PsfPlan(engine, L.sets, size=L.size, method=method)
+    d_set = torch.from_numpy(L.set_of_psf.view(np.int32)).cuda()
+    d_dz = torch.from_numpy(L.defocus_nm).cuda()
+    out = torch.empty((len(L.set_of_psf), 64, 64), dtype=torch.float32, device="cuda")
+    got = plan.run_dev(d_set, d_dz, out).cpu().numpy()
+    want = engine.psf_library_dev(L.sets, L.set_of_psf, L.defocus_nm, size=64, method=method).cpu().numpy()
+    assert np.array_equal(got, want)
+    assert np.array_equal(plan.run(L.set_of_psf, L.defocus_nm), want)
+    bad = L.set_of_psf.copy()
+    bad[3] = 999
+    from insiliscope_b200 import IscuError
+    with pytest.raises(IscuError):
+        plan.run(bad, L.defocus_nm)
+    plan.close()
