@@ -200,7 +200,7 @@ class SmlmWorkload:
         return mv.frames * (px * 14 + 24) + self.n_emitters * 32 + nz * bw * bw * 4
 
     def kernel_name(self):
-        return "RenderFramesKernel"
+        return "RenderTilesKernel"
 
     # -------------------------------------------------- the reference on the host cores
     dtype = "f64"
@@ -231,6 +231,106 @@ class SmlmWorkload:
         mv = self.mv
         t, _, adu = self.rk.render_movie(mv.events, self.frame0, mv.frames, mv.width, mv.height, mv.pixel_nm,
                                          mv.photons_per_blink, mv.background, mv.camera, *self.maps, mv.noise_seed)
+        return t
+
+
+class TwoColourWorkload(SmlmWorkload):
+    """The uneven two-colour movie: 256 x 256 px, 1,024 frames of 10 to ~8,000 ON emitters (Poisson, lognormal
+    per-frame mean), channel 0 (670 nm double helix) then channel 1 (580 nm astigmatic) splatted onto each frame,
+    then the sCMOS chain. The render form (tile shape, grid or persistent heaviest-frame-first) is autotuned once on
+    the batch, and one step replays the batch's render captured in a CUDA graph."""
+    name = ("two-colour uneven SMLM 256x256 px, 1024 frames, Poisson ON counts with lognormal per-frame mean "
+            "(median 300, clipped 10-8000), 670 nm double-helix + 580 nm astigmatic (Noll 5 = 0.1 lambda) 129^2x49 "
+            "cubic PSFs, sCMOS")
+
+    def __init__(self, rank: int):
+        from insiliscope_b200.workloads import two_colour_uneven
+        self.frame0 = rank * 1024
+        self.mv = two_colour_uneven(seed=42, frame0=self.frame0)
+
+    def setup(self, device: int):
+        import torch
+        from insiliscope_b200 import CZT_FP32, Engine, RenderGraph, generate_camera_maps
+        mv = self.mv
+        self.eng = eng = Engine(device)
+        t0 = time.perf_counter()
+        for slot, psf in enumerate(mv.psfs):
+            eng.kernel_build(slot, psf, CZT_FP32)
+        eng.synchronize()
+        self.psf_build_ms = (time.perf_counter() - t0) * 1e3
+        off, gain, rn = generate_camera_maps(mv.width, mv.height, mv.map_seed, mv.offset_mean, mv.offset_std,
+                                             mv.gain_nominal, mv.gain_std_fraction, mv.read_noise_nominal,
+                                             mv.read_noise_std_fraction)
+        eng.set_static(mv.width, mv.height, offset=off, gain=gain, read_noise=rn, flat_bg=mv.background)
+        self.ems, self.frames, _ = eng.collect_emitters(-1, mv.events, mv.bucket_start, self.frame0, mv.width,
+                                                        mv.height, mv.pixel_nm, mv.photons_per_blink)
+        self.ems = self.ems.copy()
+        dev = f"cuda:{device}"
+        self.d_em = torch.from_numpy(self.ems.view(np.uint8)).to(dev)
+        self.d_fr = torch.from_numpy(self.frames.view(np.uint8)).to(dev)
+        self.d_adu = torch.empty((mv.frames, mv.height, mv.width), dtype=torch.uint16, device=dev)
+        t0 = time.perf_counter()
+        self.autotune_ms = eng.render_autotune(self.d_em, self.d_fr, mv.frames, mv.camera, mv.noise_seed, self.d_adu)
+        self.autotune_wall_ms = (time.perf_counter() - t0) * 1e3
+        self.form = eng.render_config()
+        self.graph = RenderGraph(eng, self.d_em, self.d_fr, mv.frames, mv.camera, mv.noise_seed, None, self.d_adu)
+        self.stream = eng.torch_stream()
+        self.frames_per_step = mv.frames
+        self.n_emitters = len(self.ems)
+
+    def device_step(self):
+        self.graph.launch(sync=False)
+
+    def e2e_step(self):
+        """Host blink events -> host ADU through the C ABI: collection (each event's own kernel slot), H2D, render in
+        the autotuned form, D2H."""
+        mv = self.mv
+        ems, frames, _ = self.eng.collect_emitters(-1, mv.events, mv.bucket_start, self.frame0, mv.width, mv.height,
+                                                   mv.pixel_nm, mv.photons_per_blink, out=self._e2e_buf(),
+                                                   frames_out=self._e2e_frames())
+        _, adu = self.eng.render_frames(ems, frames, mv.camera, mv.noise_seed, want_photons=False)
+        return adu
+
+    def alg_bytes_per_launch(self):
+        mv = self.mv
+        px = mv.width * mv.height
+        sums = 0
+        for slot in range(len(mv.psfs)):
+            _, nz, _, bw = self.eng.kernel_info(slot)
+            sums += nz * bw * bw * 8
+        return mv.frames * (px * 14 + 24) + self.n_emitters * 32 + sums
+
+    def config_extra(self):
+        tw, th = self.form[1], self.form[2]
+        return {"render_form": {"config": self.form[0], "tile": f"{tw}x{th}", "persistent": self.form[3],
+                                "autotune_ms_per_form": [round(x, 4) for x in self.autotune_ms]},
+                "cuda_graph": True, "mean_emitters_per_frame": self.n_emitters / self.mv.frames,
+                "max_emitters_per_frame": int(self.frames["em_count"].max())}
+
+    cpu_sample = ("the whole 1024-frame movie per step: per frame the reference's RenderPhotonImage for channel 0, "
+                  "then for channel 1 accumulating onto it (each with its own kernel), then ApplyNoiseChain; frames in "
+                  "parallel on its own thread pool (ParallelFor), kernels built once before timing")
+    frames_per_step_cpu = 1024
+
+    def reference_setup(self, threads=0):
+        from oracle.oracle import Reference
+        from insiliscope_b200 import generate_camera_maps
+        mv = self.mv
+        if not Reference.available():
+            raise RuntimeError("the reference harness oracle/_ref/libiscref.so is not built (it needs the reference "
+                               "tree at build time)")
+        self.ref = Reference()
+        self.ref.set_threads(threads)
+        self.rks = [self.ref.kernel(req=p) for p in mv.psfs]
+        self.maps = generate_camera_maps(mv.width, mv.height, mv.map_seed, mv.offset_mean, mv.offset_std,
+                                         mv.gain_nominal, mv.gain_std_fraction, mv.read_noise_nominal,
+                                         mv.read_noise_std_fraction)
+
+    def reference_step(self):
+        mv = self.mv
+        t, _, _ = self.ref.render_movie_groups(self.rks, mv.events, self.frame0, mv.frames, mv.width, mv.height,
+                                               mv.pixel_nm, mv.photons_per_blink, mv.background, mv.camera,
+                                               *self.maps, mv.noise_seed)
         return t
 
 
@@ -454,7 +554,8 @@ class PsfLibraryWorkload:
         return time.perf_counter() - t0
 
 
-WORKLOADS = {"smlm": SmlmWorkload, "widefield": WidefieldWorkload, "psflib": PsfLibraryWorkload}
+WORKLOADS = {"smlm": SmlmWorkload, "widefield": WidefieldWorkload, "psflib": PsfLibraryWorkload,
+             "two-colour": TwoColourWorkload}
 
 
 # ----------------------------------------------------------------------------------------------------- arms
@@ -554,7 +655,8 @@ def run_ours(args):
             "vs_baseline": None, "dtype": w.dtype, "data": "synthetic",
             "config": {"workload": w.name, "frames_per_step": w.frames_per_step, "emitters_per_step": w.n_emitters,
                        "l2": "flushed before every timed step (256 MB write)", "parallelism": f"frames x{world}",
-                       "psf_build_ms": round(w.psf_build_ms, 3)},
+                       "psf_build_ms": round(w.psf_build_ms, 3), **(w.config_extra() if hasattr(w, "config_extra")
+                                                                     else {})},
             "e2e": {"value": world * w.frames_per_step / (e2e_ms / 1e3), "unit": w.metric, "ms_per_step": e2e_ms,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "timing": "host wall clock per step (blocking C-ABI calls), max over ranks"},

@@ -258,6 +258,26 @@ int iscu_render_frames_dev(iscu_ctx* ctx, const iscu_emitter* emitters_dev, cons
 int iscu_render_frames(iscu_ctx* ctx, const iscu_emitter* emitters, uint32_t n_emitters, const iscu_frame* frames,
                        uint32_t n_frames, const iscu_camera* cam, uint32_t seed, float* photons, uint16_t* adu);
 
+/* The render kernel's form (no reference counterpart: the reference renders a frame per CPU task, ParallelFor over
+ * frames, ScopeMovie.cpp:7059-7110). config 0..2: one CTA per (frame, tile) with tiles 16x16, 32x8, 8x32; 3..5: the
+ * same tiles in a persistent grid that takes (frame, tile) items heaviest frame first, for batches whose frames carry
+ * very different emitter counts. Every form gives the same bits. */
+int iscu_render_set_config(iscu_ctx* ctx, int32_t config);
+int iscu_render_get_config(iscu_ctx* ctx, int32_t* config, int32_t* tile_w, int32_t* tile_h, int32_t* persistent);
+/* Times the six forms on the given device batch (one warm-up and two timed renders each, adu_dev overwritten),
+ * keeps the fastest as the context's form; ms6 (nullable) receives each form's milliseconds per render. */
+int iscu_render_autotune(iscu_ctx* ctx, const iscu_emitter* emitters_dev, const iscu_frame* frames_dev,
+                         uint32_t n_frames, const iscu_camera* cam, uint32_t seed, uint16_t* adu_dev, float* ms6);
+/* iscu_render_frames_dev with the context's current form captured once into a CUDA graph on the context's stream;
+ * each launch replays it (the same device pointers, so refill them in place between launches). Kernel slots and
+ * camera statics must not be rebuilt while the graph lives. */
+typedef struct iscu_render_graph iscu_render_graph;
+int iscu_render_graph_create(iscu_ctx* ctx, const iscu_emitter* emitters_dev, const iscu_frame* frames_dev,
+                             uint32_t n_frames, const iscu_camera* cam, uint32_t seed, float* photons_dev,
+                             uint16_t* adu_dev, iscu_render_graph** out);
+int iscu_render_graph_launch(iscu_render_graph* graph);
+void iscu_render_graph_destroy(iscu_render_graph* graph);
+
 /* GpuSimulator::RenderFrames / SplatGpuHost::RenderFrames (GpuSimD3D11.h:98-107, SplatGpu.h:57-62) over the
  * reference's 64-byte records: the D3D11/WGSL shader's semantics (GpuSimD3D11.cpp:169-248) -- the record's float
  * weights, the halo radius test, an optional extra photon image per frame (extras: n_frames*w*h host floats, or NULL;
@@ -269,18 +289,22 @@ int iscu_render_gpu_records(iscu_ctx* ctx, const iscu_gpu_splat_emitter* emitter
 
 /* ---------------------------------------------------------------- host-side emitter collection ---------------- */
 
-/* sim::BlinkEvent (SMLMSimulation.h:82-102), the fields the render reads. */
+/* sim::BlinkEvent (SMLMSimulation.h:82-102), the fields the render reads, plus the kernel slot of the event's dye
+ * group (the engine renders each group with its own PSF kernel, ScopeMovie.cpp:7059-7110). */
 typedef struct iscu_blink_event {
    double x_um, y_um, z_nm;
    double t_start, t_end;
    double brightness;
    double excite;
-   double reserved;
+   int32_t slot;       /* used when the collecting call's slot is -1 */
+   int32_t reserved;
 } iscu_blink_event;
 
 /* CollectFrameEmitters (SMLMSimulation.cpp:55-101) for one frame: the events overlapping [frame, frame+1), in order,
- * as iscu_emitter records (kernel slot `slot`, z plane from the slot's stack by NearestZIndex,
- * PsfGeneratorBridge.cpp:40-61), min_photons applied (RenderPhotonImage's blink-min-photons). illum: the
+ * as iscu_emitter records (kernel slot `slot`, or each event's own slot when slot is -1; z plane from that slot's
+ * stack by NearestZIndex, PsfGeneratorBridge.cpp:40-61), min_photons applied (RenderPhotonImage's
+ * blink-min-photons). Several dye groups in one frame: put each group's events in the bucket one group after the
+ * other, as the engine renders them (one RenderPhotonImage per group, accumulating). illum: the
  * illumination field (w*h host floats) or NULL. Writes at most max_out records; *n_out gets the count. Returns
  * ISCU_ERR_LIMIT when max_out is too small. *n_clamped (nullable) += emitters whose z was clamped. */
 int iscu_collect_frame_emitters(iscu_ctx* ctx, int32_t slot, const iscu_blink_event* events, uint32_t n_events,

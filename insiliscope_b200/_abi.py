@@ -87,7 +87,7 @@ class Frame(C.Structure):
 class BlinkEvent(C.Structure):
     _fields_ = [("x_um", C.c_double), ("y_um", C.c_double), ("z_nm", C.c_double), ("t_start", C.c_double),
                 ("t_end", C.c_double), ("brightness", C.c_double), ("excite", C.c_double),
-                ("reserved", C.c_double)]
+                ("slot", C.c_int32), ("reserved", C.c_int32)]
 
 
 # name -> (restype, argtypes); every function include/iscu.h declares.
@@ -127,6 +127,13 @@ SIGNATURES = {
     "iscu_kernel_get_block_sums": (C.c_int, [vp, C.c_int32, vp]),
     "iscu_render_frames_dev": (C.c_int, [vp, vp, vp, C.c_uint32, C.POINTER(Camera), C.c_uint32, vp, vp]),
     "iscu_render_frames": (C.c_int, [vp, vp, C.c_uint32, vp, C.c_uint32, C.POINTER(Camera), C.c_uint32, vp, vp]),
+    "iscu_render_set_config": (C.c_int, [vp, C.c_int32]),
+    "iscu_render_get_config": (C.c_int, [vp, i32p, i32p, i32p, i32p]),
+    "iscu_render_autotune": (C.c_int, [vp, vp, vp, C.c_uint32, C.POINTER(Camera), C.c_uint32, vp, f32p]),
+    "iscu_render_graph_create": (C.c_int, [vp, vp, vp, C.c_uint32, C.POINTER(Camera), C.c_uint32, vp, vp,
+                                           C.POINTER(vp)]),
+    "iscu_render_graph_launch": (C.c_int, [vp]),
+    "iscu_render_graph_destroy": (None, [vp]),
     "iscu_render_gpu_records": (C.c_int, [vp, vp, C.c_uint32, vp, C.c_uint32, vp, C.POINTER(Camera), C.c_uint32,
                                           vp]),
     "iscu_collect_frame_emitters": (C.c_int, [vp, C.c_int32, vp, C.c_uint32, C.c_int64, C.c_uint32, C.c_uint32,

@@ -24,6 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # unit -> extra flags
 UNITS = {
     "splat_noise.cu": ["--fmad=false"],
+    "render.cu": ["--fmad=false"],
     "psf.cu": [],
     "psf_tc.cu": [],
     "psf_noalloc.cu": [],

@@ -410,7 +410,11 @@ static int FinishKernelSlot(iscu_ctx* ctx, KernelSlot& k)
 {
    k.bw = k.size + k.os - 1;
    ISCU_CK(k.sums.Reserve(static_cast<size_t>(k.nz) * k.bw * k.bw * sizeof(float)));
+   const size_t nSums = static_cast<size_t>(k.nz) * k.bw * k.bw;
+   ISCU_CK(k.sums64.Reserve(nSums * sizeof(double)));
    int rc = LaunchBlockSums(ctx, k.planes.as<float>(), k.size, k.os, k.nz, k.sums.as<float>());
+   if (rc == ISCU_OK)
+      rc = LaunchSumsToDouble(ctx, k.sums.as<float>(), nSums, k.sums64.as<double>());
    if (rc != ISCU_OK)
       return rc;
    ISCU_CK(cudaStreamSynchronize(ctx->stream));
@@ -645,7 +649,7 @@ namespace {
 // One frame's emitters (CollectFrameEmitters, SMLMSimulation.cpp:55-101, then the blink-min-photons filter,
 // :152-156) from the events ev(j) for j in [j0, j1), appended to out[n ..]. Returns ISCU_ERR_LIMIT when out is full.
 template <class EventAt>
-int CollectFrame(const KernelSlot& k, int32_t slot, EventAt ev, uint32_t j0, uint32_t j1, int64_t frame,
+int CollectFrame(const KernelSlot* kernels, int32_t callSlot, EventAt ev, uint32_t j0, uint32_t j1, int64_t frame,
                  uint32_t width, uint32_t height, double pixel_size_nm, double photons_per_blink, double drift_x_px,
                  double drift_y_px, double global_z_offset_um, const float* illum, double min_photons,
                  iscu_emitter* out, uint32_t max_out, uint32_t& n, int64_t* n_clamped)
@@ -653,6 +657,10 @@ int CollectFrame(const KernelSlot& k, int32_t slot, EventAt ev, uint32_t j0, uin
    for (uint32_t j = j0; j < j1; ++j)
    {
       const iscu_blink_event& e = ev(j);
+      const int32_t slot = callSlot >= 0 ? callSlot : e.slot;
+      if (slot < 0 || slot >= ISCU_MAX_KERNELS || !kernels[slot].valid)
+         return Fail(ISCU_ERR_STATE, "event " + std::to_string(j) + ": no kernel stack in its slot");
+      const KernelSlot& k = kernels[slot];
       double ov = std::min(static_cast<double>(frame + 1), e.t_end) - std::max(static_cast<double>(frame), e.t_start);
       if (ov <= 0.0)
          continue;
@@ -708,13 +716,13 @@ int iscu_collect_frame_emitters(iscu_ctx* ctx, int32_t slot, const iscu_blink_ev
                                 double global_z_offset_um, const float* illum, double min_photons,
                                 iscu_emitter* out, uint32_t max_out, uint32_t* n_out, int64_t* n_clamped)
 {
-   int rc = CheckSlot(ctx, slot, true);
+   int rc = slot == -1 ? (ctx ? ISCU_OK : Fail(ISCU_ERR_ARG, "null context")) : CheckSlot(ctx, slot, true);
    if (rc != ISCU_OK)
       return rc;
    if ((n_events && !events) || !n_out || (max_out && !out) || width == 0 || height == 0)
       return Fail(ISCU_ERR_ARG, "null argument or empty frame");
    uint32_t n = 0;
-   rc = CollectFrame(ctx->kernels[slot], slot, [&](uint32_t j) -> const iscu_blink_event& { return events[j]; }, 0,
+   rc = CollectFrame(ctx->kernels, slot, [&](uint32_t j) -> const iscu_blink_event& { return events[j]; }, 0,
                      n_events, frame, width, height, pixel_size_nm, photons_per_blink, drift_x_px, drift_y_px,
                      global_z_offset_um, illum, min_photons, out, max_out, n, n_clamped);
    *n_out = n;
@@ -728,14 +736,14 @@ int iscu_collect_emitters(iscu_ctx* ctx, int32_t slot, const iscu_blink_event* e
                           const float* illum, double min_photons, iscu_emitter* out, uint32_t max_out,
                           iscu_frame* frames_out, uint32_t* n_out, int64_t* n_clamped)
 {
-   int rc = CheckSlot(ctx, slot, true);
+   int rc = slot == -1 ? (ctx ? ISCU_OK : Fail(ISCU_ERR_ARG, "null context")) : CheckSlot(ctx, slot, true);
    if (rc != ISCU_OK)
       return rc;
    if (!bucket_start || !n_out || (n_frames && !frames_out) || (max_out && !out) || width == 0 || height == 0)
       return Fail(ISCU_ERR_ARG, "null argument or empty frame");
    if (bucket_start[n_frames] > bucket_start[0] && !events)
       return Fail(ISCU_ERR_ARG, "null events");
-   const KernelSlot& k = ctx->kernels[slot];
+   const KernelSlot* k = ctx->kernels;
    uint32_t n = 0;
    for (uint32_t f = 0; f < n_frames; ++f)
    {

@@ -103,6 +103,7 @@ struct PinnedBuf
 struct KernelView
 {
    const float* sums = nullptr;     // nz planes of bw x bw block sums, row-major
+   const double* sums64 = nullptr;  // the same values widened to float64 (what the render kernels read)
    const int16_t* spanLo = nullptr; // halo cut: [z * (2 camRad + 1) + dy + camRad]; nullptr: the whole square
    const int16_t* spanHi = nullptr;
    const int32_t* radius2 = nullptr;
@@ -117,6 +118,7 @@ struct KernelSlot
    double zStepNm = 0.0;
    DevBuf planes;    // nz * size * size
    DevBuf sums;      // nz * bw * bw
+   DevBuf sums64;    // nz * bw * bw float64 copies of sums
    DevBuf spanLo, spanHi, radius2;
    bool halo = false;
    double haloThreshold = 0.0;
@@ -125,6 +127,7 @@ struct KernelSlot
    {
       KernelView v;
       v.sums = sums.as<float>();
+      v.sums64 = sums64.as<double>();
       v.spanLo = halo ? spanLo.as<int16_t>() : nullptr;
       v.spanHi = halo ? spanHi.as<int16_t>() : nullptr;
       v.radius2 = halo ? radius2.as<int32_t>() : nullptr;
@@ -171,6 +174,8 @@ struct iscu_ctx
    std::recursive_mutex mu;
    std::atomic<uint64_t> launches{0};
    int smCount = 0;
+   int renderConfig = 0;           // render kernel form (iscu_render_set_config)
+   iscu::DevBuf dOrder;            // persistent render: frame order + work counter
    iscu::KernelSlot kernels[ISCU_MAX_KERNELS];
    // camera statics
    bool haveStatic = false;
@@ -212,6 +217,7 @@ int LaunchRenderGpuRecords(iscu_ctx* ctx, const iscu_gpu_splat_emitter* ems, con
                            uint32_t nFrames, const float* extras, const CameraView* cam, uint32_t seed,
                            uint16_t* adu);
 int LaunchBlockSums(iscu_ctx* ctx, const float* planes, int n, int os, int nz, float* sums);
+int LaunchSumsToDouble(iscu_ctx* ctx, const float* in, size_t n, double* out);
 int LaunchNormalizePlanes(iscu_ctx* ctx, float* planes, int planeElems, int nPlanes);
 // defocusM: each PSF's defocus in metres (the reference's resAxialM * (z - (nz - 1) / 2) for a stack's plane z).
 int BuildPsfLibrary(iscu_ctx* ctx, const iscu_psf_request* sets, uint32_t nSets, const uint32_t* setOfPsf,

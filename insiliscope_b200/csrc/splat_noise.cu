@@ -1,21 +1,13 @@
-// The per-frame hot path on sm_100a: blink splat fused with the camera noise chain, plus the block sums the splat
-// reads and the bare counter-RNG kernels.
+// sm_100a kernels beside the render (render.cu): the reference's 64-byte GPU records (the D3D11/WebGPU shader's
+// semantics), the noise chain on given photon images, the bare counter RNG, and the block sums the splat reads.
 //
 // Compiled with --fmad=false: every float64/float32 multiply and add rounds on its own, as the reference's
-// -ffp-contract=off build does, so the noise-free image and the ADU are bit for bit the CPU's.
-//
-// Splat (RenderPhotonImage, adapter/inSiliScope/Simulation/SMLMSimulation.cpp:103-160, over SplatRows /
-// SplatKernel.inl:80-167): a pixel starts at the background and adds, in the frame's emitter order,
-// float(photons * sum_j wy[j] * (sum_i wx[i] * B[r0 + j][c0 + i])) in float64 -- taps outside the block-sum array
-// skipped, the halo cut's columns only. One CTA owns a 16 x 16 pixel tile of one frame: it streams the frame's
-// emitter list through shared memory 256 records at a time, keeps (in order, by a warp-ballot compaction) the ones
-// whose square reaches the tile, derives their SplatSetup (PsfGeneratorBridge.cpp:1382-1422) once, and every thread
-// then gathers onto its own pixel. The noise chain (ApplyNoiseChain, SMLMNoise.cpp:142-216) follows in registers,
-// so the photon image never has to touch HBM.
+// -ffp-contract=off build does.
 
 #include "counter_rng.cuh"
 #include "iscu_internal.h"
 #include "noise_chain.cuh"
+#include "splat_common.cuh"
 
 #include <cstdint>
 
@@ -24,195 +16,6 @@ namespace iscu {
 namespace {
 
 constexpr int kTileX = 16, kTileY = 16, kThreads = kTileX * kTileY, kChunk = kThreads;
-
-// The background of pixel i for a frame (RenderPhotonImage's background lambda, SMLMSimulation.cpp:124-137).
-__device__ __forceinline__ float Background(const StaticView& st, uint32_t i, double bgScale)
-{
-   double bg = st.background ? static_cast<double>(st.background[i]) : st.flatBg;
-   if (st.illum)
-      bg *= static_cast<double>(st.illum[i]);
-   return static_cast<float>(bg * bgScale);
-}
-
-// ---------------------------------------------------------------------------------------------------------- splat
-struct Kernels
-{
-   KernelView k[ISCU_MAX_KERNELS];
-};
-
-struct StagedEmitter
-{
-   double photons;
-   double wx[4], wy[4];
-   int x0, y0, bx, by;
-   int nTaps, slot, plane, pad;
-};
-
-// JS Math.round (ties toward +infinity): PsfGeneratorBridge.cpp:1245-1248.
-__device__ __forceinline__ double RoundHalfUp(double v) { return floor(v + 0.5); }
-
-__device__ __forceinline__ void CatmullRom(double f, double* w)
-{
-   const double f2 = f * f, f3 = f2 * f;
-   w[0] = -0.5 * f3 + f2 - 0.5 * f;
-   w[1] = 1.5 * f3 - 2.5 * f2 + 1.0;
-   w[2] = -1.5 * f3 + 2.0 * f2 + 0.5 * f;
-   w[3] = 0.5 * f3 - 0.5 * f2;
-}
-
-// SplatSetup (PsfGeneratorBridge.cpp:1382-1422) in float64.
-__device__ __forceinline__ void Setup(const KernelView& kv, double xPx, double yPx, StagedEmitter& s)
-{
-   const int os = kv.os;
-   const double kc = kv.kc;
-   s.x0 = static_cast<int>(RoundHalfUp(xPx));
-   s.y0 = static_cast<int>(RoundHalfUp(yPx));
-   const double tx = kc + (s.x0 - xPx - 0.5) * os + 0.5;
-   const double ty = kc + (s.y0 - yPx - 0.5) * os + 0.5;
-   for (int k = 0; k < 4; ++k)
-   {
-      s.wx[k] = k == 0 ? 1.0 : 0.0;
-      s.wy[k] = k == 0 ? 1.0 : 0.0;
-   }
-   if (kv.interp == ISCU_INTERP_NEAREST)
-   {
-      s.bx = static_cast<int>(floor(tx + 0.5));
-      s.by = static_cast<int>(floor(ty + 0.5));
-      s.nTaps = 1;
-      return;
-   }
-   const int bx = static_cast<int>(floor(tx)), by = static_cast<int>(floor(ty));
-   const double fx = tx - bx, fy = ty - by;
-   if (kv.interp == ISCU_INTERP_CUBIC)
-   {
-      s.bx = bx - 1;
-      s.by = by - 1;
-      s.nTaps = 4;
-      CatmullRom(fx, s.wx);
-      CatmullRom(fy, s.wy);
-      return;
-   }
-   s.bx = bx;
-   s.by = by;
-   s.nTaps = 2;
-   s.wx[0] = 1.0 - fx;
-   s.wx[1] = fx;
-   s.wy[0] = 1.0 - fy;
-   s.wy[1] = fy;
-}
-
-// One staged emitter's contribution to pixel (X, Y), added to acc (SplatKernel.inl:51-75 per pixel).
-__device__ __forceinline__ void SplatOne(const StagedEmitter& e, const KernelView& kv, int X, int Y, float& acc)
-{
-   const int camRad = kv.camRad;
-   const int dx = X - e.x0, dy = Y - e.y0;
-   if (dx < -camRad || dx > camRad || dy < -camRad || dy > camRad)
-      return;
-   if (kv.spanLo)
-   {
-      const int row = e.plane * (2 * camRad + 1) + dy + camRad;
-      if (dx < kv.spanLo[row] || dx > kv.spanHi[row])
-         return;
-   }
-   const int os = kv.os, off = os - 1, bw = kv.bw, nt = e.nTaps;
-   const int r0 = e.by + dy * os + off, c0 = e.bx + dx * os + off;
-   const int jLo = max(0, -r0), jHi = min(nt, bw - r0);
-   const int iLo = max(0, -c0), iHi = min(nt, bw - c0);
-   const float* B = kv.sums + static_cast<size_t>(e.plane) * bw * bw;
-   double sum = 0.0;
-   for (int j = jLo; j < jHi; ++j)
-   {
-      const float* brow = B + static_cast<size_t>(r0 + j) * bw + c0;
-      double row = 0.0;
-      for (int i = iLo; i < iHi; ++i)
-         row += e.wx[i] * static_cast<double>(__ldg(brow + i));
-      sum += e.wy[j] * row;
-   }
-   acc += static_cast<float>(e.photons * sum);
-}
-
-// Stages one chunk of the frame's emitters: the ones reaching this tile, in list order, with their setup. Returns
-// how many were kept. Every thread of the CTA calls it (it synchronizes).
-__device__ __forceinline__ int StageChunk(const iscu_emitter* __restrict__ ems, uint32_t start, uint32_t count,
-                                          const Kernels& K, int tx0, int ty0, int tx1, int ty1, StagedEmitter* sEm,
-                                          int* sWarp)
-{
-   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-   bool keep = false;
-   StagedEmitter s;
-   if (static_cast<uint32_t>(t) < count)
-   {
-      const iscu_emitter em = ems[start + t];
-      const int slot = static_cast<int>(static_cast<uint32_t>(em.plane) >> 16), plane = em.plane & 0xffff;
-      if (slot < ISCU_MAX_KERNELS && em.photons > 0.0)
-      {
-         const KernelView& kv = K.k[slot];
-         if (kv.sums && plane < kv.nz)
-         {
-            Setup(kv, em.x_px, em.y_px, s);
-            s.photons = em.photons;
-            s.slot = slot;
-            s.plane = plane;
-            const int r = kv.camRad;
-            keep = s.x0 + r >= tx0 && s.x0 - r <= tx1 && s.y0 + r >= ty0 && s.y0 - r <= ty1;
-         }
-      }
-   }
-   const unsigned ballot = __ballot_sync(0xffffffffu, keep);
-   if (lane == 0)
-      sWarp[warp] = __popc(ballot);
-   __syncthreads();
-   int base = 0, total = 0;
-#pragma unroll
-   for (int w = 0; w < kThreads / 32; ++w)
-   {
-      const int c = sWarp[w];
-      base += w < warp ? c : 0;
-      total += c;
-   }
-   if (keep)
-      sEm[base + __popc(ballot & ((1u << lane) - 1u))] = s;
-   __syncthreads();
-   return total;
-}
-
-template <bool kNoise>
-__global__ void __launch_bounds__(kThreads) RenderFramesKernel(const iscu_emitter* __restrict__ ems,
-                                                                 const iscu_frame* __restrict__ frames, Kernels K,
-                                                                 StaticView st, CameraView cam, uint32_t seed,
-                                                                 float* __restrict__ photonsOut,
-                                                                 uint16_t* __restrict__ aduOut)
-{
-   __shared__ StagedEmitter sEm[kChunk];
-   __shared__ int sWarp[kThreads / 32];
-   const iscu_frame fr = frames[blockIdx.z];
-   const int tx0 = blockIdx.x * kTileX, ty0 = blockIdx.y * kTileY;
-   const int X = tx0 + (threadIdx.x % kTileX), Y = ty0 + (threadIdx.x / kTileX);
-   const int W = static_cast<int>(st.width), H = static_cast<int>(st.height);
-   const int tx1 = min(tx0 + kTileX, W) - 1, ty1 = min(ty0 + kTileY, H) - 1;
-   const bool inside = X < W && Y < H;
-   const uint32_t i = static_cast<uint32_t>(Y) * st.width + static_cast<uint32_t>(X);
-   float acc = inside ? Background(st, i, fr.bg_scale) : 0.0f;
-   for (uint32_t e0 = 0; e0 < fr.em_count; e0 += kChunk)
-   {
-      const uint32_t cnt = min(static_cast<uint32_t>(kChunk), fr.em_count - e0);
-      const int kept = StageChunk(ems, fr.em_start + e0, cnt, K, tx0, ty0, tx1, ty1, sEm, sWarp);
-      if (inside)
-         for (int k = 0; k < kept; ++k)
-            SplatOne(sEm[k], K.k[sEm[k].slot], X, Y, acc);
-      __syncthreads();
-   }
-   if (!inside)
-      return;
-   const size_t o = static_cast<size_t>(blockIdx.z) * st.width * st.height + i;
-   if (photonsOut)
-      photonsOut[o] = acc;
-   if (kNoise)
-   {
-      CounterRng u(seed, fr.frame);
-      aduOut[o] = NoisePixel(acc, i, cam, st, u);
-   }
-}
 
 // ------------------------------------------------------------------- the reference's 64-byte record (D3D11 path)
 struct StagedRecord
@@ -223,6 +26,9 @@ struct StagedRecord
    int nTaps, slot, plane, cutR2;
 };
 
+// GpuSimD3D11.cpp:169-248 / SplatGpu.wgsl: one thread per pixel gathers the frame's records in list order (the
+// record's float weights, the halo radius test, the halo spans), taps summed in float64 here; the frame's other light
+// (background, extra image) first, as SplatGpuHost splats the blinks onto it; then the noise chain.
 __global__ void __launch_bounds__(kThreads) RenderGpuRecordsKernel(const iscu_gpu_splat_emitter* __restrict__ ems,
                                                                      const iscu_frame* __restrict__ frames,
                                                                      Kernels K, StaticView st,
@@ -241,7 +47,6 @@ __global__ void __launch_bounds__(kThreads) RenderGpuRecordsKernel(const iscu_gp
    const bool inside = X < W && Y < H;
    const uint32_t i = static_cast<uint32_t>(Y) * st.width + static_cast<uint32_t>(X);
    const size_t o = static_cast<size_t>(blockIdx.z) * st.width * st.height + i;
-   // The frame's other light first (SplatGpuHost::RenderFrames: the blinks are splatted onto the extra image).
    float acc = inside ? Background(st, i, fr.bg_scale) : 0.0f;
    if (inside && extras)
       acc += extras[o];
@@ -390,10 +195,7 @@ __global__ void BlockSumsKernel(const float* __restrict__ planes, int n, int os,
    sums[(static_cast<size_t>(z) * bw + ai) * bw + bi] = static_cast<float>(acc);
 }
 
-} // namespace
-
-// ------------------------------------------------------------------------------------------------ launchers
-static Kernels KernelsOf(iscu_ctx* ctx)
+Kernels KernelsOfCtx(iscu_ctx* ctx)
 {
    Kernels K;
    for (int s = 0; s < ISCU_MAX_KERNELS; ++s)
@@ -401,23 +203,9 @@ static Kernels KernelsOf(iscu_ctx* ctx)
    return K;
 }
 
-int LaunchRenderFrames(iscu_ctx* ctx, const iscu_emitter* ems, const iscu_frame* frames, uint32_t nFrames,
-                       const CameraView* cam, uint32_t seed, float* photons, uint16_t* adu)
-{
-   if (nFrames == 0)
-      return ISCU_OK;
-   const StaticView st = ctx->Static();
-   const dim3 grid((st.width + kTileX - 1) / kTileX, (st.height + kTileY - 1) / kTileY, nFrames);
-   const Kernels K = KernelsOf(ctx);
-   if (cam)
-      RenderFramesKernel<true><<<grid, kThreads, 0, ctx->stream>>>(ems, frames, K, st, *cam, seed, photons, adu);
-   else
-      RenderFramesKernel<false><<<grid, kThreads, 0, ctx->stream>>>(ems, frames, K, st, CameraView(), seed, photons,
-                                                                    nullptr);
-   ISCU_CK_LAUNCH(ctx, "RenderFramesKernel");
-   return ISCU_OK;
-}
+} // namespace
 
+// ------------------------------------------------------------------------------------------------ launchers
 int LaunchRenderGpuRecords(iscu_ctx* ctx, const iscu_gpu_splat_emitter* ems, const iscu_frame* frames,
                            uint32_t nFrames, const float* extras, const CameraView* cam, uint32_t seed, uint16_t* adu)
 {
@@ -425,7 +213,7 @@ int LaunchRenderGpuRecords(iscu_ctx* ctx, const iscu_gpu_splat_emitter* ems, con
       return ISCU_OK;
    const StaticView st = ctx->Static();
    const dim3 grid((st.width + kTileX - 1) / kTileX, (st.height + kTileY - 1) / kTileY, nFrames);
-   RenderGpuRecordsKernel<<<grid, kThreads, 0, ctx->stream>>>(ems, frames, KernelsOf(ctx), st, extras, *cam, seed,
+   RenderGpuRecordsKernel<<<grid, kThreads, 0, ctx->stream>>>(ems, frames, KernelsOfCtx(ctx), st, extras, *cam, seed,
                                                               adu);
    ISCU_CK_LAUNCH(ctx, "RenderGpuRecordsKernel");
    return ISCU_OK;

@@ -23,7 +23,8 @@ GPU_SPLAT_EMITTER_DTYPE = np.dtype([("x0", "<i4"), ("y0", "<i4"), ("bx", "<i4"),
                                     ("n_taps", "<i4"), ("photons", "<f4"), ("cut_radius2", "<i4"),
                                     ("wx", "<f4", (4,)), ("wy", "<f4", (4,))])
 BLINK_EVENT_DTYPE = np.dtype([("x_um", "<f8"), ("y_um", "<f8"), ("z_nm", "<f8"), ("t_start", "<f8"),
-                              ("t_end", "<f8"), ("brightness", "<f8"), ("excite", "<f8"), ("reserved", "<f8")])
+                              ("t_end", "<f8"), ("brightness", "<f8"), ("excite", "<f8"), ("slot", "<i4"),
+                              ("reserved", "<i4")])
 assert EMITTER_DTYPE.itemsize == C.sizeof(_abi.Emitter) == 32
 assert FRAME_DTYPE.itemsize == C.sizeof(_abi.Frame) == 24
 assert GPU_SPLAT_EMITTER_DTYPE.itemsize == C.sizeof(_abi.GpuSplatEmitter) == 64
@@ -312,6 +313,27 @@ class Engine:
                                               _ptr(adu_dev)))
         self._after(sync)
 
+    RENDER_CONFIGS = 6
+
+    def render_config(self):
+        """(config, tile_w, tile_h, persistent) of the render kernel form in use."""
+        v = [C.c_int32() for _ in range(4)]
+        check(self.lib.iscu_render_get_config(self.h, *[C.byref(x) for x in v]))
+        return v[0].value, v[1].value, v[2].value, bool(v[3].value)
+
+    def set_render_config(self, config):
+        check(self.lib.iscu_render_set_config(self.h, int(config)))
+
+    def render_autotune(self, emitters_dev, frames_dev, n_frames, camera: CameraParams, seed, adu_dev):
+        """Times the render forms on this device batch, keeps the fastest; returns ms per render of each form."""
+        ms = (C.c_float * self.RENDER_CONFIGS)()
+        cam = camera.c()
+        self._before(True)
+        check(self.lib.iscu_render_autotune(self.h, _ptr(emitters_dev), _ptr(frames_dev), n_frames, C.byref(cam),
+                                            seed, _ptr(adu_dev), ms))
+        self._after(True)
+        return list(ms)
+
     def render_gpu_records(self, records, frames, camera: CameraParams, seed, extras=None):
         """GpuSimulator::RenderFrames over the reference's 64-byte records (GPU_SPLAT_EMITTER_DTYPE)."""
         records = np.ascontiguousarray(records, dtype=GPU_SPLAT_EMITTER_DTYPE)
@@ -360,6 +382,42 @@ class Engine:
                                              _ptr(sc), _ptr(il), min_photons, _ptr(out), len(out), _ptr(frames_out),
                                              C.byref(n), C.byref(clamped)))
         return out[: n.value], frames_out, clamped.value
+
+
+class RenderGraph:
+    """iscu_render_graph: one device batch's render captured into a CUDA graph; launch() replays it on the engine's
+    stream (refill the same device buffers in place between launches)."""
+
+    def __init__(self, engine: Engine, emitters_dev, frames_dev, n_frames, camera: CameraParams | None, seed,
+                 photons_dev=None, adu_dev=None):
+        self.engine = engine
+        self.lib = engine.lib
+        self._keep = (emitters_dev, frames_dev, photons_dev, adu_dev)
+        cam = camera.c() if camera is not None else None
+        h = C.c_void_p()
+        engine._before(True)
+        check(self.lib.iscu_render_graph_create(engine.h, _ptr(emitters_dev), _ptr(frames_dev), n_frames,
+                                                C.byref(cam) if cam is not None else None, seed, _ptr(photons_dev),
+                                                _ptr(adu_dev), C.byref(h)))
+        self.h = h
+        engine._plans.add(self)
+
+    def launch(self, sync=True):
+        self.engine._before(sync)
+        check(self.lib.iscu_render_graph_launch(self.h))
+        self.engine._after(sync)
+
+    def close(self):
+        if self.h:
+            if self.engine.h:
+                self.lib.iscu_render_graph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class PsfPlan:

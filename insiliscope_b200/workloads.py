@@ -115,6 +115,52 @@ def smlm_dstorm(seed: int = 42, sites: int = 4000, frames: int = 200, size: int 
 
 
 @dataclass
+class TwoColourMovie(SmlmMovie):
+    """A blink movie of several dye groups: an event's `slot` is its group, each group with its own PSF kernel;
+    within a frame's bucket the groups come one after the other, as the engine renders them."""
+    psfs: list = None           # PsfParams per group (psf is psfs[0])
+    frame_mean: np.ndarray = None   # each frame's Poisson mean
+
+
+def two_colour_uneven(seed: int = 42, frames: int = 1024, size: int = 256, pixel_nm: float = 108.0,
+                      median_mean: float = 300.0, sigma_log_mean: float = 1.0, mean_clip=(10.0, 8000.0),
+                      median_photons: float = 2000.0, sigma_log: float = 0.5, z_half_nm: float = 600.0,
+                      frame0: int = 0) -> TwoColourMovie:
+    """The uneven two-colour movie: 256 x 256 px sCMOS at 108 nm, 1,024 frames. Frame f carries Poisson(mu_f) ON
+    emitters, mu_f lognormal (median 300, sigma_log 1) clipped to [10, 8000]; each emitter uniform over the field,
+    z uniform in [-600, 600] nm, in channel 0 or 1 with probability 1/2, photons lognormal (median 2000, sigma_log
+    0.5). Channel 0: 670 nm with the double-helix phase mask; channel 1: 580 nm astigmatic (Noll 5 = 0.1 lambda rms).
+    Both NA 1.45 oil, 64 x 64 pupil, 4x-oversampled 32 x 32 px kernels of 49 planes 25 nm apart, Catmull-Rom; the
+    camera as the plain dSTORM movie's. Counts and properties come from numpy's PCG64 seeded with `seed`."""
+    rng = np.random.default_rng(seed)
+    mu = np.clip(median_mean * np.exp(sigma_log_mean * rng.standard_normal(frames)), *mean_clip)
+    counts = rng.poisson(mu)
+    n = int(counts.sum())
+    fi = np.repeat(np.arange(frames), counts)
+    ch = (rng.random(n) < 0.5).astype(np.int32)
+    order = np.lexsort((ch, fi))            # frame-major, channel 0 before channel 1, draw order within
+    ev = np.zeros(n, BLINK_EVENT_DTYPE)
+    ev["x_um"] = size * rng.random(n) * (pixel_nm / 1000.0)
+    ev["y_um"] = size * rng.random(n) * (pixel_nm / 1000.0)
+    ev["z_nm"] = -z_half_nm + 2.0 * z_half_nm * rng.random(n)
+    ev["brightness"] = np.exp(sigma_log * rng.standard_normal(n))
+    ev["t_start"] = (frame0 + fi).astype(np.float64)
+    ev["t_end"] = ev["t_start"] + 1.0
+    ev["excite"] = 1.0
+    ev["slot"] = ch
+    ev = ev[order]
+    bucket = np.concatenate([[0], np.cumsum(counts)]).astype(np.uint32)
+    common = dict(na=1.45, immersion_index=1.518, sample_index=1.518, working_distance_um=150.0, sample_depth_nm=0.0,
+                  pixel_size_nm=pixel_nm, oversampling=4, kernel_half_width_px=16, nz=49, z_step_nm=25.0,
+                  pupil_samples=64, interp=INTERP_CUBIC)
+    dh = PsfParams(wavelength_nm=670.0, double_helix=True, **common)
+    astig = PsfParams(wavelength_nm=580.0, zernike=noll_rms_to_osa_waves({5: 0.1}), **common)
+    cam = CameraParams(quantum_efficiency=1.0, dark_electrons=0.0, gain=2.2, read_noise_e=1.5, emccd=False)
+    return TwoColourMovie(size, size, frames, pixel_nm, median_photons, 20.0, ev, bucket, dh, cam, seed, 100.0, 2.0,
+                          2.2, 0.1 / 2.2, 1.5, 0.2, (seed ^ 0x9E3779B9) & 0xFFFFFFFF, [dh, astig], mu)
+
+
+@dataclass
 class WidefieldVolume:
     """A dye volume and what renders its focus series."""
     density: np.ndarray         # (nz, ny, nx) float32, photons per voxel per frame at focus

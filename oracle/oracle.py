@@ -189,12 +189,15 @@ class Reference:
         L.ref_kernel_spans.argtypes = [vp, vp, vp, vp]
         L.ref_nearest_z.argtypes = [vp, f64]
         L.ref_render_photon_image.argtypes = [vp, vp, u32, i64, u32, u32, f64, f64, f64, f64, f64, f64, vp, vp, f64,
-                                              f64, C.c_int, vp]
+                                              f64, C.c_int, C.c_int, vp]
         L.ref_collect_gpu_emitters.argtypes = [vp, vp, u32, i64, u32, u32, f64, f64, f64, f64, f64, C.c_int, f64, vp,
                                                u32]
         L.ref_collect_gpu_emitters.restype = u32
         L.ref_render_movie.argtypes = [vp, vp, u32, u32, u32, u32, u32, f64, f64, f64, vp, vp, vp, vp, u32, vp, vp]
         L.ref_render_movie.restype = f64
+        L.ref_render_movie_groups.argtypes = [vp, C.c_int, vp, u32, u32, u32, u32, u32, f64, f64, f64, vp, vp, vp, vp,
+                                              u32, vp, vp]
+        L.ref_render_movie_groups.restype = f64
         self.L = L
 
     def set_threads(self, n):
@@ -246,6 +249,22 @@ class Reference:
         if self.L.ref_zernike_planes(C.byref(r), _p(out)) != 0:
             raise RuntimeError(self.L.ref_last_error().decode())
         return out
+
+    def render_movie_groups(self, kernels, events, frame0, n_frames, w, h, pixel_nm, per_blink, bg, camera, offset,
+                            gain, read_noise, seed, want_photons=False, want_adu=True):
+        """The reference's multi-colour frame loop: dye group g = the events whose slot is g, splatted with kernels[g]
+        onto the frame in group order (the later groups accumulating), then the noise chain; frames in parallel on
+        its pool. Returns (seconds, photons, adu)."""
+        events = np.ascontiguousarray(events)
+        ph = np.zeros((n_frames, h, w), np.float32) if want_photons else None
+        adu = np.zeros((n_frames, h, w), np.uint16) if want_adu else None
+        cam = camera.c()
+        hs = (C.c_void_p * len(kernels))(*[k.h for k in kernels])
+        f = lambda a: None if a is None else np.ascontiguousarray(a, np.float32)
+        t = self.L.ref_render_movie_groups(hs, len(kernels), _p(events), len(events), frame0, n_frames, w, h, pixel_nm,
+                                           per_blink, bg, C.byref(cam), _p(f(offset)), _p(f(gain)),
+                                           _p(f(read_noise)), seed, _p(ph), _p(adu))
+        return t, ph, adu
 
     def kernel(self, req=None, planes=None, os_=4, z_step_nm=25.0, interp=2):
         return RefKernel(self, req, planes, os_, z_step_nm, interp)
@@ -312,13 +331,15 @@ class RefKernel:
         return self.ref.L.ref_nearest_z(self.h, z_um)
 
     def render_photon_image(self, events, frame, w, h, pixel_nm, per_blink, bg, drift_x=0.0, drift_y=0.0,
-                            global_z=0.0, illum=None, bg_map=None, bg_scale=1.0, min_photons=0.0, parallel=False):
+                            global_z=0.0, illum=None, bg_map=None, bg_scale=1.0, min_photons=0.0, parallel=False,
+                            onto=None):
+        """RenderPhotonImage; onto: an earlier dye group's image to splat onto (RenderExtras::accumulate)."""
         events = np.ascontiguousarray(events)
-        out = np.zeros((h, w), np.float32)
+        out = np.zeros((h, w), np.float32) if onto is None else np.array(onto, np.float32, copy=True)
         f = lambda a: None if a is None else np.ascontiguousarray(a, np.float32)
         self.ref.L.ref_render_photon_image(self.h, _p(events), len(events), frame, w, h, pixel_nm, per_blink, bg,
                                            drift_x, drift_y, global_z, _p(f(illum)), _p(f(bg_map)), bg_scale,
-                                           min_photons, int(parallel), _p(out))
+                                           min_photons, int(parallel), int(onto is not None), _p(out))
         return out
 
     def collect_gpu_emitters(self, events, frame, w, h, pixel_nm, per_blink, drift_x=0.0, drift_y=0.0, global_z=0.0,

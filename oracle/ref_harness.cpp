@@ -327,7 +327,7 @@ int ref_nearest_z(void* h, double zUm)
 void ref_render_photon_image(void* h, const iscu_blink_event* ev, uint32_t nEv, int64_t frame, uint32_t w, uint32_t hgt,
                              double pixelNm, double photonsPerBlink, double bg, double driftX, double driftY,
                              double globalZ, const float* illum, const float* bgMap, double bgScale,
-                             double minPhotons, int parallel, float* out)
+                             double minPhotons, int parallel, int accumulate, float* out)
 {
    const auto* c = static_cast<sim::PsfKernelCache*>(h);
    const std::vector<sim::BlinkEvent> events = ToEvents(ev, nEv);
@@ -347,7 +347,10 @@ void ref_render_photon_image(void* h, const iscu_blink_event* ev, uint32_t nEv, 
    ex.backgroundScale = bgScale;
    ex.minPhotons = minPhotons;
    ex.parallel = parallel != 0;
+   ex.accumulate = accumulate != 0;
    std::vector<float> img;
+   if (accumulate)
+      img.assign(out, out + n);   // a later dye group splats onto the earlier groups' image
    sim::RenderPhotonImage(img, w, hgt, events, frame, pixelNm, 1.3, photonsPerBlink, bg, driftX, driftY, c, globalZ,
                           nullptr, nullptr, &ex);
    std::memcpy(out, img.data(), n * sizeof(float));
@@ -401,6 +404,62 @@ double ref_render_movie(void* h, const iscu_blink_event* ev, uint32_t nEv, uint3
       std::vector<float> img;
       sim::RenderPhotonImage(img, w, hgt, fe, static_cast<long>(frame0 + k), pixelNm, 1.3, photonsPerBlink, bg, 0.0,
                              0.0, c, 0.0);
+      std::vector<uint16_t> adu;
+      sim::ApplyNoiseChain(img, adu, w, hgt, cp, m.off, m.gain, m.rn, seed, frame0 + k, false, 0);
+      if (outPhotons)
+         std::memcpy(outPhotons + k * n, img.data(), n * sizeof(float));
+      if (outAdu)
+         std::memcpy(outAdu + k * n, adu.data(), n * sizeof(uint16_t));
+   });
+   return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// The multi-colour frame loop: each dye group (events whose slot is g, rendered with caches[g]) splatted in group
+// order onto one image per frame -- the first group over the background, the later ones with
+// RenderExtras::accumulate, as the movie engine renders its dye groups (ScopeMovie.cpp:7059-7110) -- then the noise
+// chain. Frames in parallel on the reference's pool. Returns seconds.
+double ref_render_movie_groups(void* const* caches, int nGroups, const iscu_blink_event* ev, uint32_t nEv,
+                               uint32_t frame0, uint32_t nFrames, uint32_t w, uint32_t hgt, double pixelNm,
+                               double photonsPerBlink, double bg, const iscu_camera* cam, const float* off,
+                               const float* gain, const float* rn, uint32_t seed, float* outPhotons, uint16_t* outAdu)
+{
+   std::vector<std::vector<sim::BlinkEvent>> groupEvents(nGroups);
+   for (uint32_t i = 0; i < nEv; ++i)
+      if (ev[i].slot >= 0 && ev[i].slot < nGroups)
+      {
+         const std::vector<sim::BlinkEvent> one = ToEvents(ev + i, 1);
+         groupEvents[ev[i].slot].push_back(one[0]);
+      }
+   Maps m;
+   FillMaps(m, w, hgt, off, gain, rn);
+   const sim::CameraNoiseParams cp = ToCamera(*cam);
+   const size_t n = static_cast<size_t>(w) * hgt;
+   const auto t0 = std::chrono::steady_clock::now();
+   std::vector<std::vector<std::vector<uint32_t>>> buckets(nGroups);
+   for (int g = 0; g < nGroups; ++g)
+   {
+      std::vector<sim::BlinkEvent> shifted = groupEvents[g];
+      for (auto& e : shifted)
+      {
+         e.tStart -= frame0;
+         e.tEnd -= frame0;
+      }
+      buckets[g] = sim::BucketEventsByFrame(shifted, nFrames);
+   }
+   sim::ParallelFor(nFrames, [&](unsigned k) {
+      std::vector<float> img;
+      for (int g = 0; g < nGroups; ++g)
+      {
+         std::vector<sim::BlinkEvent> fe;
+         fe.reserve(buckets[g][k].size());
+         for (uint32_t i : buckets[g][k])
+            fe.push_back(groupEvents[g][i]);
+         sim::RenderExtras ex;
+         ex.accumulate = g > 0;
+         sim::RenderPhotonImage(img, w, hgt, fe, static_cast<long>(frame0 + k), pixelNm, 1.3, photonsPerBlink, bg,
+                                0.0, 0.0, static_cast<const sim::PsfKernelCache*>(caches[g]), 0.0, nullptr, nullptr,
+                                &ex);
+      }
       std::vector<uint16_t> adu;
       sim::ApplyNoiseChain(img, adu, w, hgt, cp, m.off, m.gain, m.rn, seed, frame0 + k, false, 0);
       if (outPhotons)
