@@ -303,6 +303,7 @@ class TwoColourWorkload(SmlmWorkload):
     def config_extra(self):
         tw, th = self.form[1], self.form[2]
         return {"render_form": {"config": self.form[0], "tile": f"{tw}x{th}", "persistent": self.form[3],
+                                "emitters_per_step": 2 if self.form[4] else 1,
                                 "autotune_ms_per_form": [round(x, 4) for x in self.autotune_ms]},
                 "cuda_graph": True, "mean_emitters_per_frame": self.n_emitters / self.mv.frames,
                 "max_emitters_per_frame": int(self.frames["em_count"].max())}

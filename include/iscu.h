@@ -246,35 +246,47 @@ typedef struct iscu_frame {
    double bg_scale;
 } iscu_frame;
 
-/* Frames k < n_frames: the background, then every emitter of the frame splatted in list order
+/* Frames k < n_frames: the background, then every emitter of the frame splatted in list order (emitters_dev holds
+ * n_emitters records; a frame's run is cut at n_emitters)
  * (RenderPhotonImage, SMLMSimulation.cpp:103-160: the same float additions in the same order), then, unless
  * cam is NULL, the noise chain (ApplyNoiseChain). photons_dev (nullable) receives the noise-free images,
  * adu_dev (nullable) the frames; both n_frames*w*h. Needs iscu_set_static and the kernels the emitters name. */
-int iscu_render_frames_dev(iscu_ctx* ctx, const iscu_emitter* emitters_dev, const iscu_frame* frames_dev,
-                           uint32_t n_frames, const iscu_camera* cam, uint32_t seed, float* photons_dev,
-                           uint16_t* adu_dev);
+int iscu_render_frames_dev(iscu_ctx* ctx, const iscu_emitter* emitters_dev, uint32_t n_emitters,
+                           const iscu_frame* frames_dev, uint32_t n_frames, const iscu_camera* cam, uint32_t seed,
+                           float* photons_dev, uint16_t* adu_dev);
 /* The same with host arrays (emitters: sum of em_count records; frames: n_frames; outputs host, nullable): the
  * copies in and out are part of the call. */
 int iscu_render_frames(iscu_ctx* ctx, const iscu_emitter* emitters, uint32_t n_emitters, const iscu_frame* frames,
                        uint32_t n_frames, const iscu_camera* cam, uint32_t seed, float* photons, uint16_t* adu);
 
 /* The render kernel's form (no reference counterpart: the reference renders a frame per CPU task, ParallelFor over
- * frames, ScopeMovie.cpp:7059-7110). config 0..2: one CTA per (frame, tile) with tiles 16x16, 32x8, 8x32; 3..5: the
- * same tiles in a persistent grid that takes (frame, tile) items heaviest frame first, for batches whose frames carry
- * very different emitter counts. Every form gives the same bits. */
+ * frames, ScopeMovie.cpp:7059-7110). config % 3: the CTA's tile, 16x16, 32x8 or 8x32 pixels; (config / 3) % 2: one
+ * CTA per (frame, tile), or a persistent grid that takes (frame, tile) items heaviest frame first (for batches whose
+ * frames carry very different emitter counts). Configs 0..11 render in one pass, config / 6 emitters per step of a
+ * pixel's loop (*paired 0 or 1); configs 12..17 in two passes (*paired 2): every emitter's float contribution to
+ * each pixel of its square first, computed by groups of emitters that read the same block sums (kernel slot, plane,
+ * tap origin), then the tiles add them in emitter order. The two-pass forms keep up to a quarter of the device's
+ * memory for contributions (n_emitters x square pixels floats); a batch beyond that renders in the one-pass form of
+ * the same tile and scheduling. Every form gives the same bits. */
+#define ISCU_RENDER_CONFIGS 18
 int iscu_render_set_config(iscu_ctx* ctx, int32_t config);
-int iscu_render_get_config(iscu_ctx* ctx, int32_t* config, int32_t* tile_w, int32_t* tile_h, int32_t* persistent);
-/* Times the six forms on the given device batch (one warm-up and two timed renders each, adu_dev overwritten),
- * keeps the fastest as the context's form; ms6 (nullable) receives each form's milliseconds per render. */
-int iscu_render_autotune(iscu_ctx* ctx, const iscu_emitter* emitters_dev, const iscu_frame* frames_dev,
-                         uint32_t n_frames, const iscu_camera* cam, uint32_t seed, uint16_t* adu_dev, float* ms6);
+/* The most device bytes the two-pass forms' contributions may take (0: a quarter of the device's memory). */
+int iscu_render_set_contrib_limit(iscu_ctx* ctx, uint64_t bytes);
+int iscu_render_get_config(iscu_ctx* ctx, int32_t* config, int32_t* tile_w, int32_t* tile_h, int32_t* persistent,
+                           int32_t* paired);
+/* Times the ISCU_RENDER_CONFIGS forms on the given device batch (one warm-up and two timed renders each, adu_dev
+ * overwritten), keeps the fastest as the context's form; ms (nullable, ISCU_RENDER_CONFIGS floats) receives each
+ * form's milliseconds per render. */
+int iscu_render_autotune(iscu_ctx* ctx, const iscu_emitter* emitters_dev, uint32_t n_emitters,
+                         const iscu_frame* frames_dev, uint32_t n_frames, const iscu_camera* cam, uint32_t seed,
+                         uint16_t* adu_dev, float* ms);
 /* iscu_render_frames_dev with the context's current form captured once into a CUDA graph on the context's stream;
  * each launch replays it (the same device pointers, so refill them in place between launches). Kernel slots and
  * camera statics must not be rebuilt while the graph lives. */
 typedef struct iscu_render_graph iscu_render_graph;
-int iscu_render_graph_create(iscu_ctx* ctx, const iscu_emitter* emitters_dev, const iscu_frame* frames_dev,
-                             uint32_t n_frames, const iscu_camera* cam, uint32_t seed, float* photons_dev,
-                             uint16_t* adu_dev, iscu_render_graph** out);
+int iscu_render_graph_create(iscu_ctx* ctx, const iscu_emitter* emitters_dev, uint32_t n_emitters,
+                             const iscu_frame* frames_dev, uint32_t n_frames, const iscu_camera* cam, uint32_t seed,
+                             float* photons_dev, uint16_t* adu_dev, iscu_render_graph** out);
 int iscu_render_graph_launch(iscu_render_graph* graph);
 void iscu_render_graph_destroy(iscu_render_graph* graph);
 

@@ -125,13 +125,16 @@ SIGNATURES = {
     "iscu_kernel_info": (C.c_int, [vp, C.c_int32, i32p, i32p, i32p, i32p]),
     "iscu_kernel_get_planes": (C.c_int, [vp, C.c_int32, vp]),
     "iscu_kernel_get_block_sums": (C.c_int, [vp, C.c_int32, vp]),
-    "iscu_render_frames_dev": (C.c_int, [vp, vp, vp, C.c_uint32, C.POINTER(Camera), C.c_uint32, vp, vp]),
+    "iscu_render_frames_dev": (C.c_int, [vp, vp, C.c_uint32, vp, C.c_uint32, C.POINTER(Camera), C.c_uint32, vp,
+                                         vp]),
     "iscu_render_frames": (C.c_int, [vp, vp, C.c_uint32, vp, C.c_uint32, C.POINTER(Camera), C.c_uint32, vp, vp]),
     "iscu_render_set_config": (C.c_int, [vp, C.c_int32]),
-    "iscu_render_get_config": (C.c_int, [vp, i32p, i32p, i32p, i32p]),
-    "iscu_render_autotune": (C.c_int, [vp, vp, vp, C.c_uint32, C.POINTER(Camera), C.c_uint32, vp, f32p]),
-    "iscu_render_graph_create": (C.c_int, [vp, vp, vp, C.c_uint32, C.POINTER(Camera), C.c_uint32, vp, vp,
-                                           C.POINTER(vp)]),
+    "iscu_render_set_contrib_limit": (C.c_int, [vp, C.c_uint64]),
+    "iscu_render_get_config": (C.c_int, [vp, i32p, i32p, i32p, i32p, i32p]),
+    "iscu_render_autotune": (C.c_int, [vp, vp, C.c_uint32, vp, C.c_uint32, C.POINTER(Camera), C.c_uint32, vp,
+                                       f32p]),
+    "iscu_render_graph_create": (C.c_int, [vp, vp, C.c_uint32, vp, C.c_uint32, C.POINTER(Camera), C.c_uint32, vp,
+                                           vp, C.POINTER(vp)]),
     "iscu_render_graph_launch": (C.c_int, [vp]),
     "iscu_render_graph_destroy": (None, [vp]),
     "iscu_render_gpu_records": (C.c_int, [vp, vp, C.c_uint32, vp, C.c_uint32, vp, C.POINTER(Camera), C.c_uint32,

@@ -25,6 +25,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 UNITS = {
     "splat_noise.cu": ["--fmad=false"],
     "render.cu": ["--fmad=false"],
+    "render_contrib.cu": ["--fmad=false"],
     "psf.cu": [],
     "psf_tc.cu": [],
     "psf_noalloc.cu": [],

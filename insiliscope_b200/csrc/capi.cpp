@@ -412,9 +412,13 @@ static int FinishKernelSlot(iscu_ctx* ctx, KernelSlot& k)
    ISCU_CK(k.sums.Reserve(static_cast<size_t>(k.nz) * k.bw * k.bw * sizeof(float)));
    const size_t nSums = static_cast<size_t>(k.nz) * k.bw * k.bw;
    ISCU_CK(k.sums64.Reserve(nSums * sizeof(double)));
+   PhaseGeometry(k.bw, k.os, k.padLo, k.nb);
+   ISCU_CK(k.phase.Reserve(static_cast<size_t>(k.nz) * k.os * k.os * k.nb * k.nb * sizeof(double)));
    int rc = LaunchBlockSums(ctx, k.planes.as<float>(), k.size, k.os, k.nz, k.sums.as<float>());
    if (rc == ISCU_OK)
       rc = LaunchSumsToDouble(ctx, k.sums.as<float>(), nSums, k.sums64.as<double>());
+   if (rc == ISCU_OK)
+      rc = LaunchPhaseSplit(ctx, k.sums.as<float>(), k.nz, k.bw, k.os, k.padLo, k.nb, k.phase.as<double>());
    if (rc != ISCU_OK)
       return rc;
    ISCU_CK(cudaStreamSynchronize(ctx->stream));
@@ -542,11 +546,11 @@ int iscu_kernel_get_block_sums(iscu_ctx* ctx, int32_t slot, float* out)
 }
 
 // ------------------------------------------------------------------------------------------ splat + noise
-int iscu_render_frames_dev(iscu_ctx* ctx, const iscu_emitter* emitters_dev, const iscu_frame* frames_dev,
-                           uint32_t n_frames, const iscu_camera* cam, uint32_t seed, float* photons_dev,
-                           uint16_t* adu_dev)
+int iscu_render_frames_dev(iscu_ctx* ctx, const iscu_emitter* emitters_dev, uint32_t n_emitters,
+                           const iscu_frame* frames_dev, uint32_t n_frames, const iscu_camera* cam, uint32_t seed,
+                           float* photons_dev, uint16_t* adu_dev)
 {
-   if (!ctx || (n_frames && !frames_dev))
+   if (!ctx || (n_frames && !frames_dev) || (n_emitters && !emitters_dev))
       return Fail(ISCU_ERR_ARG, "null argument");
    if (cam && !adu_dev)
       return Fail(ISCU_ERR_ARG, "a camera needs an ADU output");
@@ -558,8 +562,8 @@ int iscu_render_frames_dev(iscu_ctx* ctx, const iscu_emitter* emitters_dev, cons
    CameraView cv;
    if (cam)
       cv = MakeCameraView(*cam);
-   return LaunchRenderFrames(ctx, emitters_dev, frames_dev, n_frames, cam ? &cv : nullptr, seed, photons_dev,
-                             adu_dev);
+   return LaunchRenderFrames(ctx, emitters_dev, n_emitters, frames_dev, n_frames, cam ? &cv : nullptr, seed,
+                             photons_dev, adu_dev);
 }
 
 int iscu_render_frames(iscu_ctx* ctx, const iscu_emitter* emitters, uint32_t n_emitters, const iscu_frame* frames,
@@ -590,8 +594,8 @@ int iscu_render_frames(iscu_ctx* ctx, const iscu_emitter* emitters, uint32_t n_e
    CameraView cv;
    if (cam)
       cv = MakeCameraView(*cam);
-   int rc = LaunchRenderFrames(ctx, ctx->dEmitters.as<iscu_emitter>(), ctx->dFrames.as<iscu_frame>(), n_frames,
-                               cam ? &cv : nullptr, seed, photons ? ctx->dPhotons.as<float>() : nullptr,
+   int rc = LaunchRenderFrames(ctx, ctx->dEmitters.as<iscu_emitter>(), n_emitters, ctx->dFrames.as<iscu_frame>(),
+                               n_frames, cam ? &cv : nullptr, seed, photons ? ctx->dPhotons.as<float>() : nullptr,
                                adu ? ctx->dAdu.as<uint16_t>() : nullptr);
    if (rc != ISCU_OK)
       return rc;

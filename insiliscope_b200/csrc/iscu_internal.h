@@ -103,7 +103,12 @@ struct PinnedBuf
 struct KernelView
 {
    const float* sums = nullptr;     // nz planes of bw x bw block sums, row-major
-   const double* sums64 = nullptr;  // the same values widened to float64 (what the render kernels read)
+   const double* sums64 = nullptr;  // the same values widened to float64 (the render's general path)
+   // The float64 block sums split by oversampling phase, zero-padded: phase[z][qy][qx][ky][kx] =
+   // sums[z][ky os + qy - padLo][kx os + qx - padLo] (0 outside the bw x bw array). A cubic splat's tap (j, i) of
+   // neighbouring camera pixels then sits in neighbouring words of one phase plane.
+   const double* phase = nullptr;
+   int nb = 0, padLo = 0;
    const int16_t* spanLo = nullptr; // halo cut: [z * (2 camRad + 1) + dy + camRad]; nullptr: the whole square
    const int16_t* spanHi = nullptr;
    const int32_t* radius2 = nullptr;
@@ -119,6 +124,8 @@ struct KernelSlot
    DevBuf planes;    // nz * size * size
    DevBuf sums;      // nz * bw * bw
    DevBuf sums64;    // nz * bw * bw float64 copies of sums
+   DevBuf phase;     // nz * os * os * nb * nb float64, the phase-split padded sums
+   int nb = 0, padLo = 0;
    DevBuf spanLo, spanHi, radius2;
    bool halo = false;
    double haloThreshold = 0.0;
@@ -128,6 +135,9 @@ struct KernelSlot
       KernelView v;
       v.sums = sums.as<float>();
       v.sums64 = sums64.as<double>();
+      v.phase = phase.as<double>();
+      v.nb = nb;
+      v.padLo = padLo;
       v.spanLo = halo ? spanLo.as<int16_t>() : nullptr;
       v.spanHi = halo ? spanHi.as<int16_t>() : nullptr;
       v.radius2 = halo ? radius2.as<int32_t>() : nullptr;
@@ -164,6 +174,13 @@ struct StaticView
    uint32_t width = 0, height = 0, pixelBase = 0;
 };
 
+// Device scratch of the two-pass render (render_contrib.cu): per-emitter setup records, the (slot, plane, tap
+// origin) groups, and every emitter's float contribution to each pixel of its square.
+struct ContribScratch
+{
+   DevBuf rec, grec, keys, list, contrib, ctr;
+};
+
 } // namespace iscu
 
 // ------------------------------------------------------------------ the context
@@ -176,6 +193,8 @@ struct iscu_ctx
    int smCount = 0;
    int renderConfig = 0;           // render kernel form (iscu_render_set_config)
    iscu::DevBuf dOrder;            // persistent render: frame order + work counter
+   iscu::ContribScratch contrib;   // two-pass render scratch
+   size_t contribLimit = 0;        // most bytes the two-pass render's contributions may take (0: a quarter of HBM)
    iscu::KernelSlot kernels[ISCU_MAX_KERNELS];
    // camera statics
    bool haveStatic = false;
@@ -211,13 +230,33 @@ int LaunchCounterUniforms(iscu_ctx* ctx, uint32_t seed, uint32_t frame, uint32_t
                           uint32_t perPixel, double* out);
 int LaunchNoiseFrames(iscu_ctx* ctx, const float* photons, uint32_t nFrames, const uint32_t* frames,
                       const CameraView& cam, uint32_t seed, uint16_t* adu);
-int LaunchRenderFrames(iscu_ctx* ctx, const iscu_emitter* ems, const iscu_frame* frames, uint32_t nFrames,
-                       const CameraView* cam, uint32_t seed, float* photons, uint16_t* adu);
+// Emitter runs of the frames beyond nEmitters are cut at nEmitters.
+int LaunchRenderFrames(iscu_ctx* ctx, const iscu_emitter* ems, uint32_t nEmitters, const iscu_frame* frames,
+                       uint32_t nFrames, const CameraView* cam, uint32_t seed, float* photons, uint16_t* adu);
+// The persistent render's scratch: frames heaviest first, then the work counter (zeroed).
+size_t OrderBytes(uint32_t nFrames);
+int LaunchFrameOrder(iscu_ctx* ctx, const iscu_frame* frames, uint32_t nFrames, uint32_t* orderBuf);
+// Grows the two-pass render's scratch for nEm emitters (no launches; what a graph capture needs done before).
+// ISCU_ERR_LIMIT when the contributions would pass the context's limit.
+int ReserveContrib(iscu_ctx* ctx, uint32_t nEm, ContribScratch& sc);
+// The two-pass render (tile config 0..5 of its gather pass). ISCU_ERR_LIMIT when its contributions would pass the
+// context's limit; nothing is launched then.
+int LaunchContribRender(iscu_ctx* ctx, int tileConfig, const iscu_emitter* ems, uint32_t nEmitters,
+                        const iscu_frame* frames, uint32_t nFrames, const CameraView* cam, uint32_t seed,
+                        float* photons, uint16_t* adu, uint32_t* orderBuf, ContribScratch& scratch);
 int LaunchRenderGpuRecords(iscu_ctx* ctx, const iscu_gpu_splat_emitter* ems, const iscu_frame* frames,
                            uint32_t nFrames, const float* extras, const CameraView* cam, uint32_t seed,
                            uint16_t* adu);
 int LaunchBlockSums(iscu_ctx* ctx, const float* planes, int n, int os, int nz, float* sums);
 int LaunchSumsToDouble(iscu_ctx* ctx, const float* in, size_t n, double* out);
+// The phase-split layout's geometry for a bw x bw block-sum plane at oversampling os: a low margin padLo >= 4 (a
+// multiple of os) and nb words per phase row, covering [-padLo, bw + 4) in sum coordinates.
+inline void PhaseGeometry(int bw, int os, int& padLo, int& nb)
+{
+   padLo = os * ((4 + os - 1) / os);
+   nb = (padLo + bw + 4 + os - 1) / os;
+}
+int LaunchPhaseSplit(iscu_ctx* ctx, const float* sums, int nz, int bw, int os, int padLo, int nb, double* out);
 int LaunchNormalizePlanes(iscu_ctx* ctx, float* planes, int planeElems, int nPlanes);
 // defocusM: each PSF's defocus in metres (the reference's resAxialM * (z - (nz - 1) / 2) for a stack's plane z).
 int BuildPsfLibrary(iscu_ctx* ctx, const iscu_psf_request* sets, uint32_t nSets, const uint32_t* setOfPsf,

@@ -31,7 +31,8 @@ struct iscu_render_graph
    cudaGraph_t graph = nullptr;
    cudaGraphExec_t exec = nullptr;
    int kernels = 0;
-   iscu::DevBuf order;   // the persistent form's frame order + work counter, owned by the graph
+   iscu::DevBuf order;            // the persistent form's frame order + work counter, owned by the graph
+   iscu::ContribScratch contrib;  // the two-pass forms' scratch, owned by the graph
 };
 
 namespace iscu {
@@ -40,58 +41,77 @@ namespace {
 
 constexpr int kThreads = 256, kChunk = 256;
 
-// One staged emitter's contribution to pixel (X, Y), added to acc.
-__device__ __forceinline__ void SplatOne(const StagedEmitter& e, const KernelView& kv, int X, int Y, float& acc)
+// Whether pixel (X, Y) lies in the emitter's splat square and halo cut; its offset (dx, dy) from the centre pixel.
+__device__ __forceinline__ bool Covers(const StagedEmitter& e, int X, int Y, int& dx, int& dy)
 {
-   const int camRad = kv.camRad;
-   const int dx = X - e.x0, dy = Y - e.y0;
-   if (dx < -camRad || dx > camRad || dy < -camRad || dy > camRad)
-      return;
-   if (kv.spanLo)
+   dx = X - e.x0;
+   dy = Y - e.y0;
+   const int cr = e.camRad;
+   if (dx < -cr || dx > cr || dy < -cr || dy > cr)
+      return false;
+   if (e.spanLo && (dx < e.spanLo[dy + cr] || dx > e.spanHi[dy + cr]))
+      return false;
+   return true;
+}
+
+// The 16 taps of a fast emitter for the pixel p words from its centre pixel in the phase layout: the reference's
+// row = 0; row += wx[i] B; sum += wy[j] row, unrolled. Taps outside the bw x bw array read the layout's zero margin
+// where the reference skips them, and the sums start from the first product instead of 0: both change at most the
+// sign of a zero partial sum, which the final float add cannot see (a pixel that starts at a background other than
+// -0 is never -0).
+__device__ __forceinline__ double PhaseTaps(const StagedEmitter& e, int p)
+{
+   int q[4];
+#pragma unroll
+   for (int i = 0; i < 4; ++i)
+      q[i] = p + e.xb[i];
+   double row[4];
+#pragma unroll
+   for (int j = 0; j < 4; ++j)
    {
-      const int row = e.plane * (2 * camRad + 1) + dy + camRad;
-      if (dx < kv.spanLo[row] || dx > kv.spanHi[row])
-         return;
+      const double* pr = e.row[j];
+      double r = e.wx[0] * __ldg(pr + q[0]);
+      r += e.wx[1] * __ldg(pr + q[1]);
+      r += e.wx[2] * __ldg(pr + q[2]);
+      r += e.wx[3] * __ldg(pr + q[3]);
+      row[j] = r;
    }
+   double sum = e.wy[0] * row[0];
+   sum += e.wy[1] * row[1];
+   sum += e.wy[2] * row[2];
+   sum += e.wy[3] * row[3];
+   return sum;
+}
+
+// Any splat (1, 2 or 4 taps) from the row-major float64 block sums, taps outside the array skipped, in the
+// reference's order (SplatKernel.inl:51-171).
+__device__ __forceinline__ double GeneralTaps(const StagedEmitter& e, const KernelView& kv, int dx, int dy)
+{
    const int os = kv.os, off = os - 1, bw = kv.bw, nt = e.nTaps;
    const int r0 = e.by + dy * os + off, c0 = e.bx + dx * os + off;
    const double* B = kv.sums64 + static_cast<size_t>(e.plane) * bw * bw;
-   double sum;
-   if (nt == 4 && r0 >= 0 && r0 + 4 <= bw && c0 >= 0 && c0 + 4 <= bw)
+   const int jLo = max(0, -r0), jHi = min(nt, bw - r0);
+   const int iLo = max(0, -c0), iHi = min(nt, bw - c0);
+   double sum = 0.0;
+   for (int j = jLo; j < jHi; ++j)
    {
-      // all 16 taps inside: the reference's row = 0; row += wx[i] B; sum += wy[j] row, unrolled (starting from the
-      // first product instead of 0 changes at most the sign of a zero sum, which the float add cannot see)
-      const double* b = B + static_cast<size_t>(r0) * bw + c0;
-      double row[4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-      {
-         const double* br = b + j * bw;
-         double r = e.wx[0] * __ldg(br);
-         r += e.wx[1] * __ldg(br + 1);
-         r += e.wx[2] * __ldg(br + 2);
-         r += e.wx[3] * __ldg(br + 3);
-         row[j] = r;
-      }
-      sum = e.wy[0] * row[0];
-      sum += e.wy[1] * row[1];
-      sum += e.wy[2] * row[2];
-      sum += e.wy[3] * row[3];
+      const double* brow = B + static_cast<size_t>(r0 + j) * bw + c0;
+      double row = 0.0;
+      for (int i = iLo; i < iHi; ++i)
+         row += e.wx[i] * __ldg(brow + i);
+      sum += e.wy[j] * row;
    }
-   else
-   {
-      const int jLo = max(0, -r0), jHi = min(nt, bw - r0);
-      const int iLo = max(0, -c0), iHi = min(nt, bw - c0);
-      sum = 0.0;
-      for (int j = jLo; j < jHi; ++j)
-      {
-         const double* brow = B + static_cast<size_t>(r0 + j) * bw + c0;
-         double row = 0.0;
-         for (int i = iLo; i < iHi; ++i)
-            row += e.wx[i] * __ldg(brow + i);
-         sum += e.wy[j] * row;
-      }
-   }
+   return sum;
+}
+
+// One staged emitter's contribution to pixel (X, Y), added to acc.
+__device__ __forceinline__ void SplatSingle(const StagedEmitter& e, const Kernels& K, bool inside, int X, int Y,
+                                            float& acc)
+{
+   int dx, dy;
+   if (!inside || !Covers(e, X, Y, dx, dy))
+      return;
+   const double sum = e.fast ? PhaseTaps(e, dy * e.nb + dx) : GeneralTaps(e, K.k[e.slot], dx, dy);
    acc += static_cast<float>(e.photons * sum);
 }
 
@@ -109,21 +129,47 @@ __device__ __forceinline__ int StageChunk(const iscu_emitter* __restrict__ ems, 
    {
       const iscu_emitter em = ems[start + t];
       const int slot = static_cast<int>(static_cast<uint32_t>(em.plane) >> 16), plane = em.plane & 0xffff;
-      if (slot < ISCU_MAX_KERNELS && em.photons > 0.0 && K.k[slot].sums64 && plane < K.k[slot].nz)
+      if (slot < ISCU_MAX_KERNELS && em.photons > 0.0 && K.k[slot].sums64 && plane < K.k[slot].nz &&
+          PositionOk(em.x_px, em.y_px))
       {
          s.x0 = static_cast<int>(RoundHalfUp(em.x_px));
          s.y0 = static_cast<int>(RoundHalfUp(em.y_px));
          const int r = K.k[slot].camRad;
          keep = s.x0 + r >= tx0 && s.x0 - r <= tx1 && s.y0 + r >= ty0 && s.y0 - r <= ty1;
          s.photons = em.photons;
-         s.slot = slot;
+         s.slot = static_cast<uint8_t>(slot);
          s.plane = plane;
          xPx = em.x_px;
          yPx = em.y_px;
       }
    }
    if (keep)
-      SetupWeights(K.k[s.slot], xPx, yPx, s);
+   {
+      const KernelView& kv = K.k[s.slot];
+      SetupWeights(kv, xPx, yPx, s);
+      s.camRad = kv.camRad;
+      s.nb = kv.nb;
+      const int sq = 2 * kv.camRad + 1;
+      s.spanLo = kv.spanLo ? kv.spanLo + s.plane * sq : nullptr;
+      s.spanHi = kv.spanHi ? kv.spanHi + s.plane * sq : nullptr;
+      // The phase layout serves the splat when every tap of every pixel of its square lies inside it (rows
+      // R + dy os + j, columns C + dx os + i in padded coordinates, |dx|, |dy| <= camRad, i, j < 4).
+      const int os = kv.os, ext = kv.nb * os, span = kv.camRad * os;
+      const int R = s.by + os - 1 + kv.padLo, Cc = s.bx + os - 1 + kv.padLo;
+      s.fast = kv.phase && s.nTaps == 4 && R - span >= 0 && R + span + 3 < ext && Cc - span >= 0 &&
+               Cc + span + 3 < ext;
+      if (s.fast)
+      {
+         const int nb2 = kv.nb * kv.nb;
+         const double* base = kv.phase + static_cast<size_t>(s.plane) * os * os * nb2;
+#pragma unroll
+         for (int k = 0; k < 4; ++k)
+         {
+            s.row[k] = base + ((R + k) % os) * os * nb2 + ((R + k) / os) * kv.nb;
+            s.xb[k] = ((Cc + k) % os) * nb2 + (Cc + k) / os;
+         }
+      }
+   }
    const unsigned ballot = __ballot_sync(0xffffffffu, keep);
    if (lane == 0)
       sWarp[warp] = __popc(ballot);
@@ -142,9 +188,36 @@ __device__ __forceinline__ int StageChunk(const iscu_emitter* __restrict__ ems, 
    return total;
 }
 
+// The warp's own list: the staged emitters whose square reaches the warp's pixel rectangle [wx0, wx1] x [wy0, wy1],
+// in staged order. Returns its length.
+__device__ __forceinline__ int WarpList(const StagedEmitter* sEm, int kept, int wx0, int wx1, int wy0, int wy1,
+                                        uint16_t* list)
+{
+   const int lane = threadIdx.x & 31;
+   int n = 0;
+   for (int b = 0; b < kept; b += 32)
+   {
+      const int k = b + lane;
+      bool hit = false;
+      if (k < kept)
+      {
+         const StagedEmitter& e = sEm[k];
+         const int cr = e.camRad;
+         hit = e.x0 + cr >= wx0 && e.x0 - cr <= wx1 && e.y0 + cr >= wy0 && e.y0 - cr <= wy1;
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, hit);
+      if (hit)
+         list[n + __popc(bal & ((1u << lane) - 1u))] = static_cast<uint16_t>(k);
+      n += __popc(bal);
+   }
+   __syncwarp();
+   return n;
+}
+
 struct RenderArgs
 {
    const iscu_emitter* ems;
+   uint32_t nEm;            // emitter runs are cut at nEm
    const iscu_frame* frames;
    uint32_t nFrames;
    const uint32_t* order;   // persistent form: frames, heaviest first
@@ -157,16 +230,24 @@ struct RenderArgs
    uint16_t* aduOut;
 };
 
-template <int TX, int TY, bool kNoise, bool kPersistent>
-__global__ void __launch_bounds__(kThreads) RenderTilesKernel(RenderArgs a)
+// kPair: two emitters per step (their taps in flight together; 2 CTAs per SM by registers), else one (3 CTAs).
+template <int TX, int TY, bool kNoise, bool kPersistent, bool kPair>
+__global__ void __launch_bounds__(kThreads, kPair ? 2 : 3) RenderTilesKernel(RenderArgs a)
 {
    static_assert(TX * TY == kThreads, "one thread per pixel of the tile");
+   static_assert(TX % 32 == 0 || 32 % TX == 0, "a warp covers a rectangle of the tile");
    __shared__ StagedEmitter sEm[kChunk];
+   __shared__ uint16_t sList[kThreads / 32][kChunk];
    __shared__ int sWarp[kThreads / 32];
    __shared__ uint32_t sItem;
    const int W = static_cast<int>(a.st.width), H = static_cast<int>(a.st.height);
    const uint32_t tilesX = (W + TX - 1) / TX, tilesY = (H + TY - 1) / TY, tilesPerFrame = tilesX * tilesY;
    const uint32_t total = a.nFrames * tilesPerFrame;
+   const int warp = threadIdx.x >> 5;
+   uint16_t* list = sList[warp];
+   // the warp's pixel rectangle within the tile
+   const int wcx = TX >= 32 ? (32 * warp) % TX : 0, wcw = TX >= 32 ? 32 : TX;
+   const int wry = (32 * warp) / TX, wrh = TX >= 32 ? 1 : 32 / TX;
    for (;;)
    {
       uint32_t f, tile;
@@ -193,14 +274,41 @@ __global__ void __launch_bounds__(kThreads) RenderTilesKernel(RenderArgs a)
       const int tx1 = min(tx0 + TX, W) - 1, ty1 = min(ty0 + TY, H) - 1;
       const bool inside = X < W && Y < H;
       const uint32_t i = static_cast<uint32_t>(Y) * a.st.width + static_cast<uint32_t>(X);
+      const int wx0 = tx0 + wcx, wy0 = ty0 + wry;
       float acc = inside ? Background(a.st, i, fr.bg_scale) : 0.0f;
-      for (uint32_t e0 = 0; e0 < fr.em_count; e0 += kChunk)
+      const uint32_t emCount = fr.em_start < a.nEm ? min(fr.em_count, a.nEm - fr.em_start) : 0u;
+      for (uint32_t e0 = 0; e0 < emCount; e0 += kChunk)
       {
-         const uint32_t cnt = min(static_cast<uint32_t>(kChunk), fr.em_count - e0);
+         const uint32_t cnt = min(static_cast<uint32_t>(kChunk), emCount - e0);
          const int kept = StageChunk(a.ems, fr.em_start + e0, cnt, a.K, tx0, ty0, tx1, ty1, sEm, sWarp);
-         if (inside)
-            for (int k = 0; k < kept; ++k)
-               SplatOne(sEm[k], a.K.k[sEm[k].slot], X, Y, acc);
+         const int n = WarpList(sEm, kept, wx0, wx0 + wcw - 1, wy0, wy0 + wrh - 1, list);
+         // Two emitters per step, their taps independent (more loads in flight), their adds in list order.
+         int m = 0;
+         for (; kPair && m + 1 < n; m += 2)
+         {
+            const StagedEmitter& ea = sEm[list[m]];
+            const StagedEmitter& eb = sEm[list[m + 1]];
+            if (ea.fast && eb.fast)
+            {
+               int dxa, dya, dxb, dyb;
+               const bool ina = inside && Covers(ea, X, Y, dxa, dya);
+               const bool inb = inside && Covers(eb, X, Y, dxb, dyb);
+               // a pixel outside a square reads the centre pixel's taps (in the layout) and adds nothing
+               const double sa = PhaseTaps(ea, ina ? dya * ea.nb + dxa : 0);
+               const double sb = PhaseTaps(eb, inb ? dyb * eb.nb + dxb : 0);
+               if (ina)
+                  acc += static_cast<float>(ea.photons * sa);
+               if (inb)
+                  acc += static_cast<float>(eb.photons * sb);
+            }
+            else
+            {
+               SplatSingle(ea, a.K, inside, X, Y, acc);
+               SplatSingle(eb, a.K, inside, X, Y, acc);
+            }
+         }
+         for (; m < n; ++m)
+            SplatSingle(sEm[list[m]], a.K, inside, X, Y, acc);
          __syncthreads();
       }
       if (inside)
@@ -242,6 +350,22 @@ __global__ void IdentityOrderKernel(uint32_t n, uint32_t* __restrict__ order)
       order[i] = i;
 }
 
+// phase[z][qy][qx][ky][kx] = sums[z][ky os + qy - padLo][kx os + qx - padLo], 0 outside the array.
+__global__ void PhaseSplitKernel(const float* __restrict__ sums, int bw, int os, int padLo, int nb,
+                                 double* __restrict__ out)
+{
+   const int kx = blockIdx.x * blockDim.x + threadIdx.x;
+   const int ky = blockIdx.y;
+   const int z = blockIdx.z / (os * os), q = blockIdx.z % (os * os), qy = q / os, qx = q % os;
+   if (kx >= nb)
+      return;
+   const int r = ky * os + qy - padLo, c = kx * os + qx - padLo;
+   const double v = (r >= 0 && r < bw && c >= 0 && c < bw)
+                       ? static_cast<double>(sums[(static_cast<size_t>(z) * bw + r) * bw + c])
+                       : 0.0;
+   out[((static_cast<size_t>(blockIdx.z) * nb) + ky) * nb + kx] = v;
+}
+
 __global__ void SumsToDoubleKernel(const float* __restrict__ in, size_t n, double* __restrict__ out)
 {
    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -249,60 +373,70 @@ __global__ void SumsToDoubleKernel(const float* __restrict__ in, size_t n, doubl
       out[i] = static_cast<double>(in[i]);
 }
 
-// The six configurations: tile 16 x 16, 32 x 8, 8 x 32; grid or persistent.
+// The forms: config % 3 the tile (16 x 16, 32 x 8, 8 x 32), (config / 3) % 2 grid or persistent, config / 6 one or
+// two emitters per step.
 using RenderFn = void (*)(RenderArgs);
+template <bool kNoise, bool kPersistent, bool kPair>
+RenderFn TileVariant(int tile)
+{
+   switch (tile)
+   {
+   case 0: return RenderTilesKernel<16, 16, kNoise, kPersistent, kPair>;
+   case 1: return RenderTilesKernel<32, 8, kNoise, kPersistent, kPair>;
+   default: return RenderTilesKernel<8, 32, kNoise, kPersistent, kPair>;
+   }
+}
 template <bool kNoise>
 RenderFn Variant(int config)
 {
-   switch (config)
+   const int tile = config % 3;
+   switch (config / 3)
    {
-   case 0: return RenderTilesKernel<16, 16, kNoise, false>;
-   case 1: return RenderTilesKernel<32, 8, kNoise, false>;
-   case 2: return RenderTilesKernel<8, 32, kNoise, false>;
-   case 3: return RenderTilesKernel<16, 16, kNoise, true>;
-   case 4: return RenderTilesKernel<32, 8, kNoise, true>;
-   default: return RenderTilesKernel<8, 32, kNoise, true>;
+   case 0: return TileVariant<kNoise, false, false>(tile);
+   case 1: return TileVariant<kNoise, true, false>(tile);
+   case 2: return TileVariant<kNoise, false, true>(tile);
+   default: return TileVariant<kNoise, true, true>(tile);
    }
 }
 constexpr int kTileW[3] = {16, 32, 8}, kTileH[3] = {16, 8, 32};
 
-Kernels KernelsOf(iscu_ctx* ctx)
+// The forms 0..11 (one pass) and 12..17 (two passes, render_contrib.cu). orderBuf: OrderBytes(nFrames) bytes of
+// device scratch (the persistent forms' frame order and work counter). A two-pass form whose contributions would
+// pass the context's limit renders in the one-pass form of the same tile and scheduling (the same bits).
+int LaunchConfig(iscu_ctx* ctx, int config, const iscu_emitter* ems, uint32_t nEm, const iscu_frame* frames,
+                 uint32_t nFrames, const CameraView* cam, uint32_t seed, float* photons, uint16_t* adu,
+                 uint32_t* orderBuf, ContribScratch& sc)
 {
-   Kernels K;
-   for (int s = 0; s < ISCU_MAX_KERNELS; ++s)
-      K.k[s] = ctx->kernels[s].valid ? ctx->kernels[s].View() : KernelView();
-   return K;
-}
-
-size_t OrderBytes(uint32_t nFrames) { return (static_cast<size_t>(nFrames + 3) & ~size_t(3)) * 4 + 16; }
-
-// orderBuf: OrderBytes(nFrames) bytes of device scratch (the persistent forms' frame order and work counter).
-int LaunchConfig(iscu_ctx* ctx, int config, const iscu_emitter* ems, const iscu_frame* frames, uint32_t nFrames,
-                 const CameraView* cam, uint32_t seed, float* photons, uint16_t* adu, uint32_t* orderBuf)
-{
+   if (config >= 12)
+   {
+      const int rc = LaunchContribRender(ctx, config - 12, ems, nEm, frames, nFrames, cam, seed, photons, adu,
+                                         orderBuf, sc);
+      if (rc != ISCU_ERR_LIMIT)
+         return rc;
+      ClearError();
+      config -= 12;
+   }
    RenderArgs a;
    a.ems = ems;
+   a.nEm = nEm;
    a.frames = frames;
    a.nFrames = nFrames;
-   a.K = KernelsOf(ctx);
+   a.K = KernelsOfCtx(ctx);
    a.st = ctx->Static();
    a.cam = cam ? *cam : CameraView();
    a.seed = seed;
    a.photonsOut = photons;
    a.aduOut = cam ? adu : nullptr;
-   const bool persistent = config >= 3;
+   const bool persistent = (config / 3) % 2 == 1;
    const int tw = kTileW[config % 3], th = kTileH[config % 3];
    RenderFn fn = cam ? Variant<true>(config) : Variant<false>(config);
    if (persistent)
    {
+      const int rc = LaunchFrameOrder(ctx, frames, nFrames, orderBuf);
+      if (rc != ISCU_OK)
+         return rc;
       a.order = orderBuf;
       a.counter = orderBuf + ((nFrames + 3) & ~3u);
-      ISCU_CK(cudaMemsetAsync(a.counter, 0, sizeof(uint32_t), ctx->stream));
-      if (nFrames <= 8192)
-         FrameOrderKernel<<<(nFrames + 127) / 128, 128, 0, ctx->stream>>>(frames, nFrames, orderBuf);
-      else
-         IdentityOrderKernel<<<(nFrames + 255) / 256, 256, 0, ctx->stream>>>(nFrames, orderBuf);
-      ISCU_CK_LAUNCH(ctx, "FrameOrderKernel");
       int perSm = 0;
       ISCU_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, fn, kThreads, 0));
       const uint32_t tiles = ((a.st.width + tw - 1) / tw) * ((a.st.height + th - 1) / th);
@@ -323,6 +457,19 @@ int LaunchConfig(iscu_ctx* ctx, int config, const iscu_emitter* ems, const iscu_
 
 } // namespace
 
+size_t OrderBytes(uint32_t nFrames) { return (static_cast<size_t>(nFrames + 3) & ~size_t(3)) * 4 + 16; }
+
+int LaunchFrameOrder(iscu_ctx* ctx, const iscu_frame* frames, uint32_t nFrames, uint32_t* orderBuf)
+{
+   ISCU_CK(cudaMemsetAsync(orderBuf + ((nFrames + 3) & ~3u), 0, sizeof(uint32_t), ctx->stream));
+   if (nFrames <= 8192)
+      FrameOrderKernel<<<(nFrames + 127) / 128, 128, 0, ctx->stream>>>(frames, nFrames, orderBuf);
+   else
+      IdentityOrderKernel<<<(nFrames + 255) / 256, 256, 0, ctx->stream>>>(nFrames, orderBuf);
+   ISCU_CK_LAUNCH(ctx, "FrameOrderKernel");
+   return ISCU_OK;
+}
+
 int LaunchSumsToDouble(iscu_ctx* ctx, const float* in, size_t n, double* out)
 {
    SumsToDoubleKernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, ctx->stream>>>(in, n, out);
@@ -330,15 +477,22 @@ int LaunchSumsToDouble(iscu_ctx* ctx, const float* in, size_t n, double* out)
    return ISCU_OK;
 }
 
-int LaunchRenderFrames(iscu_ctx* ctx, const iscu_emitter* ems, const iscu_frame* frames, uint32_t nFrames,
-                       const CameraView* cam, uint32_t seed, float* photons, uint16_t* adu)
+int LaunchPhaseSplit(iscu_ctx* ctx, const float* sums, int nz, int bw, int os, int padLo, int nb, double* out)
+{
+   const dim3 grid((nb + 127) / 128, nb, nz * os * os);
+   PhaseSplitKernel<<<grid, 128, 0, ctx->stream>>>(sums, bw, os, padLo, nb, out);
+   ISCU_CK_LAUNCH(ctx, "PhaseSplitKernel");
+   return ISCU_OK;
+}
+
+int LaunchRenderFrames(iscu_ctx* ctx, const iscu_emitter* ems, uint32_t nEmitters, const iscu_frame* frames,
+                       uint32_t nFrames, const CameraView* cam, uint32_t seed, float* photons, uint16_t* adu)
 {
    if (nFrames == 0)
       return ISCU_OK;
-   if (ctx->renderConfig >= 3)
-      ISCU_CK(ctx->dOrder.Reserve(OrderBytes(nFrames)));
-   return LaunchConfig(ctx, ctx->renderConfig, ems, frames, nFrames, cam, seed, photons, adu,
-                       ctx->dOrder.as<uint32_t>());
+   ISCU_CK(ctx->dOrder.Reserve(OrderBytes(nFrames)));
+   return LaunchConfig(ctx, ctx->renderConfig, ems, nEmitters, frames, nFrames, cam, seed, photons, adu,
+                       ctx->dOrder.as<uint32_t>(), ctx->contrib);
 }
 
 } // namespace iscu
@@ -349,14 +503,25 @@ extern "C" {
 
 int iscu_render_set_config(iscu_ctx* ctx, int32_t config)
 {
-   if (!ctx || config < 0 || config > 5)
-      return Fail(ISCU_ERR_ARG, "render config 0..5 (tile 16x16, 32x8, 8x32; +3: persistent)");
+   if (!ctx || config < 0 || config >= ISCU_RENDER_CONFIGS)
+      return Fail(ISCU_ERR_ARG, "render config 0..17 (tile 16x16, 32x8, 8x32; +3: persistent; +6: two emitters "
+                                "per step; 12..17: two passes)");
    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
    ctx->renderConfig = config;
    return ISCU_OK;
 }
 
-int iscu_render_get_config(iscu_ctx* ctx, int32_t* config, int32_t* tile_w, int32_t* tile_h, int32_t* persistent)
+int iscu_render_set_contrib_limit(iscu_ctx* ctx, uint64_t bytes)
+{
+   if (!ctx)
+      return Fail(ISCU_ERR_ARG, "null context");
+   std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+   ctx->contribLimit = static_cast<size_t>(bytes);
+   return ISCU_OK;
+}
+
+int iscu_render_get_config(iscu_ctx* ctx, int32_t* config, int32_t* tile_w, int32_t* tile_h, int32_t* persistent,
+                           int32_t* paired)
 {
    if (!ctx)
       return Fail(ISCU_ERR_ARG, "null context");
@@ -368,12 +533,15 @@ int iscu_render_get_config(iscu_ctx* ctx, int32_t* config, int32_t* tile_w, int3
    if (tile_h)
       *tile_h = kTileH[c % 3];
    if (persistent)
-      *persistent = c >= 3;
+      *persistent = (c / 3) % 2;
+   if (paired)
+      *paired = c < 12 ? c / 6 : 2;
    return ISCU_OK;
 }
 
-int iscu_render_autotune(iscu_ctx* ctx, const iscu_emitter* emitters_dev, const iscu_frame* frames_dev,
-                         uint32_t n_frames, const iscu_camera* cam, uint32_t seed, uint16_t* adu_dev, float* ms6)
+int iscu_render_autotune(iscu_ctx* ctx, const iscu_emitter* emitters_dev, uint32_t n_emitters,
+                         const iscu_frame* frames_dev, uint32_t n_frames, const iscu_camera* cam, uint32_t seed,
+                         uint16_t* adu_dev, float* ms)
 {
    if (!ctx || !frames_dev || !cam || !adu_dev || n_frames == 0)
       return Fail(ISCU_ERR_ARG, "null argument or no frames");
@@ -384,45 +552,50 @@ int iscu_render_autotune(iscu_ctx* ctx, const iscu_emitter* emitters_dev, const 
    const CameraView cv = MakeCameraView(*cam);
    ISCU_CK(ctx->dOrder.Reserve(OrderBytes(n_frames)));
    uint32_t* order = ctx->dOrder.as<uint32_t>();
-   cudaEvent_t e0, e1;
-   ISCU_CK(cudaEventCreate(&e0));
-   ISCU_CK(cudaEventCreate(&e1));
+   struct Events
+   {
+      cudaEvent_t e[2] = {nullptr, nullptr};
+      ~Events()
+      {
+         for (cudaEvent_t x : e)
+            if (x)
+               cudaEventDestroy(x);
+      }
+   } ev;
+   ISCU_CK(cudaEventCreate(&ev.e[0]));
+   ISCU_CK(cudaEventCreate(&ev.e[1]));
    float best = 1e30f;
    int bestConfig = 0;
-   for (int c = 0; c < 6; ++c)
+   for (int c = 0; c < ISCU_RENDER_CONFIGS; ++c)
    {
-      int rc = LaunchConfig(ctx, c, emitters_dev, frames_dev, n_frames, &cv, seed, nullptr, adu_dev, order);   // warm
-      ISCU_CK(cudaEventRecord(e0, ctx->stream));
+      int rc = LaunchConfig(ctx, c, emitters_dev, n_emitters, frames_dev, n_frames, &cv, seed, nullptr, adu_dev,
+                            order, ctx->contrib);   // warm
+      ISCU_CK(cudaEventRecord(ev.e[0], ctx->stream));
       for (int r = 0; r < 2 && rc == ISCU_OK; ++r)
-         rc = LaunchConfig(ctx, c, emitters_dev, frames_dev, n_frames, &cv, seed, nullptr, adu_dev, order);
-      ISCU_CK(cudaEventRecord(e1, ctx->stream));
+         rc = LaunchConfig(ctx, c, emitters_dev, n_emitters, frames_dev, n_frames, &cv, seed, nullptr, adu_dev,
+                           order, ctx->contrib);
+      ISCU_CK(cudaEventRecord(ev.e[1], ctx->stream));
       if (rc != ISCU_OK)
-      {
-         cudaEventDestroy(e0);
-         cudaEventDestroy(e1);
          return rc;
-      }
-      ISCU_CK(cudaEventSynchronize(e1));
-      float ms = 0.f;
-      ISCU_CK(cudaEventElapsedTime(&ms, e0, e1));
-      ms *= 0.5f;
-      if (ms6)
-         ms6[c] = ms;
-      if (ms < best)
+      ISCU_CK(cudaEventSynchronize(ev.e[1]));
+      float t = 0.f;
+      ISCU_CK(cudaEventElapsedTime(&t, ev.e[0], ev.e[1]));
+      t *= 0.5f;
+      if (ms)
+         ms[c] = t;
+      if (t < best)
       {
-         best = ms;
+         best = t;
          bestConfig = c;
       }
    }
-   cudaEventDestroy(e0);
-   cudaEventDestroy(e1);
    ctx->renderConfig = bestConfig;
    return ISCU_OK;
 }
 
-int iscu_render_graph_create(iscu_ctx* ctx, const iscu_emitter* emitters_dev, const iscu_frame* frames_dev,
-                             uint32_t n_frames, const iscu_camera* cam, uint32_t seed, float* photons_dev,
-                             uint16_t* adu_dev, iscu_render_graph** out)
+int iscu_render_graph_create(iscu_ctx* ctx, const iscu_emitter* emitters_dev, uint32_t n_emitters,
+                             const iscu_frame* frames_dev, uint32_t n_frames, const iscu_camera* cam, uint32_t seed,
+                             float* photons_dev, uint16_t* adu_dev, iscu_render_graph** out)
 {
    if (!ctx || !out || !frames_dev || n_frames == 0 || (cam && !adu_dev))
       return Fail(ISCU_ERR_ARG, "null argument or no frames");
@@ -436,11 +609,24 @@ int iscu_render_graph_create(iscu_ctx* ctx, const iscu_emitter* emitters_dev, co
       cv = MakeCameraView(*cam);
    std::unique_ptr<iscu_render_graph> g(new iscu_render_graph());
    g->ctx = ctx;
-   ISCU_CK(g->order.Reserve(OrderBytes(n_frames)));   // scratch the capture bakes in, alive as long as the graph
+   // the scratch the capture bakes in, alive as long as the graph, allocated before the capture
+   ISCU_CK(g->order.Reserve(OrderBytes(n_frames)));
+   int config = ctx->renderConfig;
+   if (config >= 12)
+   {
+      const int rr = ReserveContrib(ctx, n_emitters, g->contrib);
+      if (rr == ISCU_ERR_LIMIT)
+      {
+         ClearError();
+         config -= 12;   // the one-pass form of the same tile and scheduling
+      }
+      else if (rr != ISCU_OK)
+         return rr;
+   }
    const uint64_t before = ctx->launches.load();
    ISCU_CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-   const int rc = LaunchConfig(ctx, ctx->renderConfig, emitters_dev, frames_dev, n_frames, cam ? &cv : nullptr, seed,
-                               photons_dev, adu_dev, g->order.as<uint32_t>());
+   const int rc = LaunchConfig(ctx, config, emitters_dev, n_emitters, frames_dev, n_frames, cam ? &cv : nullptr,
+                               seed, photons_dev, adu_dev, g->order.as<uint32_t>(), g->contrib);
    cudaGraph_t graph = nullptr;
    const cudaError_t ec = cudaStreamEndCapture(ctx->stream, &graph);
    if (rc != ISCU_OK)

@@ -34,14 +34,35 @@ __device__ __forceinline__ void CatmullRom(double f, double* w)
    w[3] = 0.5 * f3 - 0.5 * f2;
 }
 
-// One emitter's splat parameters, as SplatSetup (PsfGeneratorBridge.cpp:1382-1422) derives them.
+// One emitter's splat parameters, as SplatSetup (PsfGeneratorBridge.cpp:1382-1422) derives them, with what the
+// render's inner loop reads staged beside them.
 struct StagedEmitter
 {
    double photons;
    double wx[4], wy[4];
-   int x0, y0, bx, by;
-   int nTaps, slot, plane, pad;
+   const double* row[4];    // phase layout (fast): tap row j's words for the centre pixel
+   int xb[4];               // phase layout (fast): tap column i's word offsets
+   int x0, y0, camRad, nb;  // centre pixel, splat square radius, phase-layout row pitch
+   const int16_t* spanLo;   // halo cut of the emitter's plane, indexed by dy + camRad; null: the whole square
+   const int16_t* spanHi;
+   int bx, by, plane;
+   uint8_t nTaps, slot, fast, pad;   // fast: a 4 x 4 splat whose taps all lie in the phase layout
 };
+
+// Positions the splat accepts: finite and within +-1e9 pixels (beyond, the centre pixel leaves the int range).
+__host__ __device__ __forceinline__ bool PositionOk(double xPx, double yPx)
+{
+   return fabs(xPx) < 1e9 && fabs(yPx) < 1e9;
+}
+
+// What the splat kernels read of the context's kernel slots.
+inline Kernels KernelsOfCtx(iscu_ctx* ctx)
+{
+   Kernels K;
+   for (int s = 0; s < ISCU_MAX_KERNELS; ++s)
+      K.k[s] = ctx->kernels[s].valid ? ctx->kernels[s].View() : KernelView();
+   return K;
+}
 
 // SplatSetup in float64 from the centre pixel (x0, y0) = (round(x), round(y)) already known.
 __device__ __forceinline__ void SetupWeights(const KernelView& kv, double xPx, double yPx, StagedEmitter& s)

@@ -195,14 +195,6 @@ __global__ void BlockSumsKernel(const float* __restrict__ planes, int n, int os,
    sums[(static_cast<size_t>(z) * bw + ai) * bw + bi] = static_cast<float>(acc);
 }
 
-Kernels KernelsOfCtx(iscu_ctx* ctx)
-{
-   Kernels K;
-   for (int s = 0; s < ISCU_MAX_KERNELS; ++s)
-      K.k[s] = ctx->kernels[s].valid ? ctx->kernels[s].View() : KernelView();
-   return K;
-}
-
 } // namespace
 
 // ------------------------------------------------------------------------------------------------ launchers

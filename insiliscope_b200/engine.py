@@ -109,6 +109,15 @@ def _ptr(a) -> C.c_void_p:
     return C.c_void_p(a.data_ptr())   # torch tensor
 
 
+def _n_records(a) -> int:
+    """EMITTER_DTYPE records in a device (torch, any dtype viewed as bytes) or host emitter buffer."""
+    if a is None:
+        return 0
+    if isinstance(a, np.ndarray):
+        return a.nbytes // EMITTER_DTYPE.itemsize
+    return a.numel() * a.element_size() // EMITTER_DTYPE.itemsize
+
+
 def _f32(a, n=None):
     if a is None:
         return None
@@ -308,29 +317,35 @@ class Engine:
         """Device path on torch CUDA buffers (emitters: uint8 view of EMITTER_DTYPE records, frames likewise)."""
         cam = camera.c() if camera is not None else None
         self._before(sync)
-        check(self.lib.iscu_render_frames_dev(self.h, _ptr(emitters_dev), _ptr(frames_dev), n_frames,
+        check(self.lib.iscu_render_frames_dev(self.h, _ptr(emitters_dev), _n_records(emitters_dev), _ptr(frames_dev),
+                                              n_frames,
                                               C.byref(cam) if cam is not None else None, seed, _ptr(photons_dev),
                                               _ptr(adu_dev)))
         self._after(sync)
 
-    RENDER_CONFIGS = 6
+    RENDER_CONFIGS = 18
 
     def render_config(self):
-        """(config, tile_w, tile_h, persistent) of the render kernel form in use."""
-        v = [C.c_int32() for _ in range(4)]
+        """(config, tile_w, tile_h, persistent, paired) of the render kernel form in use; paired 0 or 1: one pass with
+        one or two emitters per step, 2: two passes."""
+        v = [C.c_int32() for _ in range(5)]
         check(self.lib.iscu_render_get_config(self.h, *[C.byref(x) for x in v]))
-        return v[0].value, v[1].value, v[2].value, bool(v[3].value)
+        return v[0].value, v[1].value, v[2].value, bool(v[3].value), bool(v[4].value)
 
     def set_render_config(self, config):
         check(self.lib.iscu_render_set_config(self.h, int(config)))
+
+    def set_contrib_limit(self, nbytes):
+        """The most device bytes the two-pass render forms' contributions may take (0: a quarter of the device)."""
+        check(self.lib.iscu_render_set_contrib_limit(self.h, int(nbytes)))
 
     def render_autotune(self, emitters_dev, frames_dev, n_frames, camera: CameraParams, seed, adu_dev):
         """Times the render forms on this device batch, keeps the fastest; returns ms per render of each form."""
         ms = (C.c_float * self.RENDER_CONFIGS)()
         cam = camera.c()
         self._before(True)
-        check(self.lib.iscu_render_autotune(self.h, _ptr(emitters_dev), _ptr(frames_dev), n_frames, C.byref(cam),
-                                            seed, _ptr(adu_dev), ms))
+        check(self.lib.iscu_render_autotune(self.h, _ptr(emitters_dev), _n_records(emitters_dev), _ptr(frames_dev),
+                                            n_frames, C.byref(cam), seed, _ptr(adu_dev), ms))
         self._after(True)
         return list(ms)
 
@@ -396,7 +411,8 @@ class RenderGraph:
         cam = camera.c() if camera is not None else None
         h = C.c_void_p()
         engine._before(True)
-        check(self.lib.iscu_render_graph_create(engine.h, _ptr(emitters_dev), _ptr(frames_dev), n_frames,
+        check(self.lib.iscu_render_graph_create(engine.h, _ptr(emitters_dev), _n_records(emitters_dev),
+                                                _ptr(frames_dev), n_frames,
                                                 C.byref(cam) if cam is not None else None, seed, _ptr(photons_dev),
                                                 _ptr(adu_dev), C.byref(h)))
         self.h = h

@@ -99,11 +99,11 @@ def test_autotune_and_graph(engine, reference, setup):
     d_em, d_fr, d_ph, d_adu = _dev(engine, ems, frames)
     try:
         ms = engine.render_autotune(d_em, d_fr, F, cam, 5, d_adu)
-        assert len(ms) == 6 and all(m > 0 for m in ms)
+        assert len(ms) == engine.RENDER_CONFIGS and all(m > 0 for m in ms)
         config = engine.render_config()[0]
         assert ms[config] == min(ms)
         ph_h, adu_h = engine.render_frames(ems, frames, cam, 5)
-        for persistent_config in (config, 4):
+        for persistent_config in (config, 4, 9, 12, 15):
             engine.set_render_config(persistent_config)
             g = RenderGraph(engine, d_em, d_fr, F, cam, 5, d_ph, d_adu)
             d_ph.zero_()
@@ -151,7 +151,7 @@ def test_heavy_frame_batch(engine, setup):
     try:
         engine.set_render_config(0)
         want = engine.render_frames(ems, frames, cam, 9)
-        for config in (3, 4, 5):
+        for config in (3, 4, 5, 6, 9, 11, 12, 13, 14, 15, 16, 17):
             engine.set_render_config(config)
             got = engine.render_frames(ems, frames, cam, 9)
             assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), config
@@ -159,8 +159,24 @@ def test_heavy_frame_batch(engine, setup):
         engine.set_render_config(0)
 
 
+def test_two_pass_over_limit_falls_back(engine, reference, setup):
+    """A two-pass form whose contributions pass the limit renders in the one-pass form: the same bits."""
+    kernels, (off, gain, rn), cam = setup
+    ev, bucket = _movie(np.random.default_rng(8))
+    ems, frames = _batch(engine, ev, bucket)
+    try:
+        engine.set_render_config(15)
+        want = engine.render_frames(ems, frames, cam, 3)
+        engine.set_contrib_limit(1024)
+        got = engine.render_frames(ems, frames, cam, 3)
+        assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+    finally:
+        engine.set_contrib_limit(0)
+        engine.set_render_config(0)
+
+
 def test_bad_config_rejected(engine):
     from insiliscope_b200 import IscuError
     with pytest.raises(IscuError):
-        engine.set_render_config(6)
-    assert engine.render_config()[0] in range(6)
+        engine.set_render_config(engine.RENDER_CONFIGS)
+    assert engine.render_config()[0] in range(engine.RENDER_CONFIGS)
