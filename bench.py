@@ -145,62 +145,101 @@ class SmlmWorkload:
         mv = self.mv
         self.eng = eng = Engine(device)
         t0 = time.perf_counter()
-        eng.kernel_build(0, mv.psf, CZT_FP32)
+        for slot, psf in enumerate(self.psfs()):
+            eng.kernel_build(slot, psf, CZT_FP32)
         eng.synchronize()
         self.psf_build_ms = (time.perf_counter() - t0) * 1e3
         off, gain, rn = generate_camera_maps(mv.width, mv.height, mv.map_seed, mv.offset_mean, mv.offset_std,
                                              mv.gain_nominal, mv.gain_std_fraction, mv.read_noise_nominal,
                                              mv.read_noise_std_fraction)
         eng.set_static(mv.width, mv.height, offset=off, gain=gain, read_noise=rn, flat_bg=mv.background)
-        self.ems, self.frames, _ = eng.collect_emitters(0, mv.events, mv.bucket_start, self.frame0, mv.width,
-                                                        mv.height, mv.pixel_nm, mv.photons_per_blink)
+        self.ems, self.frames, _ = eng.collect_emitters(self.slot, mv.events, mv.bucket_start, self.frame0,
+                                                        mv.width, mv.height, mv.pixel_nm, mv.photons_per_blink)
         self.ems = self.ems.copy()
-        self.d_em = torch.from_numpy(self.ems.view(np.uint8)).to(f"cuda:{device}")
-        self.d_fr = torch.from_numpy(self.frames.view(np.uint8)).to(f"cuda:{device}")
-        self.d_adu = torch.empty((mv.frames, mv.height, mv.width), dtype=torch.uint16, device=f"cuda:{device}")
-        self.h_adu = np.empty((mv.frames, mv.height, mv.width), np.uint16)
+        dev = f"cuda:{device}"
+        self.d_em = torch.from_numpy(self.ems.view(np.uint8)).to(dev)
+        self.d_fr = torch.from_numpy(self.frames.view(np.uint8)).to(dev)
+        self.d_adu = torch.empty((mv.frames, mv.height, mv.width), dtype=torch.uint16, device=dev)
+        t0 = time.perf_counter()
+        self.autotune_ms = eng.render_autotune(self.d_em, self.d_fr, mv.frames, mv.camera, mv.noise_seed, self.d_adu)
+        self.autotune_wall_ms = (time.perf_counter() - t0) * 1e3
+        self.form = eng.render_config()
+        # page-locked host buffers of the end-to-end call: the events and buckets in, the frames out
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8)).pin_memory().numpy().view(a.dtype)
+        self.h_events = pin(mv.events)
+        self.h_bucket = pin(np.ascontiguousarray(mv.bucket_start, np.uint32))
+        self.h_adu = torch.empty((mv.frames, mv.height, mv.width), dtype=torch.uint16).pin_memory().numpy()
         self.stream = eng.torch_stream()
         self.frames_per_step = mv.frames
         self.n_emitters = len(self.ems)
+
+    slot = 0
 
     def device_step(self):
         self.eng.render_frames_dev(self.d_em, self.d_fr, self.mv.frames, self.mv.camera, self.mv.noise_seed,
                                    None, self.d_adu, sync=False)
 
     def e2e_step(self):
-        """Host blink events -> host ADU: emitter collection, H2D, render, D2H, all through the C ABI."""
+        """Host blink events (page-locked) -> host ADU frames (page-locked) in one C-ABI call: H2D of the events,
+        emitter collection, render and noise on the device, D2H of the frames."""
         mv = self.mv
-        ems, frames, _ = self.eng.collect_emitters(0, mv.events, mv.bucket_start, self.frame0, mv.width, mv.height,
-                                                   mv.pixel_nm, mv.photons_per_blink, out=self._e2e_buf(),
-                                                   frames_out=self._e2e_frames())
-        _, adu = self.eng.render_frames(ems, frames, mv.camera, mv.noise_seed, want_photons=False)
+        _, adu, _ = self.eng.render_events(self.slot, self.h_events, self.h_bucket, self.frame0, mv.pixel_nm,
+                                           mv.photons_per_blink, mv.camera, mv.noise_seed, adu_out=self.h_adu)
         return adu
 
-    def _e2e_buf(self):
-        from insiliscope_b200 import EMITTER_DTYPE
-        if not hasattr(self, "_eb"):
-            self._eb = np.empty(len(self.mv.events), EMITTER_DTYPE)
-        return self._eb
-
-    def _e2e_frames(self):
-        from insiliscope_b200 import FRAME_DTYPE
-        if not hasattr(self, "_ef"):
-            self._ef = np.empty(self.mv.frames, FRAME_DTYPE)
-        return self._ef
-
     def e2e_bytes(self):
-        return self.n_emitters * 32 + self.mv.frames * 24, self.mv.frames * self.mv.width * self.mv.height * 2
+        return self.h_events.nbytes + self.h_bucket.nbytes, self.h_adu.nbytes
 
-    def alg_bytes_per_launch(self):
-        # Per frame: the ADU written (2 B/px) and the three float camera maps read (12 B/px); per emitter its 32-byte
-        # record; the frame table. The PSF block sums (3.4 MB) stay in L2 across the launch and count once.
+    def timing(self, on):
+        self.eng.set_render_timing(on)
+
+    def dominant(self):
+        """The render's passes, CUDA events inside the library over the timed steps: the slowest with its bytes."""
+        ms, calls = self.eng.render_pass_times()
+        name = max(ms, key=ms.get)
+        kernel = {"grouping": "ContribSetup/Scan/Scatter", "contributions": "ContribKernel",
+                  "tiles": "GatherTilesKernel" if self.form[4] == 2 else "RenderTilesKernel"}[name]
+        return kernel, self.pass_bytes(name), ms[name], {k: round(v, 4) for k, v in ms.items()}
+
+    def pass_bytes(self, name):
+        """Algorithmic HBM bytes of a render pass. Tiles: the ADU written (2 B/px), the three float camera maps
+        read (12 B/px), the frame table, each emitter's setup record (16 B), and every (emitter, square pixel)
+        contribution read once (4 B; the two-pass forms) or the emitter records (32 B; one pass). Contributions: each
+        emitter's staged record (88 B) read and its square's contributions written (4 B/px). Grouping: the emitter
+        records read (32 B) and their setup and staged records written (96 + 16 + 88 B)."""
         mv = self.mv
         px = mv.width * mv.height
-        _, nz, _, bw = self.eng.kernel_info(0)
-        return mv.frames * (px * 14 + 24) + self.n_emitters * 32 + nz * bw * bw * 4
+        two = self.form[4] == 2
+        def side(s):
+            size, _, os_, _ = self.eng.kernel_info(s)
+            return 2 * (((size - 1) // 2) // os_) + 1
+        sq = sum(side(s) ** 2 for s in self.slots_used()) / len(self.slots_used())
+        if name == "tiles":
+            per_em = 16 + 4 * sq if two else 32
+            return mv.frames * (px * 14 + 24) + self.n_emitters * per_em
+        if name == "contributions":
+            return self.n_emitters * (88 + 4 * sq)
+        return self.n_emitters * (32 + 96 + 16 + 88)
 
-    def kernel_name(self):
-        return "RenderTilesKernel"
+    def psfs(self):
+        return [self.mv.psf]
+
+    def slots_used(self):
+        return list(range(len(self.psfs())))
+
+    def config_extra(self):
+        tw, th = self.form[1], self.form[2]
+        return {"render_form": {"config": self.form[0], "tile": f"{tw}x{th}", "persistent": self.form[3],
+                                "passes": 2 if self.form[4] == 2 else 1,
+                                "autotune_ms_per_form": [round(x, 4) for x in self.autotune_ms]},
+                "mean_emitters_per_frame": self.n_emitters / self.mv.frames,
+                "max_emitters_per_frame": int(self.frames["em_count"].max())}
+
+    def alg_bytes_per_launch(self):
+        """A whole render's algorithmic bytes: its passes' (the one-pass forms: the tile pass alone)."""
+        if self.form[4] == 2:
+            return sum(self.pass_bytes(n) for n in ("grouping", "contributions", "tiles"))
+        return self.pass_bytes("tiles")
 
     # -------------------------------------------------- the reference on the host cores
     dtype = "f64"
@@ -237,76 +276,46 @@ class SmlmWorkload:
 class TwoColourWorkload(SmlmWorkload):
     """The uneven two-colour movie: 256 x 256 px, 1,024 frames of 10 to ~8,000 ON emitters (Poisson, lognormal
     per-frame mean), channel 0 (670 nm double helix) then channel 1 (580 nm astigmatic) splatted onto each frame,
-    then the sCMOS chain. The render form (tile shape, grid or persistent heaviest-frame-first) is autotuned once on
-    the batch, and one step replays the batch's render captured in a CUDA graph."""
+    then the sCMOS chain. The render form (tile shape, grid or persistent heaviest-frame-first, one or two passes) is
+    autotuned once on the batch, and one step replays the batch's render captured in a CUDA graph."""
     name = ("two-colour uneven SMLM 256x256 px, 1024 frames, Poisson ON counts with lognormal per-frame mean "
             "(median 300, clipped 10-8000), 670 nm double-helix + 580 nm astigmatic (Noll 5 = 0.1 lambda) 129^2x49 "
             "cubic PSFs, sCMOS")
+    slot = -1
 
     def __init__(self, rank: int):
         from insiliscope_b200.workloads import two_colour_uneven
         self.frame0 = rank * 1024
         self.mv = two_colour_uneven(seed=42, frame0=self.frame0)
 
+    def psfs(self):
+        return self.mv.psfs
+
     def setup(self, device: int):
-        import torch
-        from insiliscope_b200 import CZT_FP32, Engine, RenderGraph, generate_camera_maps
+        from insiliscope_b200 import RenderGraph
+        super().setup(device)
         mv = self.mv
-        self.eng = eng = Engine(device)
-        t0 = time.perf_counter()
-        for slot, psf in enumerate(mv.psfs):
-            eng.kernel_build(slot, psf, CZT_FP32)
-        eng.synchronize()
-        self.psf_build_ms = (time.perf_counter() - t0) * 1e3
-        off, gain, rn = generate_camera_maps(mv.width, mv.height, mv.map_seed, mv.offset_mean, mv.offset_std,
-                                             mv.gain_nominal, mv.gain_std_fraction, mv.read_noise_nominal,
-                                             mv.read_noise_std_fraction)
-        eng.set_static(mv.width, mv.height, offset=off, gain=gain, read_noise=rn, flat_bg=mv.background)
-        self.ems, self.frames, _ = eng.collect_emitters(-1, mv.events, mv.bucket_start, self.frame0, mv.width,
-                                                        mv.height, mv.pixel_nm, mv.photons_per_blink)
-        self.ems = self.ems.copy()
-        dev = f"cuda:{device}"
-        self.d_em = torch.from_numpy(self.ems.view(np.uint8)).to(dev)
-        self.d_fr = torch.from_numpy(self.frames.view(np.uint8)).to(dev)
-        self.d_adu = torch.empty((mv.frames, mv.height, mv.width), dtype=torch.uint16, device=dev)
-        t0 = time.perf_counter()
-        self.autotune_ms = eng.render_autotune(self.d_em, self.d_fr, mv.frames, mv.camera, mv.noise_seed, self.d_adu)
-        self.autotune_wall_ms = (time.perf_counter() - t0) * 1e3
-        self.form = eng.render_config()
-        self.graph = RenderGraph(eng, self.d_em, self.d_fr, mv.frames, mv.camera, mv.noise_seed, None, self.d_adu)
-        self.stream = eng.torch_stream()
-        self.frames_per_step = mv.frames
-        self.n_emitters = len(self.ems)
+        self.graph = RenderGraph(self.eng, self.d_em, self.d_fr, mv.frames, mv.camera, mv.noise_seed, None,
+                                 self.d_adu)
 
     def device_step(self):
         self.graph.launch(sync=False)
 
-    def e2e_step(self):
-        """Host blink events -> host ADU through the C ABI: collection (each event's own kernel slot), H2D, render in
-        the autotuned form, D2H."""
-        mv = self.mv
-        ems, frames, _ = self.eng.collect_emitters(-1, mv.events, mv.bucket_start, self.frame0, mv.width, mv.height,
-                                                   mv.pixel_nm, mv.photons_per_blink, out=self._e2e_buf(),
-                                                   frames_out=self._e2e_frames())
-        _, adu = self.eng.render_frames(ems, frames, mv.camera, mv.noise_seed, want_photons=False)
-        return adu
+    def timing(self, on):
+        pass   # graph replays carry no timing marks: dominant() times three direct renders
 
-    def alg_bytes_per_launch(self):
-        mv = self.mv
-        px = mv.width * mv.height
-        sums = 0
-        for slot in range(len(mv.psfs)):
-            _, nz, _, bw = self.eng.kernel_info(slot)
-            sums += nz * bw * bw * 8
-        return mv.frames * (px * 14 + 24) + self.n_emitters * 32 + sums
+    def dominant(self):
+        self.eng.set_render_timing(True)
+        for _ in range(3):
+            SmlmWorkload.device_step(self)
+        out = SmlmWorkload.dominant(self)
+        self.eng.set_render_timing(False)
+        return out
 
     def config_extra(self):
-        tw, th = self.form[1], self.form[2]
-        return {"render_form": {"config": self.form[0], "tile": f"{tw}x{th}", "persistent": self.form[3],
-                                "emitters_per_step": 2 if self.form[4] else 1,
-                                "autotune_ms_per_form": [round(x, 4) for x in self.autotune_ms]},
-                "cuda_graph": True, "mean_emitters_per_frame": self.n_emitters / self.mv.frames,
-                "max_emitters_per_frame": int(self.frames["em_count"].max())}
+        d = super().config_extra()
+        d["cuda_graph"] = True
+        return d
 
     cpu_sample = ("the whole 1024-frame movie per step: per frame the reference's RenderPhotonImage for channel 0, "
                   "then for channel 1 accumulating onto it (each with its own kernel), then ApplyNoiseChain; frames in "
@@ -618,6 +627,8 @@ def run_ours(args):
     torch.cuda.synchronize()
     barrier(world)
     launches0 = eng.launch_count
+    if hasattr(w, "timing"):
+        w.timing(True)
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
         barrier(world)
@@ -634,6 +645,9 @@ def run_ours(args):
     step_ms = [s.elapsed_time(e) for s, e in zip(start, stop)]
     ms = max_over_ranks(statistics.mean(step_ms), world)
     value = world * w.frames_per_step / (ms / 1e3)
+    dom = w.dominant() if hasattr(w, "dominant") else None
+    if hasattr(w, "timing"):
+        w.timing(False)
     # end to end through the C ABI with host buffers
     for _ in range(max(1, args.warmup)):
         w.e2e_step()
@@ -644,8 +658,8 @@ def run_ours(args):
     e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps, world)
     h2d, d2h = w.e2e_bytes()
     hbm, bf16, peak_kind = measured_peaks()
-    if hasattr(w, "dominant"):
-        kname, kbytes, kms, breakdown = w.dominant()
+    if dom is not None:
+        kname, kbytes, kms, breakdown = dom
     else:
         kname, kbytes, kms, breakdown = w.kernel_name(), w.alg_bytes_per_launch(), statistics.mean(step_ms), None
     tensor = getattr(w, "roofline_kind", "hbm") == "tensor"

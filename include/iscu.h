@@ -270,6 +270,12 @@ int iscu_render_frames(iscu_ctx* ctx, const iscu_emitter* emitters, uint32_t n_e
  * the same tile and scheduling. Every form gives the same bits. */
 #define ISCU_RENDER_CONFIGS 18
 int iscu_render_set_config(iscu_ctx* ctx, int32_t config);
+/* Pass timing of the renders that follow (CUDA events on the context's stream; not inside a graph capture):
+ * iscu_render_pass_times gives the mean milliseconds per render of grouping (setup, group offsets, lists),
+ * contributions, and the tile pass (splat or gather + noise; a one-pass form's whole render), and how many renders were
+ * timed. set_timing restarts the count. */
+int iscu_render_set_timing(iscu_ctx* ctx, int32_t on);
+int iscu_render_pass_times(iscu_ctx* ctx, float* ms3, uint32_t* calls);
 /* The most device bytes the two-pass forms' contributions may take (0: a quarter of the device's memory). */
 int iscu_render_set_contrib_limit(iscu_ctx* ctx, uint64_t bytes);
 int iscu_render_get_config(iscu_ctx* ctx, int32_t* config, int32_t* tile_w, int32_t* tile_h, int32_t* persistent,
@@ -336,6 +342,33 @@ int iscu_collect_emitters(iscu_ctx* ctx, int32_t slot, const iscu_blink_event* e
                           const double* drift_y_px, const double* global_z_offset_um, const double* bg_scale,
                           const float* illum, double min_photons, iscu_emitter* out, uint32_t max_out,
                           iscu_frame* frames_out, uint32_t* n_out, int64_t* n_clamped);
+
+/* The same on the device (no reference counterpart: the reference collects on the CPU): events_dev (n_events),
+ * bucket_index_dev (nullable) and bucket_start_dev (n_frames + 1) as above, the per-frame arrays and illum_dev
+ * (width*height of the context's frame) device pointers or NULL. Writes out_dev (at most max_out records),
+ * frames_out_dev (n_frames) and *n_out_dev = the records kept (more than max_out: the batch did not fit);
+ * *n_clamped_dev (nullable, zero it first) += the emitters whose z was clamped. Events whose slot holds no kernel stack
+ * are dropped (the host form fails on them). Needs iscu_set_static (the frame size). Asynchronous. */
+int iscu_collect_emitters_dev(iscu_ctx* ctx, int32_t slot, const iscu_blink_event* events_dev, uint32_t n_events,
+                              const uint32_t* bucket_index_dev, const uint32_t* bucket_start_dev, int64_t frame0,
+                              uint32_t n_frames, double pixel_size_nm, double photons_per_blink,
+                              const double* drift_x_px_dev, const double* drift_y_px_dev,
+                              const double* global_z_offset_um_dev, const double* bg_scale_dev, const float* illum_dev,
+                              double min_photons, iscu_emitter* out_dev, uint32_t max_out,
+                              iscu_frame* frames_out_dev, uint32_t* n_out_dev, int64_t* n_clamped_dev);
+
+/* Host blink events to host frames in one call (the movie engine's frame loop for one dye group batch,
+ * ScopeMovie.cpp:7059-7110: CollectFrameEmitters + RenderPhotonImage + ApplyNoiseChain per frame): the events, bucket
+ * arrays and per-frame arrays (as iscu_collect_emitters; use_illum: the context's illumination field weights the
+ * emitters) go to the device, are collected and rendered there, and photons (nullable, n_frames*w*h floats) and adu
+ * (n_frames*w*h) come back. *n_emitters (nullable) = the emitters splatted; *n_clamped (nullable) += clamped z
+ * planes. Page-locked host buffers make the copies direct. */
+int iscu_render_events(iscu_ctx* ctx, int32_t slot, const iscu_blink_event* events, uint32_t n_events,
+                       const uint32_t* bucket_index, const uint32_t* bucket_start, int64_t frame0, uint32_t n_frames,
+                       double pixel_size_nm, double photons_per_blink, const double* drift_x_px,
+                       const double* drift_y_px, const double* global_z_offset_um, const double* bg_scale,
+                       int32_t use_illum, double min_photons, const iscu_camera* cam, uint32_t seed, float* photons,
+                       uint16_t* adu, uint32_t* n_emitters, int64_t* n_clamped);
 
 /* ---------------------------------------------------------------- widefield ----------------------------------- */
 

@@ -128,7 +128,15 @@ SIGNATURES = {
     "iscu_render_frames_dev": (C.c_int, [vp, vp, C.c_uint32, vp, C.c_uint32, C.POINTER(Camera), C.c_uint32, vp,
                                          vp]),
     "iscu_render_frames": (C.c_int, [vp, vp, C.c_uint32, vp, C.c_uint32, C.POINTER(Camera), C.c_uint32, vp, vp]),
+    "iscu_collect_emitters_dev": (C.c_int, [vp, C.c_int32, vp, C.c_uint32, vp, vp, C.c_int64, C.c_uint32,
+                                            C.c_double, C.c_double, vp, vp, vp, vp, vp, C.c_double, vp, C.c_uint32,
+                                            vp, vp, vp]),
+    "iscu_render_events": (C.c_int, [vp, C.c_int32, vp, C.c_uint32, vp, vp, C.c_int64, C.c_uint32, C.c_double,
+                                     C.c_double, vp, vp, vp, vp, C.c_int32, C.c_double, C.POINTER(Camera),
+                                     C.c_uint32, vp, vp, vp, vp]),
     "iscu_render_set_config": (C.c_int, [vp, C.c_int32]),
+    "iscu_render_set_timing": (C.c_int, [vp, C.c_int32]),
+    "iscu_render_pass_times": (C.c_int, [vp, f32p, u32p]),
     "iscu_render_set_contrib_limit": (C.c_int, [vp, C.c_uint64]),
     "iscu_render_get_config": (C.c_int, [vp, i32p, i32p, i32p, i32p, i32p]),
     "iscu_render_autotune": (C.c_int, [vp, vp, C.c_uint32, vp, C.c_uint32, C.POINTER(Camera), C.c_uint32, vp,

@@ -26,6 +26,7 @@ UNITS = {
     "splat_noise.cu": ["--fmad=false"],
     "render.cu": ["--fmad=false"],
     "render_contrib.cu": ["--fmad=false"],
+    "collect.cu": ["--fmad=false"],
     "psf.cu": [],
     "psf_tc.cu": [],
     "psf_noalloc.cu": [],

@@ -247,6 +247,8 @@ void iscu_destroy(iscu_ctx* ctx)
       return;
    cudaSetDevice(ctx->device);
    cudaStreamSynchronize(ctx->stream);
+   for (cudaEvent_t e : ctx->renderMarks)
+      cudaEventDestroy(e);
    cudaStream_t s = ctx->stream;
    delete ctx;
    cudaStreamDestroy(s);

@@ -36,6 +36,14 @@ __device__ __forceinline__ void Pcg4d(uint32_t& a, uint32_t& b, uint32_t& c, uin
    d += b * c;
 }
 
+// The stream's uniform of word x: ((x >> 9) + 0.5) * 2^-23 = v * 2^-24 with v = (x >> 8) | 1, odd and below 2^24.
+// Formed exactly without an integer conversion: the double with exponent 2^28 and low word v is 2^28 + v * 2^-24,
+// and taking 2^28 away leaves v * 2^-24 (exact: the result is representable).
+__device__ __forceinline__ double UniformOf(uint32_t x)
+{
+   return __hiloint2double(0x41B00000, static_cast<int>((x >> 8) | 1u)) - 268435456.0;
+}
+
 // One frame's uniform source; Pixel(p) rewinds it to pixel p's stream. The four words of the current hash are
 // consumed in order by shifting, which keeps them in registers.
 struct CounterRng
@@ -72,7 +80,15 @@ struct CounterRng
       q1 = q2;
       q2 = q3;
       ++k;
-      return (static_cast<double>(x >> 9) + 0.5) * 1.1920928955078125e-7;
+      return UniformOf(x);
+   }
+   // After a hash drawn outside Uniform() of which `used` words (1..3) were consumed: the rest stays queued.
+   __device__ __forceinline__ void Rest(uint32_t r0, uint32_t r1, uint32_t r2, int used)
+   {
+      q0 = r0;
+      q1 = r1;
+      q2 = r2;
+      k = used;
    }
 };
 
@@ -97,12 +113,49 @@ __device__ __forceinline__ double CounterPoisson(double l, CounterRng& u)
    const double L = exp(-l);
    int k = 0;
    double p = 1.0;
-   do
+   if (u.k < 4)
    {
-      ++k;
-      p *= u.Uniform();
-   } while (p > L && k < 1000);
-   return static_cast<double>(k - 1);
+      // mid-hash (not the case for a pixel's first draw): one uniform at a time
+      do
+      {
+         ++k;
+         p *= u.Uniform();
+      } while (p > L && k < 1000);
+      return static_cast<double>(k - 1);
+   }
+   // At a hash boundary: do { ++k; p *= uniform; } while (p > L && k < 1000), a hash (four uniforms) per block;
+   // block b's fourth factor is the 4b + 4-th, so only block 249 ends at k = 1000.
+   for (int blk = 0;; ++blk)
+   {
+      uint32_t a = u.seed, b = u.frame, c = u.pix, d = u.ctr;
+      Pcg4d(a, b, c, d);
+      ++u.ctr;
+      const double u0 = UniformOf(a), u1 = UniformOf(b), u2 = UniformOf(c), u3 = UniformOf(d);
+      p *= u0;
+      if (!(p > L))
+      {
+         u.Rest(b, c, d, 1);
+         return static_cast<double>(4 * blk);
+      }
+      p *= u1;
+      if (!(p > L))
+      {
+         u.Rest(c, d, 0u, 2);
+         return static_cast<double>(4 * blk + 1);
+      }
+      p *= u2;
+      if (!(p > L))
+      {
+         u.Rest(d, 0u, 0u, 3);
+         return static_cast<double>(4 * blk + 2);
+      }
+      p *= u3;
+      if (!(p > L) || blk == 249)
+      {
+         u.k = 4;
+         return static_cast<double>(4 * blk + 3);
+      }
+   }
 }
 
 // Marsaglia-Tsang Gamma(k, 1), 1000-iteration cap (SMLMCounterRng.h:120-136).

@@ -194,6 +194,11 @@ struct iscu_ctx
    int renderConfig = 0;           // render kernel form (iscu_render_set_config)
    iscu::DevBuf dOrder;            // persistent render: frame order + work counter
    iscu::ContribScratch contrib;   // two-pass render scratch
+   // render pass timing (iscu_render_set_timing): 4 events per timed call (start, after grouping, after
+   // contributions, end)
+   bool renderTiming = false;
+   std::vector<cudaEvent_t> renderMarks;
+   size_t renderCalls = 0;
    size_t contribLimit = 0;        // most bytes the two-pass render's contributions may take (0: a quarter of HBM)
    iscu::KernelSlot kernels[ISCU_MAX_KERNELS];
    // camera statics
@@ -205,6 +210,7 @@ struct iscu_ctx
    std::vector<float> illumHost;   // the illumination field, for host-side emitter collection
    // staging for the host-pointer entry points
    iscu::DevBuf dEmitters, dFrames, dPhotons, dAdu, dExtras, dScratch;
+   iscu::DevBuf dEvents, dBuckets, dCounts, dCollect;   // device emitter collection
    iscu::PinnedBuf hIn, hOut;
    iscu::StaticView Static() const
    {
@@ -230,6 +236,15 @@ int LaunchCounterUniforms(iscu_ctx* ctx, uint32_t seed, uint32_t frame, uint32_t
                           uint32_t perPixel, double* out);
 int LaunchNoiseFrames(iscu_ctx* ctx, const float* photons, uint32_t nFrames, const uint32_t* frames,
                       const CameraView& cam, uint32_t seed, uint16_t* adu);
+// CollectFrameEmitters for a batch on the device (collect.cu): out gets the kept emitters (at most maxOut written),
+// frames the table, *nOut the count kept (may pass maxOut), *nClamped += the clamped z planes (nullable).
+int LaunchCollect(iscu_ctx* ctx, int32_t slot, const iscu_blink_event* events, uint32_t nEvents,
+                  const uint32_t* bucketIndex, const uint32_t* bucketStart, int64_t frame0, uint32_t nFrames,
+                  double pixelNm, double perBlink, const double* driftX, const double* driftY, const double* globalZ,
+                  const double* bgScale, const float* illum, double minPhotons, iscu_emitter* out, uint32_t maxOut,
+                  iscu_frame* frames, uint32_t* nOut, int64_t* nClamped);
+// The render's timing marks of the current call (nullptr when timing is off or the stream is capturing): 4 events.
+cudaEvent_t* RenderMarks(iscu_ctx* ctx);
 // Emitter runs of the frames beyond nEmitters are cut at nEmitters.
 int LaunchRenderFrames(iscu_ctx* ctx, const iscu_emitter* ems, uint32_t nEmitters, const iscu_frame* frames,
                        uint32_t nFrames, const CameraView* cam, uint32_t seed, float* photons, uint16_t* adu);

@@ -416,6 +416,10 @@ int LaunchConfig(iscu_ctx* ctx, int config, const iscu_emitter* ems, uint32_t nE
       ClearError();
       config -= 12;
    }
+   cudaEvent_t* marks = RenderMarks(ctx);
+   if (marks)
+      for (int m = 0; m < 3; ++m)
+         ISCU_CK(cudaEventRecord(marks[m], ctx->stream));
    RenderArgs a;
    a.ems = ems;
    a.nEm = nEm;
@@ -452,6 +456,8 @@ int LaunchConfig(iscu_ctx* ctx, int config, const iscu_emitter* ems, uint32_t nE
       fn<<<grid, kThreads, 0, ctx->stream>>>(a);
    }
    ISCU_CK_LAUNCH(ctx, "RenderTilesKernel");
+   if (marks)
+      ISCU_CK(cudaEventRecord(marks[3], ctx->stream));
    return ISCU_OK;
 }
 
@@ -483,6 +489,24 @@ int LaunchPhaseSplit(iscu_ctx* ctx, const float* sums, int nz, int bw, int os, i
    PhaseSplitKernel<<<grid, 128, 0, ctx->stream>>>(sums, bw, os, padLo, nb, out);
    ISCU_CK_LAUNCH(ctx, "PhaseSplitKernel");
    return ISCU_OK;
+}
+
+cudaEvent_t* RenderMarks(iscu_ctx* ctx)
+{
+   if (!ctx->renderTiming)
+      return nullptr;
+   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+   if (cudaStreamIsCapturing(ctx->stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+      return nullptr;
+   const size_t need = 4 * (ctx->renderCalls + 1);
+   while (ctx->renderMarks.size() < need)
+   {
+      cudaEvent_t e = nullptr;
+      if (cudaEventCreate(&e) != cudaSuccess)
+         return nullptr;
+      ctx->renderMarks.push_back(e);
+   }
+   return ctx->renderMarks.data() + 4 * ctx->renderCalls++;
 }
 
 int LaunchRenderFrames(iscu_ctx* ctx, const iscu_emitter* ems, uint32_t nEmitters, const iscu_frame* frames,
@@ -517,6 +541,44 @@ int iscu_render_set_contrib_limit(iscu_ctx* ctx, uint64_t bytes)
       return Fail(ISCU_ERR_ARG, "null context");
    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
    ctx->contribLimit = static_cast<size_t>(bytes);
+   return ISCU_OK;
+}
+
+int iscu_render_set_timing(iscu_ctx* ctx, int32_t on)
+{
+   if (!ctx)
+      return Fail(ISCU_ERR_ARG, "null context");
+   std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+   ClearError();
+   ISCU_CK(cudaStreamSynchronize(ctx->stream));
+   ctx->renderTiming = on != 0;
+   ctx->renderCalls = 0;
+   return ISCU_OK;
+}
+
+int iscu_render_pass_times(iscu_ctx* ctx, float* ms3, uint32_t* calls)
+{
+   if (!ctx || !ms3)
+      return Fail(ISCU_ERR_ARG, "null argument");
+   std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+   ClearError();
+   if (!ctx->renderTiming)
+      return Fail(ISCU_ERR_STATE, "render timing is off (iscu_render_set_timing)");
+   ms3[0] = ms3[1] = ms3[2] = 0.0f;
+   if (calls)
+      *calls = static_cast<uint32_t>(ctx->renderCalls);
+   if (ctx->renderCalls == 0)
+      return ISCU_OK;
+   ISCU_CK(cudaEventSynchronize(ctx->renderMarks[4 * ctx->renderCalls - 1]));
+   for (size_t c = 0; c < ctx->renderCalls; ++c)
+      for (int k = 0; k < 3; ++k)
+      {
+         float t = 0.0f;
+         ISCU_CK(cudaEventElapsedTime(&t, ctx->renderMarks[4 * c + k], ctx->renderMarks[4 * c + k + 1]));
+         ms3[k] += t;
+      }
+   for (int k = 0; k < 3; ++k)
+      ms3[k] /= static_cast<float>(ctx->renderCalls);
    return ISCU_OK;
 }
 

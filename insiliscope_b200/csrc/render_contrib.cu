@@ -763,6 +763,9 @@ int LaunchContribRender(iscu_ctx* ctx, int tileConfig, const iscu_emitter* ems, 
    const KeyMap& km = G.km;
    const int nKeys = G.nKeys, ct = G.ct;
    const size_t S = G.S;
+   cudaEvent_t* marks = RenderMarks(ctx);
+   if (marks)
+      ISCU_CK(cudaEventRecord(marks[0], ctx->stream));
    uint32_t* count = sc.keys.as<uint32_t>();
    uint32_t* start = count + nKeys;
    uint32_t* cursor = start + nKeys;
@@ -786,6 +789,8 @@ int LaunchContribRender(iscu_ctx* ctx, int tileConfig, const iscu_emitter* ems, 
          ISCU_CK_LAUNCH(ctx, "ContribScatterKernel");
          ContribItemKeysKernel<<<(nKeys + 255) / 256, 256, 0, ctx->stream>>>(nKeys, itemStart, itemKey);
          ISCU_CK_LAUNCH(ctx, "ContribItemKeysKernel");
+         if (marks)
+            ISCU_CK(cudaEventRecord(marks[1], ctx->stream));
          ContribArgs ca{km, K, count, start, itemStart, itemKey, sc.list.as<CStage>(), sc.ctr.as<uint32_t>(),
                         sc.contrib.as<float>(), static_cast<uint32_t>(S)};
          int perSm = 0;
@@ -793,6 +798,12 @@ int LaunchContribRender(iscu_ctx* ctx, int tileConfig, const iscu_emitter* ems, 
          ContribKernel<<<std::max(1, perSm) * ctx->smCount, ct + 32, 0, ctx->stream>>>(ca);
          ISCU_CK_LAUNCH(ctx, "ContribKernel");
       }
+   }
+   if (marks)
+   {
+      if (nEm == 0 || nKeys == 0)
+         ISCU_CK(cudaEventRecord(marks[1], ctx->stream));
+      ISCU_CK(cudaEventRecord(marks[2], ctx->stream));
    }
    GatherArgs ga;
    ga.frames = frames;
@@ -834,6 +845,8 @@ int LaunchContribRender(iscu_ctx* ctx, int tileConfig, const iscu_emitter* ems, 
       fn<<<grid, kGT, 0, ctx->stream>>>(ga);
    }
    ISCU_CK_LAUNCH(ctx, "GatherTilesKernel");
+   if (marks)
+      ISCU_CK(cudaEventRecord(marks[3], ctx->stream));
    return ISCU_OK;
 }
 

@@ -323,6 +323,48 @@ class Engine:
                                               _ptr(adu_dev)))
         self._after(sync)
 
+    def collect_emitters_dev(self, slot, events_dev, n_events, bucket_start_dev, n_frames, frame0, pixel_size_nm,
+                             photons_per_blink, out_dev, frames_out_dev, n_out_dev, bucket_index_dev=None,
+                             drift_x_px_dev=None, drift_y_px_dev=None, global_z_offset_um_dev=None,
+                             bg_scale_dev=None, illum_dev=None, min_photons=0.0, n_clamped_dev=None, sync=True):
+        """iscu_collect_emitters_dev on CUDA tensors (events: uint8 view of BLINK_EVENT_DTYPE records; out: of
+        EMITTER_DTYPE records, its capacity the record count; frames_out: FRAME_DTYPE records; n_out: 1 uint32/int32)."""
+        self._before(sync)
+        check(self.lib.iscu_collect_emitters_dev(
+            self.h, int(slot), _ptr(events_dev), int(n_events), _ptr(bucket_index_dev), _ptr(bucket_start_dev),
+            int(frame0), int(n_frames), float(pixel_size_nm), float(photons_per_blink), _ptr(drift_x_px_dev),
+            _ptr(drift_y_px_dev), _ptr(global_z_offset_um_dev), _ptr(bg_scale_dev), _ptr(illum_dev),
+            float(min_photons), _ptr(out_dev), _n_records(out_dev), _ptr(frames_out_dev), _ptr(n_out_dev),
+            _ptr(n_clamped_dev)))
+        self._after(sync)
+
+    def render_events(self, slot, events, bucket_start, frame0, pixel_size_nm, photons_per_blink,
+                      camera: CameraParams | None, seed, bucket_index=None, drift_x_px=None, drift_y_px=None,
+                      global_z_offset_um=None, bg_scale=None, use_illum=False, min_photons=0.0, want_photons=False,
+                      adu_out=None, photons_out=None):
+        """Host blink events -> host frames in one C-ABI call (iscu_render_events): collection, render and noise on
+        the device. Returns (photons | None, adu | None, n_emitters). Pass page-locked adu_out / photons_out (and
+        events) for direct copies."""
+        events = np.ascontiguousarray(events, dtype=BLINK_EVENT_DTYPE)
+        bs = np.ascontiguousarray(bucket_start, dtype=np.uint32)
+        nf = len(bs) - 1
+        bi = None if bucket_index is None else np.ascontiguousarray(bucket_index, dtype=np.uint32)
+        f64 = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+        dx, dy, gz, sc = f64(drift_x_px), f64(drift_y_px), f64(global_z_offset_um), f64(bg_scale)
+        shape = (nf, self.height, self.width)
+        adu = None
+        if camera is not None:
+            adu = adu_out if adu_out is not None else np.empty(shape, np.uint16)
+        ph = photons_out if photons_out is not None else (np.empty(shape, np.float32) if want_photons else None)
+        cam = camera.c() if camera is not None else None
+        n = C.c_uint32()
+        check(self.lib.iscu_render_events(self.h, int(slot), _ptr(events), len(events), _ptr(bi), _ptr(bs),
+                                          int(frame0), nf, float(pixel_size_nm), float(photons_per_blink), _ptr(dx),
+                                          _ptr(dy), _ptr(gz), _ptr(sc), int(bool(use_illum)), float(min_photons),
+                                          C.byref(cam) if cam is not None else None, int(seed), _ptr(ph), _ptr(adu),
+                                          C.byref(n), None))
+        return ph, adu, n.value
+
     RENDER_CONFIGS = 18
 
     def render_config(self):
@@ -330,10 +372,22 @@ class Engine:
         one or two emitters per step, 2: two passes."""
         v = [C.c_int32() for _ in range(5)]
         check(self.lib.iscu_render_get_config(self.h, *[C.byref(x) for x in v]))
-        return v[0].value, v[1].value, v[2].value, bool(v[3].value), bool(v[4].value)
+        return v[0].value, v[1].value, v[2].value, bool(v[3].value), v[4].value
 
     def set_render_config(self, config):
         check(self.lib.iscu_render_set_config(self.h, int(config)))
+
+    RENDER_PASSES = ("grouping", "contributions", "tiles")
+
+    def set_render_timing(self, on):
+        check(self.lib.iscu_render_set_timing(self.h, int(bool(on))))
+
+    def render_pass_times(self):
+        """Mean ms per render since set_render_timing(True): {grouping, contributions, tiles}, and the call count."""
+        ms = (C.c_float * 3)()
+        n = C.c_uint32()
+        check(self.lib.iscu_render_pass_times(self.h, ms, C.byref(n)))
+        return dict(zip(self.RENDER_PASSES, list(ms))), n.value
 
     def set_contrib_limit(self, nbytes):
         """The most device bytes the two-pass render forms' contributions may take (0: a quarter of the device)."""
