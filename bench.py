@@ -98,6 +98,15 @@ def measured_peaks():
     return 6650.0, 1590.0, "fallback"
 
 
+# DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the dominant kernels, from one ncu
+# capture each; the summaries with their commands are the named files.
+NCU_TRAFFIC = {
+    ("smlm", "GatherTilesKernel"): (139518208, "profiles/GatherTilesKernel_smlm_dstorm.md"),
+    ("smlm", "ContribKernel"): (93568768, "profiles/ContribKernel_smlm_dstorm.md"),
+    ("psflib", "CztTf32x3Kernel"): (71094272, "profiles/CztTf32x3Kernel_psf_library.md"),
+}
+
+
 # ----------------------------------------------------------------------------------------------------- dist
 def dist_setup(n_gpus):
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -139,7 +148,7 @@ class SmlmWorkload:
         self.frame0 = rank * 200
 
     # -------------------------------------------------- ours
-    def setup(self, device: int):
+    def setup(self, device: int, form=None):
         import torch
         from insiliscope_b200 import CZT_FP32, Engine, generate_camera_maps
         mv = self.mv
@@ -163,6 +172,9 @@ class SmlmWorkload:
         t0 = time.perf_counter()
         self.autotune_ms = eng.render_autotune(self.d_em, self.d_fr, mv.frames, mv.camera, mv.noise_seed, self.d_adu)
         self.autotune_wall_ms = (time.perf_counter() - t0) * 1e3
+        self.autotuned = eng.render_config()[0]
+        if form is not None:
+            eng.set_render_config(form)   # a fixed form (profiling runs), the autotuner's table still reported
         self.form = eng.render_config()
         # page-locked host buffers of the end-to-end call: the events and buckets in, the frames out
         pin = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8)).pin_memory().numpy().view(a.dtype)
@@ -202,8 +214,8 @@ class SmlmWorkload:
         return kernel, self.pass_bytes(name), ms[name], {k: round(v, 4) for k, v in ms.items()}
 
     def pass_bytes(self, name):
-        """Algorithmic HBM bytes of a render pass. Tiles: the ADU written (2 B/px), the three float camera maps
-        read (12 B/px), the frame table, each emitter's setup record (16 B), and every (emitter, square pixel)
+        """Algorithmic HBM bytes of a render pass. Tiles: the ADU written (2 B/px per frame), the three float camera
+        maps read once (12 B/px), the frame table, each emitter's setup record (16 B), and every (emitter, square pixel)
         contribution read once (4 B; the two-pass forms) or the emitter records (32 B; one pass). Contributions: each
         emitter's staged record (88 B) read and its square's contributions written (4 B/px). Grouping: the emitter
         records read (32 B) and their setup and staged records written (96 + 16 + 88 B)."""
@@ -216,7 +228,7 @@ class SmlmWorkload:
         sq = sum(side(s) ** 2 for s in self.slots_used()) / len(self.slots_used())
         if name == "tiles":
             per_em = 16 + 4 * sq if two else 32
-            return mv.frames * (px * 14 + 24) + self.n_emitters * per_em
+            return mv.frames * (px * 2 + 24) + px * 12 + self.n_emitters * per_em
         if name == "contributions":
             return self.n_emitters * (88 + 4 * sq)
         return self.n_emitters * (32 + 96 + 16 + 88)
@@ -230,7 +242,7 @@ class SmlmWorkload:
     def config_extra(self):
         tw, th = self.form[1], self.form[2]
         return {"render_form": {"config": self.form[0], "tile": f"{tw}x{th}", "persistent": self.form[3],
-                                "passes": 2 if self.form[4] == 2 else 1,
+                                "passes": 2 if self.form[4] == 2 else 1, "autotuned_config": self.autotuned,
                                 "autotune_ms_per_form": [round(x, 4) for x in self.autotune_ms]},
                 "mean_emitters_per_frame": self.n_emitters / self.mv.frames,
                 "max_emitters_per_frame": int(self.frames["em_count"].max())}
@@ -291,9 +303,9 @@ class TwoColourWorkload(SmlmWorkload):
     def psfs(self):
         return self.mv.psfs
 
-    def setup(self, device: int):
+    def setup(self, device: int, form=None):
         from insiliscope_b200 import RenderGraph
-        super().setup(device)
+        super().setup(device, form)
         mv = self.mv
         self.graph = RenderGraph(self.eng, self.d_em, self.d_fr, mv.frames, mv.camera, mv.noise_seed, None,
                                  self.d_adu)
@@ -614,7 +626,10 @@ def run_ours(args):
     from insiliscope_b200.build import build_library
     build_library()
     w = WORKLOADS[args.workload](rank)
-    w.setup(local)
+    if args.form is not None and isinstance(w, SmlmWorkload):
+        w.setup(local, form=args.form)
+    else:
+        w.setup(local)
     eng = w.eng
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")   # 256 MB > L2 (126 MB)
     start = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
@@ -677,7 +692,7 @@ def run_ours(args):
                     "timing": "host wall clock per step (blocking C-ABI calls), max over ranks"},
             "roofline": {"bound": "tensor" if tensor else "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s" if tensor else "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": None, ("alg_flops_per_launch" if tensor else "alg_bytes_per_launch"): kbytes,
+                         "traffic": NCU_TRAFFIC.get((args.workload, kname), (None,))[0], ("alg_flops_per_launch" if tensor else "alg_bytes_per_launch"): kbytes,
                          "launch_ms": kms},
             "gpu_launches": launches, "clocks": clk.summary()}
     if breakdown and tensor:
@@ -708,6 +723,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="smlm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--form", type=int, default=None,
+                    help="SMLM workloads: render form 0..17 instead of the autotuner's choice (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
