@@ -576,8 +576,108 @@ class PsfLibraryWorkload:
         return time.perf_counter() - t0
 
 
+class NllGradWorkload:
+    """The Poisson-likelihood gradient: 256 frames x 1,000 emitters, each in a 32 x 32 px ROI (64 x 64 sub-pixel
+    samples from a 32 x 32 pupil), per emitter x, y, z, N, one background per frame, 21 Zernike coefficients. One step
+    = the NLL and its adjoint gradient (the field recomputed per emitter) for all 256 frames; the data (Poisson counts
+    drawn by the engine's noise chain) stay resident, the parameters come in and the gradients go out."""
+    name = ("poisson NLL + adjoint gradient, 256 frames x 1000 emitters, 32x32 px ROIs (64^2 samples, 32^2 pupil), "
+            "x/y/z/N, 256 backgrounds, 21 Zernike (Noll 4-24)")
+    metric = "frames/s"
+    dtype = "f32"
+    cpu_kind = "port"
+    frames_per_step_cpu = 2
+    cpu_sample = ("2 of the 256 frames (2,000 ROIs): the float64 adjoint of oracle/nll_oracle.py (numpy, batched "
+                  "matmuls), data drawn by numpy's Poisson at the float64 expectation")
+
+    def __init__(self, rank: int):
+        from insiliscope_b200.workloads import nll_rois
+        self.prob = nll_rois(seed=42 + rank)
+
+    def setup(self, device: int):
+        import torch
+        from insiliscope_b200 import Engine
+        from insiliscope_b200.nll import NllModel
+        from insiliscope_b200.workloads import nll_counts
+        P = self.prob
+        self.eng = eng = Engine(device)
+        t0 = time.perf_counter()
+        self.model = NllModel(eng, P.spec)
+        self.psf_build_ms = (time.perf_counter() - t0) * 1e3
+        dev = f"cuda:{device}"
+        self.counts = nll_counts(eng, self.model, P, device=dev)
+        self.d_params = torch.from_numpy(P.params).to(dev)
+        self.d_frame = torch.from_numpy(P.frame).to(dev)
+        self.d_bg = torch.from_numpy(P.bg).to(dev)
+        self.zern = np.ascontiguousarray(P.zern, np.float64)
+        n, F = len(P.frame), len(P.bg)
+        self.d_nll = torch.zeros(1, dtype=torch.float64, device=dev)
+        self.d_err = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.g_params = torch.empty((n, 4), dtype=torch.float32, device=dev)
+        self.g_bg = torch.empty(F, dtype=torch.float64, device=dev)
+        self.g_zern = torch.empty(len(self.zern), dtype=torch.float64, device=dev)
+        pin = lambda a: torch.from_numpy(a).pin_memory()
+        self.h_params, self.h_bg = pin(P.params), pin(P.bg)
+        self.h_gp = torch.empty((n, 4), dtype=torch.float32).pin_memory()
+        self.h_gb = torch.empty(F, dtype=torch.float64).pin_memory()
+        self.stream = eng.torch_stream()
+        self.frames_per_step = F
+        self.n_emitters = n
+
+    def device_step(self):
+        self.model.run_dev(self.d_params, self.d_frame, self.d_bg, self.zern, self.counts, self.d_nll, self.d_err,
+                           self.g_params, self.g_bg, self.g_zern, sync=False)
+
+    def e2e_step(self):
+        """Page-locked parameters in, the NLL and every gradient out, through the library's model."""
+        import torch
+        # the copies on torch's own stream (ordered with the library's by the synchronizing calls)
+        self.d_params.copy_(self.h_params, non_blocking=True)
+        self.d_bg.copy_(self.h_bg, non_blocking=True)
+        self.model.run_dev(self.d_params, self.d_frame, self.d_bg, self.zern, self.counts, self.d_nll, self.d_err,
+                           self.g_params, self.g_bg, self.g_zern, sync=True)
+        self.h_gp.copy_(self.g_params, non_blocking=True)
+        self.h_gb.copy_(self.g_bg, non_blocking=True)
+        torch.cuda.synchronize()
+        return float(self.d_nll.item()), self.g_zern.cpu().numpy()
+
+    def e2e_bytes(self):
+        return self.h_params.numel() * 4 + self.h_bg.numel() * 4 + self.zern.nbytes, \
+            self.h_gp.numel() * 4 + self.h_gb.numel() * 8 + self.zern.nbytes + 8
+
+    def alg_bytes_per_launch(self):
+        # the counts read once (4 B per ROI pixel), per emitter its parameters in and gradients out (32 B)
+        R = self.prob.spec.roi
+        return self.n_emitters * (R * R * 4 + 32) + self.frames_per_step * 12
+
+    def kernel_name(self):
+        return "NllKernel"
+
+    def cpu_cores(self):
+        return os.cpu_count() or 1
+
+    def reference_setup(self, threads=0):
+        from oracle.nll_oracle import NllSpec, expected, tables
+        P = self.prob
+        self.ospec = NllSpec()
+        self.t = tables(self.ospec)
+        sel = P.frame < 2
+        self.s_params = P.params[sel].astype(np.float64)
+        self.s_frame = P.frame[sel]
+        self.s_bg = P.bg.astype(np.float64)[:2]
+        mu = expected(self.ospec, P.params_true[sel].astype(np.float64), self.s_frame,
+                      P.bg_true.astype(np.float64)[:2], P.zern_true, self.t)
+        self.s_counts = np.random.default_rng(P.noise_seed).poisson(mu).astype(np.float64)
+
+    def reference_step(self):
+        from oracle.nll_oracle import gradient
+        t0 = time.perf_counter()
+        gradient(self.ospec, self.s_params, self.s_frame, self.s_bg, self.prob.zern, self.s_counts, self.t)
+        return time.perf_counter() - t0
+
+
 WORKLOADS = {"smlm": SmlmWorkload, "widefield": WidefieldWorkload, "psflib": PsfLibraryWorkload,
-             "two-colour": TwoColourWorkload}
+             "two-colour": TwoColourWorkload, "nll-grad": NllGradWorkload}
 
 
 # ----------------------------------------------------------------------------------------------------- arms
@@ -708,6 +808,7 @@ def run_ours(args):
         line["cpu_baseline"] = cpu_baseline(w)
     if rank == 0:
         print(json.dumps(line))
+    torch.cuda.synchronize()
     eng.close()
     if world > 1:
         import torch.distributed as dist

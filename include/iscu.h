@@ -370,6 +370,43 @@ int iscu_render_events(iscu_ctx* ctx, int32_t slot, const iscu_blink_event* even
                        int32_t use_illum, double min_photons, const iscu_camera* cam, uint32_t seed, float* photons,
                        uint16_t* adu, uint32_t* n_emitters, int64_t* n_clamped);
 
+/* ---------------------------------------------------------------- Poisson-likelihood gradient ---------------- */
+
+/* The differentiable ROI model (no reference counterpart: the reference has no gradient): the Gibson-Lanni/Zernike
+ * pupil (ZernikePsf.cpp:188-248) at matched indices and depth 0, each emitter at a continuous defocus z (nm) and
+ * position (x, y) (ROI pixels), its field the separable DFT of the pupil to the ROI's os x os sub-pixel samples:
+ *   U = a exp(i (z kz + 2 pi sum_j c_j Z_j - p (kx x + ky y))),  E = A U A^T,  A[s][m] = exp(i k_m p (s + 0.5) / os)
+ *   mu = N kappa (sum of |E|^2 over a pixel's samples) + b_frame,   NLL = sum over ROI pixels of mu - k log mu
+ * with the pupil grid k_i = (i - M/2) dk, dk = 2 kMax / (M - 4) (ZernikePsf.cpp:192-193), Z_j Noll's orthonormal
+ * Zernike polynomials on rho = k / kMax (coefficients in waves rms), kappa = (p / os)^2 / (L^2 sum a), L = 2 pi / dk.
+ * This build takes a 32 x 32 pupil and roi * os = 64. */
+typedef struct iscu_nll_spec {
+   double wavelength_nm;
+   double na;
+   double n_imm;          /* immersion = sample index */
+   double pixel_nm;
+   int32_t roi;           /* ROI side in pixels */
+   int32_t os;            /* samples per pixel per axis */
+   int32_t pupil;         /* M */
+   int32_t n_zern;        /* <= 32 */
+   int32_t noll[32];      /* the Zernike modes' Noll indices */
+} iscu_nll_spec;
+
+typedef struct iscu_nll_model iscu_nll_model;
+int iscu_nll_model_create(iscu_ctx* ctx, const iscu_nll_spec* spec, iscu_nll_model** out);
+void iscu_nll_model_destroy(iscu_nll_model* model);
+int iscu_nll_model_info(iscu_nll_model* model, double* kappa, int32_t* n_zern);
+/* NLL of n_emitters ROIs (params_dev: n x (x, y, z, N) float; frame_dev: each ROI's frame < n_frames; bg_dev:
+ * n_frames float; zern: n_zern float64 host; counts_dev: n x roi x roi float) into *nll_dev (float64, device);
+ * mu_dev (nullable): the expected counts. With grad_params_dev (n x 4 float: dNLL/dx, /dy, /dz, /dN) the adjoint
+ * runs too (the field recomputed, no per-emitter PSF stored): grad_bg_dev (n_frames float64) and grad_zern_dev
+ * (n_zern float64) receive the rest. *err_dev (int32, device) = 1 when an emitter names a frame outside the batch.
+ * Asynchronous on the context's stream. */
+int iscu_nll_eval_dev(iscu_nll_model* model, uint32_t n_emitters, const float* params_dev, const int32_t* frame_dev,
+                      uint32_t n_frames, const float* bg_dev, const double* zern, const float* counts_dev,
+                      float* mu_dev, double* nll_dev, float* grad_params_dev, double* grad_bg_dev,
+                      double* grad_zern_dev, int32_t* err_dev);
+
 /* ---------------------------------------------------------------- widefield ----------------------------------- */
 
 /* Widefield mean-field 3D convolution: the dye density volume (nx x ny x nz float32, x fastest, photons per voxel

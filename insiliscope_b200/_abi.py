@@ -91,6 +91,12 @@ class BlinkEvent(C.Structure):
 
 
 # name -> (restype, argtypes); every function include/iscu.h declares.
+class NllSpec(C.Structure):
+    _fields_ = [("wavelength_nm", C.c_double), ("na", C.c_double), ("n_imm", C.c_double), ("pixel_nm", C.c_double),
+                ("roi", C.c_int32), ("os", C.c_int32), ("pupil", C.c_int32), ("n_zern", C.c_int32),
+                ("noll", C.c_int32 * 32)]
+
+
 SIGNATURES = {
     "iscu_last_error": (C.c_char_p, []),
     "iscu_abi_version": (C.c_int, []),
@@ -134,6 +140,10 @@ SIGNATURES = {
     "iscu_render_events": (C.c_int, [vp, C.c_int32, vp, C.c_uint32, vp, vp, C.c_int64, C.c_uint32, C.c_double,
                                      C.c_double, vp, vp, vp, vp, C.c_int32, C.c_double, C.POINTER(Camera),
                                      C.c_uint32, vp, vp, vp, vp]),
+    "iscu_nll_model_create": (C.c_int, [vp, C.POINTER(NllSpec), C.POINTER(vp)]),
+    "iscu_nll_model_destroy": (None, [vp]),
+    "iscu_nll_model_info": (C.c_int, [vp, f64p, i32p]),
+    "iscu_nll_eval_dev": (C.c_int, [vp, C.c_uint32, vp, vp, C.c_uint32, vp, f64p, vp, vp, vp, vp, vp, vp, vp]),
     "iscu_render_set_config": (C.c_int, [vp, C.c_int32]),
     "iscu_render_set_timing": (C.c_int, [vp, C.c_int32]),
     "iscu_render_pass_times": (C.c_int, [vp, f32p, u32p]),

@@ -27,6 +27,7 @@ UNITS = {
     "render.cu": ["--fmad=false"],
     "render_contrib.cu": ["--fmad=false"],
     "collect.cu": ["--fmad=false"],
+    "nll.cu": [],
     "psf.cu": [],
     "psf_tc.cu": [],
     "psf_noalloc.cu": [],

@@ -294,3 +294,61 @@ def psf_library(seed: int = 42, n_z: int = 64, wavelengths=(520.0, 580.0, 670.0,
     set_of = np.repeat(np.arange(len(sets), dtype=np.uint32), n_z)
     defocus = np.tile(z, len(sets)).astype(np.float64)
     return PsfLibrary(sets, set_of, defocus, size)
+
+
+@dataclass
+class NllProblem:
+    """ROIs for the Poisson-likelihood gradient: the truth the data are drawn at, and a perturbed point to
+    differentiate at."""
+    spec: object                # insiliscope_b200.nll.NllSpec
+    frame: np.ndarray           # (n,) int32
+    params_true: np.ndarray     # (n, 4) float32: x, y (ROI px), z (nm), N
+    bg_true: np.ndarray         # (F,) float32
+    zern_true: np.ndarray       # (J,) float64, waves rms
+    params: np.ndarray          # the evaluation point
+    bg: np.ndarray
+    zern: np.ndarray
+    noise_seed: int
+
+
+def nll_rois(seed: int = 42, frames: int = 256, per_frame: int = 1000, spec=None) -> NllProblem:
+    """The gradient config: 256 frames x 1,000 emitters, each in its own 32 x 32 px ROI (108 nm, NA 1.45, 670 nm):
+    x, y ~ U(14.5, 17.5) px, z ~ U(-500, 500) nm, N lognormal (median 2000, sigma_log 0.5), one background per frame
+    ~ U(5, 20) photons/px, 21 Zernike coefficients (Noll 4-24) ~ N(0, 0.03) waves rms. The evaluation point perturbs
+    the truth (x, y by N(0, 0.3) px, z by N(0, 50) nm, N by 10 %, backgrounds by 10 %, Zernike by N(0, 0.01)).
+    numpy PCG64 seeded with `seed`."""
+    from .nll import NllSpec
+    spec = spec or NllSpec()
+    rng = np.random.default_rng(seed)
+    n = frames * per_frame
+    frame = np.repeat(np.arange(frames, dtype=np.int32), per_frame)
+    c = spec.roi / 2.0
+    pt = np.column_stack([rng.uniform(c - 1.5, c + 1.5, n), rng.uniform(c - 1.5, c + 1.5, n),
+                          rng.uniform(-500.0, 500.0, n), 2000.0 * np.exp(0.5 * rng.standard_normal(n))])
+    bg = rng.uniform(5.0, 20.0, frames)
+    zt = rng.normal(0.0, 0.03, len(spec.noll))
+    p = pt + np.column_stack([rng.normal(0, 0.3, n), rng.normal(0, 0.3, n), rng.normal(0, 50.0, n),
+                              pt[:, 3] * rng.normal(0, 0.1, n)])
+    return NllProblem(spec, frame, pt.astype(np.float32), bg.astype(np.float32), zt, p.astype(np.float32),
+                      (bg * rng.uniform(0.9, 1.1, frames)).astype(np.float32), zt + rng.normal(0, 0.01, len(zt)),
+                      (seed ^ 0x9E3779B9) & 0xFFFFFFFF)
+
+
+def nll_counts(engine, model, prob: NllProblem, device="cuda"):
+    """The data: the expected counts at the truth (the gradient model's forward pass), then the engine's noise chain
+    as a photon counter (sCMOS, QE 1, gain 1 photon/ADU, no read noise, offset 0: ADU = the Poisson draw), keyed by
+    (noise seed, frame, pixel) with each frame's ROIs stacked into one roi x (per_frame roi) image."""
+    import torch
+    from .engine import CameraParams
+    pt = torch.from_numpy(prob.params_true).to(device)
+    fr = torch.from_numpy(prob.frame).to(device)
+    bg = torch.from_numpy(prob.bg_true).to(device)
+    counts0 = torch.zeros((len(prob.frame), prob.spec.roi, prob.spec.roi), dtype=torch.float32, device=device)
+    _, mu, _ = model.evaluate(pt, fr, bg, prob.zern_true, counts0, want_mu=True)
+    F = int(prob.frame.max()) + 1
+    per = len(prob.frame) // F
+    R = prob.spec.roi
+    engine.set_static(R, R * per, flat_bg=0.0)
+    cam = CameraParams(quantum_efficiency=1.0, dark_electrons=0.0, gain=1.0, read_noise_e=0.0)
+    adu = engine.noise_frames_dev(mu.reshape(F, per * R, R), np.arange(F), cam, prob.noise_seed)
+    return adu.to(torch.float32).reshape(len(prob.frame), R, R)

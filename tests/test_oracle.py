@@ -156,3 +156,39 @@ def test_psf_vs_reference(oracle, reference, dh, depth, ns):
     got = oracle.psf_planes(req, oracle.stack_defocus_m(req))
     for z in range(want.shape[0]):
         assert np.abs(got[z] - want[z]).max() <= 1e-6 * want[z].max(), z
+
+
+def test_nll_oracle_adjoint_matches_central_differences():
+    """The float64 gradient oracle's adjoint against float64 central differences (h = 1e-4 max(1, |theta|))."""
+    from oracle.nll_oracle import NllSpec, gradient, nll, tables
+    spec = NllSpec(roi=10, os=2, pupil=20)
+    rng = np.random.default_rng(5)
+    n, F = 4, 2
+    t = tables(spec)
+    pt = np.column_stack([rng.uniform(4, 6, n), rng.uniform(4, 6, n), rng.uniform(-400, 400, n),
+                          rng.uniform(800, 3000, n)])
+    frame = rng.integers(0, F, n)
+    bg = rng.uniform(5, 15, F)
+    zern = rng.normal(0, 0.03, len(spec.noll))
+    from oracle.nll_oracle import expected
+    counts = rng.poisson(expected(spec, pt, frame, bg, zern, t))
+    p = pt + np.column_stack([rng.normal(0, .3, n), rng.normal(0, .3, n), rng.normal(0, 40, n), rng.normal(0, 80, n)])
+    b, z = bg * 1.1, zern + 0.01
+    _, g, gb, gz = gradient(spec, p, frame, b, z, counts, t)
+
+    def fd(f, x, i):
+        h = 1e-4 * max(1.0, abs(x.flat[i]))
+        xp, xm = x.copy(), x.copy()
+        xp.flat[i] += h
+        xm.flat[i] -= h
+        return (f(xp) - f(xm)) / (2 * h)
+
+    for i in range(p.size):
+        d = fd(lambda P: nll(spec, P, frame, b, z, counts, t), p, i)
+        assert abs(d - g.flat[i]) <= 1e-4 * max(abs(d), 1e-2), i
+    for i in range(F):
+        d = fd(lambda B: nll(spec, p, frame, B, z, counts, t), b, i)
+        assert abs(d - gb[i]) <= 1e-4 * max(abs(d), 1e-2)
+    for j in range(len(z)):
+        d = fd(lambda Z: nll(spec, p, frame, b, Z, counts, t), z, j)
+        assert abs(d - gz[j]) <= 1e-4 * max(abs(d), 1.0), j
