@@ -146,7 +146,8 @@ __device__ __forceinline__ uint32_t SwOff(int row, int col)
 }
 
 // ------------------------------------------------------------------------------------------ the stacked operand
-// Ahat for one set, already split and in K-block order: [kb][hi, lo][row 0..127][col 0..31] floats.
+// Ahat for one set, already split, in K-block order and in the shared-memory image the MMA reads (128-byte-swizzled
+// K-major atoms): [kb][hi, lo][16 KB image of 128 rows x 32 TF32], so one 32 KB bulk copy stages a K block.
 // P <= 64 outputs, M <= 128 inputs (M % 16 == 0); rows beyond 2P and columns beyond 2M are zero.
 __global__ void AhatKernel(const float2* __restrict__ A, int M, int P, float* __restrict__ Ahat)
 {
@@ -168,9 +169,39 @@ __global__ void AhatKernel(const float2* __restrict__ A, int M, int P, float* __
    }
    float hi, lo;
    Split(v, hi, lo);
-   float* base = Ahat + static_cast<size_t>(s) * nKb * 2 * kRows * 32 + static_cast<size_t>(kb) * 2 * kRows * 32;
-   base[row * 32 + col] = hi;
-   base[kRows * 32 + row * 32 + col] = lo;
+   unsigned char* base = reinterpret_cast<unsigned char*>(Ahat) +
+                         (static_cast<size_t>(s) * nKb + kb) * 2 * kBlockBytes;
+   *reinterpret_cast<float*>(base + SwOff(row, col)) = hi;
+   *reinterpret_cast<float*>(base + kBlockBytes + SwOff(row, col)) = lo;
+}
+
+// ------------------------------------------------------------------------------------------ async copies
+__device__ __forceinline__ void MbarExpectTx(uint64_t* bar, uint32_t bytes)
+{
+   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(SmemAddr(bar)), "r"(bytes)
+                : "memory");
+}
+
+// A bulk copy global -> this CTA's shared memory (no multicast), completing `bytes` on the mbarrier.
+__device__ __forceinline__ void BulkLoad(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   SmemAddr(dst)),
+                "l"(src), "r"(bytes), "r"(SmemAddr(bar))
+                : "memory");
+}
+
+// 8 consecutive TMEM columns of this warp's 32 lanes into v[0..7].
+__device__ __forceinline__ void TmemLoad8(uint32_t taddr, float* v)
+{
+   uint32_t r[8];
+   asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                : "r"(taddr));
+   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+   for (int i = 0; i < 8; ++i)
+      v[i] = __uint_as_float(r[i]);
 }
 
 // ------------------------------------------------------------------------------------------ the fused kernel
@@ -185,17 +216,28 @@ struct TcParams
    int nPsf, M, P, normalize;
 };
 
+constexpr int kStages = 2;
+constexpr int kStageBytes = 2 * kBlockBytes;   // a K block's hi and lo images (A: 128 rows; B: up to 128 rows)
+constexpr int kPerThread = 16 * 128 / kThreads; // pupil samples of a row-pass B block per thread
+
+// Per CTA, persistent over PSFs. Per K block kb of each pass, stage s = kb % 2:
+//   wait until the MMAs that last read stage s are done (tcgen05.commit -> mma[s]);
+//   thread 0 starts the bulk copy of Ahat's K block into sA[s] (-> full[s]);
+//   the threads write the B block into sB[s]: row pass, the pupil phasors of rows [16 kb, 16 kb + 16) (their table
+//   entries loaded one K block ahead); column pass, T's columns [16 kb, 16 kb + 16) read from TMEM and split;
+//   then thread 0 waits for full[s] and issues the 12 MMAs (hi*hi, hi*lo, lo*hi over 4 K steps) and the commit.
 __global__ void __launch_bounds__(kThreads, 1) CztTf32x3Kernel(TcParams prm)
 {
    extern __shared__ __align__(1024) unsigned char smemRaw[];
-   // 1024-byte alignment of the operand region (the swizzle atom)
    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
-   unsigned char* sA = smem;                            // [2 stages][hi, lo] x kBlockBytes       (64 KB)
-   unsigned char* sB = smem + 4 * kBlockBytes;          // row pass: [2 stages][hi, lo] blocks   (64 KB)
-                                                        // column pass: [8 kb][hi, lo] x 64 rows (128 KB)
-   float* sRed = reinterpret_cast<float*>(smem + 12 * kBlockBytes);                 // 8 floats
-   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 12 * kBlockBytes + 64);       // 2 stage barriers
-   uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(smem + 12 * kBlockBytes + 96);
+   unsigned char* sA = smem;                                   // [kStages] x 32 KB
+   unsigned char* sB = smem + kStages * kStageBytes;           // [kStages] x 32 KB
+   unsigned char* tail = smem + 2 * kStages * kStageBytes;
+   double* sRed = reinterpret_cast<double*>(tail);             // 4 doubles
+   uint64_t* full = reinterpret_cast<uint64_t*>(tail + 64);    // kStages
+   uint64_t* mmaBar = reinterpret_cast<uint64_t*>(tail + 96);  // kStages
+   uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(tail + 128);
+   int* sErr = reinterpret_cast<int*>(tail + 132);
 
    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
    const int M = prm.M, P = prm.P, nKb = M / 16;
@@ -208,56 +250,106 @@ __global__ void __launch_bounds__(kThreads, 1) CztTf32x3Kernel(TcParams prm)
    }
    if (tid == 0)
    {
-      MbarInit(&bar[0], 1);
-      MbarInit(&bar[1], 1);
+      for (int s = 0; s < kStages; ++s)
+      {
+         MbarInit(&full[s], 1);
+         MbarInit(&mmaBar[s], 1);
+      }
+      *sErr = 0;
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
    }
    TcFenceBefore();
    __syncthreads();
    TcFenceAfter();
    const uint32_t tmem = *tmemSlot;
-   uint32_t phase[2] = {0u, 0u};   // the parity each stage barrier's next completion will have
+   uint32_t fullPhase[kStages] = {0u, 0u}, mmaPhase[kStages] = {0u, 0u};
+   int pending[kStages] = {0, 0};
    bool ok = true;
    const uint32_t idesc1 = InstrDesc(kRows, M), idesc2 = InstrDesc(kRows, 64);
+
+   // every thread waits for stage s's last MMAs; the outcome (and a failed copy wait of thread 0, whose flag is
+   // read after the barrier) is made uniform
+   auto drain = [&](int s) {
+      if (pending[s])
+      {
+         ok = __syncthreads_and(MbarWait(&mmaBar[s], mmaPhase[s]) && ok) != 0;
+         if (*sErr)
+            ok = false;
+         mmaPhase[s] ^= 1u;
+         pending[s] = 0;
+      }
+   };
+   // thread 0: wait for the stage's A copy, then the MMAs and the commit (a commit with no MMA completes at once,
+   // so the other threads' waits end after a failure too)
+   auto issue = [&](int s, uint32_t dTmem, uint32_t bH, uint32_t bL, uint32_t idesc, bool first) {
+      if (tid != 0)
+         return;
+      const bool copied = MbarWait(&full[s], fullPhase[s]);
+      fullPhase[s] ^= 1u;
+      if (!copied)
+         *sErr = 1;
+      TcFenceAfter();
+      if (copied && *sErr == 0)
+      {
+         const uint32_t aH = SmemAddr(sA + s * kStageBytes), aL = aH + kBlockBytes;
+#pragma unroll
+         for (int kk = 0; kk < 4; ++kk)
+         {
+            const uint32_t off = kk * 32;   // 8 TF32 = 32 bytes along K
+            Mma(dTmem, SmemDesc(aH + off), SmemDesc(bH + off), idesc, (first && kk == 0) ? 0u : 1u);
+            Mma(dTmem, SmemDesc(aH + off), SmemDesc(bL + off), idesc, 1u);
+            Mma(dTmem, SmemDesc(aL + off), SmemDesc(bH + off), idesc, 1u);
+         }
+      }
+      Commit(&mmaBar[s]);
+   };
+   auto loadA = [&](int s, const float* ahat, int kb) {
+      if (tid == 0)
+      {
+         MbarExpectTx(&full[s], kStageBytes);
+         BulkLoad(sA + s * kStageBytes, ahat + static_cast<size_t>(kb) * (kStageBytes / 4), kStageBytes, &full[s]);
+      }
+   };
 
    for (int psf = blockIdx.x; psf < prm.nPsf && ok; psf += gridDim.x)
    {
       const PsfItem it = prm.items[psf];
       const SetParams& sp = prm.sets[it.set];
       const double3* tab = prm.tables + static_cast<size_t>(it.set) * M * M;
-      const float* ahat = prm.ahat + static_cast<size_t>(it.set) * 8 * 2 * kRows * 32;
-      int pending[2] = {0, 0};   // commits on each stage barrier not yet waited for
+      const float* ahat = prm.ahat + static_cast<size_t>(it.set) * 8 * (kStageBytes / 4);
 
       // ---------------------------------------------------------------- row pass: T = A U
-      for (int kb = 0; kb < nKb && ok; ++kb)
+      double3 pre[kPerThread];
+#pragma unroll
+      for (int q = 0; q < kPerThread; ++q)
       {
-         const int s = kb & 1;
-         if (pending[s])
-         {
-            // every thread waits; the outcome is made uniform so no thread leaves a loop the others stay in
-            ok = __syncthreads_and(MbarWait(&bar[s], phase[s])) != 0;
-            phase[s] ^= 1u;
-            pending[s] = 0;
-         }
+         const int e = tid + q * kThreads, m = e & 127, nl = e >> 7;
+         pre[q] = m < M ? tab[static_cast<size_t>(nl) * M + m] : make_double3(0.0, -1.0, 0.0);
+      }
+      for (int kb = 0; kb < nKb; ++kb)
+      {
+         const int s = kb % kStages;
+         drain(s);
          if (!ok)
             break;
-         unsigned char* a = sA + s * 2 * kBlockBytes;
-         unsigned char* b = sB + s * 2 * kBlockBytes;
-         // A block kb (hi, lo): 2 x 128 rows x 8 chunks of 16 bytes
-         const float4* src = reinterpret_cast<const float4*>(ahat + static_cast<size_t>(kb) * 2 * kRows * 32);
-         for (int c = tid; c < 2 * kRows * 8; c += kThreads)
+         loadA(s, ahat, kb);
+         double3 cur[kPerThread];
+#pragma unroll
+         for (int q = 0; q < kPerThread; ++q)
+            cur[q] = pre[q];
+         if (kb + 1 < nKb)
+#pragma unroll
+            for (int q = 0; q < kPerThread; ++q)
+            {
+               const int e = tid + q * kThreads, m = e & 127, n = 16 * (kb + 1) + (e >> 7);
+               pre[q] = m < M ? tab[static_cast<size_t>(n) * M + m] : make_double3(0.0, -1.0, 0.0);
+            }
+         unsigned char* b = sB + s * kStageBytes;
+#pragma unroll
+         for (int q = 0; q < kPerThread; ++q)
          {
-            const int part = c / (kRows * 8), row = (c / 8) % kRows, ch = c % 8;
-            const float4 v = __ldg(src + c);
-            *reinterpret_cast<float4*>(a + part * kBlockBytes + SwOff(row, 4 * ch)) = v;
-         }
-         // B block kb: pupil rows n in [16 kb, 16 kb + 16) for every column m (B row m; columns: 16 real, 16 imag)
-         for (int e = tid; e < 16 * 128; e += kThreads)
-         {
-            const int m = e & 127, nl = e >> 7, n = 16 * kb + nl;
-            float2 u = make_float2(0.f, 0.f);
-            if (m < M)
-               u = PupilPhasor(tab[static_cast<size_t>(n) * M + m], sp, it.dtiM);
+            const int e = tid + q * kThreads, m = e & 127, nl = e >> 7;
+            const float2 u = PupilPhasor(cur[q], sp, it.dtiM);
             float rh, rl, ih, il;
             Split(u.x, rh, rl);
             Split(u.y, ih, il);
@@ -268,108 +360,49 @@ __global__ void __launch_bounds__(kThreads, 1) CztTf32x3Kernel(TcParams prm)
          }
          FenceProxyAsync();
          __syncthreads();
-         if (tid == 0)
-         {
-            TcFenceAfter();
-            const uint32_t aH = SmemAddr(a), aL = aH + kBlockBytes, bH = SmemAddr(b), bL = bH + kBlockBytes;
-#pragma unroll
-            for (int kk = 0; kk < 4; ++kk)
-            {
-               const uint32_t off = kk * 32;   // 8 TF32 = 32 bytes along K
-               const uint32_t acc0 = (kb > 0 || kk > 0) ? 1u : 0u;
-               Mma(tmem, SmemDesc(aH + off), SmemDesc(bH + off), idesc1, acc0);
-               Mma(tmem, SmemDesc(aH + off), SmemDesc(bL + off), idesc1, 1u);
-               Mma(tmem, SmemDesc(aL + off), SmemDesc(bH + off), idesc1, 1u);
-            }
-            Commit(&bar[s]);
-         }
+         const uint32_t bH = SmemAddr(b);
+         issue(s, tmem, bH, bH + kBlockBytes, idesc1, kb == 0);
          pending[s] = 1;
       }
-      for (int s = 0; s < 2 && ok; ++s)
-         if (pending[s])
-         {
-            ok = __syncthreads_and(MbarWait(&bar[s], phase[s])) != 0;
-            phase[s] ^= 1u;
-            pending[s] = 0;
-         }
+      for (int s = 0; s < kStages; ++s)
+         drain(s);
       if (!ok)
          break;
       TcFenceAfter();
-      // ------------------------------------------------ T from TMEM -> the column pass's B operand (split)
-      // TMEM lane r = 32 g + 16 h + i holds output row y = 16 g + i, part h; column m. B2 row y, column
-      // k = 32 (m / 16) + 16 h + m % 16, in K block m / 16.
-      if (warp < 4)
-      {
-         const int r = 32 * warp + lane, g = r >> 5, h = (r >> 4) & 1, i = r & 15, y = 16 * g + i;
-         for (int c0 = 0; c0 < M; c0 += 32)
-         {
-            float v[32];
-            TmemLoad32(tmem + (static_cast<uint32_t>(32 * warp) << 16) + c0, v);
-            if (y < 64)
-#pragma unroll
-               for (int j = 0; j < 32; ++j)
-               {
-                  const int m = c0 + j, kb = m >> 4, col = 16 * h + (m & 15);
-                  float hi, lo;
-                  Split(y < P ? v[j] : 0.f, hi, lo);
-                  unsigned char* blk = sB + kb * 2 * (kBlockBytes / 2);
-                  *reinterpret_cast<float*>(blk + SwOff(y, col)) = hi;
-                  *reinterpret_cast<float*>(blk + kBlockBytes / 2 + SwOff(y, col)) = lo;
-               }
-         }
-      }
-      TcFenceBefore();
-      FenceProxyAsync();
-      __syncthreads();
 
       // ---------------------------------------------------------------- column pass: E^T = A T^T
-      for (int kb = 0; kb < nKb && ok; ++kb)
+      // TMEM lane r = 32 g + 16 h + i holds T row y = 16 g + i, part h; column m. B2 block kb: row y, column
+      // 16 h + (m - 16 kb). Warps w and w + 4 share lanes 32 (w % 4) ..; warp w reads columns 16 kb + 8 (w / 4) ..
+      const int lg = warp & 3, ch = warp >> 2;
+      const int r = 32 * lg + lane, h = (r >> 4) & 1, y = 16 * lg + (r & 15);
+      for (int kb = 0; kb < nKb; ++kb)
       {
-         const int s = kb & 1;
-         if (pending[s])
-         {
-            // every thread waits; the outcome is made uniform so no thread leaves a loop the others stay in
-            ok = __syncthreads_and(MbarWait(&bar[s], phase[s])) != 0;
-            phase[s] ^= 1u;
-            pending[s] = 0;
-         }
+         const int s = kb % kStages;
+         drain(s);
          if (!ok)
             break;
-         unsigned char* a = sA + s * 2 * kBlockBytes;
-         const float4* src = reinterpret_cast<const float4*>(ahat + static_cast<size_t>(kb) * 2 * kRows * 32);
-         for (int c = tid; c < 2 * kRows * 8; c += kThreads)
+         loadA(s, ahat, kb);
+         float v[8];
+         TmemLoad8(tmem + (static_cast<uint32_t>(32 * lg) << 16) + 16 * kb + 8 * ch, v);
+         unsigned char* b = sB + s * kStageBytes;
+#pragma unroll
+         for (int j = 0; j < 8; ++j)
          {
-            const int part = c / (kRows * 8), row = (c / 8) % kRows, ch = c % 8;
-            const float4 v = __ldg(src + c);
-            *reinterpret_cast<float4*>(a + part * kBlockBytes + SwOff(row, 4 * ch)) = v;
+            const int col = 16 * h + 8 * ch + j;
+            float hi, lo;
+            Split(y < P ? v[j] : 0.f, hi, lo);
+            *reinterpret_cast<float*>(b + SwOff(y, col)) = hi;
+            *reinterpret_cast<float*>(b + kBlockBytes / 2 + SwOff(y, col)) = lo;
          }
+         TcFenceBefore();
          FenceProxyAsync();
          __syncthreads();
-         if (tid == 0)
-         {
-            TcFenceAfter();
-            const uint32_t aH = SmemAddr(a), aL = aH + kBlockBytes;
-            const uint32_t bH = SmemAddr(sB + kb * kBlockBytes), bL = bH + kBlockBytes / 2;
-#pragma unroll
-            for (int kk = 0; kk < 4; ++kk)
-            {
-               const uint32_t off = kk * 32;
-               const uint32_t acc0 = (kb > 0 || kk > 0) ? 1u : 0u;
-               Mma(tmem + 128, SmemDesc(aH + off), SmemDesc(bH + off), idesc2, acc0);
-               Mma(tmem + 128, SmemDesc(aH + off), SmemDesc(bL + off), idesc2, 1u);
-               Mma(tmem + 128, SmemDesc(aL + off), SmemDesc(bH + off), idesc2, 1u);
-            }
-            Commit(&bar[s]);
-         }
+         const uint32_t bH = SmemAddr(b);
+         issue(s, tmem + 128, bH, bH + kBlockBytes / 2, idesc2, kb == 0);
          pending[s] = 1;
       }
-      for (int s = 0; s < 2 && ok; ++s)
-         if (pending[s])
-         {
-            ok = __syncthreads_and(MbarWait(&bar[s], phase[s])) != 0;
-            phase[s] ^= 1u;
-            pending[s] = 0;
-         }
+      for (int s = 0; s < kStages; ++s)
+         drain(s);
       if (!ok)
          break;
       TcFenceAfter();
@@ -382,13 +415,13 @@ __global__ void __launch_bounds__(kThreads, 1) CztTf32x3Kernel(TcParams prm)
       {
          for (int c0 = 0; c0 < 64; c0 += 32)
          {
-            float v[32];
-            TmemLoad32(tmem + (static_cast<uint32_t>(32 * warp) << 16) + 128 + c0, v);
+            float vv[32];
+            TmemLoad32(tmem + (static_cast<uint32_t>(32 * warp) << 16) + 128 + c0, vv);
 #pragma unroll
             for (int j = 0; j < 32; ++j)
             {
-               const float o = __shfl_xor_sync(0xffffffffu, v[j], 16);
-               const float e = v[j] * v[j] + o * o;
+               const float o = __shfl_xor_sync(0xffffffffu, vv[j], 16);
+               const float e = vv[j] * vv[j] + o * o;
                I[c0 + j] = e;
                if (lane < 16 && x < P && c0 + j < P)
                   local += static_cast<double>(e);
@@ -399,22 +432,20 @@ __global__ void __launch_bounds__(kThreads, 1) CztTf32x3Kernel(TcParams prm)
       double total = 0.0;
       if (prm.normalize)
       {
-         // sum over the 4 epilogue warps
          for (int o = 16; o > 0; o >>= 1)
             local += __shfl_xor_sync(0xffffffffu, local, o);
-         double* red = reinterpret_cast<double*>(sRed);
          __syncthreads();
          if (lane == 0 && warp < 4)
-            red[warp] = local;
+            sRed[warp] = local;
          __syncthreads();
-         total = red[0] + red[1] + red[2] + red[3];
+         total = sRed[0] + sRed[1] + sRed[2] + sRed[3];
       }
       if (warp < 4 && lane < 16 && x < P)
       {
          float* plane = prm.out + static_cast<size_t>(psf) * P * P;
-         for (int y = 0; y < P; ++y)
-            plane[static_cast<size_t>(y) * P + x] =
-               (prm.normalize && total > 0.0) ? static_cast<float>(static_cast<double>(I[y]) / total) : I[y];
+         for (int yy = 0; yy < P; ++yy)
+            plane[static_cast<size_t>(yy) * P + x] =
+               (prm.normalize && total > 0.0) ? static_cast<float>(static_cast<double>(I[yy]) / total) : I[yy];
       }
       __syncthreads();
    }
@@ -436,7 +467,7 @@ int BuildAhat(iscu_ctx* ctx, const float2* A, int nSets, int M, int P, DevBuf& a
    if (!Tf32x3Supports(M, P))
       return Fail(ISCU_ERR_ARG, "tf32x3 chirp-Z: needs pupil samples M <= 128 (a multiple of 16) and planes of at "
                                 "most 64 x 64 (else use the fp32 method)");
-   ISCU_CK(ahat.Reserve(static_cast<size_t>(nSets) * 8 * 2 * kRows * 32 * sizeof(float)));
+   ISCU_CK(ahat.Reserve(static_cast<size_t>(nSets) * 8 * kStageBytes));
    AhatKernel<<<dim3((8 * kRows * 32 + 255) / 256, nSets), 256, 0, ctx->stream>>>(A, M, P, ahat.as<float>());
    ISCU_CK_LAUNCH(ctx, "AhatKernel");
    return ISCU_OK;
@@ -445,7 +476,7 @@ int BuildAhat(iscu_ctx* ctx, const float2* A, int nSets, int M, int P, DevBuf& a
 int LaunchCztTf32x3Core(iscu_ctx* ctx, const SetParams* sets, const double3* tables, const float* ahat,
                         const PsfItem* items, uint32_t nPsf, int M, int P, int normalize, float* out, int* dErr)
 {
-   const size_t smem = 12 * kBlockBytes + 128 + 1024;
+   const size_t smem = 2 * kStages * kStageBytes + 256 + 1024;
    ISCU_CK(cudaFuncSetAttribute(CztTf32x3Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
    TcParams prm;
    prm.sets = sets;
