@@ -67,9 +67,12 @@ __device__ __forceinline__ double BlockSumDouble(double v, double* red)
 int LaunchCztTf32x3(iscu_ctx* ctx, const SetParams* sets, const double3* tables, const float2* A, uint32_t nSets,
                     const PsfItem* items, uint32_t nPsf, int M, int P, int normalize, float* out);
 bool Tf32x3Supports(int M, int P);
-int BuildAhat(iscu_ctx* ctx, const float2* A, int nSets, int M, int P, DevBuf& ahat);
-int LaunchCztTf32x3Core(iscu_ctx* ctx, const SetParams* sets, const double3* tables, const float* ahat,
-                        const PsfItem* items, uint32_t nPsf, int M, int P, int normalize, float* out, int* dErr);
+// The split-precision kernel's per-set data (the DFT operand's K-block images and the pupil phase tables) in one
+// buffer.
+int BuildAhat(iscu_ctx* ctx, const float2* A, const SetParams* sets, const double3* tables, int nSets, int M, int P,
+              DevBuf& ahat);
+int LaunchCztTf32x3Core(iscu_ctx* ctx, const SetParams* sets, const float* ahat, int nSets, const PsfItem* items,
+                        uint32_t nPsf, int M, int P, int normalize, float* out, int* dErr);
 
 int LaunchPsfTables(iscu_ctx* ctx, const SetParams* dSets, uint32_t nSets, int M, int P, double3* dTab, float2* dA,
                     float2* dAt);

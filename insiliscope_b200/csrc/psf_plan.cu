@@ -53,7 +53,7 @@ int RunDev(iscu_psf_plan* p, const uint32_t* setOf, const double* defocusNm, uin
                                                              p->items.as<PsfItem>(), p->err.as<int>());
    ISCU_CK_LAUNCH(ctx, "PlanItemsKernel");
    if (p->method == ISCU_CZT_TF32X3)
-      return LaunchCztTf32x3Core(ctx, p->sets.as<SetParams>(), p->tab.as<double3>(), p->ahat.as<float>(),
+      return LaunchCztTf32x3Core(ctx, p->sets.as<SetParams>(), p->ahat.as<float>(), static_cast<int>(p->nSets),
                                  p->items.as<PsfItem>(), n, p->M, p->P, normalize, out, p->err.as<int>());
    return LaunchCztFp32(ctx, p->sets.as<SetParams>(), p->tab.as<double3>(), p->A.as<float2>(), p->At.as<float2>(),
                         p->items.as<PsfItem>(), n, p->M, p->P, normalize, out);
@@ -112,8 +112,9 @@ int iscu_psf_plan_create(iscu_ctx* ctx, const iscu_psf_request* sets, uint32_t n
                         p->At.as<float2>());
    if (rc != ISCU_OK)
       return rc;
-   if (method == ISCU_CZT_TF32X3 && (rc = BuildAhat(ctx, p->A.as<float2>(), static_cast<int>(n_sets), p->M, p->P,
-                                                     p->ahat)) != ISCU_OK)
+   if (method == ISCU_CZT_TF32X3 &&
+       (rc = BuildAhat(ctx, p->A.as<float2>(), p->sets.as<SetParams>(), p->tab.as<double3>(),
+                       static_cast<int>(n_sets), p->M, p->P, p->ahat)) != ISCU_OK)
       return rc;
    ISCU_CK(cudaStreamSynchronize(ctx->stream));
    *out = p.release();

@@ -33,7 +33,7 @@ namespace iscu {
 
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 512;
 constexpr int kRows = 128;             // UMMA M (2P rows, padded)
 constexpr int kBlockBytes = 128 * 128; // one operand K block: 128 rows x 32 TF32 (128 B per row)
 constexpr int kTmemCols = 256;         // row pass: columns [0, 128); column pass: [128, 192)
@@ -175,6 +175,34 @@ __global__ void AhatKernel(const float2* __restrict__ A, int M, int P, float* __
    *reinterpret_cast<float*>(base + kBlockBytes + SwOff(row, col)) = lo;
 }
 
+// The pupil's phase table for the split-precision kernel: per set and sample (base, opd3F) with
+// base = k0 opd1 + (zernike + mask) and the defocus term's obliquity opd3F (ZernikePsf.cpp:240-248), so a PSF's
+// phase is base + (k0 ni dti) opd3F: one float64 multiply-add before the reduction mod 2 pi. opd3F < 0 outside the
+// aperture.
+__global__ void PhaseTableKernel(const SetParams* __restrict__ sets, const double3* __restrict__ tables, int MM,
+                                 double2* __restrict__ out)
+{
+   const int s = blockIdx.y;
+   const int m = blockIdx.x * blockDim.x + threadIdx.x;
+   if (m >= MM)
+      return;
+   const double3 t = tables[static_cast<size_t>(s) * MM + m];
+   out[static_cast<size_t>(s) * MM + m] = t.y < 0.0 ? make_double2(0.0, -1.0)
+                                                    : make_double2(sets[s].k0 * t.x + t.z, t.y);
+}
+
+// The pupil phasor of one sample from the phase table: float64 phase, reduced mod 2 pi, then the float32 sine and
+// cosine of the reduced phase by the special-function unit (absolute error ~4e-7 over [-pi, pi]).
+__device__ __forceinline__ float2 TablePhasor(double2 t, double a)
+{
+   if (t.y < 0.0)
+      return make_float2(0.f, 0.f);
+   const double ph = ReduceTwoPi(fma(a, t.y, t.x));
+   float sn, cs;
+   __sincosf(static_cast<float>(ph), &sn, &cs);
+   return make_float2(cs, sn);
+}
+
 // ------------------------------------------------------------------------------------------ async copies
 __device__ __forceinline__ void MbarExpectTx(uint64_t* bar, uint32_t bytes)
 {
@@ -191,16 +219,16 @@ __device__ __forceinline__ void BulkLoad(void* dst, const void* src, uint32_t by
                 : "memory");
 }
 
-// 8 consecutive TMEM columns of this warp's 32 lanes into v[0..7].
-__device__ __forceinline__ void TmemLoad8(uint32_t taddr, float* v)
+// 4 consecutive TMEM columns of this warp's 32 lanes into v[0..3].
+__device__ __forceinline__ void TmemLoad4(uint32_t taddr, float* v)
 {
-   uint32_t r[8];
-   asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+   uint32_t r[4];
+   asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
                 : "r"(taddr));
    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-   for (int i = 0; i < 8; ++i)
+   for (int i = 0; i < 4; ++i)
       v[i] = __uint_as_float(r[i]);
 }
 
@@ -208,7 +236,7 @@ __device__ __forceinline__ void TmemLoad8(uint32_t taddr, float* v)
 struct TcParams
 {
    const SetParams* sets;
-   const double3* tables;
+   const double2* phase;     // [set][M * M] (base, opd3F)
    const float* ahat;
    const PsfItem* items;
    float* out;
@@ -315,16 +343,17 @@ __global__ void __launch_bounds__(kThreads, 1) CztTf32x3Kernel(TcParams prm)
    {
       const PsfItem it = prm.items[psf];
       const SetParams& sp = prm.sets[it.set];
-      const double3* tab = prm.tables + static_cast<size_t>(it.set) * M * M;
+      const double2* tab = prm.phase + static_cast<size_t>(it.set) * M * M;
+      const double aDef = sp.k0 * sp.ni * it.dtiM;
       const float* ahat = prm.ahat + static_cast<size_t>(it.set) * 8 * (kStageBytes / 4);
 
       // ---------------------------------------------------------------- row pass: T = A U
-      double3 pre[kPerThread];
+      double2 pre[kPerThread];
 #pragma unroll
       for (int q = 0; q < kPerThread; ++q)
       {
          const int e = tid + q * kThreads, m = e & 127, nl = e >> 7;
-         pre[q] = m < M ? tab[static_cast<size_t>(nl) * M + m] : make_double3(0.0, -1.0, 0.0);
+         pre[q] = m < M ? tab[static_cast<size_t>(nl) * M + m] : make_double2(0.0, -1.0);
       }
       for (int kb = 0; kb < nKb; ++kb)
       {
@@ -333,7 +362,7 @@ __global__ void __launch_bounds__(kThreads, 1) CztTf32x3Kernel(TcParams prm)
          if (!ok)
             break;
          loadA(s, ahat, kb);
-         double3 cur[kPerThread];
+         double2 cur[kPerThread];
 #pragma unroll
          for (int q = 0; q < kPerThread; ++q)
             cur[q] = pre[q];
@@ -342,14 +371,14 @@ __global__ void __launch_bounds__(kThreads, 1) CztTf32x3Kernel(TcParams prm)
             for (int q = 0; q < kPerThread; ++q)
             {
                const int e = tid + q * kThreads, m = e & 127, n = 16 * (kb + 1) + (e >> 7);
-               pre[q] = m < M ? tab[static_cast<size_t>(n) * M + m] : make_double3(0.0, -1.0, 0.0);
+               pre[q] = m < M ? tab[static_cast<size_t>(n) * M + m] : make_double2(0.0, -1.0);
             }
          unsigned char* b = sB + s * kStageBytes;
 #pragma unroll
          for (int q = 0; q < kPerThread; ++q)
          {
             const int e = tid + q * kThreads, m = e & 127, nl = e >> 7;
-            const float2 u = PupilPhasor(cur[q], sp, it.dtiM);
+            const float2 u = TablePhasor(cur[q], aDef);
             float rh, rl, ih, il;
             Split(u.x, rh, rl);
             Split(u.y, ih, il);
@@ -372,7 +401,8 @@ __global__ void __launch_bounds__(kThreads, 1) CztTf32x3Kernel(TcParams prm)
 
       // ---------------------------------------------------------------- column pass: E^T = A T^T
       // TMEM lane r = 32 g + 16 h + i holds T row y = 16 g + i, part h; column m. B2 block kb: row y, column
-      // 16 h + (m - 16 kb). Warps w and w + 4 share lanes 32 (w % 4) ..; warp w reads columns 16 kb + 8 (w / 4) ..
+      // 16 h + (m - 16 kb). Warps w, w + 4, w + 8, w + 12 share lanes 32 (w % 4) ..; warp w reads the 4 columns
+      // 16 kb + 4 (w / 4) ..
       const int lg = warp & 3, ch = warp >> 2;
       const int r = 32 * lg + lane, h = (r >> 4) & 1, y = 16 * lg + (r & 15);
       for (int kb = 0; kb < nKb; ++kb)
@@ -382,13 +412,13 @@ __global__ void __launch_bounds__(kThreads, 1) CztTf32x3Kernel(TcParams prm)
          if (!ok)
             break;
          loadA(s, ahat, kb);
-         float v[8];
-         TmemLoad8(tmem + (static_cast<uint32_t>(32 * lg) << 16) + 16 * kb + 8 * ch, v);
+         float v[4];
+         TmemLoad4(tmem + (static_cast<uint32_t>(32 * lg) << 16) + 16 * kb + 4 * ch, v);
          unsigned char* b = sB + s * kStageBytes;
 #pragma unroll
-         for (int j = 0; j < 8; ++j)
+         for (int j = 0; j < 4; ++j)
          {
-            const int col = 16 * h + 8 * ch + j;
+            const int col = 16 * h + 4 * ch + j;
             float hi, lo;
             Split(y < P ? v[j] : 0.f, hi, lo);
             *reinterpret_cast<float*>(b + SwOff(y, col)) = hi;
@@ -462,25 +492,32 @@ __global__ void __launch_bounds__(kThreads, 1) CztTf32x3Kernel(TcParams prm)
 
 bool Tf32x3Supports(int M, int P) { return M <= 128 && M % 16 == 0 && P <= 64 && P >= 1; }
 
-int BuildAhat(iscu_ctx* ctx, const float2* A, int nSets, int M, int P, DevBuf& ahat)
+size_t AhatBytes(int nSets) { return static_cast<size_t>(nSets) * 8 * kStageBytes; }
+
+int BuildAhat(iscu_ctx* ctx, const float2* A, const SetParams* sets, const double3* tables, int nSets, int M, int P,
+              DevBuf& ahat)
 {
    if (!Tf32x3Supports(M, P))
       return Fail(ISCU_ERR_ARG, "tf32x3 chirp-Z: needs pupil samples M <= 128 (a multiple of 16) and planes of at "
                                 "most 64 x 64 (else use the fp32 method)");
-   ISCU_CK(ahat.Reserve(static_cast<size_t>(nSets) * 8 * kStageBytes));
+   // the K-block images, then the phase tables
+   ISCU_CK(ahat.Reserve(AhatBytes(nSets) + static_cast<size_t>(nSets) * M * M * sizeof(double2)));
    AhatKernel<<<dim3((8 * kRows * 32 + 255) / 256, nSets), 256, 0, ctx->stream>>>(A, M, P, ahat.as<float>());
    ISCU_CK_LAUNCH(ctx, "AhatKernel");
+   PhaseTableKernel<<<dim3((M * M + 255) / 256, nSets), 256, 0, ctx->stream>>>(
+      sets, tables, M * M, reinterpret_cast<double2*>(ahat.as<char>() + AhatBytes(nSets)));
+   ISCU_CK_LAUNCH(ctx, "PhaseTableKernel");
    return ISCU_OK;
 }
 
-int LaunchCztTf32x3Core(iscu_ctx* ctx, const SetParams* sets, const double3* tables, const float* ahat,
-                        const PsfItem* items, uint32_t nPsf, int M, int P, int normalize, float* out, int* dErr)
+int LaunchCztTf32x3Core(iscu_ctx* ctx, const SetParams* sets, const float* ahat, int nSets, const PsfItem* items,
+                        uint32_t nPsf, int M, int P, int normalize, float* out, int* dErr)
 {
    const size_t smem = 2 * kStages * kStageBytes + 256 + 1024;
    ISCU_CK(cudaFuncSetAttribute(CztTf32x3Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
    TcParams prm;
    prm.sets = sets;
-   prm.tables = tables;
+   prm.phase = reinterpret_cast<const double2*>(reinterpret_cast<const char*>(ahat) + AhatBytes(nSets));
    prm.ahat = ahat;
    prm.items = items;
    prm.out = out;
@@ -499,12 +536,13 @@ int LaunchCztTf32x3(iscu_ctx* ctx, const SetParams* sets, const double3* tables,
                     const PsfItem* items, uint32_t nPsf, int M, int P, int normalize, float* out)
 {
    DevBuf dAhat, dErr;
-   int rc = BuildAhat(ctx, A, static_cast<int>(nSets), M, P, dAhat);
+   int rc = BuildAhat(ctx, A, sets, tables, static_cast<int>(nSets), M, P, dAhat);
    if (rc != ISCU_OK)
       return rc;
    ISCU_CK(dErr.Reserve(sizeof(int)));
    ISCU_CK(cudaMemsetAsync(dErr.p, 0, sizeof(int), ctx->stream));
-   rc = LaunchCztTf32x3Core(ctx, sets, tables, dAhat.as<float>(), items, nPsf, M, P, normalize, out, dErr.as<int>());
+   rc = LaunchCztTf32x3Core(ctx, sets, dAhat.as<float>(), static_cast<int>(nSets), items, nPsf, M, P, normalize, out,
+                            dErr.as<int>());
    if (rc != ISCU_OK)
       return rc;
    int err = 0;
