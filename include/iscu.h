@@ -345,7 +345,8 @@ int iscu_collect_emitters(iscu_ctx* ctx, int32_t slot, const iscu_blink_event* e
 
 /* The same on the device (no reference counterpart: the reference collects on the CPU): events_dev (n_events),
  * bucket_index_dev (nullable) and bucket_start_dev (n_frames + 1) as above, the per-frame arrays and illum_dev
- * (width*height of the context's frame) device pointers or NULL. Writes out_dev (at most max_out records),
+ * (width*height of the context's frame) device pointers or NULL. Writes out_dev (at most max_out records) and
+ * event_index_dev (nullable: each record's index into the events -- the frame's ground-truth emitter list),
  * frames_out_dev (n_frames) and *n_out_dev = the records kept (more than max_out: the batch did not fit);
  * *n_clamped_dev (nullable, zero it first) += the emitters whose z was clamped. Events whose slot holds no kernel stack
  * are dropped (the host form fails on them). Needs iscu_set_static (the frame size). Asynchronous. */
@@ -354,8 +355,9 @@ int iscu_collect_emitters_dev(iscu_ctx* ctx, int32_t slot, const iscu_blink_even
                               uint32_t n_frames, double pixel_size_nm, double photons_per_blink,
                               const double* drift_x_px_dev, const double* drift_y_px_dev,
                               const double* global_z_offset_um_dev, const double* bg_scale_dev, const float* illum_dev,
-                              double min_photons, iscu_emitter* out_dev, uint32_t max_out,
-                              iscu_frame* frames_out_dev, uint32_t* n_out_dev, int64_t* n_clamped_dev);
+                              double min_photons, iscu_emitter* out_dev, uint32_t* event_index_dev,
+                              uint32_t max_out, iscu_frame* frames_out_dev, uint32_t* n_out_dev,
+                              int64_t* n_clamped_dev);
 
 /* Host blink events to host frames in one call (the movie engine's frame loop for one dye group batch,
  * ScopeMovie.cpp:7059-7110: CollectFrameEmitters + RenderPhotonImage + ApplyNoiseChain per frame): the events, bucket
@@ -369,6 +371,35 @@ int iscu_render_events(iscu_ctx* ctx, int32_t slot, const iscu_blink_event* even
                        const double* drift_y_px, const double* global_z_offset_um, const double* bg_scale,
                        int32_t use_illum, double min_photons, const iscu_camera* cam, uint32_t seed, float* photons,
                        uint16_t* adu, uint32_t* n_emitters, int64_t* n_clamped);
+
+/* ---------------------------------------------------------------- per-movie host models ----------------------- */
+
+/* sim::DriftSettings (Drift.h:57-79). */
+typedef struct iscu_drift_settings {
+   double xy_nm_per_sqrt_sec;   /* random walk: RMS displacement after 1 s, x and y each */
+   double z_nm_per_sqrt_sec;
+   double xy_speed_nm_per_sec;  /* directed part */
+   double z_speed_nm_per_sec;
+   double xy_angle_deg;         /* < 0: drawn per seed */
+   int32_t z_direction;         /* +1 away from the coverslip, -1 towards, 0 drawn per seed */
+   int32_t reserved;
+   double angle_wander_deg;     /* 180 */
+   double z_angle_wander_deg;   /* 90 */
+   double speed_wander_pct;     /* 0 */
+   double wander_time_sec;      /* 60 */
+} iscu_drift_settings;
+
+/* sim::DriftTrajectory (Drift.cpp:24-124; host): the sample's drift (nm, camera axes, +z away from the coverslip) at
+ * frames 0 .. frames - 1 into xyz_nm[3 f + (0, 1, 2)], zero at frame 0, every draw from the counter stream of
+ * (DriftSeed(random_seed), frame): bit for bit the reference's. */
+int iscu_drift_trajectory(int64_t random_seed, int64_t frames, double frame_sec, const iscu_drift_settings* settings,
+                          double* xyz_nm);
+/* sim::BuildIlluminationField (SMLMBackground.cpp:8-38; host): profile 0 flat (out untouched), 1 Gaussian, 2 flat-top
+ * with FWHM fwhm_pct % of the width; out: width*height floats with peak 1; *mean_factor (nullable) the field's mean. */
+int iscu_illumination_field(uint32_t width, uint32_t height, int32_t profile, double fwhm_pct, float* out,
+                            double* mean_factor);
+/* sim::BackgroundFadeScale (SMLMBackground.cpp:52-55): 0.3 + 0.7 exp(-t / decay), 1 when decay <= 0. */
+double iscu_background_fade_scale(double t, double decay);
 
 /* ---------------------------------------------------------------- Poisson-likelihood gradient ---------------- */
 

@@ -91,6 +91,14 @@ class BlinkEvent(C.Structure):
 
 
 # name -> (restype, argtypes); every function include/iscu.h declares.
+class DriftSettings(C.Structure):
+    _fields_ = [("xy_nm_per_sqrt_sec", C.c_double), ("z_nm_per_sqrt_sec", C.c_double),
+                ("xy_speed_nm_per_sec", C.c_double), ("z_speed_nm_per_sec", C.c_double),
+                ("xy_angle_deg", C.c_double), ("z_direction", C.c_int32), ("reserved", C.c_int32),
+                ("angle_wander_deg", C.c_double), ("z_angle_wander_deg", C.c_double),
+                ("speed_wander_pct", C.c_double), ("wander_time_sec", C.c_double)]
+
+
 class NllSpec(C.Structure):
     _fields_ = [("wavelength_nm", C.c_double), ("na", C.c_double), ("n_imm", C.c_double), ("pixel_nm", C.c_double),
                 ("roi", C.c_int32), ("os", C.c_int32), ("pupil", C.c_int32), ("n_zern", C.c_int32),
@@ -135,11 +143,14 @@ SIGNATURES = {
                                          vp]),
     "iscu_render_frames": (C.c_int, [vp, vp, C.c_uint32, vp, C.c_uint32, C.POINTER(Camera), C.c_uint32, vp, vp]),
     "iscu_collect_emitters_dev": (C.c_int, [vp, C.c_int32, vp, C.c_uint32, vp, vp, C.c_int64, C.c_uint32,
-                                            C.c_double, C.c_double, vp, vp, vp, vp, vp, C.c_double, vp, C.c_uint32,
-                                            vp, vp, vp]),
+                                            C.c_double, C.c_double, vp, vp, vp, vp, vp, C.c_double, vp, vp,
+                                            C.c_uint32, vp, vp, vp]),
     "iscu_render_events": (C.c_int, [vp, C.c_int32, vp, C.c_uint32, vp, vp, C.c_int64, C.c_uint32, C.c_double,
                                      C.c_double, vp, vp, vp, vp, C.c_int32, C.c_double, C.POINTER(Camera),
                                      C.c_uint32, vp, vp, vp, vp]),
+    "iscu_drift_trajectory": (C.c_int, [C.c_int64, C.c_int64, C.c_double, C.POINTER(DriftSettings), vp]),
+    "iscu_illumination_field": (C.c_int, [C.c_uint32, C.c_uint32, C.c_int32, C.c_double, vp, f64p]),
+    "iscu_background_fade_scale": (C.c_double, [C.c_double, C.c_double]),
     "iscu_nll_model_create": (C.c_int, [vp, C.POINTER(NllSpec), C.POINTER(vp)]),
     "iscu_nll_model_destroy": (None, [vp]),
     "iscu_nll_model_info": (C.c_int, [vp, f64p, i32p]),

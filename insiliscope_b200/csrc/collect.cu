@@ -40,6 +40,7 @@ struct CollectArgs
    int nz[ISCU_MAX_KERNELS];
    double zStepNm[ISCU_MAX_KERNELS];
    iscu_emitter* out;
+   uint32_t* eventIndex;          // nullable: each kept emitter's event index (ground-truth rows)
    uint32_t maxOut;
    iscu_frame* frames;
    uint32_t* keptPerFrame;
@@ -58,10 +59,11 @@ __device__ __forceinline__ void Bucket(const CollectArgs& a, uint32_t f, uint32_
 
 // The emitter of candidate j in frame f, as CollectFrame computes it; false when the event is not splatted in the
 // frame (no overlap, below min photons, an empty kernel slot, an index outside the events).
-__device__ bool EmitterOf(const CollectArgs& a, uint32_t f, uint32_t j, iscu_emitter& em, bool& clamped)
+__device__ bool EmitterOf(const CollectArgs& a, uint32_t f, uint32_t j, iscu_emitter& em, bool& clamped,
+                          uint32_t& idx)
 {
    clamped = false;
-   const uint32_t idx = a.bucketIndex ? a.bucketIndex[j] : j;
+   idx = a.bucketIndex ? a.bucketIndex[j] : j;
    if (idx >= a.nEvents)
       return false;
    const iscu_blink_event e = a.events[idx];
@@ -151,7 +153,8 @@ __global__ void __launch_bounds__(kCT) CollectCountKernel(CollectArgs a)
       {
          iscu_emitter em;
          bool cl;
-         keep = EmitterOf(a, f, j, em, cl);
+         uint32_t idx;
+         keep = EmitterOf(a, f, j, em, cl, idx);
       }
       kept += static_cast<uint32_t>(__syncthreads_count(keep));
    }
@@ -230,9 +233,10 @@ __global__ void __launch_bounds__(kCT) CollectWriteKernel(CollectArgs a)
       const uint32_t j = c + threadIdx.x;
       bool keep = false, cl = false;
       iscu_emitter em;
+      uint32_t idx = 0;
       if (j < j1)
       {
-         keep = EmitterOf(a, f, j, em, cl);
+         keep = EmitterOf(a, f, j, em, cl, idx);
          clampedSum += cl ? 1ull : 0ull;
       }
       const unsigned ballot = __ballot_sync(0xffffffffu, keep);
@@ -250,7 +254,11 @@ __global__ void __launch_bounds__(kCT) CollectWriteKernel(CollectArgs a)
       {
          const uint32_t o = pos + base + __popc(ballot & ((1u << lane) - 1u));
          if (o < a.maxOut)
+         {
             a.out[o] = em;
+            if (a.eventIndex)
+               a.eventIndex[o] = idx;
+         }
       }
       pos += total;
       __syncthreads();
@@ -269,8 +277,8 @@ __global__ void __launch_bounds__(kCT) CollectWriteKernel(CollectArgs a)
 int LaunchCollect(iscu_ctx* ctx, int32_t slot, const iscu_blink_event* events, uint32_t nEvents,
                   const uint32_t* bucketIndex, const uint32_t* bucketStart, int64_t frame0, uint32_t nFrames,
                   double pixelNm, double perBlink, const double* driftX, const double* driftY, const double* globalZ,
-                  const double* bgScale, const float* illum, double minPhotons, iscu_emitter* out, uint32_t maxOut,
-                  iscu_frame* frames, uint32_t* nOut, int64_t* nClamped)
+                  const double* bgScale, const float* illum, double minPhotons, iscu_emitter* out,
+                  uint32_t* eventIndex, uint32_t maxOut, iscu_frame* frames, uint32_t* nOut, int64_t* nClamped)
 {
    if (nFrames == 0)
    {
@@ -303,6 +311,7 @@ int LaunchCollect(iscu_ctx* ctx, int32_t slot, const iscu_blink_event* events, u
       a.zStepNm[s] = k.zStepNm;
    }
    a.out = out;
+   a.eventIndex = eventIndex;
    a.maxOut = maxOut;
    a.frames = frames;
    ISCU_CK(ctx->dCollect.Reserve(static_cast<size_t>(nFrames) * sizeof(uint32_t)));
@@ -329,8 +338,9 @@ int iscu_collect_emitters_dev(iscu_ctx* ctx, int32_t slot, const iscu_blink_even
                               uint32_t n_frames, double pixel_size_nm, double photons_per_blink,
                               const double* drift_x_px_dev, const double* drift_y_px_dev,
                               const double* global_z_offset_um_dev, const double* bg_scale_dev, const float* illum_dev,
-                              double min_photons, iscu_emitter* out_dev, uint32_t max_out,
-                              iscu_frame* frames_out_dev, uint32_t* n_out_dev, int64_t* n_clamped_dev)
+                              double min_photons, iscu_emitter* out_dev, uint32_t* event_index_dev,
+                              uint32_t max_out, iscu_frame* frames_out_dev, uint32_t* n_out_dev,
+                              int64_t* n_clamped_dev)
 {
    if (!ctx || !n_out_dev || (n_frames && (!bucket_start_dev || !frames_out_dev)) || (n_events && !events_dev) ||
        (max_out && !out_dev))
@@ -347,8 +357,8 @@ int iscu_collect_emitters_dev(iscu_ctx* ctx, int32_t slot, const iscu_blink_even
       return Fail(ISCU_ERR_STATE, "no kernel stack in slot " + std::to_string(slot));
    return LaunchCollect(ctx, slot, events_dev, n_events, bucket_index_dev, bucket_start_dev, frame0, n_frames,
                         pixel_size_nm, photons_per_blink, drift_x_px_dev, drift_y_px_dev, global_z_offset_um_dev,
-                        bg_scale_dev, illum_dev, min_photons, out_dev, max_out, frames_out_dev, n_out_dev,
-                        n_clamped_dev);
+                        bg_scale_dev, illum_dev, min_photons, out_dev, event_index_dev, max_out, frames_out_dev,
+                        n_out_dev, n_clamped_dev);
 }
 
 int iscu_render_events(iscu_ctx* ctx, int32_t slot, const iscu_blink_event* events, uint32_t n_events,
@@ -425,8 +435,8 @@ int iscu_render_events(iscu_ctx* ctx, int32_t slot, const iscu_blink_event* even
    int rc = LaunchCollect(ctx, slot, ctx->dEvents.as<iscu_blink_event>(), n_events, dIdx, dBs, frame0, n_frames,
                           pixel_size_nm, photons_per_blink, devPerFrame[0], devPerFrame[1], devPerFrame[2],
                           devPerFrame[3], use_illum && ctx->haveIllum ? ctx->illum.as<float>() : nullptr,
-                          min_photons, ctx->dEmitters.as<iscu_emitter>(), nCand, ctx->dFrames.as<iscu_frame>(), dN,
-                          dClamped);
+                          min_photons, ctx->dEmitters.as<iscu_emitter>(), nullptr, nCand,
+                          ctx->dFrames.as<iscu_frame>(), dN, dClamped);
    if (rc != ISCU_OK)
       return rc;
    CameraView cv;

@@ -236,13 +236,14 @@ int LaunchCounterUniforms(iscu_ctx* ctx, uint32_t seed, uint32_t frame, uint32_t
                           uint32_t perPixel, double* out);
 int LaunchNoiseFrames(iscu_ctx* ctx, const float* photons, uint32_t nFrames, const uint32_t* frames,
                       const CameraView& cam, uint32_t seed, uint16_t* adu);
-// CollectFrameEmitters for a batch on the device (collect.cu): out gets the kept emitters (at most maxOut written),
+// CollectFrameEmitters for a batch on the device (collect.cu): out gets the kept emitters (at most maxOut written;
+// eventIndex, nullable, their events' indices),
 // frames the table, *nOut the count kept (may pass maxOut), *nClamped += the clamped z planes (nullable).
 int LaunchCollect(iscu_ctx* ctx, int32_t slot, const iscu_blink_event* events, uint32_t nEvents,
                   const uint32_t* bucketIndex, const uint32_t* bucketStart, int64_t frame0, uint32_t nFrames,
                   double pixelNm, double perBlink, const double* driftX, const double* driftY, const double* globalZ,
-                  const double* bgScale, const float* illum, double minPhotons, iscu_emitter* out, uint32_t maxOut,
-                  iscu_frame* frames, uint32_t* nOut, int64_t* nClamped);
+                  const double* bgScale, const float* illum, double minPhotons, iscu_emitter* out,
+                  uint32_t* eventIndex, uint32_t maxOut, iscu_frame* frames, uint32_t* nOut, int64_t* nClamped);
 // The render's timing marks of the current call (nullptr when timing is off or the stream is capturing): 4 events.
 cudaEvent_t* RenderMarks(iscu_ctx* ctx);
 // Emitter runs of the frames beyond nEmitters are cut at nEmitters.

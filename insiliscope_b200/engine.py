@@ -326,7 +326,8 @@ class Engine:
     def collect_emitters_dev(self, slot, events_dev, n_events, bucket_start_dev, n_frames, frame0, pixel_size_nm,
                              photons_per_blink, out_dev, frames_out_dev, n_out_dev, bucket_index_dev=None,
                              drift_x_px_dev=None, drift_y_px_dev=None, global_z_offset_um_dev=None,
-                             bg_scale_dev=None, illum_dev=None, min_photons=0.0, n_clamped_dev=None, sync=True):
+                             bg_scale_dev=None, illum_dev=None, min_photons=0.0, n_clamped_dev=None,
+                             event_index_dev=None, sync=True):
         """iscu_collect_emitters_dev on CUDA tensors (events: uint8 view of BLINK_EVENT_DTYPE records; out: of
         EMITTER_DTYPE records, its capacity the record count; frames_out: FRAME_DTYPE records; n_out: 1 uint32/int32)."""
         self._before(sync)
@@ -334,7 +335,8 @@ class Engine:
             self.h, int(slot), _ptr(events_dev), int(n_events), _ptr(bucket_index_dev), _ptr(bucket_start_dev),
             int(frame0), int(n_frames), float(pixel_size_nm), float(photons_per_blink), _ptr(drift_x_px_dev),
             _ptr(drift_y_px_dev), _ptr(global_z_offset_um_dev), _ptr(bg_scale_dev), _ptr(illum_dev),
-            float(min_photons), _ptr(out_dev), _n_records(out_dev), _ptr(frames_out_dev), _ptr(n_out_dev),
+            float(min_photons), _ptr(out_dev), _ptr(event_index_dev), _n_records(out_dev), _ptr(frames_out_dev),
+            _ptr(n_out_dev),
             _ptr(n_clamped_dev)))
         self._after(sync)
 
@@ -611,6 +613,48 @@ class WidefieldPlan:
                                       C.byref(cam) if cam is not None else None, seed, frame0,
                                       _ptr(image) if want_image else None, _ptr(adu) if cam is not None else None))
         return (image if want_image else None), (adu if camera is not None else None)
+
+
+@dataclass
+class DriftSettings:
+    """sim::DriftSettings (Drift.h:57-79)."""
+    xy_nm_per_sqrt_sec: float = 0.0
+    z_nm_per_sqrt_sec: float = 0.0
+    xy_speed_nm_per_sec: float = 0.0
+    z_speed_nm_per_sec: float = 0.0
+    xy_angle_deg: float = -1.0
+    z_direction: int = 0
+    angle_wander_deg: float = 180.0
+    z_angle_wander_deg: float = 90.0
+    speed_wander_pct: float = 0.0
+    wander_time_sec: float = 60.0
+
+    def c(self):
+        from ._abi import DriftSettings as _D
+        d = _D()
+        for k in self.__dataclass_fields__:
+            setattr(d, k, getattr(self, k))
+        return d
+
+
+def drift_trajectory(random_seed: int, frames: int, frame_sec: float, settings: DriftSettings) -> np.ndarray:
+    """The sample drift (frames, 3) nm (DriftTrajectory, Drift.cpp:114-124): the reference's bits."""
+    out = np.zeros((max(0, frames), 3), np.float64)
+    s = settings.c()
+    check(load().iscu_drift_trajectory(int(random_seed), int(frames), float(frame_sec), C.byref(s), _ptr(out)))
+    return out
+
+
+def illumination_field(width: int, height: int, profile: int, fwhm_pct: float):
+    """(field (h, w) float32 with peak 1, or None for flat; mean factor) (BuildIlluminationField)."""
+    out = np.empty((height, width), np.float32)
+    mf = C.c_double()
+    check(load().iscu_illumination_field(width, height, int(profile), float(fwhm_pct), _ptr(out), C.byref(mf)))
+    return (None if profile == 0 else out), mf.value
+
+
+def background_fade_scale(t: float, decay: float) -> float:
+    return float(load().iscu_background_fade_scale(float(t), float(decay)))
 
 
 def frames_table(counts, frame_ids=None, bg_scales=None):

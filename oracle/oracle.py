@@ -198,6 +198,11 @@ class Reference:
         L.ref_render_movie_groups.argtypes = [vp, C.c_int, vp, u32, u32, u32, u32, u32, f64, f64, f64, vp, vp, vp, vp,
                                               u32, vp, vp]
         L.ref_render_movie_groups.restype = f64
+        L.ref_drift_trajectory.argtypes = [C.c_long, C.c_long, f64, vp, C.c_int, vp]
+        L.ref_illumination_field.argtypes = [C.c_uint, C.c_uint, C.c_int, f64, vp, vp]
+        L.ref_illumination_field.restype = C.c_size_t
+        L.ref_background_fade_scale.argtypes = [f64, f64]
+        L.ref_background_fade_scale.restype = f64
         self.L = L
 
     def set_threads(self, n):
@@ -265,6 +270,24 @@ class Reference:
                                            per_blink, bg, C.byref(cam), _p(f(offset)), _p(f(gain)),
                                            _p(f(read_noise)), seed, _p(ph), _p(adu))
         return t, ph, adu
+
+    def drift_trajectory(self, seed, frames, frame_sec, s):
+        """sim::DriftTrajectory; s: an insiliscope_b200 DriftSettings. (frames, 3) nm."""
+        p = np.array([s.xy_nm_per_sqrt_sec, s.z_nm_per_sqrt_sec, s.xy_speed_nm_per_sec, s.z_speed_nm_per_sec,
+                      s.xy_angle_deg, s.angle_wander_deg, s.z_angle_wander_deg, s.speed_wander_pct,
+                      s.wander_time_sec], np.float64)
+        out = np.zeros((frames, 3), np.float64)
+        self.L.ref_drift_trajectory(seed, frames, frame_sec, _p(p), s.z_direction, _p(out))
+        return out
+
+    def illumination_field(self, w, h, profile, fwhm_pct):
+        out = np.zeros((h, w), np.float32)
+        mf = C.c_double(1.0)
+        n = self.L.ref_illumination_field(w, h, profile, fwhm_pct, _p(out), C.byref(mf))
+        return (out if n else None), mf.value
+
+    def background_fade_scale(self, t, decay):
+        return self.L.ref_background_fade_scale(t, decay)
 
     def kernel(self, req=None, planes=None, os_=4, z_step_nm=25.0, interp=2):
         return RefKernel(self, req, planes, os_, z_step_nm, interp)

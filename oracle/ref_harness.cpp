@@ -8,7 +8,9 @@
 //   CollectGpuEmitters (:219), ApplyNoiseChain (SMLMNoise.cpp:142), the camera maps (SMLMNoise.cpp:89-140), the
 //   counter RNG (SMLMCounterRng.h, core/src/rng.h), and a movie loop shaped like FluorescenceMovie::Render's
 //   (ScopeMovie.cpp:7267, :7649: frames in parallel on the reference's own thread pool, ParallelFor).
+#include "Drift.h"
 #include "PsfGeneratorBridge.h"
+#include "SMLMBackground.h"
 #include "Parallel.h"
 #include "SMLMCounterRng.h"
 #include "SMLMNoise.h"
@@ -469,5 +471,39 @@ double ref_render_movie_groups(void* const* caches, int nGroups, const iscu_blin
    });
    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
+
+// sim::DriftTrajectory with the given settings: xyz[3 f + (0, 1, 2)] nm.
+void ref_drift_trajectory(long seed, long frames, double frameSec, const double* p, int zDirection, double* xyz)
+{
+   sim::DriftSettings s;
+   s.xyNmPerSqrtSec = p[0];
+   s.zNmPerSqrtSec = p[1];
+   s.xySpeedNmPerSec = p[2];
+   s.zSpeedNmPerSec = p[3];
+   s.xyAngleDeg = p[4];
+   s.zDirection = zDirection;
+   s.angleWanderDeg = p[5];
+   s.zAngleWanderDeg = p[6];
+   s.speedWanderPct = p[7];
+   s.wanderTimeSec = p[8];
+   const std::vector<sim::DriftNm> t = sim::DriftTrajectory(seed, frames, frameSec, s);
+   for (size_t f = 0; f < t.size(); ++f)
+   {
+      xyz[3 * f] = t[f].x;
+      xyz[3 * f + 1] = t[f].y;
+      xyz[3 * f + 2] = t[f].z;
+   }
+}
+
+// sim::BuildIlluminationField: returns the number of floats written (0 for flat).
+size_t ref_illumination_field(unsigned w, unsigned h, int profile, double fwhmPct, float* out, double* meanFactor)
+{
+   const std::vector<float> f =
+      sim::BuildIlluminationField(w, h, static_cast<sim::IllumProfile>(profile), fwhmPct, meanFactor);
+   std::memcpy(out, f.data(), f.size() * sizeof(float));
+   return f.size();
+}
+
+double ref_background_fade_scale(double t, double decay) { return sim::BackgroundFadeScale(t, decay); }
 
 } // extern "C"

@@ -55,14 +55,16 @@ def _dev_collect(engine, slot, ev, bi, bs, frame0, **kw):
     d_fr = torch.zeros(nf * FRAME_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
     d_n = torch.zeros(1, dtype=torch.int32, device="cuda")
     d_cl = torch.zeros(1, dtype=torch.int64, device="cuda")
+    d_ix = torch.zeros(cap, dtype=torch.int32, device="cuda")
     per = {k: t(kw.get(k), np.float64) for k in ("drift_x_px", "drift_y_px", "global_z_offset_um", "bg_scale")}
     engine.collect_emitters_dev(slot, d_ev, len(ev), t(bs), nf, frame0, PX, 2000.0, d_out, d_fr, d_n,
                                 bucket_index_dev=t(bi), drift_x_px_dev=per["drift_x_px"],
                                 drift_y_px_dev=per["drift_y_px"], global_z_offset_um_dev=per["global_z_offset_um"],
                                 bg_scale_dev=per["bg_scale"], illum_dev=t(kw.get("illum"), np.float32),
-                                min_photons=kw.get("min_photons", 0.0), n_clamped_dev=d_cl)
+                                min_photons=kw.get("min_photons", 0.0), n_clamped_dev=d_cl, event_index_dev=d_ix)
     n = int(d_n.item())
     out = d_out.cpu().numpy().view(EMITTER_DTYPE)
+    _dev_collect.last_index = d_ix.cpu().numpy()[:min(n, cap)]
     return out[:min(n, cap)], d_fr.cpu().numpy().view(FRAME_DTYPE), n, int(d_cl.item())
 
 
@@ -86,6 +88,14 @@ def test_device_collection_matches_host(engine, kernels, slot, extras):
     assert got_e.tobytes() == want_e.tobytes()
     assert got_f.tobytes() == want_f.tobytes()
     assert cl == want_cl
+    # the ground-truth list: each emitter's event, in the frame's event order
+    ix = _dev_collect.last_index
+    for f in range(F):
+        lo, hi = got_f["em_start"][f], got_f["em_start"][f] + got_f["em_count"][f]
+        cand = bi[bs[f]:bs[f + 1]]
+        assert np.all(np.isin(ix[lo:hi], cand)) and np.all(np.diff(np.searchsorted(cand, ix[lo:hi])) > 0)
+    if not extras:
+        assert np.allclose(got_e["x_px"], ev["x_um"][ix] * 1000.0 / PX)
 
 
 def test_device_collection_overflow_reports_count(engine, kernels):
