@@ -372,6 +372,24 @@ int iscu_render_events(iscu_ctx* ctx, int32_t slot, const iscu_blink_event* even
                        int32_t use_illum, double min_photons, const iscu_camera* cam, uint32_t seed, float* photons,
                        uint16_t* adu, uint32_t* n_emitters, int64_t* n_clamped);
 
+/* iscu_render_events in two halves, so that the copies of one batch overlap the render of another (the movie engine's
+ * frame loop pipelined across batches). _async enqueues the batch in I/O slot io_slot (0 .. ISCU_EVENT_IO_SLOTS - 1,
+ * each with its own device staging) and returns at once: the events go in on the context's upload stream, the
+ * collection, render and noise run on its stream, the frames come out on its download stream. Until
+ * iscu_render_events_wait(ctx, io_slot, ...) returns, the host inputs must stay unchanged and the outputs unread;
+ * the wait blocks until the batch's frames are in the host buffers and reports its counts as iscu_render_events does.
+ * A slot holds one batch: _async on a slot not yet waited for fails with ISCU_ERR_STATE, and so does a wait on an
+ * idle slot. Page-locked host buffers let the copies run beside the kernels (pageable ones are copied synchronously).
+ * A batch that fails to enqueue leaves its slot idle. */
+#define ISCU_EVENT_IO_SLOTS 4
+int iscu_render_events_async(iscu_ctx* ctx, int32_t io_slot, int32_t slot, const iscu_blink_event* events,
+                             uint32_t n_events, const uint32_t* bucket_index, const uint32_t* bucket_start,
+                             int64_t frame0, uint32_t n_frames, double pixel_size_nm, double photons_per_blink,
+                             const double* drift_x_px, const double* drift_y_px, const double* global_z_offset_um,
+                             const double* bg_scale, int32_t use_illum, double min_photons, const iscu_camera* cam,
+                             uint32_t seed, float* photons, uint16_t* adu);
+int iscu_render_events_wait(iscu_ctx* ctx, int32_t io_slot, uint32_t* n_emitters, int64_t* n_clamped);
+
 /* ---------------------------------------------------------------- per-movie host models ----------------------- */
 
 /* sim::DriftSettings (Drift.h:57-79). */

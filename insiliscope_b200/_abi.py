@@ -148,6 +148,10 @@ SIGNATURES = {
     "iscu_render_events": (C.c_int, [vp, C.c_int32, vp, C.c_uint32, vp, vp, C.c_int64, C.c_uint32, C.c_double,
                                      C.c_double, vp, vp, vp, vp, C.c_int32, C.c_double, C.POINTER(Camera),
                                      C.c_uint32, vp, vp, vp, vp]),
+    "iscu_render_events_async": (C.c_int, [vp, C.c_int32, C.c_int32, vp, C.c_uint32, vp, vp, C.c_int64, C.c_uint32,
+                                           C.c_double, C.c_double, vp, vp, vp, vp, C.c_int32, C.c_double,
+                                           C.POINTER(Camera), C.c_uint32, vp, vp]),
+    "iscu_render_events_wait": (C.c_int, [vp, C.c_int32, u32p, C.POINTER(C.c_int64)]),
     "iscu_drift_trajectory": (C.c_int, [C.c_int64, C.c_int64, C.c_double, C.POINTER(DriftSettings), vp]),
     "iscu_illumination_field": (C.c_int, [C.c_uint32, C.c_uint32, C.c_int32, C.c_double, vp, f64p]),
     "iscu_background_fade_scale": (C.c_double, [C.c_double, C.c_double]),

@@ -247,11 +247,20 @@ void iscu_destroy(iscu_ctx* ctx)
       return;
    cudaSetDevice(ctx->device);
    cudaStreamSynchronize(ctx->stream);
+   for (cudaStream_t c : {ctx->upload, ctx->download})
+      if (c)
+         cudaStreamSynchronize(c);
    for (cudaEvent_t e : ctx->renderMarks)
       cudaEventDestroy(e);
-   cudaStream_t s = ctx->stream;
+   for (iscu::EventIo& io : ctx->eventIo)
+      for (cudaEvent_t e : {io.uploaded, io.rendered, io.downloaded})
+         if (e)
+            cudaEventDestroy(e);
+   cudaStream_t streams[3] = {ctx->stream, ctx->upload, ctx->download};
    delete ctx;
-   cudaStreamDestroy(s);
+   for (cudaStream_t c : streams)
+      if (c)
+         cudaStreamDestroy(c);
 }
 
 int iscu_synchronize(iscu_ctx* ctx)
@@ -260,6 +269,9 @@ int iscu_synchronize(iscu_ctx* ctx)
       return Fail(ISCU_ERR_ARG, "null context");
    Lock l(ctx);
    ISCU_CK(cudaStreamSynchronize(ctx->stream));
+   for (cudaStream_t c : {ctx->upload, ctx->download})
+      if (c)
+         ISCU_CK(cudaStreamSynchronize(c));
    ISCU_CK(cudaGetLastError());
    return ISCU_OK;
 }

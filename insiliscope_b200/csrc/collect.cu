@@ -327,6 +327,143 @@ int LaunchCollect(iscu_ctx* ctx, int32_t slot, const iscu_blink_event* events, u
    return ISCU_OK;
 }
 
+
+// The event render of one batch, enqueued in I/O slot io (the iscu_render_events[_async] contract): host events,
+// bucket and per-frame arrays up on the upload stream, CollectFrameEmitters + render + noise on the context's stream,
+// frames and counts down on the download stream. Returns with the work in flight; io.busy marks it.
+int EnqueueRenderEvents(iscu_ctx* ctx, EventIo& io, int32_t slot, const iscu_blink_event* events, uint32_t nEvents,
+                        const uint32_t* bucketIndex, const uint32_t* bucketStart, int64_t frame0, uint32_t nFrames,
+                        double pixelNm, double perBlink, const double* driftX, const double* driftY,
+                        const double* globalZ, const double* bgScale, int32_t useIllum, double minPhotons,
+                        const iscu_camera* cam, uint32_t seed, float* photons, uint16_t* adu)
+{
+   if ((nFrames && !bucketStart) || (nEvents && !events))
+      return Fail(ISCU_ERR_ARG, "null argument");
+   if (cam && !adu)
+      return Fail(ISCU_ERR_ARG, "a camera needs an ADU output");
+   if (slot < -1 || slot >= ISCU_MAX_KERNELS)
+      return Fail(ISCU_ERR_ARG, "kernel slot out of range (-1..3)");
+   if (nFrames > 65535)
+      return Fail(ISCU_ERR_LIMIT, "at most 65535 frames per call");
+   if (io.busy)
+      return Fail(ISCU_ERR_STATE, "the I/O slot's batch has not been waited for");
+   if (!ctx->haveStatic)
+      return Fail(ISCU_ERR_STATE, "no camera statics (iscu_set_static)");
+   if (slot >= 0 && !ctx->kernels[slot].valid)
+      return Fail(ISCU_ERR_STATE, "no kernel stack in slot " + std::to_string(slot));
+   cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+   ISCU_CK(cudaStreamIsCapturing(ctx->stream, &capturing));
+   if (capturing != cudaStreamCaptureStatusNone)
+      return Fail(ISCU_ERR_STATE, "the event render copies from host memory: not inside a stream capture");
+   for (uint32_t f = 0; f < nFrames; ++f)
+      if (bucketStart[f + 1] < bucketStart[f])
+         return Fail(ISCU_ERR_ARG, "bucket offsets must not decrease");
+   const uint32_t nIdx = nFrames ? bucketStart[nFrames] : 0;   // the index list (or the events) covers [0, nIdx)
+   const uint32_t nCand = nFrames ? bucketStart[nFrames] - bucketStart[0] : 0;
+   if (!bucketIndex && nIdx > nEvents)
+      return Fail(ISCU_ERR_ARG, "buckets reach past the events");
+   if (!ctx->upload)
+      ISCU_CK(cudaStreamCreateWithFlags(&ctx->upload, cudaStreamNonBlocking));
+   if (!ctx->download)
+      ISCU_CK(cudaStreamCreateWithFlags(&ctx->download, cudaStreamNonBlocking));
+   for (cudaEvent_t* e : {&io.uploaded, &io.rendered, &io.downloaded})
+      if (!*e)
+         ISCU_CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+   ISCU_CK(io.hostCounts.Reserve(16));
+   // the slot's device staging: events, bucket arrays, per-frame arrays, the batch's emitters and frames, the outputs
+   const size_t px = static_cast<size_t>(ctx->width) * ctx->height * nFrames;
+   const size_t evB = static_cast<size_t>(nEvents) * sizeof(iscu_blink_event);
+   const size_t idxB = bucketIndex ? static_cast<size_t>(nIdx) * sizeof(uint32_t) : 0;
+   const size_t bsB = (static_cast<size_t>(nFrames) + 1) * sizeof(uint32_t);
+   const size_t perFrameB = static_cast<size_t>(nFrames) * sizeof(double);
+   const size_t perFrameAt = (idxB + bsB + 7) & ~size_t(7);
+   ISCU_CK(io.events.Reserve(std::max<size_t>(evB, 16)));
+   ISCU_CK(io.buckets.Reserve(perFrameAt + 4 * perFrameB + 16));
+   ISCU_CK(io.emitters.Reserve(std::max<size_t>(static_cast<size_t>(nCand) * sizeof(iscu_emitter), 16)));
+   ISCU_CK(io.frames.Reserve(std::max<size_t>(static_cast<size_t>(nFrames) * sizeof(iscu_frame), 16)));
+   ISCU_CK(io.counts.Reserve(16));
+   if (photons)
+      ISCU_CK(io.photons.Reserve(std::max<size_t>(px * sizeof(float), 16)));
+   if (adu)
+      ISCU_CK(io.adu.Reserve(std::max<size_t>(px * sizeof(uint16_t), 16)));
+   char* b = io.buckets.as<char>();
+   uint32_t* dIdx = bucketIndex ? reinterpret_cast<uint32_t*>(b) : nullptr;
+   uint32_t* dBs = reinterpret_cast<uint32_t*>(b + idxB);
+   double* dPerFrame = reinterpret_cast<double*>(b + perFrameAt);
+   const double* hostPerFrame[4] = {driftX, driftY, globalZ, bgScale};
+   const double* devPerFrame[4] = {nullptr, nullptr, nullptr, nullptr};
+   uint32_t* dN = io.counts.as<uint32_t>();
+   int64_t* dClamped = reinterpret_cast<int64_t*>(io.counts.as<char>() + 8);
+
+   // upload: the slot's buffers are free (its last batch was waited for), so the copies need wait on nothing
+   cudaStream_t up = ctx->upload;
+   if (evB)
+      ISCU_CK(cudaMemcpyAsync(io.events.p, events, evB, cudaMemcpyHostToDevice, up));
+   if (idxB)
+      ISCU_CK(cudaMemcpyAsync(dIdx, bucketIndex, idxB, cudaMemcpyHostToDevice, up));
+   if (nFrames)
+      ISCU_CK(cudaMemcpyAsync(dBs, bucketStart, bsB, cudaMemcpyHostToDevice, up));
+   for (int k = 0; k < 4; ++k)
+      if (hostPerFrame[k] && nFrames)
+      {
+         ISCU_CK(cudaMemcpyAsync(dPerFrame + static_cast<size_t>(k) * nFrames, hostPerFrame[k], perFrameB,
+                                 cudaMemcpyHostToDevice, up));
+         devPerFrame[k] = dPerFrame + static_cast<size_t>(k) * nFrames;
+      }
+   ISCU_CK(cudaMemsetAsync(io.counts.p, 0, 16, up));
+   ISCU_CK(cudaEventRecord(io.uploaded, up));
+
+   // collection, render and noise on the context's stream, after the upload and after everything enqueued before
+   cudaStream_t s = ctx->stream;
+   ISCU_CK(cudaStreamWaitEvent(s, io.uploaded, 0));
+   if (nFrames)
+   {
+      int rc = LaunchCollect(ctx, slot, io.events.as<iscu_blink_event>(), nEvents, dIdx, dBs, frame0, nFrames,
+                             pixelNm, perBlink, devPerFrame[0], devPerFrame[1], devPerFrame[2], devPerFrame[3],
+                             useIllum && ctx->haveIllum ? ctx->illum.as<float>() : nullptr, minPhotons,
+                             io.emitters.as<iscu_emitter>(), nullptr, nCand, io.frames.as<iscu_frame>(), dN,
+                             dClamped);
+      if (rc != ISCU_OK)
+         return rc;
+      CameraView cv;
+      if (cam)
+         cv = MakeCameraView(*cam);
+      rc = LaunchRenderFrames(ctx, io.emitters.as<iscu_emitter>(), nCand, io.frames.as<iscu_frame>(), nFrames,
+                              cam ? &cv : nullptr, seed, photons ? io.photons.as<float>() : nullptr,
+                              adu ? io.adu.as<uint16_t>() : nullptr);
+      if (rc != ISCU_OK)
+         return rc;
+   }
+   ISCU_CK(cudaEventRecord(io.rendered, s));
+
+   // download: the frames and the counts, after the render
+   cudaStream_t down = ctx->download;
+   ISCU_CK(cudaStreamWaitEvent(down, io.rendered, 0));
+   if (photons && px)
+      ISCU_CK(cudaMemcpyAsync(photons, io.photons.p, px * sizeof(float), cudaMemcpyDeviceToHost, down));
+   if (adu && px)
+      ISCU_CK(cudaMemcpyAsync(adu, io.adu.p, px * sizeof(uint16_t), cudaMemcpyDeviceToHost, down));
+   ISCU_CK(cudaMemcpyAsync(io.hostCounts.p, io.counts.p, 16, cudaMemcpyDeviceToHost, down));
+   ISCU_CK(cudaEventRecord(io.downloaded, down));
+   io.busy = true;
+   return ISCU_OK;
+}
+
+// Waits for slot io's batch; its counts into *nEmitters (nullable) and += *nClamped (nullable). The slot is idle after.
+int WaitRenderEvents(EventIo& io, uint32_t* nEmitters, int64_t* nClamped)
+{
+   if (!io.busy)
+      return Fail(ISCU_ERR_STATE, "no batch in the I/O slot");
+   io.busy = false;
+   ISCU_CK(cudaEventSynchronize(io.downloaded));
+   const uint64_t* c = io.hostCounts.as<uint64_t>();
+   if (nEmitters)
+      *nEmitters = static_cast<uint32_t>(c[0]);
+   if (nClamped)
+      *nClamped += static_cast<int64_t>(c[1]);
+   return ISCU_OK;
+}
+
 } // namespace iscu
 
 using namespace iscu;
@@ -368,97 +505,46 @@ int iscu_render_events(iscu_ctx* ctx, int32_t slot, const iscu_blink_event* even
                        int32_t use_illum, double min_photons, const iscu_camera* cam, uint32_t seed, float* photons,
                        uint16_t* adu, uint32_t* n_emitters, int64_t* n_clamped)
 {
-   if (!ctx || (n_frames && !bucket_start) || (n_events && !events))
+   if (!ctx)
       return Fail(ISCU_ERR_ARG, "null argument");
-   if (cam && !adu)
-      return Fail(ISCU_ERR_ARG, "a camera needs an ADU output");
-   if (slot < -1 || slot >= ISCU_MAX_KERNELS)
-      return Fail(ISCU_ERR_ARG, "kernel slot out of range (-1..3)");
-   if (n_frames > 65535)
-      return Fail(ISCU_ERR_LIMIT, "at most 65535 frames per call");
    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
    ClearError();
-   if (!ctx->haveStatic)
-      return Fail(ISCU_ERR_STATE, "no camera statics (iscu_set_static)");
-   if (slot >= 0 && !ctx->kernels[slot].valid)
-      return Fail(ISCU_ERR_STATE, "no kernel stack in slot " + std::to_string(slot));
-   if (n_frames == 0)
-   {
-      if (n_emitters)
-         *n_emitters = 0;
-      return ISCU_OK;
-   }
-   for (uint32_t f = 0; f < n_frames; ++f)
-      if (bucket_start[f + 1] < bucket_start[f])
-         return Fail(ISCU_ERR_ARG, "bucket offsets must not decrease");
-   const uint32_t nIdx = bucket_start[n_frames];   // bucket_index (or the events) covers [0, bucket_start[n_frames])
-   const uint32_t nCand = bucket_start[n_frames] - bucket_start[0];
-   if (!bucket_index && nIdx > n_events)
-      return Fail(ISCU_ERR_ARG, "buckets reach past the events");
-   // device staging: events, bucket arrays, per-frame arrays, the batch's emitters and frames, the outputs
-   const size_t px = static_cast<size_t>(ctx->width) * ctx->height * n_frames;
-   const size_t evB = static_cast<size_t>(n_events) * sizeof(iscu_blink_event);
-   const size_t idxB = bucket_index ? static_cast<size_t>(nIdx) * sizeof(uint32_t) : 0;
-   const size_t bsB = (static_cast<size_t>(n_frames) + 1) * sizeof(uint32_t);
-   const size_t perFrameB = static_cast<size_t>(n_frames) * sizeof(double);
-   ISCU_CK(ctx->dEvents.Reserve(std::max<size_t>(evB, 16)));
-   ISCU_CK(ctx->dBuckets.Reserve(idxB + bsB + 4 * perFrameB + 16));
-   ISCU_CK(ctx->dEmitters.Reserve(std::max<size_t>(static_cast<size_t>(nCand) * sizeof(iscu_emitter), 16)));
-   ISCU_CK(ctx->dFrames.Reserve(static_cast<size_t>(n_frames) * sizeof(iscu_frame)));
-   ISCU_CK(ctx->dCounts.Reserve(16));
-   if (photons)
-      ISCU_CK(ctx->dPhotons.Reserve(px * sizeof(float)));
-   if (adu)
-      ISCU_CK(ctx->dAdu.Reserve(px * sizeof(uint16_t)));
-   char* b = ctx->dBuckets.as<char>();
-   uint32_t* dIdx = bucket_index ? reinterpret_cast<uint32_t*>(b) : nullptr;
-   uint32_t* dBs = reinterpret_cast<uint32_t*>(b + idxB);
-   double* dPerFrame = reinterpret_cast<double*>(b + ((idxB + bsB + 7) & ~size_t(7)));
-   const double* hostPerFrame[4] = {drift_x_px, drift_y_px, global_z_offset_um, bg_scale};
-   const double* devPerFrame[4] = {nullptr, nullptr, nullptr, nullptr};
-   cudaStream_t s = ctx->stream;
-   if (evB)
-      ISCU_CK(cudaMemcpyAsync(ctx->dEvents.p, events, evB, cudaMemcpyHostToDevice, s));
-   if (idxB)
-      ISCU_CK(cudaMemcpyAsync(dIdx, bucket_index, idxB, cudaMemcpyHostToDevice, s));
-   ISCU_CK(cudaMemcpyAsync(dBs, bucket_start, bsB, cudaMemcpyHostToDevice, s));
-   for (int k = 0; k < 4; ++k)
-      if (hostPerFrame[k])
-      {
-         ISCU_CK(cudaMemcpyAsync(dPerFrame + static_cast<size_t>(k) * n_frames, hostPerFrame[k], perFrameB,
-                                 cudaMemcpyHostToDevice, s));
-         devPerFrame[k] = dPerFrame + static_cast<size_t>(k) * n_frames;
-      }
-   uint32_t* dN = ctx->dCounts.as<uint32_t>();
-   int64_t* dClamped = reinterpret_cast<int64_t*>(ctx->dCounts.as<char>() + 8);
-   ISCU_CK(cudaMemsetAsync(ctx->dCounts.p, 0, 16, s));
-   int rc = LaunchCollect(ctx, slot, ctx->dEvents.as<iscu_blink_event>(), n_events, dIdx, dBs, frame0, n_frames,
-                          pixel_size_nm, photons_per_blink, devPerFrame[0], devPerFrame[1], devPerFrame[2],
-                          devPerFrame[3], use_illum && ctx->haveIllum ? ctx->illum.as<float>() : nullptr,
-                          min_photons, ctx->dEmitters.as<iscu_emitter>(), nullptr, nCand,
-                          ctx->dFrames.as<iscu_frame>(), dN, dClamped);
+   EventIo& io = ctx->eventIo[ISCU_EVENT_IO_SLOTS];   // the blocking call's own slot
+   int rc = EnqueueRenderEvents(ctx, io, slot, events, n_events, bucket_index, bucket_start, frame0, n_frames,
+                                pixel_size_nm, photons_per_blink, drift_x_px, drift_y_px, global_z_offset_um,
+                                bg_scale, use_illum, min_photons, cam, seed, photons, adu);
    if (rc != ISCU_OK)
       return rc;
-   CameraView cv;
-   if (cam)
-      cv = MakeCameraView(*cam);
-   rc = LaunchRenderFrames(ctx, ctx->dEmitters.as<iscu_emitter>(), nCand, ctx->dFrames.as<iscu_frame>(), n_frames,
-                           cam ? &cv : nullptr, seed, photons ? ctx->dPhotons.as<float>() : nullptr,
-                           adu ? ctx->dAdu.as<uint16_t>() : nullptr);
-   if (rc != ISCU_OK)
-      return rc;
-   if (photons)
-      ISCU_CK(cudaMemcpyAsync(photons, ctx->dPhotons.p, px * sizeof(float), cudaMemcpyDeviceToHost, s));
-   if (adu)
-      ISCU_CK(cudaMemcpyAsync(adu, ctx->dAdu.p, px * sizeof(uint16_t), cudaMemcpyDeviceToHost, s));
-   uint64_t counts[2] = {0, 0};
-   ISCU_CK(cudaMemcpyAsync(counts, ctx->dCounts.p, 16, cudaMemcpyDeviceToHost, s));
-   ISCU_CK(cudaStreamSynchronize(s));
-   if (n_emitters)
-      *n_emitters = static_cast<uint32_t>(counts[0]);
-   if (n_clamped)
-      *n_clamped += static_cast<int64_t>(counts[1]);
-   return ISCU_OK;
+   return WaitRenderEvents(io, n_emitters, n_clamped);
+}
+
+int iscu_render_events_async(iscu_ctx* ctx, int32_t io_slot, int32_t slot, const iscu_blink_event* events,
+                             uint32_t n_events, const uint32_t* bucket_index, const uint32_t* bucket_start,
+                             int64_t frame0, uint32_t n_frames, double pixel_size_nm, double photons_per_blink,
+                             const double* drift_x_px, const double* drift_y_px, const double* global_z_offset_um,
+                             const double* bg_scale, int32_t use_illum, double min_photons, const iscu_camera* cam,
+                             uint32_t seed, float* photons, uint16_t* adu)
+{
+   if (!ctx)
+      return Fail(ISCU_ERR_ARG, "null argument");
+   if (io_slot < 0 || io_slot >= ISCU_EVENT_IO_SLOTS)
+      return Fail(ISCU_ERR_ARG, "I/O slot out of range (0..3)");
+   std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+   ClearError();
+   return EnqueueRenderEvents(ctx, ctx->eventIo[io_slot], slot, events, n_events, bucket_index, bucket_start,
+                              frame0, n_frames, pixel_size_nm, photons_per_blink, drift_x_px, drift_y_px,
+                              global_z_offset_um, bg_scale, use_illum, min_photons, cam, seed, photons, adu);
+}
+
+int iscu_render_events_wait(iscu_ctx* ctx, int32_t io_slot, uint32_t* n_emitters, int64_t* n_clamped)
+{
+   if (!ctx)
+      return Fail(ISCU_ERR_ARG, "null argument");
+   if (io_slot < 0 || io_slot >= ISCU_EVENT_IO_SLOTS)
+      return Fail(ISCU_ERR_ARG, "I/O slot out of range (0..3)");
+   std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+   ClearError();
+   return WaitRenderEvents(ctx->eventIo[io_slot], n_emitters, n_clamped);
 }
 
 } // extern "C"

@@ -181,6 +181,17 @@ struct ContribScratch
    DevBuf rec, grec, keys, list, contrib, ctr;
 };
 
+// One I/O slot of the event render (iscu_render_events[_async]): the batch's device staging (events, bucket and
+// per-frame arrays, the collected emitters and frames, the counts, the frames rendered), its counts read back into
+// page-locked memory, and the events ordering upload -> render -> download.
+struct EventIo
+{
+   bool busy = false;              // enqueued, not yet waited for
+   DevBuf events, buckets, emitters, frames, counts, photons, adu;
+   PinnedBuf hostCounts;           // {n kept (uint32 in a uint64), n clamped (int64)}
+   cudaEvent_t uploaded = nullptr, rendered = nullptr, downloaded = nullptr;
+};
+
 } // namespace iscu
 
 // ------------------------------------------------------------------ the context
@@ -210,8 +221,10 @@ struct iscu_ctx
    std::vector<float> illumHost;   // the illumination field, for host-side emitter collection
    // staging for the host-pointer entry points
    iscu::DevBuf dEmitters, dFrames, dPhotons, dAdu, dExtras, dScratch;
-   iscu::DevBuf dEvents, dBuckets, dCounts, dCollect;   // device emitter collection
-   iscu::PinnedBuf hIn, hOut;
+   iscu::DevBuf dCollect;          // device emitter collection: kept emitters per frame
+   // the event render's I/O slots (the last one is the blocking call's) and its copy streams (created on first use)
+   iscu::EventIo eventIo[ISCU_EVENT_IO_SLOTS + 1];
+   cudaStream_t upload = nullptr, download = nullptr;
    iscu::StaticView Static() const
    {
       iscu::StaticView s;

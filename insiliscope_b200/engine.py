@@ -158,14 +158,16 @@ class Engine:
         self.device = device
         self.width = self.height = 0
         self._plans = weakref.WeakSet()
+        self._pending_io = {}   # I/O slot -> the host arrays of its enqueued event-render batch
 
     def close(self):
         """Destroys the context, after the plans made on it (a plan must not outlive its context)."""
         if self.h:
             for p in list(self._plans):
                 p.close()
-            self.lib.iscu_destroy(self.h)
+            self.lib.iscu_destroy(self.h)   # waits for the copies in flight first
             self.h = None
+            self._pending_io = {}
 
     def _before(self, sync):
         if sync:
@@ -340,6 +342,29 @@ class Engine:
             _ptr(n_clamped_dev)))
         self._after(sync)
 
+    def _event_batch(self, events, bucket_start, camera, bucket_index, drift_x_px, drift_y_px, global_z_offset_um,
+                     bg_scale, want_photons, adu_out, photons_out):
+        """The host arrays of one event-render batch (contiguous, the ABI's dtypes) and its outputs."""
+        events = np.ascontiguousarray(events, dtype=BLINK_EVENT_DTYPE)
+        bs = np.ascontiguousarray(bucket_start, dtype=np.uint32)
+        nf = len(bs) - 1
+        bi = None if bucket_index is None else np.ascontiguousarray(bucket_index, dtype=np.uint32)
+        f64 = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+        per_frame = tuple(f64(a) for a in (drift_x_px, drift_y_px, global_z_offset_um, bg_scale))
+        for a in per_frame:
+            if a is not None and len(a) < nf:
+                raise ValueError("a per-frame array is shorter than the batch's frames")
+        shape = (nf, self.height, self.width)
+        adu = None
+        if camera is not None:
+            adu = adu_out if adu_out is not None else np.empty(shape, np.uint16)
+        ph = photons_out if photons_out is not None else (np.empty(shape, np.float32) if want_photons else None)
+        for a, dt in ((adu, np.uint16), (ph, np.float32)):
+            if a is not None and (a.dtype != dt or not a.flags.c_contiguous or a.size < nf * self.height * self.width):
+                raise ValueError(f"an output must be a contiguous {np.dtype(dt).name} array of (frames, h, w)")
+        cam = camera.c() if camera is not None else None
+        return events, bs, nf, bi, per_frame, cam, ph, adu
+
     def render_events(self, slot, events, bucket_start, frame0, pixel_size_nm, photons_per_blink,
                       camera: CameraParams | None, seed, bucket_index=None, drift_x_px=None, drift_y_px=None,
                       global_z_offset_um=None, bg_scale=None, use_illum=False, min_photons=0.0, want_photons=False,
@@ -347,24 +372,43 @@ class Engine:
         """Host blink events -> host frames in one C-ABI call (iscu_render_events): collection, render and noise on
         the device. Returns (photons | None, adu | None, n_emitters). Pass page-locked adu_out / photons_out (and
         events) for direct copies."""
-        events = np.ascontiguousarray(events, dtype=BLINK_EVENT_DTYPE)
-        bs = np.ascontiguousarray(bucket_start, dtype=np.uint32)
-        nf = len(bs) - 1
-        bi = None if bucket_index is None else np.ascontiguousarray(bucket_index, dtype=np.uint32)
-        f64 = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64)
-        dx, dy, gz, sc = f64(drift_x_px), f64(drift_y_px), f64(global_z_offset_um), f64(bg_scale)
-        shape = (nf, self.height, self.width)
-        adu = None
-        if camera is not None:
-            adu = adu_out if adu_out is not None else np.empty(shape, np.uint16)
-        ph = photons_out if photons_out is not None else (np.empty(shape, np.float32) if want_photons else None)
-        cam = camera.c() if camera is not None else None
+        events, bs, nf, bi, pf, cam, ph, adu = self._event_batch(events, bucket_start, camera, bucket_index,
+                                                                 drift_x_px, drift_y_px, global_z_offset_um, bg_scale,
+                                                                 want_photons, adu_out, photons_out)
         n = C.c_uint32()
         check(self.lib.iscu_render_events(self.h, int(slot), _ptr(events), len(events), _ptr(bi), _ptr(bs),
-                                          int(frame0), nf, float(pixel_size_nm), float(photons_per_blink), _ptr(dx),
-                                          _ptr(dy), _ptr(gz), _ptr(sc), int(bool(use_illum)), float(min_photons),
+                                          int(frame0), nf, float(pixel_size_nm), float(photons_per_blink),
+                                          *[_ptr(a) for a in pf], int(bool(use_illum)), float(min_photons),
                                           C.byref(cam) if cam is not None else None, int(seed), _ptr(ph), _ptr(adu),
                                           C.byref(n), None))
+        return ph, adu, n.value
+
+    EVENT_IO_SLOTS = 4
+
+    def render_events_async(self, io_slot, slot, events, bucket_start, frame0, pixel_size_nm, photons_per_blink,
+                            camera: CameraParams | None, seed, bucket_index=None, drift_x_px=None, drift_y_px=None,
+                            global_z_offset_um=None, bg_scale=None, use_illum=False, min_photons=0.0,
+                            want_photons=False, adu_out=None, photons_out=None):
+        """render_events enqueued in I/O slot io_slot (iscu_render_events_async): returns at once; the batch's arrays
+        are held until render_events_wait(io_slot), which returns what render_events returns. With page-locked host
+        buffers the copies of one slot's batch run beside the render of another's."""
+        batch = self._event_batch(events, bucket_start, camera, bucket_index, drift_x_px, drift_y_px,
+                                  global_z_offset_um, bg_scale, want_photons, adu_out, photons_out)
+        events, bs, nf, bi, pf, cam, ph, adu = batch
+        check(self.lib.iscu_render_events_async(self.h, int(io_slot), int(slot), _ptr(events), len(events), _ptr(bi),
+                                                _ptr(bs), int(frame0), nf, float(pixel_size_nm),
+                                                float(photons_per_blink), *[_ptr(a) for a in pf],
+                                                int(bool(use_illum)), float(min_photons),
+                                                C.byref(cam) if cam is not None else None, int(seed), _ptr(ph),
+                                                _ptr(adu)))
+        self._pending_io[int(io_slot)] = batch   # held only once enqueued: a refused call leaves the slot's batch be
+
+    def render_events_wait(self, io_slot):
+        """Waits for the batch of I/O slot io_slot: (photons | None, adu | None, n_emitters)."""
+        n = C.c_uint32()
+        check(self.lib.iscu_render_events_wait(self.h, int(io_slot), C.byref(n), None))
+        batch = self._pending_io.pop(int(io_slot), None)
+        ph, adu = (batch[6], batch[7]) if batch is not None else (None, None)
         return ph, adu, n.value
 
     RENDER_CONFIGS = 18

@@ -138,3 +138,47 @@ def test_render_events_matches(engine, reference, oracle, kernels):
     _, adu, _ = engine.render_events(0, ev0, bs0, 0, PX, 2000.0, cam, 5)
     _, _, want = kernels[0].render_movie(ev0, 0, F, W, H, PX, 2000.0, 15.0, cam, off, gain, rn, 5)
     assert np.array_equal(adu, want)
+
+
+def test_render_events_async_pipeline(engine, kernels):
+    """Batches of one movie enqueued across the I/O slots, up to three in flight, into page-locked host frames: each
+    equals the blocking call's frames bit for bit and reports the emitters the host collection keeps; a busy slot
+    refuses a second batch and keeps its first, and an idle slot refuses a wait."""
+    from insiliscope_b200 import IscuError
+    rng = np.random.default_rng(41)
+    B, NB = 10, 6
+    ev = _events(rng, 2400, B * NB, slots=(0, 1))
+    engine.set_static(W, H, flat_bg=12.0)
+    cam = CameraParams(gain=2.0, read_noise_e=1.4)
+    batches = []
+    for b in range(NB):
+        bi, bs = _buckets(ev, B * (b + 1))
+        batches.append((bi, bs[B * b:]))
+    pinned = [torch.empty((B, H, W), dtype=torch.uint16).pin_memory().numpy() for _ in range(3)]
+    want = [engine.render_events(-1, ev, bs, B * b, PX, 2000.0, cam, 9, bucket_index=bi)
+            for b, (bi, bs) in enumerate(batches)]
+    kept = [len(engine.collect_emitters(-1, ev, bs, B * b, W, H, PX, 2000.0, bucket_index=bi)[0])
+            for b, (bi, bs) in enumerate(batches)]
+    assert [w[2] for w in want] == kept and min(kept) > 0
+    got = [None] * NB
+    for b, (bi, bs) in enumerate(batches):
+        io = b % 3
+        if b >= 3:
+            _, adu, n = engine.render_events_wait(io)
+            got[b - 3] = (adu.copy(), n)
+        engine.render_events_async(io, -1, ev, bs, B * b, PX, 2000.0, cam, 9, bucket_index=bi, adu_out=pinned[io])
+        if b == 0:
+            with pytest.raises(IscuError):
+                engine.render_events_async(0, -1, ev, bs, 0, PX, 2000.0, cam, 9, bucket_index=bi,
+                                           adu_out=pinned[1])
+    for b in range(NB - 3, NB):
+        _, adu, n = engine.render_events_wait(b % 3)
+        got[b] = (adu.copy(), n)
+    for b in range(NB):
+        assert got[b][1] == kept[b], b
+        assert np.array_equal(got[b][0], want[b][1]), b
+    with pytest.raises(IscuError):
+        engine.render_events_wait(0)
+    with pytest.raises(IscuError):
+        engine.render_events_async(engine.EVENT_IO_SLOTS, -1, ev, batches[0][1], 0, PX, 2000.0, cam, 9,
+                                   bucket_index=batches[0][0])
