@@ -610,8 +610,12 @@ class NllGradWorkload:
                   "matmuls), data drawn by numpy's Poisson at the float64 expectation")
 
     def __init__(self, rank: int):
+        from insiliscope_b200.nll import shard_problem
         from insiliscope_b200.workloads import nll_rois
-        self.prob = nll_rois(seed=42 + rank)
+        # N ranks: one problem of 256 N frames, each rank its 256 (weak scaling); the Zernike gradient is summed
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        whole = nll_rois(seed=42, frames=256 * self.world)
+        self.prob = shard_problem(whole, rank, self.world) if self.world > 1 else whole
 
     def setup(self, device: int):
         import torch
@@ -630,11 +634,12 @@ class NllGradWorkload:
         self.d_bg = torch.from_numpy(P.bg).to(dev)
         self.zern = np.ascontiguousarray(P.zern, np.float64)
         n, F = len(P.frame), len(P.bg)
-        self.d_nll = torch.zeros(1, dtype=torch.float64, device=dev)
+        # [NLL, d/dzern]: the values every rank contributes to, summed over the ranks by one all-reduce
+        self.packed = torch.zeros(1 + len(self.zern), dtype=torch.float64, device=dev)
+        self.d_nll, self.g_zern = self.packed[:1], self.packed[1:]
         self.d_err = torch.zeros(1, dtype=torch.int32, device=dev)
         self.g_params = torch.empty((n, 4), dtype=torch.float32, device=dev)
         self.g_bg = torch.empty(F, dtype=torch.float64, device=dev)
-        self.g_zern = torch.empty(len(self.zern), dtype=torch.float64, device=dev)
         pin = lambda a: torch.from_numpy(a).pin_memory()
         self.h_params, self.h_bg = pin(P.params), pin(P.bg)
         self.h_gp = torch.empty((n, 4), dtype=torch.float32).pin_memory()
@@ -644,8 +649,10 @@ class NllGradWorkload:
         self.n_emitters = n
 
     def device_step(self):
+        from insiliscope_b200.nll import reduce_shared
         self.model.run_dev(self.d_params, self.d_frame, self.d_bg, self.zern, self.counts, self.d_nll, self.d_err,
                            self.g_params, self.g_bg, self.g_zern, sync=False)
+        reduce_shared(self.packed)
 
     def e2e_step(self):
         """Page-locked parameters in, the NLL and every gradient out, through the library's model."""
@@ -655,6 +662,7 @@ class NllGradWorkload:
         self.d_bg.copy_(self.h_bg, non_blocking=True)
         self.model.run_dev(self.d_params, self.d_frame, self.d_bg, self.zern, self.counts, self.d_nll, self.d_err,
                            self.g_params, self.g_bg, self.g_zern, sync=True)
+        reduce_shared(self.packed)
         self.h_gp.copy_(self.g_params, non_blocking=True)
         self.h_gb.copy_(self.g_bg, non_blocking=True)
         torch.cuda.synchronize()

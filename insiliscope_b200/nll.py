@@ -4,6 +4,10 @@ each emitter's field instead of storing per-emitter PSFs.
 
 Parameters: per emitter (x, y) in ROI pixels, z defocus in nm, N photons; one background per frame; the Zernike
 coefficients (waves rms, Noll indices of the spec). The model is documented in include/iscu.h (iscu_nll_spec).
+
+Across ranks (one process per GPU) the frames split into contiguous ranges (shard_problem): the emitters and
+backgrounds of a frame live on one rank, so their gradients stay local, and the one exchange is the sum of the NLL
+and of the Zernike gradient over the ranks (reduce_shared: one all-reduce of 1 + J float64 values).
 """
 from __future__ import annotations
 
@@ -122,3 +126,27 @@ def poisson_nll(model: NllModel, params, bg, zern, counts, frame):
                     (go.to(zern.device) * gz.to(zern.device)).to(zern.dtype))
 
     return _PoissonNll.apply(params, bg, zern)
+
+
+def shard_problem(prob, rank: int, world: int):
+    """The rank's share of an NllProblem: its contiguous range of frames (insiliscope_b200.shard.frame_range), their
+    emitters and backgrounds, frames renumbered from 0; `frame0` (the range's first frame) keys the rank's noise draws
+    as the whole problem's. The Zernike coefficients are shared by every rank."""
+    from dataclasses import replace
+
+    from .shard import frame_range
+    F = len(prob.bg)
+    first, end = frame_range(rank, world, F)
+    sel = (prob.frame >= first) & (prob.frame < end)
+    return replace(prob, frame=(prob.frame[sel] - first).astype(np.int32), params_true=prob.params_true[sel],
+                   bg_true=prob.bg_true[first:end], params=prob.params[sel], bg=prob.bg[first:end],
+                   frame0=prob.frame0 + first)
+
+
+def reduce_shared(packed):
+    """Sums, in place over the ranks, a float64 tensor holding [NLL, d/dzern (J)] (the only gradient every rank
+    contributes to); returns it. One all-reduce; a no-op without an initialised process group of 2 or more ranks."""
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(packed, op=dist.ReduceOp.SUM)
+    return packed

@@ -309,6 +309,7 @@ class NllProblem:
     bg: np.ndarray
     zern: np.ndarray
     noise_seed: int
+    frame0: int = 0             # the first frame's number in the whole problem (a rank's share starts there)
 
 
 def nll_rois(seed: int = 42, frames: int = 256, per_frame: int = 1000, spec=None) -> NllProblem:
@@ -350,5 +351,6 @@ def nll_counts(engine, model, prob: NllProblem, device="cuda"):
     R = prob.spec.roi
     engine.set_static(R, R * per, flat_bg=0.0)
     cam = CameraParams(quantum_efficiency=1.0, dark_electrons=0.0, gain=1.0, read_noise_e=0.0)
-    adu = engine.noise_frames_dev(mu.reshape(F, per * R, R), np.arange(F), cam, prob.noise_seed)
+    adu = engine.noise_frames_dev(mu.reshape(F, per * R, R), np.arange(prob.frame0, prob.frame0 + F), cam,
+                                  prob.noise_seed)
     return adu.to(torch.float32).reshape(len(prob.frame), R, R)
