@@ -486,6 +486,41 @@ int iscu_wf_pass_times(iscu_wf_plan* plan, float* ms5);
 int iscu_wf_render_dev(iscu_wf_plan* plan, const float* density_dev, double background, const iscu_camera* cam,
                        uint32_t seed, uint32_t frame0, float* image_dev, uint16_t* adu_dev);
 
+/* ---------------------------------------------------------------- the named-kernel backend ---------------------- */
+
+/* sim::GpuBackend (WidefieldGpuHost.h:42-77) on the device, so that the reference's hosts over it -- SplatGpuHost
+ * (SplatGpu.h:40-75) and WidefieldGpuHost (WidefieldGpuHost.h:79-114), self-checks included -- run unmodified:
+ * storage buffers of 32-bit words, and the kernels those hosts dispatch by name, with their parameter blocks (up to
+ * 16 words), their buffers bound in order and their dispatch sizes in workgroups:
+ *   splat_frames (SplatGpu.wgsl; 16 x 16 pixels a workgroup, 7 buffers: 4 block-sum buffers, Stat, Dyn, Out),
+ *   wf_clear, wf_scatter, wf_mac (256 invocations a workgroup), wf_fft (256, one transform of n <= 2048 a
+ *   workgroup), wf_split, wf_expand, wf_crop, wf_frame (16 x 16) (WidefieldGpu.wgsl).
+ * Each computes what its WGSL source defines, in float32 (the noise chain included: the counter stream's float
+ * uniforms, Box-Muller, Knuth / normal Poisson, Marsaglia-Tsang). Every buffer access is checked against the bound
+ * buffers' sizes: a read out of range gives 0 and a write out of range is dropped (WebGPU's robust buffer access),
+ * and loop counts taken from buffers are bounded by the buffers' sizes, so a malformed dispatch cannot fault or
+ * hang; parameters a kernel cannot run with (an FFT length that is not a power of two up to 2048, a zero grid size)
+ * fail with ISCU_ERR_ARG. All work runs in order on the context's stream; buffers must be destroyed before their
+ * context. */
+typedef struct iscu_buffer iscu_buffer;
+/* A buffer of bytes rounded up to 4, holding data (bytes of it; nullable: zeros). */
+int iscu_buffer_create(iscu_ctx* ctx, size_t bytes, const void* data, iscu_buffer** out);
+void iscu_buffer_destroy(iscu_buffer* buf);
+size_t iscu_buffer_bytes(const iscu_buffer* buf);
+/* bytes of data into buf at offset (the host buffer may be reused when the call returns). */
+int iscu_buffer_write(iscu_buffer* buf, size_t offset, const void* data, size_t bytes);
+/* The first bytes of src into dst. */
+int iscu_buffer_copy(iscu_buffer* dst, const iscu_buffer* src, size_t bytes);
+/* The first bytes of src into dst (host), after the work before it. */
+int iscu_buffer_read(const iscu_buffer* src, size_t bytes, void* dst);
+/* The low 16 bits of src's first `words` words (GpuBackend::ReadBackLow16: the splat's ADU), narrowed on the
+ * device so that half the bytes cross to the host. */
+int iscu_buffer_read_low16(const iscu_buffer* src, size_t words, uint16_t* dst);
+/* GpuBackend::Dispatch: kernel by name, params (n_params <= 16 words; the rest of the block reads 0), bufs in
+ * binding order (their count as the kernel's source binds them), x * y * z workgroups (y, z <= 65535). */
+int iscu_dispatch(iscu_ctx* ctx, const char* kernel, const uint32_t* params, size_t n_params,
+                  iscu_buffer* const* bufs, size_t n_bufs, uint32_t x, uint32_t y, uint32_t z);
+
 #ifdef __cplusplus
 }
 #endif

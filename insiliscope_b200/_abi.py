@@ -152,6 +152,15 @@ SIGNATURES = {
                                            C.c_double, C.c_double, vp, vp, vp, vp, C.c_int32, C.c_double,
                                            C.POINTER(Camera), C.c_uint32, vp, vp]),
     "iscu_render_events_wait": (C.c_int, [vp, C.c_int32, u32p, C.POINTER(C.c_int64)]),
+    "iscu_buffer_create": (C.c_int, [vp, C.c_size_t, vp, C.POINTER(vp)]),
+    "iscu_buffer_destroy": (None, [vp]),
+    "iscu_buffer_bytes": (C.c_size_t, [vp]),
+    "iscu_buffer_write": (C.c_int, [vp, C.c_size_t, vp, C.c_size_t]),
+    "iscu_buffer_copy": (C.c_int, [vp, vp, C.c_size_t]),
+    "iscu_buffer_read": (C.c_int, [vp, C.c_size_t, vp]),
+    "iscu_buffer_read_low16": (C.c_int, [vp, C.c_size_t, vp]),
+    "iscu_dispatch": (C.c_int, [vp, C.c_char_p, vp, C.c_size_t, vp, C.c_size_t, C.c_uint32, C.c_uint32,
+                                C.c_uint32]),
     "iscu_drift_trajectory": (C.c_int, [C.c_int64, C.c_int64, C.c_double, C.POINTER(DriftSettings), vp]),
     "iscu_illumination_field": (C.c_int, [C.c_uint32, C.c_uint32, C.c_int32, C.c_double, vp, f64p]),
     "iscu_background_fade_scale": (C.c_double, [C.c_double, C.c_double]),

@@ -33,6 +33,7 @@ UNITS = {
     "psf_noalloc.cu": [],
     "psf_plan.cu": [],
     "widefield.cu": ["--fmad=false"],
+    "backend.cu": ["--fmad=false"],
     "capi.cpp": [],
     "host_models.cpp": [],
 }

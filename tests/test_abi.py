@@ -74,3 +74,17 @@ def test_errors_without_device(lib):
     assert lib.iscu_psf_geometry(C.byref(bad), None, None, None) == _abi.ISCU_ERR_ARG
     assert b"must be > 0" in lib.iscu_last_error()
     assert lib.iscu_abi_version() == 1
+
+
+def test_backend_argument_checks_without_device(lib):
+    """The named-kernel backend's calls refuse null contexts and buffers before touching a device."""
+    from insiliscope_b200 import _abi
+    h = C.c_void_p()
+    assert lib.iscu_buffer_create(None, 16, None, C.byref(h)) == _abi.ISCU_ERR_ARG
+    assert lib.iscu_buffer_bytes(None) == 0
+    assert lib.iscu_buffer_write(None, 0, None, 0) == _abi.ISCU_ERR_ARG
+    assert lib.iscu_buffer_read(None, 0, None) == _abi.ISCU_ERR_ARG
+    assert lib.iscu_buffer_read_low16(None, 0, None) == _abi.ISCU_ERR_ARG
+    assert lib.iscu_buffer_copy(None, None, 0) == _abi.ISCU_ERR_ARG
+    assert lib.iscu_dispatch(None, b"wf_clear", None, 0, None, 0, 1, 1, 1) == _abi.ISCU_ERR_ARG
+    lib.iscu_buffer_destroy(None)
