@@ -36,8 +36,6 @@ namespace {
 constexpr int kThreads = 512;
 constexpr int kRows = 128;             // UMMA M (2P rows, padded)
 constexpr int kBlockBytes = 128 * 128; // one operand K block: 128 rows x 32 TF32 (128 B per row)
-constexpr int kTmemCols = 256;         // row pass: columns [0, 128); column pass: [128, 192)
-constexpr unsigned kSpinLimit = 1u << 26;
 
 // ------------------------------------------------------------------------------------------ PTX helpers
 __device__ __forceinline__ uint32_t SmemAddr(const void* p)
@@ -62,25 +60,6 @@ __device__ __forceinline__ void Split(float x, float& hi, float& lo)
 __device__ __forceinline__ void MbarInit(uint64_t* bar, uint32_t count)
 {
    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(SmemAddr(bar)), "r"(count));
-}
-
-// Waits for the phase with the given parity to complete; false after kSpinLimit polls.
-__device__ __forceinline__ bool MbarWait(uint64_t* bar, uint32_t parity)
-{
-   const uint32_t a = SmemAddr(bar);
-   for (unsigned it = 0; it < kSpinLimit; ++it)
-   {
-      uint32_t done;
-      asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-                   : "=r"(done)
-                   : "r"(a), "r"(parity)
-                   : "memory");
-      if (done)
-         return true;
-      if (it > 64)
-         __nanosleep(64);
-   }
-   return false;
 }
 
 __device__ __forceinline__ void FenceProxyAsync() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
@@ -244,248 +223,453 @@ struct TcParams
    int nPsf, M, P, normalize;
 };
 
-constexpr int kStages = 2;
-constexpr int kStageBytes = 2 * kBlockBytes;   // a K block's hi and lo images (A: 128 rows; B: up to 128 rows)
-constexpr int kPerThread = 16 * 128 / kThreads; // pupil samples of a row-pass B block per thread
+constexpr int kAStages = 3;                        // Ahat K blocks in flight, in MMA order (both passes)
+constexpr int kRowStages = 3;                      // row-pass B blocks (pupil phasors)
+constexpr int kColStages = 2;                      // column-pass B blocks (T, split)
+constexpr int kStageBytes = 2 * kBlockBytes;       // an A or row-pass B block: hi and lo images of 128 rows
+constexpr int kColStageBytes = kBlockBytes;        // a column-pass B block: hi and lo images of 64 rows
+constexpr int kDrainWarps = 4;                     // warps 0-3, one per TMEM lane quadrant
+constexpr int kMmaWarp = 4;                        // lane 0 issues the MMAs and the Ahat copies
+constexpr int kFirstProducer = 5;                  // warps 5-15 make the pupil phasors
+constexpr int kProducerThreads = kThreads - 32 * kFirstProducer;
+constexpr int kItemsPerBlock = 1024;               // (pupil column, pair of pupil rows) items of one row-pass block
+constexpr int kItemRounds = (kItemsPerBlock + kProducerThreads - 1) / kProducerThreads;
+constexpr int kTmemRow = 0;                        // T of PSF j: columns [128 (j % 2), +128)
+constexpr int kTmemCol = 256;                      // E of PSF j: columns [256 + 64 (j % 2), +64)
+constexpr uint64_t kWaitNs = 4000000000ull;        // a wait gives up after 4 s
 
-// Per CTA, persistent over PSFs. Per K block kb of each pass, stage s = kb % 2:
-//   wait until the MMAs that last read stage s are done (tcgen05.commit -> mma[s]);
-//   thread 0 starts the bulk copy of Ahat's K block into sA[s] (-> full[s]);
-//   the threads write the B block into sB[s]: row pass, the pupil phasors of rows [16 kb, 16 kb + 16) (their table
-//   entries loaded one K block ahead); column pass, T's columns [16 kb, 16 kb + 16) read from TMEM and split;
-//   then thread 0 waits for full[s] and issues the 12 MMAs (hi*hi, hi*lo, lo*hi over 4 K steps) and the commit.
+struct Shared
+{
+   uint64_t aFull[kAStages], aEmpty[kAStages];
+   uint64_t rowFull[kRowStages], rowEmpty[kRowStages];
+   uint64_t colFull[kColStages], colEmpty[kColStages];
+   uint64_t rowDone[2], colDone[2], tFree[2], eFree[2], red[2];
+   uint64_t final;
+   double sum[2][kDrainWarps];
+   uint32_t tmemSlot;
+   int err;
+};
+constexpr size_t kSmemBytes = static_cast<size_t>(kAStages + kRowStages) * kStageBytes +
+                              static_cast<size_t>(kColStages) * kColStageBytes + sizeof(Shared) + 1024;
+
+__device__ __forceinline__ uint64_t GlobalNs()
+{
+   uint64_t t;
+   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+   return t;
+}
+
+// Waits for the phase of the given parity to complete. false after kWaitNs, or (err non-null) once *err is set.
+__device__ __forceinline__ bool MbarWait(uint64_t* bar, uint32_t parity, const volatile int* err)
+{
+   const uint32_t a = SmemAddr(bar);
+   uint64_t t0 = 0;
+   for (unsigned it = 0;; ++it)
+   {
+      uint32_t done;
+      asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                   : "=r"(done)
+                   : "r"(a), "r"(parity)
+                   : "memory");
+      if (done)
+         return true;
+      if ((it & 15) == 15)
+      {
+         if (err && *err)
+            return false;
+         const uint64_t now = GlobalNs();
+         if (t0 == 0)
+            t0 = now;
+         else if (now - t0 > kWaitNs)
+            return false;
+      }
+   }
+}
+
+__device__ __forceinline__ void MbarArrive(uint64_t* bar)
+{
+   asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(SmemAddr(bar)) : "memory");
+}
+
+// 16 consecutive TMEM columns of this warp's 32 lanes into v[0..15].
+__device__ __forceinline__ void TmemLoad16(uint32_t taddr, float* v)
+{
+   uint32_t r[16];
+   asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+                "%14, %15}, [%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15])
+                : "r"(taddr));
+   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+   for (int i = 0; i < 16; ++i)
+      v[i] = __uint_as_float(r[i]);
+}
+
+// The CTA's j-th PSF.
+__device__ __forceinline__ int PsfOf(int j) { return static_cast<int>(blockIdx.x) + j * static_cast<int>(gridDim.x); }
+
+// The MMA order of a CTA's K blocks: R(0), R(1), C(0), R(2), C(1), ..., R(n - 1), C(n - 2), C(n - 1), each pass nKb
+// blocks (R: row pass, C: column pass), so the column pass of one PSF runs on the tensor cores while the producers
+// make the next PSFs' pupils. Block t -> its PSF j, its pass and K block kb.
+__device__ __forceinline__ void JobOf(int t, int nKb, int nLocal, int& j, bool& row, int& kb)
+{
+   const int seg = t / nKb;
+   kb = t % nKb;
+   if (seg == 0)
+   {
+      j = 0;
+      row = true;
+      return;
+   }
+   const int u = seg - 1;
+   if ((u & 1) == 0 && u / 2 + 1 < nLocal)
+   {
+      j = u / 2 + 1;
+      row = true;
+   }
+   else
+   {
+      j = (u & 1) ? (u - 1) / 2 : nLocal - 1;
+      row = false;
+   }
+}
+
+// Per CTA, persistent over its PSFs (blockIdx.x + j gridDim.x), warp-specialized; the roles meet only at mbarriers:
+//   producers (warps 5-15): per row-pass K block the pupil phasors of 16 pupil rows (float64 phase, reduced mod 2 pi,
+//     SFU sine and cosine, TF32 hi/lo split) into a row-B stage -> rowFull;
+//   the MMA thread (warp 4, lane 0): the Ahat K blocks by bulk copy into the A ring (two blocks ahead), and per K
+//     block 12 MMAs (hi*hi, hi*lo, lo*hi over 4 K steps) in the MMA order of JobOf; commits free the stages and mark
+//     a pass done (rowDone / colDone);
+//   drain warps (0-3, one TMEM lane quadrant each): T of PSF j from TMEM, split, into col-B stages -> colFull (then
+//     tFree: T's columns may take PSF j + 2); then E of PSF j: |E|^2, the plane sum, the normalized plane (eFree).
+// T and E are double-buffered in TMEM (512 columns). Every wait is bounded (kWaitNs) and also ends when another role
+// has failed (Shared::err); a failed CTA stops issuing, waits for its copies and MMAs in flight, frees TMEM and
+// reports through prm.error.
 __global__ void __launch_bounds__(kThreads, 1) CztTf32x3Kernel(TcParams prm)
 {
    extern __shared__ __align__(1024) unsigned char smemRaw[];
    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
-   unsigned char* sA = smem;                                   // [kStages] x 32 KB
-   unsigned char* sB = smem + kStages * kStageBytes;           // [kStages] x 32 KB
-   unsigned char* tail = smem + 2 * kStages * kStageBytes;
-   double* sRed = reinterpret_cast<double*>(tail);             // 4 doubles
-   uint64_t* full = reinterpret_cast<uint64_t*>(tail + 64);    // kStages
-   uint64_t* mmaBar = reinterpret_cast<uint64_t*>(tail + 96);  // kStages
-   uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(tail + 128);
-   int* sErr = reinterpret_cast<int*>(tail + 132);
+   unsigned char* sA = smem;                                            // [kAStages] x 32 KB
+   unsigned char* sRowB = sA + kAStages * kStageBytes;                  // [kRowStages] x 32 KB
+   unsigned char* sColB = sRowB + kRowStages * kStageBytes;             // [kColStages] x 16 KB
+   Shared* sh = reinterpret_cast<Shared*>(sColB + kColStages * kColStageBytes);
+   volatile int* err = &sh->err;
 
    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
    const int M = prm.M, P = prm.P, nKb = M / 16;
+   const int nLocal = prm.nPsf > static_cast<int>(blockIdx.x)
+                         ? (prm.nPsf - static_cast<int>(blockIdx.x) + static_cast<int>(gridDim.x) - 1) /
+                              static_cast<int>(gridDim.x)
+                         : 0;
 
    if (warp == 0)
    {
-      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(SmemAddr(tmemSlot)),
-                   "r"(kTmemCols));
+      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(SmemAddr(&sh->tmemSlot)),
+                   "r"(512));
       asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
    }
    if (tid == 0)
    {
-      for (int s = 0; s < kStages; ++s)
+      for (int s = 0; s < kAStages; ++s)
       {
-         MbarInit(&full[s], 1);
-         MbarInit(&mmaBar[s], 1);
+         MbarInit(&sh->aFull[s], 1);
+         MbarInit(&sh->aEmpty[s], 1);
       }
-      *sErr = 0;
+      for (int s = 0; s < kRowStages; ++s)
+      {
+         MbarInit(&sh->rowFull[s], kThreads / 32 - kFirstProducer);
+         MbarInit(&sh->rowEmpty[s], 1);
+      }
+      for (int s = 0; s < kColStages; ++s)
+      {
+         MbarInit(&sh->colFull[s], kDrainWarps);
+         MbarInit(&sh->colEmpty[s], 1);
+      }
+      for (int s = 0; s < 2; ++s)
+      {
+         MbarInit(&sh->rowDone[s], 1);
+         MbarInit(&sh->colDone[s], 1);
+         MbarInit(&sh->tFree[s], kDrainWarps);
+         MbarInit(&sh->eFree[s], kDrainWarps);
+         MbarInit(&sh->red[s], kDrainWarps);
+      }
+      MbarInit(&sh->final, 1);
+      sh->err = 0;
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
    }
    TcFenceBefore();
    __syncthreads();
    TcFenceAfter();
-   const uint32_t tmem = *tmemSlot;
-   uint32_t fullPhase[kStages] = {0u, 0u}, mmaPhase[kStages] = {0u, 0u};
-   int pending[kStages] = {0, 0};
+   const uint32_t tmem = sh->tmemSlot;
    bool ok = true;
-   const uint32_t idesc1 = InstrDesc(kRows, M), idesc2 = InstrDesc(kRows, 64);
 
-   // every thread waits for stage s's last MMAs; the outcome (and a failed copy wait of thread 0, whose flag is
-   // read after the barrier) is made uniform
-   auto drain = [&](int s) {
-      if (pending[s])
-      {
-         ok = __syncthreads_and(MbarWait(&mmaBar[s], mmaPhase[s]) && ok) != 0;
-         if (*sErr)
-            ok = false;
-         mmaPhase[s] ^= 1u;
-         pending[s] = 0;
-      }
-   };
-   // thread 0: wait for the stage's A copy, then the MMAs and the commit (a commit with no MMA completes at once,
-   // so the other threads' waits end after a failure too)
-   auto issue = [&](int s, uint32_t dTmem, uint32_t bH, uint32_t bL, uint32_t idesc, bool first) {
-      if (tid != 0)
-         return;
-      const bool copied = MbarWait(&full[s], fullPhase[s]);
-      fullPhase[s] ^= 1u;
-      if (!copied)
-         *sErr = 1;
-      TcFenceAfter();
-      if (copied && *sErr == 0)
-      {
-         const uint32_t aH = SmemAddr(sA + s * kStageBytes), aL = aH + kBlockBytes;
-#pragma unroll
-         for (int kk = 0; kk < 4; ++kk)
-         {
-            const uint32_t off = kk * 32;   // 8 TF32 = 32 bytes along K
-            Mma(dTmem, SmemDesc(aH + off), SmemDesc(bH + off), idesc, (first && kk == 0) ? 0u : 1u);
-            Mma(dTmem, SmemDesc(aH + off), SmemDesc(bL + off), idesc, 1u);
-            Mma(dTmem, SmemDesc(aL + off), SmemDesc(bH + off), idesc, 1u);
-         }
-      }
-      Commit(&mmaBar[s]);
-   };
-   auto loadA = [&](int s, const float* ahat, int kb) {
-      if (tid == 0)
-      {
-         MbarExpectTx(&full[s], kStageBytes);
-         BulkLoad(sA + s * kStageBytes, ahat + static_cast<size_t>(kb) * (kStageBytes / 4), kStageBytes, &full[s]);
-      }
-   };
-
-   for (int psf = blockIdx.x; psf < prm.nPsf && ok; psf += gridDim.x)
+   if (warp >= kFirstProducer)
    {
-      const PsfItem it = prm.items[psf];
-      const SetParams& sp = prm.sets[it.set];
-      const double2* tab = prm.phase + static_cast<size_t>(it.set) * M * M;
-      const double aDef = sp.k0 * sp.ni * it.dtiM;
-      const float* ahat = prm.ahat + static_cast<size_t>(it.set) * 8 * (kStageBytes / 4);
-
-      // ---------------------------------------------------------------- row pass: T = A U
-      double2 pre[kPerThread];
-#pragma unroll
-      for (int q = 0; q < kPerThread; ++q)
+      // ---------------------------------------------------------------- producers: row-pass B blocks
+      const int ptid = tid - 32 * kFirstProducer;
+      uint32_t rowCount = 0;
+      for (int j = 0; j < nLocal && ok; ++j)
       {
-         const int e = tid + q * kThreads, m = e & 127, nl = e >> 7;
-         pre[q] = m < M ? tab[static_cast<size_t>(nl) * M + m] : make_double2(0.0, -1.0);
-      }
-      for (int kb = 0; kb < nKb; ++kb)
-      {
-         const int s = kb % kStages;
-         drain(s);
-         if (!ok)
-            break;
-         loadA(s, ahat, kb);
-         double2 cur[kPerThread];
+         const PsfItem it = prm.items[PsfOf(j)];
+         const double aDef = prm.sets[it.set].k0 * prm.sets[it.set].ni * it.dtiM;
+         const double2* tab = prm.phase + static_cast<size_t>(it.set) * M * M;
+         for (int kb = 0; kb < nKb; ++kb, ++rowCount)
+         {
+            const int rs = static_cast<int>(rowCount % kRowStages);
+            ok = __all_sync(0xffffffffu, MbarWait(&sh->rowEmpty[rs], ((rowCount / kRowStages) & 1u) ^ 1u, err));
+            if (!ok)
+               break;
+            double2 t[kItemRounds][2];
 #pragma unroll
-         for (int q = 0; q < kPerThread; ++q)
-            cur[q] = pre[q];
-         if (kb + 1 < nKb)
-#pragma unroll
-            for (int q = 0; q < kPerThread; ++q)
+            for (int r = 0; r < kItemRounds; ++r)
             {
-               const int e = tid + q * kThreads, m = e & 127, n = 16 * (kb + 1) + (e >> 7);
-               pre[q] = m < M ? tab[static_cast<size_t>(n) * M + m] : make_double2(0.0, -1.0);
+               const int item = ptid + r * kProducerThreads, m = item & 127, n = 16 * kb + 2 * (item >> 7);
+               const bool in = item < kItemsPerBlock && m < M;
+               t[r][0] = in ? tab[static_cast<size_t>(n) * M + m] : make_double2(0.0, -1.0);
+               t[r][1] = in ? tab[static_cast<size_t>(n + 1) * M + m] : make_double2(0.0, -1.0);
             }
-         unsigned char* b = sB + s * kStageBytes;
+            unsigned char* b = sRowB + rs * kStageBytes;
 #pragma unroll
-         for (int q = 0; q < kPerThread; ++q)
-         {
-            const int e = tid + q * kThreads, m = e & 127, nl = e >> 7;
-            const float2 u = TablePhasor(cur[q], aDef);
-            float rh, rl, ih, il;
-            Split(u.x, rh, rl);
-            Split(u.y, ih, il);
-            *reinterpret_cast<float*>(b + SwOff(m, nl)) = rh;
-            *reinterpret_cast<float*>(b + SwOff(m, 16 + nl)) = ih;
-            *reinterpret_cast<float*>(b + kBlockBytes + SwOff(m, nl)) = rl;
-            *reinterpret_cast<float*>(b + kBlockBytes + SwOff(m, 16 + nl)) = il;
+            for (int r = 0; r < kItemRounds; ++r)
+            {
+               const int item = ptid + r * kProducerThreads;
+               if (item < kItemsPerBlock)
+               {
+                  const int m = item & 127, nl = 2 * (item >> 7);
+                  const float2 u0 = TablePhasor(t[r][0], aDef), u1 = TablePhasor(t[r][1], aDef);
+                  float rh0, rl0, ih0, il0, rh1, rl1, ih1, il1;
+                  Split(u0.x, rh0, rl0);
+                  Split(u0.y, ih0, il0);
+                  Split(u1.x, rh1, rl1);
+                  Split(u1.y, ih1, il1);
+                  // B[m][nl], B[m][nl + 1]: the real parts of pupil rows n, n + 1; B[m][16 + nl ..]: the imaginary
+                  *reinterpret_cast<float2*>(b + SwOff(m, nl)) = make_float2(rh0, rh1);
+                  *reinterpret_cast<float2*>(b + SwOff(m, 16 + nl)) = make_float2(ih0, ih1);
+                  *reinterpret_cast<float2*>(b + kBlockBytes + SwOff(m, nl)) = make_float2(rl0, rl1);
+                  *reinterpret_cast<float2*>(b + kBlockBytes + SwOff(m, 16 + nl)) = make_float2(il0, il1);
+               }
+            }
+            FenceProxyAsync();
+            __syncwarp();
+            if (lane == 0)
+               MbarArrive(&sh->rowFull[rs]);
          }
-         FenceProxyAsync();
-         __syncthreads();
-         const uint32_t bH = SmemAddr(b);
-         issue(s, tmem, bH, bH + kBlockBytes, idesc1, kb == 0);
-         pending[s] = 1;
       }
-      for (int s = 0; s < kStages; ++s)
-         drain(s);
-      if (!ok)
-         break;
-      TcFenceAfter();
-
-      // ---------------------------------------------------------------- column pass: E^T = A T^T
-      // TMEM lane r = 32 g + 16 h + i holds T row y = 16 g + i, part h; column m. B2 block kb: row y, column
-      // 16 h + (m - 16 kb). Warps w, w + 4, w + 8, w + 12 share lanes 32 (w % 4) ..; warp w reads the 4 columns
-      // 16 kb + 4 (w / 4) ..
-      const int lg = warp & 3, ch = warp >> 2;
-      const int r = 32 * lg + lane, h = (r >> 4) & 1, y = 16 * lg + (r & 15);
-      for (int kb = 0; kb < nKb; ++kb)
+   }
+   else if (warp == kMmaWarp)
+   {
+      // ---------------------------------------------------------------- the MMA thread
+      if (lane == 0 && nLocal > 0)
       {
-         const int s = kb % kStages;
-         drain(s);
+         const int nJobs = 2 * nLocal * nKb;
+         const uint32_t idesc1 = InstrDesc(kRows, M), idesc2 = InstrDesc(kRows, 64);
+         int loaded = 0;   // A blocks whose copy was started
+         // block t's Ahat K block into stage t % kAStages, once the MMAs of block t - kAStages are done
+         auto loadA = [&](int t) -> bool {
+            const int st = t % kAStages;
+            if (t >= kAStages && !MbarWait(&sh->aEmpty[st], static_cast<uint32_t>(t / kAStages - 1) & 1u, err))
+               return false;
+            int j, kb;
+            bool row;
+            JobOf(t, nKb, nLocal, j, row, kb);
+            const float* src = prm.ahat + (static_cast<size_t>(prm.items[PsfOf(j)].set) * 8 + kb) * (kStageBytes / 4);
+            MbarExpectTx(&sh->aFull[st], kStageBytes);
+            BulkLoad(sA + st * kStageBytes, src, kStageBytes, &sh->aFull[st]);
+            loaded = t + 1;
+            return true;
+         };
+         int consumed = 0;
+         uint32_t rowCount = 0, colCount = 0;
+         for (int t = 0; t < kAStages - 1 && t < nJobs && ok; ++t)
+            ok = loadA(t);
+         for (int t = 0; t < nJobs && ok; ++t)
+         {
+            int j, kb;
+            bool row;
+            JobOf(t, nKb, nLocal, j, row, kb);
+            const uint32_t use = static_cast<uint32_t>(j >> 1) & 1u;
+            if (kb == 0)   // the accumulator's TMEM columns are free (PSF j - 2 is past them)
+               ok = MbarWait(row ? &sh->tFree[j & 1] : &sh->eFree[j & 1], use ^ 1u, err);
+            uint64_t* full;
+            uint64_t* empty;
+            uint32_t parity, bH, bL, d, idesc;
+            if (row)
+            {
+               const int rs = static_cast<int>(rowCount % kRowStages);
+               full = &sh->rowFull[rs];
+               empty = &sh->rowEmpty[rs];
+               parity = (rowCount / kRowStages) & 1u;
+               bH = SmemAddr(sRowB + rs * kStageBytes);
+               bL = bH + kBlockBytes;
+               d = tmem + kTmemRow + 128u * static_cast<uint32_t>(j & 1);
+               idesc = idesc1;
+            }
+            else
+            {
+               const int cs = static_cast<int>(colCount % kColStages);
+               full = &sh->colFull[cs];
+               empty = &sh->colEmpty[cs];
+               parity = (colCount / kColStages) & 1u;
+               bH = SmemAddr(sColB + cs * kColStageBytes);
+               bL = bH + kColStageBytes / 2;
+               d = tmem + kTmemCol + 64u * static_cast<uint32_t>(j & 1);
+               idesc = idesc2;
+            }
+            ok = ok && MbarWait(full, parity, err);
+            ok = ok && MbarWait(&sh->aFull[t % kAStages], static_cast<uint32_t>(t / kAStages) & 1u, err);
+            if (!ok)
+               break;
+            consumed = t + 1;
+            TcFenceAfter();
+            const uint32_t aH = SmemAddr(sA + (t % kAStages) * kStageBytes), aL = aH + kBlockBytes;
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk)
+            {
+               const uint32_t off = kk * 32;   // 8 TF32 = 32 bytes along K
+               Mma(d, SmemDesc(aH + off), SmemDesc(bH + off), idesc, (kb == 0 && kk == 0) ? 0u : 1u);
+               Mma(d, SmemDesc(aH + off), SmemDesc(bL + off), idesc, 1u);
+               Mma(d, SmemDesc(aL + off), SmemDesc(bH + off), idesc, 1u);
+            }
+            Commit(empty);
+            Commit(&sh->aEmpty[t % kAStages]);
+            if (kb == nKb - 1)
+               Commit(row ? &sh->rowDone[j & 1] : &sh->colDone[j & 1]);
+            if (row)
+               ++rowCount;
+            else
+               ++colCount;
+            if (t + kAStages - 1 < nJobs)
+               ok = loadA(t + kAStages - 1);   // waits for the MMAs of block t - 1
+         }
+         if (!ok)
+         {
+            *err = 1;
+            // let the copies and MMAs in flight land before the CTA frees its memory
+            for (int t = consumed; t < loaded; ++t)
+               MbarWait(&sh->aFull[t % kAStages], static_cast<uint32_t>(t / kAStages) & 1u, nullptr);
+            Commit(&sh->final);
+            MbarWait(&sh->final, 0u, nullptr);
+         }
+      }
+   }
+   else
+   {
+      // ---------------------------------------------------------------- drain warps
+      // TMEM lane r = 32 w + 16 h + i of T holds row y = 16 w + i, part h (columns: the pupil column m); of E, output
+      // x = 16 w + i, part h (columns: y).
+      const int h = (lane >> 4) & 1, y = 16 * warp + (lane & 15), x = y;
+      const uint32_t quad = static_cast<uint32_t>(32 * warp) << 16;
+      uint32_t colCount = 0;
+      for (int j = 0; j < nLocal && ok; ++j)
+      {
+         const uint32_t use = static_cast<uint32_t>(j >> 1) & 1u;
+         ok = __all_sync(0xffffffffu, MbarWait(&sh->rowDone[j & 1], use, err));
          if (!ok)
             break;
-         loadA(s, ahat, kb);
-         float v[4];
-         TmemLoad4(tmem + (static_cast<uint32_t>(32 * lg) << 16) + 16 * kb + 4 * ch, v);
-         unsigned char* b = sB + s * kStageBytes;
-#pragma unroll
-         for (int j = 0; j < 4; ++j)
+         TcFenceAfter();
+         for (int kb = 0; kb < nKb; ++kb, ++colCount)
          {
-            const int col = 16 * h + 4 * ch + j;
-            float hi, lo;
-            Split(y < P ? v[j] : 0.f, hi, lo);
-            *reinterpret_cast<float*>(b + SwOff(y, col)) = hi;
-            *reinterpret_cast<float*>(b + kBlockBytes / 2 + SwOff(y, col)) = lo;
+            const int cs = static_cast<int>(colCount % kColStages);
+            ok = __all_sync(0xffffffffu, MbarWait(&sh->colEmpty[cs], ((colCount / kColStages) & 1u) ^ 1u, err));
+            if (!ok)
+               break;
+            float v[16];
+            TmemLoad16(tmem + quad + kTmemRow + 128u * static_cast<uint32_t>(j & 1) + 16u * kb, v);
+            float hi[16], lo[16];
+#pragma unroll
+            for (int c = 0; c < 16; ++c)
+               Split(y < P ? v[c] : 0.f, hi[c], lo[c]);
+            // B[y][16 h + c] = part h of T[y][16 kb + c]
+            unsigned char* b = sColB + cs * kColStageBytes;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+            {
+               *reinterpret_cast<float4*>(b + SwOff(y, 16 * h + 4 * q)) =
+                  make_float4(hi[4 * q], hi[4 * q + 1], hi[4 * q + 2], hi[4 * q + 3]);
+               *reinterpret_cast<float4*>(b + kColStageBytes / 2 + SwOff(y, 16 * h + 4 * q)) =
+                  make_float4(lo[4 * q], lo[4 * q + 1], lo[4 * q + 2], lo[4 * q + 3]);
+            }
+            FenceProxyAsync();
+            __syncwarp();
+            if (lane == 0)
+               MbarArrive(&sh->colFull[cs]);
          }
+         if (!ok)
+            break;
          TcFenceBefore();
-         FenceProxyAsync();
-         __syncthreads();
-         const uint32_t bH = SmemAddr(b);
-         issue(s, tmem + 128, bH, bH + kBlockBytes / 2, idesc2, kb == 0);
-         pending[s] = 1;
-      }
-      for (int s = 0; s < kStages; ++s)
-         drain(s);
-      if (!ok)
-         break;
-      TcFenceAfter();
-      // ------------------------------------------------ |E|^2, the plane sum, the normalized plane
-      // TMEM lane r = 32 g + 16 h + i holds x = 16 g + i, part h; columns 128 + y.
-      float I[64];
-      double local = 0.0;
-      const int x = 16 * warp + (lane & 15);
-      if (warp < 4)
-      {
+         __syncwarp();
+         if (lane == 0)
+            MbarArrive(&sh->tFree[j & 1]);
+         // ------------------------------------------------ |E|^2, the plane sum, the normalized plane
+         ok = __all_sync(0xffffffffu, MbarWait(&sh->colDone[j & 1], use, err));
+         if (!ok)
+            break;
+         TcFenceAfter();
+         float I[64];
+         double local = 0.0;
+#pragma unroll
          for (int c0 = 0; c0 < 64; c0 += 32)
          {
             float vv[32];
-            TmemLoad32(tmem + (static_cast<uint32_t>(32 * warp) << 16) + 128 + c0, vv);
+            TmemLoad32(tmem + quad + kTmemCol + 64u * static_cast<uint32_t>(j & 1) + c0, vv);
 #pragma unroll
-            for (int j = 0; j < 32; ++j)
+            for (int c = 0; c < 32; ++c)
             {
-               const float o = __shfl_xor_sync(0xffffffffu, vv[j], 16);
-               const float e = vv[j] * vv[j] + o * o;
-               I[c0 + j] = e;
-               if (lane < 16 && x < P && c0 + j < P)
+               const float o = __shfl_xor_sync(0xffffffffu, vv[c], 16);
+               const float e = vv[c] * vv[c] + o * o;
+               I[c0 + c] = e;
+               if (lane < 16 && x < P && c0 + c < P)
                   local += static_cast<double>(e);
             }
          }
+         TcFenceBefore();
+         __syncwarp();
+         if (lane == 0)
+            MbarArrive(&sh->eFree[j & 1]);
+         double total = 0.0;
+         if (prm.normalize)
+         {
+            for (int o = 16; o > 0; o >>= 1)
+               local += __shfl_xor_sync(0xffffffffu, local, o);
+            if (lane == 0)
+            {
+               sh->sum[j & 1][warp] = local;
+               MbarArrive(&sh->red[j & 1]);
+            }
+            ok = __all_sync(0xffffffffu, MbarWait(&sh->red[j & 1], use, err));
+            if (!ok)
+               break;
+            const volatile double* s = sh->sum[j & 1];
+            total = s[0] + s[1] + s[2] + s[3];
+         }
+         // lanes 0-15 store rows y < 32 of column x, lanes 16-31 rows y >= 32
+         if (x < P)
+         {
+            float* plane = prm.out + static_cast<size_t>(PsfOf(j)) * P * P;
+            const int y0 = 32 * h;
+#pragma unroll
+            for (int c = 0; c < 32; ++c)
+            {
+               const int yy = y0 + c;
+               const float e = h ? I[32 + c] : I[c];
+               if (yy < P)
+                  plane[static_cast<size_t>(yy) * P + x] =
+                     (prm.normalize && total > 0.0) ? static_cast<float>(static_cast<double>(e) / total) : e;
+            }
+         }
       }
-      TcFenceBefore();
-      double total = 0.0;
-      if (prm.normalize)
-      {
-         for (int o = 16; o > 0; o >>= 1)
-            local += __shfl_xor_sync(0xffffffffu, local, o);
-         __syncthreads();
-         if (lane == 0 && warp < 4)
-            sRed[warp] = local;
-         __syncthreads();
-         total = sRed[0] + sRed[1] + sRed[2] + sRed[3];
-      }
-      if (warp < 4 && lane < 16 && x < P)
-      {
-         float* plane = prm.out + static_cast<size_t>(psf) * P * P;
-         for (int yy = 0; yy < P; ++yy)
-            plane[static_cast<size_t>(yy) * P + x] =
-               (prm.normalize && total > 0.0) ? static_cast<float>(static_cast<double>(I[yy]) / total) : I[yy];
-      }
-      __syncthreads();
    }
-   if (!ok && tid == 0)
-      atomicExch(prm.error, 1);
+   if (!ok)
+      *err = 1;
    TcFenceBefore();
    __syncthreads();
    TcFenceAfter();
+   if (tid == 0 && *err)
+      atomicExch(prm.error, 1);
    if (warp == 0)
-      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
 }
 
 } // namespace
@@ -493,6 +677,8 @@ __global__ void __launch_bounds__(kThreads, 1) CztTf32x3Kernel(TcParams prm)
 bool Tf32x3Supports(int M, int P) { return M <= 128 && M % 16 == 0 && P <= 64 && P >= 1; }
 
 size_t AhatBytes(int nSets) { return static_cast<size_t>(nSets) * 8 * kStageBytes; }
+
+static_assert(kSmemBytes <= 227 * 1024, "the chirp-Z kernel's shared memory");
 
 int BuildAhat(iscu_ctx* ctx, const float2* A, const SetParams* sets, const double3* tables, int nSets, int M, int P,
               DevBuf& ahat)
@@ -513,7 +699,7 @@ int BuildAhat(iscu_ctx* ctx, const float2* A, const SetParams* sets, const doubl
 int LaunchCztTf32x3Core(iscu_ctx* ctx, const SetParams* sets, const float* ahat, int nSets, const PsfItem* items,
                         uint32_t nPsf, int M, int P, int normalize, float* out, int* dErr)
 {
-   const size_t smem = 2 * kStages * kStageBytes + 256 + 1024;
+   const size_t smem = kSmemBytes;
    ISCU_CK(cudaFuncSetAttribute(CztTf32x3Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
    TcParams prm;
    prm.sets = sets;
