@@ -43,11 +43,12 @@ __device__ __forceinline__ uint32_t SmemAddr(const void* p)
    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
+// TF32 rounding (to nearest, ties away from zero: cvt.rna.tf32.f32) on the integer pipe: adding half a TF32 unit in
+// the last place to the magnitude bits and clearing the 13 bits TF32 drops rounds the magnitude half away from zero,
+// the carry moving into the exponent where it must (finite inputs).
 __device__ __forceinline__ float ToTf32(float x)
 {
-   uint32_t r;
-   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-   return __uint_as_float(r);
+   return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
 
 // hi = tf32(x), lo = tf32(x - hi)
@@ -170,16 +171,30 @@ __global__ void PhaseTableKernel(const SetParams* __restrict__ sets, const doubl
                                                     : make_double2(sets[s].k0 * t.x + t.z, t.y);
 }
 
-// The pupil phasor of one sample from the phase table: float64 phase, reduced mod 2 pi, then the float32 sine and
-// cosine of the reduced phase by the special-function unit (absolute error ~4e-7 over [-pi, pi]).
+// The pupil phasor of one sample from the phase table: the float64 phase x = base + a opd3F, reduced by quarter turns,
+// x = n pi/2 + r with n = rint(x 2/pi) (formed by adding and taking away 1.5 2^52, exact for |x 2/pi| < 2^51; n's low
+// bits are then the low word of the sum) and |r| <= pi/4 in float64 (pi/2's remaining 6e-17 times n is far below
+// float32's resolution for these phases), then the sine and cosine of r in float32 by their Taylor series (sine to
+// r^9, cosine to r^8: truncation below 3e-8 on [-pi/4, pi/4]; ~1e-7 with float32 rounding) on the FMA pipe, and the
+// quadrant n mod 4 placing them. Outside the aperture: 0.
 __device__ __forceinline__ float2 TablePhasor(double2 t, double a)
 {
-   if (t.y < 0.0)
-      return make_float2(0.f, 0.f);
-   const double ph = ReduceTwoPi(fma(a, t.y, t.x));
-   float sn, cs;
-   __sincosf(static_cast<float>(ph), &sn, &cs);
-   return make_float2(cs, sn);
+   // (no early return outside the aperture: the samples of a thread stay branch-free, so their float64 chains
+   // interleave; the entry (0, -1) gives a finite phase, zeroed at the end)
+   const double x = fma(a, t.y, t.x);
+   const double kRound = 6755399441055744.0;   // 1.5 2^52
+   const double nr = fma(x, 0.63661977236758134308, kRound);   // x 2/pi + 1.5 2^52
+   const int q = __double2loint(nr);
+   const double n = nr - kRound;
+   const float r = static_cast<float>(fma(-n, 1.5707963267948966192, x));
+   const float r2 = r * r;
+   const float sn = fmaf(r * r2, fmaf(r2, fmaf(r2, fmaf(r2, 1.0f / 362880.0f, -1.0f / 5040.0f), 1.0f / 120.0f),
+                                      -1.0f / 6.0f), r);
+   const float cs = fmaf(r2, fmaf(r2, fmaf(r2, fmaf(r2, 1.0f / 40320.0f, -1.0f / 720.0f), 1.0f / 24.0f), -0.5f), 1.0f);
+   // (cos x, sin x) = (cos r, sin r) turned by q quarter turns
+   const float c0 = (q & 1) ? sn : cs, s0 = (q & 1) ? cs : sn;
+   const bool in = t.y >= 0.0;
+   return make_float2(in ? ((q + 1) & 2 ? -c0 : c0) : 0.f, in ? (q & 2 ? -s0 : s0) : 0.f);
 }
 
 // ------------------------------------------------------------------------------------------ async copies
@@ -228,15 +243,22 @@ constexpr int kRowStages = 3;                      // row-pass B blocks (pupil p
 constexpr int kColStages = 2;                      // column-pass B blocks (T, split)
 constexpr int kStageBytes = 2 * kBlockBytes;       // an A or row-pass B block: hi and lo images of 128 rows
 constexpr int kColStageBytes = kBlockBytes;        // a column-pass B block: hi and lo images of 64 rows
+// Warp roles. Warps share an SM sub-partition (scheduler) when equal mod 4: the MMA warp's (0) holds no producer.
 constexpr int kDrainWarps = 4;                     // warps 0-3, one per TMEM lane quadrant
-constexpr int kMmaWarp = 4;                        // lane 0 issues the MMAs and the Ahat copies
-constexpr int kFirstProducer = 5;                  // warps 5-15 make the pupil phasors
-constexpr int kProducerThreads = kThreads - 32 * kFirstProducer;
-constexpr int kItemsPerBlock = 1024;               // (pupil column, pair of pupil rows) items of one row-pass block
+constexpr int kMmaWarp = 4;                        // lane 0 issues the row-pass MMAs
+constexpr int kLoadWarp = 8;                       // lane 0 issues the Ahat copies
+constexpr int kColMmaWarp = 12;                    // lane 0 issues the column-pass MMAs
+constexpr int kProducerWarps = 9;                  // warps 5-7, 9-11, 13-15 make the pupil phasors
+constexpr int kProducerThreads = 32 * kProducerWarps;
+constexpr int kItemsPerBlock = 512;                // (pupil column, 4 pupil rows) items of one row-pass block
 constexpr int kItemRounds = (kItemsPerBlock + kProducerThreads - 1) / kProducerThreads;
+
+// A producer warp's index 0..8 (warps 5-7, 9-11, 13-15).
+__device__ __forceinline__ int ProducerIndex(int warp) { return warp - 5 - (warp >= 9) - (warp >= 13); }
 constexpr int kTmemRow = 0;                        // T of PSF j: columns [128 (j % 2), +128)
 constexpr int kTmemCol = 256;                      // E of PSF j: columns [256 + 64 (j % 2), +64)
 constexpr uint64_t kWaitNs = 4000000000ull;        // a wait gives up after 4 s
+constexpr int kSetCache = 160;                     // PSF sets staged in shared memory (the MMA thread's A sources)
 
 struct Shared
 {
@@ -244,8 +266,9 @@ struct Shared
    uint64_t rowFull[kRowStages], rowEmpty[kRowStages];
    uint64_t colFull[kColStages], colEmpty[kColStages];
    uint64_t rowDone[2], colDone[2], tFree[2], eFree[2], red[2];
-   uint64_t final;
+   uint64_t final[2];
    double sum[2][kDrainWarps];
+   int set[kSetCache];   // the set of the CTA's j-th PSF, j < kSetCache
    uint32_t tmemSlot;
    int err;
 };
@@ -260,7 +283,9 @@ __device__ __forceinline__ uint64_t GlobalNs()
 }
 
 // Waits for the phase of the given parity to complete. false after kWaitNs, or (err non-null) once *err is set.
-__device__ __forceinline__ bool MbarWait(uint64_t* bar, uint32_t parity, const volatile int* err)
+// backoff: after a few polls the thread sleeps between polls, leaving its scheduler's issue slots to the warps that
+// share it (the MMA thread polls without it: its waits are on the critical path).
+__device__ __forceinline__ bool MbarWait(uint64_t* bar, uint32_t parity, const volatile int* err, bool backoff = true)
 {
    const uint32_t a = SmemAddr(bar);
    uint64_t t0 = 0;
@@ -273,6 +298,8 @@ __device__ __forceinline__ bool MbarWait(uint64_t* bar, uint32_t parity, const v
                    : "memory");
       if (done)
          return true;
+      if (backoff && it >= 2)
+         __nanosleep(it < 16 ? 32 : 128);
       if ((it & 15) == 15)
       {
          if (err && *err)
@@ -307,41 +334,17 @@ __device__ __forceinline__ void TmemLoad16(uint32_t taddr, float* v)
       v[i] = __uint_as_float(r[i]);
 }
 
-// The CTA's j-th PSF.
-__device__ __forceinline__ int PsfOf(int j) { return static_cast<int>(blockIdx.x) + j * static_cast<int>(gridDim.x); }
-
-// The MMA order of a CTA's K blocks: R(0), R(1), C(0), R(2), C(1), ..., R(n - 1), C(n - 2), C(n - 1), each pass nKb
-// blocks (R: row pass, C: column pass), so the column pass of one PSF runs on the tensor cores while the producers
-// make the next PSFs' pupils. Block t -> its PSF j, its pass and K block kb.
-__device__ __forceinline__ void JobOf(int t, int nKb, int nLocal, int& j, bool& row, int& kb)
-{
-   const int seg = t / nKb;
-   kb = t % nKb;
-   if (seg == 0)
-   {
-      j = 0;
-      row = true;
-      return;
-   }
-   const int u = seg - 1;
-   if ((u & 1) == 0 && u / 2 + 1 < nLocal)
-   {
-      j = u / 2 + 1;
-      row = true;
-   }
-   else
-   {
-      j = (u & 1) ? (u - 1) / 2 : nLocal - 1;
-      row = false;
-   }
-}
-
-// Per CTA, persistent over its PSFs (blockIdx.x + j gridDim.x), warp-specialized; the roles meet only at mbarriers:
-//   producers (warps 5-15): per row-pass K block the pupil phasors of 16 pupil rows (float64 phase, reduced mod 2 pi,
-//     SFU sine and cosine, TF32 hi/lo split) into a row-B stage -> rowFull;
-//   the MMA thread (warp 4, lane 0): the Ahat K blocks by bulk copy into the A ring (two blocks ahead), and per K
-//     block 12 MMAs (hi*hi, hi*lo, lo*hi over 4 K steps) in the MMA order of JobOf; commits free the stages and mark
-//     a pass done (rowDone / colDone);
+// Per CTA, persistent over a contiguous run of PSFs (neighbours in the item list usually share their request set),
+// warp-specialized; the roles meet only at mbarriers:
+//   producers (warps 5-7, 9-11, 13-15): per row-pass K block the pupil phasors of 16 pupil rows (float64 phase,
+//     reduced by quarter turns, float32 sine and cosine, TF32 hi/lo split) into a row-B stage -> rowFull;
+//   the copy thread (warp 8, lane 0): the Ahat K blocks by bulk copy into the A ring, in the MMA order, each once the
+//     MMAs that used the stage kAStages slots earlier are done (aEmpty);
+//   the MMA threads (warp 4 the row passes R(j), warp 12 the column passes C(j), each lane 0): the Ahat order is R(0),
+//     then per PSF j >= 1 R(j) and C(j - 1) K block by K block, then C(n - 1), so the column pass of one PSF runs
+//     beside the row pass of the next; when PSFs j and j - 1 share their set, one Ahat copy serves both blocks (its
+//     stage frees when both threads' MMAs are done). Per K block 12 MMAs (hi*hi, hi*lo, lo*hi over 4 K steps);
+//     commits free the stages and mark a pass done (rowDone / colDone);
 //   drain warps (0-3, one TMEM lane quadrant each): T of PSF j from TMEM, split, into col-B stages -> colFull (then
 //     tFree: T's columns may take PSF j + 2); then E of PSF j: |E|^2, the plane sum, the normalized plane (eFree).
 // T and E are double-buffered in TMEM (512 columns). Every wait is bounded (kWaitNs) and also ends when another role
@@ -359,10 +362,11 @@ __global__ void __launch_bounds__(kThreads, 1) CztTf32x3Kernel(TcParams prm)
 
    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
    const int M = prm.M, P = prm.P, nKb = M / 16;
-   const int nLocal = prm.nPsf > static_cast<int>(blockIdx.x)
-                         ? (prm.nPsf - static_cast<int>(blockIdx.x) + static_cast<int>(gridDim.x) - 1) /
-                              static_cast<int>(gridDim.x)
-                         : 0;
+   // this CTA's PSFs: psf0 .. psf0 + nLocal - 1
+   const int perCta = prm.nPsf / static_cast<int>(gridDim.x), extra = prm.nPsf % static_cast<int>(gridDim.x);
+   const int cta = static_cast<int>(blockIdx.x);
+   const int psf0 = cta * perCta + min(cta, extra), nLocal = perCta + (cta < extra ? 1 : 0);
+   auto psfOf = [&](int j) { return psf0 + j; };
 
    if (warp == 0)
    {
@@ -375,11 +379,11 @@ __global__ void __launch_bounds__(kThreads, 1) CztTf32x3Kernel(TcParams prm)
       for (int s = 0; s < kAStages; ++s)
       {
          MbarInit(&sh->aFull[s], 1);
-         MbarInit(&sh->aEmpty[s], 1);
+         MbarInit(&sh->aEmpty[s], 2);   // the row-pass and the column-pass MMA threads
       }
       for (int s = 0; s < kRowStages; ++s)
       {
-         MbarInit(&sh->rowFull[s], kThreads / 32 - kFirstProducer);
+         MbarInit(&sh->rowFull[s], kProducerWarps);
          MbarInit(&sh->rowEmpty[s], 1);
       }
       for (int s = 0; s < kColStages; ++s)
@@ -395,41 +399,67 @@ __global__ void __launch_bounds__(kThreads, 1) CztTf32x3Kernel(TcParams prm)
          MbarInit(&sh->eFree[s], kDrainWarps);
          MbarInit(&sh->red[s], kDrainWarps);
       }
-      MbarInit(&sh->final, 1);
+      MbarInit(&sh->final[0], 1);
+      MbarInit(&sh->final[1], 1);
       sh->err = 0;
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
    }
+   for (int j = tid; j < nLocal && j < kSetCache; j += kThreads)
+      sh->set[j] = prm.items[psfOf(j)].set;
    TcFenceBefore();
    __syncthreads();
    TcFenceAfter();
    const uint32_t tmem = sh->tmemSlot;
    bool ok = true;
+   auto setOf = [&](int j) { return j < kSetCache ? sh->set[j] : prm.items[psfOf(j)].set; };
 
-   if (warp >= kFirstProducer)
+   if (warp > kMmaWarp && warp != kLoadWarp && warp != kColMmaWarp)
    {
       // ---------------------------------------------------------------- producers: row-pass B blocks
-      const int ptid = tid - 32 * kFirstProducer;
+      // A thread's work per row-pass block: items ptid + r kProducerThreads (pupil column m, pupil rows n .. n + 3).
+      // The table entries of the next block are in flight while a block computes, and the next PSF's item and
+      // defocus factor are fetched half a PSF ahead.
+      const int ptid = 32 * ProducerIndex(warp) + lane;
+      auto load = [&](const double2* tab, int kb, double2 (*dst)[4]) {
+#pragma unroll
+         for (int r = 0; r < kItemRounds; ++r)
+         {
+            const int item = ptid + r * kProducerThreads, m = item & 127, n = 16 * kb + 4 * (item >> 7);
+            const bool in = item < kItemsPerBlock && m < M;
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+               dst[r][c] = in ? tab[static_cast<size_t>(n + c) * M + m] : make_double2(0.0, -1.0);
+         }
+      };
+      PsfItem itNext = prm.items[psfOf(0)];
+      double k0niNext = prm.sets[itNext.set].k0 * prm.sets[itNext.set].ni;
+      double2 nxt[kItemRounds][4];
+      load(prm.phase + static_cast<size_t>(itNext.set) * M * M, 0, nxt);
       uint32_t rowCount = 0;
       for (int j = 0; j < nLocal && ok; ++j)
       {
-         const PsfItem it = prm.items[PsfOf(j)];
-         const double aDef = prm.sets[it.set].k0 * prm.sets[it.set].ni * it.dtiM;
-         const double2* tab = prm.phase + static_cast<size_t>(it.set) * M * M;
+         const double aDef = k0niNext * itNext.dtiM;
+         const double2* tab = prm.phase + static_cast<size_t>(itNext.set) * M * M;
+         if (j + 1 < nLocal)
+            itNext = prm.items[psfOf(j + 1)];
          for (int kb = 0; kb < nKb; ++kb, ++rowCount)
          {
+            if (kb == nKb / 2 && j + 1 < nLocal)   // (the next PSF's item has landed)
+               k0niNext = prm.sets[itNext.set].k0 * prm.sets[itNext.set].ni;
+            double2 cur[kItemRounds][4];
+#pragma unroll
+            for (int r = 0; r < kItemRounds; ++r)
+#pragma unroll
+               for (int c = 0; c < 4; ++c)
+                  cur[r][c] = nxt[r][c];
+            if (kb + 1 < nKb)
+               load(tab, kb + 1, nxt);
+            else if (j + 1 < nLocal)
+               load(prm.phase + static_cast<size_t>(itNext.set) * M * M, 0, nxt);
             const int rs = static_cast<int>(rowCount % kRowStages);
             ok = __all_sync(0xffffffffu, MbarWait(&sh->rowEmpty[rs], ((rowCount / kRowStages) & 1u) ^ 1u, err));
             if (!ok)
                break;
-            double2 t[kItemRounds][2];
-#pragma unroll
-            for (int r = 0; r < kItemRounds; ++r)
-            {
-               const int item = ptid + r * kProducerThreads, m = item & 127, n = 16 * kb + 2 * (item >> 7);
-               const bool in = item < kItemsPerBlock && m < M;
-               t[r][0] = in ? tab[static_cast<size_t>(n) * M + m] : make_double2(0.0, -1.0);
-               t[r][1] = in ? tab[static_cast<size_t>(n + 1) * M + m] : make_double2(0.0, -1.0);
-            }
             unsigned char* b = sRowB + rs * kStageBytes;
 #pragma unroll
             for (int r = 0; r < kItemRounds; ++r)
@@ -437,18 +467,21 @@ __global__ void __launch_bounds__(kThreads, 1) CztTf32x3Kernel(TcParams prm)
                const int item = ptid + r * kProducerThreads;
                if (item < kItemsPerBlock)
                {
-                  const int m = item & 127, nl = 2 * (item >> 7);
-                  const float2 u0 = TablePhasor(t[r][0], aDef), u1 = TablePhasor(t[r][1], aDef);
-                  float rh0, rl0, ih0, il0, rh1, rl1, ih1, il1;
-                  Split(u0.x, rh0, rl0);
-                  Split(u0.y, ih0, il0);
-                  Split(u1.x, rh1, rl1);
-                  Split(u1.y, ih1, il1);
-                  // B[m][nl], B[m][nl + 1]: the real parts of pupil rows n, n + 1; B[m][16 + nl ..]: the imaginary
-                  *reinterpret_cast<float2*>(b + SwOff(m, nl)) = make_float2(rh0, rh1);
-                  *reinterpret_cast<float2*>(b + SwOff(m, 16 + nl)) = make_float2(ih0, ih1);
-                  *reinterpret_cast<float2*>(b + kBlockBytes + SwOff(m, nl)) = make_float2(rl0, rl1);
-                  *reinterpret_cast<float2*>(b + kBlockBytes + SwOff(m, 16 + nl)) = make_float2(il0, il1);
+                  const int m = item & 127, nl = 4 * (item >> 7);
+                  float rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+                  for (int c = 0; c < 4; ++c)
+                  {
+                     const float2 u = TablePhasor(cur[r][c], aDef);
+                     Split(u.x, rh[c], rl[c]);
+                     Split(u.y, ih[c], il[c]);
+                  }
+                  // B[m][nl + c]: the real part of pupil row 16 kb + nl + c; B[m][16 + nl + c]: the imaginary part
+                  *reinterpret_cast<float4*>(b + SwOff(m, nl)) = make_float4(rh[0], rh[1], rh[2], rh[3]);
+                  *reinterpret_cast<float4*>(b + SwOff(m, 16 + nl)) = make_float4(ih[0], ih[1], ih[2], ih[3]);
+                  *reinterpret_cast<float4*>(b + kBlockBytes + SwOff(m, nl)) = make_float4(rl[0], rl[1], rl[2], rl[3]);
+                  *reinterpret_cast<float4*>(b + kBlockBytes + SwOff(m, 16 + nl)) =
+                     make_float4(il[0], il[1], il[2], il[3]);
                }
             }
             FenceProxyAsync();
@@ -458,103 +491,131 @@ __global__ void __launch_bounds__(kThreads, 1) CztTf32x3Kernel(TcParams prm)
          }
       }
    }
-   else if (warp == kMmaWarp)
+   else if (warp == kLoadWarp)
    {
-      // ---------------------------------------------------------------- the MMA thread
+      // ---------------------------------------------------------------- the Ahat copies, in MMA order
       if (lane == 0 && nLocal > 0)
       {
-         const int nJobs = 2 * nLocal * nKb;
-         const uint32_t idesc1 = InstrDesc(kRows, M), idesc2 = InstrDesc(kRows, 64);
-         int loaded = 0;   // A blocks whose copy was started
-         // block t's Ahat K block into stage t % kAStages, once the MMAs of block t - kAStages are done
-         auto loadA = [&](int t) -> bool {
-            const int st = t % kAStages;
-            if (t >= kAStages && !MbarWait(&sh->aEmpty[st], static_cast<uint32_t>(t / kAStages - 1) & 1u, err))
-               return false;
-            int j, kb;
-            bool row;
-            JobOf(t, nKb, nLocal, j, row, kb);
-            const float* src = prm.ahat + (static_cast<size_t>(prm.items[PsfOf(j)].set) * 8 + kb) * (kStageBytes / 4);
-            MbarExpectTx(&sh->aFull[st], kStageBytes);
-            BulkLoad(sA + st * kStageBytes, src, kStageBytes, &sh->aFull[st]);
-            loaded = t + 1;
-            return true;
-         };
-         int consumed = 0;
-         uint32_t rowCount = 0, colCount = 0;
-         for (int t = 0; t < kAStages - 1 && t < nJobs && ok; ++t)
-            ok = loadA(t);
-         for (int t = 0; t < nJobs && ok; ++t)
+         int slot = 0;
+         int last[kAStages] = {-1, -1, -1};   // the latest slot copied into each stage
+         for (int seg = 0; seg <= nLocal && ok; ++seg)
          {
-            int j, kb;
-            bool row;
-            JobOf(t, nKb, nLocal, j, row, kb);
-            const uint32_t use = static_cast<uint32_t>(j >> 1) & 1u;
-            if (kb == 0)   // the accumulator's TMEM columns are free (PSF j - 2 is past them)
-               ok = MbarWait(row ? &sh->tFree[j & 1] : &sh->eFree[j & 1], use ^ 1u, err);
-            uint64_t* full;
-            uint64_t* empty;
-            uint32_t parity, bH, bL, d, idesc;
-            if (row)
-            {
-               const int rs = static_cast<int>(rowCount % kRowStages);
-               full = &sh->rowFull[rs];
-               empty = &sh->rowEmpty[rs];
-               parity = (rowCount / kRowStages) & 1u;
-               bH = SmemAddr(sRowB + rs * kStageBytes);
-               bL = bH + kBlockBytes;
-               d = tmem + kTmemRow + 128u * static_cast<uint32_t>(j & 1);
-               idesc = idesc1;
-            }
-            else
-            {
-               const int cs = static_cast<int>(colCount % kColStages);
-               full = &sh->colFull[cs];
-               empty = &sh->colEmpty[cs];
-               parity = (colCount / kColStages) & 1u;
-               bH = SmemAddr(sColB + cs * kColStageBytes);
-               bL = bH + kColStageBytes / 2;
-               d = tmem + kTmemCol + 64u * static_cast<uint32_t>(j & 1);
-               idesc = idesc2;
-            }
-            ok = ok && MbarWait(full, parity, err);
-            ok = ok && MbarWait(&sh->aFull[t % kAStages], static_cast<uint32_t>(t / kAStages) & 1u, err);
-            if (!ok)
-               break;
-            consumed = t + 1;
-            TcFenceAfter();
-            const uint32_t aH = SmemAddr(sA + (t % kAStages) * kStageBytes), aL = aH + kBlockBytes;
-#pragma unroll
-            for (int kk = 0; kk < 4; ++kk)
-            {
-               const uint32_t off = kk * 32;   // 8 TF32 = 32 bytes along K
-               Mma(d, SmemDesc(aH + off), SmemDesc(bH + off), idesc, (kb == 0 && kk == 0) ? 0u : 1u);
-               Mma(d, SmemDesc(aH + off), SmemDesc(bL + off), idesc, 1u);
-               Mma(d, SmemDesc(aL + off), SmemDesc(bH + off), idesc, 1u);
-            }
-            Commit(empty);
-            Commit(&sh->aEmpty[t % kAStages]);
-            if (kb == nKb - 1)
-               Commit(row ? &sh->rowDone[j & 1] : &sh->colDone[j & 1]);
-            if (row)
-               ++rowCount;
-            else
-               ++colCount;
-            if (t + kAStages - 1 < nJobs)
-               ok = loadA(t + kAStages - 1);   // waits for the MMAs of block t - 1
+            const int jR = seg < nLocal ? seg : -1, jC = seg - 1;
+            const bool shared = jR >= 0 && jC >= 0 && setOf(jR) == setOf(jC);
+            for (int kb = 0; kb < nKb && ok; ++kb)
+               for (int part = 0; part < 2 && ok; ++part)
+               {
+                  const int jj = part == 0 ? jR : jC;
+                  if (jj < 0 || (part == 1 && shared))
+                     continue;
+                  const int st = slot % kAStages;
+                  if (slot >= kAStages)   // the MMAs of the slot kAStages earlier are done with the stage
+                     ok = MbarWait(&sh->aEmpty[st], static_cast<uint32_t>(slot / kAStages - 1) & 1u, err);
+                  if (!ok)
+                     break;
+                  MbarExpectTx(&sh->aFull[st], kStageBytes);
+                  BulkLoad(sA + st * kStageBytes,
+                           prm.ahat + (static_cast<size_t>(setOf(jj)) * 8 + kb) * (kStageBytes / 4), kStageBytes,
+                           &sh->aFull[st]);
+                  last[st] = slot++;
+               }
          }
          if (!ok)
          {
             *err = 1;
-            // let the copies and MMAs in flight land before the CTA frees its memory
-            for (int t = consumed; t < loaded; ++t)
-               MbarWait(&sh->aFull[t % kAStages], static_cast<uint32_t>(t / kAStages) & 1u, nullptr);
-            Commit(&sh->final);
-            MbarWait(&sh->final, 0u, nullptr);
+            for (int st = 0; st < kAStages; ++st)   // the copies in flight land before the CTA frees its memory
+               if (last[st] >= 0)
+                  MbarWait(&sh->aFull[st], static_cast<uint32_t>(last[st] / kAStages) & 1u, nullptr);
          }
       }
    }
-   else
+   else if (warp == kMmaWarp || warp == kColMmaWarp)
+   {
+      // ---------------------------------------------------------------- the MMA threads
+      // Warp 4 issues the row passes, warp 12 the column passes: their accumulators are apart in TMEM, so each
+      // thread's waits and bookkeeping overlap the other's MMAs (one thread's queue of MMAs is short).
+      const int mine = warp == kMmaWarp ? 0 : 1;
+      if (lane == 0 && nLocal > 0)
+      {
+         const bool row = mine == 0;
+         const uint32_t idesc = row ? InstrDesc(kRows, M) : InstrDesc(kRows, 64);
+         uint32_t count = 0;   // this thread's K blocks so far (its B ring's position)
+         int slot = 0;
+         for (int seg = 0; seg <= nLocal && ok; ++seg)
+         {
+            const int jR = seg < nLocal ? seg : -1, jC = seg - 1;
+            const bool shared = jR >= 0 && jC >= 0 && setOf(jR) == setOf(jC);
+            for (int kb = 0; kb < nKb && ok; ++kb)
+               for (int part = 0; part < 2 && ok; ++part)
+               {
+                  const int jj = part == 0 ? jR : jC;
+                  if (jj < 0)
+                     continue;
+                  const int st = slot % kAStages;
+                  const uint32_t aParity = static_cast<uint32_t>(slot / kAStages) & 1u;
+                  if (!shared || part == 1)   // the next block takes the next Ahat slot
+                     ++slot;
+                  if (part != mine)
+                     continue;
+                  // K block kb of PSF jj's pass on Ahat stage st
+                  const uint32_t use = static_cast<uint32_t>(jj >> 1) & 1u;
+                  if (kb == 0)   // the accumulator's TMEM columns are free (PSF jj - 2 is past them)
+                     ok = MbarWait(row ? &sh->tFree[jj & 1] : &sh->eFree[jj & 1], use ^ 1u, err, false);
+                  uint64_t* full;
+                  uint64_t* empty;
+                  uint32_t parity, bH, bL, d;
+                  if (row)
+                  {
+                     const int rs = static_cast<int>(count % kRowStages);
+                     full = &sh->rowFull[rs];
+                     empty = &sh->rowEmpty[rs];
+                     parity = (count / kRowStages) & 1u;
+                     bH = SmemAddr(sRowB + rs * kStageBytes);
+                     bL = bH + kBlockBytes;
+                     d = tmem + kTmemRow + 128u * static_cast<uint32_t>(jj & 1);
+                  }
+                  else
+                  {
+                     const int cs = static_cast<int>(count % kColStages);
+                     full = &sh->colFull[cs];
+                     empty = &sh->colEmpty[cs];
+                     parity = (count / kColStages) & 1u;
+                     bH = SmemAddr(sColB + cs * kColStageBytes);
+                     bL = bH + kColStageBytes / 2;
+                     d = tmem + kTmemCol + 64u * static_cast<uint32_t>(jj & 1);
+                  }
+                  ok = ok && MbarWait(&sh->aFull[st], aParity, err, false);
+                  ok = ok && MbarWait(full, parity, err, false);
+                  if (!ok)
+                     break;
+                  TcFenceAfter();
+                  const uint32_t aH = SmemAddr(sA + st * kStageBytes), aL = aH + kBlockBytes;
+#pragma unroll
+                  for (int kk = 0; kk < 4; ++kk)
+                  {
+                     const uint32_t off = kk * 32;   // 8 TF32 = 32 bytes along K
+                     Mma(d, SmemDesc(aH + off), SmemDesc(bH + off), idesc, (kb == 0 && kk == 0) ? 0u : 1u);
+                     Mma(d, SmemDesc(aH + off), SmemDesc(bL + off), idesc, 1u);
+                     Mma(d, SmemDesc(aL + off), SmemDesc(bH + off), idesc, 1u);
+                  }
+                  Commit(empty);
+                  Commit(&sh->aEmpty[st]);
+                  if (!shared)   // the slot's only user arrives for both
+                     Commit(&sh->aEmpty[st]);
+                  if (kb == nKb - 1)
+                     Commit(row ? &sh->rowDone[jj & 1] : &sh->colDone[jj & 1]);
+                  ++count;
+               }
+         }
+         if (!ok)
+         {
+            *err = 1;
+            Commit(&sh->final[mine]);   // this thread's MMAs in flight finish before the CTA frees its TMEM
+            MbarWait(&sh->final[mine], 0u, nullptr);
+         }
+      }
+   }
+   else if (warp < kDrainWarps)
    {
       // ---------------------------------------------------------------- drain warps
       // TMEM lane r = 32 w + 16 h + i of T holds row y = 16 w + i, part h (columns: the pupil column m); of E, output
@@ -608,7 +669,7 @@ __global__ void __launch_bounds__(kThreads, 1) CztTf32x3Kernel(TcParams prm)
             break;
          TcFenceAfter();
          float I[64];
-         double local = 0.0;
+         float part[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};   // eight float partial sums of 8 values each
 #pragma unroll
          for (int c0 = 0; c0 < 64; c0 += 32)
          {
@@ -620,10 +681,15 @@ __global__ void __launch_bounds__(kThreads, 1) CztTf32x3Kernel(TcParams prm)
                const float o = __shfl_xor_sync(0xffffffffu, vv[c], 16);
                const float e = vv[c] * vv[c] + o * o;
                I[c0 + c] = e;
-               if (lane < 16 && x < P && c0 + c < P)
-                  local += static_cast<double>(e);
+               if (c0 + c < P)
+                  part[(c0 + c) >> 3] += e;
             }
          }
+         double local = 0.0;
+         if (lane < 16 && x < P)
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+               local += static_cast<double>(part[k]);
          TcFenceBefore();
          __syncwarp();
          if (lane == 0)
@@ -644,10 +710,12 @@ __global__ void __launch_bounds__(kThreads, 1) CztTf32x3Kernel(TcParams prm)
             const volatile double* s = sh->sum[j & 1];
             total = s[0] + s[1] + s[2] + s[3];
          }
-         // lanes 0-15 store rows y < 32 of column x, lanes 16-31 rows y >= 32
+         // lanes 0-15 store rows y < 32 of column x, lanes 16-31 rows y >= 32; the plane times 1 / sum (the float
+         // product is within an ulp or two of the float64 quotient)
          if (x < P)
          {
-            float* plane = prm.out + static_cast<size_t>(PsfOf(j)) * P * P;
+            float* plane = prm.out + static_cast<size_t>(psfOf(j)) * P * P;
+            const float scale = (prm.normalize && total > 0.0) ? static_cast<float>(1.0 / total) : 1.0f;
             const int y0 = 32 * h;
 #pragma unroll
             for (int c = 0; c < 32; ++c)
@@ -655,8 +723,7 @@ __global__ void __launch_bounds__(kThreads, 1) CztTf32x3Kernel(TcParams prm)
                const int yy = y0 + c;
                const float e = h ? I[32 + c] : I[c];
                if (yy < P)
-                  plane[static_cast<size_t>(yy) * P + x] =
-                     (prm.normalize && total > 0.0) ? static_cast<float>(static_cast<double>(e) / total) : e;
+                  plane[static_cast<size_t>(yy) * P + x] = e * scale;
             }
          }
       }
