@@ -12,16 +12,15 @@
 // k = 32 j + 16 h' + c is input q = 16 j + c, part h' -- so one 32-wide K block holds 16 input indices' real and
 // imaginary parts, and one warp's 32 TMEM lanes hold 16 outputs' real and imaginary parts.
 //
-// TF32 x 3: every operand x is split into hi = tf32(x) and lo = tf32(x - hi); a product is hi*hi + hi*lo + lo*hi
-// (the dropped lo*lo and the roundings are ~2^-21 relative), accumulated in float32 in TMEM. The pupil phasors come
-// from float64 phases (psf_common.cuh) and are split in registers; the row-pass result is read from TMEM, split and
-// written as the column pass's B operand; |E|^2 and the plane's sum-1 normalization finish in registers.
+// TF32 x 3: every operand x is split into hi = tf32(x) and lo = x - hi (read by the tensor cores as TF32); a product
+// is hi*hi + hi*lo + lo*hi (the dropped lo*lo and the roundings are ~2^-21 relative), accumulated in float32 in TMEM.
+// The pupil phasors come from float64 phases (the per-set phase tables) and are split in registers; the row-pass
+// result is read from TMEM, split and written as the column pass's B operand; |E|^2 and the plane's sum-1
+// normalization finish in registers.
 //
-// Per CTA (persistent over PSFs, 256 threads): operands staged in shared memory in the canonical 128-byte-swizzled
-// K-major layout (8-row x 128-byte atoms, 1024-byte aligned), two stages for the A/B K blocks of the row pass; one
-// thread issues tcgen05.mma (M = 128, K = 8 per instruction) and tcgen05.commit to an mbarrier per stage; warps 0-3
-// read TMEM back with tcgen05.ld. Every mbarrier wait is bounded: on timeout the CTA records an error, stops issuing,
-// frees its TMEM and returns.
+// The kernel (CztTf32x3Kernel, below) is persistent and warp-specialized: producer warps build the pupil operand, a
+// copy thread streams the DFT operand with bulk copies, two threads issue the MMAs (row passes, column passes) and
+// four warps drain TMEM; the roles meet only at mbarriers with bounded waits.
 
 #include "iscu_internal.h"
 #include "psf_common.cuh"
@@ -51,11 +50,12 @@ __device__ __forceinline__ float ToTf32(float x)
    return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
 
-// hi = tf32(x), lo = tf32(x - hi)
+// hi = tf32(x), lo = x - hi (exact in float32; the tensor cores read its TF32 part, truncated: |x - hi - lo_tf32| <
+// 2^-21 |x|)
 __device__ __forceinline__ void Split(float x, float& hi, float& lo)
 {
    hi = ToTf32(x);
-   lo = ToTf32(x - hi);
+   lo = x - hi;
 }
 
 __device__ __forceinline__ void MbarInit(uint64_t* bar, uint32_t count)
@@ -171,30 +171,22 @@ __global__ void PhaseTableKernel(const SetParams* __restrict__ sets, const doubl
                                                     : make_double2(sets[s].k0 * t.x + t.z, t.y);
 }
 
-// The pupil phasor of one sample from the phase table: the float64 phase x = base + a opd3F, reduced by quarter turns,
-// x = n pi/2 + r with n = rint(x 2/pi) (formed by adding and taking away 1.5 2^52, exact for |x 2/pi| < 2^51; n's low
-// bits are then the low word of the sum) and |r| <= pi/4 in float64 (pi/2's remaining 6e-17 times n is far below
-// float32's resolution for these phases), then the sine and cosine of r in float32 by their Taylor series (sine to
-// r^9, cosine to r^8: truncation below 3e-8 on [-pi/4, pi/4]; ~1e-7 with float32 rounding) on the FMA pipe, and the
-// quadrant n mod 4 placing them. Outside the aperture: 0.
+// The pupil phasor of one sample from the phase table: the float64 phase x = base + a opd3F, reduced mod 2 pi as
+// x - 2 pi n with n = rint(x / 2 pi) (formed by adding and taking away 1.5 2^52, exact for |x / 2 pi| < 2^51) and
+// 2 pi's float64 value (its remaining 2.4e-16 times n is far below float32's resolution for these phases), then the
+// float32 sine and cosine of the reduced phase by the special-function unit (absolute error ~4e-7 over [-pi, pi]).
+// Branch-free, so a thread's samples interleave: outside the aperture (opd3F < 0) the entry (0, -1) gives a finite
+// phase, zeroed at the end.
 __device__ __forceinline__ float2 TablePhasor(double2 t, double a)
 {
-   // (no early return outside the aperture: the samples of a thread stay branch-free, so their float64 chains
-   // interleave; the entry (0, -1) gives a finite phase, zeroed at the end)
    const double x = fma(a, t.y, t.x);
    const double kRound = 6755399441055744.0;   // 1.5 2^52
-   const double nr = fma(x, 0.63661977236758134308, kRound);   // x 2/pi + 1.5 2^52
-   const int q = __double2loint(nr);
-   const double n = nr - kRound;
-   const float r = static_cast<float>(fma(-n, 1.5707963267948966192, x));
-   const float r2 = r * r;
-   const float sn = fmaf(r * r2, fmaf(r2, fmaf(r2, fmaf(r2, 1.0f / 362880.0f, -1.0f / 5040.0f), 1.0f / 120.0f),
-                                      -1.0f / 6.0f), r);
-   const float cs = fmaf(r2, fmaf(r2, fmaf(r2, fmaf(r2, 1.0f / 40320.0f, -1.0f / 720.0f), 1.0f / 24.0f), -0.5f), 1.0f);
-   // (cos x, sin x) = (cos r, sin r) turned by q quarter turns
-   const float c0 = (q & 1) ? sn : cs, s0 = (q & 1) ? cs : sn;
+   const double n = fma(x, 0.15915494309189533577, kRound) - kRound;
+   const float r = static_cast<float>(fma(-n, 6.283185307179586232, x));
+   float sn, cs;
+   __sincosf(r, &sn, &cs);
    const bool in = t.y >= 0.0;
-   return make_float2(in ? ((q + 1) & 2 ? -c0 : c0) : 0.f, in ? (q & 2 ? -s0 : s0) : 0.f);
+   return make_float2(in ? cs : 0.f, in ? sn : 0.f);
 }
 
 // ------------------------------------------------------------------------------------------ async copies
