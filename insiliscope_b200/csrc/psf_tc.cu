@@ -250,7 +250,7 @@ __device__ __forceinline__ int ProducerIndex(int warp) { return warp - 5 - (warp
 constexpr int kTmemRow = 0;                        // T of PSF j: columns [128 (j % 2), +128)
 constexpr int kTmemCol = 256;                      // E of PSF j: columns [256 + 64 (j % 2), +64)
 constexpr uint64_t kWaitNs = 4000000000ull;        // a wait gives up after 4 s
-constexpr int kSetCache = 160;                     // PSF sets staged in shared memory (the MMA thread's A sources)
+constexpr int kSetCache = 96;                      // PSFs whose set and defocus factor are staged in shared memory
 
 struct Shared
 {
@@ -260,7 +260,8 @@ struct Shared
    uint64_t rowDone[2], colDone[2], tFree[2], eFree[2], red[2];
    uint64_t final[2];
    double sum[2][kDrainWarps];
-   int set[kSetCache];   // the set of the CTA's j-th PSF, j < kSetCache
+   double aDef[kSetCache];   // k0 ni (ti - ti0) of the CTA's j-th PSF, j < kSetCache
+   int set[kSetCache];       // its set
    uint32_t tmemSlot;
    int err;
 };
@@ -397,7 +398,11 @@ __global__ void __launch_bounds__(kThreads, 1) CztTf32x3Kernel(TcParams prm)
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
    }
    for (int j = tid; j < nLocal && j < kSetCache; j += kThreads)
-      sh->set[j] = prm.items[psfOf(j)].set;
+   {
+      const PsfItem it = prm.items[psfOf(j)];
+      sh->set[j] = it.set;
+      sh->aDef[j] = prm.sets[it.set].k0 * prm.sets[it.set].ni * it.dtiM;
+   }
    TcFenceBefore();
    __syncthreads();
    TcFenceAfter();
@@ -409,8 +414,7 @@ __global__ void __launch_bounds__(kThreads, 1) CztTf32x3Kernel(TcParams prm)
    {
       // ---------------------------------------------------------------- producers: row-pass B blocks
       // A thread's work per row-pass block: items ptid + r kProducerThreads (pupil column m, pupil rows n .. n + 3).
-      // The table entries of the next block are in flight while a block computes, and the next PSF's item and
-      // defocus factor are fetched half a PSF ahead.
+      // The table entries of the next block are in flight while a block computes.
       const int ptid = 32 * ProducerIndex(warp) + lane;
       auto load = [&](const double2* tab, int kb, double2 (*dst)[4]) {
 #pragma unroll
@@ -423,21 +427,23 @@ __global__ void __launch_bounds__(kThreads, 1) CztTf32x3Kernel(TcParams prm)
                dst[r][c] = in ? tab[static_cast<size_t>(n + c) * M + m] : make_double2(0.0, -1.0);
          }
       };
-      PsfItem itNext = prm.items[psfOf(0)];
-      double k0niNext = prm.sets[itNext.set].k0 * prm.sets[itNext.set].ni;
+      // the defocus factor of PSF j (staged in shared memory for j < kSetCache)
+      auto aDefOf = [&](int j) {
+         if (j < kSetCache)
+            return sh->aDef[j];
+         const PsfItem it = prm.items[psfOf(j)];
+         return prm.sets[it.set].k0 * prm.sets[it.set].ni * it.dtiM;
+      };
       double2 nxt[kItemRounds][4];
-      load(prm.phase + static_cast<size_t>(itNext.set) * M * M, 0, nxt);
+      load(prm.phase + static_cast<size_t>(setOf(0)) * M * M, 0, nxt);
       uint32_t rowCount = 0;
       for (int j = 0; j < nLocal && ok; ++j)
       {
-         const double aDef = k0niNext * itNext.dtiM;
-         const double2* tab = prm.phase + static_cast<size_t>(itNext.set) * M * M;
-         if (j + 1 < nLocal)
-            itNext = prm.items[psfOf(j + 1)];
+         const double aDef = aDefOf(j);
+         const double2* tab = prm.phase + static_cast<size_t>(setOf(j)) * M * M;
+         const double2* tabNext = j + 1 < nLocal ? prm.phase + static_cast<size_t>(setOf(j + 1)) * M * M : tab;
          for (int kb = 0; kb < nKb; ++kb, ++rowCount)
          {
-            if (kb == nKb / 2 && j + 1 < nLocal)   // (the next PSF's item has landed)
-               k0niNext = prm.sets[itNext.set].k0 * prm.sets[itNext.set].ni;
             double2 cur[kItemRounds][4];
 #pragma unroll
             for (int r = 0; r < kItemRounds; ++r)
@@ -447,7 +453,7 @@ __global__ void __launch_bounds__(kThreads, 1) CztTf32x3Kernel(TcParams prm)
             if (kb + 1 < nKb)
                load(tab, kb + 1, nxt);
             else if (j + 1 < nLocal)
-               load(prm.phase + static_cast<size_t>(itNext.set) * M * M, 0, nxt);
+               load(tabNext, 0, nxt);
             const int rs = static_cast<int>(rowCount % kRowStages);
             ok = __all_sync(0xffffffffu, MbarWait(&sh->rowEmpty[rs], ((rowCount / kRowStages) & 1u) ^ 1u, err));
             if (!ok)
