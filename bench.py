@@ -103,7 +103,7 @@ def measured_peaks():
 NCU_TRAFFIC = {
     ("smlm", "GatherTilesKernel"): (139518208, "profiles/GatherTilesKernel_smlm_dstorm.md"),
     ("smlm", "ContribKernel"): (93568768, "profiles/ContribKernel_smlm_dstorm.md"),
-    ("psflib", "CztTf32x3Kernel"): (59642624, "profiles/CztTf32x3Kernel_psf_library.md"),
+    ("psflib", "CztTf32x3Kernel"): (52487168, "profiles/CztTf32x3Kernel_psf_library.md"),
     ("two-colour", "GatherTilesKernel"): (2182043649, "profiles/GatherTilesKernel_two_colour.md"),
 }
 
