@@ -390,6 +390,58 @@ int iscu_render_events_async(iscu_ctx* ctx, int32_t io_slot, int32_t slot, const
                              uint32_t seed, float* photons, uint16_t* adu);
 int iscu_render_events_wait(iscu_ctx* ctx, int32_t io_slot, uint32_t* n_emitters, int64_t* n_clamped);
 
+/* ---------------------------------------------------------------- blink schedules ----------------------------- */
+
+/* The world core's blink kinetics (core/src/dyes.h Kinetics): rates per second, times in seconds. */
+typedef struct iscu_kinetics {
+   double activation_rate_per_sec;
+   double on_sec;
+   double off_sec;
+   double bleach_prob;
+   double photon_cv;
+   double initial_on_sec;       /* dSTORM: ON from t = 0 for Exp(initial_on_sec) before the blinks (0: none) */
+} iscu_kinetics;
+
+/* core LabelMode */
+#define ISCU_LABEL_DSTORM 0
+#define ISCU_LABEL_PALM 1
+#define ISCU_LABEL_DNA_PAINT 2
+#define ISCU_LABEL_WIDEFIELD 3
+typedef struct iscu_label {
+   int32_t mode;                /* ISCU_LABEL_* */
+   int32_t reserved;
+   iscu_kinetics kin;
+} iscu_label;
+
+/* One fluorescent dye: its address in the core's hash scheme (h1: its structure element's H1, e.g. DyeH1 of a
+ * microtubule; k: the site, e.g. the protofilament; n: the index), its id (H2.a), structure and position (um). */
+typedef struct iscu_dye {
+   double x, y, z;
+   uint32_t h1;
+   int32_t k, n;
+   uint32_t id;
+   int32_t structure;
+   int32_t reserved;
+} iscu_dye;
+
+/* The blink rows of isc_events_in_window (insiliscope.h:304-313): x, y, z, tOn, tOff, brightness, id, structure,
+ * state (0: a blink), aux (0). */
+#define ISCU_EVENT_STRIDE 10
+
+/* Each dye's blinks overlapping [t0, t1) (tOn < t1, tOff > t0), as the world core schedules them (dyes.cpp: dSTORM
+ * and PALM LabelSchedule, DNA-PAINT PersistentBlinks, WideField none), bit for bit: the same address-keyed draws and
+ * float64 arithmetic with fdlibm's log / exp / cos. Rows per dye in the order the core appends them, dyes in input
+ * order. History: n_seg = 0 the label's kinetics; n_seg >= 1 segments of constant kinetics starting at
+ * hist_t_start[s] (host arrays, the first 0, increasing, at most 64), as isc_world_set_kinetics_history. dyes_dev,
+ * rows_dev (max_rows x ISCU_EVENT_STRIDE doubles), dye_first_dev (nullable, n_dyes + 1: each dye's first row, then
+ * the total) and *n_rows_dev (the total rows, written even past max_rows; rows at or beyond max_rows are dropped)
+ * are device memory. Bounds on the per-dye work (ISCU_ERR_LIMIT beyond): a finite window of at most 36000 s ending by
+ * 1e6 s, activation rates at most 1e5 per s, ON times at most 1000 s. Asynchronous. */
+int iscu_dye_blinks_dev(iscu_ctx* ctx, const iscu_label* label, const double* hist_t_start,
+                        const iscu_kinetics* hist_kin, uint32_t n_seg, const iscu_dye* dyes_dev, uint32_t n_dyes,
+                        double t0, double t1, double* rows_dev, uint32_t max_rows, uint32_t* dye_first_dev,
+                        uint32_t* n_rows_dev);
+
 /* ---------------------------------------------------------------- per-movie host models ----------------------- */
 
 /* sim::DriftSettings (Drift.h:57-79). */

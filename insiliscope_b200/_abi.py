@@ -99,6 +99,15 @@ class DriftSettings(C.Structure):
                 ("speed_wander_pct", C.c_double), ("wander_time_sec", C.c_double)]
 
 
+class Kinetics(C.Structure):
+    _fields_ = [("activation_rate_per_sec", C.c_double), ("on_sec", C.c_double), ("off_sec", C.c_double),
+                ("bleach_prob", C.c_double), ("photon_cv", C.c_double), ("initial_on_sec", C.c_double)]
+
+
+class Label(C.Structure):
+    _fields_ = [("mode", C.c_int32), ("reserved", C.c_int32), ("kin", Kinetics)]
+
+
 class NllSpec(C.Structure):
     _fields_ = [("wavelength_nm", C.c_double), ("na", C.c_double), ("n_imm", C.c_double), ("pixel_nm", C.c_double),
                 ("roi", C.c_int32), ("os", C.c_int32), ("pupil", C.c_int32), ("n_zern", C.c_int32),
@@ -161,6 +170,8 @@ SIGNATURES = {
     "iscu_buffer_read_low16": (C.c_int, [vp, C.c_size_t, vp]),
     "iscu_dispatch": (C.c_int, [vp, C.c_char_p, vp, C.c_size_t, vp, C.c_size_t, C.c_uint32, C.c_uint32,
                                 C.c_uint32]),
+    "iscu_dye_blinks_dev": (C.c_int, [vp, vp, vp, vp, C.c_uint32, vp, C.c_uint32, C.c_double, C.c_double, vp,
+                                      C.c_uint32, vp, vp]),
     "iscu_drift_trajectory": (C.c_int, [C.c_int64, C.c_int64, C.c_double, C.POINTER(DriftSettings), vp]),
     "iscu_illumination_field": (C.c_int, [C.c_uint32, C.c_uint32, C.c_int32, C.c_double, vp, f64p]),
     "iscu_background_fade_scale": (C.c_double, [C.c_double, C.c_double]),

@@ -34,6 +34,7 @@ UNITS = {
     "psf_plan.cu": [],
     "widefield.cu": ["--fmad=false"],
     "backend.cu": ["--fmad=false"],
+    "schedule.cu": ["--fmad=false"],
     "capi.cpp": [],
     "host_models.cpp": [],
 }

@@ -223,6 +223,7 @@ struct iscu_ctx
    iscu::DevBuf dEmitters, dFrames, dPhotons, dAdu, dExtras, dScratch;
    iscu::DevBuf dCollect;          // device emitter collection: kept emitters per frame
    iscu::DevBuf dLow16;            // the named-kernel backend's narrowed read-back (iscu_buffer_read_low16)
+   iscu::DevBuf dSchedule;         // blink schedules: the history, per-dye counts and first rows
    // the event render's I/O slots (the last one is the blocking call's) and its copy streams (created on first use)
    iscu::EventIo eventIo[ISCU_EVENT_IO_SLOTS + 1];
    cudaStream_t upload = nullptr, download = nullptr;

@@ -25,6 +25,11 @@ GPU_SPLAT_EMITTER_DTYPE = np.dtype([("x0", "<i4"), ("y0", "<i4"), ("bx", "<i4"),
 BLINK_EVENT_DTYPE = np.dtype([("x_um", "<f8"), ("y_um", "<f8"), ("z_nm", "<f8"), ("t_start", "<f8"),
                               ("t_end", "<f8"), ("brightness", "<f8"), ("excite", "<f8"), ("slot", "<i4"),
                               ("reserved", "<i4")])
+DYE_DTYPE = np.dtype([("x", "<f8"), ("y", "<f8"), ("z", "<f8"), ("h1", "<u4"), ("k", "<i4"), ("n", "<i4"),
+                      ("id", "<u4"), ("structure", "<i4"), ("reserved", "<i4")])
+EVENT_STRIDE = 10   # isc_events_in_window's row: x, y, z, tOn, tOff, brightness, id, structure, state, aux
+LABEL_DSTORM, LABEL_PALM, LABEL_DNA_PAINT, LABEL_WIDEFIELD = 0, 1, 2, 3
+assert DYE_DTYPE.itemsize == 48
 assert EMITTER_DTYPE.itemsize == C.sizeof(_abi.Emitter) == 32
 assert FRAME_DTYPE.itemsize == C.sizeof(_abi.Frame) == 24
 assert GPU_SPLAT_EMITTER_DTYPE.itemsize == C.sizeof(_abi.GpuSplatEmitter) == 64
@@ -410,6 +415,49 @@ class Engine:
         batch = self._pending_io.pop(int(io_slot), None)
         ph, adu = (batch[6], batch[7]) if batch is not None else (None, None)
         return ph, adu, n.value
+
+    # -------------------------------------------------------------------------------------------- blink schedules
+    @staticmethod
+    def _kinetics(k) -> _abi.Kinetics:
+        """A Kinetics struct from a dict / sequence (activation rate, on, off, bleach probability, photon CV, initial
+        on)."""
+        names = ("activation_rate_per_sec", "on_sec", "off_sec", "bleach_prob", "photon_cv", "initial_on_sec")
+        vals = [k[n] for n in names] if isinstance(k, dict) else list(k)
+        return _abi.Kinetics(*[float(v) for v in vals])
+
+    def dye_blinks_dev(self, mode, kinetics, dyes_dev, n_dyes, t0, t1, rows_dev, n_rows_dev, history=None,
+                       dye_first_dev=None, sync=True):
+        """iscu_dye_blinks_dev: each dye's blinks overlapping [t0, t1) as the world core schedules them. dyes_dev: a
+        uint8 CUDA view of DYE_DTYPE records; rows_dev: float64 CUDA (max rows, EVENT_STRIDE); n_rows_dev: 1 int32;
+        history: (t_start sequence, kinetics sequence) or None."""
+        label = _abi.Label(int(mode), 0, self._kinetics(kinetics))
+        starts = kin = None
+        n_seg = 0
+        if history is not None:
+            st, ks = history
+            n_seg = len(st)
+            starts = np.ascontiguousarray(st, np.float64)
+            kin = (_abi.Kinetics * n_seg)(*[self._kinetics(k) for k in ks])
+        max_rows = 0 if rows_dev is None else rows_dev.numel() // EVENT_STRIDE
+        self._before(sync)
+        check(self.lib.iscu_dye_blinks_dev(self.h, C.byref(label), _ptr(starts), kin, n_seg, _ptr(dyes_dev),
+                                           int(n_dyes), float(t0), float(t1), _ptr(rows_dev), max_rows,
+                                           _ptr(dye_first_dev), _ptr(n_rows_dev)))
+        self._after(sync)
+
+    def dye_blinks(self, mode, kinetics, dyes, t0, t1, history=None):
+        """Host form: dyes (DYE_DTYPE) -> (rows (m, EVENT_STRIDE) float64, first (n + 1,) per dye's first row)."""
+        import torch
+        dyes = np.ascontiguousarray(dyes, dtype=DYE_DTYPE)
+        dev = f"cuda:{self.device}"
+        d_dyes = torch.from_numpy(dyes.view(np.uint8)).to(dev)
+        d_n = torch.zeros(1, dtype=torch.int32, device=dev)
+        d_first = torch.zeros(len(dyes) + 1, dtype=torch.int32, device=dev)
+        self.dye_blinks_dev(mode, kinetics, d_dyes, len(dyes), t0, t1, None, d_n, history, d_first)
+        total = int(d_n.item())
+        rows = torch.empty((max(total, 1), EVENT_STRIDE), dtype=torch.float64, device=dev)
+        self.dye_blinks_dev(mode, kinetics, d_dyes, len(dyes), t0, t1, rows, d_n, history, d_first)
+        return rows[:total].cpu().numpy(), d_first.cpu().numpy().astype(np.int64)
 
     RENDER_CONFIGS = 18
 

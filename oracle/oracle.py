@@ -175,6 +175,10 @@ class Reference:
         L.ref_camera_maps.argtypes = [u32, u32, C.c_uint64, f64, f64, f64, f64, f64, f64, u32, u32, vp, vp, vp]
         L.ref_noise_chain.argtypes = [vp, u32, u32, vp, vp, vp, vp, u32, u32, u32, C.c_int, vp]
         L.ref_psf_geometry.argtypes = [vp, vp]
+        L.ref_dye_blinks.argtypes = [C.c_int, vp, vp, vp, C.c_int, u32, i32, i32, f64, f64, vp, C.c_int]
+        L.ref_dye_blinks.restype = C.c_int
+        L.ref_dye_h1.argtypes = [u32, i32, i32, C.c_int]
+        L.ref_dye_h1.restype = u32
         L.ref_zernike_planes.argtypes = [vp, vp]
         L.ref_kernel_build.argtypes = [vp]
         L.ref_kernel_build.restype = vp
@@ -291,6 +295,28 @@ class Reference:
 
     def kernel(self, req=None, planes=None, os_=4, z_step_nm=25.0, interp=2):
         return RefKernel(self, req, planes, os_, z_step_nm, interp)
+
+    def dye_blinks(self, mode, kin, h1, k, n, t0, t1, history=None):
+        """One dye's blinks overlapping [t0, t1) from the world core's own schedules: (m, 3) float64 rows of
+        (tOn, tOff, brightness)."""
+        kin = np.ascontiguousarray(kin, np.float64)
+        st = hk = None
+        n_seg = 0
+        if history is not None:
+            st = np.ascontiguousarray(history[0], np.float64)
+            hk = np.ascontiguousarray(history[1], np.float64).reshape(-1, 6)
+            n_seg = len(st)
+        cap = 64
+        while True:
+            out = np.zeros((cap, 3), np.float64)
+            m = self.L.ref_dye_blinks(int(mode), _p(kin), _p(st), _p(hk), n_seg, int(h1) & 0xFFFFFFFF, int(k),
+                                      int(n), float(t0), float(t1), _p(out), cap)
+            if m <= cap:
+                return out[:m]
+            cap = m
+
+    def dye_h1(self, seed, cx, cy, mt_index):
+        return int(self.L.ref_dye_h1(int(seed) & 0xFFFFFFFF, int(cx), int(cy), int(mt_index)))
 
 
 def _geometry(req):

@@ -17,6 +17,7 @@
 #include "SMLMSimulation.h"
 #include "SMLMZernike.h"
 #include "ZernikePsf.h"
+#include "dyes.h"
 #include "rng.h"
 
 #include "../include/iscu.h"
@@ -505,5 +506,56 @@ size_t ref_illumination_field(unsigned w, unsigned h, int profile, double fwhmPc
 }
 
 double ref_background_fade_scale(double t, double decay) { return sim::BackgroundFadeScale(t, decay); }
+
+// One dye's blinks overlapping [t0, t1) as the world core schedules them (core/src/dyes.cpp): dSTORM / PALM through
+// LabelSchedule run without a horizon (then filtered), DNA-PAINT through PersistentBlinks. kin: 6 doubles
+// (activation rate, on, off, bleach probability, photon CV, initial on); hist: nSeg start times and 6 nSeg kinetics
+// (0 segments: none). out: (tOn, tOff, brightness) rows, at most cap; returns the number of rows.
+int ref_dye_blinks(int mode, const double* kin, const double* histStart, const double* histKin, int nSeg, uint32_t h1,
+                   int32_t k, int32_t n, double t0, double t1, double* out, int cap)
+{
+   auto kinOf = [](const double* v) {
+      isc::Kinetics q;
+      q.activationRatePerSec = v[0];
+      q.onSec = v[1];
+      q.offSec = v[2];
+      q.bleachProb = v[3];
+      q.photonCV = v[4];
+      q.initialOnSec = v[5];
+      return q;
+   };
+   isc::Label label;
+   label.mode = static_cast<isc::LabelMode>(mode);
+   label.kin = kinOf(kin);
+   isc::KineticsHistory hist;
+   for (int s = 0; s < nSeg; ++s)
+   {
+      hist.tStart.push_back(histStart[s]);
+      hist.kin.push_back(kinOf(histKin + 6 * s));
+   }
+   const isc::KineticsHistory* h = nSeg > 0 ? &hist : nullptr;
+   std::vector<isc::Blink> blinks;
+   if (label.mode == isc::LabelMode::DnaPaint)
+      isc::PersistentBlinks(h1, k, n, label.kin, t0, t1, blinks, h);
+   else
+      isc::LabelSchedule(h1, k, n, label, &blinks, nullptr, INFINITY, h);
+   int m = 0;
+   for (const isc::Blink& b : blinks)
+   {
+      if (!(b.tOn < t1) || !(b.tOff > t0))
+         continue;
+      if (m < cap)
+      {
+         out[3 * m] = b.tOn;
+         out[3 * m + 1] = b.tOff;
+         out[3 * m + 2] = b.brightness;
+      }
+      ++m;
+   }
+   return m;
+}
+
+// The core's DyeH1 (dyes.cpp:175-178): H1 of microtubule mtIndex of cell (cx, cy).
+uint32_t ref_dye_h1(uint32_t seed, int32_t cx, int32_t cy, int mtIndex) { return isc::DyeH1(seed, cx, cy, mtIndex); }
 
 } // extern "C"
