@@ -703,8 +703,101 @@ class NllGradWorkload:
         return time.perf_counter() - t0
 
 
+class ScheduleWorkload:
+    """The step before the render: the blinks of 1,048,576 dSTORM dyes (the world core's schedules: first
+    activation, ON / dark cycles with log-normal brightness, bleaching) overlapping one 1 s window late in a movie,
+    [100, 101) s, so each dye's schedule is walked from its activation. The dyes stay resident; one step = the count,
+    scan and row passes of iscu_dye_blinks_dev. e2e: page-locked dyes in, the window's event rows out."""
+    name = ("blink schedules: 1,048,576 dSTORM dyes (activation 0.05/s, ON 40 ms, dark 2 s, bleach 0.3, photon CV "
+            "0.5, initial ON 0.2 s), events of the window [100, 101) s")
+    metric = "dyes/s"
+    dtype = "f64"
+    cpu_kind = "reference"
+    KIN = [0.05, 0.04, 2.0, 0.3, 0.5, 0.2]
+    T0, T1 = 100.0, 101.0
+
+    def __init__(self, rank: int):
+        from insiliscope_b200 import DYE_DTYPE
+        rng = np.random.default_rng(42 + rank)
+        n = 1 << 20
+        d = np.zeros(n, DYE_DTYPE)
+        d["h1"] = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+        d["k"] = rng.integers(0, 13, n)
+        d["n"] = rng.integers(0, 5000, n)
+        d["id"] = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+        d["x"], d["y"], d["z"] = rng.uniform(-50, 50, (3, n))
+        self.dyes = d
+        self.frames_per_step_cpu = 1 << 17
+        self.cpu_sample = (f"{self.frames_per_step_cpu} of the 1,048,576 dyes per step: the core's LabelSchedule per "
+                           "dye (dyes.cpp, compiled from its sources) on the reference's thread pool (ParallelFor)")
+
+    def setup(self, device: int):
+        import torch
+        from insiliscope_b200 import EVENT_STRIDE, LABEL_DSTORM, Engine
+        self.eng = eng = Engine(device)
+        self.mode = LABEL_DSTORM
+        dev = f"cuda:{device}"
+        n = len(self.dyes)
+        self.d_dyes = torch.from_numpy(self.dyes.view(np.uint8)).to(dev)
+        self.d_n = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.d_first = torch.zeros(n + 1, dtype=torch.int32, device=dev)
+        eng.dye_blinks_dev(self.mode, self.KIN, self.d_dyes, n, self.T0, self.T1, None, self.d_n,
+                           dye_first_dev=self.d_first)
+        self.n_rows = int(self.d_n.item())
+        self.d_rows = torch.empty((max(1, self.n_rows), EVENT_STRIDE), dtype=torch.float64, device=dev)
+        self.h_dyes = torch.from_numpy(self.dyes.view(np.uint8)).pin_memory()
+        self.h_rows = torch.empty((max(1, self.n_rows), EVENT_STRIDE), dtype=torch.float64).pin_memory()
+        self.stream = eng.torch_stream()
+        self.frames_per_step = n
+        self.n_emitters = self.n_rows
+        self.psf_build_ms = 0.0
+
+    def device_step(self):
+        self.eng.dye_blinks_dev(self.mode, self.KIN, self.d_dyes, len(self.dyes), self.T0, self.T1, self.d_rows,
+                                self.d_n, dye_first_dev=self.d_first, sync=False)
+
+    def e2e_step(self):
+        """Page-locked dyes in, the window's rows out; the copies on torch's own stream, ordered with the library's by
+        the synchronizing call (a pinned block used on the library's stream would outlive that stream)."""
+        import torch
+        self.d_dyes.copy_(self.h_dyes, non_blocking=True)
+        self.eng.dye_blinks_dev(self.mode, self.KIN, self.d_dyes, len(self.dyes), self.T0, self.T1, self.d_rows,
+                                self.d_n, dye_first_dev=self.d_first, sync=True)
+        self.h_rows.copy_(self.d_rows, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return self.h_rows
+
+    def e2e_bytes(self):
+        return self.h_dyes.numel(), self.h_rows.numel() * 8
+
+    def kernel_name(self):
+        return "CountKernel+ScanKernel+RowsKernel"
+
+    def alg_bytes_per_launch(self):
+        # the dyes read by the count and the row pass (48 B each), per-dye counts and first rows (8 B), the rows (80 B)
+        return len(self.dyes) * (2 * 48 + 8) + self.n_rows * 80
+
+    def config_extra(self):
+        return {"rows_per_step": self.n_rows}
+
+    def cpu_cores(self):
+        return self.ref.threads()
+
+    def reference_setup(self, threads=0):
+        from oracle.oracle import Reference
+        if not Reference.available():
+            raise RuntimeError("the reference harness oracle/_ref/libiscref.so is not built (it needs the reference "
+                               "tree at build time)")
+        self.ref = Reference()
+        self.ref.set_threads(threads)
+
+    def reference_step(self):
+        _, sec = self.ref.dye_blinks_batch(0, self.KIN, self.dyes[:self.frames_per_step_cpu], self.T0, self.T1)
+        return sec
+
+
 WORKLOADS = {"smlm": SmlmWorkload, "widefield": WidefieldWorkload, "psflib": PsfLibraryWorkload,
-             "two-colour": TwoColourWorkload, "nll-grad": NllGradWorkload}
+             "two-colour": TwoColourWorkload, "nll-grad": NllGradWorkload, "schedules": ScheduleWorkload}
 
 
 # ----------------------------------------------------------------------------------------------------- arms

@@ -177,6 +177,8 @@ class Reference:
         L.ref_psf_geometry.argtypes = [vp, vp]
         L.ref_dye_blinks.argtypes = [C.c_int, vp, vp, vp, C.c_int, u32, i32, i32, f64, f64, vp, C.c_int]
         L.ref_dye_blinks.restype = C.c_int
+        L.ref_dye_blinks_batch.argtypes = [C.c_int, vp, vp, vp, C.c_int, vp, u32, f64, f64, vp]
+        L.ref_dye_blinks_batch.restype = f64
         L.ref_dye_h1.argtypes = [u32, i32, i32, C.c_int]
         L.ref_dye_h1.restype = u32
         L.ref_zernike_planes.argtypes = [vp, vp]
@@ -314,6 +316,21 @@ class Reference:
             if m <= cap:
                 return out[:m]
             cap = m
+
+    def dye_blinks_batch(self, mode, kin, dyes, t0, t1, history=None):
+        """The core's schedules over a DYE_DTYPE array on the reference's thread pool: (per-dye row counts, seconds)."""
+        kin = np.ascontiguousarray(kin, np.float64)
+        st = hk = None
+        n_seg = 0
+        if history is not None:
+            st = np.ascontiguousarray(history[0], np.float64)
+            hk = np.ascontiguousarray(history[1], np.float64).reshape(-1, 6)
+            n_seg = len(st)
+        dyes = np.ascontiguousarray(dyes)
+        counts = np.zeros(len(dyes), np.uint32)
+        sec = self.L.ref_dye_blinks_batch(int(mode), _p(kin), _p(st), _p(hk), n_seg, _p(dyes), len(dyes), float(t0),
+                                          float(t1), _p(counts))
+        return counts, sec
 
     def dye_h1(self, seed, cx, cy, mt_index):
         return int(self.L.ref_dye_h1(int(seed) & 0xFFFFFFFF, int(cx), int(cy), int(mt_index)))

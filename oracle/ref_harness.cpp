@@ -22,6 +22,7 @@
 
 #include "../include/iscu.h"
 
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -544,7 +545,7 @@ int ref_dye_blinks(int mode, const double* kin, const double* histStart, const d
    {
       if (!(b.tOn < t1) || !(b.tOff > t0))
          continue;
-      if (m < cap)
+      if (m < cap && out)
       {
          out[3 * m] = b.tOn;
          out[3 * m + 1] = b.tOff;
@@ -553,6 +554,23 @@ int ref_dye_blinks(int mode, const double* kin, const double* histStart, const d
       ++m;
    }
    return m;
+}
+
+// The same over n dyes (iscu_dye records), in parallel on the reference's thread pool (sim::ParallelFor, as the
+// world schedules its dye blocks on its pool): counts[i] = dye i's rows; returns the wall seconds of the work.
+double ref_dye_blinks_batch(int mode, const double* kin, const double* histStart, const double* histKin, int nSeg,
+                            const iscu_dye* dyes, uint32_t n, double t0, double t1, uint32_t* counts)
+{
+   const auto start = std::chrono::steady_clock::now();
+   const unsigned chunks = std::max(1u, std::min(n, 4096u));
+   sim::ParallelFor(chunks, [&](unsigned c) {
+      const uint32_t lo = static_cast<uint32_t>(static_cast<uint64_t>(n) * c / chunks);
+      const uint32_t hi = static_cast<uint32_t>(static_cast<uint64_t>(n) * (c + 1) / chunks);
+      for (uint32_t i = lo; i < hi; ++i)
+         counts[i] = static_cast<uint32_t>(ref_dye_blinks(mode, kin, histStart, histKin, nSeg, dyes[i].h1, dyes[i].k,
+                                                          dyes[i].n, t0, t1, nullptr, 0));
+   });
+   return std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
 }
 
 // The core's DyeH1 (dyes.cpp:175-178): H1 of microtubule mtIndex of cell (cx, cy).
