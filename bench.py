@@ -657,6 +657,7 @@ class NllGradWorkload:
     def e2e_step(self):
         """Page-locked parameters in, the NLL and every gradient out, through the library's model."""
         import torch
+        from insiliscope_b200.nll import reduce_shared
         # the copies on torch's own stream (ordered with the library's by the synchronizing calls)
         self.d_params.copy_(self.h_params, non_blocking=True)
         self.d_bg.copy_(self.h_bg, non_blocking=True)
