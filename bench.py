@@ -383,7 +383,8 @@ class WidefieldWorkload:
     metric = "frames/s"
 
     # pass names and their algorithmic bytes (computed in setup)
-    PASSES = ("XForwardKernel", "YForwardKernel", "ZKernel<convolve>", "YInverseKernel", "XInverseKernel")
+    PASSES = ("XForwardKernel", "YForwardKernel", "ZKernel<convolve>", "YInverseKernel", "XInverseKernel",
+              "WfNoiseKernel")
 
     def __init__(self, rank: int):
         from insiliscope_b200.workloads import widefield_cells
@@ -422,7 +423,8 @@ class WidefieldWorkload:
                            NK * ny * nz * 8 + NK * G[1] * nz * 8,          # y forward
                            2 * NK * G[1] * nz * 8 + NK * G[1] * G[2] * 8,  # z: spectra in/out + the PSF spectrum
                            NK * G[1] * nz * 8 + NK * ny * nz * 8,          # y inverse
-                           NK * ny * nz * 8 + vox * 2 + nx * ny * 4]       # x inverse: ADU out + offset map
+                           NK * ny * nz * 8 + vox * 4,                     # x inverse: photon frames out
+                           vox * 4 + vox * 2 + nx * ny * 4]                # noise: photons in, ADU out + offset map
 
     def device_step(self):
         wv = self.wv
@@ -445,7 +447,7 @@ class WidefieldWorkload:
             self.device_step()
             times.append(self.plan.pass_times())
         self.plan.set_timing(False)
-        mean = [statistics.mean(t[i] for t in times) for i in range(5)]
+        mean = [statistics.mean(t[i] for t in times) for i in range(len(self.PASSES))]
         i = int(np.argmax(mean))
         return self.PASSES[i], self.pass_bytes[i], mean[i], dict(zip(self.PASSES, [round(m, 4) for m in mean]))
 
@@ -453,7 +455,7 @@ class WidefieldWorkload:
         return sum(self.pass_bytes)
 
     def kernel_name(self):
-        return "widefield step (5 passes)"
+        return "widefield step (6 passes)"
 
     # -------------------------------------------------- CPU: the float64 FFT convolution port (scipy, all cores)
     dtype = "f32"

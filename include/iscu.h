@@ -530,10 +530,12 @@ int iscu_wf_convolve_dev(iscu_wf_plan* plan, const float* density_dev, float* im
 int iscu_wf_render(iscu_wf_plan* plan, const float* density, double background, const iscu_camera* cam,
                    uint32_t seed, uint32_t frame0, float* image, uint16_t* adu);
 /* Phase timing of a plan's renders (the reference's ISC_TIMING phases, Timing.h:123): with it on, every render
- * records CUDA events around its five passes; iscu_wf_pass_times gives the last render's pass durations in ms
- * (x forward, y forward, z convolve, y inverse, x inverse + noise), waiting for it. */
+ * records CUDA events around its ISCU_WF_PASSES passes; iscu_wf_pass_times gives the last render's pass durations
+ * in ms (x forward, y forward, z convolve, y inverse, x inverse, camera noise -- 0 without a camera), waiting for
+ * it. */
+#define ISCU_WF_PASSES 6
 int iscu_wf_set_timing(iscu_wf_plan* plan, int32_t on);
-int iscu_wf_pass_times(iscu_wf_plan* plan, float* ms5);
+int iscu_wf_pass_times(iscu_wf_plan* plan, float* ms);
 /* The same on device buffers (the camera maps of iscu_set_static apply when their size is nx x ny). */
 int iscu_wf_render_dev(iscu_wf_plan* plan, const float* density_dev, double background, const iscu_camera* cam,
                        uint32_t seed, uint32_t frame0, float* image_dev, uint16_t* adu_dev);

@@ -9,8 +9,8 @@
 // sum_k dye plane k (x) PSF plane f - k + kz/2. Then max(0, .) + background per pixel (WidefieldImages::Render,
 // WidefieldRender.cpp:547) and ApplyNoiseChain per plane (SMLMNoise.cpp:142-216) in the same kernel.
 //
-// Passes (each a batch of 1D transforms in shared memory; the padded halves are never loaded, stored or
-// transformed beyond the first butterfly stage that reads their zeros):
+// Passes (each a batch of 1D transforms; the padded halves are never loaded, stored or transformed beyond the first
+// butterfly stage that reads their zeros):
 //   XForward   rows of nx reals -> GX-point real FFT through a GX/2-point complex FFT of packed pairs -> GX/2+1 bins,
 //              stored k-major, y contiguous: A[z][k][y]
 //   YForward   A rows (ny values, zero-padded to GY) -> GY-point FFT -> B[z][k][ky]
@@ -21,7 +21,18 @@
 //              columns, scale 1/(GX GY GZ), max(0, .) + background, noise chain -> uint16 frames (and the image)
 // Forward transforms are decimation in frequency (natural order in, bit-reversed out) and inverse transforms
 // decimation in time (bit-reversed in, natural out), so no pass ever permutes: the spectra B and the PSF spectrum
-// are stored with ky and kz in bit-reversed order. Butterflies are fused in pairs (radix 4 per thread).
+// are stored with ky and kz in bit-reversed order.
+//
+// Each N-point transform is split into groups of up to five radix-2 stages (N = R_0 R_1 ... , R_g <= 32). A thread
+// holds the R_g points of one group in registers -- points j + q m, m < R_g, q the group's smallest span -- does
+// the R_g-point DFT there (constant roots of unity only) and then one table twiddle per point: DIF group g of
+// block size M = q R_g is, per j < q, an R_g-point DFT of the stride-q points followed by W_M^(j rev(m)) on output
+// slot m. The inverse groups are the conjugate transposes (conjugate twiddle first, then the R_g-point inverse DFT
+// with bit-reversed input), run in reverse group order. The first group loads straight from global memory and the
+// last one of an inverse stores straight back, so a 1024-point transform is one shared-memory exchange. Layouts:
+// rows (Y) pad one point per R_last points, so both the stride-q reads of the first group and the contiguous reads
+// of the last one hit 16 distinct 8-byte bank pairs per half warp; columns (Z, X: lines fastest) pad X's line
+// stride to an odd count for the passes that walk along a line.
 //
 // Compiled with --fmad=false for the noise chain's exactness; the FFT arithmetic uses explicit __fmaf_rn.
 
@@ -32,16 +43,38 @@
 #include <cmath>
 #include <vector>
 
+namespace iscu {
+
+// One transform length's group plan: groups of r[g] radix-2 stages from the largest span down; tw[g] is the offset of
+// group g's twiddle table (q R entries, slot-major) in the plan's table buffer, -1 where q = 1.
+struct LinePlan
+{
+   int logN = 0, groups = 0;
+   int r[3] = {0, 0, 0};
+   int tw[3] = {-1, -1, -1};
+};
+
+__host__ __device__ inline int LogQ(const LinePlan& P, int g)
+{
+   int s = 0;
+   for (int i = 0; i <= g; ++i)
+      s += P.r[i];
+   return P.logN - s;
+}
+
+} // namespace iscu
+
 struct iscu_wf_plan
 {
    iscu_ctx* ctx = nullptr;
    uint32_t nx = 0, ny = 0, nz = 0, kx = 0, ky = 0, kz = 0;
    uint32_t GX = 0, GY = 0, GZ = 0, H = 0, NK = 0, G = 0;
    int logH = 0, logGY = 0, logGZ = 0;
-   iscu::DevBuf A, B, Kh, tw, image, adu;
-   // Pass timing (iscu_wf_set_timing): events before XForward and after each of the five passes.
+   iscu::LinePlan px, py, pz;
+   iscu::DevBuf A, B, Kh, tw, twg, image, adu;
+   // Pass timing (iscu_wf_set_timing): events before XForward and after each of the ISCU_WF_PASSES passes.
    bool timing = false;
-   cudaEvent_t ev[6] = {};
+   cudaEvent_t ev[ISCU_WF_PASSES + 1] = {};
    void Mark(int i) const
    {
       if (timing)
@@ -53,8 +86,14 @@ namespace iscu {
 
 namespace {
 
+// Resident CTAs per SM the FFT passes are compiled for (registers per thread <= 64K / (256 x this)).
+#ifndef ISCU_WF_MIN_CTAS
+#define ISCU_WF_MIN_CTAS 2
+#endif
 constexpr int kThreads = 256;
-constexpr size_t kSmemLimit = 64 * 1024;
+constexpr int kMinCtas = ISCU_WF_MIN_CTAS;
+constexpr size_t kSmemBudget = 100 * 1024;   // lines per CTA are sized to this
+constexpr size_t kSmemMax = 227 * 1024;
 
 __device__ __forceinline__ float2 Cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 Csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
@@ -64,116 +103,224 @@ __device__ __forceinline__ float2 Cmul(float2 a, float2 b)
 }
 __device__ __forceinline__ float2 Conj(float2 a) { return make_float2(a.x, -a.y); }
 
-// W_M^j = exp(-2 pi i j / M) from the G-point table, M = 2^logM dividing G = 2^logG; conjugated for inverse
-// transforms. Every size here is a power of two, so index arithmetic is shifts and masks.
-__device__ __forceinline__ float2 Tw(const float2* __restrict__ tw, int logG, int logM, int j, bool inv)
+// 8-byte asynchronous global -> shared copies (no registers held while in flight); a thread waits for its own.
+__device__ __forceinline__ void CopyAsync8(float2* dst, const float2* src)
 {
-   const float2 w = __ldg(tw + (j << (logG - logM)));
-   return inv ? Conj(w) : w;
+   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(dst))),
+                "l"(src)
+                : "memory");
 }
+__device__ __forceinline__ void CopyAsyncWait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 __device__ __forceinline__ int Rev(int n, int logN) { return static_cast<int>(__brev(static_cast<unsigned>(n)) >> (32 - logN)); }
 
-// Lines in shared memory: element n of line b at s[b * ls + n * es]. kColumns: es > 1, ls = 1 (threads walk the
-// lines fastest); else rows (es = 1, threads walk the elements fastest).
-template <bool kColumns>
-__device__ __forceinline__ void TupleOf(int t, int logTuples, int logNl, int& b, int& u)
+__host__ __device__ constexpr int Log2i(int v) { return v <= 1 ? 0 : 1 + Log2i(v >> 1); }
+
+// cos(2 pi e / 32) for e = 0..8 (the first octant of the 32nd roots of unity).
+__device__ __forceinline__ float Cos32Octant(int e)
 {
-   if (kColumns)
+   switch (e)
    {
-      b = t & ((1 << logNl) - 1);
-      u = t >> logNl;
-   }
-   else
-   {
-      b = t >> logTuples;
-      u = t & ((1 << logTuples) - 1);
+   case 0: return 1.0f;
+   case 1: return 0.98078528040323044913f;
+   case 2: return 0.92387953251128675613f;
+   case 3: return 0.83146961230254523708f;
+   case 4: return 0.70710678118654752440f;
+   case 5: return 0.55557023301960222474f;
+   case 6: return 0.38268343236508977173f;
+   case 7: return 0.19509032201612826785f;
+   default: return 0.0f;
    }
 }
 
-// Decimation-in-frequency FFT of nl = 2^logNl lines of N = 2^logN points: natural order in, bit-reversed order out.
-template <bool kColumns>
-__device__ void DifLines(float2* s, int logN, int logNl, int ls, int es, const float2* __restrict__ tw, int logG,
-                         bool inv)
+__device__ __forceinline__ float Cos32(int e)
 {
-   const int N = 1 << logN, total4 = (N >> 2) << logNl, total2 = (N >> 1) << logNl;
-   int logQ = logN - 2;
-   for (; logQ >= 0; logQ -= 2)
+   e &= 31;
+   if (e <= 8)
+      return Cos32Octant(e);
+   if (e <= 16)
+      return -Cos32Octant(16 - e);
+   if (e <= 24)
+      return -Cos32Octant(e - 16);
+   return Cos32Octant(32 - e);
+}
+
+// x W_32^e, W_32 = exp(-2 pi i / 32), conjugated for inverse transforms. Every call site has e fixed once its loops
+// are unrolled, so the branches fold away.
+template <bool kInv>
+__device__ __forceinline__ float2 RootMul(float2 x, int e)
+{
+   e &= 31;
+   if (e == 0)
+      return x;
+   if (e == 16)
+      return make_float2(-x.x, -x.y);
+   if (e == 8 || e == 24)
+      return ((e == 8) != kInv) ? make_float2(x.y, -x.x) : make_float2(-x.y, x.x);   // times -i : times +i
+   const float c = Cos32(e), s = Cos32(e - 8);                                       // sin(2 pi e / 32)
+   return Cmul(x, make_float2(c, kInv ? s : -s));
+}
+
+// R-point DFT in registers, decimation in frequency: natural order in, bit-reversed order out. kHalf: the upper
+// half of the input is zero (and not read).
+template <int R, bool kInv, bool kHalf>
+__device__ __forceinline__ void DifReg(float2 (&v)[R])
+{
+#pragma unroll
+   for (int s = R / 2; s >= 1; s >>= 1)
    {
-      const int q = 1 << logQ;
-      for (int t = threadIdx.x; t < total4; t += blockDim.x)
+#pragma unroll
+      for (int i = 0; i < R / 2; ++i)
       {
-         int b, u;
-         TupleOf<kColumns>(t, logN - 2, logNl, b, u);
-         const int j = u & (q - 1), i = ((u >> logQ) << (logQ + 2)) | j;
-         float2* L = s + b * ls;
-         const float2 e0 = L[i * es], e1 = L[(i + q) * es], e2 = L[(i + 2 * q) * es], e3 = L[(i + 3 * q) * es];
-         const float2 a0 = Cadd(e0, e2), a1 = Cadd(e1, e3);
-         const float2 a2 = Cmul(Csub(e0, e2), Tw(tw, logG, logQ + 2, j, inv));
-         const float2 a3 = Cmul(Csub(e1, e3), Tw(tw, logG, logQ + 2, j + q, inv));
-         const float2 w = Tw(tw, logG, logQ + 1, j, inv);
-         L[i * es] = Cadd(a0, a1);
-         L[(i + q) * es] = Cmul(Csub(a0, a1), w);
-         L[(i + 2 * q) * es] = Cadd(a2, a3);
-         L[(i + 3 * q) * es] = Cmul(Csub(a2, a3), w);
+         const int lo = (i / s) * 2 * s + i % s, hi = lo + s, e = (i % s) * (32 / (2 * s));
+         if (kHalf && s == R / 2)
+         {
+            v[hi] = RootMul<kInv>(v[lo], e);
+         }
+         else
+         {
+            const float2 a = v[lo], b = v[hi];
+            v[lo] = Cadd(a, b);
+            v[hi] = RootMul<kInv>(Csub(a, b), e);
+         }
       }
-      __syncthreads();
    }
-   if (logQ == -1)   // logN odd: the last stage, span 1
+}
+
+// R-point DFT in registers, decimation in time: bit-reversed order in, natural order out.
+template <int R, bool kInv>
+__device__ __forceinline__ void DitReg(float2 (&v)[R])
+{
+#pragma unroll
+   for (int s = 1; s < R; s <<= 1)
    {
-      for (int t = threadIdx.x; t < total2; t += blockDim.x)
+#pragma unroll
+      for (int i = 0; i < R / 2; ++i)
       {
-         int b, u;
-         TupleOf<kColumns>(t, logN - 1, logNl, b, u);
-         float2* L = s + b * ls;
-         const float2 a = L[2 * u * es], c = L[(2 * u + 1) * es];
-         L[2 * u * es] = Cadd(a, c);
-         L[(2 * u + 1) * es] = Csub(a, c);
+         const int lo = (i / s) * 2 * s + i % s, hi = lo + s;
+         const float2 a = v[lo], b = RootMul<kInv>(v[hi], (i % s) * (32 / (2 * s)));
+         v[lo] = Cadd(a, b);
+         v[hi] = Csub(a, b);
       }
+   }
+}
+
+// Output slot m (m >= 1) of a group times its table twiddle W_M^(j rev(m)) (conjugated for inverse transforms);
+// table entry m q + j, so the lanes of a warp walking j read consecutive entries.
+template <int R, bool kInv>
+__device__ __forceinline__ void Twiddle(float2 (&v)[R], const float2* __restrict__ tw, int q, int j)
+{
+#pragma unroll
+   for (int m = 1; m < R; ++m)
+   {
+      float2 w = __ldg(tw + m * q + j);
+      if (kInv)
+         w.y = -w.y;
+      v[m] = Cmul(v[m], w);
+   }
+}
+
+// Shared-memory layouts. Rows: point i of line b at b * np + i + (i >> rl), np = N + N / 2^rl. Columns: point i of
+// line b at i * ls + b.
+struct RowAddr
+{
+   float2* s;
+   int np, rl;
+   __device__ __forceinline__ float2& operator()(int b, int i) const { return s[b * np + i + (i >> rl)]; }
+};
+
+struct ColAddr
+{
+   float2* s;
+   int ls;
+   __device__ __forceinline__ float2& operator()(int b, int i) const { return s[i * ls + b]; }
+};
+
+// One group on lines held in shared memory, in place: the DIF group (then its twiddles) or, for kInv, the inverse
+// group (conjugate twiddles, then the DIT DFT). Rows: lanes walk the tasks of a line; columns: lanes walk the lines
+// (BL of them, a power of two; lines >= nb are skipped).
+template <int R, bool kInv, bool kCols, class Addr>
+__device__ void SmemGroup(const Addr& S, int nb, int BL, int logBL, int logN, int logQ, const float2* __restrict__ tw)
+{
+   constexpr int r = Log2i(R);
+   const int logT = logN - r, q = 1 << logQ;
+   const int total = kCols ? (BL << logT) : (nb << logT);
+   for (int t = threadIdx.x; t < total; t += blockDim.x)
+   {
+      int b, u;
+      if (kCols)
+      {
+         b = t & (BL - 1);
+         u = t >> logBL;
+         if (b >= nb)
+            continue;
+      }
+      else
+      {
+         b = t >> logT;
+         u = t & ((1 << logT) - 1);
+      }
+      const int j = u & (q - 1), base = ((u >> logQ) << (logQ + r)) | j;
+      float2 v[R];
+#pragma unroll
+      for (int m = 0; m < R; ++m)
+         v[m] = S(b, base + m * q);
+      if (!kInv)
+      {
+         DifReg<R, false, false>(v);
+         if (tw)
+            Twiddle<R, false>(v, tw, q, j);
+      }
+      else
+      {
+         if (tw)
+            Twiddle<R, true>(v, tw, q, j);
+         DitReg<R, true>(v);
+      }
+#pragma unroll
+      for (int m = 0; m < R; ++m)
+         S(b, base + m * q) = v[m];
+   }
+}
+
+#define ISCU_RADIX_SWITCH(r, ...)                                                                                       \
+   switch (r)                                                                                                          \
+   {                                                                                                                   \
+   case 1: { constexpr int R = 2; __VA_ARGS__; } break;                                                                \
+   case 2: { constexpr int R = 4; __VA_ARGS__; } break;                                                                \
+   case 3: { constexpr int R = 8; __VA_ARGS__; } break;                                                                \
+   case 4: { constexpr int R = 16; __VA_ARGS__; } break;                                                               \
+   default: { constexpr int R = 32; __VA_ARGS__; } break;                                                              \
+   }
+
+__device__ __forceinline__ const float2* GroupTw(const LinePlan& P, const float2* twg, int g)
+{
+   return P.tw[g] >= 0 ? twg + P.tw[g] : nullptr;
+}
+
+// Forward groups 1 .. groups-1 of lines already in shared memory (group 0 done by the pass's loader).
+template <bool kCols, class Addr>
+__device__ void ForwardRest(const LinePlan& P, const float2* twg, const Addr& S, int nb, int BL, int logBL)
+{
+   for (int g = 1; g < P.groups; ++g)
+   {
+      const int logQ = LogQ(P, g);
+      const float2* tw = GroupTw(P, twg, g);
+      ISCU_RADIX_SWITCH(P.r[g], (SmemGroup<R, false, kCols>(S, nb, BL, logBL, P.logN, logQ, tw)));
       __syncthreads();
    }
 }
 
-// Decimation-in-time FFT: bit-reversed order in, natural order out.
-template <bool kColumns>
-__device__ void DitLines(float2* s, int logN, int logNl, int ls, int es, const float2* __restrict__ tw, int logG,
-                         bool inv)
+// Inverse groups groups-1 .. first (down to group `first`) of lines in shared memory.
+template <bool kCols, class Addr>
+__device__ void InverseRest(const LinePlan& P, const float2* twg, const Addr& S, int nb, int BL, int logBL, int last,
+                            int first)
 {
-   const int N = 1 << logN, total4 = (N >> 2) << logNl, total2 = (N >> 1) << logNl;
-   int logQ = 0;
-   if (logN & 1)   // the first stage, span 1
+   for (int g = last; g >= first; --g)
    {
-      for (int t = threadIdx.x; t < total2; t += blockDim.x)
-      {
-         int b, u;
-         TupleOf<kColumns>(t, logN - 1, logNl, b, u);
-         float2* L = s + b * ls;
-         const float2 a = L[2 * u * es], c = L[(2 * u + 1) * es];
-         L[2 * u * es] = Cadd(a, c);
-         L[(2 * u + 1) * es] = Csub(a, c);
-      }
-      __syncthreads();
-      logQ = 1;
-   }
-   for (; logQ < logN; logQ += 2)
-   {
-      const int q = 1 << logQ;
-      for (int t = threadIdx.x; t < total4; t += blockDim.x)
-      {
-         int b, u;
-         TupleOf<kColumns>(t, logN - 2, logNl, b, u);
-         const int j = u & (q - 1), i = ((u >> logQ) << (logQ + 2)) | j;
-         float2* L = s + b * ls;
-         const float2 w = Tw(tw, logG, logQ + 1, j, inv);
-         const float2 e0 = L[i * es], e1 = Cmul(L[(i + q) * es], w);
-         const float2 e2 = L[(i + 2 * q) * es], e3 = Cmul(L[(i + 3 * q) * es], w);
-         const float2 a0 = Cadd(e0, e1), a1 = Csub(e0, e1), a2 = Cadd(e2, e3), a3 = Csub(e2, e3);
-         const float2 b2 = Cmul(a2, Tw(tw, logG, logQ + 2, j, inv)), b3 = Cmul(a3, Tw(tw, logG, logQ + 2, j + q, inv));
-         L[i * es] = Cadd(a0, b2);
-         L[(i + 2 * q) * es] = Csub(a0, b2);
-         L[(i + q) * es] = Cadd(a1, b3);
-         L[(i + 3 * q) * es] = Csub(a1, b3);
-      }
+      const int logQ = LogQ(P, g);
+      const float2* tw = GroupTw(P, twg, g);
+      ISCU_RADIX_SWITCH(P.r[g], (SmemGroup<R, true, kCols>(S, nb, BL, logBL, P.logN, logQ, tw)));
       __syncthreads();
    }
 }
@@ -183,181 +330,398 @@ struct Dims
 {
    int nxv, nyv, nzv;   // valid extent of the input (volume or PSF)
    int GX, GY, GZ, H, NK, G, logH, logGY, logGZ, logG, logGX;
+   LinePlan px, py, pz;   // group plans of the H-, GY- and GZ-point transforms
 };
 
-// Rows of `in` (nzv x nyv x nxv) -> A[z][k][y], k <= H, y < nyv. grid (ceil(nyv / BY), nzv); smem BY * H float2.
-__global__ void __launch_bounds__(kThreads) XForwardKernel(const float* __restrict__ in, Dims d, int BY,
-                                                           const float2* __restrict__ tw, float2* __restrict__ A)
+// X forward group 0: packed pairs z[n] = x[2n] + i x[2n+1] of row b straight from global memory (lanes walk j, so
+// the loads coalesce), DIF group, twiddles, into the column layout.
+template <int R, bool kHalf>
+__device__ void XFirst(const ColAddr& S, const float* __restrict__ src, int nxv, int nb, int logQ,
+                       const float2* __restrict__ tw, bool pairs)
+{
+   const int q = 1 << logQ, total = nb << logQ;
+   for (int t = threadIdx.x; t < total; t += blockDim.x)
+   {
+      const int b = t >> logQ, j = t & (q - 1);
+      const float* row = src + static_cast<size_t>(b) * nxv;
+      float2 v[R];
+#pragma unroll
+      for (int m = 0; m < (kHalf ? R / 2 : R); ++m)
+      {
+         const int n = j + m * q;
+         if (pairs)
+            v[m] = 2 * n < nxv ? __ldg(reinterpret_cast<const float2*>(row) + n) : make_float2(0.f, 0.f);
+         else
+            v[m] = make_float2(2 * n < nxv ? __ldg(row + 2 * n) : 0.f, 2 * n + 1 < nxv ? __ldg(row + 2 * n + 1) : 0.f);
+      }
+      DifReg<R, false, kHalf>(v);
+      if (tw)
+         Twiddle<R, false>(v, tw, q, j);
+#pragma unroll
+      for (int m = 0; m < R; ++m)
+         S(b, j + m * q) = v[m];
+   }
+}
+
+// Rows of `in` (nzv x nyv x nxv) -> A[z][k][y], k <= H, y < nyv. grid (ceil(nyv / BY), nzv); BY a power of two;
+// smem H * (BY + 1) float2.
+__global__ void __launch_bounds__(kThreads, kMinCtas) XForwardKernel(const float* __restrict__ in, Dims d, int BY, int logBY,
+                                                           const float2* __restrict__ tw, const float2* __restrict__ twg,
+                                                           float2* __restrict__ A)
 {
    extern __shared__ float2 s[];
    const int z = blockIdx.y, y0 = blockIdx.x * BY;
    const int nb = min(BY, d.nyv - y0), H = d.H;
+   const ColAddr S{s, BY + 1};
    const float* src = in + (static_cast<size_t>(z) * d.nyv + y0) * d.nxv;
-   // packed pairs z[n] = x[2n] + i x[2n+1], natural order (the DIF input)
-   for (int t = threadIdx.x; t < BY * H; t += blockDim.x)
-   {
-      const int b = t / H, n = t % H;
-      float2 v = make_float2(0.f, 0.f);
-      if (b < nb)
-      {
-         const float* row = src + static_cast<size_t>(b) * d.nxv;
-         if (2 * n < d.nxv)
-            v.x = row[2 * n];
-         if (2 * n + 1 < d.nxv)
-            v.y = row[2 * n + 1];
-      }
-      s[b * H + n] = v;
-   }
+   const LinePlan& P = d.px;
+   const bool pairs = (d.nxv & 1) == 0 && (reinterpret_cast<uintptr_t>(in) & 7) == 0;
+   const int logQ0 = LogQ(P, 0);
+   const float2* tw0 = GroupTw(P, twg, 0);
+   if (d.nxv <= H)
+      ISCU_RADIX_SWITCH(P.r[0], (XFirst<R, true>(S, src, d.nxv, nb, logQ0, tw0, pairs)))
+   else
+      ISCU_RADIX_SWITCH(P.r[0], (XFirst<R, false>(S, src, d.nxv, nb, logQ0, tw0, pairs)))
    __syncthreads();
-   DifLines<false>(s, d.logH, __ffs(BY) - 1, H, 1, tw, d.logG, false);
+   ForwardRest<true>(P, twg, S, nb, BY, logBY);
    // X[k] = ((Z[k] + conj Z[H-k]) - i W_GX^k (Z[k] - conj Z[H-k])) / 2, Z in bit-reversed order
    for (int t = threadIdx.x; t < (H + 1) * BY; t += blockDim.x)
    {
-      const int k = t / BY, b = t % BY;
+      const int k = t >> logBY, b = t & (BY - 1);
       if (b >= nb)
          continue;
-      const float2 zk = s[b * H + Rev(k & (H - 1), d.logH)];
-      const float2 zm = Conj(s[b * H + Rev((H - k) & (H - 1), d.logH)]);
+      const float2 zk = S(b, Rev(k & (H - 1), d.logH));
+      const float2 zm = Conj(S(b, Rev((H - k) & (H - 1), d.logH)));
       const float2 e = Cadd(zk, zm), o = Csub(zk, zm);
-      const float2 w = Tw(tw, d.logG, d.logGX, k, false);
+      const float2 w = __ldg(tw + (k << (d.logG - d.logGX)));
       const float2 wo = Cmul(w, o);   // then times -i: (x, y) -> (y, -x)
       const float2 X = make_float2(0.5f * (e.x + wo.y), 0.5f * (e.y - wo.x));
       A[(static_cast<size_t>(z) * d.NK + k) * d.nyv + y0 + b] = X;
    }
 }
 
-// A rows (nyv values per (z, k)) -> B[z][k][p], p = bit-reversed ky. grid (ceil(NK / BK), nzv).
-__global__ void __launch_bounds__(kThreads) YForwardKernel(const float2* __restrict__ A, Dims d, int BK,
-                                                           const float2* __restrict__ tw, float2* __restrict__ B)
+// Y forward group 0: rows of A (nyv values, zero beyond) straight from global memory, lanes walking j.
+template <int R, bool kHalf>
+__device__ void YFirst(const RowAddr& S, const float2* __restrict__ rows, int nyv, int nb, int logQ,
+                       const float2* __restrict__ tw)
+{
+   const int q = 1 << logQ, total = nb << logQ;
+   for (int t = threadIdx.x; t < total; t += blockDim.x)
+   {
+      const int b = t >> logQ, j = t & (q - 1);
+      const float2* row = rows + static_cast<size_t>(b) * nyv;
+      float2 v[R];
+#pragma unroll
+      for (int m = 0; m < (kHalf ? R / 2 : R); ++m)
+      {
+         const int n = j + m * q;
+         v[m] = n < nyv ? __ldg(row + n) : make_float2(0.f, 0.f);
+      }
+      DifReg<R, false, kHalf>(v);
+      if (tw)
+         Twiddle<R, false>(v, tw, q, j);
+#pragma unroll
+      for (int m = 0; m < R; ++m)
+         S(b, j + m * q) = v[m];
+   }
+}
+
+__device__ __forceinline__ RowAddr RowsOf(float2* s, const LinePlan& P)
+{
+   const int rl = P.r[P.groups - 1];
+   return RowAddr{s, (1 << P.logN) + ((1 << P.logN) >> rl), rl};
+}
+
+// A rows (nyv values per (z, k)) -> B[z][k][p], p = bit-reversed ky. grid (ceil(NK / BK), nzv); smem BK rows.
+__global__ void __launch_bounds__(kThreads, kMinCtas) YForwardKernel(const float2* __restrict__ A, Dims d, int BK,
+                                                           const float2* __restrict__ twg, float2* __restrict__ B)
 {
    extern __shared__ float2 s[];
    const int z = blockIdx.y, k0 = blockIdx.x * BK, nb = min(BK, d.NK - k0), N = d.GY;
-   for (int t = threadIdx.x; t < BK * N; t += blockDim.x)
-   {
-      const int b = t / N, n = t % N;
-      float2 v = make_float2(0.f, 0.f);
-      if (b < nb && n < d.nyv)
-         v = A[(static_cast<size_t>(z) * d.NK + k0 + b) * d.nyv + n];
-      s[b * N + n] = v;
-   }
+   const LinePlan& P = d.py;
+   const RowAddr S = RowsOf(s, P);
+   const float2* rows = A + (static_cast<size_t>(z) * d.NK + k0) * d.nyv;
+   const int logQ0 = LogQ(P, 0);
+   const float2* tw0 = GroupTw(P, twg, 0);
+   if (2 * d.nyv <= N)
+      ISCU_RADIX_SWITCH(P.r[0], (YFirst<R, true>(S, rows, d.nyv, nb, logQ0, tw0)))
+   else
+      ISCU_RADIX_SWITCH(P.r[0], (YFirst<R, false>(S, rows, d.nyv, nb, logQ0, tw0)))
    __syncthreads();
-   DifLines<false>(s, d.logGY, __ffs(BK) - 1, N, 1, tw, d.logG, false);
+   ForwardRest<false>(P, twg, S, nb, 1, 0);
+   float2* out = B + (static_cast<size_t>(z) * d.NK + k0) * N;
    for (int t = threadIdx.x; t < nb * N; t += blockDim.x)
    {
-      const int b = t / N, p = t % N;
-      B[(static_cast<size_t>(z) * d.NK + k0 + b) * N + p] = s[b * N + p];
+      const int b = t >> d.logGY, p = t & (N - 1);
+      out[static_cast<size_t>(b) * N + p] = S(b, p);
+   }
+}
+
+// Y inverse group 0: conjugate twiddles, DIT, natural order out; rows [oy, oy + nyv) to global memory.
+template <int R>
+__device__ void YLast(const RowAddr& S, float2* __restrict__ rows, int nyv, int oy, int nb, int logQ,
+                      const float2* __restrict__ tw)
+{
+   const int q = 1 << logQ, total = nb << logQ;
+   for (int t = threadIdx.x; t < total; t += blockDim.x)
+   {
+      const int b = t >> logQ, j = t & (q - 1);
+      float2 v[R];
+#pragma unroll
+      for (int m = 0; m < R; ++m)
+         v[m] = S(b, j + m * q);
+      if (tw)
+         Twiddle<R, true>(v, tw, q, j);
+      DitReg<R, true>(v);
+      float2* row = rows + static_cast<size_t>(b) * nyv;
+#pragma unroll
+      for (int m = 0; m < R; ++m)
+      {
+         const int y = j + m * q - oy;
+         if (y >= 0 && y < nyv)
+            row[y] = v[m];
+      }
+   }
+}
+
+// B rows (bit-reversed ky) -> inverse GY-point FFT -> rows [oy, oy + nyv) into A[z][k][y]. grid (ceil(NK / BK), nzv).
+__global__ void __launch_bounds__(kThreads, kMinCtas) YInverseKernel(const float2* __restrict__ B, Dims d, int BK, int oy,
+                                                           const float2* __restrict__ twg, float2* __restrict__ A)
+{
+   extern __shared__ float2 s[];
+   const int z = blockIdx.y, k0 = blockIdx.x * BK, nb = min(BK, d.NK - k0), N = d.GY;
+   const LinePlan& P = d.py;
+   const RowAddr S = RowsOf(s, P);
+   const float2* in = B + (static_cast<size_t>(z) * d.NK + k0) * N;
+   for (int t = threadIdx.x; t < nb * N; t += blockDim.x)
+      CopyAsync8(&S(t >> d.logGY, t & (N - 1)), in + t);
+   CopyAsyncWait();
+   __syncthreads();
+   InverseRest<false>(P, twg, S, nb, 1, 0, P.groups - 1, 1);
+   float2* rows = A + (static_cast<size_t>(z) * d.NK + k0) * d.nyv;
+   ISCU_RADIX_SWITCH(P.r[0], (YLast<R>(S, rows, d.nyv, oy, nb, LogQ(P, 0), GroupTw(P, twg, 0))));
+}
+
+// Z forward group 0: columns straight from global memory (lanes walk the columns), DIF group, twiddles.
+template <int R, bool kHalf>
+__device__ void ZFirst(const ColAddr& S, const float2* __restrict__ B, size_t plane, size_t col, int nzv, int nb,
+                       int BL, int logBL, int logQ, const float2* __restrict__ tw)
+{
+   const int q = 1 << logQ, total = BL << logQ;
+   for (int t = threadIdx.x; t < total; t += blockDim.x)
+   {
+      const int b = t & (BL - 1), j = t >> logBL;
+      if (b >= nb)
+         continue;
+      float2 v[R];
+#pragma unroll
+      for (int m = 0; m < (kHalf ? R / 2 : R); ++m)
+      {
+         const int n = j + m * q;
+         v[m] = n < nzv ? __ldg(B + n * plane + col + b) : make_float2(0.f, 0.f);
+      }
+      DifReg<R, false, kHalf>(v);
+      if (tw)
+         Twiddle<R, false>(v, tw, q, j);
+#pragma unroll
+      for (int m = 0; m < R; ++m)
+         S(b, j + m * q) = v[m];
+   }
+}
+
+// The last forward group (span 1, contiguous points; skipped when group 0 was the only one), then either the
+// spectrum out to Kh (kConvolve false) or times the PSF spectrum (KS: this CTA's columns of Kh, prefetched into
+// shared memory) and the first inverse group, back into shared memory.
+template <int R, bool kConvolve>
+__device__ void ZTurn(const ColAddr& S, const float2* KS, float2* __restrict__ Kh, size_t plane, size_t col, int nb,
+                      int BL, int logBL, int logN, bool dif, bool dit)
+{
+   constexpr int r = Log2i(R);
+   const int logT = logN - r, total = BL << logT;
+   for (int t = threadIdx.x; t < total; t += blockDim.x)
+   {
+      const int b = t & (BL - 1), base = (t >> logBL) << r;
+      if (b >= nb)
+         continue;
+      float2 v[R];
+#pragma unroll
+      for (int m = 0; m < R; ++m)
+         v[m] = S(b, base + m);
+      if (dif)
+         DifReg<R, false, false>(v);
+      if constexpr (!kConvolve)
+      {
+#pragma unroll
+         for (int m = 0; m < R; ++m)
+            Kh[(base + m) * plane + col + b] = v[m];
+      }
+      else
+      {
+#pragma unroll
+         for (int m = 0; m < R; ++m)
+            v[m] = Cmul(v[m], KS[(base + m) * BL + b]);
+         if (dit)
+            DitReg<R, true>(v);
+#pragma unroll
+         for (int m = 0; m < R; ++m)
+            S(b, base + m) = v[m];
+      }
+   }
+}
+
+// Z inverse group 0: conjugate twiddles, DIT (skipped when group 0 was the only one, ZTurn did it), planes
+// [oz, oz + nzv) to global memory.
+template <int R>
+__device__ void ZLast(const ColAddr& S, float2* __restrict__ B, size_t plane, size_t col, int nzv, int oz, int nb,
+                      int BL, int logBL, int logQ, const float2* __restrict__ tw, bool dit)
+{
+   const int q = 1 << logQ, total = BL << logQ;
+   for (int t = threadIdx.x; t < total; t += blockDim.x)
+   {
+      const int b = t & (BL - 1), j = t >> logBL;
+      if (b >= nb)
+         continue;
+      float2 v[R];
+#pragma unroll
+      for (int m = 0; m < R; ++m)
+         v[m] = S(b, j + m * q);
+      if (dit)
+      {
+         if (tw)
+            Twiddle<R, true>(v, tw, q, j);
+         DitReg<R, true>(v);
+      }
+#pragma unroll
+      for (int m = 0; m < R; ++m)
+      {
+         const int zz = j + m * q - oz;
+         if (zz >= 0 && zz < nzv)
+            B[zz * plane + col + b] = v[m];
+      }
    }
 }
 
 // Columns along z of B (nzv planes) -> GZ-point forward FFT -> either the PSF spectrum Kh[pz][k][p] (all GZ planes,
 // forward only) or, times Kh, the inverse FFT cropped to planes [oz, oz + nzv) back into B.
-// grid (ceil(GY / BZ), NK); smem GZ * BZ float2, column layout.
+// grid (ceil(GY / BZ), NK), BZ a power of two; smem GZ * BZ float2, column layout (twice that when convolving: the
+// PSF spectrum's columns are copied in asynchronously while group 0 loads and transforms B).
 template <bool kConvolve>
-__global__ void __launch_bounds__(kThreads) ZKernel(float2* __restrict__ B, Dims d, int BZ, int oz,
-                                                    const float2* __restrict__ tw, float2* __restrict__ Kh)
+__global__ void __launch_bounds__(kThreads, kMinCtas) ZKernel(float2* __restrict__ B, Dims d, int BZ, int logBZ, int oz,
+                                                    const float2* __restrict__ twg, float2* __restrict__ Kh)
 {
    extern __shared__ float2 s[];
-   const int k = blockIdx.y, p0 = blockIdx.x * BZ, nb = min(BZ, d.GY - p0), N = d.GZ;
+   const int k = blockIdx.y, p0 = blockIdx.x * BZ, nb = min(BZ, d.GY - p0);
    const size_t plane = static_cast<size_t>(d.NK) * d.GY;
    const size_t col = static_cast<size_t>(k) * d.GY + p0;
-   for (int t = threadIdx.x; t < N * BZ; t += blockDim.x)
-   {
-      const int n = t / BZ, b = t % BZ;
-      float2 v = make_float2(0.f, 0.f);
-      if (b < nb && n < d.nzv)
-         v = B[n * plane + col + b];
-      s[n * BZ + b] = v;
-   }
-   __syncthreads();
-   DifLines<true>(s, d.logGZ, __ffs(BZ) - 1, 1, BZ, tw, d.logG, false);
-   if (!kConvolve)
-   {
-      for (int t = threadIdx.x; t < N * BZ; t += blockDim.x)
+   const LinePlan& P = d.pz;
+   const ColAddr S{s, BZ};
+   float2* KS = s + (static_cast<size_t>(d.GZ) << logBZ);
+   if (kConvolve)
+      for (int t = threadIdx.x; t < (d.GZ << logBZ); t += blockDim.x)
       {
-         const int n = t / BZ, b = t % BZ;
+         const int b = t & (BZ - 1), n = t >> logBZ;
          if (b < nb)
-            Kh[n * plane + col + b] = s[n * BZ + b];
+            CopyAsync8(KS + t, Kh + n * plane + col + b);
       }
-      return;
-   }
-   for (int t = threadIdx.x; t < N * BZ; t += blockDim.x)
-   {
-      const int n = t / BZ, b = t % BZ;
-      if (b < nb)
-         s[n * BZ + b] = Cmul(s[n * BZ + b], Kh[n * plane + col + b]);
-   }
+   const int logQ0 = LogQ(P, 0);
+   const float2* tw0 = GroupTw(P, twg, 0);
+   if (2 * d.nzv <= (1 << P.logN))
+      ISCU_RADIX_SWITCH(P.r[0], (ZFirst<R, true>(S, B, plane, col, d.nzv, nb, BZ, logBZ, logQ0, tw0)))
+   else
+      ISCU_RADIX_SWITCH(P.r[0], (ZFirst<R, false>(S, B, plane, col, d.nzv, nb, BZ, logBZ, logQ0, tw0)))
    __syncthreads();
-   DitLines<true>(s, d.logGZ, __ffs(BZ) - 1, 1, BZ, tw, d.logG, true);
-   for (int t = threadIdx.x; t < d.nzv * BZ; t += blockDim.x)
+   for (int g = 1; g < P.groups - 1; ++g)
    {
-      const int n = t / BZ, b = t % BZ;
-      if (b < nb)
-         B[n * plane + col + b] = s[(n + oz) * BZ + b];
+      ISCU_RADIX_SWITCH(P.r[g], (SmemGroup<R, false, true>(S, nb, BZ, logBZ, P.logN, LogQ(P, g), GroupTw(P, twg, g))));
+      __syncthreads();
    }
+   const bool single = P.groups == 1;
+   if (kConvolve)
+   {
+      CopyAsyncWait();
+      __syncthreads();
+   }
+   ISCU_RADIX_SWITCH(P.r[P.groups - 1],
+                     (ZTurn<R, kConvolve>(S, KS, Kh, plane, col, nb, BZ, logBZ, P.logN, !single, true)));
+   if (!kConvolve)
+      return;
+   __syncthreads();
+   if (!single)
+      InverseRest<true>(P, twg, S, nb, BZ, logBZ, P.groups - 2, 1);
+   ISCU_RADIX_SWITCH(P.r[0], (ZLast<R>(S, B, plane, col, d.nzv, oz, nb, BZ, logBZ, logQ0, tw0, !single)));
 }
 
-// B rows (bit-reversed ky) -> inverse GY-point FFT -> rows [oy, oy + nyv) into A[z][k][y]. grid (ceil(NK / BK), nzv).
-__global__ void __launch_bounds__(kThreads) YInverseKernel(const float2* __restrict__ B, Dims d, int BK, int oy,
-                                                           const float2* __restrict__ tw, float2* __restrict__ A)
+// X inverse, the last DIF group's inverse (span 1, no twiddles) straight from A: Z'[k] = (X[k] + conj X[H-k]) +
+// i W_GX^-k (X[k] - conj X[H-k]) at bit-reversed slots, lanes walking the rows.
+template <int R>
+__device__ void XLoad(const ColAddr& S, const float2* __restrict__ Az, int nyv, int y0, int nb, int BL, int logBL,
+                      int H, int logH, const float2* __restrict__ tw, int twShift)
 {
-   extern __shared__ float2 s[];
-   const int z = blockIdx.y, k0 = blockIdx.x * BK, nb = min(BK, d.NK - k0), N = d.GY;
-   for (int t = threadIdx.x; t < BK * N; t += blockDim.x)
+   constexpr int r = Log2i(R);
+   const int logT = logH - r, total = BL << logT;
+   for (int t = threadIdx.x; t < total; t += blockDim.x)
    {
-      const int b = t / N, p = t % N;
-      s[b * N + p] = b < nb ? B[(static_cast<size_t>(z) * d.NK + k0 + b) * N + p] : make_float2(0.f, 0.f);
-   }
-   __syncthreads();
-   DitLines<false>(s, d.logGY, __ffs(BK) - 1, N, 1, tw, d.logG, true);
-   for (int t = threadIdx.x; t < nb * d.nyv; t += blockDim.x)
-   {
-      const int b = t / d.nyv, y = t % d.nyv;
-      A[(static_cast<size_t>(z) * d.NK + k0 + b) * d.nyv + y] = s[b * N + y + oy];
+      const int b = t & (BL - 1), base = (t >> logBL) << r;
+      if (b >= nb)
+         continue;
+      float2 v[R];
+#pragma unroll
+      for (int m = 0; m < R; ++m)
+      {
+         const int k = Rev(base + m, logH);
+         const float2 xk = __ldg(Az + static_cast<size_t>(k) * nyv + y0 + b);
+         const float2 xm = Conj(__ldg(Az + static_cast<size_t>(H - k) * nyv + y0 + b));
+         const float2 w = Conj(__ldg(tw + (k << twShift)));
+         const float2 e = Cadd(xk, xm), o = Cmul(Csub(xk, xm), w);
+         v[m] = make_float2(e.x - o.y, e.y + o.x);   // e + i o
+      }
+      DitReg<R, true>(v);
+#pragma unroll
+      for (int m = 0; m < R; ++m)
+         S(b, base + m) = v[m];
    }
 }
 
 // A (half spectrum along x, per (z, y)) -> GX reals -> columns [ox, ox + nxv), scaled, max(0, .) + background ->
-// image and/or noise chain. grid (ceil(nyv / BY), nzv).
-__global__ void __launch_bounds__(kThreads) XInverseKernel(const float2* __restrict__ A, Dims d, int BY, int ox,
-                                                           float scale, float background, const float2* __restrict__ tw,
-                                                           StaticView st, CameraView cam, int noise, uint32_t seed,
-                                                           uint32_t frame0, float* __restrict__ image,
-                                                           uint16_t* __restrict__ adu)
+// the photon frames. grid (ceil(nyv / BY), nzv), BY a power of two; smem H * (BY + 1) float2.
+__global__ void __launch_bounds__(kThreads, kMinCtas) XInverseKernel(const float2* __restrict__ A, Dims d, int BY,
+                                                                     int logBY, int ox, float scale, float background,
+                                                                     const float2* __restrict__ tw,
+                                                                     const float2* __restrict__ twg,
+                                                                     float* __restrict__ image)
 {
    extern __shared__ float2 s[];
    const int z = blockIdx.y, y0 = blockIdx.x * BY, nb = min(BY, d.nyv - y0), H = d.H;
-   // Z'[k] = (X[k] + conj X[H-k]) + i W_GX^-k (X[k] - conj X[H-k]), k < H, into bit-reversed positions.
-   for (int t = threadIdx.x; t < H * BY; t += blockDim.x)
-   {
-      const int k = t / BY, b = t % BY;
-      float2 v = make_float2(0.f, 0.f);
-      if (b < nb)
-      {
-         const float2 xk = A[(static_cast<size_t>(z) * d.NK + k) * d.nyv + y0 + b];
-         const float2 xm = Conj(A[(static_cast<size_t>(z) * d.NK + (H - k)) * d.nyv + y0 + b]);
-         const float2 e = Cadd(xk, xm), o = Cmul(Csub(xk, xm), Tw(tw, d.logG, d.logGX, k, true));
-         v = make_float2(e.x - o.y, e.y + o.x);   // e + i o
-      }
-      s[b * H + Rev(k, d.logH)] = v;
-   }
+   const LinePlan& P = d.px;
+   const ColAddr S{s, BY + 1};
+   const float2* Az = A + static_cast<size_t>(z) * d.NK * d.nyv;
+   ISCU_RADIX_SWITCH(P.r[P.groups - 1],
+                     (XLoad<R>(S, Az, d.nyv, y0, nb, BY, logBY, H, d.logH, tw, d.logG - d.logGX)));
    __syncthreads();
-   DitLines<false>(s, d.logH, __ffs(BY) - 1, H, 1, tw, d.logG, true);
-   const uint32_t W = static_cast<uint32_t>(d.nxv);
-   CounterRng u(seed, frame0 + static_cast<uint32_t>(z));
+   InverseRest<true>(P, twg, S, nb, BY, logBY, P.groups - 2, 0);
+   float* out = image + (static_cast<size_t>(z) * d.nyv + y0) * d.nxv;
    for (int t = threadIdx.x; t < nb * d.nxv; t += blockDim.x)
    {
       const int b = t / d.nxv, x = t % d.nxv;
       const int m = x + ox;
-      const float2 c = s[b * H + (m >> 1)];
+      const float2 c = S(b, m >> 1);
       const float v = (m & 1 ? c.y : c.x) * scale;
-      const float photons = (v > 0.f ? v : 0.f) + background;
-      const uint32_t i = static_cast<uint32_t>(y0 + b) * W + static_cast<uint32_t>(x);
-      const size_t o = static_cast<size_t>(z) * d.nyv * W + i;
-      if (image)
-         image[o] = photons;
-      if (noise)
-         adu[o] = NoisePixel(photons, i, cam, st, u);
+      out[t] = (v > 0.f ? v : 0.f) + background;
    }
+}
+
+// The noise chain of every pixel of the photon frames (frame frame0 + plane) -> ADU. A kernel of its own: the
+// float64 chain wants many resident warps, the transforms wants registers. grid (ceil(nx ny / 256), nz).
+__global__ void __launch_bounds__(256) WfNoiseKernel(const float* __restrict__ photons, uint32_t npix, StaticView st,
+                                                     CameraView cam, uint32_t seed, uint32_t frame0,
+                                                     uint16_t* __restrict__ adu)
+{
+   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= npix)
+      return;
+   const size_t o = static_cast<size_t>(blockIdx.y) * npix + i;
+   CounterRng u(seed, frame0 + blockIdx.y);
+   adu[o] = NoisePixel(photons[o], i, cam, st, u);
 }
 
 __global__ void TwiddleKernel(int G, float2* tw)
@@ -368,6 +732,19 @@ __global__ void TwiddleKernel(int G, float2* tw)
    double sn, cs;
    sincospi(-2.0 * j / G, &sn, &cs);
    tw[j] = make_float2(static_cast<float>(cs), static_cast<float>(sn));
+}
+
+// A group's table: entry m q + j = W_M^(j rev_r(m)), M = q 2^r, rounded from float64.
+__global__ void GroupTwiddleKernel(int logQ, int r, float2* out)
+{
+   const int M = 1 << (logQ + r), i = blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= M)
+      return;
+   const int m = i >> logQ, j = i & ((1 << logQ) - 1);
+   const int e = j * (r ? static_cast<int>(__brev(static_cast<unsigned>(m)) >> (32 - r)) : 0);
+   double sn, cs;
+   sincospi(-2.0 * e / M, &sn, &cs);
+   out[i] = make_float2(static_cast<float>(cs), static_cast<float>(sn));
 }
 
 int Log2(uint32_t v)
@@ -386,26 +763,91 @@ uint32_t Pow2AtLeast(uint32_t v)
    return p;
 }
 
-int LinesPerCta(int N, int cap)
+// Group sizes for an N = 2^logN point transform: one group up to 32 points; else groups of 2^3..2^5. Rows: the
+// last (span-1) group at least 16 points, so that every group but the last has a smallest span q >= 16 (the padded
+// row layout is conflict-free for those). Columns (lanes walk the lines, any q is conflict-free): the larger group
+// first, for more loads in flight per thread where group 0 reads global memory.
+LinePlan MakeLinePlan(int logN, bool cols)
 {
-   int b = static_cast<int>(kSmemLimit / (static_cast<size_t>(N) * sizeof(float2)));
-   return std::max(1, std::min(b, cap));
+   LinePlan P;
+   P.logN = logN;
+   if (logN <= 5)
+   {
+      P.groups = 1;
+      P.r[0] = logN;
+   }
+   else if (logN <= 10)
+   {
+      P.groups = 2;
+      if (cols)
+         P.r[0] = std::min(5, (logN + 1) / 2);
+      else
+         P.r[0] = logN - (logN >= 9 ? logN - 5 : 4);
+      P.r[1] = logN - P.r[0];
+   }
+   else
+   {
+      P.groups = 3;
+      P.r[1] = 4;
+      P.r[2] = 4;
+      P.r[0] = logN - 8;
+   }
+   return P;
 }
+
+// Assigns the tables of the groups with q > 1 at `offset` (float2 entries) onwards; returns the entries used.
+int PlaceTables(LinePlan& P, int offset)
+{
+   int used = 0;
+   for (int g = 0; g < P.groups; ++g)
+   {
+      const int logQ = LogQ(P, g);
+      if (logQ == 0)
+         continue;
+      P.tw[g] = offset + used;
+      used += 1 << (logQ + P.r[g]);
+   }
+   return used;
+}
+
+int PowTwoAtMost(int v)
+{
+   int p = 1;
+   while (p * 2 <= v)
+      p *= 2;
+   return p;
+}
+
+// Lines per CTA for each pass, sized to the shared-memory budget.
+int XLines(int H) { return PowTwoAtMost(std::max<int>(1, std::min<int>(16, kSmemBudget / (static_cast<size_t>(H) * sizeof(float2)) - 1))); }
+size_t XSmem(int H, int BY) { return static_cast<size_t>(H) * (BY + 1) * sizeof(float2); }
+size_t RowBytes(const LinePlan& P)
+{
+   const int N = 1 << P.logN;
+   return static_cast<size_t>(N + (N >> P.r[P.groups - 1])) * sizeof(float2);
+}
+int YLines(const LinePlan& P)
+{
+   const int N = 1 << P.logN;
+   return std::max<int>(1, std::min<int>(std::max(1, 8192 / N), static_cast<int>(kSmemBudget / RowBytes(P))));
+}
+int ZLines(int GZ) { return PowTwoAtMost(std::max<int>(1, std::min<int>(32, kSmemBudget / (2 * static_cast<size_t>(GZ) * sizeof(float2))))); }
 
 // The forward x and y passes of a (kzv x kyv x kxv) volume into A, B.
 int ForwardXY(iscu_wf_plan* p, const float* in, const Dims& d, float2* A, float2* B, bool mark = false)
 {
    iscu_ctx* ctx = p->ctx;
    const float2* tw = p->tw.as<float2>();
-   const int BY = LinesPerCta(d.H, 16);
-   XForwardKernel<<<dim3((d.nyv + BY - 1) / BY, d.nzv), kThreads, BY * d.H * sizeof(float2), ctx->stream>>>(
-      in, d, BY, tw, A);
+   const float2* twg = p->twg.as<float2>();
+   const int BY = XLines(d.H);
+   XForwardKernel<<<dim3((d.nyv + BY - 1) / BY, d.nzv), kThreads, XSmem(d.H, BY), ctx->stream>>>(
+      in, d, BY, Log2(BY), tw, twg, A);
    ISCU_CK_LAUNCH(ctx, "XForwardKernel");
    if (mark)
       p->Mark(1);
-   const int BK = LinesPerCta(d.GY, 16);
-   YForwardKernel<<<dim3((d.NK + BK - 1) / BK, d.nzv), kThreads, BK * d.GY * sizeof(float2), ctx->stream>>>(
-      A, d, BK, tw, B);
+   const int BK = YLines(d.py);
+   YForwardKernel<<<dim3((d.NK + BK - 1) / BK, d.nzv), kThreads, BK * RowBytes(d.py), ctx->stream>>>(
+      A, d, BK, twg, B);
    ISCU_CK_LAUNCH(ctx, "YForwardKernel");
    return ISCU_OK;
 }
@@ -427,12 +869,15 @@ Dims MakeDims(const iscu_wf_plan* p, uint32_t nxv, uint32_t nyv, uint32_t nzv)
    d.logGZ = p->logGZ;
    d.logG = Log2(p->G);
    d.logGX = Log2(p->GX);
+   d.px = p->px;
+   d.py = p->py;
+   d.pz = p->pz;
    return d;
 }
 
 int SetFftSmem()
 {
-   const int bytes = static_cast<int>(kSmemLimit);
+   const int bytes = static_cast<int>(kSmemMax);
    ISCU_CK(cudaFuncSetAttribute(XForwardKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
    ISCU_CK(cudaFuncSetAttribute(YForwardKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
    ISCU_CK(cudaFuncSetAttribute(ZKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
@@ -449,20 +894,21 @@ static int ConvolveToA(iscu_wf_plan* p, const float* density)
 {
    iscu_ctx* ctx = p->ctx;
    const Dims d = MakeDims(p, p->nx, p->ny, p->nz);
-   const float2* tw = p->tw.as<float2>();
+   const float2* twg = p->twg.as<float2>();
    p->Mark(0);
    int rc = ForwardXY(p, density, d, p->A.as<float2>(), p->B.as<float2>(), true);
    if (rc != ISCU_OK)
       return rc;
    p->Mark(2);
-   const int BZ = LinesPerCta(d.GZ, 32);
-   ZKernel<true><<<dim3((d.GY + BZ - 1) / BZ, d.NK), kThreads, d.GZ * BZ * sizeof(float2), ctx->stream>>>(
-      p->B.as<float2>(), d, BZ, static_cast<int>(p->kz / 2), tw, p->Kh.as<float2>());
+   const int BZ = ZLines(d.GZ);
+   ZKernel<true><<<dim3((d.GY + BZ - 1) / BZ, d.NK), kThreads, 2 * static_cast<size_t>(d.GZ) * BZ * sizeof(float2),
+                   ctx->stream>>>(p->B.as<float2>(), d, BZ, Log2(BZ), static_cast<int>(p->kz / 2), twg,
+                                  p->Kh.as<float2>());
    ISCU_CK_LAUNCH(ctx, "ZKernel<convolve>");
    p->Mark(3);
-   const int BK = LinesPerCta(d.GY, 16);
-   YInverseKernel<<<dim3((d.NK + BK - 1) / BK, d.nzv), kThreads, BK * d.GY * sizeof(float2), ctx->stream>>>(
-      p->B.as<float2>(), d, BK, static_cast<int>(p->ky / 2), tw, p->A.as<float2>());
+   const int BK = YLines(d.py);
+   YInverseKernel<<<dim3((d.NK + BK - 1) / BK, d.nzv), kThreads, BK * RowBytes(d.py), ctx->stream>>>(
+      p->B.as<float2>(), d, BK, static_cast<int>(p->ky / 2), twg, p->A.as<float2>());
    ISCU_CK_LAUNCH(ctx, "YInverseKernel");
    p->Mark(4);
    return ISCU_OK;
@@ -478,15 +924,26 @@ static int FinishX(iscu_wf_plan* p, double background, const iscu_camera* cam, u
       st = ctx->Static();
    st.width = p->nx;
    st.height = p->ny;
-   const CameraView cv = cam ? MakeCameraView(*cam) : CameraView();
    const float scale = static_cast<float>(1.0 / (static_cast<double>(p->GX) * p->GY * p->GZ));
-   // Few rows per CTA: the float64 noise chain that ends this pass wants occupancy more than row batching.
-   const int BY = LinesPerCta(d.H, 4);
-   XInverseKernel<<<dim3((d.nyv + BY - 1) / BY, d.nzv), kThreads, BY * d.H * sizeof(float2), ctx->stream>>>(
-      p->A.as<float2>(), d, BY, static_cast<int>(p->kx / 2), scale, static_cast<float>(background),
-      p->tw.as<float2>(), st, cv, cam ? 1 : 0, seed, frame0, image, adu);
+   if (!image)
+   {
+      ISCU_CK(p->image.Reserve(static_cast<size_t>(p->nx) * p->ny * p->nz * sizeof(float)));
+      image = p->image.as<float>();
+   }
+   const int BY = XLines(d.H);
+   XInverseKernel<<<dim3((d.nyv + BY - 1) / BY, d.nzv), kThreads, XSmem(d.H, BY), ctx->stream>>>(
+      p->A.as<float2>(), d, BY, Log2(BY), static_cast<int>(p->kx / 2), scale, static_cast<float>(background),
+      p->tw.as<float2>(), p->twg.as<float2>(), image);
    ISCU_CK_LAUNCH(ctx, "XInverseKernel");
    p->Mark(5);
+   if (cam)
+   {
+      const CameraView cv = MakeCameraView(*cam);
+      const uint32_t npix = p->nx * p->ny;
+      WfNoiseKernel<<<dim3((npix + 255) / 256, p->nz), 256, 0, ctx->stream>>>(image, npix, st, cv, seed, frame0, adu);
+      ISCU_CK_LAUNCH(ctx, "WfNoiseKernel");
+   }
+   p->Mark(6);
    return ISCU_OK;
 }
 
@@ -527,16 +984,32 @@ int iscu_wf_plan_create(iscu_ctx* ctx, uint32_t nx, uint32_t ny, uint32_t nz, co
    p->logH = Log2(p->H);
    p->logGY = Log2(p->GY);
    p->logGZ = Log2(p->GZ);
+   p->px = MakeLinePlan(p->logH, true);
+   p->py = MakeLinePlan(p->logGY, false);
+   p->pz = MakeLinePlan(p->logGZ, true);
+   int entries = PlaceTables(p->px, 0);
+   entries += PlaceTables(p->py, entries);
+   entries += PlaceTables(p->pz, entries);
    int rc = SetFftSmem();
    if (rc != ISCU_OK)
       return rc;
    const uint32_t nzA = std::max(nz, kz), nyA = std::max(ny, ky);
    ISCU_CK(p->tw.Reserve(p->G * sizeof(float2)));
+   ISCU_CK(p->twg.Reserve(std::max(entries, 1) * sizeof(float2)));
    ISCU_CK(p->A.Reserve(static_cast<size_t>(nzA) * p->NK * nyA * sizeof(float2)));
    ISCU_CK(p->B.Reserve(static_cast<size_t>(nzA) * p->NK * p->GY * sizeof(float2)));
    ISCU_CK(p->Kh.Reserve(static_cast<size_t>(p->GZ) * p->NK * p->GY * sizeof(float2)));
    TwiddleKernel<<<(p->G + 255) / 256, 256, 0, ctx->stream>>>(static_cast<int>(p->G), p->tw.as<float2>());
    ISCU_CK_LAUNCH(ctx, "TwiddleKernel");
+   for (const LinePlan* P : {&p->px, &p->py, &p->pz})
+      for (int g = 0; g < P->groups; ++g)
+         if (P->tw[g] >= 0)
+         {
+            const int M = 1 << (LogQ(*P, g) + P->r[g]);
+            GroupTwiddleKernel<<<(M + 255) / 256, 256, 0, ctx->stream>>>(LogQ(*P, g), P->r[g],
+                                                                          p->twg.as<float2>() + P->tw[g]);
+            ISCU_CK_LAUNCH(ctx, "GroupTwiddleKernel");
+         }
    // The PSF's spectrum: its own x and y passes (kx x ky x kz valid), then the forward z transform of all GZ planes.
    DevBuf dPsf;
    const size_t psfBytes = static_cast<size_t>(kx) * ky * kz * sizeof(float);
@@ -546,9 +1019,9 @@ int iscu_wf_plan_create(iscu_ctx* ctx, uint32_t nx, uint32_t ny, uint32_t nz, co
    rc = ForwardXY(p.get(), dPsf.as<float>(), dk, p->A.as<float2>(), p->B.as<float2>());
    if (rc != ISCU_OK)
       return rc;
-   const int BZ = LinesPerCta(dk.GZ, 32);
-   ZKernel<false><<<dim3((dk.GY + BZ - 1) / BZ, dk.NK), kThreads, dk.GZ * BZ * sizeof(float2), ctx->stream>>>(
-      p->B.as<float2>(), dk, BZ, 0, p->tw.as<float2>(), p->Kh.as<float2>());
+   const int BZ = ZLines(dk.GZ);
+   ZKernel<false><<<dim3((dk.GY + BZ - 1) / BZ, dk.NK), kThreads, static_cast<size_t>(dk.GZ) * BZ * sizeof(float2),
+                    ctx->stream>>>(p->B.as<float2>(), dk, BZ, Log2(BZ), 0, p->twg.as<float2>(), p->Kh.as<float2>());
    ISCU_CK_LAUNCH(ctx, "ZKernel<spectrum>");
    ISCU_CK(cudaStreamSynchronize(ctx->stream));
    *out = p.release();
@@ -562,23 +1035,23 @@ int iscu_wf_set_timing(iscu_wf_plan* plan, int32_t on)
    std::lock_guard<std::recursive_mutex> lock(plan->ctx->mu);
    ClearError();
    if (on && !plan->ev[0])
-      for (int i = 0; i < 6; ++i)
+      for (int i = 0; i <= ISCU_WF_PASSES; ++i)
          ISCU_CK(cudaEventCreate(&plan->ev[i]));
    plan->timing = on != 0;
    return ISCU_OK;
 }
 
-int iscu_wf_pass_times(iscu_wf_plan* plan, float* ms5)
+int iscu_wf_pass_times(iscu_wf_plan* plan, float* ms)
 {
-   if (!plan || !ms5)
+   if (!plan || !ms)
       return Fail(ISCU_ERR_ARG, "null argument");
    if (!plan->timing)
       return Fail(ISCU_ERR_STATE, "pass timing is off (iscu_wf_set_timing)");
    std::lock_guard<std::recursive_mutex> lock(plan->ctx->mu);
    ClearError();
-   ISCU_CK(cudaEventSynchronize(plan->ev[5]));
-   for (int i = 0; i < 5; ++i)
-      ISCU_CK(cudaEventElapsedTime(ms5 + i, plan->ev[i], plan->ev[i + 1]));
+   ISCU_CK(cudaEventSynchronize(plan->ev[ISCU_WF_PASSES]));
+   for (int i = 0; i < ISCU_WF_PASSES; ++i)
+      ISCU_CK(cudaEventElapsedTime(ms + i, plan->ev[i], plan->ev[i + 1]));
    return ISCU_OK;
 }
 
@@ -587,7 +1060,7 @@ void iscu_wf_plan_destroy(iscu_wf_plan* plan)
    if (!plan)
       return;
    cudaStreamSynchronize(plan->ctx->stream);
-   for (int i = 0; i < 6; ++i)
+   for (int i = 0; i <= ISCU_WF_PASSES; ++i)
       if (plan->ev[i])
          cudaEventDestroy(plan->ev[i]);
    delete plan;

@@ -669,8 +669,9 @@ class WidefieldPlan:
         check(self.lib.iscu_wf_set_timing(self.h, int(on)))
 
     def pass_times(self):
-        """The last render's pass durations (ms): x forward, y forward, z convolve, y inverse, x inverse + noise."""
-        ms = (C.c_float * 5)()
+        """The last render's pass durations (ms): x forward, y forward, z convolve, y inverse, x inverse, camera noise
+        (0 without a camera)."""
+        ms = (C.c_float * 6)()
         check(self.lib.iscu_wf_pass_times(self.h, ms))
         return list(ms)
 
