@@ -124,37 +124,38 @@ __device__ __forceinline__ double CounterPoisson(double l, CounterRng& u)
       return static_cast<double>(k - 1);
    }
    // At a hash boundary: do { ++k; p *= uniform; } while (p > L && k < 1000), a hash (four uniforms) per block;
-   // block b's fourth factor is the 4b + 4-th, so only block 249 ends at k = 1000.
+   // block b's fourth factor is the 4b + 4-th, so only block 249 ends at k = 1000. Every factor lies in (0, 1), so
+   // the rounded products never increase: when the block's last product is still above L so are the three before
+   // it, and one test per block decides whether the loop goes on. The products are the same roundings in the same
+   // order as one factor at a time.
    for (int blk = 0;; ++blk)
    {
       uint32_t a = u.seed, b = u.frame, c = u.pix, d = u.ctr;
       Pcg4d(a, b, c, d);
       ++u.ctr;
-      const double u0 = UniformOf(a), u1 = UniformOf(b), u2 = UniformOf(c), u3 = UniformOf(d);
-      p *= u0;
-      if (!(p > L))
+      const double p1 = p * UniformOf(a), p2 = p1 * UniformOf(b), p3 = p2 * UniformOf(c), p4 = p3 * UniformOf(d);
+      if (p4 > L && blk != 249)
+      {
+         p = p4;
+         continue;
+      }
+      if (!(p1 > L))
       {
          u.Rest(b, c, d, 1);
          return static_cast<double>(4 * blk);
       }
-      p *= u1;
-      if (!(p > L))
+      if (!(p2 > L))
       {
          u.Rest(c, d, 0u, 2);
          return static_cast<double>(4 * blk + 1);
       }
-      p *= u2;
-      if (!(p > L))
+      if (!(p3 > L))
       {
          u.Rest(d, 0u, 0u, 3);
          return static_cast<double>(4 * blk + 2);
       }
-      p *= u3;
-      if (!(p > L) || blk == 249)
-      {
-         u.k = 4;
-         return static_cast<double>(4 * blk + 3);
-      }
+      u.k = 4;
+      return static_cast<double>(4 * blk + 3);
    }
 }
 
