@@ -536,6 +536,15 @@ int iscu_wf_render(iscu_wf_plan* plan, const float* density, double background, 
 #define ISCU_WF_PASSES 6
 int iscu_wf_set_timing(iscu_wf_plan* plan, int32_t on);
 int iscu_wf_pass_times(iscu_wf_plan* plan, float* ms);
+/* The focus series pipelined across calls (a movie of volumes, or one volume's repeats): _async enqueues a render of
+ * host buffers in I/O slot io_slot (0 .. ISCU_EVENT_IO_SLOTS - 1) -- the volume's H2D on an upload stream, the passes
+ * on the context's stream after it and after everything enqueued before, the frames' D2H on a download stream after
+ * them -- and returns; _wait waits for that slot's frames. One slot's copies run beside another's passes. The host
+ * buffers (page-locked for the copies to overlap) are not touched by the caller until the wait; a slot takes a new
+ * render only after its wait. Arguments as iscu_wf_render. */
+int iscu_wf_render_async(iscu_wf_plan* plan, int32_t io_slot, const float* density, double background,
+                         const iscu_camera* cam, uint32_t seed, uint32_t frame0, float* image, uint16_t* adu);
+int iscu_wf_render_wait(iscu_wf_plan* plan, int32_t io_slot);
 /* The same on device buffers (the camera maps of iscu_set_static apply when their size is nx x ny). */
 int iscu_wf_render_dev(iscu_wf_plan* plan, const float* density_dev, double background, const iscu_camera* cam,
                        uint32_t seed, uint32_t frame0, float* image_dev, uint16_t* adu_dev);

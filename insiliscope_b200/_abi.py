@@ -203,6 +203,9 @@ SIGNATURES = {
     "iscu_wf_set_timing": (C.c_int, [vp, C.c_int32]),
     "iscu_wf_pass_times": (C.c_int, [vp, f32p]),
     "iscu_wf_render": (C.c_int, [vp, vp, C.c_double, C.POINTER(Camera), C.c_uint32, C.c_uint32, vp, vp]),
+    "iscu_wf_render_async": (C.c_int, [vp, C.c_int32, vp, C.c_double, C.POINTER(Camera), C.c_uint32, C.c_uint32,
+                                       vp, vp]),
+    "iscu_wf_render_wait": (C.c_int, [vp, C.c_int32]),
     "iscu_wf_render_dev": (C.c_int, [vp, vp, C.c_double, C.POINTER(Camera), C.c_uint32, C.c_uint32, vp, vp]),
     "iscu_collect_emitters": (C.c_int, [vp, C.c_int32, vp, vp, vp, C.c_int64, C.c_uint32, C.c_uint32, C.c_uint32,
                                         C.c_double, C.c_double, vp, vp, vp, vp, vp, C.c_double, vp, C.c_uint32, vp,

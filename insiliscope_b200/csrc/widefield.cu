@@ -72,6 +72,13 @@ struct iscu_wf_plan
    int logH = 0, logGY = 0, logGZ = 0;
    iscu::LinePlan px, py, pz;
    iscu::DevBuf A, B, Kh, tw, twg, image, adu;
+   // Pipelined renders (iscu_wf_render_async): per I/O slot the volume, the frames and the three stage events.
+   struct Io
+   {
+      bool busy = false;
+      iscu::DevBuf density, image, adu;
+      cudaEvent_t uploaded = nullptr, rendered = nullptr, downloaded = nullptr;
+   } io[ISCU_EVENT_IO_SLOTS];
    // Pass timing (iscu_wf_set_timing): events before XForward and after each of the ISCU_WF_PASSES passes.
    bool timing = false;
    cudaEvent_t ev[ISCU_WF_PASSES + 1] = {};
@@ -1060,6 +1067,13 @@ void iscu_wf_plan_destroy(iscu_wf_plan* plan)
    if (!plan)
       return;
    cudaStreamSynchronize(plan->ctx->stream);
+   for (auto& io : plan->io)
+      for (cudaEvent_t e : {io.uploaded, io.rendered, io.downloaded})
+         if (e)
+         {
+            cudaEventSynchronize(e);
+            cudaEventDestroy(e);
+         }
    for (int i = 0; i <= ISCU_WF_PASSES; ++i)
       if (plan->ev[i])
          cudaEventDestroy(plan->ev[i]);
@@ -1102,6 +1116,74 @@ int iscu_wf_render_dev(iscu_wf_plan* plan, const float* density_dev, double back
    if (rc != ISCU_OK)
       return rc;
    return FinishX(plan, background, cam, seed, frame0, image_dev, adu_dev);
+}
+
+int iscu_wf_render_async(iscu_wf_plan* plan, int32_t io_slot, const float* density, double background,
+                         const iscu_camera* cam, uint32_t seed, uint32_t frame0, float* image, uint16_t* adu)
+{
+   if (!plan || !density || (cam && !adu) || (!cam && !image))
+      return Fail(ISCU_ERR_ARG, "null argument");
+   if (io_slot < 0 || io_slot >= ISCU_EVENT_IO_SLOTS)
+      return Fail(ISCU_ERR_ARG, "I/O slot out of range (0..3)");
+   iscu_ctx* ctx = plan->ctx;
+   std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+   ClearError();
+   auto& io = plan->io[io_slot];
+   if (io.busy)
+      return Fail(ISCU_ERR_STATE, "the I/O slot's render has not been waited for");
+   cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+   ISCU_CK(cudaStreamIsCapturing(ctx->stream, &capturing));
+   if (capturing != cudaStreamCaptureStatusNone)
+      return Fail(ISCU_ERR_STATE, "the pipelined render copies from host memory: not inside a stream capture");
+   if (!ctx->upload)
+      ISCU_CK(cudaStreamCreateWithFlags(&ctx->upload, cudaStreamNonBlocking));
+   if (!ctx->download)
+      ISCU_CK(cudaStreamCreateWithFlags(&ctx->download, cudaStreamNonBlocking));
+   for (cudaEvent_t* e : {&io.uploaded, &io.rendered, &io.downloaded})
+      if (!*e)
+         ISCU_CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+   const size_t n = static_cast<size_t>(plan->nx) * plan->ny * plan->nz;
+   ISCU_CK(io.density.Reserve(n * sizeof(float)));
+   if (image)
+      ISCU_CK(io.image.Reserve(n * sizeof(float)));
+   if (adu)
+      ISCU_CK(io.adu.Reserve(n * sizeof(uint16_t)));
+   // the slot's buffers are free (its last render was waited for), so the upload waits on nothing
+   ISCU_CK(cudaMemcpyAsync(io.density.p, density, n * sizeof(float), cudaMemcpyHostToDevice, ctx->upload));
+   ISCU_CK(cudaEventRecord(io.uploaded, ctx->upload));
+   ISCU_CK(cudaStreamWaitEvent(ctx->stream, io.uploaded, 0));
+   int rc = ConvolveToA(plan, io.density.as<float>());
+   if (rc != ISCU_OK)
+      return rc;
+   rc = FinishX(plan, background, cam, seed, frame0, image ? io.image.as<float>() : nullptr,
+                adu ? io.adu.as<uint16_t>() : nullptr);
+   if (rc != ISCU_OK)
+      return rc;
+   ISCU_CK(cudaEventRecord(io.rendered, ctx->stream));
+   ISCU_CK(cudaStreamWaitEvent(ctx->download, io.rendered, 0));
+   if (image)
+      ISCU_CK(cudaMemcpyAsync(image, io.image.p, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->download));
+   if (adu)
+      ISCU_CK(cudaMemcpyAsync(adu, io.adu.p, n * sizeof(uint16_t), cudaMemcpyDeviceToHost, ctx->download));
+   ISCU_CK(cudaEventRecord(io.downloaded, ctx->download));
+   io.busy = true;
+   return ISCU_OK;
+}
+
+int iscu_wf_render_wait(iscu_wf_plan* plan, int32_t io_slot)
+{
+   if (!plan)
+      return Fail(ISCU_ERR_ARG, "null plan");
+   if (io_slot < 0 || io_slot >= ISCU_EVENT_IO_SLOTS)
+      return Fail(ISCU_ERR_ARG, "I/O slot out of range (0..3)");
+   std::lock_guard<std::recursive_mutex> lock(plan->ctx->mu);
+   ClearError();
+   auto& io = plan->io[io_slot];
+   if (!io.busy)
+      return Fail(ISCU_ERR_STATE, "no render in the I/O slot");
+   io.busy = false;
+   ISCU_CK(cudaEventSynchronize(io.downloaded));
+   return ISCU_OK;
 }
 
 int iscu_wf_render(iscu_wf_plan* plan, const float* density, double background, const iscu_camera* cam,

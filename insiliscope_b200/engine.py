@@ -646,6 +646,7 @@ class WidefieldPlan:
         h = C.c_void_p()
         check(self.lib.iscu_wf_plan_create(engine.h, nx, ny, nz, _ptr(psf), kx, ky, kz, C.byref(h)))
         self.h = h
+        self._pending_io = {}   # I/O slot -> the host arrays of its enqueued render
         engine._plans.add(self)
 
     def close(self):
@@ -706,6 +707,29 @@ class WidefieldPlan:
                                       C.byref(cam) if cam is not None else None, seed, frame0,
                                       _ptr(image) if want_image else None, _ptr(adu) if cam is not None else None))
         return (image if want_image else None), (adu if camera is not None else None)
+
+    def render_async(self, io_slot, density, background, camera: CameraParams | None, seed, frame0=0, adu=None,
+                     image=None):
+        """Enqueues render() in I/O slot io_slot (0..3) and returns at once (iscu_wf_render_async): the volume's
+        upload, the passes and the frames' download run behind the calls before it. density, adu and image are
+        caller-owned contiguous arrays (page-locked for the copies to overlap) that stay untouched until
+        render_wait(io_slot)."""
+        if density.dtype != np.float32 or not density.flags.c_contiguous or density.shape != self.shape:
+            raise ValueError("density: a C-contiguous float32 array of the plan's shape")
+        for name, arr, dt in (("adu", adu, np.uint16), ("image", image, np.float32)):
+            if arr is not None and (arr.dtype != dt or not arr.flags.c_contiguous or arr.shape != self.shape):
+                raise ValueError(f"{name}: a C-contiguous {np.dtype(dt).name} array of the plan's shape")
+        cam = camera.c() if camera is not None else None
+        check(self.lib.iscu_wf_render_async(self.h, int(io_slot), _ptr(density), float(background),
+                                            C.byref(cam) if cam is not None else None, seed, frame0,
+                                            _ptr(image) if image is not None else None,
+                                            _ptr(adu) if adu is not None else None))
+        self._pending_io[int(io_slot)] = (density, adu, image)   # held only once enqueued
+
+    def render_wait(self, io_slot):
+        """Waits for I/O slot io_slot's frames (iscu_wf_render_wait)."""
+        check(self.lib.iscu_wf_render_wait(self.h, int(io_slot)))
+        self._pending_io.pop(int(io_slot), None)
 
 
 @dataclass

@@ -88,3 +88,12 @@ def test_backend_argument_checks_without_device(lib):
     assert lib.iscu_buffer_copy(None, None, 0) == _abi.ISCU_ERR_ARG
     assert lib.iscu_dispatch(None, b"wf_clear", None, 0, None, 0, 1, 1, 1) == _abi.ISCU_ERR_ARG
     lib.iscu_buffer_destroy(None)
+
+
+def test_widefield_pipeline_argument_checks_without_device(lib):
+    """The pipelined focus-series calls refuse a null plan, null buffers and slots out of range before any device
+    work."""
+    from insiliscope_b200 import _abi
+    assert lib.iscu_wf_render_async(None, 0, None, 0.0, None, 0, 0, None, None) == _abi.ISCU_ERR_ARG
+    assert lib.iscu_wf_render_wait(None, 0) == _abi.ISCU_ERR_ARG
+    assert b"null" in lib.iscu_last_error()

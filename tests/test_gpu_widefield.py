@@ -32,6 +32,39 @@ def test_convolution_vs_oracle(engine, vol_shape, psf_shape):
     plan.close()
 
 
+def test_pipelined_renders_equal_blocking(engine):
+    """Four focus series through three I/O slots (render_async / render_wait, copies beside the passes of the next
+    series) give the blocking render's frames bit for bit, each with its own frame numbers."""
+    import torch
+    rng = np.random.default_rng(11)
+    nz, ny, nx = 8, 40, 48
+    psf = rng.random((6, 9, 11)).astype(np.float32)
+    psf /= psf.sum()
+    vols = [(rng.random((nz, ny, nx)) * 40).astype(np.float32) for _ in range(4)]
+    cam = CameraParams(quantum_efficiency=1.0, gain=1.0, read_noise_e=50.0, emccd=True, em_gain=300.0,
+                       cic_electrons=0.002, bit_depth=16)
+    engine.set_static(nx, ny, offset=np.full(nx * ny, 100.0, np.float32))
+    plan = WidefieldPlan(engine, (nz, ny, nx), psf)
+    want = [plan.render(v, 5.0, cam, 31, frame0=nz * i)[1] for i, v in enumerate(vols)]
+    pinned = [torch.from_numpy(v).pin_memory().numpy() for v in vols]
+    outs = [torch.empty((nz, ny, nx), dtype=torch.uint16).pin_memory().numpy() for _ in range(3)]
+    got = [None] * 4
+    for i in range(4):
+        io = i % 3
+        if i >= 3:
+            plan.render_wait(io)
+            got[i - 3] = outs[io].copy()
+        plan.render_async(io, pinned[i], 5.0, cam, 31, frame0=nz * i, adu=outs[io])
+    for i in range(1, 4):
+        plan.render_wait(i % 3)
+        got[i] = outs[i % 3].copy()
+    for i in range(4):
+        assert np.array_equal(got[i], want[i]), i
+    with pytest.raises(Exception):
+        plan.render_wait(0)   # nothing enqueued in the slot any more
+    plan.close()
+
+
 def test_render_noise_bit_exact_on_image(engine, oracle):
     """The frames' ADU are ApplyNoiseChain (EMCCD) of the expected image, frame = frame0 + plane, with the camera
     offset map: bit for bit the oracle's chain on the GPU's own expected image."""
