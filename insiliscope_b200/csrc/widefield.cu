@@ -50,8 +50,8 @@ namespace iscu {
 struct LinePlan
 {
    int logN = 0, groups = 0;
-   int r[3] = {0, 0, 0};
-   int tw[3] = {-1, -1, -1};
+   int r[4] = {0, 0, 0, 0};
+   int tw[4] = {-1, -1, -1, -1};
 };
 
 __host__ __device__ inline int LogQ(const LinePlan& P, int g)
@@ -60,6 +60,51 @@ __host__ __device__ inline int LogQ(const LinePlan& P, int g)
    for (int i = 0; i <= g; ++i)
       s += P.r[i];
    return P.logN - s;
+}
+
+// Group sizes for an N = 2^logN point transform: one group up to 32 points; else groups of 2^3..2^5. Rows: the
+// last (span-1) group at least 16 points, so that every group but the last has a smallest span q >= 16 (the padded
+// row layout is conflict-free for those). Columns (lanes walk the lines, any q is conflict-free): the larger group
+// first, for more loads in flight per thread where group 0 reads global memory.
+__host__ __device__ constexpr LinePlan MakeLinePlan(int logN, bool cols)
+{
+   LinePlan P;
+   P.logN = logN;
+   if (logN <= 5)
+   {
+      P.groups = 1;
+      P.r[0] = logN;
+   }
+   else if (logN <= 10)
+   {
+      P.groups = 2;
+      if (cols)
+         P.r[0] = (logN + 1) / 2 < 5 ? (logN + 1) / 2 : 5;
+      else
+         P.r[0] = logN - (logN >= 9 ? logN - 5 : 4);
+      P.r[1] = logN - P.r[0];
+   }
+   else
+   {
+      P.groups = 3;
+      P.r[1] = 4;
+      P.r[2] = 4;
+      P.r[0] = logN - 8;
+   }
+   return P;
+}
+
+// Assigns the tables of the groups with q > 1 at `offset` (float2 entries) onwards; returns the entries used.
+// The z pass's plan: groups of at most 16 points, the smaller group first (it reads the zero-padded half).
+__host__ __device__ constexpr LinePlan MakeZPlan(int logN)
+{
+   LinePlan P;
+   P.logN = logN;
+   P.groups = (logN + 3) / 4;
+   for (int g = 1; g < P.groups; ++g)
+      P.r[g] = 4;
+   P.r[0] = logN - 4 * (P.groups - 1);
+   return P;
 }
 
 } // namespace iscu
@@ -97,6 +142,11 @@ namespace {
 #ifndef ISCU_WF_MIN_CTAS
 #define ISCU_WF_MIN_CTAS 2
 #endif
+// Stage buffers of the z pass: 2 = persistent CTAs copying the next column block in while transforming one; 1 = a
+// CTA per column block.
+#ifndef ISCU_WF_Z_STAGES
+#define ISCU_WF_Z_STAGES 1
+#endif
 constexpr int kThreads = 256;
 constexpr int kMinCtas = ISCU_WF_MIN_CTAS;
 constexpr size_t kSmemBudget = 100 * 1024;   // lines per CTA are sized to this
@@ -117,7 +167,16 @@ __device__ __forceinline__ void CopyAsync8(float2* dst, const float2* src)
                 "l"(src)
                 : "memory");
 }
+__device__ __forceinline__ void CopyAsync16(float2* dst, const float2* src)
+{
+   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(dst))),
+                "l"(src)
+                : "memory");
+}
 __device__ __forceinline__ void CopyAsyncWait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+__device__ __forceinline__ void CopyAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// Waits for all of this thread's copy groups but the most recently committed one.
+__device__ __forceinline__ void CopyAsyncWaitPrior() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 __device__ __forceinline__ int Rev(int n, int logN) { return static_cast<int>(__brev(static_cast<unsigned>(n)) >> (32 - logN)); }
 
@@ -247,7 +306,7 @@ struct ColAddr
 // group (conjugate twiddles, then the DIT DFT). Rows: lanes walk the tasks of a line; columns: lanes walk the lines
 // (BL of them, a power of two; lines >= nb are skipped).
 template <int R, bool kInv, bool kCols, class Addr>
-__device__ void SmemGroup(const Addr& S, int nb, int BL, int logBL, int logN, int logQ, const float2* __restrict__ tw)
+__device__ __forceinline__ void SmemGroup(const Addr& S, int nb, int BL, int logBL, int logN, int logQ, const float2* __restrict__ tw)
 {
    constexpr int r = Log2i(R);
    const int logT = logN - r, q = 1 << logQ;
@@ -300,14 +359,45 @@ __device__ void SmemGroup(const Addr& S, int nb, int BL, int logBL, int logN, in
    default: { constexpr int R = 32; __VA_ARGS__; } break;                                                              \
    }
 
+// The z pass runs groups of at most 16 points (its plans keep r <= 4), so its kernels carry no 32-point code.
+#define ISCU_RADIX_SWITCH16(r, ...)                                                                                     \
+   switch (r)                                                                                                          \
+   {                                                                                                                   \
+   case 1: { constexpr int R = 2; __VA_ARGS__; } break;                                                                \
+   case 2: { constexpr int R = 4; __VA_ARGS__; } break;                                                                \
+   case 3: { constexpr int R = 8; __VA_ARGS__; } break;                                                                \
+   default: { constexpr int R = 16; __VA_ARGS__; } break;                                                              \
+   }
+
 __device__ __forceinline__ const float2* GroupTw(const LinePlan& P, const float2* twg, int g)
 {
    return P.tw[g] >= 0 ? twg + P.tw[g] : nullptr;
 }
 
+// The plan a pass runs: for a codelet (kLogN > 0) the compile-time plan of that length -- every span, pad and index
+// shift then folds into the instructions -- with the runtime plan's table offsets; else the runtime plan.
+// kKind: 0 rows (y), 1 columns (x), 2 the z pass.
+template <int kLogN, int kKind>
+__device__ __forceinline__ LinePlan Fixed(const LinePlan& runtime)
+{
+   if constexpr (kLogN == 0)
+      return runtime;
+   else
+   {
+      constexpr LinePlan C = kKind == 2 ? MakeZPlan(kLogN) : MakeLinePlan(kLogN, kKind == 1);
+      LinePlan P = runtime;
+      P.logN = C.logN;
+      P.groups = C.groups;
+#pragma unroll
+      for (int g = 0; g < 4; ++g)
+         P.r[g] = C.r[g];
+      return P;
+   }
+}
+
 // Forward groups 1 .. groups-1 of lines already in shared memory (group 0 done by the pass's loader).
 template <bool kCols, class Addr>
-__device__ void ForwardRest(const LinePlan& P, const float2* twg, const Addr& S, int nb, int BL, int logBL)
+__device__ __forceinline__ void ForwardRest(const LinePlan& P, const float2* twg, const Addr& S, int nb, int BL, int logBL)
 {
    for (int g = 1; g < P.groups; ++g)
    {
@@ -318,16 +408,19 @@ __device__ void ForwardRest(const LinePlan& P, const float2* twg, const Addr& S,
    }
 }
 
-// Inverse groups groups-1 .. first (down to group `first`) of lines in shared memory.
-template <bool kCols, class Addr>
-__device__ void InverseRest(const LinePlan& P, const float2* twg, const Addr& S, int nb, int BL, int logBL, int last,
+// Inverse groups last .. first of lines in shared memory (kMax16: plans of groups of at most 16 points).
+template <bool kCols, bool kMax16 = false, class Addr>
+__device__ __forceinline__ void InverseRest(const LinePlan& P, const float2* twg, const Addr& S, int nb, int BL, int logBL, int last,
                             int first)
 {
    for (int g = last; g >= first; --g)
    {
       const int logQ = LogQ(P, g);
       const float2* tw = GroupTw(P, twg, g);
-      ISCU_RADIX_SWITCH(P.r[g], (SmemGroup<R, true, kCols>(S, nb, BL, logBL, P.logN, logQ, tw)));
+      if (kMax16)
+         ISCU_RADIX_SWITCH16(P.r[g], (SmemGroup<R, true, kCols>(S, nb, BL, logBL, P.logN, logQ, tw)))
+      else
+         ISCU_RADIX_SWITCH(P.r[g], (SmemGroup<R, true, kCols>(S, nb, BL, logBL, P.logN, logQ, tw)))
       __syncthreads();
    }
 }
@@ -343,7 +436,7 @@ struct Dims
 // X forward group 0: packed pairs z[n] = x[2n] + i x[2n+1] of row b straight from global memory (lanes walk j, so
 // the loads coalesce), DIF group, twiddles, into the column layout.
 template <int R, bool kHalf>
-__device__ void XFirst(const ColAddr& S, const float* __restrict__ src, int nxv, int nb, int logQ,
+__device__ __forceinline__ void XFirst(const ColAddr& S, const float* __restrict__ src, int nxv, int nb, int logQ,
                        const float2* __restrict__ tw, bool pairs)
 {
    const int q = 1 << logQ, total = nb << logQ;
@@ -371,17 +464,18 @@ __device__ void XFirst(const ColAddr& S, const float* __restrict__ src, int nxv,
 }
 
 // Rows of `in` (nzv x nyv x nxv) -> A[z][k][y], k <= H, y < nyv. grid (ceil(nyv / BY), nzv); BY a power of two;
-// smem H * (BY + 1) float2.
+// smem H * (BY + 1) float2. kLogH: the codelet's log2 H (0: any H).
+template <int kLogH>
 __global__ void __launch_bounds__(kThreads, kMinCtas) XForwardKernel(const float* __restrict__ in, Dims d, int BY, int logBY,
                                                            const float2* __restrict__ tw, const float2* __restrict__ twg,
                                                            float2* __restrict__ A)
 {
    extern __shared__ float2 s[];
+   const LinePlan P = Fixed<kLogH, 1>(d.px);
    const int z = blockIdx.y, y0 = blockIdx.x * BY;
-   const int nb = min(BY, d.nyv - y0), H = d.H;
+   const int nb = min(BY, d.nyv - y0), H = 1 << P.logN, logH = P.logN;
    const ColAddr S{s, BY + 1};
    const float* src = in + (static_cast<size_t>(z) * d.nyv + y0) * d.nxv;
-   const LinePlan& P = d.px;
    const bool pairs = (d.nxv & 1) == 0 && (reinterpret_cast<uintptr_t>(in) & 7) == 0;
    const int logQ0 = LogQ(P, 0);
    const float2* tw0 = GroupTw(P, twg, 0);
@@ -397,8 +491,8 @@ __global__ void __launch_bounds__(kThreads, kMinCtas) XForwardKernel(const float
       const int k = t >> logBY, b = t & (BY - 1);
       if (b >= nb)
          continue;
-      const float2 zk = S(b, Rev(k & (H - 1), d.logH));
-      const float2 zm = Conj(S(b, Rev((H - k) & (H - 1), d.logH)));
+      const float2 zk = S(b, Rev(k & (H - 1), logH));
+      const float2 zm = Conj(S(b, Rev((H - k) & (H - 1), logH)));
       const float2 e = Cadd(zk, zm), o = Csub(zk, zm);
       const float2 w = __ldg(tw + (k << (d.logG - d.logGX)));
       const float2 wo = Cmul(w, o);   // then times -i: (x, y) -> (y, -x)
@@ -409,7 +503,7 @@ __global__ void __launch_bounds__(kThreads, kMinCtas) XForwardKernel(const float
 
 // Y forward group 0: rows of A (nyv values, zero beyond) straight from global memory, lanes walking j.
 template <int R, bool kHalf>
-__device__ void YFirst(const RowAddr& S, const float2* __restrict__ rows, int nyv, int nb, int logQ,
+__device__ __forceinline__ void YFirst(const RowAddr& S, const float2* __restrict__ rows, int nyv, int nb, int logQ,
                        const float2* __restrict__ tw)
 {
    const int q = 1 << logQ, total = nb << logQ;
@@ -440,12 +534,14 @@ __device__ __forceinline__ RowAddr RowsOf(float2* s, const LinePlan& P)
 }
 
 // A rows (nyv values per (z, k)) -> B[z][k][p], p = bit-reversed ky. grid (ceil(NK / BK), nzv); smem BK rows.
+// kLogN: the codelet's log2 GY (0: any GY).
+template <int kLogN>
 __global__ void __launch_bounds__(kThreads, kMinCtas) YForwardKernel(const float2* __restrict__ A, Dims d, int BK,
                                                            const float2* __restrict__ twg, float2* __restrict__ B)
 {
    extern __shared__ float2 s[];
-   const int z = blockIdx.y, k0 = blockIdx.x * BK, nb = min(BK, d.NK - k0), N = d.GY;
-   const LinePlan& P = d.py;
+   const LinePlan P = Fixed<kLogN, 0>(d.py);
+   const int z = blockIdx.y, k0 = blockIdx.x * BK, nb = min(BK, d.NK - k0), N = 1 << P.logN;
    const RowAddr S = RowsOf(s, P);
    const float2* rows = A + (static_cast<size_t>(z) * d.NK + k0) * d.nyv;
    const int logQ0 = LogQ(P, 0);
@@ -459,14 +555,14 @@ __global__ void __launch_bounds__(kThreads, kMinCtas) YForwardKernel(const float
    float2* out = B + (static_cast<size_t>(z) * d.NK + k0) * N;
    for (int t = threadIdx.x; t < nb * N; t += blockDim.x)
    {
-      const int b = t >> d.logGY, p = t & (N - 1);
+      const int b = t >> P.logN, p = t & (N - 1);
       out[static_cast<size_t>(b) * N + p] = S(b, p);
    }
 }
 
 // Y inverse group 0: conjugate twiddles, DIT, natural order out; rows [oy, oy + nyv) to global memory.
 template <int R>
-__device__ void YLast(const RowAddr& S, float2* __restrict__ rows, int nyv, int oy, int nb, int logQ,
+__device__ __forceinline__ void YLast(const RowAddr& S, float2* __restrict__ rows, int nyv, int oy, int nb, int logQ,
                       const float2* __restrict__ tw)
 {
    const int q = 1 << logQ, total = nb << logQ;
@@ -492,16 +588,17 @@ __device__ void YLast(const RowAddr& S, float2* __restrict__ rows, int nyv, int 
 }
 
 // B rows (bit-reversed ky) -> inverse GY-point FFT -> rows [oy, oy + nyv) into A[z][k][y]. grid (ceil(NK / BK), nzv).
+template <int kLogN>
 __global__ void __launch_bounds__(kThreads, kMinCtas) YInverseKernel(const float2* __restrict__ B, Dims d, int BK, int oy,
                                                            const float2* __restrict__ twg, float2* __restrict__ A)
 {
    extern __shared__ float2 s[];
-   const int z = blockIdx.y, k0 = blockIdx.x * BK, nb = min(BK, d.NK - k0), N = d.GY;
-   const LinePlan& P = d.py;
+   const LinePlan P = Fixed<kLogN, 0>(d.py);
+   const int z = blockIdx.y, k0 = blockIdx.x * BK, nb = min(BK, d.NK - k0), N = 1 << P.logN;
    const RowAddr S = RowsOf(s, P);
    const float2* in = B + (static_cast<size_t>(z) * d.NK + k0) * N;
    for (int t = threadIdx.x; t < nb * N; t += blockDim.x)
-      CopyAsync8(&S(t >> d.logGY, t & (N - 1)), in + t);
+      CopyAsync8(&S(t >> P.logN, t & (N - 1)), in + t);
    CopyAsyncWait();
    __syncthreads();
    InverseRest<false>(P, twg, S, nb, 1, 0, P.groups - 1, 1);
@@ -509,10 +606,53 @@ __global__ void __launch_bounds__(kThreads, kMinCtas) YInverseKernel(const float
    ISCU_RADIX_SWITCH(P.r[0], (YLast<R>(S, rows, d.nyv, oy, nb, LogQ(P, 0), GroupTw(P, twg, 0))));
 }
 
-// Z forward group 0: columns straight from global memory (lanes walk the columns), DIF group, twiddles.
+// The asynchronous copies of one block of columns into a stage buffer: B's nzv planes at in[n BZ + b] and, when
+// convolving, the PSF spectrum's GZ planes after them. 16-byte copies of column pairs (nb is even whenever BZ >= 2:
+// GY and BZ are powers of two, GY >= 4), else 8-byte ones.
+template <bool kConvolve>
+__device__ __forceinline__ void ZPrefetch(const float2* __restrict__ B, const float2* __restrict__ Kh, size_t plane, size_t col,
+                          int nzv, int GZ, int nb, int BZ, int logBZ, float2* in)
+{
+   float2* ks = in + (static_cast<size_t>(nzv) << logBZ);
+   if ((nb & 1) == 0)
+   {
+      const int logPairs = logBZ - 1, pairs = BZ >> 1;
+      for (int t = threadIdx.x; t < (nzv << logPairs); t += blockDim.x)
+      {
+         const int n = t >> logPairs, b = (t & (pairs - 1)) << 1;
+         if (b < nb)
+            CopyAsync16(in + (n << logBZ) + b, B + n * plane + col + b);
+      }
+      if (kConvolve)
+         for (int t = threadIdx.x; t < (GZ << logPairs); t += blockDim.x)
+         {
+            const int n = t >> logPairs, b = (t & (pairs - 1)) << 1;
+            if (b < nb)
+               CopyAsync16(ks + (n << logBZ) + b, Kh + n * plane + col + b);
+         }
+   }
+   else
+   {
+      for (int t = threadIdx.x; t < (nzv << logBZ); t += blockDim.x)
+      {
+         const int n = t >> logBZ, b = t & (BZ - 1);
+         if (b < nb)
+            CopyAsync8(in + t, B + n * plane + col + b);
+      }
+      if (kConvolve)
+         for (int t = threadIdx.x; t < (GZ << logBZ); t += blockDim.x)
+         {
+            const int n = t >> logBZ, b = t & (BZ - 1);
+            if (b < nb)
+               CopyAsync8(ks + t, Kh + n * plane + col + b);
+         }
+   }
+}
+
+// Z forward group 0: the block's columns from its stage buffer (lanes walk the columns), DIF group, twiddles.
 template <int R, bool kHalf>
-__device__ void ZFirst(const ColAddr& S, const float2* __restrict__ B, size_t plane, size_t col, int nzv, int nb,
-                       int BL, int logBL, int logQ, const float2* __restrict__ tw)
+__device__ __forceinline__ void ZFirst(const ColAddr& S, const float2* in, int nzv, int nb, int BL, int logBL, int logQ,
+                       const float2* __restrict__ tw)
 {
    const int q = 1 << logQ, total = BL << logQ;
    for (int t = threadIdx.x; t < total; t += blockDim.x)
@@ -525,7 +665,7 @@ __device__ void ZFirst(const ColAddr& S, const float2* __restrict__ B, size_t pl
       for (int m = 0; m < (kHalf ? R / 2 : R); ++m)
       {
          const int n = j + m * q;
-         v[m] = n < nzv ? __ldg(B + n * plane + col + b) : make_float2(0.f, 0.f);
+         v[m] = n < nzv ? in[(n << logBL) + b] : make_float2(0.f, 0.f);
       }
       DifReg<R, false, kHalf>(v);
       if (tw)
@@ -540,7 +680,7 @@ __device__ void ZFirst(const ColAddr& S, const float2* __restrict__ B, size_t pl
 // spectrum out to Kh (kConvolve false) or times the PSF spectrum (KS: this CTA's columns of Kh, prefetched into
 // shared memory) and the first inverse group, back into shared memory.
 template <int R, bool kConvolve>
-__device__ void ZTurn(const ColAddr& S, const float2* KS, float2* __restrict__ Kh, size_t plane, size_t col, int nb,
+__device__ __forceinline__ void ZTurn(const ColAddr& S, const float2* KS, float2* __restrict__ Kh, size_t plane, size_t col, int nb,
                       int BL, int logBL, int logN, bool dif, bool dit)
 {
    constexpr int r = Log2i(R);
@@ -579,7 +719,7 @@ __device__ void ZTurn(const ColAddr& S, const float2* KS, float2* __restrict__ K
 // Z inverse group 0: conjugate twiddles, DIT (skipped when group 0 was the only one, ZTurn did it), planes
 // [oz, oz + nzv) to global memory.
 template <int R>
-__device__ void ZLast(const ColAddr& S, float2* __restrict__ B, size_t plane, size_t col, int nzv, int oz, int nb,
+__device__ __forceinline__ void ZLast(const ColAddr& S, float2* __restrict__ B, size_t plane, size_t col, int nzv, int oz, int nb,
                       int BL, int logBL, int logQ, const float2* __restrict__ tw, bool dit)
 {
    const int q = 1 << logQ, total = BL << logQ;
@@ -609,59 +749,91 @@ __device__ void ZLast(const ColAddr& S, float2* __restrict__ B, size_t plane, si
 }
 
 // Columns along z of B (nzv planes) -> GZ-point forward FFT -> either the PSF spectrum Kh[pz][k][p] (all GZ planes,
-// forward only) or, times Kh, the inverse FFT cropped to planes [oz, oz + nzv) back into B.
-// grid (ceil(GY / BZ), NK), BZ a power of two; smem GZ * BZ float2, column layout (twice that when convolving: the
-// PSF spectrum's columns are copied in asynchronously while group 0 loads and transforms B).
-template <bool kConvolve>
-__global__ void __launch_bounds__(kThreads, kMinCtas) ZKernel(float2* __restrict__ B, Dims d, int BZ, int logBZ, int oz,
-                                                    const float2* __restrict__ twg, float2* __restrict__ Kh)
+// forward only) or, times Kh, the inverse FFT cropped to planes [oz, oz + nzv) back into B. Persistent: CTA c takes
+// column blocks c, c + gridDim.x, ... (block blk: k = blk / blocksPerK, columns from p0 = (blk % blocksPerK) BZ),
+// and with stages = 2 the next block's B planes and PSF spectrum are copied into shared memory while this one is
+// transformed (stages = 1 where two stage buffers do not fit: the copies then follow the block). BZ a power of two;
+// smem (GZ + stages (nzv + GZ when convolving)) BZ float2, column layout.
+template <bool kConvolve, int kLogN>
+__global__ void __launch_bounds__(kThreads, kMinCtas) ZKernel(float2* __restrict__ B, Dims d, int BZ, int logBZ,
+                                                              int blocksPerK, int nBlocks, int stages, int oz,
+                                                              const float2* __restrict__ twg, float2* __restrict__ Kh)
 {
    extern __shared__ float2 s[];
-   const int k = blockIdx.y, p0 = blockIdx.x * BZ, nb = min(BZ, d.GY - p0);
    const size_t plane = static_cast<size_t>(d.NK) * d.GY;
-   const size_t col = static_cast<size_t>(k) * d.GY + p0;
-   const LinePlan& P = d.pz;
+   const LinePlan P = Fixed<kLogN, 2>(d.pz);
+   const int GZ = 1 << P.logN;
    const ColAddr S{s, BZ};
-   float2* KS = s + (static_cast<size_t>(d.GZ) << logBZ);
-   if (kConvolve)
-      for (int t = threadIdx.x; t < (d.GZ << logBZ); t += blockDim.x)
-      {
-         const int b = t & (BZ - 1), n = t >> logBZ;
-         if (b < nb)
-            CopyAsync8(KS + t, Kh + n * plane + col + b);
-      }
+   const size_t stageElems = static_cast<size_t>(d.nzv + (kConvolve ? GZ : 0)) << logBZ;
+   float2* stage0 = s + (static_cast<size_t>(GZ) << logBZ);
    const int logQ0 = LogQ(P, 0);
    const float2* tw0 = GroupTw(P, twg, 0);
-   if (2 * d.nzv <= (1 << P.logN))
-      ISCU_RADIX_SWITCH(P.r[0], (ZFirst<R, true>(S, B, plane, col, d.nzv, nb, BZ, logBZ, logQ0, tw0)))
-   else
-      ISCU_RADIX_SWITCH(P.r[0], (ZFirst<R, false>(S, B, plane, col, d.nzv, nb, BZ, logBZ, logQ0, tw0)))
-   __syncthreads();
-   for (int g = 1; g < P.groups - 1; ++g)
+   const bool half = 2 * d.nzv <= (1 << P.logN), single = P.groups == 1;
+   auto colOf = [&](int blk, int& nb) {
+      const int k = blk / blocksPerK, p0 = (blk - k * blocksPerK) << logBZ;
+      nb = min(BZ, d.GY - p0);
+      return static_cast<size_t>(k) * d.GY + p0;
+   };
+   int blk = blockIdx.x;
+   if (blk < nBlocks)
    {
-      ISCU_RADIX_SWITCH(P.r[g], (SmemGroup<R, false, true>(S, nb, BZ, logBZ, P.logN, LogQ(P, g), GroupTw(P, twg, g))));
-      __syncthreads();
+      int nb;
+      const size_t col = colOf(blk, nb);
+      ZPrefetch<kConvolve>(B, Kh, plane, col, d.nzv, GZ, nb, BZ, logBZ, stage0);
    }
-   const bool single = P.groups == 1;
-   if (kConvolve)
+   CopyAsyncCommit();
+   for (int i = 0; blk < nBlocks; ++i, blk += gridDim.x)
    {
-      CopyAsyncWait();
+      const int buf = stages == 2 ? (i & 1) : 0, next = blk + gridDim.x;
+      if (stages == 2 && next < nBlocks)
+      {
+         int nbn;
+         const size_t coln = colOf(next, nbn);
+         ZPrefetch<kConvolve>(B, Kh, plane, coln, d.nzv, GZ, nbn, BZ, logBZ, stage0 + (buf ^ 1) * stageElems);
+      }
+      CopyAsyncCommit();
+      CopyAsyncWaitPrior();   // this block's copies (the group before the one just committed)
       __syncthreads();
+      int nb;
+      const size_t col = colOf(blk, nb);
+      const float2* in = stage0 + buf * stageElems;
+      const float2* KS = in + (static_cast<size_t>(d.nzv) << logBZ);
+      if (half)
+         ISCU_RADIX_SWITCH16(P.r[0], (ZFirst<R, true>(S, in, d.nzv, nb, BZ, logBZ, logQ0, tw0)))
+      else
+         ISCU_RADIX_SWITCH16(P.r[0], (ZFirst<R, false>(S, in, d.nzv, nb, BZ, logBZ, logQ0, tw0)))
+      __syncthreads();
+      for (int g = 1; g < P.groups - 1; ++g)
+      {
+         ISCU_RADIX_SWITCH16(P.r[g],
+                           (SmemGroup<R, false, true>(S, nb, BZ, logBZ, P.logN, LogQ(P, g), GroupTw(P, twg, g))));
+         __syncthreads();
+      }
+      ISCU_RADIX_SWITCH16(P.r[P.groups - 1],
+                        (ZTurn<R, kConvolve>(S, KS, Kh, plane, col, nb, BZ, logBZ, P.logN, !single, true)));
+      if (kConvolve)
+      {
+         __syncthreads();
+         if (!single)
+            InverseRest<true, true>(P, twg, S, nb, BZ, logBZ, P.groups - 2, 1);
+         ISCU_RADIX_SWITCH16(P.r[0], (ZLast<R>(S, B, plane, col, d.nzv, oz, nb, BZ, logBZ, logQ0, tw0, !single)));
+      }
+      __syncthreads();   // the block's shared memory (S and its stage buffer) is free again
+      if (stages == 1 && next < nBlocks)
+      {
+         int nbn;
+         const size_t coln = colOf(next, nbn);
+         ZPrefetch<kConvolve>(B, Kh, plane, coln, d.nzv, GZ, nbn, BZ, logBZ, stage0);
+         CopyAsyncCommit();
+      }
    }
-   ISCU_RADIX_SWITCH(P.r[P.groups - 1],
-                     (ZTurn<R, kConvolve>(S, KS, Kh, plane, col, nb, BZ, logBZ, P.logN, !single, true)));
-   if (!kConvolve)
-      return;
-   __syncthreads();
-   if (!single)
-      InverseRest<true>(P, twg, S, nb, BZ, logBZ, P.groups - 2, 1);
-   ISCU_RADIX_SWITCH(P.r[0], (ZLast<R>(S, B, plane, col, d.nzv, oz, nb, BZ, logBZ, logQ0, tw0, !single)));
+   CopyAsyncWait();
 }
 
 // X inverse, the last DIF group's inverse (span 1, no twiddles) straight from A: Z'[k] = (X[k] + conj X[H-k]) +
 // i W_GX^-k (X[k] - conj X[H-k]) at bit-reversed slots, lanes walking the rows.
 template <int R>
-__device__ void XLoad(const ColAddr& S, const float2* __restrict__ Az, int nyv, int y0, int nb, int BL, int logBL,
+__device__ __forceinline__ void XLoad(const ColAddr& S, const float2* __restrict__ Az, int nyv, int y0, int nb, int BL, int logBL,
                       int H, int logH, const float2* __restrict__ tw, int twShift)
 {
    constexpr int r = Log2i(R);
@@ -691,6 +863,7 @@ __device__ void XLoad(const ColAddr& S, const float2* __restrict__ Az, int nyv, 
 
 // A (half spectrum along x, per (z, y)) -> GX reals -> columns [ox, ox + nxv), scaled, max(0, .) + background ->
 // the photon frames. grid (ceil(nyv / BY), nzv), BY a power of two; smem H * (BY + 1) float2.
+template <int kLogH>
 __global__ void __launch_bounds__(kThreads, kMinCtas) XInverseKernel(const float2* __restrict__ A, Dims d, int BY,
                                                                      int logBY, int ox, float scale, float background,
                                                                      const float2* __restrict__ tw,
@@ -698,12 +871,12 @@ __global__ void __launch_bounds__(kThreads, kMinCtas) XInverseKernel(const float
                                                                      float* __restrict__ image)
 {
    extern __shared__ float2 s[];
-   const int z = blockIdx.y, y0 = blockIdx.x * BY, nb = min(BY, d.nyv - y0), H = d.H;
-   const LinePlan& P = d.px;
+   const LinePlan P = Fixed<kLogH, 1>(d.px);
+   const int z = blockIdx.y, y0 = blockIdx.x * BY, nb = min(BY, d.nyv - y0), H = 1 << P.logN;
    const ColAddr S{s, BY + 1};
    const float2* Az = A + static_cast<size_t>(z) * d.NK * d.nyv;
    ISCU_RADIX_SWITCH(P.r[P.groups - 1],
-                     (XLoad<R>(S, Az, d.nyv, y0, nb, BY, logBY, H, d.logH, tw, d.logG - d.logGX)));
+                     (XLoad<R>(S, Az, d.nyv, y0, nb, BY, logBY, H, P.logN, tw, d.logG - d.logGX)));
    __syncthreads();
    InverseRest<true>(P, twg, S, nb, BY, logBY, P.groups - 2, 0);
    float* out = image + (static_cast<size_t>(z) * d.nyv + y0) * d.nxv;
@@ -770,39 +943,6 @@ uint32_t Pow2AtLeast(uint32_t v)
    return p;
 }
 
-// Group sizes for an N = 2^logN point transform: one group up to 32 points; else groups of 2^3..2^5. Rows: the
-// last (span-1) group at least 16 points, so that every group but the last has a smallest span q >= 16 (the padded
-// row layout is conflict-free for those). Columns (lanes walk the lines, any q is conflict-free): the larger group
-// first, for more loads in flight per thread where group 0 reads global memory.
-LinePlan MakeLinePlan(int logN, bool cols)
-{
-   LinePlan P;
-   P.logN = logN;
-   if (logN <= 5)
-   {
-      P.groups = 1;
-      P.r[0] = logN;
-   }
-   else if (logN <= 10)
-   {
-      P.groups = 2;
-      if (cols)
-         P.r[0] = std::min(5, (logN + 1) / 2);
-      else
-         P.r[0] = logN - (logN >= 9 ? logN - 5 : 4);
-      P.r[1] = logN - P.r[0];
-   }
-   else
-   {
-      P.groups = 3;
-      P.r[1] = 4;
-      P.r[2] = 4;
-      P.r[0] = logN - 8;
-   }
-   return P;
-}
-
-// Assigns the tables of the groups with q > 1 at `offset` (float2 entries) onwards; returns the entries used.
 int PlaceTables(LinePlan& P, int offset)
 {
    int used = 0;
@@ -838,7 +978,35 @@ int YLines(const LinePlan& P)
    const int N = 1 << P.logN;
    return std::max<int>(1, std::min<int>(std::max(1, 8192 / N), static_cast<int>(kSmemBudget / RowBytes(P))));
 }
-int ZLines(int GZ) { return PowTwoAtMost(std::max<int>(1, std::min<int>(32, kSmemBudget / (2 * static_cast<size_t>(GZ) * sizeof(float2))))); }
+// The z pass's column blocks: BZ columns per block (a power of two), `stages` stage buffers, the persistent grid.
+struct ZLaunch
+{
+   int BZ = 1, logBZ = 0, stages = 1, blocksPerK = 1, nBlocks = 1, grid = 1;
+   size_t smem = 0;
+};
+
+size_t ZSmem(const Dims& d, int BZ, int stages, bool convolve)
+{
+   return (static_cast<size_t>(d.GZ) + stages * static_cast<size_t>(d.nzv + (convolve ? d.GZ : 0))) * BZ *
+          sizeof(float2);
+}
+
+template <bool kConvolve, int kLogN>
+int ZPlan(const iscu_ctx* ctx, const Dims& d, ZLaunch& z);
+
+// Codelets: the transform lengths each pass is compiled for (log2 of X's half length H, of GY, of GZ); any other
+// length runs the runtime-plan kernel (K = 0).
+#define ISCU_WF_CODELETS(logN, a, b, c, ...)                                                                            \
+   switch (logN)                                                                                                       \
+   {                                                                                                                   \
+   case a: { constexpr int K = a; __VA_ARGS__; } break;                                                                \
+   case b: { constexpr int K = b; __VA_ARGS__; } break;                                                                \
+   case c: { constexpr int K = c; __VA_ARGS__; } break;                                                                \
+   default: { constexpr int K = 0; __VA_ARGS__; } break;                                                               \
+   }
+#define ISCU_WF_X_CODELETS(logN, ...) ISCU_WF_CODELETS(logN, 8, 9, 10, __VA_ARGS__)
+#define ISCU_WF_Y_CODELETS(logN, ...) ISCU_WF_CODELETS(logN, 9, 10, 11, __VA_ARGS__)
+#define ISCU_WF_Z_CODELETS(logN, ...) ISCU_WF_CODELETS(logN, 6, 7, 8, __VA_ARGS__)
 
 // The forward x and y passes of a (kzv x kyv x kxv) volume into A, B.
 int ForwardXY(iscu_wf_plan* p, const float* in, const Dims& d, float2* A, float2* B, bool mark = false)
@@ -847,14 +1015,14 @@ int ForwardXY(iscu_wf_plan* p, const float* in, const Dims& d, float2* A, float2
    const float2* tw = p->tw.as<float2>();
    const float2* twg = p->twg.as<float2>();
    const int BY = XLines(d.H);
-   XForwardKernel<<<dim3((d.nyv + BY - 1) / BY, d.nzv), kThreads, XSmem(d.H, BY), ctx->stream>>>(
-      in, d, BY, Log2(BY), tw, twg, A);
+   ISCU_WF_X_CODELETS(d.logH, (XForwardKernel<K><<<dim3((d.nyv + BY - 1) / BY, d.nzv), kThreads, XSmem(d.H, BY),
+                                                 ctx->stream>>>(in, d, BY, Log2(BY), tw, twg, A)));
    ISCU_CK_LAUNCH(ctx, "XForwardKernel");
    if (mark)
       p->Mark(1);
    const int BK = YLines(d.py);
-   YForwardKernel<<<dim3((d.NK + BK - 1) / BK, d.nzv), kThreads, BK * RowBytes(d.py), ctx->stream>>>(
-      A, d, BK, twg, B);
+   ISCU_WF_Y_CODELETS(d.logGY, (YForwardKernel<K><<<dim3((d.NK + BK - 1) / BK, d.nzv), kThreads,
+                                                    BK * RowBytes(d.py), ctx->stream>>>(A, d, BK, twg, B)));
    ISCU_CK_LAUNCH(ctx, "YForwardKernel");
    return ISCU_OK;
 }
@@ -882,15 +1050,39 @@ Dims MakeDims(const iscu_wf_plan* p, uint32_t nxv, uint32_t nyv, uint32_t nzv)
    return d;
 }
 
-int SetFftSmem()
+// The shared-memory ceiling of the kernels a plan of these lengths launches.
+int SetFftSmem(int logH, int logGY, int logGZ)
 {
    const int bytes = static_cast<int>(kSmemMax);
-   ISCU_CK(cudaFuncSetAttribute(XForwardKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-   ISCU_CK(cudaFuncSetAttribute(YForwardKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-   ISCU_CK(cudaFuncSetAttribute(ZKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-   ISCU_CK(cudaFuncSetAttribute(ZKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-   ISCU_CK(cudaFuncSetAttribute(YInverseKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-   ISCU_CK(cudaFuncSetAttribute(XInverseKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+   const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+   ISCU_WF_X_CODELETS(logH, ISCU_CK(cudaFuncSetAttribute(XForwardKernel<K>, attr, bytes));
+                      ISCU_CK(cudaFuncSetAttribute(XInverseKernel<K>, attr, bytes)));
+   ISCU_WF_Y_CODELETS(logGY, ISCU_CK(cudaFuncSetAttribute(YForwardKernel<K>, attr, bytes));
+                      ISCU_CK(cudaFuncSetAttribute(YInverseKernel<K>, attr, bytes)));
+   ISCU_WF_Z_CODELETS(logGZ, ISCU_CK(cudaFuncSetAttribute(ZKernel<true, K>, attr, bytes));
+                      ISCU_CK(cudaFuncSetAttribute(ZKernel<false, K>, attr, bytes)));
+   return ISCU_OK;
+}
+
+template <bool kConvolve, int kLogN>
+int ZPlan(const iscu_ctx* ctx, const Dims& d, ZLaunch& z)
+{
+   // 16 columns per block (8 when the buffers would pass the budget, ...), double-buffered where that fits
+   z.BZ = ISCU_WF_Z_STAGES == 2 ? 16 : 32;
+   z.stages = ISCU_WF_Z_STAGES;
+   while (z.BZ > 1 && ZSmem(d, z.BZ, z.stages, kConvolve) > kSmemBudget)
+      z.BZ >>= 1;
+   if (ZSmem(d, z.BZ, z.stages, kConvolve) > kSmemBudget)
+      z.stages = 1;
+   z.smem = ZSmem(d, z.BZ, z.stages, kConvolve);
+   if (z.smem > kSmemMax)
+      return Fail(ISCU_ERR_LIMIT, "widefield plan: a z column block does not fit in shared memory");
+   z.logBZ = Log2(z.BZ);
+   z.blocksPerK = (d.GY + z.BZ - 1) / z.BZ;
+   z.nBlocks = z.blocksPerK * d.NK;
+   int perSm = 0;
+   ISCU_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, ZKernel<kConvolve, kLogN>, kThreads, z.smem));
+   z.grid = z.stages == 2 ? std::max(1, std::min(z.nBlocks, std::max(1, perSm) * ctx->smCount)) : z.nBlocks;
    return ISCU_OK;
 }
 
@@ -907,15 +1099,17 @@ static int ConvolveToA(iscu_wf_plan* p, const float* density)
    if (rc != ISCU_OK)
       return rc;
    p->Mark(2);
-   const int BZ = ZLines(d.GZ);
-   ZKernel<true><<<dim3((d.GY + BZ - 1) / BZ, d.NK), kThreads, 2 * static_cast<size_t>(d.GZ) * BZ * sizeof(float2),
-                   ctx->stream>>>(p->B.as<float2>(), d, BZ, Log2(BZ), static_cast<int>(p->kz / 2), twg,
-                                  p->Kh.as<float2>());
+   int rc2 = ISCU_OK;
+   ISCU_WF_Z_CODELETS(d.logGZ, ZLaunch zl; rc2 = ZPlan<true, K>(ctx, d, zl); if (rc2 != ISCU_OK) return rc2;
+                      (ZKernel<true, K><<<zl.grid, kThreads, zl.smem, ctx->stream>>>(
+                         p->B.as<float2>(), d, zl.BZ, zl.logBZ, zl.blocksPerK, zl.nBlocks, zl.stages,
+                         static_cast<int>(p->kz / 2), twg, p->Kh.as<float2>())));
    ISCU_CK_LAUNCH(ctx, "ZKernel<convolve>");
    p->Mark(3);
    const int BK = YLines(d.py);
-   YInverseKernel<<<dim3((d.NK + BK - 1) / BK, d.nzv), kThreads, BK * RowBytes(d.py), ctx->stream>>>(
-      p->B.as<float2>(), d, BK, static_cast<int>(p->ky / 2), twg, p->A.as<float2>());
+   ISCU_WF_Y_CODELETS(d.logGY, (YInverseKernel<K><<<dim3((d.NK + BK - 1) / BK, d.nzv), kThreads,
+                                                    BK * RowBytes(d.py), ctx->stream>>>(
+                                   p->B.as<float2>(), d, BK, static_cast<int>(p->ky / 2), twg, p->A.as<float2>())));
    ISCU_CK_LAUNCH(ctx, "YInverseKernel");
    p->Mark(4);
    return ISCU_OK;
@@ -938,9 +1132,10 @@ static int FinishX(iscu_wf_plan* p, double background, const iscu_camera* cam, u
       image = p->image.as<float>();
    }
    const int BY = XLines(d.H);
-   XInverseKernel<<<dim3((d.nyv + BY - 1) / BY, d.nzv), kThreads, XSmem(d.H, BY), ctx->stream>>>(
-      p->A.as<float2>(), d, BY, Log2(BY), static_cast<int>(p->kx / 2), scale, static_cast<float>(background),
-      p->tw.as<float2>(), p->twg.as<float2>(), image);
+   ISCU_WF_X_CODELETS(d.logH, (XInverseKernel<K><<<dim3((d.nyv + BY - 1) / BY, d.nzv), kThreads, XSmem(d.H, BY),
+                                                   ctx->stream>>>(
+                                  p->A.as<float2>(), d, BY, Log2(BY), static_cast<int>(p->kx / 2), scale,
+                                  static_cast<float>(background), p->tw.as<float2>(), p->twg.as<float2>(), image)));
    ISCU_CK_LAUNCH(ctx, "XInverseKernel");
    p->Mark(5);
    if (cam)
@@ -993,11 +1188,11 @@ int iscu_wf_plan_create(iscu_ctx* ctx, uint32_t nx, uint32_t ny, uint32_t nz, co
    p->logGZ = Log2(p->GZ);
    p->px = MakeLinePlan(p->logH, true);
    p->py = MakeLinePlan(p->logGY, false);
-   p->pz = MakeLinePlan(p->logGZ, true);
+   p->pz = MakeZPlan(p->logGZ);
    int entries = PlaceTables(p->px, 0);
    entries += PlaceTables(p->py, entries);
    entries += PlaceTables(p->pz, entries);
-   int rc = SetFftSmem();
+   int rc = SetFftSmem(p->logH, p->logGY, p->logGZ);
    if (rc != ISCU_OK)
       return rc;
    const uint32_t nzA = std::max(nz, kz), nyA = std::max(ny, ky);
@@ -1026,9 +1221,10 @@ int iscu_wf_plan_create(iscu_ctx* ctx, uint32_t nx, uint32_t ny, uint32_t nz, co
    rc = ForwardXY(p.get(), dPsf.as<float>(), dk, p->A.as<float2>(), p->B.as<float2>());
    if (rc != ISCU_OK)
       return rc;
-   const int BZ = ZLines(dk.GZ);
-   ZKernel<false><<<dim3((dk.GY + BZ - 1) / BZ, dk.NK), kThreads, static_cast<size_t>(dk.GZ) * BZ * sizeof(float2),
-                    ctx->stream>>>(p->B.as<float2>(), dk, BZ, Log2(BZ), 0, p->twg.as<float2>(), p->Kh.as<float2>());
+   ISCU_WF_Z_CODELETS(dk.logGZ, ZLaunch zl; rc = ZPlan<false, K>(ctx, dk, zl); if (rc != ISCU_OK) return rc;
+                      (ZKernel<false, K><<<zl.grid, kThreads, zl.smem, ctx->stream>>>(
+                         p->B.as<float2>(), dk, zl.BZ, zl.logBZ, zl.blocksPerK, zl.nBlocks, zl.stages, 0,
+                         p->twg.as<float2>(), p->Kh.as<float2>())));
    ISCU_CK_LAUNCH(ctx, "ZKernel<spectrum>");
    ISCU_CK(cudaStreamSynchronize(ctx->stream));
    *out = p.release();

@@ -136,3 +136,40 @@ def test_large_pupil_psf_vs_oracle(engine, oracle):
     want = oracle.psf_planes(req, dz * 1e-9, size=96, normalize=True)
     for i in range(3):
         assert np.abs(got[i] - want[i]).max() <= TOL * want[i].max(), i
+
+
+@pytest.mark.parametrize("vol_shape,psf_shape,grid", [((24, 200, 160), (12, 100, 120), (512, 512, 64)),
+                                                      ((130, 20, 24), (127, 9, 11), (64, 32, 256))])
+def test_codelet_lengths_vs_oracle(engine, vol_shape, psf_shape, grid):
+    """Grids whose transform lengths run the compiled-in codelets other than the full-size ones (x half length 256,
+    y 512, z 64; z 256) against the float64 oracle."""
+    import torch
+    rng = np.random.default_rng(sum(vol_shape))
+    vol = rng.random(vol_shape).astype(np.float32)
+    vol[vol < 0.7] = 0.0
+    psf = rng.random(psf_shape).astype(np.float32) - 0.2
+    plan = WidefieldPlan(engine, vol_shape, psf)
+    assert plan.grid() == grid
+    got = plan.convolve_dev(torch.from_numpy(vol).cuda()).cpu().numpy()
+    want = np.maximum(fft_convolve_same_f64(vol, psf), 0.0)
+    assert _rel(got, want) <= TOL
+    plan.close()
+
+
+def test_codelet_2048_impulse(engine):
+    """A 2048 x 2048 grid (x half length 1024, y 2048 codelets): unit dyes image to the PSF shifted there."""
+    import torch
+    rng = np.random.default_rng(12)
+    psf = rng.random((1, 1019, 1019)).astype(np.float32) * np.float32(1e-4)
+    psf[0, 509, 509] += 1.0
+    plan = WidefieldPlan(engine, (2, 1030, 1030), psf)
+    assert plan.grid() == (2048, 2048, 4)
+    for (z0, y0, x0) in ((0, 515, 515), (1, 3, 1020)):
+        vol = torch.zeros((2, 1030, 1030), dtype=torch.float32, device="cuda")
+        vol[z0, y0, x0] = 1.0
+        got = plan.convolve_dev(vol).cpu().numpy()
+        want = np.zeros((2, 1030, 1030), np.float32)
+        ys, xs = slice(max(0, y0 - 509), min(1030, y0 + 510)), slice(max(0, x0 - 509), min(1030, x0 + 510))
+        want[z0, ys, xs] = psf[0, ys.start - y0 + 509: ys.stop - y0 + 509, xs.start - x0 + 509: xs.stop - x0 + 509]
+        assert _rel(got, want) <= TOL, (z0, y0, x0)
+    plan.close()
