@@ -105,6 +105,8 @@ NCU_TRAFFIC = {
     ("smlm", "ContribKernel"): (93568768, "profiles/ContribKernel_smlm_dstorm.md"),
     ("psflib", "CztTf32x3Kernel"): (52487168, "profiles/CztTf32x3Kernel_psf_library.md"),
     ("two-colour", "GatherTilesKernel"): (2182043649, "profiles/GatherTilesKernel_two_colour.md"),
+    ("widefield", "WfNoiseKernel"): (73977088, "profiles/widefield_cells_launches.md"),
+    ("widefield", "ZKernel<convolve>"): (1045289728, "profiles/widefield_cells_launches.md"),
 }
 
 

@@ -147,6 +147,10 @@ namespace {
 #ifndef ISCU_WF_Z_STAGES
 #define ISCU_WF_Z_STAGES 1
 #endif
+// Columns per z block with one stage buffer (a power of two).
+#ifndef ISCU_WF_Z_COLUMNS
+#define ISCU_WF_Z_COLUMNS 32
+#endif
 constexpr int kThreads = 256;
 constexpr int kMinCtas = ISCU_WF_MIN_CTAS;
 constexpr size_t kSmemBudget = 100 * 1024;   // lines per CTA are sized to this
@@ -1068,7 +1072,7 @@ template <bool kConvolve, int kLogN>
 int ZPlan(const iscu_ctx* ctx, const Dims& d, ZLaunch& z)
 {
    // 16 columns per block (8 when the buffers would pass the budget, ...), double-buffered where that fits
-   z.BZ = ISCU_WF_Z_STAGES == 2 ? 16 : 32;
+   z.BZ = ISCU_WF_Z_STAGES == 2 ? 16 : ISCU_WF_Z_COLUMNS;
    z.stages = ISCU_WF_Z_STAGES;
    while (z.BZ > 1 && ZSmem(d, z.BZ, z.stages, kConvolve) > kSmemBudget)
       z.BZ >>= 1;
