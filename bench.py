@@ -819,8 +819,125 @@ class ScheduleWorkload:
         return sec
 
 
+class BinnedWorkload:
+    """The binned blink regime (the reference's approximate SMLM render of dense frames): 200 frames of 128 x 128 px
+    with about 2,400 ON emitters each (12.7 per um^2, just above the reference's switch to binned at 12.5), deposited
+    on 2 x 2 cells per pixel and convolved with the SMLM kernel's 49 planes at the cell pitch (R = 33 cells); then
+    20 photons/px background and the EMCCD chain. The emitter records stay resident; one step = background fill,
+    iscu_binned_render_dev, iscu_noise_frames_dev. e2e: page-locked emitter records and frame table in, ADU out."""
+    name = ("binned blinks: 128x128 px, 200 frames, ~2,400 ON emitters per frame (12.7 per um^2), u = 2 cells per "
+            "pixel, SMLM kernel (NA 1.45, 670 nm, 49 planes), 20 photons/px background, EMCCD gain 300")
+    metric = "frames/s"
+    dtype = "f64"
+    cpu_kind = "reference"
+    BACKGROUND = 20.0
+
+    def __init__(self, rank: int):
+        from insiliscope_b200.workloads import binned_dense
+        self.mv = binned_dense(seed=42 + rank)
+        self.frames_per_step_cpu = 40
+        self.cpu_sample = (f"{self.frames_per_step_cpu} of the 200 frames per step: the reference's "
+                           "BinnedBlinkRenderer::Render per frame (BinnedBlinks.cpp, float FFTs, compiled from its "
+                           "sources; frames in parallel on its thread pool) and ApplyNoiseChain per frame")
+
+    def setup(self, device: int):
+        import torch
+        from insiliscope_b200 import BinnedRenderer, Engine, generate_camera_maps
+        mv = self.mv
+        self.eng = eng = Engine(device)
+        dev = f"cuda:{device}"
+        t0 = time.perf_counter()
+        eng.kernel_build(0, mv.psf)
+        eng.synchronize()
+        self.psf_build_ms = (time.perf_counter() - t0) * 1e3
+        self.binned = BinnedRenderer(eng, mv.width, mv.height, mv.upscale, slot=0)
+        off, _, _ = generate_camera_maps(mv.width, mv.height, 7, 100.0, 2.0, 1.0, 0.0, 50.0, 0.0)
+        self.offset = off
+        eng.set_static(mv.width, mv.height, offset=off)
+        n = mv.n_frames
+        self.d_em = torch.from_numpy(mv.emitters.view(np.uint8)).to(dev)
+        self.d_fr = torch.from_numpy(mv.frames.view(np.uint8)).to(dev)
+        self.d_idx = torch.arange(n, dtype=torch.int32, device=dev)
+        self.d_img = torch.empty((n, mv.height, mv.width), dtype=torch.float32, device=dev)
+        self.d_adu = torch.empty((n, mv.height, mv.width), dtype=torch.uint16, device=dev)
+        self.h_em = torch.from_numpy(mv.emitters.view(np.uint8)).pin_memory()
+        self.h_fr = torch.from_numpy(mv.frames.view(np.uint8)).pin_memory()
+        self.h_adu = torch.empty((n, mv.height, mv.width), dtype=torch.uint16).pin_memory()
+        self.stream = eng.torch_stream()
+        self.frames_per_step = n
+        self.n_emitters = len(mv.emitters)
+
+    def _step(self, sync):
+        mv = self.mv
+        self.d_img.fill_(self.BACKGROUND)
+        self.binned.render_dev(self.d_em, self.d_fr, mv.n_frames, self.d_img, sync=False)
+        self.eng.noise_frames_dev(self.d_img, self.d_idx, mv.camera, mv.noise_seed, out=self.d_adu, sync=sync)
+
+    def device_step(self):
+        self._step(False)
+
+    def e2e_step(self):
+        """Page-locked records in, ADU out, the copies on torch's own stream ordered with the library's by the
+        synchronizing calls."""
+        import torch
+        self.d_em.copy_(self.h_em, non_blocking=True)
+        self.d_fr.copy_(self.h_fr, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        self._step(True)
+        self.h_adu.copy_(self.d_adu, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return self.h_adu
+
+    def e2e_bytes(self):
+        return self.h_em.numel() + self.h_fr.numel(), self.h_adu.numel() * 2
+
+    def kernel_name(self):
+        return "BinnedRenderKernel+noise"
+
+    def alg_bytes_per_launch(self):
+        # the emitter records (32 B) and frame table, the photon frames written by the fill, read and written by the
+        # render and read by the noise chain (4 x 4 B per pixel), the ADU out and the offset map
+        px = self.mv.n_frames * self.mv.width * self.mv.height
+        return len(self.mv.emitters) * 32 + self.mv.n_frames * 24 + px * 16 + px * 2 + self.mv.width * self.mv.height * 4
+
+    def config_extra(self):
+        return {"upscale": self.binned.upscale, "radius_cells": self.binned.radius,
+                "emitters_per_frame": round(len(self.mv.emitters) / self.mv.n_frames, 1)}
+
+    def cpu_cores(self):
+        return self.ref.threads()
+
+    def reference_setup(self, threads=0):
+        from oracle.oracle import Reference
+        if not Reference.available():
+            raise RuntimeError("the reference harness oracle/_ref/libiscref.so is not built (it needs the reference "
+                               "tree at build time)")
+        self.ref = Reference()
+        self.ref.set_threads(threads)
+        self.ref_kernel = self.ref.kernel(req=self.mv.psf)
+        k = self.frames_per_step_cpu
+        fr = self.mv.frames[:k].copy()
+        last = int(fr[-1]["em_start"] + fr[-1]["em_count"])
+        self.ref_em = self.mv.emitters[:last]
+        self.ref_fr = fr
+        if not hasattr(self, "offset"):
+            from insiliscope_b200 import generate_camera_maps
+            self.offset, _, _ = generate_camera_maps(self.mv.width, self.mv.height, 7, 100.0, 2.0, 1.0, 0.0, 50.0, 0.0)
+
+    def reference_step(self):
+        mv = self.mv
+        t0 = time.perf_counter()
+        img = np.full((len(self.ref_fr), mv.height, mv.width), self.BACKGROUND, np.float32)
+        self.ref.binned_render(self.ref_kernel, 0.0, mv.width, mv.height, mv.upscale, self.ref_em, self.ref_fr, img)
+        off = self.offset.reshape(mv.height, mv.width)
+        for k in range(len(self.ref_fr)):
+            self.ref.noise_chain(img[k], mv.camera, off, None, None, mv.noise_seed, k, parallel=True)
+        return time.perf_counter() - t0
+
+
 WORKLOADS = {"smlm": SmlmWorkload, "widefield": WidefieldWorkload, "psflib": PsfLibraryWorkload,
-             "two-colour": TwoColourWorkload, "nll-grad": NllGradWorkload, "schedules": ScheduleWorkload}
+             "two-colour": TwoColourWorkload, "nll-grad": NllGradWorkload, "schedules": ScheduleWorkload,
+             "binned": BinnedWorkload}
 
 
 # ----------------------------------------------------------------------------------------------------- arms

@@ -584,6 +584,34 @@ int iscu_buffer_read_low16(const iscu_buffer* src, size_t words, uint16_t* dst);
 int iscu_dispatch(iscu_ctx* ctx, const char* kernel, const uint32_t* params, size_t n_params,
                   iscu_buffer* const* bufs, size_t n_bufs, uint32_t x, uint32_t y, uint32_t z);
 
+/* ------------------------------------------------------- binned blinks (approximate SMLM) ----------------------- */
+
+/* sim::BinnedBlinkRenderer (BinnedBlinks.h:35-60, BinnedBlinks.cpp:150-248): a frame's emitters deposited at the
+ * nearest cell of a grid of u cells per camera pixel (cell floor((x + 0.5) u), per axis), one density per PSF plane,
+ * each convolved with that plane's kernel at the cell pitch out to R cells, summed, max(0, .) per cell, u x u cells
+ * summed into each pixel. The plane kernels are KernelWidefieldPsf::Kernel (WidefieldRender.cpp:300-322): cell
+ * (dx, dy) = the sum of the oversampled plane over the r x r block from (s0 + dx r, s0 + dy r), r = os / u,
+ * s0 = floor((n - 1) / 2 - r / 2 + 1); R the kernel's reach (KernelWidefieldPsf::Radius), capped by the slot's halo
+ * cut at ceil((sqrt(max radius2) + 1) u). The convolution is a direct sum in float64 (the reference runs it as float
+ * FFTs over a grid padded by R; the two agree to the float FFT's rounding).
+ * create: kernel slot `slot` (u = the largest divisor of its oversampling up to `upscale`,
+ * KernelWidefieldPsf::ValidUpscale) or, slot < 0, the in-focus Gaussian of sigma_px (u = upscale clamped to 1..8,
+ * R = ceil(3 sigma u), exp(-(x^2 + y^2) / (2 (sigma u)^2)) normalized to sum 1), for width x height frames. */
+typedef struct iscu_binned iscu_binned;
+int iscu_binned_create(iscu_ctx* ctx, int32_t slot, double sigma_px, uint32_t width, uint32_t height,
+                       int32_t upscale, iscu_binned** out);
+/* The renderer's u (cells per pixel), R (kernel radius in cells) and plane count (any output NULL). */
+int iscu_binned_info(iscu_binned* b, int32_t* upscale, int32_t* radius_cells, int32_t* planes);
+/* The plane kernels, nz x (2R + 1)^2 floats (row-major, dy outer), into host memory. */
+int iscu_binned_kernels(iscu_binned* b, float* out);
+void iscu_binned_destroy(iscu_binned* b);
+/* Frames k < n_frames of a batch (as iscu_render_frames_dev: frame k's emitters are emitters_dev[em_start ..
+ * em_start + em_count), z index = plane & 0xFFFF, clamped to the kernel's planes; emitters with photons <= 0 and
+ * those whose cell lies more than R outside the frame are skipped): img_dev[k * w * h ..] += the binned photon image
+ * (BinnedBlinkRenderer::Render); alone_dev (nullable) += the same values. */
+int iscu_binned_render_dev(iscu_binned* b, const iscu_emitter* emitters_dev, uint32_t n_emitters,
+                           const iscu_frame* frames_dev, uint32_t n_frames, float* img_dev, float* alone_dev);
+
 #ifdef __cplusplus
 }
 #endif

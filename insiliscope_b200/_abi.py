@@ -170,6 +170,11 @@ SIGNATURES = {
     "iscu_buffer_read_low16": (C.c_int, [vp, C.c_size_t, vp]),
     "iscu_dispatch": (C.c_int, [vp, C.c_char_p, vp, C.c_size_t, vp, C.c_size_t, C.c_uint32, C.c_uint32,
                                 C.c_uint32]),
+    "iscu_binned_create": (C.c_int, [vp, C.c_int32, C.c_double, C.c_uint32, C.c_uint32, C.c_int32, vp]),
+    "iscu_binned_info": (C.c_int, [vp, vp, vp, vp]),
+    "iscu_binned_kernels": (C.c_int, [vp, vp]),
+    "iscu_binned_destroy": (None, [vp]),
+    "iscu_binned_render_dev": (C.c_int, [vp, vp, C.c_uint32, vp, C.c_uint32, vp, vp]),
     "iscu_dye_blinks_dev": (C.c_int, [vp, vp, vp, vp, C.c_uint32, vp, C.c_uint32, C.c_double, C.c_double, vp,
                                       C.c_uint32, vp, vp]),
     "iscu_drift_trajectory": (C.c_int, [C.c_int64, C.c_int64, C.c_double, C.POINTER(DriftSettings), vp]),

@@ -35,6 +35,7 @@ UNITS = {
     "widefield.cu": ["--fmad=false"],
     "backend.cu": ["--fmad=false"],
     "schedule.cu": ["--fmad=false"],
+    "binned.cu": [],
     "capi.cpp": [],
     "host_models.cpp": [],
 }

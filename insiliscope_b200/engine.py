@@ -238,18 +238,23 @@ class Engine:
         check(self.lib.iscu_set_static(self.h, width, height, pixel_base, *[_ptr(a) for a in arrs], float(flat_bg)))
         self.width, self.height = width, height
 
-    def noise_frames_dev(self, photons, frames, camera: CameraParams, seed):
-        """ApplyNoiseChain on (n, h, w) float32 CUDA photons; frames: the frame index of each. Returns uint16."""
+    def noise_frames_dev(self, photons, frames, camera: CameraParams, seed, out=None, sync=True):
+        """ApplyNoiseChain on (n, h, w) float32 CUDA photons; frames: the frame index of each (host indices, or an
+        int32/uint32 CUDA tensor of them). Returns the uint16 frames (into `out` when given)."""
         import torch
         photons = photons.contiguous()
-        fr = torch.as_tensor(np.asarray(frames, dtype=np.int64).astype(np.uint32).view(np.int32),
-                             device=photons.device)
-        out = torch.empty(photons.shape, dtype=torch.uint16, device=photons.device)
+        if isinstance(frames, torch.Tensor):
+            fr = frames
+        else:
+            fr = torch.as_tensor(np.asarray(frames, dtype=np.int64).astype(np.uint32).view(np.int32),
+                                 device=photons.device)
+        if out is None:
+            out = torch.empty(photons.shape, dtype=torch.uint16, device=photons.device)
         cam = camera.c()
-        self._before(True)
+        self._before(sync)
         check(self.lib.iscu_noise_frames_dev(self.h, _ptr(photons), photons.shape[0], _ptr(fr), C.byref(cam), seed,
                                              _ptr(out)))
-        self.synchronize()
+        self._after(sync)
         return out
 
     # -------------------------------------------------------------------------------------------- PSF
@@ -730,6 +735,51 @@ class WidefieldPlan:
         """Waits for I/O slot io_slot's frames (iscu_wf_render_wait)."""
         check(self.lib.iscu_wf_render_wait(self.h, int(io_slot)))
         self._pending_io.pop(int(io_slot), None)
+
+
+class BinnedRenderer:
+    """iscu_binned: the binned blink regime (sim::BinnedBlinkRenderer) for width x height frames, on kernel slot
+    `slot` or (slot < 0) the in-focus Gaussian of sigma_px."""
+
+    def __init__(self, engine: Engine, width, height, upscale, slot=-1, sigma_px=0.0):
+        self.engine = engine
+        self.lib = engine.lib
+        self.width, self.height = int(width), int(height)
+        h = C.c_void_p()
+        check(self.lib.iscu_binned_create(engine.h, int(slot), float(sigma_px), self.width, self.height,
+                                          int(upscale), C.byref(h)))
+        self.h = h
+        u, r, nz = C.c_int32(), C.c_int32(), C.c_int32()
+        check(self.lib.iscu_binned_info(self.h, C.byref(u), C.byref(r), C.byref(nz)))
+        self.upscale, self.radius, self.planes = u.value, r.value, nz.value
+        engine._plans.add(self)
+
+    def kernels(self):
+        """The plane kernels at the cell pitch, (planes, 2R + 1, 2R + 1) float32."""
+        D = 2 * self.radius + 1
+        out = np.empty((self.planes, D, D), np.float32)
+        check(self.lib.iscu_binned_kernels(self.h, _ptr(out)))
+        return out
+
+    def render_dev(self, emitters_dev, frames_dev, n_frames, img_dev, alone_dev=None, sync=True):
+        """img_dev (n_frames, h, w) float32 CUDA += the frames' binned blink images (iscu_binned_render_dev);
+        emitters / frames as Engine.render_frames_dev."""
+        self.engine._before(sync)
+        check(self.lib.iscu_binned_render_dev(self.h, _ptr(emitters_dev), _n_records(emitters_dev), _ptr(frames_dev),
+                                              int(n_frames), _ptr(img_dev), _ptr(alone_dev)))
+        self.engine._after(sync)
+
+    def close(self):
+        if self.h:
+            if self.engine.h:
+                self.lib.iscu_binned_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 @dataclass

@@ -12,7 +12,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .engine import BLINK_EVENT_DTYPE, INTERP_CUBIC, CameraParams, PsfParams
+from .engine import BLINK_EVENT_DTYPE, EMITTER_DTYPE, FRAME_DTYPE, INTERP_CUBIC, CameraParams, PsfParams
 
 SITE_SALT = 0x5157E5
 M32 = np.uint64(0xFFFFFFFF)
@@ -112,6 +112,59 @@ def smlm_dstorm(seed: int = 42, sites: int = 4000, frames: int = 200, size: int 
     cam = CameraParams(quantum_efficiency=1.0, dark_electrons=0.0, gain=2.2, read_noise_e=1.5, emccd=False)
     return SmlmMovie(size, size, frames, pixel_nm, median_photons, 20.0, ev, bucket, psf, cam, seed, 100.0, 2.0, 2.2,
                      0.1 / 2.2, 1.5, 0.2, (seed ^ 0x9E3779B9) & 0xFFFFFFFF)
+
+
+@dataclass
+class BinnedMovie:
+    """Frames of the binned blink regime: each frame's emitters as CollectFrameEmitters leaves them (position in
+    pixels, detected photons, z plane), frame-major."""
+    width: int
+    height: int
+    n_frames: int
+    pixel_nm: float
+    upscale: int
+    psf: PsfParams
+    camera: CameraParams
+    emitters: np.ndarray        # EMITTER_DTYPE
+    frames: np.ndarray          # FRAME_DTYPE
+    noise_seed: int
+
+
+def binned_dense(seed: int = 42, sites: int = 60000, frames: int = 200, size: int = 128, pixel_nm: float = 108.0,
+                 p_on: float = 0.04, median_photons: float = 2000.0, sigma_log: float = 0.5, z_half_nm: float = 600.0,
+                 upscale: int = 2) -> BinnedMovie:
+    """Dense blink frames for the binned regime: 128 x 128 px at 108 nm, 60,000 sites uniform over the field (z
+    uniform in [-600, 600] nm), each ON in a frame with probability 0.04 -- about 2,400 per frame, 12.7 per um^2, just
+    above the density at which the reference switches to binned (12.5 per um^2) -- photons lognormal (median 2000,
+    sigma_log 0.5); the SMLM movie's PSF kernel (oversampling 4, 49 planes 25 nm apart, plane = the nearest, as
+    NearestZIndex rounds), u = 2 cells per pixel; EMCCD camera (gain 300, read noise 50 e-, CIC 0.002)."""
+    s = np.arange(sites, dtype=np.uint64)
+    st = np.uint64((seed ^ SITE_SALT) & 0xFFFFFFFF)
+    x_px = size * hash_unit(st, s, 0, 0)
+    y_px = size * hash_unit(st, s, 0, 1)
+    z_nm = -z_half_nm + 2.0 * z_half_nm * hash_unit(st, s, 0, 2)
+    plane = np.clip(np.floor(z_nm / 25.0 + 24.0 + 0.5), 0, 48).astype(np.int32)
+    f = np.arange(frames, dtype=np.uint64)
+    F, S = np.meshgrid(f, s, indexing="ij")
+    on = hash_unit(seed, S, F, 0) < p_on
+    fi, si = np.nonzero(on)
+    em = np.zeros(len(fi), EMITTER_DTYPE)
+    em["x_px"] = x_px[si] - 0.5   # pixel centres at integers: the camera's pixel x spans [x - 0.5, x + 0.5)
+    em["y_px"] = y_px[si] - 0.5
+    em["photons"] = median_photons * np.exp(sigma_log * hash_normal(seed, S[fi, si], F[fi, si], 1))
+    em["plane"] = plane[si]
+    counts = np.bincount(fi, minlength=frames)
+    fr = np.zeros(frames, FRAME_DTYPE)
+    fr["em_start"] = np.concatenate([[0], np.cumsum(counts)[:-1]])
+    fr["em_count"] = counts
+    fr["frame"] = np.arange(frames)
+    fr["bg_scale"] = 1.0
+    psf = PsfParams(wavelength_nm=670.0, na=1.45, immersion_index=1.518, sample_index=1.518,
+                    working_distance_um=150.0, sample_depth_nm=0.0, pixel_size_nm=pixel_nm, oversampling=4,
+                    kernel_half_width_px=16, nz=49, z_step_nm=25.0, pupil_samples=64, interp=INTERP_CUBIC)
+    cam = CameraParams(quantum_efficiency=1.0, gain=1.0, read_noise_e=50.0, emccd=True, em_gain=300.0,
+                       cic_electrons=0.002, bit_depth=16)
+    return BinnedMovie(size, size, frames, pixel_nm, upscale, psf, cam, em, fr, (seed ^ 0x9E3779B9) & 0xFFFFFFFF)
 
 
 @dataclass

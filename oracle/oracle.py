@@ -209,6 +209,8 @@ class Reference:
         L.ref_illumination_field.restype = C.c_size_t
         L.ref_background_fade_scale.argtypes = [f64, f64]
         L.ref_background_fade_scale.restype = f64
+        L.ref_binned_render.argtypes = [vp, f64, C.c_uint, C.c_uint, C.c_int, vp, vp, u32, vp, vp, vp]
+        L.ref_binned_render.restype = f64
         self.L = L
 
     def set_threads(self, n):
@@ -332,6 +334,21 @@ class Reference:
                                           float(t1), _p(counts))
         return counts, sec
 
+    def binned_render(self, kernel, sigma_px, w, h, upscale, emitters, frames, img=None):
+        """sim::BinnedBlinkRenderer: Setup on `kernel` (a RefKernel; None: the Gaussian of sigma_px), Render of each
+        frame's emitters (EMITTER_DTYPE / FRAME_DTYPE records) into img (n, h, w) float32 (+=; zeros when None), frames
+        in parallel on the reference's pool. Returns (img, u, R, wall seconds)."""
+        em = np.ascontiguousarray(emitters)
+        fr = np.ascontiguousarray(frames)
+        if img is None:
+            img = np.zeros((len(fr), h, w), np.float32)
+        u, r = C.c_int(), C.c_int()
+        sec = self.L.ref_binned_render(kernel.h if kernel is not None else None, sigma_px, w, h, upscale, _p(em),
+                                       _p(fr), len(fr), _p(img), C.byref(u), C.byref(r))
+        if sec < 0:
+            raise RuntimeError("BinnedBlinkRenderer::Setup refused")
+        return img, u.value, r.value, sec
+
     def dye_h1(self, seed, cx, cy, mt_index):
         return int(self.L.ref_dye_h1(int(seed) & 0xFFFFFFFF, int(cx), int(cy), int(mt_index)))
 
@@ -429,6 +446,81 @@ class RefKernel:
                                         bg, C.byref(cam), _p(f(offset)), _p(f(gain)), _p(f(read_noise)), seed,
                                         _p(ph), _p(adu))
         return t, ph, adu
+
+
+def binned_cell_kernels_f64(planes, os_, upscale, radius2=None):
+    """The binned renderer's plane kernels at the cell pitch (KernelWidefieldPsf, WidefieldRender.cpp:262-322;
+    BinnedBlinkRenderer::Setup, BinnedBlinks.cpp:150-188): u = the largest divisor of os up to upscale, r = os / u
+    oversampled samples per cell, s0 = floor((n - 1) / 2 - r / 2 + 1); cell (dx, dy) = the float64 sum over the r x r
+    block from (s0 + dx r, s0 + dy r) clipped to the plane, rows then columns, as float32; R = the cells that reach
+    the plane, capped by the halo cut at ceil((sqrt(max radius2) + 1) u). Returns (K (nz, 2R+1, 2R+1), u, R)."""
+    P = np.asarray(planes, np.float32)
+    nz, n, _ = P.shape
+    os_ = max(1, int(os_))
+    u = 1
+    for c in range(max(1, min(int(upscale), os_)), 1, -1):
+        if os_ % c == 0:
+            u = c
+            break
+    r = max(1, os_ // u)
+    s0 = int(np.floor((n - 1) / 2.0 - r / 2.0 + 1.0))
+    d_min = int(np.ceil((-s0 - r + 1) / float(r)))
+    d_max = int(np.floor((n - 1 - s0) / float(r)))
+    R = max(1, max(-d_min, d_max))
+    if radius2 is not None and len(radius2):
+        r2 = int(np.max(radius2))
+        if r2 >= 0:
+            R = min(R, int(np.ceil((np.sqrt(float(r2)) + 1.0) * u)))
+    R = max(1, R)
+    d = np.arange(-R, R + 1)
+    ya = s0 + d * r
+    acc = np.zeros((nz, 2 * R + 1, 2 * R + 1), np.float64)
+    for iy in range(r):                      # the block's rows, then its columns: the reference's summation order
+        y = ya + iy
+        for ix in range(r):
+            x = ya + ix
+            ok = ((y >= 0) & (y < n))[:, None] & ((x >= 0) & (x < n))[None, :]
+            v = P[:, np.clip(y, 0, n - 1)][:, :, np.clip(x, 0, n - 1)].astype(np.float64)
+            acc += np.where(ok[None], v, 0.0)
+    return acc.astype(np.float32), u, R
+
+
+def binned_gauss_kernel_f64(sigma_px, upscale):
+    """The renderer's kernel without a PSF (BinnedBlinks.cpp:190-212): u = upscale clamped to 1..8,
+    R = ceil(3 sigma u), exp(-(x^2 + y^2) / (2 (sigma u)^2)) normalized in float64, as float32."""
+    u = max(1, min(int(upscale), 8))
+    R = max(1, int(np.ceil(3.0 * sigma_px * u)))
+    x = np.arange(-R, R + 1, dtype=np.float64)
+    sc = sigma_px * u
+    k = np.exp(-(x[None, :] ** 2 + x[:, None] ** 2) / (2.0 * sc * sc))
+    return (k / k.sum()).astype(np.float32)[None], u, R
+
+
+def binned_render_f64(K, u, R, emitters, frames, w, h):
+    """BinnedBlinkRenderer::Render (BinnedBlinks.cpp:216-246) as the linear convolution it computes, in float64:
+    per frame every emitter with photons > 0 at cell floor((x + 0.5) u) (skipped beyond R cells outside the frame),
+    plane (plane & 0xFFFF) clamped, adds float32(photons) x K[plane] around its cell; the cells (float32) clamped at
+    0 are summed u x u per pixel in float64. Returns (n, h, w) float32."""
+    K = np.asarray(K, np.float64)
+    nz = K.shape[0]
+    cw, ch = w * u, h * u
+    out = np.zeros((len(frames), h, w), np.float32)
+    for k, fr in enumerate(frames):
+        canvas = np.zeros((ch + 4 * R, cw + 4 * R), np.float64)   # cells -2R .. c + 2R
+        for e in emitters[int(fr["em_start"]): int(fr["em_start"]) + int(fr["em_count"])]:
+            if not (e["photons"] > 0.0):
+                continue
+            cx = int(np.floor((e["x_px"] + 0.5) * u))
+            cy = int(np.floor((e["y_px"] + 0.5) * u))
+            if cx < -R or cy < -R or cx >= cw + R or cy >= ch + R:
+                continue
+            p = min(nz - 1, max(0, int(e["plane"]) & 0xFFFF))
+            ph = float(np.float32(e["photons"]))
+            canvas[cy + R: cy + 3 * R + 1, cx + R: cx + 3 * R + 1] += ph * K[p]
+        cells = canvas[2 * R: 2 * R + ch, 2 * R: 2 * R + cw].astype(np.float32)
+        cells = np.maximum(cells, np.float32(0)).astype(np.float64)
+        out[k] = cells.reshape(h, u, w, u).sum(axis=(1, 3)).astype(np.float32)
+    return out
 
 
 def fft_convolve_same_f64(volume: np.ndarray, psf: np.ndarray) -> np.ndarray:

@@ -8,6 +8,7 @@
 //   CollectGpuEmitters (:219), ApplyNoiseChain (SMLMNoise.cpp:142), the camera maps (SMLMNoise.cpp:89-140), the
 //   counter RNG (SMLMCounterRng.h, core/src/rng.h), and a movie loop shaped like FluorescenceMovie::Render's
 //   (ScopeMovie.cpp:7267, :7649: frames in parallel on the reference's own thread pool, ParallelFor).
+#include "BinnedBlinks.h"
 #include "Drift.h"
 #include "PsfGeneratorBridge.h"
 #include "SMLMBackground.h"
@@ -575,5 +576,34 @@ double ref_dye_blinks_batch(int mode, const double* kin, const double* histStart
 
 // The core's DyeH1 (dyes.cpp:175-178): H1 of microtubule mtIndex of cell (cx, cy).
 uint32_t ref_dye_h1(uint32_t seed, int32_t cx, int32_t cy, int mtIndex) { return isc::DyeH1(seed, cx, cy, mtIndex); }
+
+// sim::BinnedBlinkRenderer (BinnedBlinks.cpp): Setup on the kernel cache h (null: the Gaussian of sigmaPx), then for
+// frames k < nFrames Render of emitters [frames[k].em_start, + em_count) (iscu_emitter: position, photons, z index in
+// plane & 0xFFFF) into img[k * w * hgt ..] (+=), frames in parallel on the reference's thread pool as its movie loop
+// runs them (one frame per worker, its FFT lines serial). u and R out (nullable). Returns the wall seconds of the
+// renders, or -1 when Setup refuses.
+double ref_binned_render(void* h, double sigmaPx, unsigned w, unsigned hgt, int upscale, const iscu_emitter* em,
+                         const iscu_frame* frames, uint32_t nFrames, float* img, int* uOut, int* rOut)
+{
+   sim::BinnedBlinkRenderer r;
+   if (!r.Setup(static_cast<const sim::PsfKernelCache*>(h), sigmaPx, w, hgt, upscale))
+      return -1.0;
+   if (uOut)
+      *uOut = r.Upscale();
+   if (rOut)
+      *rOut = r.RadiusCells();
+   const size_t px = static_cast<size_t>(w) * hgt;
+   const auto start = std::chrono::steady_clock::now();
+   sim::ParallelFor(nFrames, [&](unsigned k) {
+      std::vector<sim::FrameEmitter> list;
+      list.reserve(frames[k].em_count);
+      for (uint32_t i = frames[k].em_start; i < frames[k].em_start + frames[k].em_count; ++i)
+         list.push_back({em[i].x_px, em[i].y_px, em[i].photons, 1.0, em[i].plane & 0xFFFF});
+      std::vector<float> frame(img + k * px, img + (k + 1) * px);
+      r.Render(list, frame);
+      std::copy(frame.begin(), frame.end(), img + k * px);
+   });
+   return std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
+}
 
 } // extern "C"
