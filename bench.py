@@ -819,6 +819,75 @@ class ScheduleWorkload:
         return sec
 
 
+class TiffWorkload:
+    """The movie file: 200 frames of 512 x 512 uint16 ADU (100 MB) from device memory into a classic TIFF in the
+    box's temporary directory (iscu_tiff_pages_dev: 8 MB chunks through the context's two page-locked halves, each
+    chunk's copy beside the previous chunk's file writes; the description on page 1). No kernel runs: the pages are
+    the ADU frames as they are, so the device work is the copies. One step = open, 200 pages, close."""
+    name = ("movie file: 200 frames of 512x512 uint16 ADU from device memory to a classic TIFF (description on "
+            "page 1) in the temporary directory")
+    metric = "frames/s"
+    dtype = "u16"
+    cpu_kind = "reference"
+    DESC = "insiliscope movie frames=200 w=512 h=512"
+
+    def __init__(self, rank: int):
+        import tempfile
+        self.rank = rank
+        self.frames = np.random.default_rng(42 + rank).integers(0, 65536, (200, 512, 512)).astype(np.uint16)
+        self.dir = tempfile.mkdtemp(prefix="iscu_tiff_")
+        self.frames_per_step_cpu = 200
+        self.cpu_sample = ("all 200 frames per step: the reference's TiffWriter (cli/tiff_writer.h, compiled from its "
+                           "sources) writing them from host vectors, as the CLI does")
+
+    def setup(self, device: int):
+        import torch
+        from insiliscope_b200 import Engine
+        self.eng = Engine(device)
+        self.d_frames = torch.from_numpy(self.frames).to(f"cuda:{device}")
+        self.path = os.path.join(self.dir, f"movie_{self.rank}.tif")
+        self.stream = self.eng.torch_stream()
+        self.frames_per_step = len(self.frames)
+        self.n_emitters = 0
+        self.psf_build_ms = 0.0
+
+    def device_step(self):
+        from insiliscope_b200 import TiffWriter
+        with TiffWriter(self.path) as t:
+            t.pages_dev(self.eng, self.d_frames, self.DESC)
+
+    def e2e_step(self):
+        self.device_step()
+
+    def e2e_bytes(self):
+        return 0, self.frames.nbytes
+
+    def kernel_name(self):
+        return "pages from device memory (copies + file writes)"
+
+    def alg_bytes_per_launch(self):
+        return self.frames.nbytes   # each frame read from HBM once
+
+    def cpu_cores(self):
+        return 1
+
+    def reference_setup(self, threads=0):
+        from oracle.oracle import Reference
+        if not Reference.available():
+            raise RuntimeError("the reference harness oracle/_ref/libiscref.so is not built (it needs the reference "
+                               "tree at build time)")
+        self.ref = Reference()
+        self.ref_path = os.path.join(self.dir, f"movie_ref_{self.rank}.tif")
+
+    def reference_step(self):
+        t0 = time.perf_counter()
+        t = self.ref.tiff(self.ref_path)
+        for k in range(len(self.frames)):
+            t.page(self.frames[k], 512, 512, self.DESC if k == 0 else None)
+        t.close()
+        return time.perf_counter() - t0
+
+
 class BinnedWorkload:
     """The binned blink regime (the reference's approximate SMLM render of dense frames): 200 frames of 128 x 128 px
     with about 2,400 ON emitters each (12.7 per um^2, just above the reference's switch to binned at 12.5), deposited
@@ -937,7 +1006,7 @@ class BinnedWorkload:
 
 WORKLOADS = {"smlm": SmlmWorkload, "widefield": WidefieldWorkload, "psflib": PsfLibraryWorkload,
              "two-colour": TwoColourWorkload, "nll-grad": NllGradWorkload, "schedules": ScheduleWorkload,
-             "binned": BinnedWorkload}
+             "binned": BinnedWorkload, "tiff": TiffWorkload}
 
 
 # ----------------------------------------------------------------------------------------------------- arms

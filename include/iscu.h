@@ -37,7 +37,8 @@ enum iscu_status {
    ISCU_ERR_STATE = 3,   /* the context lacks what the call needs (no kernel in the slot, no camera maps) */
    ISCU_ERR_LIMIT = 4,   /* a size beyond a documented maximum */
    ISCU_ERR_TIMEOUT = 5, /* a bounded device-side wait ran out (the context stays usable) */
-   ISCU_ERR_NODEV = 6    /* no CUDA device, or not an sm_100 device */
+   ISCU_ERR_NODEV = 6,   /* no CUDA device, or not an sm_100 device */
+   ISCU_ERR_IO = 7       /* a file could not be opened or written (the message is the reference writer's) */
 };
 
 /* Interpolation of the splat's sub-pixel read (sim::PsfInterpMode, PsfGeneratorBridge.h:68-74). Fft has no GPU path
@@ -583,6 +584,36 @@ int iscu_buffer_read_low16(const iscu_buffer* src, size_t words, uint16_t* dst);
  * binding order (their count as the kernel's source binds them), x * y * z workgroups (y, z <= 65535). */
 int iscu_dispatch(iscu_ctx* ctx, const char* kernel, const uint32_t* params, size_t n_params,
                   iscu_buffer* const* bufs, size_t n_bufs, uint32_t x, uint32_t y, uint32_t z);
+
+/* ---------------------------------------------------------------- movie files ------------------------------------ */
+
+/* The CLI's movie file (TiffWriter, cli/tiff_writer.h), byte for byte: a little-endian baseline TIFF, one
+ * uncompressed grey page per frame -- uint16 ADU, or float32 -- with an optional description (the CLI gives one on
+ * page 1); a BigTIFF (64-bit offsets) when big_tiff is set or expected_bytes + 64 MB reaches 2^32 - 1, else a
+ * classic file that refuses a page that would pass 4 GB. Every page is flushed and checked; a failure leaves the
+ * writer failed (ISCU_ERR_IO, the reference writer's message) and the file as written so far. Not thread-safe per
+ * writer. iscu_tiff_bytes is TiffWriter::Bytes: an upper bound of a file's size, the expected_bytes to pass. */
+typedef struct iscu_tiff iscu_tiff;
+uint64_t iscu_tiff_bytes(uint64_t width, uint64_t height, uint64_t pages, uint64_t bytes_per_sample,
+                         uint64_t desc_bytes);
+int iscu_tiff_open(const char* path, uint64_t expected_bytes, int32_t big_tiff, iscu_tiff** out);
+/* Whether the file is a BigTIFF, its pages so far and its bytes (any output NULL). */
+int iscu_tiff_info(iscu_tiff* t, int32_t* big, uint64_t* pages, uint64_t* bytes);
+/* A page of w x h samples (desc NULL or "": none). */
+int iscu_tiff_page_u16(iscu_tiff* t, const uint16_t* px, uint32_t w, uint32_t h, const char* desc);
+int iscu_tiff_page_f32(iscu_tiff* t, const float* px, uint32_t w, uint32_t h, const char* desc);
+/* A uint16 page of which only rows 0 .. rows - 1 are given (rows x w samples), the rest left for iscu_tiff_rows
+ * (TiffWriter::PageRows / Rows: a movie written in strips; the finished file equals whole-page writes). */
+int iscu_tiff_page_rows(iscu_tiff* t, const uint16_t* px, uint32_t rows, uint32_t w, uint32_t h, const char* desc);
+int iscu_tiff_rows(iscu_tiff* t, uint64_t page, uint32_t y0, uint32_t rows, const uint16_t* px);
+/* n_frames uint16 frames of w x h from device memory (after the work enqueued on ctx's stream), one page each,
+ * first_desc on the first: the frames cross to the host in chunks of about 8 MB through two page-locked halves
+ * that the context keeps for all its writers, the copy of one chunk on a copy stream while the previous one is
+ * written. */
+int iscu_tiff_pages_dev(iscu_tiff* t, iscu_ctx* ctx, const uint16_t* frames_dev, uint32_t n_frames, uint32_t w,
+                        uint32_t h, const char* first_desc);
+/* Closes the file and frees the writer; ISCU_ERR_IO when a write (or this close) failed. */
+int iscu_tiff_close(iscu_tiff* t);
 
 /* ------------------------------------------------------- binned blinks (approximate SMLM) ----------------------- */
 

@@ -17,6 +17,7 @@ ISCU_ERR_STATE = 3
 ISCU_ERR_LIMIT = 4
 ISCU_ERR_TIMEOUT = 5
 ISCU_ERR_NODEV = 6
+ISCU_ERR_IO = 7
 
 INTERP_NEAREST, INTERP_LINEAR, INTERP_CUBIC = 0, 1, 2
 CZT_FP32, CZT_TF32X3 = 0, 1
@@ -170,6 +171,15 @@ SIGNATURES = {
     "iscu_buffer_read_low16": (C.c_int, [vp, C.c_size_t, vp]),
     "iscu_dispatch": (C.c_int, [vp, C.c_char_p, vp, C.c_size_t, vp, C.c_size_t, C.c_uint32, C.c_uint32,
                                 C.c_uint32]),
+    "iscu_tiff_bytes": (C.c_uint64, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64]),
+    "iscu_tiff_open": (C.c_int, [C.c_char_p, C.c_uint64, C.c_int32, vp]),
+    "iscu_tiff_info": (C.c_int, [vp, vp, vp, vp]),
+    "iscu_tiff_page_u16": (C.c_int, [vp, vp, C.c_uint32, C.c_uint32, C.c_char_p]),
+    "iscu_tiff_page_f32": (C.c_int, [vp, vp, C.c_uint32, C.c_uint32, C.c_char_p]),
+    "iscu_tiff_page_rows": (C.c_int, [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_char_p]),
+    "iscu_tiff_rows": (C.c_int, [vp, C.c_uint64, C.c_uint32, C.c_uint32, vp]),
+    "iscu_tiff_pages_dev": (C.c_int, [vp, vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_char_p]),
+    "iscu_tiff_close": (C.c_int, [vp]),
     "iscu_binned_create": (C.c_int, [vp, C.c_int32, C.c_double, C.c_uint32, C.c_uint32, C.c_int32, vp]),
     "iscu_binned_info": (C.c_int, [vp, vp, vp, vp]),
     "iscu_binned_kernels": (C.c_int, [vp, vp]),

@@ -36,6 +36,7 @@ UNITS = {
     "backend.cu": ["--fmad=false"],
     "schedule.cu": ["--fmad=false"],
     "binned.cu": [],
+    "tiff.cpp": [],
     "capi.cpp": [],
     "host_models.cpp": [],
 }

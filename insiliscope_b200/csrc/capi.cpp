@@ -256,6 +256,9 @@ void iscu_destroy(iscu_ctx* ctx)
       for (cudaEvent_t e : {io.uploaded, io.rendered, io.downloaded})
          if (e)
             cudaEventDestroy(e);
+   for (cudaEvent_t e : ctx->fileCopied)
+      if (e)
+         cudaEventDestroy(e);
    cudaStream_t streams[3] = {ctx->stream, ctx->upload, ctx->download};
    delete ctx;
    for (cudaStream_t c : streams)

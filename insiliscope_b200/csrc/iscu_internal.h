@@ -227,6 +227,9 @@ struct iscu_ctx
    // the event render's I/O slots (the last one is the blocking call's) and its copy streams (created on first use)
    iscu::EventIo eventIo[ISCU_EVENT_IO_SLOTS + 1];
    cudaStream_t upload = nullptr, download = nullptr;
+   // movie files from device frames (iscu_tiff_pages_dev): two page-locked halves, kept for the context's writers
+   iscu::PinnedBuf fileStage[2];
+   cudaEvent_t fileCopied[2] = {nullptr, nullptr};
    iscu::StaticView Static() const
    {
       iscu::StaticView s;

@@ -737,6 +737,78 @@ class WidefieldPlan:
         self._pending_io.pop(int(io_slot), None)
 
 
+class TiffWriter:
+    """iscu_tiff: the CLI's movie file (cli/tiff_writer.h) byte for byte -- classic TIFF or BigTIFF, one uncompressed
+    grey page per frame. Failures raise IscuError (code ISCU_ERR_IO) with the reference writer's message."""
+
+    def __init__(self, path, expected_bytes=0, big=False):
+        self.lib = load()
+        self.h = None
+        h = C.c_void_p()
+        check(self.lib.iscu_tiff_open(str(path).encode(), int(expected_bytes), int(big), C.byref(h)))
+        self.h = h
+
+    @staticmethod
+    def bytes(w, h, pages, bytes_per_sample, desc_bytes):
+        """TiffWriter::Bytes: an upper bound of the file's size (the expected_bytes to pass)."""
+        return int(load().iscu_tiff_bytes(w, h, pages, bytes_per_sample, desc_bytes))
+
+    @staticmethod
+    def _d(desc):
+        return None if desc is None else desc.encode()
+
+    def info(self):
+        """(is a BigTIFF, pages, bytes)."""
+        big, pages, n = C.c_int32(), C.c_uint64(), C.c_uint64()
+        check(self.lib.iscu_tiff_info(self.h, C.byref(big), C.byref(pages), C.byref(n)))
+        return bool(big.value), pages.value, n.value
+
+    def page(self, px, desc=None):
+        """One page of a (h, w) uint16 or float32 image."""
+        px = np.ascontiguousarray(px)
+        h, w = px.shape
+        if px.dtype == np.float32:
+            check(self.lib.iscu_tiff_page_f32(self.h, _ptr(px), w, h, self._d(desc)))
+        else:
+            px = np.ascontiguousarray(px, np.uint16)
+            check(self.lib.iscu_tiff_page_u16(self.h, _ptr(px), w, h, self._d(desc)))
+
+    def page_rows(self, px, w, h, desc=None):
+        """A uint16 page of w x h of which px (rows, w) holds the first rows; rows() fills the rest."""
+        px = np.ascontiguousarray(px, np.uint16)
+        check(self.lib.iscu_tiff_page_rows(self.h, _ptr(px), px.shape[0], w, h, self._d(desc)))
+
+    def rows(self, page, y0, px):
+        px = np.ascontiguousarray(px, np.uint16)
+        check(self.lib.iscu_tiff_rows(self.h, page, y0, px.shape[0], _ptr(px)))
+
+    def pages_dev(self, engine: Engine, frames_dev, first_desc=None):
+        """The (n, h, w) uint16 CUDA frames, one page each (iscu_tiff_pages_dev: copied out in chunks through two
+        page-locked halves while the previous chunk is written)."""
+        n, h, w = frames_dev.shape
+        frames_dev = frames_dev.contiguous()
+        check(self.lib.iscu_tiff_pages_dev(self.h, engine.h, _ptr(frames_dev), n, w, h, self._d(first_desc)))
+
+    def close(self):
+        if self.h:
+            h, self.h = self.h, None
+            check(self.lib.iscu_tiff_close(h))
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            if self.h:
+                self.lib.iscu_tiff_close(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
 class BinnedRenderer:
     """iscu_binned: the binned blink regime (sim::BinnedBlinkRenderer) for width x height frames, on kernel slot
     `slot` or (slot < 0) the in-focus Gaussian of sigma_px."""

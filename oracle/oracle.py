@@ -211,6 +211,18 @@ class Reference:
         L.ref_background_fade_scale.restype = f64
         L.ref_binned_render.argtypes = [vp, f64, C.c_uint, C.c_uint, C.c_int, vp, vp, u32, vp, vp, vp]
         L.ref_binned_render.restype = f64
+        u64 = C.c_uint64
+        L.ref_tiff_open.argtypes = [C.c_char_p, u64, C.c_int]
+        L.ref_tiff_open.restype = vp
+        L.ref_tiff_bytes.argtypes = [u64, u64, u64, u64, u64]
+        L.ref_tiff_bytes.restype = u64
+        L.ref_tiff_page_u16.argtypes = [vp, vp, C.c_size_t, u32, u32, C.c_char_p]
+        L.ref_tiff_page_f32.argtypes = [vp, vp, C.c_size_t, u32, u32, C.c_char_p]
+        L.ref_tiff_page_rows.argtypes = [vp, vp, u32, u32, u32, C.c_char_p]
+        L.ref_tiff_rows.argtypes = [vp, u64, u32, u32, vp]
+        L.ref_tiff_big.argtypes = [vp]
+        L.ref_tiff_error.argtypes = [vp, C.c_char_p, C.c_size_t]
+        L.ref_tiff_close.argtypes = [vp]
         self.L = L
 
     def set_threads(self, n):
@@ -334,6 +346,10 @@ class Reference:
                                           float(t1), _p(counts))
         return counts, sec
 
+    def tiff(self, path, expected_bytes=0, big=False):
+        """The reference's TiffWriter (cli/tiff_writer.h) on `path`."""
+        return RefTiff(self, path, expected_bytes, big)
+
     def binned_render(self, kernel, sigma_px, w, h, upscale, emitters, frames, img=None):
         """sim::BinnedBlinkRenderer: Setup on `kernel` (a RefKernel; None: the Gaussian of sigma_px), Render of each
         frame's emitters (EMITTER_DTYPE / FRAME_DTYPE records) into img (n, h, w) float32 (+=; zeros when None), frames
@@ -351,6 +367,45 @@ class Reference:
 
     def dye_h1(self, seed, cx, cy, mt_index):
         return int(self.L.ref_dye_h1(int(seed) & 0xFFFFFFFF, int(cx), int(cy), int(mt_index)))
+
+
+class RefTiff:
+    """A TiffWriter in the reference harness: page / page_rows / rows return the writer's bool, error() its
+    message."""
+
+    def __init__(self, ref, path, expected_bytes, big):
+        self.L = ref.L
+        self.h = self.L.ref_tiff_open(str(path).encode(), int(expected_bytes), int(big))
+
+    @staticmethod
+    def _d(desc):
+        return None if desc is None else desc.encode()
+
+    def page(self, px, w, h, desc=None):
+        px = np.ascontiguousarray(px)
+        fn = self.L.ref_tiff_page_f32 if px.dtype == np.float32 else self.L.ref_tiff_page_u16
+        return bool(fn(self.h, _p(px), px.size, w, h, self._d(desc)))
+
+    def page_rows(self, px, rows, w, h, desc=None):
+        px = np.ascontiguousarray(px, np.uint16)
+        return bool(self.L.ref_tiff_page_rows(self.h, _p(px), rows, w, h, self._d(desc)))
+
+    def rows(self, page, y0, rows, px):
+        px = np.ascontiguousarray(px, np.uint16)
+        return bool(self.L.ref_tiff_rows(self.h, page, y0, rows, _p(px)))
+
+    def big(self):
+        return bool(self.L.ref_tiff_big(self.h))
+
+    def error(self):
+        buf = C.create_string_buffer(4096)
+        self.L.ref_tiff_error(self.h, buf, 4096)
+        return buf.value.decode()
+
+    def close(self):
+        ok = bool(self.L.ref_tiff_close(self.h))
+        self.h = None
+        return ok
 
 
 def _geometry(req):

@@ -20,6 +20,7 @@
 #include "ZernikePsf.h"
 #include "dyes.h"
 #include "rng.h"
+#include "tiff_writer.h"
 
 #include "../include/iscu.h"
 
@@ -576,6 +577,43 @@ double ref_dye_blinks_batch(int mode, const double* kin, const double* histStart
 
 // The core's DyeH1 (dyes.cpp:175-178): H1 of microtubule mtIndex of cell (cx, cy).
 uint32_t ref_dye_h1(uint32_t seed, int32_t cx, int32_t cy, int mtIndex) { return isc::DyeH1(seed, cx, cy, mtIndex); }
+
+// The CLI's movie writer (cli/tiff_writer.h, header-only, included from where it lies): open, pages, row strips,
+// close. n_px: the samples px holds (the writer reads w x h of them only when the page is written).
+void* ref_tiff_open(const char* path, uint64_t expected, int big) { return new TiffWriter(path, expected, big != 0); }
+uint64_t ref_tiff_bytes(uint64_t w, uint64_t h, uint64_t pages, uint64_t bps, uint64_t desc)
+{
+   return TiffWriter::Bytes(w, h, pages, bps, desc);
+}
+int ref_tiff_page_u16(void* t, const uint16_t* px, size_t n_px, uint32_t w, uint32_t hgt, const char* desc)
+{
+   return static_cast<TiffWriter*>(t)->Page(std::vector<uint16_t>(px, px + n_px), w, hgt, desc ? desc : "") ? 1 : 0;
+}
+int ref_tiff_page_f32(void* t, const float* px, size_t n_px, uint32_t w, uint32_t hgt, const char* desc)
+{
+   return static_cast<TiffWriter*>(t)->Page(std::vector<float>(px, px + n_px), w, hgt, desc ? desc : "") ? 1 : 0;
+}
+int ref_tiff_page_rows(void* t, const uint16_t* px, uint32_t rows, uint32_t w, uint32_t hgt, const char* desc)
+{
+   return static_cast<TiffWriter*>(t)->PageRows(px, rows, w, hgt, desc ? desc : "") ? 1 : 0;
+}
+int ref_tiff_rows(void* t, uint64_t page, uint32_t y0, uint32_t rows, const uint16_t* px)
+{
+   return static_cast<TiffWriter*>(t)->Rows(page, y0, rows, px) ? 1 : 0;
+}
+int ref_tiff_big(void* t) { return static_cast<TiffWriter*>(t)->big() ? 1 : 0; }
+// The writer's message ("" when nothing went wrong), into out (cap bytes).
+void ref_tiff_error(void* t, char* out, size_t cap)
+{
+   std::snprintf(out, cap, "%s", static_cast<TiffWriter*>(t)->error().c_str());
+}
+int ref_tiff_close(void* t)
+{
+   auto* w = static_cast<TiffWriter*>(t);
+   const bool ok = w->Close();
+   delete w;
+   return ok ? 1 : 0;
+}
 
 // sim::BinnedBlinkRenderer (BinnedBlinks.cpp): Setup on the kernel cache h (null: the Gaussian of sigmaPx), then for
 // frames k < nFrames Render of emitters [frames[k].em_start, + em_count) (iscu_emitter: position, photons, z index in
