@@ -820,12 +820,14 @@ class ScheduleWorkload:
 
 
 class TiffWorkload:
-    """The movie file: 200 frames of 512 x 512 uint16 ADU (100 MB) from device memory into a classic TIFF in the
-    box's temporary directory (iscu_tiff_pages_dev: 8 MB chunks through the context's two page-locked halves, each
-    chunk's copy beside the previous chunk's file writes; the description on page 1). No kernel runs: the pages are
-    the ADU frames as they are, so the device work is the copies. One step = open, 200 pages, close."""
+    """The movie file: 200 frames of 512 x 512 uint16 ADU (100 MB) from device memory into a classic TIFF in
+    memory-backed storage (/dev/shm where the box has it, so that both arms time the writer, not the disk's
+    writeback; the temporary directory otherwise) (iscu_tiff_pages_dev: 8 MB chunks through the context's two
+    page-locked halves, each chunk's copy beside the previous chunk's file writes; the description on page 1). No
+    kernel runs: the pages are the ADU frames as they are, so the device work is the copies. One step = open, 200
+    pages, close."""
     name = ("movie file: 200 frames of 512x512 uint16 ADU from device memory to a classic TIFF (description on "
-            "page 1) in the temporary directory")
+            "page 1) in memory-backed storage")
     metric = "frames/s"
     dtype = "u16"
     cpu_kind = "reference"
@@ -835,7 +837,8 @@ class TiffWorkload:
         import tempfile
         self.rank = rank
         self.frames = np.random.default_rng(42 + rank).integers(0, 65536, (200, 512, 512)).astype(np.uint16)
-        self.dir = tempfile.mkdtemp(prefix="iscu_tiff_")
+        shm = "/dev/shm"
+        self.dir = tempfile.mkdtemp(prefix="iscu_tiff_", dir=shm if os.path.isdir(shm) else None)
         self.frames_per_step_cpu = 200
         self.cpu_sample = ("all 200 frames per step: the reference's TiffWriter (cli/tiff_writer.h, compiled from its "
                            "sources) writing them from host vectors, as the CLI does")
