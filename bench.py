@@ -819,6 +819,90 @@ class ScheduleWorkload:
         return sec
 
 
+class CsvWorkload:
+    """Ground-truth table text: 482,304 rows (the two-colour movie's emitter rows) of 20 numeric columns in the
+    tables' formats (frame %d, times and world positions %.6f, camera positions %.3f, photons %.4f, fractions %.6g,
+    wavelength %.4g), formatted as AppendCsvNumber writes each number and laid out as GroundTruth's rows. The
+    columns stay resident; one step = iscu_csv_table_dev (row lengths, scan, rows written; its total read back).
+    e2e: the float64 columns in, the text out."""
+    name = ("ground-truth table text: 482,304 rows x 20 numeric columns (%d, %.6f, %.3f, %.4f, %.6g, %.4g as the "
+            "emitter table uses them), AppendCsvNumber's printf rounding")
+    metric = "rows/s"
+    dtype = "f64"
+    cpu_kind = "reference"
+    FMTS = ["%d", "%.6f", "%.3f", "%.3f", "%.3f", "%.6f", "%.6f", "%.6f", "%.6f", "%.6f", "%.6f", "%.6g", "%.4f",
+            "%.4f", "%.4f", "%.4f", "%.4f", "%.4f", "%.4g", "%.6g"]
+
+    def __init__(self, rank: int):
+        rng = np.random.default_rng(42 + rank)
+        n = 482304
+        cols = [np.sort(rng.integers(0, 1024, n)).astype(np.float64), rng.integers(0, 1024, n) * 0.05]
+        cols += [rng.uniform(0, 27648, n), rng.uniform(0, 27648, n), rng.normal(0, 300, n)]   # x, y, z [nm]
+        cols += [rng.uniform(-14, 14, n) for _ in range(6)]                                     # world / site [um]
+        cols += [rng.random(n)]                                                                # on fraction
+        cols += [rng.lognormal(7, 1, n) for _ in range(6)]                                     # photons
+        cols += [rng.choice([580.0, 670.0], n), rng.random(n)]                                 # wavelength, excite
+        self.cols = np.ascontiguousarray(np.stack(cols))
+        self.frames_per_step_cpu = n
+        self.cpu_sample = ("all 482,304 rows per step: the reference's AppendCsvNumber per cell (CsvNumber.cpp, "
+                           "compiled from its sources) in GroundTruth's Rows chunks of 16,384 rows on its thread pool")
+
+    def setup(self, device: int):
+        import torch
+        from insiliscope_b200 import Engine
+        self.eng = Engine(device)
+        dev = f"cuda:{device}"
+        self.d_cols = torch.from_numpy(self.cols).to(dev)
+        text = self.eng.csv_table_dev(self.d_cols, self.FMTS)
+        self.n_text = text.numel()
+        self.d_out = torch.empty(self.n_text, dtype=torch.uint8, device=dev)
+        self.h_cols = torch.from_numpy(self.cols).pin_memory()
+        self.h_out = torch.empty(self.n_text, dtype=torch.uint8).pin_memory()
+        self.stream = self.eng.torch_stream()
+        self.frames_per_step = self.cols.shape[1]
+        self.n_emitters = 0
+        self.psf_build_ms = 0.0
+
+    def device_step(self):
+        self.eng.csv_table_dev(self.d_cols, self.FMTS, out_dev=self.d_out)
+
+    def e2e_step(self):
+        import torch
+        self.d_cols.copy_(self.h_cols, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        self.eng.csv_table_dev(self.d_cols, self.FMTS, out_dev=self.d_out)
+        self.h_out.copy_(self.d_out, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return self.h_out
+
+    def e2e_bytes(self):
+        return self.cols.nbytes, self.n_text
+
+    def kernel_name(self):
+        return "CsvRowLengthsKernel+CsvScanBlocksKernel+CsvWriteRowsKernel"
+
+    def alg_bytes_per_launch(self):
+        return 2 * self.cols.nbytes + self.n_text + self.cols.shape[1] * 4 * 2   # columns twice, text, row lengths
+
+    def config_extra(self):
+        return {"text_bytes": self.n_text}
+
+    def cpu_cores(self):
+        return self.ref.threads()
+
+    def reference_setup(self, threads=0):
+        from oracle.oracle import Reference
+        if not Reference.available():
+            raise RuntimeError("the reference harness oracle/_ref/libiscref.so is not built (it needs the reference "
+                               "tree at build time)")
+        self.ref = Reference()
+        self.ref.set_threads(threads)
+
+    def reference_step(self):
+        _, sec = self.ref.csv_table(self.cols, self.FMTS)
+        return sec
+
+
 class TiffWorkload:
     """The movie file: 200 frames of 512 x 512 uint16 ADU (100 MB) from device memory into a classic TIFF in
     memory-backed storage (/dev/shm where the box has it, so that both arms time the writer, not the disk's
@@ -1009,7 +1093,7 @@ class BinnedWorkload:
 
 WORKLOADS = {"smlm": SmlmWorkload, "widefield": WidefieldWorkload, "psflib": PsfLibraryWorkload,
              "two-colour": TwoColourWorkload, "nll-grad": NllGradWorkload, "schedules": ScheduleWorkload,
-             "binned": BinnedWorkload, "tiff": TiffWorkload}
+             "binned": BinnedWorkload, "tiff": TiffWorkload, "csv": CsvWorkload}
 
 
 # ----------------------------------------------------------------------------------------------------- arms

@@ -615,6 +615,22 @@ int iscu_tiff_pages_dev(iscu_tiff* t, iscu_ctx* ctx, const uint16_t* frames_dev,
 /* Closes the file and frees the writer; ISCU_ERR_IO when a write (or this close) failed. */
 int iscu_tiff_close(iscu_tiff* t);
 
+/* Ground-truth table text. Numbers as sim::AppendCsvNumber writes them (CsvNumber.cpp:13-32): printf's conversion of
+ * "%.<p>f" or "%.<p>g" (p one digit) in the "C" locale -- the exact binary value rounded half to even -- at most 47
+ * characters, nothing for NaN and infinities; "%d": the value (an integer, |v| < 2^53) as GroundTruth.cpp's Int
+ * writes it (std::to_chars). iscu_csv_numbers_dev: n values into 48-byte fields (the text, NUL-padded) and their
+ * lengths. */
+int iscu_csv_numbers_dev(iscu_ctx* ctx, const double* values_dev, uint32_t n, const char* fmt, char* fields_dev,
+                         uint8_t* lengths_dev);
+/* A numeric table's rows as GroundTruth's tables lay them out (GroundTruth::FramesCsv, GroundTruth.cpp:307-339):
+ * row r = its n_cols cells joined by ',' and ended by '
+', cell (r, c) = columns_dev[c * n_rows + r] in format
+ * fmts[c] (host array of n_cols <= 64 formats as above). The text goes to out_dev, *out_bytes its length; returns when
+ * it is written (synchronizes). When it needs more than out_capacity bytes, the first out_capacity are written,
+ * *out_bytes says how many it needs and the call returns ISCU_ERR_LIMIT. */
+int iscu_csv_table_dev(iscu_ctx* ctx, const double* columns_dev, uint32_t n_rows, uint32_t n_cols,
+                       const char* const* fmts, char* out_dev, uint64_t out_capacity, uint64_t* out_bytes);
+
 /* ------------------------------------------------------- binned blinks (approximate SMLM) ----------------------- */
 
 /* sim::BinnedBlinkRenderer (BinnedBlinks.h:35-60, BinnedBlinks.cpp:150-248): a frame's emitters deposited at the

@@ -37,6 +37,7 @@ UNITS = {
     "schedule.cu": ["--fmad=false"],
     "binned.cu": [],
     "tiff.cpp": [],
+    "csv.cu": [],
     "capi.cpp": [],
     "host_models.cpp": [],
 }

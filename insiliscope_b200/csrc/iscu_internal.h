@@ -229,6 +229,7 @@ struct iscu_ctx
    cudaStream_t upload = nullptr, download = nullptr;
    // movie files from device frames (iscu_tiff_pages_dev): two page-locked halves, kept for the context's writers
    iscu::PinnedBuf fileStage[2];
+   iscu::DevBuf dCsv;              // CSV tables: row lengths and block offsets
    cudaEvent_t fileCopied[2] = {nullptr, nullptr};
    iscu::StaticView Static() const
    {

@@ -281,6 +281,37 @@ class Engine:
                                                     int(normalize), _ptr(out)))
         return out
 
+    def csv_numbers_dev(self, values_dev, fmt, sync=True):
+        """AppendCsvNumber of each float64 CUDA value (iscu_csv_numbers_dev): (fields (n, 48) uint8, lengths (n,)
+        uint8) CUDA tensors."""
+        import torch
+        n = values_dev.numel()
+        fields = torch.empty((n, 48), dtype=torch.uint8, device=values_dev.device)
+        lens = torch.empty(n, dtype=torch.uint8, device=values_dev.device)
+        self._before(sync)
+        check(self.lib.iscu_csv_numbers_dev(self.h, _ptr(values_dev.contiguous()), n, fmt.encode(), _ptr(fields),
+                                            _ptr(lens)))
+        self._after(sync)
+        return fields, lens
+
+    def csv_table_dev(self, columns_dev, fmts, out_dev=None):
+        """A numeric table's rows (iscu_csv_table_dev; columns_dev (n_cols, n_rows) float64 CUDA): the text as a uint8
+        CUDA tensor (a view of out_dev when given, which must hold it)."""
+        import torch
+        cols = columns_dev.contiguous()
+        n_cols, n_rows = cols.shape
+        f = (C.c_char_p * n_cols)(*[x.encode() for x in fmts])
+        nbytes = C.c_uint64()
+        self._before(True)
+        if out_dev is None:
+            rc = self.lib.iscu_csv_table_dev(self.h, _ptr(cols), n_rows, n_cols, f, None, 0, C.byref(nbytes))
+            if rc != _abi.ISCU_ERR_LIMIT:
+                check(rc)
+            out_dev = torch.empty(max(1, nbytes.value), dtype=torch.uint8, device=cols.device)
+        check(self.lib.iscu_csv_table_dev(self.h, _ptr(cols), n_rows, n_cols, f, _ptr(out_dev), out_dev.numel(),
+                                          C.byref(nbytes)))
+        return out_dev[:nbytes.value]
+
     def kernel_build(self, slot, req: PsfParams, method=CZT_FP32):
         r = req.c()
         check(self.lib.iscu_kernel_build(self.h, slot, C.byref(r), method))

@@ -223,6 +223,9 @@ class Reference:
         L.ref_tiff_big.argtypes = [vp]
         L.ref_tiff_error.argtypes = [vp, C.c_char_p, C.c_size_t]
         L.ref_tiff_close.argtypes = [vp]
+        L.ref_csv_numbers.argtypes = [vp, u32, C.c_char_p, vp, vp]
+        L.ref_csv_table.argtypes = [vp, u32, u32, vp, vp, C.c_size_t]
+        L.ref_csv_table.restype = C.c_size_t
         self.L = L
 
     def set_threads(self, n):
@@ -345,6 +348,29 @@ class Reference:
         sec = self.L.ref_dye_blinks_batch(int(mode), _p(kin), _p(st), _p(hk), n_seg, _p(dyes), len(dyes), float(t0),
                                           float(t1), _p(counts))
         return counts, sec
+
+    def csv_numbers(self, values, fmt):
+        """sim::AppendCsvNumber of each value (CsvNumber.cpp): a list of str."""
+        v = np.ascontiguousarray(values, np.float64)
+        fields = np.zeros((len(v), 48), np.uint8)
+        lens = np.zeros(len(v), np.uint8)
+        self.L.ref_csv_numbers(_p(v), len(v), fmt.encode(), _p(fields), _p(lens))
+        return [bytes(fields[i, :lens[i]]).decode() for i in range(len(v))]
+
+    def csv_table(self, columns, fmts):
+        """A numeric table (columns: (n_cols, n_rows) float64) as GroundTruth's Rows formats it, on the reference's
+        thread pool: (the text as bytes, wall seconds)."""
+        import time
+        cols = np.ascontiguousarray(columns, np.float64)
+        n_cols, n_rows = cols.shape
+        f = (C.c_char_p * n_cols)(*[x.encode() for x in fmts])
+        t0 = time.perf_counter()
+        need = self.L.ref_csv_table(_p(cols), n_rows, n_cols, f, None, 0)
+        out = np.zeros(max(1, need), np.uint8)
+        t1 = time.perf_counter()
+        self.L.ref_csv_table(_p(cols), n_rows, n_cols, f, _p(out), need)
+        sec = time.perf_counter() - t1
+        return bytes(out[:need]), sec
 
     def tiff(self, path, expected_bytes=0, big=False):
         """The reference's TiffWriter (cli/tiff_writer.h) on `path`."""

@@ -9,6 +9,7 @@
 //   counter RNG (SMLMCounterRng.h, core/src/rng.h), and a movie loop shaped like FluorescenceMovie::Render's
 //   (ScopeMovie.cpp:7267, :7649: frames in parallel on the reference's own thread pool, ParallelFor).
 #include "BinnedBlinks.h"
+#include "CsvNumber.h"
 #include "Drift.h"
 #include "PsfGeneratorBridge.h"
 #include "SMLMBackground.h"
@@ -25,6 +26,7 @@
 #include "../include/iscu.h"
 
 #include <algorithm>
+#include <charconv>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -577,6 +579,56 @@ double ref_dye_blinks_batch(int mode, const double* kin, const double* histStart
 
 // The core's DyeH1 (dyes.cpp:175-178): H1 of microtubule mtIndex of cell (cx, cy).
 uint32_t ref_dye_h1(uint32_t seed, int32_t cx, int32_t cy, int mtIndex) { return isc::DyeH1(seed, cx, cy, mtIndex); }
+
+// sim::AppendCsvNumber (CsvNumber.cpp) of n values in format fmt: into 48-byte fields (NUL-padded) and lengths.
+void ref_csv_numbers(const double* v, uint32_t n, const char* fmt, char* fields, uint8_t* lens)
+{
+   for (uint32_t i = 0; i < n; ++i)
+   {
+      std::string s;
+      sim::AppendCsvNumber(s, v[i], fmt);
+      std::memset(fields + static_cast<size_t>(i) * 48, 0, 48);
+      std::memcpy(fields + static_cast<size_t>(i) * 48, s.data(), s.size());
+      lens[i] = static_cast<uint8_t>(s.size());
+   }
+}
+
+// A numeric table formatted as GroundTruth's Rows does it (GroundTruth.cpp:80-111: chunks of 16384 rows on the
+// thread pool, each row's cells by AppendCsvNumber -- or, for "%d", std::to_chars of the value -- joined by ',' and
+// ended by '\n'), columns column-major; the text into out (capacity cap), returns its length (or the length needed).
+size_t ref_csv_table(const double* cols, uint32_t nRows, uint32_t nCols, const char* const* fmts, char* out,
+                     size_t cap)
+{
+   const size_t kChunk = 16384;
+   const size_t chunks = (nRows + kChunk - 1) / kChunk;
+   std::vector<std::string> parts(chunks);
+   sim::ParallelFor(static_cast<unsigned>(chunks), [&](unsigned c) {
+      std::string& s = parts[c];
+      const size_t a = c * kChunk, b = std::min<size_t>(nRows, a + kChunk);
+      for (size_t r = a; r < b; ++r)
+         for (uint32_t k = 0; k < nCols; ++k)
+         {
+            const double v = cols[static_cast<size_t>(k) * nRows + r];
+            if (std::strcmp(fmts[k], "%d") == 0)
+            {
+               char t[24];
+               const std::to_chars_result e = std::to_chars(t, t + sizeof t, static_cast<long long>(v));
+               s.append(t, e.ptr);
+            }
+            else
+               sim::AppendCsvNumber(s, v, fmts[k]);
+            s += k + 1 < nCols ? ',' : '\n';
+         }
+   });
+   size_t n = 0;
+   for (const std::string& s : parts)
+   {
+      if (n + s.size() <= cap)
+         std::memcpy(out + n, s.data(), s.size());
+      n += s.size();
+   }
+   return n;
+}
 
 // The CLI's movie writer (cli/tiff_writer.h, header-only, included from where it lies): open, pages, row strips,
 // close. n_px: the samples px holds (the writer reads w x h of them only when the page is written).
