@@ -819,6 +819,105 @@ class ScheduleWorkload:
         return sec
 
 
+class FftPlaceWorkload:
+    """The splat's Fft placement (a next-row extra the reference runs on the CPU only): for 32,000 emitters (the
+    SMLM movie's 200 frames at 160 ON each: positions uniform over 128 x 128 px, planes over the 49 of its kernel,
+    129 x 129 samples at oversampling 4) each emitter's kernel plane shifted by its sub-cell offset and the shifted
+    plane's block sums (iscu_fft_place_dev). The records stay resident; one step = one call. e2e: records in, the
+    block sums and origins out."""
+    name = ("Fft placement: 32,000 emitters' shifted kernel planes (129 x 129 samples, 49 planes, oversampling 4) "
+            "and their block sums")
+    metric = "emitters/s"
+    dtype = "f64"
+    cpu_kind = "reference"
+
+    def __init__(self, rank: int):
+        from insiliscope_b200 import EMITTER_DTYPE
+        rng = np.random.default_rng(42 + rank)
+        n = 32000
+        em = np.zeros(n, EMITTER_DTYPE)
+        em["x_px"], em["y_px"] = rng.uniform(-0.5, 127.5, (2, n))
+        em["photons"] = 2000.0 * np.exp(0.5 * rng.normal(size=n))
+        em["plane"] = rng.integers(0, 49, n)
+        self.em = em
+        self.frames_per_step_cpu = 1024
+        self.cpu_sample = ("1,024 of the 32,000 emitters per step: the reference's PlanSplat with the Fft placement "
+                           "(FftShiftKernelTile's FFT row and column shifts, then BuildBlockSums; compiled from its "
+                           "sources) on its thread pool")
+
+    def _psf(self):
+        from insiliscope_b200.workloads import smlm_dstorm
+        return smlm_dstorm(frames=1).psf
+
+    def setup(self, device: int):
+        import torch
+        from insiliscope_b200 import Engine
+        self.eng = eng = Engine(device)
+        t0 = time.perf_counter()
+        eng.kernel_build(0, self._psf())
+        eng.synchronize()
+        self.psf_build_ms = (time.perf_counter() - t0) * 1e3
+        dev = f"cuda:{device}"
+        self.d_em = torch.from_numpy(self.em.view(np.uint8)).to(dev)
+        size, nz, os_, bw = eng.kernel_info(0)
+        n = len(self.em)
+        self.bw = bw
+        self.d_sums = torch.empty((n, bw, bw), dtype=torch.float32, device=dev)
+        self.d_org = torch.empty((n, 4), dtype=torch.int32, device=dev)
+        self.h_em = torch.from_numpy(self.em.view(np.uint8)).pin_memory()
+        self.h_sums = torch.empty((n, bw, bw), dtype=torch.float32).pin_memory()
+        self.h_org = torch.empty((n, 4), dtype=torch.int32).pin_memory()
+        self.stream = eng.torch_stream()
+        self.frames_per_step = n
+        self.n_emitters = n
+        self.plane_bytes = size * size * 4
+
+    def device_step(self):
+        from insiliscope_b200.engine import _ptr
+        from insiliscope_b200._abi import check
+        check(self.eng.lib.iscu_fft_place_dev(self.eng.h, 0, _ptr(self.d_em), len(self.em), _ptr(self.d_sums),
+                                              _ptr(self.d_org)))
+
+    def e2e_step(self):
+        import torch
+        self.d_em.copy_(self.h_em, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        self.device_step()
+        self.eng.synchronize()
+        self.h_sums.copy_(self.d_sums, non_blocking=True)
+        self.h_org.copy_(self.d_org, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return self.h_sums
+
+    def e2e_bytes(self):
+        return self.h_em.numel(), self.h_sums.numel() * 4 + self.h_org.numel() * 4
+
+    def kernel_name(self):
+        return "FftPlaceKernel"
+
+    def alg_bytes_per_launch(self):
+        # per emitter: its record, its plane read, its block sums and origin written
+        return len(self.em) * (32 + self.plane_bytes + self.bw * self.bw * 4 + 16)
+
+    def cpu_cores(self):
+        return self.ref.threads()
+
+    def reference_setup(self, threads=0):
+        from oracle.oracle import Reference
+        if not Reference.available():
+            raise RuntimeError("the reference harness oracle/_ref/libiscref.so is not built (it needs the reference "
+                               "tree at build time)")
+        self.ref = Reference()
+        self.ref.set_threads(threads)
+        self.ref_kernel = self.ref.kernel(req=self._psf())
+        k = self.frames_per_step_cpu
+        self.ref_xy = np.stack([self.em["x_px"][:k], self.em["y_px"][:k]], axis=1)
+        self.ref_z = self.em["plane"][:k].astype(np.int32)
+
+    def reference_step(self):
+        return self.ref_kernel.plan_splat_fft_batch(self.ref_xy, self.ref_z)
+
+
 class CsvWorkload:
     """Ground-truth table text: 482,304 rows (the two-colour movie's emitter rows) of 20 numeric columns in the
     tables' formats (frame %d, times and world positions %.6f, camera positions %.3f, photons %.4f, fractions %.6g,
@@ -1093,7 +1192,7 @@ class BinnedWorkload:
 
 WORKLOADS = {"smlm": SmlmWorkload, "widefield": WidefieldWorkload, "psflib": PsfLibraryWorkload,
              "two-colour": TwoColourWorkload, "nll-grad": NllGradWorkload, "schedules": ScheduleWorkload,
-             "binned": BinnedWorkload, "tiff": TiffWorkload, "csv": CsvWorkload}
+             "binned": BinnedWorkload, "tiff": TiffWorkload, "csv": CsvWorkload, "fftplace": FftPlaceWorkload}
 
 
 # ----------------------------------------------------------------------------------------------------- arms

@@ -615,6 +615,17 @@ int iscu_tiff_pages_dev(iscu_tiff* t, iscu_ctx* ctx, const uint16_t* frames_dev,
 /* Closes the file and frees the writer; ISCU_ERR_IO when a write (or this close) failed. */
 int iscu_tiff_close(iscu_tiff* t);
 
+/* The splat's Fft placement (PlanSplat with PsfInterpMode::Fft, PsfGeneratorBridge.cpp:1441-1456; the reference
+ * computes it on the CPU only): for emitters k < n of emitters_dev (z index = plane & 0xFFFF of slot `slot`'s stack),
+ * the kernel plane shifted by the emitter's sub-cell offset (FftShiftKernelTile, :1293-1370: g(i) = f(i + s),
+ * band-limited, s = t - floor(t + 0.5) of the nearest setup's tap coordinate t per axis) and its block sums
+ * (BuildBlockSums) into sums_dev[k * bw * bw ..] (bw = size + os - 1), and origins_dev[4k ..] = (x0, y0, bx, by): the
+ * centre pixel and the tap the one-tap splat reads those sums at. An emitter PlanSplat refuses (photons <= 0, a plane
+ * outside the stack) gets x0 = INT32_MIN and zero sums. Computed in float64 as the shift's convolution form (no
+ * transform); planes up to 161 x 161 samples. */
+int iscu_fft_place_dev(iscu_ctx* ctx, int32_t slot, const iscu_emitter* emitters_dev, uint32_t n_emitters,
+                       float* sums_dev, int32_t* origins_dev);
+
 /* Ground-truth table text. Numbers as sim::AppendCsvNumber writes them (CsvNumber.cpp:13-32): printf's conversion of
  * "%.<p>f" or "%.<p>g" (p one digit) in the "C" locale -- the exact binary value rounded half to even -- at most 47
  * characters, nothing for NaN and infinities; "%d": the value (an integer, |v| < 2^53) as GroundTruth.cpp's Int

@@ -38,6 +38,7 @@ UNITS = {
     "binned.cu": [],
     "tiff.cpp": [],
     "csv.cu": [],
+    "fft_place.cu": [],
     "capi.cpp": [],
     "host_models.cpp": [],
 }

@@ -281,6 +281,19 @@ class Engine:
                                                     int(normalize), _ptr(out)))
         return out
 
+    def fft_place_dev(self, slot, emitters_dev, sync=True):
+        """The Fft placement of each emitter (iscu_fft_place_dev; emitters: uint8 view of EMITTER_DTYPE records):
+        (shifted block sums (n, bw, bw) float32, origins (n, 4) int32: x0, y0, bx, by) CUDA tensors."""
+        import torch
+        n = _n_records(emitters_dev)
+        size, nz, os_, bw = self.kernel_info(slot)[:4]
+        sums = torch.empty((n, bw, bw), dtype=torch.float32, device=emitters_dev.device)
+        origins = torch.empty((n, 4), dtype=torch.int32, device=emitters_dev.device)
+        self._before(sync)
+        check(self.lib.iscu_fft_place_dev(self.h, slot, _ptr(emitters_dev), n, _ptr(sums), _ptr(origins)))
+        self._after(sync)
+        return sums, origins
+
     def csv_numbers_dev(self, values_dev, fmt, sync=True):
         """AppendCsvNumber of each float64 CUDA value (iscu_csv_numbers_dev): (fields (n, 48) uint8, lengths (n,)
         uint8) CUDA tensors."""

@@ -224,6 +224,10 @@ class Reference:
         L.ref_tiff_error.argtypes = [vp, C.c_char_p, C.c_size_t]
         L.ref_tiff_close.argtypes = [vp]
         L.ref_csv_numbers.argtypes = [vp, u32, C.c_char_p, vp, vp]
+        L.ref_plan_splat_fft.argtypes = [vp, f64, f64, C.c_int, vp, vp]
+        L.ref_plan_splat_fft.restype = C.c_int
+        L.ref_plan_splat_fft_batch.argtypes = [vp, vp, vp, u32]
+        L.ref_plan_splat_fft_batch.restype = f64
         L.ref_csv_table.argtypes = [vp, u32, u32, vp, vp, C.c_size_t]
         L.ref_csv_table.restype = C.c_size_t
         self.L = L
@@ -479,6 +483,21 @@ class RefKernel:
         self.ref.L.ref_kernel_block_sums(self.h, _p(out))
         return out
 
+    def plan_splat_fft(self, x, y, z):
+        """PlanSplat with the Fft placement: (shifted block sums (bw, bw) float32, (x0, y0, bx, by))."""
+        size, nz, os_, bw = self.info()
+        sums = np.zeros((bw, bw), np.float32)
+        st = np.zeros(4, np.int32)
+        if not self.ref.L.ref_plan_splat_fft(self.h, x, y, z, _p(sums), _p(st)):
+            raise RuntimeError("PlanSplat refused")
+        return sums, tuple(int(v) for v in st)
+
+    def plan_splat_fft_batch(self, xy, z):
+        """PlanSplat (Fft) for each emitter on the reference's pool; wall seconds."""
+        xy = np.ascontiguousarray(xy, np.float64)
+        z = np.ascontiguousarray(z, np.int32)
+        return self.ref.L.ref_plan_splat_fft_batch(self.h, _p(xy), _p(z), len(z))
+
     def halo(self, threshold):
         return RefKernel(self.ref, handle=self.ref.L.ref_kernel_halo(self.h, threshold))
 
@@ -602,6 +621,42 @@ def binned_render_f64(K, u, R, emitters, frames, w, h):
         cells = np.maximum(cells, np.float32(0)).astype(np.float64)
         out[k] = cells.reshape(h, u, w, u).sum(axis=(1, 3)).astype(np.float32)
     return out
+
+
+def fft_shift_tile_f64(plane, shift_x, shift_y):
+    """FftShiftKernelTile (PsfGeneratorBridge.cpp:1293-1370) in float64: each row of the n x n plane zero-padded to
+    N (the power of two >= 2n), transformed, times exp(2 pi i kk shift / N) with kk the wrapped frequency (k - N from
+    N/2 on), transformed back over N, the first n kept (complex); then the same along the columns of that; the real
+    part as float32 -- g(i) = f(i + shift), band-limited."""
+    P = np.asarray(plane, np.float64)
+    n = P.shape[0]
+    N = 1
+    while N < 2 * n:
+        N <<= 1
+    kk = np.arange(N)
+    kk = np.where(kk < N // 2, kk, kk - N)
+
+    def shift_lines(a, s):   # lines along the last axis
+        A = np.fft.fft(a, N, axis=-1) * np.exp(2j * np.pi * kk * s / N)
+        return np.fft.ifft(A, axis=-1)[..., :n]
+
+    mid = shift_lines(P, shift_x)
+    out = shift_lines(mid.T, shift_y).T
+    return out.real.astype(np.float32)
+
+
+def fft_place_f64(planes, os_, x, y, z):
+    """The Fft placement of one emitter (PlanSplat, PsfGeneratorBridge.cpp:1441-1456): the nearest setup's centre
+    pixel x0 = floor(x + 0.5) and tap origin t = kc + (x0 - x - 0.5) os + 0.5 (kc = (n - 1) / 2), its rounding half up
+    r = floor(t + 0.5), the plane shifted by (tx - rx, ty - ry); returns (the shifted plane, (x0, y0, rx, ry))."""
+    P = np.asarray(planes[z])
+    n = P.shape[0]
+    kc = (n - 1) / 2.0
+    x0, y0 = int(np.floor(x + 0.5)), int(np.floor(y + 0.5))
+    tx = kc + (x0 - x - 0.5) * os_ + 0.5
+    ty = kc + (y0 - y - 0.5) * os_ + 0.5
+    rx, ry = np.floor(tx + 0.5), np.floor(ty + 0.5)
+    return fft_shift_tile_f64(P, tx - rx, ty - ry), (x0, y0, int(rx), int(ry))
 
 
 def fft_convolve_same_f64(volume: np.ndarray, psf: np.ndarray) -> np.ndarray:

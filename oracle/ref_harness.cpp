@@ -580,6 +580,40 @@ double ref_dye_blinks_batch(int mode, const double* kin, const double* histStart
 // The core's DyeH1 (dyes.cpp:175-178): H1 of microtubule mtIndex of cell (cx, cy).
 uint32_t ref_dye_h1(uint32_t seed, int32_t cx, int32_t cy, int mtIndex) { return isc::DyeH1(seed, cx, cy, mtIndex); }
 
+// PlanSplat with the Fft placement (PsfGeneratorBridge.cpp:1441-1456) for an emitter at (x, y) px on plane z of
+// kernel cache h: its shifted block sums (bw x bw floats) into sums and (x0, y0, bx, by) into st4. Returns bw, or 0
+// when PlanSplat refuses.
+int ref_plan_splat_fft(void* h, double x, double y, int z, float* sums, int* st4)
+{
+   const auto* c = static_cast<const sim::PsfKernelCache*>(h);
+   sim::SplatPlan plan;
+   if (!sim::PlanSplat(*c, z, x, y, 1.0, sim::PsfInterpMode::Fft, plan, false))
+      return 0;
+   std::copy(plan.shiftedSums.begin(), plan.shiftedSums.end(), sums);
+   st4[0] = plan.st.x0;
+   st4[1] = plan.st.y0;
+   st4[2] = plan.st.bx;
+   st4[3] = plan.st.by;
+   return c->blockSumWidth;
+}
+
+// The same for n emitters (x, y, z), emitters in parallel on the reference's pool; wall seconds.
+double ref_plan_splat_fft_batch(void* h, const double* xy, const int* z, uint32_t n)
+{
+   const auto* c = static_cast<const sim::PsfKernelCache*>(h);
+   const auto t0 = std::chrono::steady_clock::now();
+   const unsigned chunks = std::max(1u, std::min(n, 256u));
+   sim::ParallelFor(chunks, [&](unsigned k) {
+      for (uint32_t i = static_cast<uint32_t>(static_cast<uint64_t>(n) * k / chunks);
+           i < static_cast<uint32_t>(static_cast<uint64_t>(n) * (k + 1) / chunks); ++i)
+      {
+         sim::SplatPlan plan;
+         sim::PlanSplat(*c, z[i], xy[2 * i], xy[2 * i + 1], 1.0, sim::PsfInterpMode::Fft, plan, false);
+      }
+   });
+   return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
 // sim::AppendCsvNumber (CsvNumber.cpp) of n values in format fmt: into 48-byte fields (NUL-padded) and lengths.
 void ref_csv_numbers(const double* v, uint32_t n, const char* fmt, char* fields, uint8_t* lens)
 {
