@@ -622,9 +622,17 @@ int iscu_tiff_close(iscu_tiff* t);
  * (BuildBlockSums) into sums_dev[k * bw * bw ..] (bw = size + os - 1), and origins_dev[4k ..] = (x0, y0, bx, by): the
  * centre pixel and the tap the one-tap splat reads those sums at. An emitter PlanSplat refuses (photons <= 0, a plane
  * outside the stack) gets x0 = INT32_MIN and zero sums. Computed in float64 as the shift's convolution form (no
- * transform); planes up to 161 x 161 samples. */
+ * transform); planes up to 157 x 157 samples. */
 int iscu_fft_place_dev(iscu_ctx* ctx, int32_t slot, const iscu_emitter* emitters_dev, uint32_t n_emitters,
                        float* sums_dev, int32_t* origins_dev);
+/* Frames rendered with the Fft placement (RenderPhotonImage for a kernel whose interpolation is Fft): as
+ * iscu_render_frames_dev -- background, every emitter of the frame in list order, the noise chain unless cam is
+ * NULL -- with every emitter on slot `slot` (z index = plane & 0xFFFF) placed by iscu_fft_place_dev and splatted at
+ * its one tap from its own shifted block sums, inside its square and the slot's halo cut. The placements live in a
+ * context buffer of n_emitters x (size + os - 1)^2 floats (batches up to 16 GB of it). */
+int iscu_render_fft_frames_dev(iscu_ctx* ctx, int32_t slot, const iscu_emitter* emitters_dev, uint32_t n_emitters,
+                               const iscu_frame* frames_dev, uint32_t n_frames, const iscu_camera* cam, uint32_t seed,
+                               float* photons_dev, uint16_t* adu_dev);
 
 /* Ground-truth table text. Numbers as sim::AppendCsvNumber writes them (CsvNumber.cpp:13-32): printf's conversion of
  * "%.<p>f" or "%.<p>g" (p one digit) in the "C" locale -- the exact binary value rounded half to even -- at most 47

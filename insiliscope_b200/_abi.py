@@ -172,6 +172,8 @@ SIGNATURES = {
     "iscu_dispatch": (C.c_int, [vp, C.c_char_p, vp, C.c_size_t, vp, C.c_size_t, C.c_uint32, C.c_uint32,
                                 C.c_uint32]),
     "iscu_fft_place_dev": (C.c_int, [vp, C.c_int32, vp, C.c_uint32, vp, vp]),
+    "iscu_render_fft_frames_dev": (C.c_int, [vp, C.c_int32, vp, C.c_uint32, vp, C.c_uint32, C.POINTER(Camera), C.c_uint32,
+                                             vp, vp]),
     "iscu_csv_numbers_dev": (C.c_int, [vp, vp, C.c_uint32, C.c_char_p, vp, vp]),
     "iscu_csv_table_dev": (C.c_int, [vp, vp, C.c_uint32, C.c_uint32, vp, vp, C.c_uint64, vp]),
     "iscu_tiff_bytes": (C.c_uint64, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64]),

@@ -38,7 +38,7 @@ UNITS = {
     "binned.cu": [],
     "tiff.cpp": [],
     "csv.cu": [],
-    "fft_place.cu": [],
+    "fft_place.cu": ["--fmad=false"],
     "capi.cpp": [],
     "host_models.cpp": [],
 }

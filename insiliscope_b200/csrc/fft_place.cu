@@ -9,12 +9,21 @@
 // convolution: y[i] = sum_j x[j] h(i - j + s) with h(t) = (1/N) sum_kk exp(2 pi i kk t / N), whose geometric sum is
 //   h(t) = sin(pi t) / (N tan(pi t / N)) - i sin(pi t) / N        (t not an integer;  h(d) = [d == 0] for integers),
 // so each emitter is 2 n^3 complex multiply-adds in float64 with no transform: a CTA per emitter holds the plane and
-// the shifted plane in shared memory, evaluates h for the 2n - 1 offsets of each axis once, and produces four output
+// the shifted plane in shared memory, evaluates h for the 2n - 1 offsets of each axis once, and produces eight output
 // columns per pass (each a row pass for those columns, then their column pass), so the complex intermediate is never
 // stored whole. The shifted plane's block sums follow as BuildBlockSums (PsfGeneratorBridge.cpp:1021-1047) forms
 // them: float64 row sums over each os x os block, then their sum, rounded to float.
+//
+// Frames in the Fft placement (RenderPhotonImage with a kernel whose interpolation is Fft, SMLMSimulation.cpp:103-160,
+// SplatRows / SplatKernel.inl with one tap): a CTA per 16 x 16 pixels of a frame starts each pixel at its background,
+// stages the frame's emitters whose square reaches the tile (in list order, 256 at a time) and adds, per pixel in
+// that order, float(photons x the emitter's shifted sums at (by + dy os + os - 1, bx + dx os + os - 1)) where the
+// pixel lies in the square and the halo cut's span; then the photon frame and/or the noise chain. Compiled with
+// --fmad=false for the noise chain's exactness (the shift's explicit fma calls are unaffected).
 
 #include "iscu_internal.h"
+#include "noise_chain.cuh"
+#include "splat_common.cuh"
 
 #include <climits>
 
@@ -22,8 +31,8 @@ namespace iscu {
 namespace {
 
 constexpr int kThreads = 192;   // one thread per row / output index
-constexpr int kCols = 4;        // output columns per pass
-constexpr int kMaxN = 161;     // 2 n^2 floats + (6 n - 2) complex doubles within 227 KB of shared memory
+constexpr int kCols = 8;        // output columns per pass (independent float64 chains per thread)
+constexpr int kMaxN = 157;     // 2 n^2 floats + (12 n - 2) complex doubles within 227 KB of shared memory
 
 size_t PlaceSmem(int n)
 {
@@ -90,7 +99,7 @@ __global__ void __launch_bounds__(kThreads) FftPlaceKernel(const iscu_emitter* _
    const int r = threadIdx.x;
    for (int c0 = 0; c0 < n; c0 += kCols)
    {
-      // row pass for columns c0 .. c0 + 3: M[c][y] = sum_j K[y][j] h_x(c0 + c - j)
+      // row pass for columns c0 .. c0 + 7: M[c][y] = sum_j K[y][j] h_x(c0 + c - j)
       if (r < n)
       {
          double re[kCols] = {}, im[kCols] = {};
@@ -160,6 +169,106 @@ __global__ void __launch_bounds__(kThreads) FftPlaceKernel(const iscu_emitter* _
    }
 }
 
+constexpr int kTile = 16;   // render: 16 x 16 pixels, one thread each
+
+struct FftStaged
+{
+   double photons;
+   const float* sums;   // the emitter's shifted block sums
+   const int16_t* spanLo;
+   const int16_t* spanHi;
+   int x0, y0, bx, by;
+};
+
+// grid (ceil(W / 16), ceil(H / 16), frames). Frame k's emitters are ems[em_start, + em_count) cut at nEm; emitter e's
+// placement is sums[e * bw * bw ..] and origins[4e ..] (x0 = INT32_MIN: not drawn).
+__global__ void __launch_bounds__(kTile * kTile) RenderFftKernel(const iscu_emitter* __restrict__ ems, uint32_t nEm,
+                                                                const iscu_frame* __restrict__ frames,
+                                                                const float* __restrict__ sums,
+                                                                const int32_t* __restrict__ origins, KernelView kv,
+                                                                StaticView st, CameraView cam, int noise,
+                                                                uint32_t seed, float* __restrict__ photonsOut,
+                                                                uint16_t* __restrict__ aduOut)
+{
+   __shared__ FftStaged sEm[kTile * kTile];
+   __shared__ int sWarp[kTile * kTile / 32];
+   const int W = static_cast<int>(st.width), H = static_cast<int>(st.height);
+   const int tx0 = blockIdx.x * kTile, ty0 = blockIdx.y * kTile;
+   const int X = tx0 + (threadIdx.x & (kTile - 1)), Y = ty0 + (threadIdx.x >> 4);
+   const int tx1 = min(tx0 + kTile, W) - 1, ty1 = min(ty0 + kTile, H) - 1;
+   const bool inside = X < W && Y < H;
+   const uint32_t i = static_cast<uint32_t>(Y) * st.width + static_cast<uint32_t>(X);
+   const iscu_frame fr = frames[blockIdx.z];
+   const int os = kv.os, off = os - 1, bw = kv.bw, cr = kv.camRad, sq = 2 * cr + 1;
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   float acc = inside ? Background(st, i, fr.bg_scale) : 0.0f;
+   const uint32_t count = fr.em_start < nEm ? min(fr.em_count, nEm - fr.em_start) : 0u;
+   for (uint32_t e0 = 0; e0 < count; e0 += kTile * kTile)
+   {
+      FftStaged s;
+      bool keep = false;
+      const uint32_t e = fr.em_start + e0 + threadIdx.x;
+      if (e0 + threadIdx.x < count)
+      {
+         const int x0 = origins[4 * e];
+         if (x0 != INT32_MIN)
+         {
+            s.x0 = x0;
+            s.y0 = origins[4 * e + 1];
+            keep = s.x0 + cr >= tx0 && s.x0 - cr <= tx1 && s.y0 + cr >= ty0 && s.y0 - cr <= ty1;
+            s.bx = origins[4 * e + 2];
+            s.by = origins[4 * e + 3];
+            s.photons = ems[e].photons;
+            s.sums = sums + static_cast<size_t>(e) * bw * bw;
+            const int plane = ems[e].plane & 0xFFFF;
+            s.spanLo = kv.spanLo ? kv.spanLo + plane * sq : nullptr;
+            s.spanHi = kv.spanHi ? kv.spanHi + plane * sq : nullptr;
+         }
+      }
+      const unsigned ballot = __ballot_sync(0xFFFFFFFFu, keep);
+      if (lane == 0)
+         sWarp[warp] = __popc(ballot);
+      __syncthreads();
+      int base = 0, total = 0;
+#pragma unroll
+      for (int w = 0; w < kTile * kTile / 32; ++w)
+      {
+         base += w < warp ? sWarp[w] : 0;
+         total += sWarp[w];
+      }
+      if (keep)
+         sEm[base + __popc(ballot & ((1u << lane) - 1u))] = s;
+      __syncthreads();
+      if (inside)
+         for (int k = 0; k < total; ++k)
+         {
+            const FftStaged& t = sEm[k];
+            const int dx = X - t.x0, dy = Y - t.y0;
+            if (dx < -cr || dx > cr || dy < -cr || dy > cr)
+               continue;
+            if (t.spanLo && (dx < t.spanLo[dy + cr] || dx > t.spanHi[dy + cr]))
+               continue;
+            const int r0 = t.by + dy * os + off, c0 = t.bx + dx * os + off;
+            // one tap (weights 1): the sums value, or nothing outside the array (the reference's skipped tap)
+            const double sum = r0 >= 0 && r0 < bw && c0 >= 0 && c0 < bw
+                                  ? 1.0 * (1.0 * static_cast<double>(__ldg(t.sums + r0 * bw + c0)))
+                                  : 0.0;
+            acc += static_cast<float>(t.photons * sum);
+         }
+      __syncthreads();
+   }
+   if (!inside)
+      return;
+   const size_t o = static_cast<size_t>(blockIdx.z) * st.width * st.height + i;
+   if (photonsOut)
+      photonsOut[o] = acc;
+   if (noise)
+   {
+      CounterRng u(seed, fr.frame);
+      aduOut[o] = NoisePixel(acc, i, cam, st, u);
+   }
+}
+
 } // namespace
 } // namespace iscu
 
@@ -180,7 +289,7 @@ int iscu_fft_place_dev(iscu_ctx* ctx, int32_t slot, const iscu_emitter* emitters
    if (!k.valid)
       return Fail(ISCU_ERR_STATE, "no kernel stack in slot " + std::to_string(slot));
    if (k.size > kMaxN)
-      return Fail(ISCU_ERR_LIMIT, "the Fft placement takes planes of up to 161 x 161 samples");
+      return Fail(ISCU_ERR_LIMIT, "the Fft placement takes planes of up to 157 x 157 samples");
    if (!n_emitters)
       return ISCU_OK;
    if (n_emitters > 0x7FFFFFFFu)
@@ -190,6 +299,45 @@ int iscu_fft_place_dev(iscu_ctx* ctx, int32_t slot, const iscu_emitter* emitters
    FftPlaceKernel<<<n_emitters, kThreads, smem, ctx->stream>>>(emitters_dev, k.planes.as<float>(), k.size, k.nz,
                                                                std::max(1, k.os), sums_dev, origins_dev);
    ISCU_CK_LAUNCH(ctx, "FftPlaceKernel");
+   return ISCU_OK;
+}
+
+int iscu_render_fft_frames_dev(iscu_ctx* ctx, int32_t slot, const iscu_emitter* emitters_dev, uint32_t n_emitters,
+                               const iscu_frame* frames_dev, uint32_t n_frames, const iscu_camera* cam, uint32_t seed,
+                               float* photons_dev, uint16_t* adu_dev)
+{
+   if (!ctx || (n_emitters && !emitters_dev) || (n_frames && !frames_dev) || (cam && !adu_dev) ||
+       (!cam && !photons_dev))
+      return Fail(ISCU_ERR_ARG, "null argument");
+   if (slot < 0 || slot >= ISCU_MAX_KERNELS)
+      return Fail(ISCU_ERR_ARG, "kernel slot out of range (0..3)");
+   if (n_frames > 65535)
+      return Fail(ISCU_ERR_LIMIT, "at most 65535 frames per call");
+   std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+   ClearError();
+   if (!ctx->haveStatic)
+      return Fail(ISCU_ERR_STATE, "no camera statics (iscu_set_static)");
+   const KernelSlot& k = ctx->kernels[slot];
+   if (!k.valid)
+      return Fail(ISCU_ERR_STATE, "no kernel stack in slot " + std::to_string(slot));
+   if (!n_frames)
+      return ISCU_OK;
+   const size_t bw = static_cast<size_t>(k.bw), per = bw * bw * sizeof(float);
+   if (static_cast<size_t>(n_emitters) * per > (size_t(16) << 30))
+      return Fail(ISCU_ERR_LIMIT, "the batch's shifted block sums pass 16 GB: split the frames");
+   ISCU_CK(ctx->dFftPlace.Reserve(std::max<size_t>(1, n_emitters) * (per + 16)));
+   float* sums = ctx->dFftPlace.as<float>();
+   int32_t* origins = reinterpret_cast<int32_t*>(ctx->dFftPlace.as<char>() + static_cast<size_t>(n_emitters) * per);
+   int rc = iscu_fft_place_dev(ctx, slot, emitters_dev, n_emitters, sums, origins);
+   if (rc != ISCU_OK)
+      return rc;
+   StaticView st = ctx->Static();
+   const CameraView cv = cam ? MakeCameraView(*cam) : CameraView();
+   const dim3 grid((st.width + kTile - 1) / kTile, (st.height + kTile - 1) / kTile, n_frames);
+   RenderFftKernel<<<grid, kTile * kTile, 0, ctx->stream>>>(emitters_dev, n_emitters, frames_dev, sums, origins,
+                                                            k.View(), st, cv, cam ? 1 : 0, seed, photons_dev,
+                                                            adu_dev);
+   ISCU_CK_LAUNCH(ctx, "RenderFftKernel");
    return ISCU_OK;
 }
 

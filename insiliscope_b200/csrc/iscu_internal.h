@@ -230,6 +230,7 @@ struct iscu_ctx
    // movie files from device frames (iscu_tiff_pages_dev): two page-locked halves, kept for the context's writers
    iscu::PinnedBuf fileStage[2];
    iscu::DevBuf dCsv;              // CSV tables: row lengths and block offsets
+   iscu::DevBuf dFftPlace;         // Fft-placement frames: each emitter's shifted block sums and origin
    cudaEvent_t fileCopied[2] = {nullptr, nullptr};
    iscu::StaticView Static() const
    {

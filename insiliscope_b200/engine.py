@@ -294,6 +294,16 @@ class Engine:
         self._after(sync)
         return sums, origins
 
+    def render_fft_frames_dev(self, slot, emitters_dev, frames_dev, n_frames, camera: CameraParams | None, seed,
+                              photons_dev=None, adu_dev=None, sync=True):
+        """Frames with the Fft placement (iscu_render_fft_frames_dev) on torch CUDA buffers, as render_frames_dev."""
+        cam = camera.c() if camera is not None else None
+        self._before(sync)
+        check(self.lib.iscu_render_fft_frames_dev(self.h, slot, _ptr(emitters_dev), _n_records(emitters_dev),
+                                                  _ptr(frames_dev), n_frames, C.byref(cam) if cam is not None else None,
+                                                  seed, _ptr(photons_dev), _ptr(adu_dev)))
+        self._after(sync)
+
     def csv_numbers_dev(self, values_dev, fmt, sync=True):
         """AppendCsvNumber of each float64 CUDA value (iscu_csv_numbers_dev): (fields (n, 48) uint8, lengths (n,)
         uint8) CUDA tensors."""
