@@ -819,6 +819,112 @@ class ScheduleWorkload:
         return sec
 
 
+class WfShiftWorkload:
+    """Frames of a drifting widefield sample (RenderShiftedImages, a next-row widefield extra): 64 frames on a 1024 x
+    1024 grid from 6 channels' spectra (two foci of a persistent and two bleaching populations), each frame its own
+    bleach coefficients, focus weight and xy drift (sub-cell pose included), a 1024 x 1024 window at 2 cells per pixel
+    -> 512 x 512 camera frames. The spectra stay resident; one step = iscu_wf_shifted_frames_dev. e2e: the frames'
+    coefficients and shifts in, the camera frames out."""
+    name = ("drifting widefield frames: 64 frames from 6 channel spectra on a 1024x1024 grid (two foci, bleach "
+            "basis, drift phase ramp), 2 cells per pixel -> 512x512")
+    metric = "frames/s"
+    dtype = "f32"
+    cpu_kind = "reference"
+    NX = NY = 1024
+    UP = 2
+
+    def __init__(self, rank: int):
+        rng = np.random.default_rng(42 + rank)
+        nx, ny = self.NX, self.NY
+        fy = np.fft.fftfreq(ny)[:, None]
+        fx = np.fft.rfftfreq(nx)[None, :]
+        band = np.exp(-(fx ** 2 + fy ** 2) / (2 * 0.08 ** 2))
+        self.spectra = np.stack([(np.fft.rfft2(rng.random((ny, nx)).astype(np.float32) ** 4 * 50) * band)
+                                 .astype(np.complex64) for _ in range(6)])
+        n = 64
+        self.a = rng.uniform(0.2, 1.0, (n, 2))
+        self.w = rng.uniform(0.0, 1.0, n)
+        self.drift = rng.uniform(-6.0, 6.0, (n, 2))
+        self.frac = (0.25, -0.125)
+        f32 = np.float32
+        coef = np.zeros((n, 6), np.float32)
+        for f in range(n):
+            w0, w1 = f32(1.0 - self.w[f]), f32(self.w[f])
+            coef[f] = [w0, f32(self.a[f, 0]) * w0, f32(self.a[f, 1]) * w0, w1, f32(self.a[f, 0]) * w1,
+                       f32(self.a[f, 1]) * w1]
+        self.coef = coef
+        self.shift = np.stack([self.frac[0] - self.drift[:, 0], self.frac[1] - self.drift[:, 1]], axis=1)
+        self.window = (0, 0, nx, ny)
+        self.frames_per_step_cpu = 8
+        self.cpu_sample = ("8 of the 64 frames per step: the reference's RenderShiftedImages (WidefieldRender.cpp, "
+                           "RealFft2d's float transforms on its thread pool; compiled from its sources) per frame")
+
+    def setup(self, device: int):
+        import torch
+        from insiliscope_b200 import Engine, WidefieldShift
+        self.eng = Engine(device)
+        dev = f"cuda:{device}"
+        self.plan = WidefieldShift(self.eng, self.NX, self.NY)
+        self.d_spec = torch.from_numpy(self.spectra).to(dev)
+        self.d_coef = torch.from_numpy(self.coef).to(dev)
+        self.d_shift = torch.from_numpy(self.shift).to(dev)
+        n = len(self.coef)
+        shape = (n, self.NY // self.UP, self.NX // self.UP)
+        self.d_cam = torch.zeros(shape, dtype=torch.float32, device=dev)
+        self.h_coef = torch.from_numpy(self.coef).pin_memory()
+        self.h_shift = torch.from_numpy(self.shift).pin_memory()
+        self.h_cam = torch.empty(shape, dtype=torch.float32).pin_memory()
+        self.stream = self.eng.torch_stream()
+        self.frames_per_step = n
+        self.n_emitters = 0
+        self.psf_build_ms = 0.0
+
+    def device_step(self):
+        self.d_cam.zero_()
+        self.plan.frames_dev(self.d_spec, self.d_coef, self.d_shift, self.window, self.UP, self.d_cam, sync=False)
+
+    def e2e_step(self):
+        import torch
+        self.d_coef.copy_(self.h_coef, non_blocking=True)
+        self.d_shift.copy_(self.h_shift, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        self.d_cam.zero_()
+        self.plan.frames_dev(self.d_spec, self.d_coef, self.d_shift, self.window, self.UP, self.d_cam, sync=True)
+        self.h_cam.copy_(self.d_cam, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return self.h_cam
+
+    def e2e_bytes(self):
+        return self.h_coef.numel() * 4 + self.h_shift.numel() * 8, self.h_cam.numel() * 4
+
+    def kernel_name(self):
+        return "ShiftColumnsKernel+ShiftRowsKernel"
+
+    def alg_bytes_per_launch(self):
+        n = len(self.coef)
+        spec = self.spectra[0].nbytes
+        # per frame: the 6 channels read, the column-pass spectrum written and read back, the camera frame out
+        return n * (6 * spec + 2 * spec + self.h_cam[0].numel() * 8)
+
+    def cpu_cores(self):
+        return self.ref.threads()
+
+    def reference_setup(self, threads=0):
+        from oracle.oracle import Reference
+        if not Reference.available():
+            raise RuntimeError("the reference harness oracle/_ref/libiscref.so is not built (it needs the reference "
+                               "tree at build time)")
+        self.ref = Reference()
+        self.ref.set_threads(threads)
+
+    def reference_step(self):
+        t0 = time.perf_counter()
+        for f in range(self.frames_per_step_cpu):
+            self.ref.shifted_images(self.NX, self.NY, self.spectra[:3], self.a[f], self.frac, self.drift[f],
+                                    self.window, self.UP, spec1=self.spectra[3:], w=float(self.w[f]))
+        return time.perf_counter() - t0
+
+
 class FftPlaceWorkload:
     """The splat's Fft placement (a next-row extra the reference runs on the CPU only): for 32,000 emitters (the
     SMLM movie's 200 frames at 160 ON each: positions uniform over 128 x 128 px, planes over the 49 of its kernel,
@@ -1192,7 +1298,8 @@ class BinnedWorkload:
 
 WORKLOADS = {"smlm": SmlmWorkload, "widefield": WidefieldWorkload, "psflib": PsfLibraryWorkload,
              "two-colour": TwoColourWorkload, "nll-grad": NllGradWorkload, "schedules": ScheduleWorkload,
-             "binned": BinnedWorkload, "tiff": TiffWorkload, "csv": CsvWorkload, "fftplace": FftPlaceWorkload}
+             "binned": BinnedWorkload, "tiff": TiffWorkload, "csv": CsvWorkload, "fftplace": FftPlaceWorkload,
+             "wfshift": WfShiftWorkload}
 
 
 # ----------------------------------------------------------------------------------------------------- arms

@@ -546,6 +546,22 @@ int iscu_wf_pass_times(iscu_wf_plan* plan, float* ms);
 int iscu_wf_render_async(iscu_wf_plan* plan, int32_t io_slot, const float* density, double background,
                          const iscu_camera* cam, uint32_t seed, uint32_t frame0, float* image, uint16_t* adu);
 int iscu_wf_render_wait(iscu_wf_plan* plan, int32_t io_slot);
+/* Frames of a drifting sample from its channels' spectra (WidefieldDriftFrames::Render / RenderShiftedImages,
+ * WidefieldRender.cpp:2905-2935; ShiftedCamera and ApplyShiftRamp, DriftShift.cpp:23-71) on an nx x ny grid (powers
+ * of two: the reference's GPU-mode grid, WidefieldRender.h:336). Per frame f: S = sum_c coef[f][c] spectra[c] (float
+ * complex, channels in the order the reference adds them -- the near focus's persistent and bleach channels, then
+ * the far focus's -- coefficients already multiplied as it does: float(a_j) x float(w_i); zero coefficients skipped),
+ * times exp(2 pi i (kx sx / nx + ky' sy / ny)) with (sx, sy) = shift[f] cells (ky' the signed row frequency, the
+ * Nyquist terms their cosine only), the inverse real transform (1 / (nx ny)), the window [y0, y0 + ch) x [x0, x0 +
+ * cw), each cell clamped at 0, up x up cells summed in float64 x scale and added to cam[f] ((ch / up) x (cw / up)).
+ * spectra_dev: n_channels x ny x (nx / 2 + 1) complex (interleaved float pairs) in RealFft2d's layout; coef_dev:
+ * n_frames x n_channels floats; shift_dev: n_frames x 2 doubles. */
+typedef struct iscu_wf_shift iscu_wf_shift;
+int iscu_wf_shift_create(iscu_ctx* ctx, uint32_t nx, uint32_t ny, iscu_wf_shift** out);
+void iscu_wf_shift_destroy(iscu_wf_shift* s);
+int iscu_wf_shifted_frames_dev(iscu_wf_shift* s, const float* spectra_dev, uint32_t n_channels, const float* coef_dev,
+                               const double* shift_dev, uint32_t n_frames, uint32_t x0, uint32_t y0, uint32_t cw,
+                               uint32_t ch, uint32_t up, float scale, float* cam_dev);
 /* The same on device buffers (the camera maps of iscu_set_static apply when their size is nx x ny). */
 int iscu_wf_render_dev(iscu_wf_plan* plan, const float* density_dev, double background, const iscu_camera* cam,
                        uint32_t seed, uint32_t frame0, float* image_dev, uint16_t* adu_dev);

@@ -223,6 +223,10 @@ SIGNATURES = {
     "iscu_wf_set_timing": (C.c_int, [vp, C.c_int32]),
     "iscu_wf_pass_times": (C.c_int, [vp, f32p]),
     "iscu_wf_render": (C.c_int, [vp, vp, C.c_double, C.POINTER(Camera), C.c_uint32, C.c_uint32, vp, vp]),
+    "iscu_wf_shift_create": (C.c_int, [vp, C.c_uint32, C.c_uint32, vp]),
+    "iscu_wf_shift_destroy": (None, [vp]),
+    "iscu_wf_shifted_frames_dev": (C.c_int, [vp, vp, C.c_uint32, vp, vp, C.c_uint32, C.c_uint32, C.c_uint32,
+                                             C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, vp]),
     "iscu_wf_render_async": (C.c_int, [vp, C.c_int32, vp, C.c_double, C.POINTER(Camera), C.c_uint32, C.c_uint32,
                                        vp, vp]),
     "iscu_wf_render_wait": (C.c_int, [vp, C.c_int32]),

@@ -134,6 +134,16 @@ struct iscu_wf_plan
    }
 };
 
+// Frames of a drifting widefield sample from its channels' spectra (iscu_wf_shifted_frames_dev): the grid's plans and
+// twiddle tables, and the spectra of the frames between the two passes.
+struct iscu_wf_shift
+{
+   iscu_ctx* ctx = nullptr;
+   uint32_t nx = 0, ny = 0, H = 0, W = 0, G = 0;
+   iscu::LinePlan px, py;
+   iscu::DevBuf tw, twg, T;
+};
+
 namespace iscu {
 
 namespace {
@@ -908,6 +918,184 @@ __global__ void __launch_bounds__(256) WfNoiseKernel(const float* __restrict__ p
    adu[o] = NoisePixel(photons[o], i, cam, st, u);
 }
 
+// ---------------------------------------------------------------------------- drifting sample (RenderShiftedImages)
+// The frame's spectrum S = sum_c coef[c] spec[c] (float complex, channels in order, zero coefficients skipped, as
+// RenderShiftedImages adds them, WidefieldRender.cpp:2905-2935), times ApplyShiftRamp's phase (DriftShift.cpp:23-48:
+// exp(2 pi i (kx sx / nx + ky' sy / ny)), ky' the signed row frequency, the Nyquist terms their cosine only; the
+// product formed in float64 and rounded to float), then the inverse transform, as conj(forward(conj S)): column pass
+// (along ky, every kx) here, row pass (the packed real inverse along kx, the window's rows) in ShiftRowsKernel.
+
+struct ShiftArgs
+{
+   const float2* spec;   // channels x ny x W, RealFft2d's layout
+   const float* coef;    // frames x channels
+   const double* shift;  // frames x 2: (fracX, fracY) in cells
+   int nChannels, nx, ny, W;
+};
+
+// Column pass group 0: S conjugated, straight from the channels (lanes walk kx), DIF group, twiddles.
+template <int R>
+__device__ __forceinline__ void ShiftFirst(const ColAddr& S, const ShiftArgs& a, int f, int kx0, int nb, int BL,
+                                          int logBL, int logQ, const float2* __restrict__ tw, const double2* py)
+{
+   const int q = 1 << logQ, total = BL << logQ;
+   const float* coef = a.coef + static_cast<size_t>(f) * a.nChannels;
+   const double sx = a.shift[2 * f];
+   const bool ramp = a.shift[2 * f] != 0.0 || a.shift[2 * f + 1] != 0.0;
+   for (int t = threadIdx.x; t < total; t += blockDim.x)
+   {
+      const int b = t & (BL - 1), j = t >> logBL, kx = kx0 + b;
+      if (b >= nb)
+         continue;
+      double2 pxv = make_double2(1.0, 0.0);
+      if (ramp)
+      {
+         double sn, cs;
+         sincospi(2.0 * kx * sx / a.nx, &sn, &cs);
+         pxv = make_double2(cs, kx == a.nx / 2 ? 0.0 : sn);
+      }
+      float2 v[R];
+#pragma unroll
+      for (int m = 0; m < R; ++m)
+      {
+         const int ky = j + m * q;
+         float2 acc = make_float2(0.f, 0.f);
+         for (int c = 0; c < a.nChannels; ++c)
+         {
+            const float w = coef[c];
+            if (w == 0.0f)
+               continue;
+            const float2 sp = __ldg(a.spec + (static_cast<size_t>(c) * a.ny + ky) * a.W + kx);
+            acc.x = acc.x + w * sp.x;
+            acc.y = acc.y + w * sp.y;
+         }
+         if (ramp)
+         {
+            const double2 pyv = py[ky];
+            const double pr = pxv.x * pyv.x - pxv.y * pyv.y, pi = pxv.x * pyv.y + pxv.y * pyv.x;
+            const double vr = acc.x, vi = acc.y;
+            acc = make_float2(static_cast<float>(vr * pr - vi * pi), static_cast<float>(vr * pi + vi * pr));
+         }
+         v[m] = make_float2(acc.x, -acc.y);   // conjugated: the forward transform then gives the inverse's conjugate
+      }
+      DifReg<R, false, false>(v);
+      if (tw)
+         Twiddle<R, false>(v, tw, q, j);
+#pragma unroll
+      for (int m = 0; m < R; ++m)
+         S(b, j + m * q) = v[m];
+   }
+}
+
+// grid (ceil(W / BZ), frames), BZ a power of two; smem ny * BZ float2 + ny double2 (the row ramp).
+// T[f][p][kx] = forward_y(conj S)[rev p], every column kx < W.
+__global__ void __launch_bounds__(kThreads, kMinCtas) ShiftColumnsKernel(ShiftArgs a, LinePlan P, int BZ, int logBZ,
+                                                                        const float2* __restrict__ twg,
+                                                                        float2* __restrict__ T)
+{
+   extern __shared__ __align__(16) unsigned char smem[];
+   double2* py = reinterpret_cast<double2*>(smem);
+   float2* s = reinterpret_cast<float2*>(py + a.ny);
+   const ColAddr S{s, BZ};
+   const int f = blockIdx.y, kx0 = blockIdx.x * BZ, nb = min(BZ, a.W - kx0);
+   const double sy = a.shift[2 * f + 1];
+   for (int ky = threadIdx.x; ky < a.ny; ky += blockDim.x)
+   {
+      const int k = ky <= a.ny / 2 ? ky : ky - a.ny;
+      double sn, cs;
+      sincospi(2.0 * k * sy / a.ny, &sn, &cs);
+      py[ky] = make_double2(cs, ky == a.ny / 2 ? 0.0 : sn);
+   }
+   __syncthreads();
+   ISCU_RADIX_SWITCH(P.r[0], (ShiftFirst<R>(S, a, f, kx0, nb, BZ, logBZ, LogQ(P, 0), GroupTw(P, twg, 0), py)));
+   __syncthreads();
+   ForwardRest<true>(P, twg, S, nb, BZ, logBZ);
+   float2* out = T + static_cast<size_t>(f) * a.ny * a.W;
+   for (int t = threadIdx.x; t < (a.ny << logBZ); t += blockDim.x)
+   {
+      const int b = t & (BZ - 1), p = t >> logBZ;
+      if (b < nb)
+         out[static_cast<size_t>(p) * a.W + kx0 + b] = S(b, p);
+   }
+}
+
+// Row pass, the last DIF group's inverse (span 1) from the staged rows: Z'[k] = (X[k] + conj X[H-k]) +
+// i W_nx^-k (X[k] - conj X[H-k]) at bit-reversed slots, X the row's half spectrum.
+template <int R>
+__device__ __forceinline__ void ShiftRowLoad(const ColAddr& S, const float2* rows, int W, int nb, int BL, int logBL,
+                                            int H, int logH, const float2* __restrict__ tw, int twShift)
+{
+   constexpr int r = Log2i(R);
+   const int logT = logH - r, total = BL << logT;
+   for (int t = threadIdx.x; t < total; t += blockDim.x)
+   {
+      const int b = t & (BL - 1), base = (t >> logBL) << r;
+      if (b >= nb)
+         continue;
+      const float2* X = rows + b * W;
+      float2 v[R];
+#pragma unroll
+      for (int m = 0; m < R; ++m)
+      {
+         const int k = Rev(base + m, logH);
+         const float2 xk = X[k], xm = Conj(X[H - k]);
+         const float2 w = Conj(__ldg(tw + (k << twShift)));
+         const float2 e = Cadd(xk, xm), o = Cmul(Csub(xk, xm), w);
+         v[m] = make_float2(e.x - o.y, e.y + o.x);
+      }
+      DitReg<R, true>(v);
+#pragma unroll
+      for (int m = 0; m < R; ++m)
+         S(b, base + m) = v[m];
+   }
+}
+
+// grid (ceil(camRows / rowsPerCta), frames); BL lines (a power of two >= rowsPerCta up); smem BL W float2 (the rows)
+// + H (BL + 1) float2 (the transform). cam[f][Y][X] += float(sum over up x up cells of max(0, cell) (float64) x
+// scale), the cells at rows y0 + Y up + sy, columns x0 + X up + sx of the image (1 / (nx ny)) x inverse.
+__global__ void __launch_bounds__(kThreads, kMinCtas) ShiftRowsKernel(const float2* __restrict__ T, LinePlan P, int nx,
+                                                                     int ny, int W, int BL, int logBL, int rowsPerCta,
+                                                                     int up, int x0, int y0, int camW, int camH,
+                                                                     float scale, const float2* __restrict__ tw,
+                                                                     int twShift, const float2* __restrict__ twg,
+                                                                     float* __restrict__ cam)
+{
+   extern __shared__ __align__(16) unsigned char smem[];
+   float2* rows = reinterpret_cast<float2*>(smem);
+   const ColAddr S{rows + BL * W, BL + 1};
+   const int f = blockIdx.y, Y0 = blockIdx.x * rowsPerCta, camRows = min(rowsPerCta, camH - Y0);
+   const int nb = camRows * up, H = nx / 2;
+   const int logNy = Log2i(ny);
+   // the window's rows, conjugated back: the unnormalised inverse along y, half spectrum along x
+   const float2* Tf = T + static_cast<size_t>(f) * ny * W;
+   for (int t = threadIdx.x; t < nb * W; t += blockDim.x)
+   {
+      const int b = t / W, k = t - b * W;
+      const int y = y0 + Y0 * up + b;
+      rows[t] = Conj(__ldg(Tf + static_cast<size_t>(Rev(y, logNy)) * W + k));
+   }
+   __syncthreads();
+   ISCU_RADIX_SWITCH(P.r[P.groups - 1], (ShiftRowLoad<R>(S, rows, W, nb, BL, logBL, H, P.logN, tw, twShift)));
+   __syncthreads();
+   InverseRest<true>(P, twg, S, nb, BL, logBL, P.groups - 2, 0);
+   const float norm = 1.0f / (static_cast<float>(nx) * static_cast<float>(ny));
+   for (int t = threadIdx.x; t < camRows * camW; t += blockDim.x)
+   {
+      const int Yc = t / camW, X = t - Yc * camW;
+      double acc = 0.0;
+      for (int sy = 0; sy < up; ++sy)
+         for (int sx = 0; sx < up; ++sx)
+         {
+            const int b = Yc * up + sy, x = x0 + X * up + sx;
+            const float2 c = S(b, x >> 1);
+            const float v = (x & 1 ? c.y : c.x) * norm;
+            acc += v > 0.f ? v : 0.f;
+         }
+      float& o = cam[(static_cast<size_t>(f) * camH + Y0 + Yc) * camW + X];
+      o += static_cast<float>(acc * scale);
+   }
+}
+
 __global__ void TwiddleKernel(int G, float2* tw)
 {
    const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1413,6 +1601,109 @@ int iscu_wf_render(iscu_wf_plan* plan, const float* density, double background, 
    if (adu)
       ISCU_CK(cudaMemcpyAsync(adu, plan->adu.p, n * sizeof(uint16_t), cudaMemcpyDeviceToHost, ctx->stream));
    ISCU_CK(cudaStreamSynchronize(ctx->stream));
+   return ISCU_OK;
+}
+
+int iscu_wf_shift_create(iscu_ctx* ctx, uint32_t nx, uint32_t ny, iscu_wf_shift** out)
+{
+   if (!ctx || !out)
+      return Fail(ISCU_ERR_ARG, "null argument");
+   *out = nullptr;
+   if (nx < 8 || nx > 4096 || (nx & (nx - 1)) || ny < 4 || ny > 8192 || (ny & (ny - 1)))
+      return Fail(ISCU_ERR_ARG, "drifting frames: nx a power of two in 8..4096, ny a power of two in 4..8192");
+   std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+   ClearError();
+   std::unique_ptr<iscu_wf_shift> s(new iscu_wf_shift());
+   s->ctx = ctx;
+   s->nx = nx;
+   s->ny = ny;
+   s->H = nx / 2;
+   s->W = nx / 2 + 1;
+   s->G = std::max(nx, ny);
+   s->px = MakeLinePlan(Log2(s->H), true);
+   s->py = MakeLinePlan(Log2(ny), true);
+   int entries = PlaceTables(s->px, 0);
+   entries += PlaceTables(s->py, entries);
+   const int bytes = static_cast<int>(kSmemMax);
+   ISCU_CK(cudaFuncSetAttribute(ShiftColumnsKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+   ISCU_CK(cudaFuncSetAttribute(ShiftRowsKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+   ISCU_CK(s->tw.Reserve(s->G * sizeof(float2)));
+   ISCU_CK(s->twg.Reserve(std::max(entries, 1) * sizeof(float2)));
+   TwiddleKernel<<<(s->G + 255) / 256, 256, 0, ctx->stream>>>(static_cast<int>(s->G), s->tw.as<float2>());
+   ISCU_CK_LAUNCH(ctx, "TwiddleKernel");
+   for (const LinePlan* P : {&s->px, &s->py})
+      for (int g = 0; g < P->groups; ++g)
+         if (P->tw[g] >= 0)
+         {
+            const int M = 1 << (LogQ(*P, g) + P->r[g]);
+            GroupTwiddleKernel<<<(M + 255) / 256, 256, 0, ctx->stream>>>(LogQ(*P, g), P->r[g],
+                                                                          s->twg.as<float2>() + P->tw[g]);
+            ISCU_CK_LAUNCH(ctx, "GroupTwiddleKernel");
+         }
+   ISCU_CK(cudaStreamSynchronize(ctx->stream));
+   *out = s.release();
+   return ISCU_OK;
+}
+
+void iscu_wf_shift_destroy(iscu_wf_shift* s)
+{
+   if (!s)
+      return;
+   cudaStreamSynchronize(s->ctx->stream);
+   delete s;
+}
+
+int iscu_wf_shifted_frames_dev(iscu_wf_shift* s, const float* spectra_dev, uint32_t n_channels, const float* coef_dev,
+                               const double* shift_dev, uint32_t n_frames, uint32_t x0, uint32_t y0, uint32_t cw,
+                               uint32_t ch, uint32_t up, float scale, float* cam_dev)
+{
+   if (!s || (n_frames && (!spectra_dev || !coef_dev || !shift_dev || !cam_dev)))
+      return Fail(ISCU_ERR_ARG, "null argument");
+   if (n_frames > 65535)
+      return Fail(ISCU_ERR_LIMIT, "at most 65535 frames per call");
+   if (up < 1 || static_cast<uint64_t>(x0) + cw > s->nx || static_cast<uint64_t>(y0) + ch > s->ny)
+      return Fail(ISCU_ERR_ARG, "the window must lie in the grid and up be >= 1");
+   iscu_ctx* ctx = s->ctx;
+   std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+   ClearError();
+   const int camW = static_cast<int>(cw / up), camH = static_cast<int>(ch / up);
+   if (!n_frames || !n_channels || camW == 0 || camH == 0)
+      return ISCU_OK;
+   const size_t budget = 200 * 1024;
+   // column pass: BZ columns per CTA, with the row ramp table
+   const size_t rampBytes = static_cast<size_t>(s->ny) * sizeof(double2);
+   int BZ = 1;
+   while (BZ < 32 && rampBytes + static_cast<size_t>(s->ny) * (2 * BZ) * sizeof(float2) <= budget)
+      BZ *= 2;
+   // row pass: BL lines (a power of two >= up), the staged rows and the transform's columns
+   int BL = 16;
+   while (BL > 1 && static_cast<size_t>(BL) * s->W * sizeof(float2) + static_cast<size_t>(s->H) * (BL + 1) *
+                                                                         sizeof(float2) > budget)
+      BL /= 2;
+   if (BL < static_cast<int>(up))
+      return Fail(ISCU_ERR_LIMIT, "drifting frames: " + std::to_string(up) + " cells per pixel need more rows in "
+                                  "shared memory than this grid's width leaves");
+   const int rowsPerCta = BL / static_cast<int>(up);
+   ISCU_CK(s->T.Reserve(static_cast<size_t>(n_frames) * s->ny * s->W * sizeof(float2)));
+   ShiftArgs a;
+   a.spec = reinterpret_cast<const float2*>(spectra_dev);
+   a.coef = coef_dev;
+   a.shift = shift_dev;
+   a.nChannels = static_cast<int>(n_channels);
+   a.nx = static_cast<int>(s->nx);
+   a.ny = static_cast<int>(s->ny);
+   a.W = static_cast<int>(s->W);
+   const size_t smemA = rampBytes + static_cast<size_t>(s->ny) * BZ * sizeof(float2);
+   ShiftColumnsKernel<<<dim3((s->W + BZ - 1) / BZ, n_frames), kThreads, smemA, ctx->stream>>>(
+      a, s->py, BZ, Log2(BZ), s->twg.as<float2>(), s->T.as<float2>());
+   ISCU_CK_LAUNCH(ctx, "ShiftColumnsKernel");
+   const size_t smemB = static_cast<size_t>(BL) * s->W * sizeof(float2) + static_cast<size_t>(s->H) * (BL + 1) *
+                                                                             sizeof(float2);
+   ShiftRowsKernel<<<dim3((camH + rowsPerCta - 1) / rowsPerCta, n_frames), kThreads, smemB, ctx->stream>>>(
+      s->T.as<float2>(), s->px, static_cast<int>(s->nx), static_cast<int>(s->ny), static_cast<int>(s->W), BL,
+      Log2(BL), rowsPerCta, static_cast<int>(up), static_cast<int>(x0), static_cast<int>(y0), camW, camH, scale,
+      s->tw.as<float2>(), Log2(s->G) - Log2(s->nx), s->twg.as<float2>(), cam_dev);
+   ISCU_CK_LAUNCH(ctx, "ShiftRowsKernel");
    return ISCU_OK;
 }
 

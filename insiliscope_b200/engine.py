@@ -791,6 +791,44 @@ class WidefieldPlan:
         self._pending_io.pop(int(io_slot), None)
 
 
+class WidefieldShift:
+    """iscu_wf_shift: frames of a drifting widefield sample from its channels' spectra on an nx x ny grid
+    (RenderShiftedImages)."""
+
+    def __init__(self, engine: Engine, nx, ny):
+        self.engine = engine
+        self.lib = engine.lib
+        self.nx, self.ny = int(nx), int(ny)
+        h = C.c_void_p()
+        check(self.lib.iscu_wf_shift_create(engine.h, self.nx, self.ny, C.byref(h)))
+        self.h = h
+        engine._plans.add(self)
+
+    def frames_dev(self, spectra_dev, coef_dev, shift_dev, window, up, cam_dev, scale=1.0, sync=True):
+        """cam_dev (n_frames, ch/up, cw/up) float32 CUDA += the frames (iscu_wf_shifted_frames_dev): spectra_dev
+        complex64 (n_ch, ny, nx/2 + 1), coef_dev float32 (n_frames, n_ch), shift_dev float64 (n_frames, 2)."""
+        x0, y0, cw, ch = window
+        n_ch = spectra_dev.shape[0]
+        n_frames = coef_dev.shape[0]
+        self.engine._before(sync)
+        check(self.lib.iscu_wf_shifted_frames_dev(self.h, _ptr(spectra_dev.contiguous()), n_ch,
+                                                  _ptr(coef_dev.contiguous()), _ptr(shift_dev.contiguous()), n_frames,
+                                                  x0, y0, cw, ch, up, float(scale), _ptr(cam_dev)))
+        self.engine._after(sync)
+
+    def close(self):
+        if self.h:
+            if self.engine.h:
+                self.lib.iscu_wf_shift_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class TiffWriter:
     """iscu_tiff: the CLI's movie file (cli/tiff_writer.h) byte for byte -- classic TIFF or BigTIFF, one uncompressed
     grey page per frame. Failures raise IscuError (code ISCU_ERR_IO) with the reference writer's message."""

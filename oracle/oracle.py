@@ -224,6 +224,8 @@ class Reference:
         L.ref_tiff_error.argtypes = [vp, C.c_char_p, C.c_size_t]
         L.ref_tiff_close.argtypes = [vp]
         L.ref_csv_numbers.argtypes = [vp, u32, C.c_char_p, vp, vp]
+        L.ref_shifted_images.argtypes = [C.c_uint, C.c_uint, vp, vp, C.c_int, f64, vp, f64, f64, f64, f64, C.c_uint,
+                                         C.c_uint, C.c_uint, C.c_uint, C.c_uint, vp]
         L.ref_plan_splat_fft.argtypes = [vp, f64, f64, C.c_int, vp, vp]
         L.ref_plan_splat_fft.restype = C.c_int
         L.ref_plan_splat_fft_batch.argtypes = [vp, vp, vp, u32]
@@ -375,6 +377,18 @@ class Reference:
         self.L.ref_csv_table(_p(cols), n_rows, n_cols, f, _p(out), need)
         sec = time.perf_counter() - t1
         return bytes(out[:need]), sec
+
+    def shifted_images(self, nx, ny, spec0, a, frac, drift, window, up, spec1=None, w=0.0, cam=None):
+        """RenderShiftedImages of channels' spectra (complex64 (n_ch, ny, nx/2 + 1): persistent, then bleach) at one
+        or two foci: the camera frame (ch/up, cw/up) float32 (+= onto cam when given)."""
+        x0, y0, cw, ch = window
+        s0 = np.ascontiguousarray(spec0, np.complex64)
+        s1 = None if spec1 is None else np.ascontiguousarray(spec1, np.complex64)
+        av = np.ascontiguousarray(a, np.float64)
+        out = np.zeros((ch // up, cw // up), np.float32) if cam is None else np.array(cam, np.float32, copy=True)
+        self.L.ref_shifted_images(nx, ny, _p(s0), _p(s1), s0.shape[0], w, _p(av), frac[0], frac[1], drift[0],
+                                  drift[1], x0, y0, cw, ch, up, _p(out))
+        return out
 
     def tiff(self, path, expected_bytes=0, big=False):
         """The reference's TiffWriter (cli/tiff_writer.h) on `path`."""
@@ -657,6 +671,43 @@ def fft_place_f64(planes, os_, x, y, z):
     ty = kc + (y0 - y - 0.5) * os_ + 0.5
     rx, ry = np.floor(tx + 0.5), np.floor(ty + 0.5)
     return fft_shift_tile_f64(P, tx - rx, ty - ry), (x0, y0, int(rx), int(ry))
+
+
+def shifted_frame_f64(spectra, coef, shift, nx, ny, window, up, scale=1.0):
+    """RenderShiftedImages (WidefieldRender.cpp:2905-2935; ApplyShiftRamp / ShiftedCamera, DriftShift.cpp:23-71) in
+    float64: S = sum of coef[c] x spectra[c] (zero coefficients skipped), times exp(2 pi i (kx sx / nx + ky' sy / ny))
+    (Nyquist terms: their cosine), the inverse as RealFft2d's (a complex inverse along y, then along x the packed
+    real inverse of the half spectrum: Z[k] = (X[k] + conj X[H-k]) + i conj(w^k) (X[k] - conj X[H-k]), H = nx / 2),
+    / (nx ny); the window's cells clamped at 0, summed up x up per pixel, times scale."""
+    x0, y0, cw, ch = window
+    H, W = nx // 2, nx // 2 + 1
+    S = np.zeros((ny, W), np.complex128)
+    for c, s in zip(coef, spectra):
+        if c != 0:
+            S += float(c) * np.asarray(s, np.complex128)
+    sx, sy = shift
+    if sx != 0 or sy != 0:
+        kx = np.arange(W)
+        px = np.exp(2j * np.pi * kx * sx / nx)
+        px[kx == nx // 2] = np.cos(2 * np.pi * (nx // 2) * sx / nx)
+        ky = np.arange(ny)
+        kys = np.where(ky <= ny // 2, ky, ky - ny)
+        py = np.exp(2j * np.pi * kys * sy / ny)
+        py[ky == ny // 2] = np.cos(2 * np.pi * (ny // 2) * sy / ny)
+        S = S * py[:, None] * px[None, :]
+    X = np.fft.ifft(S, axis=0) * ny                 # unnormalised inverse along y
+    k = np.arange(H)
+    w = np.exp(-2j * np.pi * k / nx)
+    xk, xm = X[:, k], np.conj(X[:, H - k])
+    Z = (xk + xm) + 1j * np.conj(w) * (xk - xm)
+    z = np.fft.ifft(Z, axis=1) * H
+    img = np.empty((ny, nx))
+    img[:, 0::2], img[:, 1::2] = z.real, z.imag
+    img /= nx * ny
+    cells = np.maximum(img[y0:y0 + ch, x0:x0 + cw], 0.0)
+    Hc, Wc = ch // up, cw // up
+    cam = cells[:Hc * up, :Wc * up].reshape(Hc, up, Wc, up).sum(axis=(1, 3)) * scale
+    return cam.astype(np.float32)
 
 
 def fft_convolve_same_f64(volume: np.ndarray, psf: np.ndarray) -> np.ndarray:

@@ -11,6 +11,7 @@
 #include "BinnedBlinks.h"
 #include "CsvNumber.h"
 #include "Drift.h"
+#include "WidefieldRender.h"
 #include "PsfGeneratorBridge.h"
 #include "SMLMBackground.h"
 #include "Parallel.h"
@@ -579,6 +580,39 @@ double ref_dye_blinks_batch(int mode, const double* kin, const double* histStart
 
 // The core's DyeH1 (dyes.cpp:175-178): H1 of microtubule mtIndex of cell (cx, cy).
 uint32_t ref_dye_h1(uint32_t seed, int32_t cx, int32_t cy, int mtIndex) { return isc::DyeH1(seed, cx, cy, mtIndex); }
+
+// RenderShiftedImages (WidefieldRender.cpp:2905-2935) on WidefieldImages made from given spectra (nCh channels of
+// ny x (nx/2 + 1) complex each: the persistent one, then nCh - 1 bleach ones) at a near focus (spec0) and, when
+// spec1 is given, a far one, weight w; bleach coefficients a (nCh - 1); the images' sub-cell pose (fracX, fracY) and
+// the frame's drift (dx, dy) cells; the FOV window (x0, y0, cw, ch) at up cells per pixel. cam (+=).
+void ref_shifted_images(unsigned nx, unsigned ny, const float* spec0, const float* spec1, int nCh, double w,
+                        const double* a, double fracX, double fracY, double dx, double dy, unsigned x0, unsigned y0,
+                        unsigned cw, unsigned ch, unsigned up, float* cam)
+{
+   auto fft = std::make_shared<const sim::RealFft2d>(nx, ny);
+   const size_t n = fft->SpecSize();
+   auto make = [&](const float* spec, sim::WidefieldImages& im) {
+      const auto* c = reinterpret_cast<const sim::cfloat*>(spec);
+      im.cw = cw;
+      im.ch = ch;
+      im.upscale = up;
+      im.specPersistent.assign(c, c + n);
+      for (int k = 1; k < nCh; ++k)
+         im.specBleach.emplace_back(c + k * n, c + (k + 1) * n);
+      im.fft = fft;
+      im.fovX0 = x0;
+      im.fovY0 = y0;
+      im.fracX = fracX;
+      im.fracY = fracY;
+   };
+   sim::WidefieldImages i0, i1;
+   make(spec0, i0);
+   if (spec1)
+      make(spec1, i1);
+   std::vector<float> img(cam, cam + static_cast<size_t>(cw / up) * (ch / up));
+   sim::RenderShiftedImages(i0, spec1 ? &i1 : nullptr, w, std::vector<double>(a, a + nCh - 1), dx, dy, img);
+   std::copy(img.begin(), img.end(), cam);
+}
 
 // PlanSplat with the Fft placement (PsfGeneratorBridge.cpp:1441-1456) for an emitter at (x, y) px on plane z of
 // kernel cache h: its shifted block sums (bw x bw floats) into sums and (x0, y0, bx, by) into st4. Returns bw, or 0
