@@ -165,6 +165,7 @@ constexpr int kThreads = 256;
 constexpr int kMinCtas = ISCU_WF_MIN_CTAS;
 constexpr size_t kSmemBudget = 100 * 1024;   // lines per CTA are sized to this
 constexpr size_t kSmemMax = 227 * 1024;
+constexpr size_t kSmemPair = 112 * 1024;   // dynamic shared memory of a CTA that leaves room for a second on its SM
 
 __device__ __forceinline__ float2 Cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 Csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
@@ -957,21 +958,37 @@ __device__ __forceinline__ void ShiftFirst(const ColAddr& S, const ShiftArgs& a,
       float2 v[R];
 #pragma unroll
       for (int m = 0; m < R; ++m)
+         v[m] = make_float2(0.f, 0.f);
+      // channels in order, a channel's loads issued eight at a time (every point's sum keeps the channel order)
+      constexpr int kBatch = R < 8 ? R : 8;
+      for (int c = 0; c < a.nChannels; ++c)
       {
-         const int ky = j + m * q;
-         float2 acc = make_float2(0.f, 0.f);
-         for (int c = 0; c < a.nChannels; ++c)
+         const float w = coef[c];
+         if (w == 0.0f)
+            continue;
+         const float2* sc = a.spec + (static_cast<size_t>(c) * a.ny + j) * a.W + kx;
+#pragma unroll
+         for (int m0 = 0; m0 < R; m0 += kBatch)
          {
-            const float w = coef[c];
-            if (w == 0.0f)
-               continue;
-            const float2 sp = __ldg(a.spec + (static_cast<size_t>(c) * a.ny + ky) * a.W + kx);
-            acc.x = acc.x + w * sp.x;
-            acc.y = acc.y + w * sp.y;
+            float2 sp[kBatch];
+#pragma unroll
+            for (int u = 0; u < kBatch; ++u)
+               sp[u] = __ldg(sc + static_cast<size_t>(m0 + u) * q * a.W);
+#pragma unroll
+            for (int u = 0; u < kBatch; ++u)
+            {
+               v[m0 + u].x = v[m0 + u].x + w * sp[u].x;
+               v[m0 + u].y = v[m0 + u].y + w * sp[u].y;
+            }
          }
+      }
+#pragma unroll
+      for (int m = 0; m < R; ++m)
+      {
+         float2 acc = v[m];
          if (ramp)
          {
-            const double2 pyv = py[ky];
+            const double2 pyv = py[j + m * q];
             const double pr = pxv.x * pyv.x - pxv.y * pyv.y, pi = pxv.x * pyv.y + pxv.y * pyv.x;
             const double vr = acc.x, vi = acc.y;
             acc = make_float2(static_cast<float>(vr * pr - vi * pi), static_cast<float>(vr * pi + vi * pr));
@@ -1068,31 +1085,65 @@ __global__ void __launch_bounds__(kThreads, kMinCtas) ShiftRowsKernel(const floa
    const int logNy = Log2i(ny);
    // the window's rows, conjugated back: the unnormalised inverse along y, half spectrum along x
    const float2* Tf = T + static_cast<size_t>(f) * ny * W;
-   for (int t = threadIdx.x; t < nb * W; t += blockDim.x)
+   constexpr int kU = 8;   // loads in flight per thread
+   const int nIn = nb * W;
+   for (int t0 = threadIdx.x; t0 < nIn; t0 += kU * blockDim.x)
    {
-      const int b = t / W, k = t - b * W;
-      const int y = y0 + Y0 * up + b;
-      rows[t] = Conj(__ldg(Tf + static_cast<size_t>(Rev(y, logNy)) * W + k));
+      float2 v[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u)
+      {
+         const int t = t0 + u * blockDim.x;
+         if (t < nIn)
+         {
+            const int b = t / W, k = t - b * W;
+            const int y = y0 + Y0 * up + b;
+            v[u] = __ldg(Tf + static_cast<size_t>(Rev(y, logNy)) * W + k);
+         }
+      }
+#pragma unroll
+      for (int u = 0; u < kU; ++u)
+      {
+         const int t = t0 + u * blockDim.x;
+         if (t < nIn)
+            rows[t] = Conj(v[u]);
+      }
    }
    __syncthreads();
    ISCU_RADIX_SWITCH(P.r[P.groups - 1], (ShiftRowLoad<R>(S, rows, W, nb, BL, logBL, H, P.logN, tw, twShift)));
    __syncthreads();
    InverseRest<true>(P, twg, S, nb, BL, logBL, P.groups - 2, 0);
    const float norm = 1.0f / (static_cast<float>(nx) * static_cast<float>(ny));
-   for (int t = threadIdx.x; t < camRows * camW; t += blockDim.x)
+   const int nOut = camRows * camW;
+   float* camF = cam + (static_cast<size_t>(f) * camH + Y0) * camW;
+   for (int t0 = threadIdx.x; t0 < nOut; t0 += kU * blockDim.x)
    {
-      const int Yc = t / camW, X = t - Yc * camW;
-      double acc = 0.0;
-      for (int sy = 0; sy < up; ++sy)
-         for (int sx = 0; sx < up; ++sx)
-         {
-            const int b = Yc * up + sy, x = x0 + X * up + sx;
-            const float2 c = S(b, x >> 1);
-            const float v = (x & 1 ? c.y : c.x) * norm;
-            acc += v > 0.f ? v : 0.f;
-         }
-      float& o = cam[(static_cast<size_t>(f) * camH + Y0 + Yc) * camW + X];
-      o += static_cast<float>(acc * scale);
+      float o[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u)
+      {
+         const int t = t0 + u * blockDim.x;
+         if (t < nOut)
+            o[u] = camF[t];
+      }
+#pragma unroll
+      for (int u = 0; u < kU; ++u)
+      {
+         const int t = t0 + u * blockDim.x;
+         if (t >= nOut)
+            continue;
+         const int Yc = t / camW, X = t - Yc * camW;
+         double acc = 0.0;
+         for (int sy = 0; sy < up; ++sy)
+            for (int sx = 0; sx < up; ++sx)
+            {
+               const int b = Yc * up + sy, x = x0 + X * up + sx;
+               const float2 c = S(b, x >> 1);
+               const float v = (x & 1 ? c.y : c.x) * norm;
+               acc += v > 0.f ? v : 0.f;
+            }
+         camF[t] = o[u] + static_cast<float>(acc * scale);
+      }
    }
 }
 
@@ -1675,11 +1726,17 @@ int iscu_wf_shifted_frames_dev(iscu_wf_shift* s, const float* spectra_dev, uint3
    int BZ = 1;
    while (BZ < 32 && rampBytes + static_cast<size_t>(s->ny) * (2 * BZ) * sizeof(float2) <= budget)
       BZ *= 2;
-   // row pass: BL lines (a power of two >= up), the staged rows and the transform's columns
+   // row pass: BL lines (a power of two >= up), the staged rows and the transform's columns; the largest BL <= 16
+   // that lets two CTAs share an SM, else the largest that fits one
+   const auto rowBytes = [&](int bl) {
+      return static_cast<size_t>(bl) * s->W * sizeof(float2) + static_cast<size_t>(s->H) * (bl + 1) * sizeof(float2);
+   };
    int BL = 16;
-   while (BL > 1 && static_cast<size_t>(BL) * s->W * sizeof(float2) + static_cast<size_t>(s->H) * (BL + 1) *
-                                                                         sizeof(float2) > budget)
+   while (BL / 2 >= static_cast<int>(up) && rowBytes(BL) > kSmemPair)
       BL /= 2;
+   if (rowBytes(BL) > kSmemPair)
+      for (BL = 16; BL > 1 && rowBytes(BL) > budget; BL /= 2)
+         ;
    if (BL < static_cast<int>(up))
       return Fail(ISCU_ERR_LIMIT, "drifting frames: " + std::to_string(up) + " cells per pixel need more rows in "
                                   "shared memory than this grid's width leaves");
