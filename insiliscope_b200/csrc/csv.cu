@@ -5,8 +5,9 @@
 //
 // A table is two passes over its rows with a scan between them, so no cell text is stored: pass 1 formats each
 // row's cells (a thread per row, reading the column-major table coalesced) to count its bytes and sums them per block
-// of 1024 rows; one thread scans the block sums; pass 2 scans the row lengths inside each block, formats the row
-// again and writes it at its offset (writes past the caller's capacity are dropped and reported).
+// of 1024 rows; one thread scans the block sums; pass 2 formats each row again into its place in a shared-memory span
+// of 256 rows, which the CTA then stores with aligned 16-byte stores (writes past the caller's capacity are dropped
+// and reported).
 
 #include "iscu_internal.h"
 #include "csv_format.cuh"
@@ -128,19 +129,38 @@ __global__ void CsvScanBlocksKernel(unsigned long long* blockSum, uint32_t nBloc
    blockSum[nBlocks] = t;
 }
 
-// Pass 2: each row at its offset (the block's, plus the rows before it in the block), formatted again.
-__global__ void __launch_bounds__(kRows) CsvWriteRowsKernel(const double* __restrict__ cols, uint32_t nRows,
+// Pass 2: each row at its offset, formatted again. A CTA takes kSpan rows of a block (their offset: the block's, plus
+// the rows before them in the block), lays its rows out in shared memory at the output's 16-byte phase, and the CTA
+// stores the span with aligned 16-byte stores (bytes at its two ends, and past the caller's capacity, one at a time).
+// A span longer than the staging buffer is written straight from each thread.
+constexpr int kSpan = 256;                     // rows (threads) per CTA of pass 2
+constexpr int kStage = 64 * 1024;              // staging bytes per CTA
+
+__global__ void __launch_bounds__(kSpan) CsvWriteRowsKernel(const double* __restrict__ cols, uint32_t nRows,
                                                            uint32_t nCols, Fmts f,
                                                            const uint32_t* __restrict__ rowLen,
                                                            const unsigned long long* __restrict__ blockOff,
                                                            char* __restrict__ out, unsigned long long cap)
 {
-   __shared__ unsigned long long warpSum[kRows / 32];
-   const uint32_t r = blockIdx.x * kRows + threadIdx.x;
-   const unsigned long long len = r < nRows ? rowLen[r] : 0;
-   // inclusive scan inside the warp, then across the warps
-   unsigned long long s = len;
+   extern __shared__ uint4 stage4[];
+   char* stage = reinterpret_cast<char*>(stage4);
+   __shared__ unsigned long long warpSum[kSpan / 32];
+   __shared__ unsigned long long spanBefore[kSpan / 32];
+   const uint32_t block = blockIdx.x / (kRows / kSpan), sub = blockIdx.x % (kRows / kSpan);
+   const uint32_t blockRow0 = block * kRows;
+   const uint32_t r = blockRow0 + sub * kSpan + threadIdx.x;
    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   // the block's rows before this span: sub * kSpan lengths
+   unsigned long long pre = 0;
+   for (uint32_t i = threadIdx.x; i < sub * kSpan; i += kSpan)
+      pre += blockRow0 + i < nRows ? rowLen[blockRow0 + i] : 0u;
+   for (int o = 16; o; o >>= 1)
+      pre += __shfl_down_sync(0xFFFFFFFFu, pre, o);
+   if (lane == 0)
+      spanBefore[warp] = pre;
+   // this row's offset inside the span: an inclusive scan inside the warp, then across the warps
+   const unsigned long long len = r < nRows ? rowLen[r] : 0;
+   unsigned long long s = len;
    for (int o = 1; o < 32; o <<= 1)
    {
       const unsigned long long y = __shfl_up_sync(0xFFFFFFFFu, s, o);
@@ -150,22 +170,53 @@ __global__ void __launch_bounds__(kRows) CsvWriteRowsKernel(const double* __rest
    if (lane == 31)
       warpSum[warp] = s;
    __syncthreads();
-   unsigned long long before = 0;
-   for (int w = 0; w < warp; ++w)
-      before += warpSum[w];
-   if (r >= nRows)
-      return;
-   unsigned long long at = blockOff[blockIdx.x] + before + s - len;
-   char buf[48];
-   for (uint32_t c = 0; c < nCols; ++c)
+   unsigned long long before = 0, spanBytes = 0, spanAt = blockOff[block];
+   for (int w = 0; w < kSpan / 32; ++w)
    {
-      const int n = FormatCell(cols[static_cast<size_t>(c) * nRows + r], f.c[c], buf);
-      for (int j = 0; j < n; ++j, ++at)
-         if (at < cap)
-            out[at] = buf[j];
-      if (at < cap)
-         out[at] = c + 1 < nCols ? ',' : '\n';
-      ++at;
+      before += w < warp ? warpSum[w] : 0u;
+      spanBytes += warpSum[w];
+      spanAt += spanBefore[w];
+   }
+   const unsigned long long rowAt = before + s - len;   // inside the span
+   const int phase = static_cast<int>(spanAt & 15u);
+   const bool staged = phase + spanBytes <= static_cast<unsigned long long>(kStage) &&
+                       (reinterpret_cast<uintptr_t>(out) & 15u) == 0;
+   if (r < nRows)
+   {
+      char buf[48];
+      unsigned long long at = staged ? phase + rowAt : spanAt + rowAt;
+      char* dst = staged ? stage : out;
+      const unsigned long long lim = staged ? ~0ull : cap;
+      for (uint32_t c = 0; c < nCols; ++c)
+      {
+         const int n = FormatCell(cols[static_cast<size_t>(c) * nRows + r], f.c[c], buf);
+         for (int j = 0; j < n; ++j, ++at)
+            if (at < lim)
+               dst[at] = buf[j];
+         if (at < lim)
+            dst[at] = c + 1 < nCols ? ',' : '\n';
+         ++at;
+      }
+   }
+   if (!staged)
+      return;
+   __syncthreads();
+   // stage[phase + k] is out[spanAt + k]; the 16-byte chunks of out from spanAt - phase
+   const unsigned long long g0 = spanAt - phase, g1 = spanAt + spanBytes;
+   const uint32_t chunks = static_cast<uint32_t>((g1 - g0 + 15) / 16);
+   uint4* out4 = reinterpret_cast<uint4*>(out + g0);
+   for (uint32_t k = threadIdx.x; k < chunks; k += kSpan)
+   {
+      const unsigned long long c0 = g0 + 16ull * k;
+      if (c0 >= spanAt && c0 + 16 <= g1 && c0 + 16 <= cap)
+         out4[k] = stage4[k];
+      else
+         for (int j = 0; j < 16; ++j)
+         {
+            const unsigned long long g = c0 + j;
+            if (g >= spanAt && g < g1 && g < cap)
+               out[g] = stage[16 * k + j];
+         }
    }
 }
 
@@ -219,9 +270,14 @@ int iscu_csv_table_dev(iscu_ctx* ctx, const double* columns_dev, uint32_t n_rows
    ISCU_CK_LAUNCH(ctx, "CsvRowLengthsKernel");
    CsvScanBlocksKernel<<<1, 1, 0, ctx->stream>>>(blockSum, blocks);
    ISCU_CK_LAUNCH(ctx, "CsvScanBlocksKernel");
-   CsvWriteRowsKernel<<<blocks, kRows, 0, ctx->stream>>>(columns_dev, n_rows, n_cols, f, rowLen, blockSum, out_dev,
-                                                          out_capacity);
-   ISCU_CK_LAUNCH(ctx, "CsvWriteRowsKernel");
+   if (out_capacity)   // (a call that only sizes the text writes nothing)
+   {
+      ISCU_CK(cudaFuncSetAttribute(CsvWriteRowsKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kStage));
+      CsvWriteRowsKernel<<<blocks * (kRows / kSpan), kSpan, kStage, ctx->stream>>>(columns_dev, n_rows, n_cols, f,
+                                                                                  rowLen, blockSum, out_dev,
+                                                                                  out_capacity);
+      ISCU_CK_LAUNCH(ctx, "CsvWriteRowsKernel");
+   }
    unsigned long long total = 0;
    ISCU_CK(cudaMemcpyAsync(&total, blockSum + blocks, 8, cudaMemcpyDeviceToHost, ctx->stream));
    ISCU_CK(cudaStreamSynchronize(ctx->stream));

@@ -161,6 +161,66 @@ __host__ __device__ inline void Expand(uint64_t m, int e, Expansion& x)
       x.ip[i] = rev[nr - 1 - i];
 }
 
+// The same expansion when the integer part and the fraction both fit 64 bits (|x| < 2^64 with at most 60 fraction
+// bits: every value the tables hold but the tiny ones); the fraction's digits as f * 10, shifted, in one word.
+struct SmallExpansion
+{
+   char ip[20];
+   int nip;
+   bool ipZero;
+   uint64_t f;
+   int k;
+
+   __host__ __device__ int Next()
+   {
+      if (k == 0)
+         return 0;
+      f *= 10u;   // f < 2^60: no overflow
+      const int d = static_cast<int>(f >> k);
+      f &= (uint64_t(1) << k) - 1u;
+      return d;
+   }
+   __host__ __device__ bool FracNonzero() const { return k > 0 && f != 0; }
+};
+
+// m 2^e fits SmallExpansion: e >= 0 with m 2^e < 2^64, or -60 <= e < 0.
+__host__ __device__ inline bool FitsSmall(uint64_t m, int e)
+{
+   if (e < 0)
+      return e >= -60;
+   return e < 64 && (e == 0 || (m >> (64 - e)) == 0);
+}
+
+__host__ __device__ inline void ExpandSmall(uint64_t m, int e, SmallExpansion& x)
+{
+   uint64_t ipart;
+   if (e >= 0)
+   {
+      ipart = m << e;
+      x.k = 0;
+      x.f = 0;
+   }
+   else
+   {
+      x.k = -e;
+      ipart = m >> x.k;
+      x.f = m & ((uint64_t(1) << x.k) - 1u);
+   }
+   char rev[20];
+   int nr = 0;
+   while (ipart)
+   {
+      rev[nr++] = static_cast<char>('0' + ipart % 10u);
+      ipart /= 10u;
+   }
+   x.ipZero = nr == 0;
+   if (x.ipZero)
+      rev[nr++] = '0';
+   x.nip = nr;
+   for (int i = 0; i < nr; ++i)
+      x.ip[i] = rev[nr - 1 - i];
+}
+
 // Adds one unit in the last place of the n digits d (ASCII); true when they all carried (999 -> 000).
 __host__ __device__ inline bool Increment(char* d, int n)
 {
@@ -177,51 +237,18 @@ __host__ __device__ inline bool Increment(char* d, int n)
    return true;
 }
 
-// printf(fmt, v) as AppendCsvNumber keeps it: into out (>= 48 bytes), returns the length (0 for NaN / infinity).
-// kind 'f' or 'g', prec 0..9.
-__host__ __device__ inline int Format(double v, char kind, int prec, char* out)
+// The layout of printf's conversion from the value's digits: the sign, then %.pf or %.Pg (kMaxOut characters of
+// conversion, kMaxDigits digits of %.pf at most for this expansion).
+template <int kMaxOut, int kMaxDigits, class Exp>
+__host__ __device__ inline int Layout(bool neg, uint64_t m, Exp& x, char kind, int prec, char* out)
 {
-   uint64_t bits;
-   {
-      union
-      {
-         double d;
-         uint64_t u;
-      } c;
-      c.d = v;
-      bits = c.u;
-   }
-   const bool neg = (bits >> 63) != 0;
-   const int be = static_cast<int>((bits >> 52) & 0x7FF);
-   const uint64_t frac = bits & ((uint64_t(1) << 52) - 1);
-   if (be == 0x7FF)
-      return 0;   // NaN, infinity: nothing
-   uint64_t m;
-   int e;
-   if (be == 0)
-   {
-      m = frac;
-      e = -1074;
-   }
-   else
-   {
-      m = frac | (uint64_t(1) << 52);
-      e = be - 1075;
-   }
-   while (m && !(m & 1) && e < 0)   // fewer fraction bits, the same value
-   {
-      m >>= 1;
-      ++e;
-   }
-   char s[360];   // the whole conversion, then its first 47 characters
+   char s[kMaxOut];   // the whole conversion, then its first 47 characters
    int n = 0;
    if (neg)
       s[n++] = '-';
-   Expansion x;
-   Expand(m, e, x);
    if (kind == 'f')
    {
-      char d[340];   // integer digits, then prec fraction digits
+      char d[kMaxDigits];   // integer digits, then prec fraction digits
       int nd = 0;
       for (int i = 0; i < x.nip; ++i)
          d[nd++] = x.ip[i];
@@ -360,6 +387,55 @@ __host__ __device__ inline int Format(double v, char kind, int prec, char* out)
    for (int i = 0; i < len; ++i)
       out[i] = s[i];
    return len;
+}
+
+// printf(fmt, v) as AppendCsvNumber keeps it: into out (>= 48 bytes), returns the length (0 for NaN / infinity).
+// kind 'f' or 'g', prec 0..9.
+__host__ __device__ inline int Format(double v, char kind, int prec, char* out)
+{
+   uint64_t bits;
+   {
+      union
+      {
+         double d;
+         uint64_t u;
+      } c;
+      c.d = v;
+      bits = c.u;
+   }
+   const bool neg = (bits >> 63) != 0;
+   const int be = static_cast<int>((bits >> 52) & 0x7FF);
+   const uint64_t frac = bits & ((uint64_t(1) << 52) - 1);
+   if (be == 0x7FF)
+      return 0;   // NaN, infinity: nothing
+   uint64_t m;
+   int e;
+   if (be == 0)
+   {
+      m = frac;
+      e = -1074;
+   }
+   else
+   {
+      m = frac | (uint64_t(1) << 52);
+      e = be - 1075;
+   }
+   while (m && !(m & 1) && e < 0)   // fewer fraction bits, the same value
+   {
+      m >>= 1;
+      ++e;
+   }
+   if (m == 0)
+      e = 0;
+   if (FitsSmall(m, e))
+   {
+      SmallExpansion x;
+      ExpandSmall(m, e, x);
+      return Layout<40, 32>(neg, m, x, kind, prec, out);
+   }
+   Expansion x;
+   Expand(m, e, x);
+   return Layout<360, 340>(neg, m, x, kind, prec, out);
 }
 
 } // namespace csv

@@ -449,56 +449,111 @@ __global__ void __launch_bounds__(128) RowsKernel(Params p)
    DyeRows(p, dye, s);
 }
 
-// Exclusive scan of n counts into first[0..n] (first[n] = the total, and *total), one CTA walking the array in
-// chunks of 1024 with a running carry.
-__global__ void __launch_bounds__(1024) ScanKernel(const uint32_t* __restrict__ counts, uint32_t n,
-                                                   uint32_t* __restrict__ first, uint32_t* __restrict__ total)
+// Exclusive scan of n counts into first[0..n] (first[n] = the total, and *total) in three launches: the sums of
+// blocks of kScanItems counts, their exclusive scan by one CTA, and each block's scan from its offset.
+constexpr int kScanThreads = 1024, kScanPer = 4, kScanItems = kScanThreads * kScanPer;
+
+// Inclusive scan of x across the CTA (warp scans, then the warps' totals); the CTA's total in *blockTotal.
+__device__ __forceinline__ uint32_t CtaInclusiveScan(uint32_t x, uint32_t* warpSums, uint32_t* blockTotal)
 {
-   __shared__ uint32_t warpSums[32];
-   __shared__ uint32_t carry;
-   const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-   if (tid == 0)
-      carry = 0;
-   __syncthreads();
-   for (uint32_t base = 0; base < n; base += 1024)
+   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   for (int o = 1; o < 32; o <<= 1)
    {
-      const uint32_t i = base + tid;
-      const uint32_t v = i < n ? counts[i] : 0u;
-      uint32_t x = v;
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= static_cast<uint32_t>(o))
+         x += y;
+   }
+   if (lane == 31)
+      warpSums[warp] = x;
+   __syncthreads();
+   if (warp == 0)
+   {
+      uint32_t w = lane < (blockDim.x >> 5) ? warpSums[lane] : 0u;
       for (int o = 1; o < 32; o <<= 1)
       {
-         const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+         const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
          if (lane >= static_cast<uint32_t>(o))
-            x += y;
+            w += y;
       }
+      warpSums[lane] = w;   // inclusive over warps
       if (lane == 31)
-         warpSums[warp] = x;
-      __syncthreads();
-      if (warp == 0)
-      {
-         uint32_t w = warpSums[lane];
-         for (int o = 1; o < 32; o <<= 1)
-         {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= static_cast<uint32_t>(o))
-               w += y;
-         }
-         warpSums[lane] = w;   // inclusive over warps
-      }
-      __syncthreads();
-      const uint32_t before = carry + (warp ? warpSums[warp - 1] : 0u) + x - v;
-      if (i < n)
-         first[i] = before;
-      __syncthreads();
-      if (tid == 1023)
-         carry = before + v;
-      __syncthreads();
+         *blockTotal = w;
    }
-   if (tid == 0)
+   __syncthreads();
+   return x + (warp ? warpSums[warp - 1] : 0u);
+}
+
+__global__ void __launch_bounds__(kScanThreads) ScanSumsKernel(const uint32_t* __restrict__ counts, uint32_t n,
+                                                               uint32_t* __restrict__ sums)
+{
+   __shared__ uint32_t warpSums[32];
+   const size_t i0 = static_cast<size_t>(blockIdx.x) * kScanItems + static_cast<size_t>(threadIdx.x) * kScanPer;
+   uint32_t x = 0;
+#pragma unroll
+   for (int k = 0; k < kScanPer; ++k)
+      if (i0 + k < n)
+         x += counts[i0 + k];
+   for (int o = 16; o; o >>= 1)
+      x += __shfl_down_sync(0xffffffffu, x, o);
+   if ((threadIdx.x & 31) == 0)
+      warpSums[threadIdx.x >> 5] = x;
+   __syncthreads();
+   if (threadIdx.x == 0)
+   {
+      uint32_t t = 0;
+      for (int w = 0; w < kScanThreads / 32; ++w)
+         t += warpSums[w];
+      sums[blockIdx.x] = t;
+   }
+}
+
+// The block sums' exclusive scan in place (nb of them), the total into first[n] and *total.
+__global__ void __launch_bounds__(kScanThreads) ScanOffsetsKernel(uint32_t* __restrict__ sums, uint32_t nb,
+                                                                  uint32_t* __restrict__ first, uint32_t n,
+                                                                  uint32_t* __restrict__ total)
+{
+   __shared__ uint32_t warpSums[32];
+   __shared__ uint32_t chunkTotal;
+   uint32_t carry = 0;
+   for (uint32_t base = 0; base < nb; base += kScanThreads)
+   {
+      const uint32_t i = base + threadIdx.x;
+      const uint32_t v = i < nb ? sums[i] : 0u;
+      const uint32_t inc = CtaInclusiveScan(v, warpSums, &chunkTotal);
+      if (i < nb)
+         sums[i] = carry + inc - v;
+      carry += chunkTotal;
+      __syncthreads();   // warpSums and chunkTotal are rewritten by the next chunk
+   }
+   if (threadIdx.x == 0)
    {
       first[n] = carry;
       *total = carry;
    }
+}
+
+__global__ void __launch_bounds__(kScanThreads) ScanWriteKernel(const uint32_t* __restrict__ counts, uint32_t n,
+                                                                const uint32_t* __restrict__ offsets,
+                                                                uint32_t* __restrict__ first)
+{
+   __shared__ uint32_t warpSums[32];
+   __shared__ uint32_t blockTotal;
+   const size_t i0 = static_cast<size_t>(blockIdx.x) * kScanItems + static_cast<size_t>(threadIdx.x) * kScanPer;
+   uint32_t v[kScanPer], x = 0;
+#pragma unroll
+   for (int k = 0; k < kScanPer; ++k)
+   {
+      v[k] = i0 + k < n ? counts[i0 + k] : 0u;
+      x += v[k];
+   }
+   uint32_t at = offsets[blockIdx.x] + CtaInclusiveScan(x, warpSums, &blockTotal) - x;
+#pragma unroll
+   for (int k = 0; k < kScanPer; ++k)
+      if (i0 + k < n)
+      {
+         first[i0 + k] = at;
+         at += v[k];
+      }
 }
 
 } // namespace
@@ -551,12 +606,14 @@ extern "C" int iscu_dye_blinks_dev(iscu_ctx* ctx, const iscu_label* label, const
    const size_t histB = static_cast<size_t>(n_seg) * (sizeof(double) + sizeof(Kin));
    const size_t cntB = static_cast<size_t>(n_dyes) * sizeof(uint32_t);
    const size_t firstB = (static_cast<size_t>(n_dyes) + 1) * sizeof(uint32_t);
-   ISCU_CK(ctx->dSchedule.Reserve(histB + cntB + (dye_first_dev ? 0 : firstB) + 64));
+   const size_t sumsB = ((static_cast<size_t>(n_dyes) + kScanItems - 1) / kScanItems) * sizeof(uint32_t);
+   ISCU_CK(ctx->dSchedule.Reserve(histB + cntB + (dye_first_dev ? 0 : firstB) + sumsB + 64));
    char* b = ctx->dSchedule.as<char>();
    double* dStart = reinterpret_cast<double*>(b);
    Kin* dKin = reinterpret_cast<Kin*>(b + static_cast<size_t>(n_seg) * sizeof(double));
    uint32_t* dCounts = reinterpret_cast<uint32_t*>(b + ((histB + 15) & ~size_t(15)));
    uint32_t* dFirst = dye_first_dev ? dye_first_dev : dCounts + n_dyes;
+   uint32_t* dSums = dCounts + n_dyes + (dye_first_dev ? 0 : static_cast<size_t>(n_dyes) + 1);
    if (n_seg)
    {
       std::vector<Kin> kin(n_seg);
@@ -583,8 +640,13 @@ extern "C" int iscu_dye_blinks_dev(iscu_ctx* ctx, const iscu_label* label, const
    const unsigned blocks = (n_dyes + 127) / 128;
    CountKernel<<<blocks, 128, 0, s>>>(p);
    ISCU_CK_LAUNCH(ctx, "CountKernel");
-   ScanKernel<<<1, 1024, 0, s>>>(dCounts, n_dyes, dFirst, n_rows_dev);
-   ISCU_CK_LAUNCH(ctx, "ScanKernel");
+   const uint32_t scanBlocks = static_cast<uint32_t>((static_cast<size_t>(n_dyes) + kScanItems - 1) / kScanItems);
+   ScanSumsKernel<<<scanBlocks, kScanThreads, 0, s>>>(dCounts, n_dyes, dSums);
+   ISCU_CK_LAUNCH(ctx, "ScanSumsKernel");
+   ScanOffsetsKernel<<<1, kScanThreads, 0, s>>>(dSums, scanBlocks, dFirst, n_dyes, n_rows_dev);
+   ISCU_CK_LAUNCH(ctx, "ScanOffsetsKernel");
+   ScanWriteKernel<<<scanBlocks, kScanThreads, 0, s>>>(dCounts, n_dyes, dSums, dFirst);
+   ISCU_CK_LAUNCH(ctx, "ScanWriteKernel");
    if (max_rows)
    {
       RowsKernel<<<blocks, 128, 0, s>>>(p);

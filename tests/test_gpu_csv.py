@@ -52,3 +52,45 @@ def test_table_equals_reference(engine, reference):
         engine.csv_table_dev(d, fmts, out_dev=short)
     assert e.value.code == 4 and str(len(want)) in str(e.value)
     assert bytes(short.cpu().numpy()) == want[:1000]
+
+
+def _checker_table(cols, fmts):
+    return "".join(",".join(printf(cols[c, r], fmts[c]) for c in range(len(fmts))) + "\n"
+                   for r in range(cols.shape[1])).encode()
+
+
+def test_table_spans_staged_and_direct(engine):
+    """Rows written through the shared-memory spans (16-byte stores) and straight from the threads (a span longer than
+    the staging buffer, or an output that does not start on 16 bytes), byte for byte against the checker, with the
+    bytes around the text untouched and an output that ends inside the last 16-byte chunk."""
+    import torch
+    rng = np.random.default_rng(9)
+    n = 5000   # 20 spans of 256 rows of 64 columns, each span longer than the staging buffer
+    fmts = ["%d"] + ["%.9f"] * 63
+    cols = rng.normal(0, 1e3, (64, n))
+    cols[0] = np.arange(n)
+    cols[1:, n // 2:] *= 1e12
+    cols[5, 7] = np.nan
+    want = _checker_table(cols, fmts)
+    d = torch.from_numpy(cols).cuda()
+    for start in (0, 3, 16):
+        buf = torch.full((len(want) + 64,), 0xAB, dtype=torch.uint8, device="cuda")
+        got = engine.csv_table_dev(d, fmts, out_dev=buf[start:start + len(want) + 40])
+        assert bytes(got.cpu().numpy()) == want, start
+        b = buf.cpu().numpy()
+        assert not (b[:start] != 0xAB).any() and not (b[start + len(want):] != 0xAB).any(), start
+    # short rows only (every span staged when the output starts on 16 bytes), and the output ending 7 bytes before the
+    # text does
+    small = d[:8, :3000].contiguous()
+    want8 = _checker_table(cols[:8, :3000], fmts[:8])
+    for start in (0, 5, 16):
+        buf = torch.full((len(want8) + 64,), 0xAB, dtype=torch.uint8, device="cuda")
+        got = engine.csv_table_dev(small, fmts[:8], out_dev=buf[start:start + len(want8) + 40])
+        assert bytes(got.cpu().numpy()) == want8, start
+        b = buf.cpu().numpy()
+        assert not (b[:start] != 0xAB).any() and not (b[start + len(want8):] != 0xAB).any(), start
+    buf = torch.full((len(want8) + 32,), 0xAB, dtype=torch.uint8, device="cuda")
+    with pytest.raises(IscuError):
+        engine.csv_table_dev(small, fmts[:8], out_dev=buf[:len(want8) - 7])
+    b = buf.cpu().numpy()
+    assert bytes(b[:len(want8) - 7]) == want8[:-7] and not (b[len(want8) - 7:] != 0xAB).any()

@@ -84,3 +84,22 @@ def test_row_cap_and_empty(engine, dyes):
     assert np.array_equal(small.cpu().numpy(), rows[:10])
     r0, f0 = engine.dye_blinks(LABEL_DSTORM, kin, dyes[:0], 0.0, 10.0)
     assert len(r0) == 0 and list(f0) == [0]
+
+
+@pytest.mark.parametrize("reps", [3, 9, 60])
+def test_first_rows_over_many_scan_blocks(engine, dyes, reps):
+    """The dyes' first rows (an exclusive scan of their counts, 4,096 counts per scan block) over one block and a
+    part (4,500 dyes), several (13,500) and many (90,000): each dye's count and rows as in the short list."""
+    kin = _kin(0.5, 0.01, 0.02, 0.001, 0.7)   # long schedules: counts up to hundreds
+    rows1, first1 = engine.dye_blinks(LABEL_PALM, kin, dyes, 0.0, 20.0)
+    big = np.tile(dyes, reps)
+    rows, first = engine.dye_blinks(LABEL_PALM, kin, big, 0.0, 20.0)
+    assert first[0] == 0 and first[-1] == len(rows) == reps * len(rows1)
+    assert np.array_equal(np.diff(first), np.tile(np.diff(first1), reps))
+    assert np.array_equal(rows, np.tile(rows1, (reps, 1)))
+    import torch   # the same through the scratch first-row array (no caller array)
+    d_dyes = torch.from_numpy(np.ascontiguousarray(big).view(np.uint8)).cuda()
+    out = torch.zeros((len(rows), EVENT_STRIDE), dtype=torch.float64, device="cuda")
+    d_n = torch.zeros(1, dtype=torch.int32, device="cuda")
+    engine.dye_blinks_dev(LABEL_PALM, kin, d_dyes, len(big), 0.0, 20.0, out, d_n)
+    assert int(d_n.item()) == len(rows) and np.array_equal(out.cpu().numpy(), rows)
