@@ -107,6 +107,7 @@ NCU_TRAFFIC = {
     ("two-colour", "GatherTilesKernel"): (2182043649, "profiles/GatherTilesKernel_two_colour.md"),
     ("widefield", "WfNoiseKernel"): (73977088, "profiles/widefield_cells_launches.md"),
     ("widefield", "ZKernel<convolve>"): (1045289728, "profiles/widefield_cells_launches.md"),
+    ("wfshift", "ShiftColumnsKernel+ShiftRowsKernel"): (636056576, "profiles/shift_frames_launches.md"),
 }
 
 
@@ -794,7 +795,7 @@ class ScheduleWorkload:
         return self.h_dyes.numel(), self.h_rows.numel() * 8
 
     def kernel_name(self):
-        return "CountKernel+ScanKernel+RowsKernel"
+        return "CountKernel+ScanSumsKernel+ScanOffsetsKernel+ScanWriteKernel+RowsKernel"
 
     def alg_bytes_per_launch(self):
         # the dyes read by the count and the row pass (48 B each), per-dye counts and first rows (8 B), the rows (80 B)

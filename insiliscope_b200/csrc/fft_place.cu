@@ -8,11 +8,16 @@
 // (complex) values; then the same along the columns; the real part is the shifted plane. That line operation is a
 // convolution: y[i] = sum_j x[j] h(i - j + s) with h(t) = (1/N) sum_kk exp(2 pi i kk t / N), whose geometric sum is
 //   h(t) = sin(pi t) / (N tan(pi t / N)) - i sin(pi t) / N        (t not an integer;  h(d) = [d == 0] for integers),
-// so each emitter is 2 n^3 complex multiply-adds in float64 with no transform: a CTA per emitter holds the plane and
-// the shifted plane in shared memory, evaluates h for the 2n - 1 offsets of each axis once, and produces eight output
-// columns per pass (each a row pass for those columns, then their column pass), so the complex intermediate is never
-// stored whole. The shifted plane's block sums follow as BuildBlockSums (PsfGeneratorBridge.cpp:1021-1047) forms
-// them: float64 row sums over each os x os block, then their sum, rounded to float.
+// whose imaginary part is -(-1)^d sin(pi s) / N at t = d + s: the same magnitude at every offset. So the imaginary
+// halves of both line passes collapse into one number, Z = sum of (-1)^(y + x) K[y][x] over the plane, and the shifted
+// plane is two real convolutions and a rank-one term,
+//   T[i][x] = sum_y Re h_y(i - y) sum_j K[y][j] Re h_x(x - j)  -  (-1)^(i + x) S_x S_y Z,   S = sin(pi s) / N,
+// 2 n^3 float64 multiply-adds per emitter and no transform: a CTA per emitter holds the plane and the shifted plane in
+// shared memory, evaluates Re h for the offsets of each axis once, and produces eight output columns per pass (their
+// row pass, then their column pass, each thread keeping 8 outputs along the line and a 15-value window of h in
+// registers), so the intermediate is never stored whole. The shifted plane's block sums follow as BuildBlockSums
+// (PsfGeneratorBridge.cpp:1021-1047) forms them: float64 row sums over each os x os block, then their sum, rounded to
+// float.
 //
 // Frames in the Fft placement (RenderPhotonImage with a kernel whose interpolation is Fft, SMLMSimulation.cpp:103-160,
 // SplatRows / SplatKernel.inl with one tap): a CTA per 16 x 16 pixels of a frame starts each pixel at its background,
@@ -30,42 +35,68 @@
 namespace iscu {
 namespace {
 
-constexpr int kThreads = 192;   // one thread per row / output index
+constexpr int kThreads = 192;   // a thread per row (row pass) / per column and 8-row block (column pass)
 constexpr int kCols = 8;        // output columns per pass (independent float64 chains per thread)
-constexpr int kMaxN = 157;     // 2 n^2 floats + (12 n - 2) complex doubles within 227 KB of shared memory
+constexpr int kMaxN = 157;      // the planes and the tables below within 227 KB of shared memory
 
-size_t PlaceSmem(int n)
+// Re h(d + s) for the offsets d = -(n - 1) .. n + 6, at index d + n - 1 (the 7 past n - 1 are zero: the padding
+// columns and rows of a pass), stored skewed -- index i in slot i + i / 8 -- so that lanes 8 indices apart read other
+// banks.
+__host__ __device__ constexpr int HSlot(int i) { return i + (i >> 3); }
+__host__ __device__ constexpr int HEntries(int n) { return 2 * n + 6; }
+__host__ __device__ constexpr int HSlots(int n) { return HSlot(HEntries(n) - 1) + 1; }
+// row strides of the plane and of the row pass's columns: odd, so that lanes a row apart read other banks
+__host__ __device__ constexpr int OddStride(int n) { return n | 1; }
+
+// The shifted plane is kept as a ring of its last RingWidth(os) columns (a power of two >= kCols + os - 1: a pass's
+// columns and the os - 1 before them, which its block sums read), row stride RingWidth + 1.
+__host__ __device__ constexpr int RingWidth(int os)
 {
-   return 2 * static_cast<size_t>(n) * n * sizeof(float) + 2 * (2 * static_cast<size_t>(n) - 1) * sizeof(double2) +
-          static_cast<size_t>(kCols) * n * sizeof(double2);
+   int w = 1;
+   while (w < kCols + os - 1)
+      w <<= 1;
+   return w;
 }
 
-// h(d + s) for the 2n - 1 offsets d = -(n - 1) .. n - 1, into h[d + n - 1].
-__device__ void ShiftKernel(double s, int n, int N, double2* h)
+size_t PlaceSmem(int n, int os)
 {
-   for (int i = threadIdx.x; i < 2 * n - 1; i += blockDim.x)
+   const size_t ns = OddStride(n);
+   return 2 * static_cast<size_t>(HSlots(n)) * sizeof(double) + static_cast<size_t>(kCols) * ns * sizeof(double) +
+          (ns * n + static_cast<size_t>(n) * (RingWidth(os) + 1)) * sizeof(float);
+}
+
+__device__ void ShiftKernel(double s, int n, int N, double* h)
+{
+   for (int i = threadIdx.x; i < HEntries(n); i += blockDim.x)
    {
       const int d = i - (n - 1);
-      if (s == 0.0)
+      double v;
+      if (d > n - 1)
+         v = 0.0;
+      else if (s == 0.0)
+         v = d == 0 ? 1.0 : 0.0;
+      else
       {
-         h[i] = make_double2(d == 0 ? 1.0 : 0.0, 0.0);
-         continue;
+         const double t = d + s, u = t / N;
+         v = sinpi(t) * cospi(u) / (N * sinpi(u));
       }
-      const double t = d + s, sp = sinpi(t), u = t / N;
-      h[i] = make_double2(sp * cospi(u) / (N * sinpi(u)), -sp / N);
+      h[HSlot(i)] = v;
    }
 }
 
-__global__ void __launch_bounds__(kThreads) FftPlaceKernel(const iscu_emitter* __restrict__ em,
+__global__ void __launch_bounds__(kThreads, 1) FftPlaceKernel(const iscu_emitter* __restrict__ em,
                                                           const float* __restrict__ planes, int n, int nz, int os,
                                                           float* __restrict__ sums, int32_t* __restrict__ origins)
 {
    extern __shared__ __align__(16) unsigned char smem[];
-   double2* hx = reinterpret_cast<double2*>(smem);
-   double2* hy = hx + (2 * n - 1);
-   double2* M = hy + (2 * n - 1);                                   // kCols columns of the row pass, n each
-   float* K = reinterpret_cast<float*>(M + kCols * n);              // the plane
-   float* T = K + n * n;                                            // the shifted plane
+   __shared__ double warpZ[kThreads / 32];
+   const int ns = OddStride(n);
+   double* hx = reinterpret_cast<double*>(smem);
+   double* hy = hx + HSlots(n);
+   double* M = hy + HSlots(n);                                      // kCols columns of the row pass, stride ns
+   float* K = reinterpret_cast<float*>(M + kCols * ns);             // the plane, row stride ns
+   float* T = K + ns * n;                                           // the shifted plane's last columns (a ring)
+   const int ringMask = RingWidth(os) - 1, rs = RingWidth(os) + 1;
    const int bw = n + os - 1;
    const iscu_emitter m = em[blockIdx.x];
    float* out = sums + static_cast<size_t>(blockIdx.x) * bw * bw;
@@ -90,75 +121,140 @@ __global__ void __launch_bounds__(kThreads) FftPlaceKernel(const iscu_emitter* _
    int N = 1;
    while (N < 2 * n)
       N <<= 1;
+   // the plane, and Z = sum over it of (-1)^(y + x) K[y][x]
    const float* P = planes + static_cast<size_t>(z) * n * n;
-   for (int i = threadIdx.x; i < n * n; i += blockDim.x)
-      K[i] = P[i];
+   double zs = 0.0;
+   for (int i0 = threadIdx.x; i0 < n * n; i0 += 8 * kThreads)
+   {
+      float v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+         v[u] = i0 + u * kThreads < n * n ? __ldg(P + i0 + u * kThreads) : 0.f;
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+      {
+         const int i = i0 + u * kThreads;
+         if (i < n * n)
+         {
+            const int y = i / n, x = i - y * n;
+            K[y * ns + x] = v[u];
+            zs += (x + y) & 1 ? -static_cast<double>(v[u]) : static_cast<double>(v[u]);
+         }
+      }
+   }
+   for (int o = 16; o; o >>= 1)
+      zs += __shfl_down_sync(0xFFFFFFFFu, zs, o);
+   if ((threadIdx.x & 31) == 0)
+      warpZ[threadIdx.x >> 5] = zs;
    ShiftKernel(tx - rx, n, N, hx);
    ShiftKernel(ty - ry, n, N, hy);
    __syncthreads();
-   const int r = threadIdx.x;
+   double Z = 0.0;
+   for (int w = 0; w < kThreads / 32; ++w)
+      Z += warpZ[w];
+   // Im h(d + s) = -(-1)^d sin(pi s) / N, so the imaginary halves of both passes collapse: the shifted plane is
+   // T[i][x] = sum_y Re h_y(i - y) sum_j K[y][j] Re h_x(x - j)  -  (-1)^(i + x) S_x S_y Z,  S = sin(pi s) / N.
+   const double corr = (sinpi(tx - rx) / N) * (sinpi(ty - ry) / N) * Z;
+   const int nb8 = n & ~7;   // the steps of both passes taken eight at a time
    for (int c0 = 0; c0 < n; c0 += kCols)
    {
-      // row pass for columns c0 .. c0 + 7: M[c][y] = sum_j K[y][j] h_x(c0 + c - j)
+      // row pass for columns c0 .. c0 + 7 (a thread per row r): M[c][r] = sum_j K[r][j] Re h_x(c0 + c - j), j in
+      // order. Over steps j .. j + 7 the h indices c0 + c - j' + n - 1 span 15 values: loaded once (all lanes the same).
+      const int r = threadIdx.x;
       if (r < n)
       {
-         double re[kCols] = {}, im[kCols] = {};
-         const float* row = K + r * n;
-         for (int j = 0; j < n; ++j)
+         double re[kCols] = {};
+         const float* row = K + r * ns;
+         const int base = c0 + n - 1;
+         int j = 0;
+         for (; j < nb8; j += 8)
+         {
+            double hw[15];   // hw[t] = h index base - j - 7 + t
+#pragma unroll
+            for (int t = 0; t < 15; ++t)
+               hw[t] = hx[HSlot(base - j - 7 + t)];
+            float kv[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+               kv[u] = row[j + u];
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+            {
+               const double k = kv[u];
+#pragma unroll
+               for (int c = 0; c < kCols; ++c)
+                  re[c] = fma(k, hw[7 - u + c], re[c]);
+            }
+         }
+         for (; j < n; ++j)
          {
             const double k = row[j];
 #pragma unroll
             for (int c = 0; c < kCols; ++c)
-            {
-               const int x = c0 + c;
-               const double2 h = hx[min(x, n - 1) - j + n - 1];
-               re[c] = fma(k, h.x, re[c]);
-               im[c] = fma(k, h.y, im[c]);
-            }
+               re[c] = fma(k, hx[HSlot(base - j + c)], re[c]);
          }
 #pragma unroll
          for (int c = 0; c < kCols; ++c)
-            M[c * n + r] = make_double2(re[c], im[c]);
+            M[c * ns + r] = re[c];
       }
       __syncthreads();
-      // column pass: T[i][x] = Re sum_y h_y(i - y) M[x][y]
-      if (r < n)
+      // column pass (a thread per column c and rows i0 .. i0 + 7): T[i][c0 + c] = sum_y Re h_y(i - y) M[c][y] (y in
+      // order) minus the rank-one term; over steps y .. y + 7 the h indices i - y' + n - 1 span 15 values.
+      const int c = threadIdx.x & (kCols - 1), i0 = (threadIdx.x / kCols) * 8;
+      if (i0 < n)
       {
-         double acc[kCols] = {};
-         for (int y = 0; y < n; ++y)
+         double acc[8] = {};
+         const double* col = M + c * ns;
+         const int base = i0 + n - 1;
+         int y = 0;
+         for (; y < nb8; y += 8)
          {
-            const double2 h = hy[r - y + n - 1];
+            double hw[15];   // hw[t] = h index base - y - 7 + t
 #pragma unroll
-            for (int c = 0; c < kCols; ++c)
+            for (int t = 0; t < 15; ++t)
+               hw[t] = hy[HSlot(base - y - 7 + t)];
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
             {
-               const double2 v = M[c * n + y];
-               acc[c] = fma(h.x, v.x, acc[c]);
-               acc[c] = fma(-h.y, v.y, acc[c]);
+               const double v = col[y + u];
+#pragma unroll
+               for (int k = 0; k < 8; ++k)
+                  acc[k] = fma(hw[7 - u + k], v, acc[k]);
             }
          }
+         for (; y < n; ++y)
+         {
+            const double v = col[y];
 #pragma unroll
-         for (int c = 0; c < kCols; ++c)
-            if (c0 + c < n)
-               T[r * n + c0 + c] = static_cast<float>(acc[c]);
+            for (int k = 0; k < 8; ++k)
+               acc[k] = fma(hy[HSlot(base - y + k)], v, acc[k]);
+         }
+         const int x = c0 + c;
+#pragma unroll
+         for (int k = 0; k < 8; ++k)
+            if (i0 + k < n && x < n)
+               T[(i0 + k) * rs + (x & ringMask)] = static_cast<float>(acc[k] + ((i0 + k + x) & 1 ? corr : -corr));
       }
       __syncthreads();
-   }
-   // block sums of the shifted plane
-   const int off = os - 1;
-   for (int i = threadIdx.x; i < bw * bw; i += blockDim.x)
-   {
-      const int ai = i / bw, bi = i - ai * bw;
-      const int a = ai - off, ya = max(0, a), yb = min(n - 1, a + off);
-      const int b = bi - off, xa = max(0, b), xb = min(n - 1, b + off);
-      double acc = 0.0;
-      for (int y = ya; y <= yb; ++y)
+      // the block sums whose last column is this pass's (all the rest on the last pass), as BuildBlockSums: float64
+      // row sums over the block's columns, then their sum over its rows
+      const int off = os - 1;
+      const int nbi = c0 + kCols >= n ? bw - c0 : kCols;
+      for (int i = threadIdx.x; i < bw * nbi; i += blockDim.x)
       {
-         double hsum = 0.0;
-         for (int x = xa; x <= xb; ++x)
-            hsum += static_cast<double>(T[y * n + x]);
-         acc += hsum;
+         const int ai = i / nbi, bi = c0 + (i - ai * nbi);
+         const int a = ai - off, ya = max(0, a), yb = min(n - 1, a + off);
+         const int b = bi - off, xa = max(0, b), xb = min(n - 1, b + off);
+         double acc = 0.0;
+         for (int y = ya; y <= yb; ++y)
+         {
+            double hsum = 0.0;
+            for (int x = xa; x <= xb; ++x)
+               hsum += static_cast<double>(T[y * rs + (x & ringMask)]);
+            acc += hsum;
+         }
+         out[ai * bw + bi] = static_cast<float>(acc);
       }
-      out[i] = static_cast<float>(acc);
    }
    if (threadIdx.x == 0)
    {
@@ -294,7 +390,7 @@ int iscu_fft_place_dev(iscu_ctx* ctx, int32_t slot, const iscu_emitter* emitters
       return ISCU_OK;
    if (n_emitters > 0x7FFFFFFFu)
       return Fail(ISCU_ERR_LIMIT, "too many emitters per call");
-   const size_t smem = PlaceSmem(k.size);
+   const size_t smem = PlaceSmem(k.size, std::max(1, k.os));
    ISCU_CK(cudaFuncSetAttribute(FftPlaceKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
    FftPlaceKernel<<<n_emitters, kThreads, smem, ctx->stream>>>(emitters_dev, k.planes.as<float>(), k.size, k.nz,
                                                                std::max(1, k.os), sums_dev, origins_dev);

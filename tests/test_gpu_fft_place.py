@@ -78,3 +78,27 @@ def test_fft_frames_equal_reference(engine, reference, halo):
         assert np.abs(got[f] - want).max() <= 1e-6 * np.abs(want).max(), f
     if halo is not None:
         engine.kernel_set_halo(3, 0.0)
+
+
+@pytest.mark.parametrize("n,os_", [(7, 1), (17, 2), (31, 3), (157, 3)])
+def test_plane_sizes(engine, oracle, n, os_):
+    """Plane sizes beside the SMLM kernel's 129 (odd, the half width a multiple of the oversampling): shorter than one
+    eight-step block (7), one past two blocks (17), seven past three (31) and the largest (157), against the float64
+    restatement within 1e-6 of the sums' maximum."""
+    import torch
+    rng = np.random.default_rng(n)
+    nz = 3
+    planes = (rng.random((nz, n, n)) ** 3).astype(np.float32)
+    engine.kernel_set_planes(3, planes, os_, 100.0)
+    xy = rng.uniform(5.0, 60.0, (12, 2))
+    xy[0] = [20.0, 30.0]
+    z = rng.integers(0, nz, len(xy))
+    em = np.zeros(len(z), EMITTER_DTYPE)
+    em["x_px"], em["y_px"], em["plane"], em["photons"] = xy[:, 0], xy[:, 1], z, 500.0
+    sums, origins = engine.fft_place_dev(3, torch.from_numpy(em.view(np.uint8)).cuda())
+    sums, origins = sums.cpu().numpy(), origins.cpu().numpy()
+    for i, ((x, y), p) in enumerate(zip(xy, z)):
+        tile, st = fft_place_f64(planes, os_, x, y, int(p))
+        assert tuple(origins[i]) == st
+        ora = oracle.block_sums(tile[None], os_)[0]
+        assert np.abs(sums[i] - ora).max() <= 1e-6 * np.abs(ora).max(), (n, i)
