@@ -1721,11 +1721,16 @@ int iscu_wf_shifted_frames_dev(iscu_wf_shift* s, const float* spectra_dev, uint3
    if (!n_frames || !n_channels || camW == 0 || camH == 0)
       return ISCU_OK;
    const size_t budget = 200 * 1024;
-   // column pass: BZ columns per CTA, with the row ramp table
+   // column pass: BZ columns per CTA, with the row ramp table; the largest BZ <= 32 that lets two CTAs share an SM,
+   // else the largest that fits one
    const size_t rampBytes = static_cast<size_t>(s->ny) * sizeof(double2);
+   const auto colBytes = [&](int bz) { return rampBytes + static_cast<size_t>(s->ny) * bz * sizeof(float2); };
    int BZ = 1;
-   while (BZ < 32 && rampBytes + static_cast<size_t>(s->ny) * (2 * BZ) * sizeof(float2) <= budget)
+   while (BZ < 32 && colBytes(2 * BZ) <= kSmemPair)
       BZ *= 2;
+   if (colBytes(BZ) > kSmemPair)   // (BZ = 1)
+      while (BZ < 32 && colBytes(2 * BZ) <= budget)
+         BZ *= 2;
    // row pass: BL lines (a power of two >= up), the staged rows and the transform's columns; the largest BL <= 16
    // that lets two CTAs share an SM, else the largest that fits one
    const auto rowBytes = [&](int bl) {
