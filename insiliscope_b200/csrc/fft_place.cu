@@ -13,8 +13,8 @@
 // plane is two real convolutions and a rank-one term,
 //   T[i][x] = sum_y Re h_y(i - y) sum_j K[y][j] Re h_x(x - j)  -  (-1)^(i + x) S_x S_y Z,   S = sin(pi s) / N,
 // 2 n^3 float64 multiply-adds per emitter and no transform: a CTA per emitter holds the plane and the shifted plane in
-// shared memory, evaluates Re h for the offsets of each axis once, and produces eight output columns per pass (their
-// row pass, then their column pass, each thread keeping 8 outputs along the line and a 15-value window of h in
+// shared memory, evaluates Re h for the offsets of each axis once, and produces 16 output columns per pass (their
+// row pass, then their column pass, each thread keeping 16 outputs along the line and a 23-value window of h in
 // registers), so the intermediate is never stored whole. The shifted plane's block sums follow as BuildBlockSums
 // (PsfGeneratorBridge.cpp:1021-1047) forms them: float64 row sums over each os x os block, then their sum, rounded to
 // float.
@@ -35,15 +35,16 @@
 namespace iscu {
 namespace {
 
-constexpr int kThreads = 192;   // a thread per row (row pass) / per column and 8-row block (column pass)
-constexpr int kCols = 8;        // output columns per pass (independent float64 chains per thread)
+constexpr int kThreads = 192;   // a thread per row (row pass) / per column and 16-row block (column pass)
+constexpr int kCols = 16;       // output columns per pass (independent float64 chains per thread of the row pass)
+constexpr int kRB = 16;         // output rows per thread of the column pass
 constexpr int kMaxN = 157;      // the planes and the tables below within 227 KB of shared memory
 
-// Re h(d + s) for the offsets d = -(n - 1) .. n + 6, at index d + n - 1 (the 7 past n - 1 are zero: the padding
+// Re h(d + s) for the offsets d = -(n - 1) .. n + 14, at index d + n - 1 (the 15 past n - 1 are zero: the padding
 // columns and rows of a pass), stored skewed -- index i in slot i + i / 8 -- so that lanes 8 indices apart read other
 // banks.
 __host__ __device__ constexpr int HSlot(int i) { return i + (i >> 3); }
-__host__ __device__ constexpr int HEntries(int n) { return 2 * n + 6; }
+__host__ __device__ constexpr int HEntries(int n) { return 2 * n + (kCols > kRB ? kCols : kRB) - 2; }
 __host__ __device__ constexpr int HSlots(int n) { return HSlot(HEntries(n) - 1) + 1; }
 // row strides of the plane and of the row pass's columns: odd, so that lanes a row apart read other banks
 __host__ __device__ constexpr int OddStride(int n) { return n | 1; }
@@ -84,7 +85,7 @@ __device__ void ShiftKernel(double s, int n, int N, double* h)
    }
 }
 
-__global__ void __launch_bounds__(kThreads, 1) FftPlaceKernel(const iscu_emitter* __restrict__ em,
+__global__ void __launch_bounds__(kThreads, 2) FftPlaceKernel(const iscu_emitter* __restrict__ em,
                                                           const float* __restrict__ planes, int n, int nz, int os,
                                                           float* __restrict__ sums, int32_t* __restrict__ origins)
 {
@@ -158,8 +159,8 @@ __global__ void __launch_bounds__(kThreads, 1) FftPlaceKernel(const iscu_emitter
    const int nb8 = n & ~7;   // the steps of both passes taken eight at a time
    for (int c0 = 0; c0 < n; c0 += kCols)
    {
-      // row pass for columns c0 .. c0 + 7 (a thread per row r): M[c][r] = sum_j K[r][j] Re h_x(c0 + c - j), j in
-      // order. Over steps j .. j + 7 the h indices c0 + c - j' + n - 1 span 15 values: loaded once (all lanes the same).
+      // row pass for columns c0 .. c0 + 15 (a thread per row r): M[c][r] = sum_j K[r][j] Re h_x(c0 + c - j), j in
+      // order. Over steps j .. j + 7 the h indices c0 + c - j' + n - 1 span 23 values: loaded once (all lanes the same).
       const int r = threadIdx.x;
       if (r < n)
       {
@@ -169,9 +170,9 @@ __global__ void __launch_bounds__(kThreads, 1) FftPlaceKernel(const iscu_emitter
          int j = 0;
          for (; j < nb8; j += 8)
          {
-            double hw[15];   // hw[t] = h index base - j - 7 + t
+            double hw[kCols + 7];   // hw[t] = h index base - j - 7 + t
 #pragma unroll
-            for (int t = 0; t < 15; ++t)
+            for (int t = 0; t < kCols + 7; ++t)
                hw[t] = hx[HSlot(base - j - 7 + t)];
             float kv[8];
 #pragma unroll
@@ -198,27 +199,27 @@ __global__ void __launch_bounds__(kThreads, 1) FftPlaceKernel(const iscu_emitter
             M[c * ns + r] = re[c];
       }
       __syncthreads();
-      // column pass (a thread per column c and rows i0 .. i0 + 7): T[i][c0 + c] = sum_y Re h_y(i - y) M[c][y] (y in
-      // order) minus the rank-one term; over steps y .. y + 7 the h indices i - y' + n - 1 span 15 values.
-      const int c = threadIdx.x & (kCols - 1), i0 = (threadIdx.x / kCols) * 8;
+      // column pass (a thread per column c and rows i0 .. i0 + 15): T[i][c0 + c] = sum_y Re h_y(i - y) M[c][y] (y in
+      // order) minus the rank-one term; over steps y .. y + 7 the h indices i - y' + n - 1 span 23 values.
+      const int c = threadIdx.x & (kCols - 1), i0 = (threadIdx.x / kCols) * kRB;
       if (i0 < n)
       {
-         double acc[8] = {};
+         double acc[kRB] = {};
          const double* col = M + c * ns;
          const int base = i0 + n - 1;
          int y = 0;
          for (; y < nb8; y += 8)
          {
-            double hw[15];   // hw[t] = h index base - y - 7 + t
+            double hw[kRB + 7];   // hw[t] = h index base - y - 7 + t
 #pragma unroll
-            for (int t = 0; t < 15; ++t)
+            for (int t = 0; t < kRB + 7; ++t)
                hw[t] = hy[HSlot(base - y - 7 + t)];
 #pragma unroll
             for (int u = 0; u < 8; ++u)
             {
                const double v = col[y + u];
 #pragma unroll
-               for (int k = 0; k < 8; ++k)
+               for (int k = 0; k < kRB; ++k)
                   acc[k] = fma(hw[7 - u + k], v, acc[k]);
             }
          }
@@ -226,12 +227,12 @@ __global__ void __launch_bounds__(kThreads, 1) FftPlaceKernel(const iscu_emitter
          {
             const double v = col[y];
 #pragma unroll
-            for (int k = 0; k < 8; ++k)
+            for (int k = 0; k < kRB; ++k)
                acc[k] = fma(hy[HSlot(base - y + k)], v, acc[k]);
          }
          const int x = c0 + c;
 #pragma unroll
-         for (int k = 0; k < 8; ++k)
+         for (int k = 0; k < kRB; ++k)
             if (i0 + k < n && x < n)
                T[(i0 + k) * rs + (x & ringMask)] = static_cast<float>(acc[k] + ((i0 + k + x) & 1 ? corr : -corr));
       }
