@@ -228,12 +228,26 @@ class SmlmWorkload:
         self.eng.set_render_timing(on)
 
     def dominant(self):
-        """The render's passes, CUDA events inside the library over the timed steps: the slowest with its bytes."""
+        """The render's passes, CUDA events inside the library over the timed steps: the slowest, with the movie's
+        algorithmic bytes (movie_bytes) as the bytes it is judged by; each pass's own traffic as this design moves
+        it (pass_bytes: the two-pass forms' contribution buffer included) in the breakdown."""
         ms, calls = self.eng.render_pass_times()
         name = max(ms, key=ms.get)
         kernel = {"grouping": "ContribSetup/Scan/Scatter", "contributions": "ContribKernel",
                   "tiles": "GatherTilesKernel" if self.form[4] == 2 else "RenderTilesKernel"}[name]
-        return kernel, self.pass_bytes(name), ms[name], {k: round(v, 4) for k, v in ms.items()}
+        passes = ("grouping", "contributions", "tiles") if self.form[4] == 2 else ("tiles",)
+        return kernel, self.movie_bytes(), ms[name], {"pass_ms": {k: round(v, 4) for k, v in ms.items()},
+                                                      "design_bytes": {k: self.pass_bytes(k) for k in passes}}
+
+    def movie_bytes(self):
+        """The step's algorithmic HBM bytes: per frame the ADU written (2 B/px) and the camera maps read as one float4
+        per pixel (16 B/px), per emitter its 64-byte device record; the kernels' block sums (L2-resident) once."""
+        mv = self.mv
+        sums = 0
+        for s in self.slots_used():
+            _, nz, _, bw = self.eng.kernel_info(s)
+            sums += nz * bw * bw * 4
+        return mv.frames * mv.width * mv.height * 18 + self.n_emitters * 64 + sums
 
     def pass_bytes(self, name):
         """Algorithmic HBM bytes of a render pass. Tiles: the ADU written (2 B/px per frame), the three float camera
@@ -270,10 +284,7 @@ class SmlmWorkload:
                 "max_emitters_per_frame": int(self.frames["em_count"].max())}
 
     def alg_bytes_per_launch(self):
-        """A whole render's algorithmic bytes: its passes' (the one-pass forms: the tile pass alone)."""
-        if self.form[4] == 2:
-            return sum(self.pass_bytes(n) for n in ("grouping", "contributions", "tiles"))
-        return self.pass_bytes("tiles")
+        return self.movie_bytes()
 
     # -------------------------------------------------- the reference on the host cores
     dtype = "f64"
@@ -288,7 +299,6 @@ class SmlmWorkload:
 
     def reference_setup(self, threads=0):
         from oracle.oracle import Reference
-        from insiliscope_b200 import generate_camera_maps
         mv = self.mv
         if not Reference.available():
             raise RuntimeError("the reference harness oracle/_ref/libiscref.so is not built (it needs the reference "
@@ -296,7 +306,8 @@ class SmlmWorkload:
         self.ref = Reference()
         self.ref.set_threads(threads)
         self.rk = self.ref.kernel(req=mv.psf)
-        self.maps = generate_camera_maps(mv.width, mv.height, mv.map_seed, mv.offset_mean, mv.offset_std,
+        # the reference's own map generators (PixelOffsetMap / GainMap / ReadNoiseMap), nothing of this package
+        self.maps = self.ref.camera_maps(mv.width, mv.height, mv.map_seed, mv.offset_mean, mv.offset_std,
                                          mv.gain_nominal, mv.gain_std_fraction, mv.read_noise_nominal,
                                          mv.read_noise_std_fraction)
 
@@ -358,7 +369,6 @@ class TwoColourWorkload(SmlmWorkload):
 
     def reference_setup(self, threads=0):
         from oracle.oracle import Reference
-        from insiliscope_b200 import generate_camera_maps
         mv = self.mv
         if not Reference.available():
             raise RuntimeError("the reference harness oracle/_ref/libiscref.so is not built (it needs the reference "
@@ -366,7 +376,7 @@ class TwoColourWorkload(SmlmWorkload):
         self.ref = Reference()
         self.ref.set_threads(threads)
         self.rks = [self.ref.kernel(req=p) for p in mv.psfs]
-        self.maps = generate_camera_maps(mv.width, mv.height, mv.map_seed, mv.offset_mean, mv.offset_std,
+        self.maps = self.ref.camera_maps(mv.width, mv.height, mv.map_seed, mv.offset_mean, mv.offset_std,
                                          mv.gain_nominal, mv.gain_std_fraction, mv.read_noise_nominal,
                                          mv.read_noise_std_fraction)
 
@@ -1322,16 +1332,14 @@ class BinnedWorkload:
         last = int(fr[-1]["em_start"] + fr[-1]["em_count"])
         self.ref_em = self.mv.emitters[:last]
         self.ref_fr = fr
-        if not hasattr(self, "offset"):
-            from insiliscope_b200 import generate_camera_maps
-            self.offset, _, _ = generate_camera_maps(self.mv.width, self.mv.height, 7, 100.0, 2.0, 1.0, 0.0, 50.0, 0.0)
+        self.ref_offset, _, _ = self.ref.camera_maps(self.mv.width, self.mv.height, 7, 100.0, 2.0, 1.0, 0.0, 50.0, 0.0)
 
     def reference_step(self):
         mv = self.mv
         t0 = time.perf_counter()
         img = np.full((len(self.ref_fr), mv.height, mv.width), self.BACKGROUND, np.float32)
         self.ref.binned_render(self.ref_kernel, 0.0, mv.width, mv.height, mv.upscale, self.ref_em, self.ref_fr, img)
-        off = self.offset.reshape(mv.height, mv.width)
+        off = self.ref_offset.reshape(mv.height, mv.width)
         for k in range(len(self.ref_fr)):
             self.ref.noise_chain(img[k], mv.camera, off, None, None, mv.noise_seed, k, parallel=True)
         return time.perf_counter() - t0
@@ -1344,6 +1352,27 @@ WORKLOADS = {"smlm": SmlmWorkload, "widefield": WidefieldWorkload, "psflib": Psf
 
 
 # ----------------------------------------------------------------------------------------------------- arms
+L2_NOTE = "flushed before every timed step (256 MB write)"
+
+
+def common_config(w, n_gpus):
+    """The workload's configuration, the same dict in both arms (the GPU arm's own details go to `details`)."""
+    return {"workload": w.name, "l2": L2_NOTE, "parallelism": f"frames x{n_gpus}"}
+
+
+def repo_libraries():
+    """This repository's shared libraries mapped into the process (which native code ran)."""
+    out = set()
+    try:
+        for line in open("/proc/self/maps"):
+            p = line.split()[-1] if line.strip() else ""
+            if p.endswith(".so") and p.startswith(ROOT):
+                out.add(os.path.relpath(p, ROOT))
+    except OSError:
+        pass
+    return sorted(out)
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -1362,10 +1391,11 @@ def run_reference(args):
     line = {"metric": w.metric, "value": value, "unit": w.metric, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": w.dtype, "data": "synthetic", "impl": "reference",
-            "config": {"workload": w.name, "frames_per_step": w.frames_per_step_cpu},
+            "config": common_config(w, args.gpus),
             "cpu_baseline": {"value": value, "unit": w.metric, "cores": w.cpu_cores(), "kind": w.cpu_kind,
-                             "sample": w.cpu_sample},
-            "e2e": {"value": value, "unit": w.metric, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                             "sample": w.cpu_sample, "units_per_step": w.frames_per_step_cpu},
+            "e2e": {"value": value, "unit": w.metric, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "native_libraries": repo_libraries()}
     print(json.dumps(line))
     return 0
 
@@ -1446,10 +1476,10 @@ def run_ours(args):
     line = {"metric": w.metric, "value": value, "unit": w.metric, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": w.dtype, "data": "synthetic",
-            "config": {"workload": w.name, "frames_per_step": w.frames_per_step, "emitters_per_step": w.n_emitters,
-                       "l2": "flushed before every timed step (256 MB write)", "parallelism": f"frames x{world}",
-                       "psf_build_ms": round(w.psf_build_ms, 3), **(w.config_extra() if hasattr(w, "config_extra")
-                                                                     else {})},
+            "config": common_config(w, world),
+            "details": {"frames_per_step": w.frames_per_step, "emitters_per_step": w.n_emitters,
+                        "psf_build_ms": round(w.psf_build_ms, 3), **(w.config_extra() if hasattr(w, "config_extra")
+                                                                      else {})},
             "e2e": {"value": world * w.frames_per_step / (e2e_ms / 1e3), "unit": w.metric, "ms_per_step": e2e_ms,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "timing": (f"host wall clock over the steps, pipelined over {getattr(w, 'e2e_slots', 3)} I/O "
@@ -1468,9 +1498,16 @@ def run_ours(args):
         line["roofline"]["issued_tflops"] = 3 * achieved
         line["plain_fp32"] = breakdown
     elif breakdown:
-        line["roofline"]["pass_ms"] = breakdown
-        line["roofline"]["step_alg_bytes"] = w.alg_bytes_per_launch()
-        line["roofline"]["step_achieved"] = w.alg_bytes_per_launch() / (statistics.mean(step_ms) / 1e3) / 1e9
+        line["roofline"]["pass_ms"] = breakdown.get("pass_ms", breakdown)
+        if "design_bytes" in breakdown:
+            line["roofline"]["design_bytes_per_pass"] = breakdown["design_bytes"]
+        step_bytes = kbytes if "design_bytes" in breakdown else w.alg_bytes_per_launch()
+        line["roofline"]["step_alg_bytes"] = step_bytes
+        line["roofline"]["step_achieved"] = step_bytes / (statistics.mean(step_ms) / 1e3) / 1e9
+        line["roofline"]["step_frac"] = line["roofline"]["step_achieved"] / peak
+    tr = line["roofline"]["traffic"]
+    if tr:
+        line["roofline"]["traffic_over_alg"] = tr / kbytes if not tensor else None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(w)
     if rank == 0:

@@ -180,8 +180,9 @@ int iscu_psf_plan_run(iscu_psf_plan* plan, const uint32_t* set_of_psf, const dou
  * synchronization a cudaFree implies. Its temporaries (set parameters, PSF items, pupil tables, DFT matrices) live in
  * one statically sized device array of ISCU_NOALLOC_SCRATCH_BYTES that every GPU loading libiscu.so holds until exit;
  * the call itself allocates nothing on the device. Limits: at most ISCU_NOALLOC_MAX_SETS sets and
- * ISCU_NOALLOC_MAX_PSF PSFs, pupil samples M <= 128, plane size <= 129, and the layout within the array (sets,
- * items, M*M*24 bytes of tables and 2*P*M*8 bytes of DFT matrices per set) must fit; beyond: ISCU_ERR_LIMIT.
+ * ISCU_NOALLOC_MAX_PSF PSFs, pupil samples M <= 128, plane size P <= 129 with (M*M + P*M)*8 <= 227 KB (one CTA's
+ * shared memory: at M = 128, P <= 99), and the layout within the array (sets, items, M*M*24 bytes of tables and
+ * 2*P*M*8 bytes of DFT matrices per set) must fit; beyond: ISCU_ERR_LIMIT, before any copy or launch.
  * The first call on a device looks up the array's device address (cudaGetSymbolAddress), so make that first call
  * before any stream capture. All calls share the array: calls whose work overlaps on the GPU (other threads or
  * contexts) race. Returns when the planes are in out_dev. */
@@ -205,6 +206,10 @@ int iscu_kernel_set_planes(iscu_ctx* ctx, int32_t slot, const float* planes, int
                            int32_t oversampling, double z_step_nm, int32_t interp);
 /* The halo cut (WithHaloCut, PsfGeneratorBridge.cpp:1137-1243) for a slot's stack; threshold <= 0 removes it. */
 int iscu_kernel_set_halo(iscu_ctx* ctx, int32_t slot, double threshold);
+/* A cut slot's spans (PsfHaloSpans::lo / hi / radius2, PsfGeneratorBridge.h:228-237): lo and hi nz * (2 camRad + 1)
+ * int16 each (camRad = the half width in camera pixels; a row with lo > hi is empty), radius2 nz int32 (-1: nothing
+ * kept). ISCU_ERR_STATE when the slot has no cut. */
+int iscu_kernel_get_halo(iscu_ctx* ctx, int32_t slot, int16_t* lo, int16_t* hi, int32_t* radius2);
 /* Geometry of a slot: size, nz, oversampling, block-sum width. */
 int iscu_kernel_info(iscu_ctx* ctx, int32_t slot, int32_t* size, int32_t* nz, int32_t* oversampling,
                      int32_t* block_sum_width);

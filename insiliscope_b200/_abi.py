@@ -146,6 +146,7 @@ SIGNATURES = {
     "iscu_kernel_set_planes": (C.c_int, [vp, C.c_int32, vp, C.c_int32, C.c_int32, C.c_int32, C.c_double,
                                          C.c_int32]),
     "iscu_kernel_set_halo": (C.c_int, [vp, C.c_int32, C.c_double]),
+    "iscu_kernel_get_halo": (C.c_int, [vp, C.c_int32, vp, vp, vp]),
     "iscu_kernel_info": (C.c_int, [vp, C.c_int32, i32p, i32p, i32p, i32p]),
     "iscu_kernel_get_planes": (C.c_int, [vp, C.c_int32, vp]),
     "iscu_kernel_get_block_sums": (C.c_int, [vp, C.c_int32, vp]),

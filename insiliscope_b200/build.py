@@ -39,6 +39,7 @@ UNITS = {
     "tiff.cpp": [],
     "csv.cu": [],
     "fft_place.cu": ["--fmad=false"],
+    "halo.cu": [],
     "capi.cpp": [],
     "host_models.cpp": [],
 }

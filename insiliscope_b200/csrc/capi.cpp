@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <random>
 #include <string>
 #include <vector>
@@ -99,112 +100,42 @@ int UploadMap(iscu_ctx* ctx, DevBuf& buf, bool& have, const float* host, size_t 
    return ISCU_OK;
 }
 
-// GaussianRng (SMLMNoise.cpp:17-35) with mean 0, sd 1: direct Box-Muller, two separate draws.
-double MapGauss(std::mt19937_64& rng)
+// The sensor's static maps draw from one std::mt19937_64 stream: the offset map's w h standard normals, then the
+// gain map's, then the read-noise map's -- the order in which the reference generates them (SMLMNoise.cpp:89-140,
+// called offset, gain, read noise by SplatGpu.cpp:500-502). Normal number j is made from engine outputs 2j and 2j + 1
+// taken as uniforms in [0, 1) (std::generate_canonical, what std::uniform_real_distribution(0, 1) returns) by the
+// direct Box-Muller form sqrt(-2 ln a) cos(2 pi b), a raised to 1e-300 (GaussianRng, SMLMNoise.cpp:17-35). A window
+// of rows keeps a slice of each map: the engine jumps over the outputs of the pixels left out with discard().
+class SensorNormalStream
 {
-   std::uniform_real_distribution<double> unif(0.0, 1.0);
-   double u1 = unif(rng);
-   if (u1 < 1e-300)
-      u1 = 1e-300;
-   double u2 = unif(rng);
-   const double z0 = std::sqrt(-2.0 * std::log(u1)) * std::cos(2.0 * 3.14159265358979323846 * u2);
-   return 0.0 + 1.0 * z0;
-}
-
-void SkipGaussians(std::mt19937_64& rng, size_t k)
-{
-   std::uniform_real_distribution<double> unif(0.0, 1.0);
-   for (size_t i = 0; i < 2 * k; ++i)
-      (void)unif(rng);
-}
-
-// A window's rows of a w x h map (SMLMNoise.cpp:66-78's MapRows).
-struct MapRows
-{
-   size_t i0 = 0, i1 = 0, n = 0;
-   MapRows(unsigned w, unsigned h, unsigned keepY0, unsigned keepRows)
+public:
+   explicit SensorNormalStream(uint64_t seed) : eng_(seed) {}
+   // Normal number j of the stream; j may not decrease from one call to the next.
+   double Normal(uint64_t j)
    {
-      const unsigned rows = keepRows ? std::min(keepRows, h - std::min(h, keepY0)) : h;
-      i0 = keepRows ? static_cast<size_t>(keepY0) * w : 0;
-      i1 = i0 + static_cast<size_t>(rows) * w;
-      n = static_cast<size_t>(w) * h;
+      const uint64_t at = 2 * j;
+      if (at > used_)
+      {
+         eng_.discard(at - used_);
+         used_ = at;
+      }
+      const double a = Uniform();
+      const double b = Uniform();
+      return std::sqrt(-2.0 * std::log(a < 1e-300 ? 1e-300 : a)) * std::cos(kTwoPi * b);
    }
+
+private:
+   static constexpr double kTwoPi = 2.0 * 3.14159265358979323846;   // exact doubling of the double nearest pi
+   double Uniform()
+   {
+      ++used_;
+      return std::generate_canonical<double, std::numeric_limits<double>::digits>(eng_);
+   }
+   std::mt19937_64 eng_;
+   uint64_t used_ = 0;
 };
 
-// The halo spans of one plane (HaloPlaneSpans, PsfGeneratorBridge.cpp:1137-1183) from its row-major block sums.
-void HaloPlane(const float* B, int bw, int os, int halfOv, int camRad, double thr, int16_t* lo, int16_t* hi,
-               int32_t& radius2)
-{
-   const int n = 2 * camRad + 1;
-   std::vector<float> colMax(static_cast<size_t>(bw) * n);
-   for (int r = 0; r < bw; ++r)
-   {
-      const float* row = B + static_cast<size_t>(r) * bw;
-      for (int dx = -camRad; dx <= camRad; ++dx)
-      {
-         const int c0 = std::max(0, halfOv - 2 + dx * os), c1 = std::min(bw - 1, halfOv + os + 1 + dx * os);
-         float m = 0.0f;
-         for (int c = c0; c <= c1; ++c)
-            m = std::max(m, row[c]);
-         colMax[static_cast<size_t>(r) * n + (dx + camRad)] = m;
-      }
-   }
-   radius2 = -1;
-   for (int dy = -camRad; dy <= camRad; ++dy)
-   {
-      const int r0 = std::max(0, halfOv - 2 + dy * os), r1 = std::min(bw - 1, halfOv + os + 1 + dy * os);
-      int l = camRad + 1, h = -camRad - 1;
-      for (int dx = -camRad; dx <= camRad; ++dx)
-      {
-         float m = 0.0f;
-         for (int r = r0; r <= r1; ++r)
-            m = std::max(m, colMax[static_cast<size_t>(r) * n + (dx + camRad)]);
-         if (static_cast<double>(m) >= thr)
-         {
-            l = std::min(l, dx);
-            h = std::max(h, dx);
-         }
-      }
-      lo[dy + camRad] = static_cast<int16_t>(l);
-      hi[dy + camRad] = static_cast<int16_t>(h);
-      if (l <= h)
-         radius2 = std::max(radius2, dy * dy + std::max(l * l, h * h));
-   }
-}
-
 } // namespace
-
-int BuildHalo(iscu_ctx* ctx, KernelSlot& k, double threshold)
-{
-   k.halo = false;
-   k.haloThreshold = 0.0;
-   const int camRad = k.halfOv / k.os;
-   // WithHaloCut (PsfGeneratorBridge.cpp:1186-1243): threshold <= 0 or camRad out of range: the whole square.
-   if (!(threshold > 0.0) || camRad < 1 || camRad > 16000)
-      return ISCU_OK;
-   const int n = 2 * camRad + 1;
-   std::vector<float> sums(static_cast<size_t>(k.nz) * k.bw * k.bw);
-   ISCU_CK(cudaMemcpyAsync(sums.data(), k.sums.p, sums.size() * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
-   ISCU_CK(cudaStreamSynchronize(ctx->stream));
-   const double overshoot = k.interp == ISCU_INTERP_CUBIC ? 1.5625 : 1.0;
-   std::vector<int16_t> lo(static_cast<size_t>(n) * k.nz), hi(lo.size());
-   k.radius2Host.assign(static_cast<size_t>(k.nz), -1);
-   for (int z = 0; z < k.nz; ++z)
-      HaloPlane(sums.data() + static_cast<size_t>(z) * k.bw * k.bw, k.bw, k.os, k.halfOv, camRad,
-                threshold / overshoot, lo.data() + static_cast<size_t>(z) * n, hi.data() + static_cast<size_t>(z) * n,
-                k.radius2Host[static_cast<size_t>(z)]);
-   ISCU_CK(k.spanLo.Reserve(lo.size() * sizeof(int16_t)));
-   ISCU_CK(k.spanHi.Reserve(hi.size() * sizeof(int16_t)));
-   ISCU_CK(k.radius2.Reserve(k.radius2Host.size() * sizeof(int32_t)));
-   ISCU_CK(cudaMemcpyAsync(k.spanLo.p, lo.data(), lo.size() * sizeof(int16_t), cudaMemcpyHostToDevice, ctx->stream));
-   ISCU_CK(cudaMemcpyAsync(k.spanHi.p, hi.data(), hi.size() * sizeof(int16_t), cudaMemcpyHostToDevice, ctx->stream));
-   ISCU_CK(cudaMemcpyAsync(k.radius2.p, k.radius2Host.data(), k.radius2Host.size() * sizeof(int32_t),
-                           cudaMemcpyHostToDevice, ctx->stream));
-   ISCU_CK(cudaStreamSynchronize(ctx->stream));
-   k.halo = true;
-   k.haloThreshold = threshold;
-   return ISCU_OK;
-}
 
 } // namespace iscu
 
@@ -341,37 +272,37 @@ int iscu_generate_camera_maps(uint32_t width, uint32_t height, uint64_t seed, do
    ClearError();
    if (width == 0 || height == 0)
       return Fail(ISCU_ERR_ARG, "map size must be > 0");
-   std::mt19937_64 rng(seed);
-   const MapRows R(width, height, keep_y0, keep_rows);
-   const size_t kept = R.i1 - R.i0;
-   // PixelOffsetMap::Generate (SMLMNoise.cpp:89-102).
-   SkipGaussians(rng, R.i0);
-   for (size_t i = 0; i < kept; ++i)
+   const uint64_t n = static_cast<uint64_t>(width) * height;
+   uint32_t y0 = 0, rows = height;
+   if (keep_rows)
    {
-      const float v = static_cast<float>(offset_mean_adu + offset_std_adu * MapGauss(rng));
+      y0 = std::min(keep_y0, height);
+      rows = std::min(keep_rows, height - y0);
+   }
+   const uint64_t first = static_cast<uint64_t>(y0) * width, count = static_cast<uint64_t>(rows) * width;
+   SensorNormalStream s(seed);
+   // The offset map (PixelOffsetMap::Generate, SMLMNoise.cpp:89-102): normals [0, n).
+   for (uint64_t i = 0; i < count; ++i)
+   {
+      const float v = static_cast<float>(offset_mean_adu + offset_std_adu * s.Normal(first + i));
       if (offset)
          offset[i] = v;
    }
-   SkipGaussians(rng, R.n - R.i1);
-   // PixelGainMap::Generate (SMLMNoise.cpp:119-140): floored at 4 % of the nominal gain.
-   SkipGaussians(rng, R.i0);
-   const double floorGain = 0.04 * gain_nominal;
-   for (size_t i = 0; i < kept; ++i)
+   // The gain map (PixelGainMap::Generate, SMLMNoise.cpp:119-140): normals [n, 2n), floored at 4 % of the nominal.
+   const double gainFloor = 0.04 * gain_nominal;
+   for (uint64_t i = 0; i < count; ++i)
    {
-      const double v = gain_nominal * (1.0 + gain_std_fraction * MapGauss(rng));
+      const double v = gain_nominal * (1.0 + gain_std_fraction * s.Normal(n + first + i));
       if (gain)
-         gain[i] = static_cast<float>(v < floorGain ? floorGain : v);
+         gain[i] = static_cast<float>(std::max(v, gainFloor));
    }
-   SkipGaussians(rng, R.n - R.i1);
-   // PixelReadNoiseMap::Generate (SMLMNoise.cpp:104-117): clamped at 0.
-   SkipGaussians(rng, R.i0);
-   for (size_t i = 0; i < kept; ++i)
+   // The read-noise map (PixelReadNoiseMap::Generate, SMLMNoise.cpp:104-117): normals [2n, 3n), not below 0.
+   for (uint64_t i = 0; i < count; ++i)
    {
-      const double v = read_noise_nominal * (1.0 + read_noise_std_fraction * MapGauss(rng));
+      const double v = read_noise_nominal * (1.0 + read_noise_std_fraction * s.Normal(2 * n + first + i));
       if (read_noise)
-         read_noise[i] = static_cast<float>(v < 0.0 ? 0.0 : v);
+         read_noise[i] = static_cast<float>(std::max(v, 0.0));
    }
-   SkipGaussians(rng, R.n - R.i1);
    return ISCU_OK;
 }
 
@@ -512,6 +443,20 @@ int iscu_kernel_set_halo(iscu_ctx* ctx, int32_t slot, double threshold)
       return rc;
    Lock l(ctx);
    return BuildHalo(ctx, ctx->kernels[slot], threshold);
+}
+
+int iscu_kernel_get_halo(iscu_ctx* ctx, int32_t slot, int16_t* lo, int16_t* hi, int32_t* radius2)
+{
+   int rc = CheckSlot(ctx, slot, true);
+   if (rc != ISCU_OK)
+      return rc;
+   if (!lo || !hi || !radius2)
+      return Fail(ISCU_ERR_ARG, "null argument");
+   Lock l(ctx);
+   const KernelSlot& k = ctx->kernels[slot];
+   if (!k.halo)
+      return Fail(ISCU_ERR_STATE, "slot " + std::to_string(slot) + " has no halo cut");
+   return GetHaloSpans(ctx, k, lo, hi, radius2);
 }
 
 int iscu_kernel_info(iscu_ctx* ctx, int32_t slot, int32_t* size, int32_t* nz, int32_t* oversampling,

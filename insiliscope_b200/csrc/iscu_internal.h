@@ -298,7 +298,10 @@ int LaunchNormalizePlanes(iscu_ctx* ctx, float* planes, int planeElems, int nPla
 int BuildPsfLibrary(iscu_ctx* ctx, const iscu_psf_request* sets, uint32_t nSets, const uint32_t* setOfPsf,
                     const double* defocusM, uint32_t nPsf, int32_t size, int32_t normalize, int32_t method,
                     float* out);
+// The halo cut of a slot's stack from its device block sums (halo.cu); threshold <= 0: none.
 int BuildHalo(iscu_ctx* ctx, KernelSlot& k, double threshold);
+// Copies a cut slot's spans (nz (2 camRad + 1) each) and per-plane radius2 (nz) to host memory.
+int GetHaloSpans(iscu_ctx* ctx, const KernelSlot& k, int16_t* lo, int16_t* hi, int32_t* radius2);
 
 // PSF geometry helpers (ZernikePsf.cpp:118-158).
 struct PsfGeometry

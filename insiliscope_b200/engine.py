@@ -274,9 +274,17 @@ class Engine:
     def psf_library_noalloc_dev(self, sets, set_of_psf, defocus_nm, out, size=0, normalize=True):
         """iscu_psf_library_noalloc_dev: the FP32 PSF library with no device allocation in the call (its
         temporaries in the library's static device array); out: a caller-owned (n, P, P) float32 CUDA tensor."""
+        import torch
         reqs = (PsfRequest * len(sets))(*[s.c() for s in sets])
         so = np.ascontiguousarray(set_of_psf, dtype=np.uint32)
         dz = np.ascontiguousarray(defocus_nm, dtype=np.float64)
+        if len(dz) != len(so):
+            raise ValueError(f"defocus_nm has {len(dz)} entries, set_of_psf {len(so)}")
+        P = size if size > 0 else sets[0].geometry()[0]
+        if not (isinstance(out, torch.Tensor) and out.dtype == torch.float32 and out.is_cuda
+                and out.device.index == self.device and out.is_contiguous() and out.numel() >= len(so) * P * P):
+            raise ValueError(f"out must be a contiguous float32 tensor on cuda:{self.device} with at least "
+                             f"{len(so)} x {P} x {P} elements")
         check(self.lib.iscu_psf_library_noalloc_dev(self.h, reqs, len(sets), _ptr(so), _ptr(dz), len(so), size,
                                                     int(normalize), _ptr(out)))
         return out
@@ -347,6 +355,15 @@ class Engine:
 
     def kernel_set_halo(self, slot, threshold):
         check(self.lib.iscu_kernel_set_halo(self.h, slot, float(threshold)))
+
+    def kernel_halo(self, slot):
+        """A cut slot's spans: (lo, hi) of shape (nz, 2 camRad + 1) int16 and radius2 (nz,) int32."""
+        size, nz, os_, _ = self.kernel_info(slot)
+        n = 2 * (((size - 1) // 2) // os_) + 1
+        lo, hi = np.empty((nz, n), np.int16), np.empty((nz, n), np.int16)
+        r2 = np.empty(nz, np.int32)
+        check(self.lib.iscu_kernel_get_halo(self.h, slot, _ptr(lo), _ptr(hi), _ptr(r2)))
+        return lo, hi, r2
 
     def kernel_info(self, slot):
         v = [C.c_int32() for _ in range(4)]

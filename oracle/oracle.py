@@ -17,14 +17,20 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libiscref.so")
-REF_TREE = "/root/reference"
-
 vp = C.c_void_p
 
 
-def build(reference: bool = True) -> None:
-    """Builds liboracle.so, and _ref/libiscref.so when the reference tree is present."""
-    targets = ["oracle"] + (["ref"] if reference and os.path.isdir(REF_TREE) else [])
+def reference_tree(tree: str | None = None) -> str | None:
+    """The reference's source tree: the argument, else $ISC_REFERENCE_TREE; None when neither names a directory."""
+    tree = tree or os.environ.get("ISC_REFERENCE_TREE")
+    return tree if tree and os.path.isdir(tree) else None
+
+
+def build(reference: bool = True, tree: str | None = None) -> None:
+    """Builds liboracle.so, and _ref/libiscref.so when the reference tree is known (argument or $ISC_REFERENCE_TREE)
+    and present; without it an already built _ref/ is kept as it is."""
+    src = reference_tree(tree) if reference else None
+    targets = ["oracle"] + (["ref", f"REF={src}"] if src else [])
     subprocess.run(["make", "-s", "-C", HERE, "-j8", *targets], check=True)
 
 
@@ -227,6 +233,13 @@ class Reference:
         L.ref_shifted_images.argtypes = [C.c_uint, C.c_uint, vp, vp, C.c_int, f64, vp, f64, f64, f64, f64, C.c_uint,
                                          C.c_uint, C.c_uint, C.c_uint, C.c_uint, vp]
         L.ref_plan_splat_fft.argtypes = [vp, f64, f64, C.c_int, vp, vp]
+        L.ref_wf_grid.argtypes = [C.c_int, f64, C.c_uint, C.c_uint, f64, f64, f64, f64, vp]
+        L.ref_wf_scene_create.argtypes = [vp, C.c_int, f64, f64, C.c_uint, C.c_uint, f64, f64, f64, f64, C.c_long,
+                                          C.c_uint, vp, f64, C.c_int, vp]
+        L.ref_wf_scene_create.restype = vp
+        L.ref_wf_scene_series.argtypes = [vp, vp, C.c_uint, vp]
+        L.ref_wf_scene_series.restype = f64
+        L.ref_wf_scene_destroy.argtypes = [vp]
         L.ref_plan_splat_fft.restype = C.c_int
         L.ref_plan_splat_fft_batch.argtypes = [vp, vp, vp, u32]
         L.ref_plan_splat_fft_batch.restype = f64
@@ -515,6 +528,30 @@ class RefKernel:
     def halo(self, threshold):
         return RefKernel(self.ref, handle=self.ref.L.ref_kernel_halo(self.h, threshold))
 
+    def wf_grid(self, upscale, pixel_um, width, height, origin_um, margin_um, zplane_nm):
+        """WidefieldScene::GridSpecFor of the widefield scene below: (grid nx, grid ny, FOV cell x0, FOV cell y0)."""
+        g = np.zeros(4, np.uint32)
+        self.ref.L.ref_wf_grid(upscale, pixel_um, width, height, origin_um[0], origin_um[1], margin_um, zplane_nm,
+                               _p(g))
+        return tuple(int(v) for v in g)
+
+    def wf_scene(self, counts, upscale, cap_um, pixel_um, width, height, origin_um, margin_um, zplane_nm, k0=0,
+                 focus0_um=0.0, gpu_mode=True):
+        """The reference's widefield scene (WidefieldScene over KernelWidefieldPsf of this kernel) on a dense
+        persistent dye grid counts (nzd, gny, gnx), the grid wf_grid gives."""
+        return RefWfScene(self, counts, upscale, cap_um, pixel_um, width, height, origin_um, margin_um, zplane_nm,
+                          k0, focus0_um, gpu_mode)
+
+    def wf_focus_series(self, counts, foci_um, upscale, cap_um, pixel_um, width, height, origin_um, margin_um,
+                        zplane_nm, k0=0, gpu_mode=True):
+        """wf_scene(...).series(foci_um): camera frames (n, height, width) float32 and (FFT nx, FFT ny, radius)."""
+        sc = self.wf_scene(counts, upscale, cap_um, pixel_um, width, height, origin_um, margin_um, zplane_nm, k0,
+                           foci_um[0], gpu_mode)
+        try:
+            return sc.series(foci_um)[0], sc.info
+        finally:
+            sc.close()
+
     def spans(self):
         size, nz, os_, _ = self.info()
         cam = ((size - 1) // 2) // os_
@@ -560,6 +597,42 @@ class RefKernel:
                                         bg, C.byref(cam), _p(f(offset)), _p(f(gain)), _p(f(read_noise)), seed,
                                         _p(ph), _p(adu))
         return t, ph, adu
+
+
+class RefWfScene:
+    """A reference WidefieldScene (ref_wf_scene_create): series(foci) -> (frames, wall seconds)."""
+
+    def __init__(self, kernel, counts, upscale, cap_um, pixel_um, width, height, origin_um, margin_um, zplane_nm, k0,
+                 focus0_um, gpu_mode):
+        self.L = kernel.ref.L
+        self.counts = np.ascontiguousarray(counts, np.float32)
+        self.shape = (height, width)
+        info = np.zeros(3, np.uint32)
+        self.h = self.L.ref_wf_scene_create(kernel.h, upscale, cap_um, pixel_um, width, height, origin_um[0],
+                                            origin_um[1], margin_um, zplane_nm, k0, self.counts.shape[0],
+                                            _p(self.counts), focus0_um, int(gpu_mode), _p(info))
+        if not self.h:
+            raise RuntimeError(self.L.ref_last_error().decode())
+        self.info = tuple(int(v) for v in info)
+
+    def series(self, foci_um):
+        foci = np.ascontiguousarray(foci_um, np.float64)
+        out = np.zeros((len(foci),) + self.shape, np.float32)
+        sec = self.L.ref_wf_scene_series(self.h, _p(foci), len(foci), _p(out))
+        if sec < 0:
+            raise RuntimeError(self.L.ref_last_error().decode())
+        return out, sec
+
+    def close(self):
+        if self.h:
+            self.L.ref_wf_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def binned_cell_kernels_f64(planes, os_, upscale, radius2=None):
@@ -710,13 +783,50 @@ def shifted_frame_f64(spectra, coef, shift, nx, ny, window, up, scale=1.0):
     return cam.astype(np.float32)
 
 
+def wf_kernel_volume_f64(cell_kernels, zstep_nm, zplane_nm, nzd):
+    """The widefield scene's kernel for every dye-plane-to-focus offset of a focus series taken at the dye planes'
+    centres, as one (2 nzd - 1)-plane volume: plane j serves a dye plane d = nzd - 1 - j planes above the focus
+    (defocus d zplane). PlanFocus (WidefieldRender.cpp:1460-1522) with KernelWidefieldPsf::PlaneCoord (:282-287):
+    t = defocus 1000 / zStep + (nz - 1) / 2 clamped to the stack [0, nz - 1], p0 = floor(t) (the last plane: frac 0),
+    weights (1 - frac, frac) as float32; the plane w0 K[p0] + w1 K[p0 + 1] in float64."""
+    K = np.asarray(cell_kernels, np.float64)
+    nzk = K.shape[0]
+    out = np.zeros((2 * nzd - 1,) + K.shape[1:], np.float64)
+    for j in range(2 * nzd - 1):
+        d = nzd - 1 - j
+        t = d * zplane_nm / zstep_nm + (nzk - 1) / 2.0 if nzk > 1 and zstep_nm > 0 else 0.0
+        t = min(nzk - 1.0, max(0.0, t))
+        p0 = int(np.floor(t))
+        frac = t - p0
+        if p0 >= nzk - 1:
+            p0, frac = nzk - 1, 0.0
+        out[j] = float(np.float32(1.0 - frac)) * K[p0]
+        if frac > 0.0:
+            out[j] += float(np.float32(frac)) * K[p0 + 1]
+    return out
+
+
+def wf_scene_f64(counts, kernel_volume, fov, upscale):
+    """The widefield scene's camera frames in float64 for foci at the dye planes' centres: per focus f the linear
+    convolution sum_k counts[k] (x) kernel_volume[f - k + nzd - 1] over the whole grid (ChannelImageStep /
+    ChannelImageFinish, WidefieldRender.cpp:1724-1878), the FOV cells (x0, y0, cw, ch) cut out, then each camera pixel
+    the sum of max(0, cell) over its upscale x upscale cells (WidefieldImages::Render, :547-586)."""
+    x0, y0, cw, ch = fov
+    u = int(upscale)
+    full = fft_convolve_same_f64(counts, kernel_volume)
+    cells = np.maximum(full[:, y0:y0 + ch, x0:x0 + cw], 0.0)
+    n = cells.shape[0]
+    return cells.reshape(n, ch // u, u, cw // u, u).sum(axis=(2, 4))
+
+
 def fft_convolve_same_f64(volume: np.ndarray, psf: np.ndarray) -> np.ndarray:
     """Linear 3D convolution of volume (nz, ny, nx) with psf (kz, ky, kx) centred on (kz//2, ky//2, kx//2), cropped
     to the volume, in float64 (the widefield mean-field focus series' oracle)."""
     v = np.asarray(volume, np.float64)
     k = np.asarray(psf, np.float64)
     shape = [a + b - 1 for a, b in zip(v.shape, k.shape)]
-    F = np.fft.rfftn(v, shape) * np.fft.rfftn(k, shape)
-    full = np.fft.irfftn(F, shape)
+    axes = list(range(v.ndim))
+    F = np.fft.rfftn(v, shape, axes=axes) * np.fft.rfftn(k, shape, axes=axes)
+    full = np.fft.irfftn(F, shape, axes=axes)
     sl = tuple(slice(kk // 2, kk // 2 + n) for kk, n in zip(k.shape, v.shape))
     return full[sl]

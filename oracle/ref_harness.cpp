@@ -614,6 +614,110 @@ void ref_shifted_images(unsigned nx, unsigned ny, const float* spec0, const floa
    std::copy(img.begin(), img.end(), cam);
 }
 
+// The reference's widefield scene on a dense persistent dye grid: WidefieldScene::GridSpecFor / UpdateFromGrid /
+// FocusSeries (WidefieldRender.cpp:891, :1180, :2845) with KernelWidefieldPsf(kernel, upscale) (:263-330) under a
+// FlatIllumination wider than any margin, unit frame dose and collection efficiency 1 (a cell's value is its dye
+// count: the mean-field image of one structure), each focus's images binned by WidefieldImages::Render (:547) into a
+// width x height camera frame.
+struct RefWfScene
+{
+   sim::WidefieldSceneSpec spec;
+   sim::FlatIllumination pattern{1e6, 1e6};
+   std::unique_ptr<sim::KernelWidefieldPsf> psf;
+   sim::WidefieldScene scene;
+};
+
+static sim::WidefieldSceneSpec WfSpec(int upscale, double capUm, double pixelUm, unsigned width, unsigned height,
+                                      double originXUm, double originYUm, double marginUm, double zPlaneNm)
+{
+   sim::WidefieldSceneSpec spec;
+   spec.originXUm = originXUm;
+   spec.originYUm = originYUm;
+   spec.width = width;
+   spec.height = height;
+   spec.pixelUm = pixelUm;
+   spec.grid.upscale = upscale;
+   spec.grid.zPlaneNm = zPlaneNm;
+   spec.marginUm = marginUm;
+   spec.kernelCapUm = capUm;
+   spec.unitDose = 1.0;
+   spec.eta = 1.0;
+   spec.bleachingMask = 0;
+   spec.persistentMask = 1;
+   return spec;
+}
+
+// The grid such a scene renders on: grid4 = (nx, ny, FOV cell x0, FOV cell y0).
+void ref_wf_grid(int upscale, double pixelUm, unsigned width, unsigned height, double originXUm, double originYUm,
+                 double marginUm, double zPlaneNm, unsigned* grid4)
+{
+   const auto spec = WfSpec(upscale, 1.0, pixelUm, width, height, originXUm, originYUm, marginUm, zPlaneNm);
+   unsigned fx = 0, fy = 0;
+   const sim::WidefieldGridSpec g = sim::WidefieldScene::GridSpecFor(sim::FlatIllumination(1e6, 1e6), spec, &fx, &fy);
+   grid4[0] = g.nx;
+   grid4[1] = g.ny;
+   grid4[2] = fx;
+   grid4[3] = fy;
+}
+
+// The scene over kernel h and counts (nzd x ny x nx of the grid above; plane i at world plane k0 + i), focused at
+// focus0; gpuMode: power-of-two FFTs, no coarse bands (WidefieldScene::SetGpuMode). info3 = (FFT nx, FFT ny, kernel
+// radius). Null (the error in ref_last_error) on a failure.
+void* ref_wf_scene_create(void* h, int upscale, double capUm, double pixelUm, unsigned width, unsigned height,
+                          double originXUm, double originYUm, double marginUm, double zPlaneNm, long k0, unsigned nzd,
+                          const float* counts, double focus0, int gpuMode, unsigned* info3)
+{
+   auto s = std::make_unique<RefWfScene>();
+   s->spec = WfSpec(upscale, capUm, pixelUm, width, height, originXUm, originYUm, marginUm, zPlaneNm);
+   s->spec.focusWorldUm = focus0;
+   const sim::WidefieldGridSpec g = sim::WidefieldScene::GridSpecFor(s->pattern, s->spec);
+   sim::WidefieldDyeGrid grid;
+   grid.spec = g;
+   grid.k0 = k0;
+   grid.nz = nzd;
+   grid.persistent.assign(counts, counts + static_cast<size_t>(nzd) * g.nx * g.ny);
+   double total = 0.0;
+   for (float v : grid.persistent)
+      total += v;
+   grid.nPersistent = static_cast<long>(total + 0.5);
+   s->psf = std::make_unique<sim::KernelWidefieldPsf>(*static_cast<const sim::PsfKernelCache*>(h), upscale);
+   s->scene.SetGpuMode(gpuMode != 0);
+   std::string err;
+   if (!s->scene.UpdateFromGrid(grid, s->pattern, s->spec, *s->psf, err))
+   {
+      g_err = err;
+      return nullptr;
+   }
+   info3[0] = s->scene.FftSizeX();
+   info3[1] = s->scene.FftSizeY();
+   info3[2] = static_cast<unsigned>(s->scene.KernelRadius());
+   return s.release();
+}
+
+// FocusSeries at nFoci foci (world um), each focus's camera frame (width x height, Render from 0) into out. Returns
+// the wall seconds of the series and the renders, or -1 (the error in ref_last_error).
+double ref_wf_scene_series(void* sc, const double* foci, unsigned nFoci, float* out)
+{
+   auto* s = static_cast<RefWfScene*>(sc);
+   const auto t0 = std::chrono::steady_clock::now();
+   std::vector<sim::WidefieldImages> images;
+   std::string err;
+   if (!s->scene.FocusSeries(std::vector<double>(foci, foci + nFoci), images, err))
+   {
+      g_err = err;
+      return -1.0;
+   }
+   const size_t frame = static_cast<size_t>(s->spec.width) * s->spec.height;
+   sim::ParallelFor(nFoci, [&](unsigned i) {
+      std::vector<float> cam(frame, 0.0f);
+      images[i].Render({}, cam);
+      std::copy(cam.begin(), cam.end(), out + i * frame);
+   });
+   return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void ref_wf_scene_destroy(void* sc) { delete static_cast<RefWfScene*>(sc); }
+
 // PlanSplat with the Fft placement (PsfGeneratorBridge.cpp:1441-1456) for an emitter at (x, y) px on plane z of
 // kernel cache h: its shifted block sums (bw x bw floats) into sums and (x0, y0, bx, by) into st4. Returns bw, or 0
 // when PlanSplat refuses.

@@ -10,7 +10,7 @@
                       inputs: camera maps, noise chain (sCMOS and EMCCD), a kernel stack, its block sums and rendered
                       frames -- the absolute ADU values no committed reference golden pins (glibc version recorded).
 
-Usage: python tests/golden/make_golden.py   (needs /root/reference and `make -C oracle ref`)
+Usage: ISC_REFERENCE_TREE=<reference tree> python tests/golden/make_golden.py   (after `make -C oracle ref`)
 """
 from __future__ import annotations
 
@@ -25,7 +25,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = "/root/reference"
+REF = os.environ.get("ISC_REFERENCE_TREE", "")
 sys.path.insert(0, ROOT)
 
 
@@ -111,6 +111,8 @@ def make_ref_outputs():
 
 
 if __name__ == "__main__":
+    if not os.path.isdir(REF):
+        sys.exit("set ISC_REFERENCE_TREE to the reference's source tree")
     make_pcg4d()
     make_zernike()
     make_ref_outputs()

@@ -46,6 +46,23 @@ def test_camera_maps_match_oracle(lib, oracle):
             assert np.array_equal(x, y)
 
 
+def test_camera_maps_match_reference(lib, reference):
+    """The maps equal the reference's PixelOffsetMap / PixelGainMap / PixelReadNoiseMap (SMLMNoise.cpp:89-140,
+    compiled from its sources) bit for bit: whole sensors, row windows (first rows, middle, last rows, past the end),
+    the gain floor reached (a large spread) and the read-noise clamp at 0."""
+    from insiliscope_b200 import generate_camera_maps
+    cases = [(128, 128, 42, 0, 0, 0.1 / 2.2, 0.2), (256, 256, 42, 0, 0, 0.1 / 2.2, 0.2), (37, 23, 7, 0, 5, 0.3, 0.4),
+             (37, 23, 7, 9, 6, 0.3, 0.4), (37, 23, 7, 20, 10, 0.3, 0.4), (64, 16, 3, 2, 1, 1.5, 1.5),
+             (1, 1, 5, 0, 0, 0.1, 0.1)]
+    for w, h, seed, y0, rows, gfrac, rfrac in cases:
+        a = generate_camera_maps(w, h, seed, 100.0, 2.0, 2.2, gfrac, 1.5, rfrac, y0, rows)
+        b = reference.camera_maps(w, h, seed, 100.0, 2.0, 2.2, gfrac, 1.5, rfrac, y0, rows)
+        for x, y in zip(a, b):
+            assert x.shape == y.shape and np.array_equal(x, y), (w, h, seed, y0, rows)
+    g = generate_camera_maps(64, 16, 3, 100.0, 2.0, 2.2, 1.5, 1.5, 1.5)
+    assert (g[1] == np.float32(0.04 * 2.2)).any() and (g[2] == 0).any()   # the floor and the clamp were exercised
+
+
 def test_psf_geometry_matches_oracle(lib, oracle):
     from insiliscope_b200 import PsfParams
     for half, os_, nz, m, wl in ((16, 4, 49, 64, 670.0), (8, 4, 64, 128, 520.0), (70, 4, 71, 0, 660.0),

@@ -142,3 +142,22 @@ def test_reference_records_selfcheck(engine, reference, oracle, emccd):
     same = (got == want).mean()
     assert same >= 0.99, same
     assert np.abs(got.astype(float) - want).sum() <= 0.001 * want.sum()
+
+
+@pytest.mark.parametrize("interp,half,thr", [(INTERP_CUBIC, 16, 1e-4), (INTERP_CUBIC, 7, 2e-3), (INTERP_LINEAR, 9, 5e-4),
+                                             (INTERP_NEAREST, 12, 1e-5), (INTERP_CUBIC, 16, 0.5)])
+def test_halo_spans_equal_reference(engine, reference, interp, half, thr):
+    """The halo cut computed on the device from the resident block sums equals the reference's WithHaloCut spans
+    (PsfHaloSpans lo / hi / radius2) for every plane and row, empty rows and a threshold nothing reaches included."""
+    req = _kernel_req(interp, half=half, nz=13)
+    k = reference.kernel(req=req)
+    engine.kernel_set_planes(2, k.planes(), 4, 60.0, interp)
+    engine.kernel_set_halo(2, thr)
+    lo, hi, r2 = engine.kernel_halo(2)
+    want = k.halo(thr).spans()
+    assert want is not None
+    assert np.array_equal(lo.ravel(), want[0]) and np.array_equal(hi.ravel(), want[1])
+    assert np.array_equal(r2, want[2])
+    if thr >= 0.5:
+        assert (r2 == -1).all() and (lo > hi).all()
+    engine.kernel_set_halo(2, 0.0)
