@@ -146,10 +146,16 @@ class SmlmWorkload:
     name = "smlm-dstorm sCMOS 128x128 px, 200 frames, 4000 sites, ~160 ON/frame, 129^2x49 cubic PSF"
     metric = "frames/s"
 
+    FRAMES_PER_RANK = 200
+
     def __init__(self, rank: int):
+        from insiliscope_b200.shard import frame_range
         from insiliscope_b200.workloads import smlm_dstorm
-        self.mv = smlm_dstorm(seed=42, frame0=rank * 200)
-        self.frame0 = rank * 200
+        # weak scaling: the whole job renders a 200 N-frame movie, rank r its frame_range (200 frames from 200 r)
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        first, end = frame_range(rank, world, self.FRAMES_PER_RANK * world)
+        self.mv = smlm_dstorm(seed=42, frames=end - first, frame0=first)
+        self.frame0 = first
 
     # -------------------------------------------------- ours
     def setup(self, device: int, form=None):
@@ -238,6 +244,38 @@ class SmlmWorkload:
         passes = ("grouping", "contributions", "tiles") if self.form[4] == 2 else ("tiles",)
         return kernel, self.movie_bytes(), ms[name], {"pass_ms": {k: round(v, 4) for k, v in ms.items()},
                                                       "design_bytes": {k: self.pass_bytes(k) for k in passes}}
+
+    def time_render(self, form, reps=5, graph=None):
+        """ms per render of the batch in render form `form` (direct launches; or a captured graph's replays)."""
+        import torch
+        if graph is None:
+            self.eng.set_render_config(form)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        step = graph.launch if graph is not None else SmlmWorkload.device_step.__get__(self)
+        with torch.cuda.stream(self.stream):
+            step() if graph is None else step(sync=False)
+            s.record(self.stream)
+            for _ in range(reps):
+                step() if graph is None else step(sync=False)
+            e.record(self.stream)
+        e.synchronize()
+        return s.elapsed_time(e) / reps
+
+    def plain_form(self, step_ms):
+        """The batching pattern against the plain form on this GPU: the autotuned form (launched directly and, where
+        the step replays a captured graph, as the step), the same tile's persistent heaviest-frame-first form, and
+        the plain grid form (form 0: one pass, one CTA per 16 x 16 tile, no persistence, no graph)."""
+        auto = self.form[0]
+        persistent = 6 * (auto // 6) + 3 + auto % 3
+        grid = 6 * (auto // 6) + auto % 3
+        out = {"step_ms": round(step_ms, 4), "autotuned_form": auto,
+               "autotuned_direct_ms": round(self.time_render(auto), 4),
+               "persistent_form": persistent, "persistent_ms": round(self.time_render(persistent), 4),
+               "grid_form": grid, "grid_ms": round(self.time_render(grid), 4),
+               "plain_form": 0, "plain_ms": round(self.time_render(0), 4)}
+        self.eng.set_render_config(auto)
+        out["speedup_vs_plain"] = round(out["plain_ms"] / step_ms, 3)
+        return out
 
     def movie_bytes(self):
         """The step's algorithmic HBM bytes: per frame the ADU written (2 B/px) and the camera maps read as one float4
@@ -362,10 +400,16 @@ class TwoColourWorkload(SmlmWorkload):
         d["cuda_graph"] = True
         return d
 
-    cpu_sample = ("the whole 1024-frame movie per step: per frame the reference's RenderPhotonImage for channel 0, "
-                  "then for channel 1 accumulating onto it (each with its own kernel), then ApplyNoiseChain; frames in "
-                  "parallel on its own thread pool (ParallelFor), kernels built once before timing")
-    frames_per_step_cpu = 1024
+    def plain_form(self, step_ms):
+        out = SmlmWorkload.plain_form(self, step_ms)
+        out["graph_replay_ms"] = round(self.time_render(None, graph=self.graph), 4)
+        return out
+
+    cpu_sample = ("the movie's last 256 frames per step (25 % of its emitters, its heaviest frame among them): per "
+                  "frame the reference's RenderPhotonImage for channel 0, then for channel 1 accumulating onto it "
+                  "(each with its own kernel), then ApplyNoiseChain; frames in parallel on its own thread pool "
+                  "(ParallelFor), kernels built once before timing")
+    frames_per_step_cpu = 256
 
     def reference_setup(self, threads=0):
         from oracle.oracle import Reference
@@ -382,44 +426,53 @@ class TwoColourWorkload(SmlmWorkload):
 
     def reference_step(self):
         mv = self.mv
-        t, _, _ = self.ref.render_movie_groups(self.rks, mv.events, self.frame0, mv.frames, mv.width, mv.height,
+        first = self.frame0 + mv.frames - self.frames_per_step_cpu
+        t, _, _ = self.ref.render_movie_groups(self.rks, mv.events, first, self.frames_per_step_cpu, mv.width,
+                                               mv.height,
                                                mv.pixel_nm, mv.photons_per_blink, mv.background, mv.camera,
                                                *self.maps, mv.noise_seed)
         return t
 
 
 class WidefieldWorkload:
-    """The widefield mean-field focus series: a 512 x 512 x 64 dye volume convolved with a 512 x 512 x 64 3D PSF
-    (1024 x 1024 x 128 FFT grid), max(0, .) + 5 photons/px background, EMCCD chain; one step = 64 frames."""
-    name = ("widefield 3D FFT convolution 512x512x64 volume (50 cells, nuclei, 200 filaments each) x 512x512x64 "
-            "Gibson-Lanni PSF (NA 1.4, 520 nm), EMCCD gain 300, 5 photons/px background")
+    """The widefield mean-field focus series as the reference's widefield scene: a 512 x 512 x 64 dye grid of
+    100 x 100 x 200 nm cells imaged at every plane's centre through the 3D Gibson-Lanni kernel stack (513 x 513
+    samples, 65 planes 200 nm apart, built on the device; a dye plane beyond the stack's reach seen through its last
+    plane, as PlanFocus clamps), the kernel radius uncapped (256 cells), linear convolution on a 1024 x 1024 x 128 FFT
+    grid, max(0, .) + 5 photons/px background, EMCCD chain; one step = 64 frames."""
+    name = ("widefield 3D FFT convolution 512x512x64 volume (50 cells, nuclei, 200 filaments each) x 513x513x65 "
+            "Gibson-Lanni kernel stack (NA 1.4, 520 nm), EMCCD gain 300, 5 photons/px background")
     metric = "frames/s"
 
     # pass names and their algorithmic bytes (computed in setup)
     PASSES = ("XForwardKernel", "YForwardKernel", "ZKernel<convolve>", "YInverseKernel", "XInverseKernel",
               "WfNoiseKernel")
     e2e_stages = "the six FFT-convolution and noise passes"
+    KERNEL_CAP_UM = 30.0
 
     def __init__(self, rank: int):
         from insiliscope_b200.workloads import widefield_cells
         self.rank = rank
         self.wv = widefield_cells(seed=42 + rank)
         self.frame0 = rank * 64
+        req = self.wv.psf
+        req.nz = 65
+        req.kernel_half_width_px = 256
+        self.req = req
 
     def setup(self, device: int):
         import torch
-        from insiliscope_b200 import Engine, WidefieldPlan, generate_camera_maps
+        from insiliscope_b200 import CZT_FP32, Engine, WidefieldPlan, generate_camera_maps
         wv = self.wv
         nz, ny, nx = wv.density.shape
         self.eng = eng = Engine(device)
         t0 = time.perf_counter()
-        kz, ky, kx = wv.psf_shape
-        psf = eng.psf_library_dev([wv.psf], np.zeros(kz, np.uint32), wv.psf_defocus_nm, size=kx,
-                                  normalize=True).cpu().numpy()
+        eng.kernel_build(0, self.req, CZT_FP32)
         eng.synchronize()
         self.psf_build_ms = (time.perf_counter() - t0) * 1e3
         t0 = time.perf_counter()
-        self.plan = WidefieldPlan(eng, (nz, ny, nx), psf)
+        self.plan = WidefieldPlan.from_kernel(eng, 0, 1, wv.voxel_nm[0] / 1000.0, self.KERNEL_CAP_UM, wv.voxel_nm[2],
+                                              (nz, ny, nx), (0, 0, nx, ny))
         self.plan_ms = (time.perf_counter() - t0) * 1e3
         off, _, _ = generate_camera_maps(nx, ny, wv.map_seed, wv.offset_mean, wv.offset_std, 1.0, 0.0, 50.0, 0.0)
         eng.set_static(nx, ny, offset=off)
@@ -488,41 +541,52 @@ class WidefieldWorkload:
     def kernel_name(self):
         return "widefield step (6 passes)"
 
-    # -------------------------------------------------- CPU: the float64 FFT convolution port (scipy, all cores)
+    def config_extra(self):
+        return {"plan_ms": round(self.plan_ms, 3), "fft_grid": list(self.plan.grid()),
+                "kernel_radius_cells": self.plan.kernel_radius}
+
+    # -------------------------------------------------- CPU: the reference's widefield scene on the host cores
     dtype = "f32"
-    frames_per_step_cpu = 64
-    cpu_kind = "port"
-    cpu_sample = ("the whole 64-frame focus series per step: float64 3D FFT convolution on the same padded grid "
-                  "(scipy.fft, all cores; the PSF spectrum precomputed, as the plan keeps it) + max(0, .) + background "
-                  "+ the oracle's EMCCD chain (frames in parallel)")
+    frames_per_step_cpu = 8
+    cpu_kind = "reference"
+    cpu_sample = ("8 of the 64 foci per step: the reference's WidefieldScene::FocusSeries (its plane and kernel "
+                  "spectra cached from the scene's set-up, as the reference keeps them; GPU mode: power-of-two FFTs) "
+                  "+ WidefieldImages::Render per focus on its thread pool, then its ApplyNoiseChain (EMCCD) per frame "
+                  "with the background; the scene over the reference's own 513 x 513 x 65 kernel stack "
+                  "(ComputeZernikePsfPlanes), compiled from its sources")
 
     def reference_setup(self, threads=0):
-        import scipy.fft as sf
-        from oracle.oracle import Oracle
-        self.orc = Oracle()
-        kz, ky, kx = self.wv.psf_shape
-        k = np.zeros((kz, ky, kx))
-        k[kz // 2, ky // 2, kx // 2] = 1.0   # the timing does not depend on the PSF's values
-        self.shape = [1 << int(np.ceil(np.log2(a + b - 1))) for a, b in zip(self.wv.density.shape, k.shape)]
-        self.Kf = sf.rfftn(k, self.shape, workers=-1)
-        self.kshape = k.shape
+        from oracle.oracle import Reference
+        if not Reference.available():
+            raise RuntimeError("the reference harness oracle/_ref/libiscref.so is not built (it needs the reference "
+                               "tree at build time)")
+        wv = self.wv
+        nz, ny, nx = wv.density.shape
+        self.ref = Reference()
+        self.ref.set_threads(threads)
+        self.rk = self.ref.kernel(req=self.req)
+        gx, gy, fx, fy = self.rk.wf_grid(1, 0.1, nx, ny, (0.05, 0.05), 0.0, wv.voxel_nm[2])
+        counts = np.zeros((nz, gy, gx), np.float32)
+        counts[:, fy:fy + ny, fx:fx + nx] = wv.density
+        self.scene = self.rk.wf_scene(counts, 1, self.KERNEL_CAP_UM, 0.1, nx, ny, (0.05, 0.05), 0.0, wv.voxel_nm[2],
+                                      focus0_um=0.1, gpu_mode=True)
+        self.ref_off, _, _ = self.ref.camera_maps(nx, ny, wv.map_seed, wv.offset_mean, wv.offset_std, 1.0, 0.0, 50.0,
+                                                  0.0)
+        self.ref_off = self.ref_off.reshape(ny, nx)
+        self.focus_planes = np.arange(0, nz, nz // self.frames_per_step_cpu)[:self.frames_per_step_cpu]
+        self.foci = (self.focus_planes + 0.5) * (wv.voxel_nm[2] / 1000.0)
 
     def cpu_cores(self):
-        return os.cpu_count() or 1
+        return self.ref.threads()
 
     def reference_step(self):
-        import scipy.fft as sf
-        from concurrent.futures import ThreadPoolExecutor
         wv = self.wv
         t0 = time.perf_counter()
-        F = sf.rfftn(wv.density.astype(np.float64), self.shape, workers=-1) * self.Kf
-        full = sf.irfftn(F, self.shape, workers=-1)
-        (kz, ky, kx), (nz, ny, nx) = self.kshape, wv.density.shape
-        img = (np.maximum(full[kz // 2: kz // 2 + nz, ky // 2: ky // 2 + ny, kx // 2: kx // 2 + nx], 0.0) +
-               wv.background).astype(np.float32)
-        with ThreadPoolExecutor(self.cpu_cores()) as ex:
-            list(ex.map(lambda f: self.orc.noise_chain(img[f], wv.camera, None, None, None, wv.noise_seed,
-                                                       self.frame0 + f), range(nz)))
+        frames, _ = self.scene.series(self.foci)
+        frames += np.float32(wv.background)
+        for i, f in enumerate(self.focus_planes):
+            self.ref.noise_chain(frames[i], wv.camera, self.ref_off, None, None, wv.noise_seed, self.frame0 + int(f),
+                                 parallel=True)
         return time.perf_counter() - t0
 
 
@@ -542,8 +606,11 @@ class PsfLibraryWorkload:
                   "ComputeZernikePsfPlanes (float64 Bluestein chirp-Z, planes in parallel on its thread pool)")
 
     def __init__(self, rank: int):
+        from insiliscope_b200.shard import library_shard
         from insiliscope_b200.workloads import psf_library
-        self.lib = psf_library(seed=42 + rank)
+        # weak scaling: the whole job's library has 64 N z-planes per set (4,096 N PSFs), rank r its contiguous range
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.lib = library_shard(psf_library(seed=42, n_z=64 * world), rank, world)
 
     def setup(self, device: int):
         import torch
@@ -567,6 +634,10 @@ class PsfLibraryWorkload:
     def device_step(self):
         self.plan.run_dev(self.d_set, self.d_dz, self.d_out, sync=False)
 
+    def timing(self, on):
+        if not on:   # after the timed steps: keep the library they made for the accuracy check
+            self.h_acc = self.d_out.cpu().numpy()
+
     def e2e_step(self):
         L = self.lib
         self.plan.run(L.set_of_psf, L.defocus_nm, out=self.h_out)
@@ -579,24 +650,53 @@ class PsfLibraryWorkload:
         P, M = self.plan.P, self.plan.M
         return 8.0 * (P * M * M + P * P * M) * self.frames_per_step   # 8 real flops per complex MAC
 
-    def dominant(self):
+    def time_plan(self, plan, reps=5):
         import torch
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(self.stream):
+            plan.run_dev(self.d_set, self.d_dz, self.d_out, sync=False)   # warm
+            s.record(self.stream)
+            for _ in range(reps):
+                plan.run_dev(self.d_set, self.d_dz, self.d_out, sync=False)
+            e.record(self.stream)
+        e.synchronize()
+        return s.elapsed_time(e) / reps
+
+    def dominant(self):
         self.plan.check()
-        ms = []
-        for plan in (self.plan, self.plan32):
-            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            with torch.cuda.stream(self.stream):
-                plan.run_dev(self.d_set, self.d_dz, self.d_out, sync=False)   # warm
-                s.record(self.stream)
-                for _ in range(5):
-                    plan.run_dev(self.d_set, self.d_dz, self.d_out, sync=False)
-                e.record(self.stream)
-            e.synchronize()
-            ms.append(s.elapsed_time(e) / 5)
-        self.fp32_ms = ms[1]
-        return "CztTf32x3Kernel", self.flops_per_launch(), ms[0], {"tf32x3_ms": round(ms[0], 4),
-                                                                 "plain_fp32_ms": round(ms[1], 4),
-                                                                 "speedup_vs_plain_fp32": round(ms[1] / ms[0], 3)}
+        ms = self.time_plan(self.plan)
+        return "CztTf32x3Kernel", self.flops_per_launch(), ms, {"tf32x3_ms": round(ms, 4)}
+
+    def plain_form(self, step_ms):
+        """The precision pattern against the plain FP32 form on this GPU: the same library through the SIMT float32
+        chirp-Z (both products in shared memory, FP32 FMA)."""
+        tc, fp32 = self.time_plan(self.plan), self.time_plan(self.plan32)
+        return {"tf32x3_ms": round(tc, 4), "plain_fp32_ms": round(fp32, 4), "speedup_vs_plain": round(fp32 / tc, 3)}
+
+    def accuracy(self):
+        """Every PSF of the library (the device's TF32 x 3 planes) against the float64 oracle: per PSF
+        max |I - I64| / max I64 and ||I - I64|| / ||I64||, worst and median over the 4,096."""
+        from concurrent.futures import ThreadPoolExecutor
+        from oracle.oracle import Oracle
+        L = self.lib
+        got = self.h_acc
+        orc = Oracle()
+        n = len(L.set_of_psf)
+        err, l2 = np.zeros(n), np.zeros(n)
+
+        def one(si):
+            idx = np.nonzero(L.set_of_psf == si)[0]
+            if len(idx) == 0:
+                return
+            want = orc.psf_planes(L.sets[si], L.defocus_nm[idx] * 1e-9, size=L.size, normalize=True)
+            d = got[idx].astype(np.float64) - want
+            err[idx] = np.abs(d).max(axis=(1, 2)) / want.max(axis=(1, 2))
+            l2[idx] = np.sqrt((d ** 2).sum(axis=(1, 2)) / (want ** 2).sum(axis=(1, 2)))
+
+        with ThreadPoolExecutor(os.cpu_count() or 1) as ex:
+            list(ex.map(one, range(len(L.sets))))
+        return {"psfs": n, "max_rel_err_worst": float(err.max()), "max_rel_err_median": float(np.median(err)),
+                "rel_l2_worst": float(l2.max()), "target": 1e-5, "against": "float64 oracle (direct DFT chirp-Z)"}
 
     def alg_bytes_per_launch(self):
         return self.frames_per_step * self.lib.size ** 2 * 4
@@ -705,6 +805,54 @@ class NllGradWorkload:
     def e2e_bytes(self):
         return self.h_params.numel() * 4 + self.h_bg.numel() * 4 + self.zern.nbytes, \
             self.h_gp.numel() * 4 + self.h_gb.numel() * 8 + self.zern.nbytes + 8
+
+    def plain_form(self, step_ms):
+        """The differentiation pattern against the plain FP32 form on this GPU: the same gradient by central
+        differences of the FP32 forward kernel (no adjoint) -- each ROI's x, y, z and N perturbed for all emitters at
+        once (an ROI depends only on its own emitter), every frame's background at once, each Zernike coefficient on
+        its own: 2 x (4 + 1 + 21) = 52 forward passes writing the expected counts, and per-ROI NLLs reduced by torch."""
+        import torch
+        m, k = self.model, self.counts
+        mu = torch.empty_like(k)
+        nll = torch.zeros(1, dtype=torch.float64, device=k.device)
+        fr = self.d_frame.long()
+        F = self.d_bg.shape[0]
+
+        def roi_nll(params, bg, zern):
+            m.run_dev(params, self.d_frame, bg, zern, k, nll, self.d_err, mu=mu, sync=False)
+            return (mu - k * torch.log(mu)).sum(dim=(1, 2))
+
+        def fd():
+            with torch.cuda.stream(self.stream):
+                gp = torch.empty_like(self.d_params)
+                for col, h in enumerate((1e-2, 1e-2, 0.5, None)):
+                    hh = h if h is not None else 1e-3 * self.d_params[:, 3]
+                    pp, pm = self.d_params.clone(), self.d_params.clone()
+                    pp[:, col] += hh
+                    pm[:, col] -= hh
+                    gp[:, col] = (roi_nll(pp, self.d_bg, self.zern) - roi_nll(pm, self.d_bg, self.zern)) / (2 * hh)
+                hb = 1e-3 * self.d_bg
+                dp = roi_nll(self.d_params, self.d_bg + hb, self.zern) - roi_nll(self.d_params, self.d_bg - hb,
+                                                                                self.zern)
+                gb = torch.zeros(F, dtype=torch.float32, device=k.device).index_add_(0, fr, dp) / (2 * hb)
+                gz = []
+                for j in range(len(self.zern)):
+                    zp, zm = self.zern.copy(), self.zern.copy()
+                    zp[j] += 1e-4
+                    zm[j] -= 1e-4
+                    gz.append((roi_nll(self.d_params, self.d_bg, zp).sum() -
+                               roi_nll(self.d_params, self.d_bg, zm).sum()) / 2e-4)
+                return gp, gb, torch.stack(gz)
+
+        fd()   # warm
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(self.stream)
+        fd()
+        e.record(self.stream)
+        e.synchronize()
+        fd_ms = s.elapsed_time(e)
+        return {"adjoint_ms": round(step_ms, 4), "plain_central_differences_ms": round(fd_ms, 4),
+                "forward_passes_plain": 52, "speedup_vs_plain": round(fd_ms / step_ms, 3)}
 
     def alg_bytes_per_launch(self):
         # the counts read once (4 B per ROI pixel), per emitter its parameters in and gradients out (32 B)
@@ -1349,6 +1497,8 @@ WORKLOADS = {"smlm": SmlmWorkload, "widefield": WidefieldWorkload, "psflib": Psf
              "two-colour": TwoColourWorkload, "nll-grad": NllGradWorkload, "schedules": ScheduleWorkload,
              "binned": BinnedWorkload, "tiff": TiffWorkload, "csv": CsvWorkload, "fftplace": FftPlaceWorkload,
              "wfshift": WfShiftWorkload}
+for _key, _cls in WORKLOADS.items():
+    _cls.key = _key
 
 
 # ----------------------------------------------------------------------------------------------------- arms
@@ -1373,62 +1523,82 @@ def repo_libraries():
     return sorted(out)
 
 
+SUBCONFIGS = (("C1", "widefield"), ("C2", "psflib"), ("C3", "two-colour"), ("C4", "nll-grad"))
+
+
+def measure_reference(w, steps, warmup, n_gpus):
+    """The reference's CPU path on the host cores: warm-up steps, then the mean of `steps` timed steps."""
+    try:
+        w.reference_setup(threads=0)
+    except RuntimeError as e:
+        return {"impl": "reference", "unavailable": str(e)}
+    for _ in range(warmup):
+        w.reference_step()
+    times = [w.reference_step() for _ in range(steps)]
+    ms = 1e3 * statistics.mean(times)
+    value = w.frames_per_step_cpu / (ms / 1e3)
+    return {"metric": w.metric, "value": value, "unit": w.metric, "n_gpus": n_gpus, "steps": steps,
+            "warmup": warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": w.dtype, "data": "synthetic", "impl": "reference",
+            "config": common_config(w, n_gpus),
+            "cpu_baseline": {"value": value, "unit": w.metric, "cores": w.cpu_cores(), "kind": w.cpu_kind,
+                             "sample": w.cpu_sample, "units_per_step": w.frames_per_step_cpu},
+            "e2e": {"value": value, "unit": w.metric, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    w = WORKLOADS[args.workload](0)
-    try:
-        w.reference_setup(threads=0)
-    except RuntimeError as e:
-        print(json.dumps({"impl": "reference", "unavailable": str(e)}))
-        return 0
-    for _ in range(args.warmup):
-        w.reference_step()
-    times = [w.reference_step() for _ in range(args.steps)]
-    ms = 1e3 * statistics.mean(times)
-    value = w.frames_per_step_cpu / (ms / 1e3)
-    line = {"metric": w.metric, "value": value, "unit": w.metric, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": w.dtype, "data": "synthetic", "impl": "reference",
-            "config": common_config(w, args.gpus),
-            "cpu_baseline": {"value": value, "unit": w.metric, "cores": w.cpu_cores(), "kind": w.cpu_kind,
-                             "sample": w.cpu_sample, "units_per_step": w.frames_per_step_cpu},
-            "e2e": {"value": value, "unit": w.metric, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "native_libraries": repo_libraries()}
+    if args.workload != "all":
+        line = measure_reference(WORKLOADS[args.workload](0), args.steps, args.warmup, args.gpus)
+    else:
+        line = measure_reference(SmlmWorkload(0), args.steps, args.warmup, args.gpus)
+        line["configs"] = {key: compact(measure_reference(WORKLOADS[name](0), min(args.steps, 5),
+                                                          min(args.warmup, 2), args.gpus))
+                           for key, name in SUBCONFIGS}
+    line["native_libraries"] = repo_libraries()
     print(json.dumps(line))
     return 0
 
 
-def cpu_baseline(w):
-    """The CPU path on this box's host cores, a bounded sample (the workload's own), best of 3 after one warm-up."""
+def cpu_leg(w, repeats=3):
+    """The CPU path on this box's host cores, a bounded sample (the workload's own), best of `repeats` after one
+    warm-up; and, where a workload checks its output against the float64 oracle at full size, that check."""
     try:
         w.reference_setup(threads=0)
     except RuntimeError:
-        return None
+        return None, None
     w.reference_step()
-    best = min(w.reference_step() for _ in range(3))
-    return {"value": w.frames_per_step_cpu / best, "unit": w.metric, "cores": w.cpu_cores(), "kind": w.cpu_kind,
-            "sample": w.cpu_sample + "; best of 3"}
+    best = min(w.reference_step() for _ in range(repeats))
+    base = {"value": w.frames_per_step_cpu / best, "unit": w.metric, "cores": w.cpu_cores(), "kind": w.cpu_kind,
+            "sample": w.cpu_sample + f"; best of {repeats}"}
+    return base, (w.accuracy() if hasattr(w, "accuracy") else None)
 
 
-def run_ours(args):
+COMPACT_KEYS = ("metric", "value", "unit", "ms_per_step", "steps", "warmup", "dtype", "config", "details", "e2e",
+                "roofline", "cpu_baseline", "plain_form", "accuracy", "gpu_launches", "clocks", "unavailable", "impl")
+
+
+def compact(line):
+    return {k: line[k] for k in COMPACT_KEYS if k in line}
+
+
+def measure_ours(w, args, world, rank, local, steps, warmup, cpu=True):
+    """One workload on this rank's GPU: W untimed steps, K steps timed with CUDA events (L2 flushed before each,
+    clocks sampled), the slowest pass's roofline, the end-to-end run through the C ABI with host buffers, the plain
+    form beside it where the workload has one, and (rank 0, one GPU) the CPU baseline. Returns the JSON line."""
     import torch
-    world, rank, local = dist_setup(args.gpus)
-    torch.cuda.set_device(local)
-    from insiliscope_b200.build import build_library
-    build_library()
-    w = WORKLOADS[args.workload](rank)
     if args.form is not None and isinstance(w, SmlmWorkload):
         w.setup(local, form=args.form)
     else:
         w.setup(local)
     eng = w.eng
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")   # 256 MB > L2 (126 MB)
-    start = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    stop = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    start = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    stop = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
     with torch.cuda.stream(w.stream):
-        for i in range(args.warmup):
+        for i in range(warmup):
             flush.fill_(float(i))
             w.device_step()
     eng.synchronize()
@@ -1441,7 +1611,7 @@ def run_ours(args):
         torch.cuda.synchronize()
         barrier(world)
         with torch.cuda.stream(w.stream):
-            for i in range(args.steps):
+            for i in range(steps):
                 flush.fill_(float(i + 1))
                 start[i].record(w.stream)
                 w.device_step()
@@ -1456,14 +1626,15 @@ def run_ours(args):
     dom = w.dominant() if hasattr(w, "dominant") else None
     if hasattr(w, "timing"):
         w.timing(False)
+    plain = w.plain_form(statistics.mean(step_ms)) if hasattr(w, "plain_form") else None
     # end to end through the C ABI with host buffers
     pipelined = hasattr(w, "e2e_run")
     run = w.e2e_run if pipelined else (lambda k: [w.e2e_step() for _ in range(k)])
-    run(max(1, args.warmup))
+    run(max(1, warmup))
     barrier(world)
     t0 = time.perf_counter()
-    run(args.steps)
-    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps, world)
+    run(steps)
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / steps, world)
     h2d, d2h = w.e2e_bytes()
     hbm, bf16, peak_kind = measured_peaks()
     if dom is not None:
@@ -1473,8 +1644,8 @@ def run_ours(args):
     tensor = getattr(w, "roofline_kind", "hbm") == "tensor"
     achieved = kbytes / (kms / 1e3) / (1e12 if tensor else 1e9)
     peak = bf16 if tensor else hbm
-    line = {"metric": w.metric, "value": value, "unit": w.metric, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+    line = {"metric": w.metric, "value": value, "unit": w.metric, "n_gpus": world, "steps": steps,
+            "warmup": warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": w.dtype, "data": "synthetic",
             "config": common_config(w, world),
             "details": {"frames_per_step": w.frames_per_step, "emitters_per_step": w.n_emitters,
@@ -1489,14 +1660,13 @@ def run_ours(args):
                               "host wall clock per step (blocking C-ABI calls), max over ranks"},
             "roofline": {"bound": "tensor" if tensor else "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s" if tensor else "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": NCU_TRAFFIC.get((args.workload, kname), (None,))[0], ("alg_flops_per_launch" if tensor else "alg_bytes_per_launch"): kbytes,
-                         "launch_ms": kms},
+                         "traffic": NCU_TRAFFIC.get((w.key, kname), (None,))[0],
+                         ("alg_flops_per_launch" if tensor else "alg_bytes_per_launch"): kbytes, "launch_ms": kms},
             "gpu_launches": launches, "clocks": clk.summary()}
     if breakdown and tensor:
         line["roofline"]["peak_note"] = ("measured dense bf16 cuBLAS peak; the kernel issues TF32 MMAs (nominal TF32 "
                                          "dense rate is half of bf16) and 3 of them per product (hi*hi, hi*lo, lo*hi)")
         line["roofline"]["issued_tflops"] = 3 * achieved
-        line["plain_fp32"] = breakdown
     elif breakdown:
         line["roofline"]["pass_ms"] = breakdown.get("pass_ms", breakdown)
         if "design_bytes" in breakdown:
@@ -1506,14 +1676,49 @@ def run_ours(args):
         line["roofline"]["step_achieved"] = step_bytes / (statistics.mean(step_ms) / 1e3) / 1e9
         line["roofline"]["step_frac"] = line["roofline"]["step_achieved"] / peak
     tr = line["roofline"]["traffic"]
-    if tr:
-        line["roofline"]["traffic_over_alg"] = tr / kbytes if not tensor else None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(w)
-    if rank == 0:
-        print(json.dumps(line))
+    if tr and not tensor:
+        line["roofline"]["traffic_over_alg"] = tr / kbytes
+    if plain is not None:
+        line["plain_form"] = plain
+    if cpu and rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"], acc = cpu_leg(w, 3 if steps >= 10 else 2)
+        if acc is not None:
+            line["accuracy"] = acc
     torch.cuda.synchronize()
     eng.close()
+    return line
+
+
+def launch_ranks(args):
+    """--gpus N without a launcher: run this script under torch.distributed.run with N local ranks (one per GPU,
+    rendezvous on 127.0.0.1) and pass its exit code through."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__), *sys.argv[1:]]
+    return subprocess.call(cmd)
+
+
+def run_ours(args):
+    import torch
+    world, rank, local = dist_setup(args.gpus)
+    if world != args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE {world}")
+    torch.cuda.set_device(local)
+    from insiliscope_b200.build import build_library
+    build_library()
+    if args.workload != "all":
+        line = measure_ours(WORKLOADS[args.workload](rank), args, world, rank, local, args.steps, args.warmup)
+    else:
+        line = measure_ours(SmlmWorkload(rank), args, world, rank, local, args.steps, args.warmup)
+        line["configs"] = {key: compact(measure_ours(WORKLOADS[name](rank), args, world, rank, local,
+                                                     min(args.steps, 10), args.warmup))
+                           for key, name in SUBCONFIGS}
+    line["native_libraries"] = repo_libraries()
+    if rank == 0:
+        print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -1526,13 +1731,17 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="smlm")
+    ap.add_argument("--workload", choices=["all"] + sorted(WORKLOADS), default="all",
+                    help="all (default): the SMLM movie as the headline with the widefield, PSF-library, two-colour "
+                         "and gradient configurations as sub-records; or one workload alone")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--form", type=int, default=None,
                     help="SMLM workloads: render form 0..17 instead of the autotuner's choice (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return launch_ranks(args)
     return run_reference(args) if args.impl == "reference" else run_ours(args)
 
 

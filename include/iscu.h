@@ -525,10 +525,26 @@ typedef struct iscu_wf_plan iscu_wf_plan;
 int iscu_wf_plan_create(iscu_ctx* ctx, uint32_t nx, uint32_t ny, uint32_t nz, const float* psf, uint32_t kx,
                         uint32_t ky, uint32_t kz, iscu_wf_plan** out);
 void iscu_wf_plan_destroy(iscu_wf_plan* plan);
-/* The padded FFT grid of a plan (each axis a power of two >= the linear-convolution length). */
+/* The reference's widefield scene as a plan (WidefieldScene::UpdateFromGrid + FocusSeries + WidefieldImages::Render,
+ * WidefieldRender.cpp:1180, :2845, :547; the kernel KernelWidefieldPsf, :263-330): the dye grid is nx x ny x nz cells
+ * at pixel_um / upscale (dye plane i at its centre, planes plane_nm thick) and the series images it at every dye
+ * plane's centre. The PSF comes from kernel slot `slot` (upscale must divide its oversampling): each cell the float64
+ * sum of its (os / upscale)^2 oversampled samples, the radius capped at kernel_cap_um; dye plane k seen from focus f
+ * through the slot's plane at t = (k - f) plane_nm / z_step + (nz_slot - 1) / 2 -- clamped to the stack, between two
+ * planes the linear blend (PlanFocus, :1460-1522). Frames are the camera window: cells [fov_x0, fov_x0 + upscale
+ * fov_w) x [fov_y0, fov_y0 + upscale fov_h) of the grid, each pixel the float64 sum of its upscale x upscale cells
+ * clamped at 0, + background, then the noise chain: fov_w x fov_h x nz frames from every render call
+ * (iscu_wf_render*, iscu_wf_convolve_dev). */
+int iscu_wf_plan_from_kernel(iscu_ctx* ctx, int32_t slot, int32_t upscale, double pixel_um, double kernel_cap_um,
+                             double plane_nm, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t fov_x0, uint32_t fov_y0,
+                             uint32_t fov_w, uint32_t fov_h, iscu_wf_plan** out);
+/* A plan's frame size (the grid's nx x ny, or a from-kernel plan's camera window) and its kernel radius in cells. */
+int iscu_wf_plan_frame(iscu_wf_plan* plan, uint32_t* width, uint32_t* height, int32_t* kernel_radius);
+/* The padded FFT grid of a plan (each axis a power of two holding the kernel and the volume's "same" window,
+ * n + k/2 points, of the circular convolution). */
 int iscu_wf_plan_grid(iscu_wf_plan* plan, uint32_t* gx, uint32_t* gy, uint32_t* gz);
-/* density_dev (nx*ny*nz) -> image_dev (nx*ny*nz): the convolution, max(0, .) per voxel (WidefieldImages::Render's
- * clamp, WidefieldRender.cpp:547). */
+/* density_dev (nx*ny*nz) -> image_dev (the frames: nx*ny*nz, or a from-kernel plan's window): the convolution,
+ * max(0, .) per voxel (WidefieldImages::Render's clamp, WidefieldRender.cpp:547). */
 int iscu_wf_convolve_dev(iscu_wf_plan* plan, const float* density_dev, float* image_dev);
 /* Convolution, max(0, .) + background, then the noise chain per image plane (frame f = frame0 + plane; cam NULL: no
  * noise), host buffers: the widefield movie of one focus series. adu: nx*ny*nz uint16 (needed with cam). image

@@ -56,6 +56,18 @@ __global__ void CellKernelsKernel(const float* __restrict__ planes, int n, int n
    out[i] = static_cast<float>(acc);
 }
 
+} // namespace
+
+int LaunchCellKernels(iscu_ctx* ctx, const float* planes, int n, int nz, int r, int s0, int R, float* out)
+{
+   const int D = 2 * R + 1, total = nz * D * D;
+   CellKernelsKernel<<<(total + 255) / 256, 256, 0, ctx->stream>>>(planes, n, nz, r, s0, R, out);
+   ISCU_CK_LAUNCH(ctx, "CellKernelsKernel");
+   return ISCU_OK;
+}
+
+namespace {
+
 struct Staged
 {
    int cx, cy;   // the emitter's cell (unpadded grid)

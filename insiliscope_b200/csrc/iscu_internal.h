@@ -298,6 +298,9 @@ int LaunchNormalizePlanes(iscu_ctx* ctx, float* planes, int planeElems, int nPla
 int BuildPsfLibrary(iscu_ctx* ctx, const iscu_psf_request* sets, uint32_t nSets, const uint32_t* setOfPsf,
                     const double* defocusM, uint32_t nPsf, int32_t size, int32_t normalize, int32_t method,
                     float* out);
+// KernelWidefieldPsf::Kernel's cells (binned.cu): plane p's cell (dx, dy), |dx|, |dy| <= R, is the float64 sum of the
+// n x n oversampled plane over [s0 + dy r, +r) x [s0 + dx r, +r) clipped to it, as float; out nz x (2R+1)^2.
+int LaunchCellKernels(iscu_ctx* ctx, const float* planes, int n, int nz, int r, int s0, int R, float* out);
 // The halo cut of a slot's stack from its device block sums (halo.cu); threshold <= 0: none.
 int BuildHalo(iscu_ctx* ctx, KernelSlot& k, double threshold);
 // Copies a cut slot's spans (nz (2 camRad + 1) each) and per-plane radius2 (nz) to host memory.

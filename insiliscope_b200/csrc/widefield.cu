@@ -117,6 +117,14 @@ struct iscu_wf_plan
    int logH = 0, logGY = 0, logGZ = 0;
    iscu::LinePlan px, py, pz;
    iscu::DevBuf A, B, Kh, tw, twg, image, adu;
+   // The camera (iscu_wf_plan_from_kernel): frames are the FOV cells [fovX0, fovX0 + up fovW) x [fovY0, fovY0 + up
+   // fovH) of the grid, up x up cells per pixel; without one (camera false) a frame is the whole nx x ny grid.
+   bool camera = false;
+   uint32_t fovX0 = 0, fovY0 = 0, fovW = 0, fovH = 0, up = 1;
+   iscu::DevBuf cells;   // camera plans: the clamped cell images before binning
+   uint32_t FrameW() const { return camera ? fovW : nx; }
+   uint32_t FrameH() const { return camera ? fovH : ny; }
+   size_t FrameElems() const { return static_cast<size_t>(FrameW()) * FrameH() * nz; }
    // Pipelined renders (iscu_wf_render_async): per I/O slot the volume, the frames and the three stage events.
    struct Io
    {
@@ -919,6 +927,46 @@ __global__ void __launch_bounds__(256) WfNoiseKernel(const float* __restrict__ p
    adu[o] = NoisePixel(photons[o], i, cam, st, u);
 }
 
+// A camera plan's photon frames (WidefieldImages::Render, WidefieldRender.cpp:547-586): pixel (X, Y) of plane z is the
+// float64 sum, row by row, of its up x up cells (already clamped at 0) of the FOV window, as float, plus the
+// background. grid (ceil(fovW fovH / 256), nz).
+__global__ void __launch_bounds__(256) WfBinKernel(const float* __restrict__ cells, uint32_t nx, uint32_t ny,
+                                                   uint32_t fovX0, uint32_t fovY0, uint32_t fovW, uint32_t fovH,
+                                                   uint32_t up, float background, float* __restrict__ photons)
+{
+   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= fovW * fovH)
+      return;
+   const uint32_t X = i % fovW, Y = i / fovW;
+   const float* plane = cells + static_cast<size_t>(blockIdx.y) * nx * ny;
+   double acc = 0.0;
+   for (uint32_t sy = 0; sy < up; ++sy)
+   {
+      const float* row = plane + static_cast<size_t>(fovY0 + Y * up + sy) * nx + fovX0 + X * up;
+      for (uint32_t sx = 0; sx < up; ++sx)
+         acc += row[sx];
+   }
+   photons[static_cast<size_t>(blockIdx.y) * fovW * fovH + i] = static_cast<float>(acc) + background;
+}
+
+// The kernel volume of a plan made from a kernel slot: plane j = w0[j] K[p0[j]] + w1[j] K[p1[j]] of the D x D cell
+// kernels K (the second term only where w1 != 0), the blend WidefieldScene applies to kernel spectra
+// (ChannelImageStep, WidefieldRender.cpp:1790-1801) made here on the cells.
+__global__ void WfKernelVolumeKernel(const float* __restrict__ K, int D2, const int2* __restrict__ planes,
+                                     const float2* __restrict__ weights, int kz, float* __restrict__ out)
+{
+   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= kz * D2)
+      return;
+   const int j = i / D2, c = i - j * D2;
+   const int2 p = planes[j];
+   const float2 w = weights[j];
+   float v = w.x * K[static_cast<size_t>(p.x) * D2 + c];
+   if (w.y != 0.0f)
+      v = v + w.y * K[static_cast<size_t>(p.y) * D2 + c];
+   out[i] = v;
+}
+
 // ---------------------------------------------------------------------------- drifting sample (RenderShiftedImages)
 // The frame's spectrum S = sum_c coef[c] spec[c] (float complex, channels in order, zero coefficients skipped, as
 // RenderShiftedImages adds them, WidefieldRender.cpp:2905-2935), times ApplyShiftRamp's phase (DriftShift.cpp:23-48:
@@ -1364,27 +1412,42 @@ static int FinishX(iscu_wf_plan* p, double background, const iscu_camera* cam, u
    iscu_ctx* ctx = p->ctx;
    const Dims d = MakeDims(p, p->nx, p->ny, p->nz);
    StaticView st;
-   if (ctx->haveStatic && ctx->width == p->nx && ctx->height == p->ny)
+   const uint32_t fw = p->FrameW(), fh = p->FrameH();
+   if (ctx->haveStatic && ctx->width == fw && ctx->height == fh)
       st = ctx->Static();
-   st.width = p->nx;
-   st.height = p->ny;
+   st.width = fw;
+   st.height = fh;
    const float scale = static_cast<float>(1.0 / (static_cast<double>(p->GX) * p->GY * p->GZ));
    if (!image)
    {
-      ISCU_CK(p->image.Reserve(static_cast<size_t>(p->nx) * p->ny * p->nz * sizeof(float)));
+      ISCU_CK(p->image.Reserve(p->FrameElems() * sizeof(float)));
       image = p->image.as<float>();
+   }
+   // a camera plan clamps the grid's cells first (no background) and bins its FOV window after
+   float* xout = image;
+   if (p->camera)
+   {
+      ISCU_CK(p->cells.Reserve(static_cast<size_t>(p->nx) * p->ny * p->nz * sizeof(float)));
+      xout = p->cells.as<float>();
    }
    const int BY = XLines(d.H);
    ISCU_WF_X_CODELETS(d.logH, (XInverseKernel<K><<<dim3((d.nyv + BY - 1) / BY, d.nzv), kThreads, XSmem(d.H, BY),
                                                    ctx->stream>>>(
                                   p->A.as<float2>(), d, BY, Log2(BY), static_cast<int>(p->kx / 2), scale,
-                                  static_cast<float>(background), p->tw.as<float2>(), p->twg.as<float2>(), image)));
+                                  p->camera ? 0.0f : static_cast<float>(background), p->tw.as<float2>(),
+                                  p->twg.as<float2>(), xout)));
    ISCU_CK_LAUNCH(ctx, "XInverseKernel");
+   if (p->camera)
+   {
+      WfBinKernel<<<dim3((fw * fh + 255) / 256, p->nz), 256, 0, ctx->stream>>>(
+         xout, p->nx, p->ny, p->fovX0, p->fovY0, fw, fh, p->up, static_cast<float>(background), image);
+      ISCU_CK_LAUNCH(ctx, "WfBinKernel");
+   }
    p->Mark(5);
    if (cam)
    {
       const CameraView cv = MakeCameraView(*cam);
-      const uint32_t npix = p->nx * p->ny;
+      const uint32_t npix = fw * fh;
       WfNoiseKernel<<<dim3((npix + 255) / 256, p->nz), 256, 0, ctx->stream>>>(image, npix, st, cv, seed, frame0, adu);
       ISCU_CK_LAUNCH(ctx, "WfNoiseKernel");
    }
@@ -1394,20 +1457,21 @@ static int FinishX(iscu_wf_plan* p, double background, const iscu_camera* cam, u
 
 } // namespace iscu
 
-using namespace iscu;
+namespace iscu {
+namespace {
 
-extern "C" {
-
-int iscu_wf_plan_create(iscu_ctx* ctx, uint32_t nx, uint32_t ny, uint32_t nz, const float* psf, uint32_t kx,
-                        uint32_t ky, uint32_t kz, iscu_wf_plan** out)
+// The FFT length of one axis: a power of two that holds the kernel (k) and the volume's "same" window (n points from
+// k/2 on) of the circular convolution with nothing wrapped into it -- n + k/2 points (the output point i + k/2 reads
+// kernel taps i + k/2 - j for input points j < n: none of them wraps into [0, k) once the length passes n + k/2 - 1).
+uint32_t AxisLength(uint32_t n, uint32_t k, uint32_t least)
 {
-   if (!ctx || !psf || !out)
-      return Fail(ISCU_ERR_ARG, "null argument");
-   *out = nullptr;
-   if (nx < 2 || ny < 1 || nz < 1 || kx < 1 || ky < 1 || kz < 1 || nx % 2 != 0)
-      return Fail(ISCU_ERR_ARG, "widefield plan: nx even >= 2, all other sizes >= 1");
-   std::lock_guard<std::recursive_mutex> lock(ctx->mu);
-   ClearError();
+   return Pow2AtLeast(std::max({n + k / 2, k, least}));
+}
+
+// A plan's geometry, tables and PSF spectrum; psf is a device pointer when psfOnDevice (kx*ky*kz floats).
+int MakePlan(iscu_ctx* ctx, uint32_t nx, uint32_t ny, uint32_t nz, const float* psf, bool psfOnDevice, uint32_t kx,
+             uint32_t ky, uint32_t kz, std::unique_ptr<iscu_wf_plan>& out)
+{
    std::unique_ptr<iscu_wf_plan> p(new iscu_wf_plan());
    p->ctx = ctx;
    p->nx = nx;
@@ -1416,9 +1480,9 @@ int iscu_wf_plan_create(iscu_ctx* ctx, uint32_t nx, uint32_t ny, uint32_t nz, co
    p->kx = kx;
    p->ky = ky;
    p->kz = kz;
-   p->GX = Pow2AtLeast(std::max(nx + kx - 1, 8u));
-   p->GY = Pow2AtLeast(std::max(ny + ky - 1, 4u));
-   p->GZ = Pow2AtLeast(std::max(nz + kz - 1, 4u));
+   p->GX = AxisLength(nx, kx, 8u);
+   p->GY = AxisLength(ny, ky, 4u);
+   p->GZ = AxisLength(nz, kz, 4u);
    if (p->GX > 4096 || p->GY > 8192 || p->GZ > 8192)
       return Fail(ISCU_ERR_LIMIT, "widefield plan: padded grid beyond 4096 x 8192 x 8192");
    if (kx > p->GX || ky > p->GY)
@@ -1458,10 +1522,14 @@ int iscu_wf_plan_create(iscu_ctx* ctx, uint32_t nx, uint32_t ny, uint32_t nz, co
    // The PSF's spectrum: its own x and y passes (kx x ky x kz valid), then the forward z transform of all GZ planes.
    DevBuf dPsf;
    const size_t psfBytes = static_cast<size_t>(kx) * ky * kz * sizeof(float);
-   ISCU_CK(dPsf.Reserve(psfBytes));
-   ISCU_CK(cudaMemcpyAsync(dPsf.p, psf, psfBytes, cudaMemcpyHostToDevice, ctx->stream));
+   if (!psfOnDevice)
+   {
+      ISCU_CK(dPsf.Reserve(psfBytes));
+      ISCU_CK(cudaMemcpyAsync(dPsf.p, psf, psfBytes, cudaMemcpyHostToDevice, ctx->stream));
+      psf = dPsf.as<float>();
+   }
    const Dims dk = MakeDims(p.get(), kx, ky, kz);
-   rc = ForwardXY(p.get(), dPsf.as<float>(), dk, p->A.as<float2>(), p->B.as<float2>());
+   rc = ForwardXY(p.get(), psf, dk, p->A.as<float2>(), p->B.as<float2>());
    if (rc != ISCU_OK)
       return rc;
    ISCU_WF_Z_CODELETS(dk.logGZ, ZLaunch zl; rc = ZPlan<false, K>(ctx, dk, zl); if (rc != ISCU_OK) return rc;
@@ -1470,7 +1538,139 @@ int iscu_wf_plan_create(iscu_ctx* ctx, uint32_t nx, uint32_t ny, uint32_t nz, co
                          p->twg.as<float2>(), p->Kh.as<float2>())));
    ISCU_CK_LAUNCH(ctx, "ZKernel<spectrum>");
    ISCU_CK(cudaStreamSynchronize(ctx->stream));
+   out = std::move(p);
+   return ISCU_OK;
+}
+
+// KernelWidefieldPsf (WidefieldRender.cpp:263-330) of a kernel slot at `up` grid cells per camera pixel: r = os / up
+// oversampled samples per cell, cell 0 from sample s0 = floor(kc - r / 2 + 1), the natural radius (the cells whose
+// block meets the plane) capped at ceil(capUm / pitch - 1e-9) cells (WidefieldScene::SetupFft, :1315-1322).
+void CellGeometry(const KernelSlot& k, int up, double pixelUm, double capUm, int& r, int& s0, int& R)
+{
+   const int n = k.size;
+   r = std::max(1, k.os / up);
+   const double kc = (n - 1) / 2.0;
+   s0 = static_cast<int>(std::floor(kc - r / 2.0 + 1.0));
+   const int dMin = static_cast<int>(std::ceil((-s0 - r + 1) / static_cast<double>(r)));
+   const int dMax = static_cast<int>(std::floor((n - 1 - s0) / static_cast<double>(r)));
+   const int natural = std::max(1, std::max(-dMin, dMax));
+   const double pitch = pixelUm / up;
+   const int cap = std::max(1, static_cast<int>(std::ceil(capUm / pitch - 1e-9)));
+   R = std::max(1, std::min(cap, natural));
+}
+
+} // namespace
+} // namespace iscu
+
+using namespace iscu;
+
+extern "C" {
+
+int iscu_wf_plan_create(iscu_ctx* ctx, uint32_t nx, uint32_t ny, uint32_t nz, const float* psf, uint32_t kx,
+                        uint32_t ky, uint32_t kz, iscu_wf_plan** out)
+{
+   if (!ctx || !psf || !out)
+      return Fail(ISCU_ERR_ARG, "null argument");
+   *out = nullptr;
+   if (nx < 2 || ny < 1 || nz < 1 || kx < 1 || ky < 1 || kz < 1 || nx % 2 != 0)
+      return Fail(ISCU_ERR_ARG, "widefield plan: nx even >= 2, all other sizes >= 1");
+   std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+   ClearError();
+   std::unique_ptr<iscu_wf_plan> p;
+   const int rc = MakePlan(ctx, nx, ny, nz, psf, false, kx, ky, kz, p);
+   if (rc != ISCU_OK)
+      return rc;
    *out = p.release();
+   return ISCU_OK;
+}
+
+int iscu_wf_plan_from_kernel(iscu_ctx* ctx, int32_t slot, int32_t upscale, double pixel_um, double kernel_cap_um,
+                             double plane_nm, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t fov_x0, uint32_t fov_y0,
+                             uint32_t fov_w, uint32_t fov_h, iscu_wf_plan** out)
+{
+   if (!ctx || !out)
+      return Fail(ISCU_ERR_ARG, "null argument");
+   *out = nullptr;
+   if (slot < 0 || slot >= ISCU_MAX_KERNELS)
+      return Fail(ISCU_ERR_ARG, "kernel slot out of range (0..3)");
+   if (nx < 2 || ny < 1 || nz < 1 || nx % 2 != 0)
+      return Fail(ISCU_ERR_ARG, "widefield plan: nx even >= 2, ny and nz >= 1");
+   if (!(pixel_um > 0.0) || !(kernel_cap_um > 0.0) || !(plane_nm > 0.0))
+      return Fail(ISCU_ERR_ARG, "widefield plan: pixel size, kernel cap and plane thickness must be > 0");
+   const uint64_t up = upscale < 1 ? 1u : static_cast<uint64_t>(upscale);
+   if (fov_w == 0 || fov_h == 0 || fov_x0 + up * fov_w > nx || fov_y0 + up * fov_h > ny)
+      return Fail(ISCU_ERR_ARG, "widefield plan: the camera window (fov_x0 + upscale fov_w, fov_y0 + upscale fov_h) "
+                                "must lie inside the nx x ny grid");
+   std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+   ClearError();
+   const KernelSlot& k = ctx->kernels[slot];
+   if (!k.valid)
+      return Fail(ISCU_ERR_STATE, "no kernel stack in slot " + std::to_string(slot));
+   if (k.os % static_cast<int>(up) != 0)
+      return Fail(ISCU_ERR_ARG, "widefield plan: upscale must divide the kernel's oversampling (" +
+                                    std::to_string(k.os) + ")");
+   int r = 1, s0 = 0, R = 1;
+   CellGeometry(k, static_cast<int>(up), pixel_um, kernel_cap_um, r, s0, R);
+   const int D = 2 * R + 1, D2 = D * D, nzk = k.nz;
+   const uint32_t kz = 2 * nz - 1;
+   // The kernel plane of each dye-plane offset d = nz - 1 - j (a dye plane d planes above the focus): PlanFocus
+   // (WidefieldRender.cpp:1460-1522) with KernelWidefieldPsf::PlaneCoord (:282-287): t = defocus 1000 / zStep +
+   // (nz - 1) / 2 clamped to the stack, p0 = floor(t), weights 1 - frac and frac as floats (the last plane: frac 0).
+   std::vector<int2> planes(kz);
+   std::vector<float2> weights(kz);
+   for (uint32_t j = 0; j < kz; ++j)
+   {
+      const double defocusUm = (static_cast<double>(nz) - 1.0 - j) * (plane_nm / 1000.0);
+      double t = (nzk <= 1 || !(k.zStepNm > 0.0)) ? 0.0 : defocusUm * 1000.0 / k.zStepNm + (nzk - 1) / 2.0;
+      t = std::min<double>(nzk - 1, std::max(0.0, t));
+      int p0 = static_cast<int>(std::floor(t));
+      double frac = t - p0;
+      if (p0 >= nzk - 1)
+      {
+         p0 = nzk - 1;
+         frac = 0.0;
+      }
+      planes[j] = make_int2(p0, frac > 0.0 ? p0 + 1 : p0);
+      weights[j] = make_float2(static_cast<float>(1.0 - frac), static_cast<float>(frac));
+   }
+   DevBuf dCells, dVol, dPlanes, dWeights;
+   ISCU_CK(dCells.Reserve(static_cast<size_t>(nzk) * D2 * sizeof(float)));
+   ISCU_CK(dVol.Reserve(static_cast<size_t>(kz) * D2 * sizeof(float)));
+   ISCU_CK(dPlanes.Reserve(kz * sizeof(int2)));
+   ISCU_CK(dWeights.Reserve(kz * sizeof(float2)));
+   ISCU_CK(cudaMemcpyAsync(dPlanes.p, planes.data(), kz * sizeof(int2), cudaMemcpyHostToDevice, ctx->stream));
+   ISCU_CK(cudaMemcpyAsync(dWeights.p, weights.data(), kz * sizeof(float2), cudaMemcpyHostToDevice, ctx->stream));
+   int rc = LaunchCellKernels(ctx, k.planes.as<float>(), k.size, nzk, r, s0, R, dCells.as<float>());
+   if (rc != ISCU_OK)
+      return rc;
+   const size_t total = static_cast<size_t>(kz) * D2;
+   WfKernelVolumeKernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, ctx->stream>>>(
+      dCells.as<float>(), D2, dPlanes.as<int2>(), dWeights.as<float2>(), static_cast<int>(kz), dVol.as<float>());
+   ISCU_CK_LAUNCH(ctx, "WfKernelVolumeKernel");
+   std::unique_ptr<iscu_wf_plan> p;
+   rc = MakePlan(ctx, nx, ny, nz, dVol.as<float>(), true, D, D, kz, p);
+   if (rc != ISCU_OK)
+      return rc;
+   p->camera = true;
+   p->fovX0 = fov_x0;
+   p->fovY0 = fov_y0;
+   p->fovW = fov_w;
+   p->fovH = fov_h;
+   p->up = static_cast<uint32_t>(up);
+   *out = p.release();
+   return ISCU_OK;
+}
+
+int iscu_wf_plan_frame(iscu_wf_plan* plan, uint32_t* width, uint32_t* height, int32_t* kernel_radius)
+{
+   if (!plan)
+      return Fail(ISCU_ERR_ARG, "null plan");
+   if (width)
+      *width = plan->FrameW();
+   if (height)
+      *height = plan->FrameH();
+   if (kernel_radius)
+      *kernel_radius = static_cast<int32_t>(plan->kx / 2);
    return ISCU_OK;
 }
 
@@ -1581,12 +1781,12 @@ int iscu_wf_render_async(iscu_wf_plan* plan, int32_t io_slot, const float* densi
    for (cudaEvent_t* e : {&io.uploaded, &io.rendered, &io.downloaded})
       if (!*e)
          ISCU_CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
-   const size_t n = static_cast<size_t>(plan->nx) * plan->ny * plan->nz;
+   const size_t n = static_cast<size_t>(plan->nx) * plan->ny * plan->nz, nf = plan->FrameElems();
    ISCU_CK(io.density.Reserve(n * sizeof(float)));
    if (image)
-      ISCU_CK(io.image.Reserve(n * sizeof(float)));
+      ISCU_CK(io.image.Reserve(nf * sizeof(float)));
    if (adu)
-      ISCU_CK(io.adu.Reserve(n * sizeof(uint16_t)));
+      ISCU_CK(io.adu.Reserve(nf * sizeof(uint16_t)));
    // the slot's buffers are free (its last render was waited for), so the upload waits on nothing
    ISCU_CK(cudaMemcpyAsync(io.density.p, density, n * sizeof(float), cudaMemcpyHostToDevice, ctx->upload));
    ISCU_CK(cudaEventRecord(io.uploaded, ctx->upload));
@@ -1601,9 +1801,9 @@ int iscu_wf_render_async(iscu_wf_plan* plan, int32_t io_slot, const float* densi
    ISCU_CK(cudaEventRecord(io.rendered, ctx->stream));
    ISCU_CK(cudaStreamWaitEvent(ctx->download, io.rendered, 0));
    if (image)
-      ISCU_CK(cudaMemcpyAsync(image, io.image.p, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->download));
+      ISCU_CK(cudaMemcpyAsync(image, io.image.p, nf * sizeof(float), cudaMemcpyDeviceToHost, ctx->download));
    if (adu)
-      ISCU_CK(cudaMemcpyAsync(adu, io.adu.p, n * sizeof(uint16_t), cudaMemcpyDeviceToHost, ctx->download));
+      ISCU_CK(cudaMemcpyAsync(adu, io.adu.p, nf * sizeof(uint16_t), cudaMemcpyDeviceToHost, ctx->download));
    ISCU_CK(cudaEventRecord(io.downloaded, ctx->download));
    io.busy = true;
    return ISCU_OK;
@@ -1633,12 +1833,12 @@ int iscu_wf_render(iscu_wf_plan* plan, const float* density, double background, 
    iscu_ctx* ctx = plan->ctx;
    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
    ClearError();
-   const size_t n = static_cast<size_t>(plan->nx) * plan->ny * plan->nz;
+   const size_t n = static_cast<size_t>(plan->nx) * plan->ny * plan->nz, nf = plan->FrameElems();
    ISCU_CK(ctx->dScratch.Reserve(n * sizeof(float)));
    if (image)
-      ISCU_CK(plan->image.Reserve(n * sizeof(float)));
+      ISCU_CK(plan->image.Reserve(nf * sizeof(float)));
    if (adu)
-      ISCU_CK(plan->adu.Reserve(n * sizeof(uint16_t)));
+      ISCU_CK(plan->adu.Reserve(nf * sizeof(uint16_t)));
    ISCU_CK(cudaMemcpyAsync(ctx->dScratch.p, density, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
    int rc = ConvolveToA(plan, ctx->dScratch.as<float>());
    if (rc != ISCU_OK)
@@ -1648,9 +1848,9 @@ int iscu_wf_render(iscu_wf_plan* plan, const float* density, double background, 
    if (rc != ISCU_OK)
       return rc;
    if (image)
-      ISCU_CK(cudaMemcpyAsync(image, plan->image.p, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+      ISCU_CK(cudaMemcpyAsync(image, plan->image.p, nf * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
    if (adu)
-      ISCU_CK(cudaMemcpyAsync(adu, plan->adu.p, n * sizeof(uint16_t), cudaMemcpyDeviceToHost, ctx->stream));
+      ISCU_CK(cudaMemcpyAsync(adu, plan->adu.p, nf * sizeof(uint16_t), cudaMemcpyDeviceToHost, ctx->stream));
    ISCU_CK(cudaStreamSynchronize(ctx->stream));
    return ISCU_OK;
 }

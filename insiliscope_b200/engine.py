@@ -712,18 +712,37 @@ class PsfPlan:
 class WidefieldPlan:
     """iscu_wf_plan: the focus series of a dye volume (nz, ny, nx) under a 3D PSF (kz, ky, kx), PSF spectrum resident."""
 
-    def __init__(self, engine: Engine, shape, psf):
-        psf = np.ascontiguousarray(psf, dtype=np.float32)
+    def __init__(self, engine: Engine, shape, psf, _handle=None):
         self.engine = engine
         self.lib = engine.lib
         self.shape = tuple(int(v) for v in shape)   # (nz, ny, nx)
         nz, ny, nx = self.shape
-        kz, ky, kx = psf.shape
-        h = C.c_void_p()
-        check(self.lib.iscu_wf_plan_create(engine.h, nx, ny, nz, _ptr(psf), kx, ky, kz, C.byref(h)))
-        self.h = h
+        if _handle is None:
+            psf = np.ascontiguousarray(psf, dtype=np.float32)
+            kz, ky, kx = psf.shape
+            h = C.c_void_p()
+            check(self.lib.iscu_wf_plan_create(engine.h, nx, ny, nz, _ptr(psf), kx, ky, kz, C.byref(h)))
+            _handle = h
+        self.h = _handle
+        w, hh, r = C.c_uint32(), C.c_uint32(), C.c_int32()
+        check(self.lib.iscu_wf_plan_frame(self.h, C.byref(w), C.byref(hh), C.byref(r)))
+        self.frame_shape = (nz, hh.value, w.value)   # the frames every render writes
+        self.kernel_radius = r.value
         self._pending_io = {}   # I/O slot -> the host arrays of its enqueued render
         engine._plans.add(self)
+
+    @classmethod
+    def from_kernel(cls, engine: Engine, slot, upscale, pixel_um, kernel_cap_um, plane_nm, shape, fov):
+        """The reference's widefield scene over kernel slot `slot` (iscu_wf_plan_from_kernel): a dye grid of shape
+        (nz, ny, nx) cells at pixel_um / upscale, planes plane_nm thick, imaged at every plane's centre; frames are the
+        camera window fov = (x0, y0, width, height) (cells x0, y0; width x height camera pixels of upscale^2 cells)."""
+        nz, ny, nx = (int(v) for v in shape)
+        x0, y0, w, h = (int(v) for v in fov)
+        hd = C.c_void_p()
+        check(engine.lib.iscu_wf_plan_from_kernel(engine.h, int(slot), int(upscale), float(pixel_um),
+                                                  float(kernel_cap_um), float(plane_nm), nx, ny, nz, x0, y0, w, h,
+                                                  C.byref(hd)))
+        return cls(engine, (nz, ny, nx), None, _handle=hd)
 
     def close(self):
         if self.h:
@@ -755,7 +774,7 @@ class WidefieldPlan:
     def convolve_dev(self, density_dev, image_dev=None, sync=True):
         import torch
         if image_dev is None:
-            image_dev = torch.empty(self.shape, dtype=torch.float32, device=density_dev.device)
+            image_dev = torch.empty(self.frame_shape, dtype=torch.float32, device=density_dev.device)
         self.engine._before(sync)
         check(self.lib.iscu_wf_convolve_dev(self.h, _ptr(density_dev), _ptr(image_dev)))
         self.engine._after(sync)
@@ -775,9 +794,9 @@ class WidefieldPlan:
         """Host path: density (nz, ny, nx) float32 -> (image | None, adu | None)."""
         density = np.ascontiguousarray(density, dtype=np.float32)
         if want_image and image is None:
-            image = np.empty(self.shape, np.float32)
+            image = np.empty(self.frame_shape, np.float32)
         if camera is not None and adu is None:
-            adu = np.empty(self.shape, np.uint16)
+            adu = np.empty(self.frame_shape, np.uint16)
         cam = camera.c() if camera is not None else None
         check(self.lib.iscu_wf_render(self.h, _ptr(density), float(background),
                                       C.byref(cam) if cam is not None else None, seed, frame0,
@@ -793,8 +812,8 @@ class WidefieldPlan:
         if density.dtype != np.float32 or not density.flags.c_contiguous or density.shape != self.shape:
             raise ValueError("density: a C-contiguous float32 array of the plan's shape")
         for name, arr, dt in (("adu", adu, np.uint16), ("image", image, np.float32)):
-            if arr is not None and (arr.dtype != dt or not arr.flags.c_contiguous or arr.shape != self.shape):
-                raise ValueError(f"{name}: a C-contiguous {np.dtype(dt).name} array of the plan's shape")
+            if arr is not None and (arr.dtype != dt or not arr.flags.c_contiguous or arr.shape != self.frame_shape):
+                raise ValueError(f"{name}: a C-contiguous {np.dtype(dt).name} array of the plan's frame shape")
         cam = camera.c() if camera is not None else None
         check(self.lib.iscu_wf_render_async(self.h, int(io_slot), _ptr(density), float(background),
                                             C.byref(cam) if cam is not None else None, seed, frame0,

@@ -1,4 +1,5 @@
-"""Frames across ranks: one process per GPU, each rendering a contiguous range of a movie's frames.
+"""Frames (and PSFs) across ranks: one process per GPU, each rendering a contiguous range of a movie's frames or of a
+PSF library's PSFs.
 
 A frame is a pure function of (spec, frame) -- the emitters are per (site, frame) hashes, the noise is keyed by
 (seed, frame, pixel), the drift is a precomputed per-frame table -- so ranks need no exchange on the data path: each
@@ -44,3 +45,12 @@ def gather_movie(frames, n_frames: int, device=None):
     parts = [torch.empty_like(pad) for _ in range(world)]
     dist.all_gather(parts, pad)
     return torch.cat([p[: e - b] for p, (b, e) in zip(parts, sizes)])
+
+
+def library_shard(lib, rank: int, world: int):
+    """The rank's share of a PSF library (workloads.PsfLibrary): its contiguous range of PSFs (frame_range over the
+    library's PSFs) with every request set, so each rank builds the same DFT operands and computes its PSFs alone; the
+    library is the ranks' ranges in rank order (gather_movie along the PSF axis)."""
+    from dataclasses import replace
+    first, end = frame_range(rank, world, len(lib.set_of_psf))
+    return replace(lib, set_of_psf=lib.set_of_psf[first:end], defocus_nm=lib.defocus_nm[first:end])

@@ -173,3 +173,59 @@ def test_codelet_2048_impulse(engine):
         want[z0, ys, xs] = psf[0, ys.start - y0 + 509: ys.stop - y0 + 509, xs.start - x0 + 509: xs.stop - x0 + 509]
         assert _rel(got, want) <= TOL, (z0, y0, x0)
     plan.close()
+
+
+def test_scene_plan_equals_reference_scene(engine, reference):
+    """The widefield scene as a device plan (iscu_wf_plan_from_kernel: KernelWidefieldPsf's cells made on the device
+    from a kernel slot, PlanFocus's clamped and blended planes, the grid's linear convolution, the FOV window, binning)
+    against the reference's WidefieldScene + FocusSeries + Render compiled from its sources, on the pinned cases of
+    tests/test_widefield_oracle.py (margins, resampling, clamped and blended planes, a capped radius)."""
+    import torch
+    from tests.test_widefield_oracle import CASES, scene_case
+    for case in CASES:
+        os_, up, half, nzk, step, plane, W, H, nzd, margin, cap = case
+        k, counts, want, want64, (gx, gy, fx, fy, u, Rc, _) = scene_case(reference, case)
+        engine.kernel_set_planes(1, k.planes(), os_, step, 2)
+        plan = WidefieldPlan.from_kernel(engine, 1, up, 0.1, cap, plane, counts.shape, (fx, fy, W, H))
+        assert plan.frame_shape == (nzd, H, W) and plan.kernel_radius == Rc
+        got = plan.convolve_dev(torch.from_numpy(counts).cuda()).cpu().numpy()
+        assert _rel(got, want) <= TOL, case
+        assert _rel(got, want64) <= TOL, case
+        plan.close()
+
+
+def test_scene_plan_full_size_against_reference(engine, reference):
+    """The widefield config at full size as the reference's scene: a 512 x 512 x 64 dye grid of 100 x 100 x 200 nm
+    cells (the FOV, no margin; the reference's extra far-edge cell row and column left empty), the 3D Gibson-Lanni
+    kernel stack (NA 1.4, 520 nm, 513 x 513 samples, 65 planes 200 nm apart) built on the device, the radius uncapped
+    (256 cells); four foci of the series against the reference's FocusSeries within 1e-5 of the frame maximum."""
+    import torch
+    from insiliscope_b200 import CZT_FP32
+    from insiliscope_b200.workloads import widefield_cells
+    wv = widefield_cells(seed=42)
+    nz, ny, nx = wv.density.shape
+    req = wv.psf
+    req.nz = 65
+    req.kernel_half_width_px = 256
+    engine.kernel_build(2, req, CZT_FP32)
+    planes = engine.kernel_planes(2)
+    assert planes.shape == (65, 513, 513)
+    plan = WidefieldPlan.from_kernel(engine, 2, 1, 0.1, 30.0, 200.0, (nz, ny, nx), (0, 0, nx, ny))
+    assert plan.kernel_radius == 256 and plan.grid() == (1024, 1024, 128)
+    got = plan.convolve_dev(torch.from_numpy(wv.density).cuda()).cpu().numpy()
+    k = reference.kernel(planes=planes, os_=1, z_step_nm=200.0, interp=2)
+    gx, gy, fx, fy = k.wf_grid(1, 0.1, nx, ny, (0.05, 0.05), 0.0, 200.0)
+    assert (gx, gy, fx, fy) == (nx + 1, ny + 1, 0, 0)
+    counts = np.zeros((nz, gy, gx), np.float32)
+    counts[:, :ny, :nx] = wv.density
+    foci = [0, 21, 42, 63]
+    reference.set_threads(0)
+    try:
+        want, info = k.wf_focus_series(counts, (np.array(foci) + 0.5) * 0.2, 1, 30.0, 0.1, nx, ny, (0.05, 0.05), 0.0,
+                                       200.0)
+    finally:
+        reference.set_threads(1)
+    assert info[2] == 256
+    errs = [_rel(got[f], want[i]) for i, f in enumerate(foci)]
+    print("widefield 512x512x64 vs the reference scene, foci", foci, "max rel error", errs)
+    assert max(errs) <= TOL
