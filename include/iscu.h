@@ -583,6 +583,55 @@ void iscu_wf_shift_destroy(iscu_wf_shift* s);
 int iscu_wf_shifted_frames_dev(iscu_wf_shift* s, const float* spectra_dev, uint32_t n_channels, const float* coef_dev,
                                const double* shift_dev, uint32_t n_frames, uint32_t x0, uint32_t y0, uint32_t cw,
                                uint32_t ch, uint32_t up, float scale, float* cam_dev);
+/* Focus jobs: the GPU side of a widefield scene (sim::WidefieldAccelerator, WidefieldRender.h:342-359; the job is
+ * WidefieldGpuJob, :306-337, as WidefieldScene::JobFor builds it, WidefieldRender.cpp:1953-2029). A job engine keeps
+ * plane spectra resident by key and kernel spectra by plane index, both within one geometry value (a new geometry or
+ * transform size drops them). iscu_wf_job_images: the job's kernel spectra not yet resident are uploaded (RealFft2d's
+ * layout: ny_fft rows of nx_fft/2 + 1 complex, interleaved float pairs), its new planes (sparse cells of the nx x ny
+ * dye grid, row-major, and their values) scattered and transformed, then each channel's image: sum over its deps of
+ * plane spectrum x (w0 K[p0] + w1 K[p1]) (ChannelImageStep, :1790-1801), the sub-cell shift (ApplyShiftRamp,
+ * DriftShift.cpp:24-48), the inverse transform (1 / (nx_fft ny_fft)) and the FOV window [fov_y0, + ch) x [fov_x0, + cw)
+ * (ChannelImageFinish, WidefieldRender.cpp:1844-1878) into images[c] (host, cw x ch floats, not clamped). FFT sizes:
+ * powers of two in 16..2048. budget_bytes (0: a quarter of the device) caps the plane spectra; iscu_wf_job_fits says
+ * whether `planes` spectra of that size fit it (WidefieldAccelerator::Fits). */
+typedef struct iscu_wf_job iscu_wf_job;
+typedef struct iscu_wf_job_kernel {
+   int32_t p;
+   int32_t reserved;
+   const float* spec;
+} iscu_wf_job_kernel;
+typedef struct iscu_wf_job_plane {
+   uint64_t key;
+   const uint32_t* cells;
+   const float* values;
+   uint32_t count;
+   uint32_t reserved;
+} iscu_wf_job_plane;
+typedef struct iscu_wf_job_dep {
+   uint64_t key;
+   int32_t p0, p1;
+   float w0, w1;
+   int32_t two;
+   int32_t reserved;
+} iscu_wf_job_dep;
+typedef struct iscu_wf_job_desc {
+   uint32_t nx_fft, ny_fft, nx, ny, fov_x0, fov_y0, cw, ch;
+   double frac_x, frac_y;
+   uint64_t geometry;
+   const iscu_wf_job_kernel* kernels;
+   uint32_t n_kernels;
+   uint32_t n_planes;
+   const iscu_wf_job_plane* planes;
+   const iscu_wf_job_dep* deps;            /* channel c: deps[channel_start[c] .. channel_start[c + 1]) */
+   const uint32_t* channel_start;          /* n_channels + 1 entries */
+   uint32_t n_channels;
+   uint32_t reserved;
+} iscu_wf_job_desc;
+int iscu_wf_job_create(iscu_ctx* ctx, uint64_t budget_bytes, iscu_wf_job** out);
+void iscu_wf_job_destroy(iscu_wf_job* job);
+int iscu_wf_job_has_plane(iscu_wf_job* job, uint64_t geometry, uint64_t key);
+int iscu_wf_job_fits(iscu_wf_job* job, uint64_t geometry, uint32_t nx_fft, uint32_t ny_fft, uint64_t planes);
+int iscu_wf_job_images(iscu_wf_job* job, const iscu_wf_job_desc* desc, float* const* images);
 /* The same on device buffers (the camera maps of iscu_set_static apply when their size is nx x ny). */
 int iscu_wf_render_dev(iscu_wf_plan* plan, const float* density_dev, double background, const iscu_camera* cam,
                        uint32_t seed, uint32_t frame0, float* image_dev, uint16_t* adu_dev);

@@ -222,6 +222,11 @@ SIGNATURES = {
     "iscu_wf_plan_from_kernel": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_uint32,
                                            C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                            C.POINTER(vp)]),
+    "iscu_wf_job_create": (C.c_int, [vp, C.c_uint64, C.POINTER(vp)]),
+    "iscu_wf_job_destroy": (None, [vp]),
+    "iscu_wf_job_has_plane": (C.c_int, [vp, C.c_uint64, C.c_uint64]),
+    "iscu_wf_job_fits": (C.c_int, [vp, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64]),
+    "iscu_wf_job_images": (C.c_int, [vp, vp, vp]),
     "iscu_wf_plan_frame": (C.c_int, [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_int32)]),
     "iscu_wf_plan_grid": (C.c_int, [vp, u32p, u32p, u32p]),
     "iscu_wf_convolve_dev": (C.c_int, [vp, vp, vp]),

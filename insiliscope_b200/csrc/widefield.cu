@@ -889,7 +889,7 @@ __device__ __forceinline__ void XLoad(const ColAddr& S, const float2* __restrict
 template <int kLogH>
 __global__ void __launch_bounds__(kThreads, kMinCtas) XInverseKernel(const float2* __restrict__ A, Dims d, int BY,
                                                                      int logBY, int ox, float scale, float background,
-                                                                     const float2* __restrict__ tw,
+                                                                     int clamp, const float2* __restrict__ tw,
                                                                      const float2* __restrict__ twg,
                                                                      float* __restrict__ image)
 {
@@ -909,7 +909,7 @@ __global__ void __launch_bounds__(kThreads, kMinCtas) XInverseKernel(const float
       const int m = x + ox;
       const float2 c = S(b, m >> 1);
       const float v = (m & 1 ? c.y : c.x) * scale;
-      out[t] = (v > 0.f ? v : 0.f) + background;
+      out[t] = (clamp && !(v > 0.f) ? 0.f : v) + background;
    }
 }
 
@@ -1434,7 +1434,7 @@ static int FinishX(iscu_wf_plan* p, double background, const iscu_camera* cam, u
    ISCU_WF_X_CODELETS(d.logH, (XInverseKernel<K><<<dim3((d.nyv + BY - 1) / BY, d.nzv), kThreads, XSmem(d.H, BY),
                                                    ctx->stream>>>(
                                   p->A.as<float2>(), d, BY, Log2(BY), static_cast<int>(p->kx / 2), scale,
-                                  p->camera ? 0.0f : static_cast<float>(background), p->tw.as<float2>(),
+                                  p->camera ? 0.0f : static_cast<float>(background), 1, p->tw.as<float2>(),
                                   p->twg.as<float2>(), xout)));
    ISCU_CK_LAUNCH(ctx, "XInverseKernel");
    if (p->camera)
@@ -1460,12 +1460,151 @@ static int FinishX(iscu_wf_plan* p, double background, const iscu_camera* cam, u
 namespace iscu {
 namespace {
 
+// ------------------------------------------------------------------------ focus jobs (WidefieldAccelerator)
+// Dense dye planes from a job's sparse ones: plane q's cell cells[i] (row-major in the nx x ny dye grid) += values[i]
+// for i in [start[q], start[q+1]). dense: planes x ny x nx, zeroed before.
+__global__ void JobScatterKernel(const uint32_t* __restrict__ cells, const float* __restrict__ values,
+                                 const uint32_t* __restrict__ start, uint32_t nPlanes, size_t planeCells,
+                                 float* __restrict__ dense)
+{
+   const uint32_t q = blockIdx.y;
+   if (q >= nPlanes)
+      return;
+   for (uint32_t i = start[q] + blockIdx.x * blockDim.x + threadIdx.x; i < start[q + 1]; i += gridDim.x * blockDim.x)
+      dense[q * planeCells + cells[i]] = values[i];
+}
+
+// A kernel spectrum in RealFft2d's layout (spec[ky W + kx], W = GX/2 + 1, ky natural) into the transforms' layout
+// (out[kx GY + rev(ky)]).
+__global__ void JobKernelLayoutKernel(const float2* __restrict__ spec, int NK, int GY, int logGY,
+                                      float2* __restrict__ out)
+{
+   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   if (i >= NK * GY)
+      return;
+   const int ky = i / NK, kx = i - ky * NK;
+   out[static_cast<size_t>(kx) * GY + Rev(ky, logGY)] = spec[i];
+}
+
+// A job's channel spectra (ChannelImageStep, WidefieldRender.cpp:1790-1801): per frequency, channel c's
+// S = sum over its deps d (in order) of plane P[d] x (w0 K[p0] + w1 K[p1]) in float (the blend and the product
+// term by term, as the reference forms them), then the sub-cell shift (ApplyShiftRamp, DriftShift.cpp:24-48):
+// S x (px[kx] py[ky]) formed in float64 and rounded to float, Nyquist terms their cosine only -- px and py
+// tabulated on the host. Spectra in the transforms' layout (kx-major, ky bit-reversed); out: channels x NK x GY.
+struct JobDep
+{
+   uint32_t plane, k0, k1;   // slots of the plane's spectrum and of its kernels (k1 only when two)
+   float w0, w1;
+   int32_t two;
+};
+
+__global__ void JobMacKernel(const float2* __restrict__ planes, const float2* __restrict__ kernels,
+                             const JobDep* __restrict__ deps, const uint32_t* __restrict__ chanStart,
+                             uint32_t nChannels, const double2* __restrict__ px, const double2* __restrict__ py,
+                             int ramp, int NK, int GY, int logGY, float2* __restrict__ out)
+{
+   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+   const size_t n = static_cast<size_t>(NK) * GY;
+   if (i >= static_cast<int>(n))
+      return;
+   double2 r = make_double2(1.0, 0.0);
+   if (ramp)
+   {
+      const int kx = i / GY, ky = Rev(i - kx * GY, logGY);
+      const double2 a = px[kx], b = py[ky];
+      r = make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+   }
+   for (uint32_t c = 0; c < nChannels; ++c)
+   {
+      float sr = 0.0f, si = 0.0f;
+      for (uint32_t j = chanStart[c]; j < chanStart[c + 1]; ++j)
+      {
+         const JobDep d = deps[j];
+         const float2 k0 = kernels[d.k0 * n + i];
+         float kr = d.w0 * k0.x, ki = d.w0 * k0.y;
+         if (d.two)
+         {
+            const float2 k1 = kernels[d.k1 * n + i];
+            kr += d.w1 * k1.x;
+            ki += d.w1 * k1.y;
+         }
+         const float2 a = planes[d.plane * n + i];
+         sr += a.x * kr - a.y * ki;
+         si += a.x * ki + a.y * kr;
+      }
+      float2 v = make_float2(sr, si);
+      if (ramp)
+      {
+         const double vr = sr, vi = si;
+         v = make_float2(static_cast<float>(vr * r.x - vi * r.y), static_cast<float>(vr * r.y + vi * r.x));
+      }
+      out[c * n + i] = v;
+   }
+}
+
+} // namespace
+} // namespace iscu
+
+// A widefield focus-job engine (iscu_wf_job_*): one 2D transform geometry at a time; plane spectra resident by key and
+// kernel spectra by plane index, both for the geometry value they were made in.
+struct iscu_wf_job
+{
+   iscu_ctx* ctx = nullptr;
+   size_t budget = 0;                     // device bytes the plane spectra may hold
+   uint64_t geometry = 0;
+   bool haveGeometry = false;
+   std::unique_ptr<iscu_wf_plan> plan;    // the NX x NY transforms (GX = NX, GY = NY)
+   std::vector<uint64_t> planeKeys;       // slot -> key
+   std::vector<int32_t> kernelPs;         // slot -> plane index p
+   iscu::DevBuf planes, kernels, dense, A, B, images, deps, starts, cells, values, rampX, rampY, stage;
+   size_t planeCap = 0, kernelCap = 0;
+   size_t Spec() const { return static_cast<size_t>(plan->NK) * plan->GY; }
+};
+
+namespace iscu {
+namespace {
+
 // The FFT length of one axis: a power of two that holds the kernel (k) and the volume's "same" window (n points from
 // k/2 on) of the circular convolution with nothing wrapped into it -- n + k/2 points (the output point i + k/2 reads
 // kernel taps i + k/2 - j for input points j < n: none of them wraps into [0, k) once the length passes n + k/2 - 1).
 uint32_t AxisLength(uint32_t n, uint32_t k, uint32_t least)
 {
    return Pow2AtLeast(std::max({n + k / 2, k, least}));
+}
+
+// The transforms' group plans, shared-memory ceilings and twiddle tables of a plan whose GX, GY and GZ are set.
+int InitTables(iscu_wf_plan* p)
+{
+   iscu_ctx* ctx = p->ctx;
+   p->H = p->GX / 2;
+   p->NK = p->H + 1;
+   p->G = std::max(p->GX, std::max(p->GY, p->GZ));
+   p->logH = Log2(p->H);
+   p->logGY = Log2(p->GY);
+   p->logGZ = Log2(p->GZ);
+   p->px = MakeLinePlan(p->logH, true);
+   p->py = MakeLinePlan(p->logGY, false);
+   p->pz = MakeZPlan(p->logGZ);
+   int entries = PlaceTables(p->px, 0);
+   entries += PlaceTables(p->py, entries);
+   entries += PlaceTables(p->pz, entries);
+   const int rc = SetFftSmem(p->logH, p->logGY, p->logGZ);
+   if (rc != ISCU_OK)
+      return rc;
+   ISCU_CK(p->tw.Reserve(p->G * sizeof(float2)));
+   ISCU_CK(p->twg.Reserve(std::max(entries, 1) * sizeof(float2)));
+   TwiddleKernel<<<(p->G + 255) / 256, 256, 0, ctx->stream>>>(static_cast<int>(p->G), p->tw.as<float2>());
+   ISCU_CK_LAUNCH(ctx, "TwiddleKernel");
+   for (const LinePlan* P : {&p->px, &p->py, &p->pz})
+      for (int g = 0; g < P->groups; ++g)
+         if (P->tw[g] >= 0)
+         {
+            const int M = 1 << (LogQ(*P, g) + P->r[g]);
+            GroupTwiddleKernel<<<(M + 255) / 256, 256, 0, ctx->stream>>>(LogQ(*P, g), P->r[g],
+                                                                          p->twg.as<float2>() + P->tw[g]);
+            ISCU_CK_LAUNCH(ctx, "GroupTwiddleKernel");
+         }
+   return ISCU_OK;
 }
 
 // A plan's geometry, tables and PSF spectrum; psf is a device pointer when psfOnDevice (kx*ky*kz floats).
@@ -1487,38 +1626,13 @@ int MakePlan(iscu_ctx* ctx, uint32_t nx, uint32_t ny, uint32_t nz, const float* 
       return Fail(ISCU_ERR_LIMIT, "widefield plan: padded grid beyond 4096 x 8192 x 8192");
    if (kx > p->GX || ky > p->GY)
       return Fail(ISCU_ERR_ARG, "widefield plan: PSF wider than the grid");
-   p->H = p->GX / 2;
-   p->NK = p->H + 1;
-   p->G = std::max(p->GX, std::max(p->GY, p->GZ));
-   p->logH = Log2(p->H);
-   p->logGY = Log2(p->GY);
-   p->logGZ = Log2(p->GZ);
-   p->px = MakeLinePlan(p->logH, true);
-   p->py = MakeLinePlan(p->logGY, false);
-   p->pz = MakeZPlan(p->logGZ);
-   int entries = PlaceTables(p->px, 0);
-   entries += PlaceTables(p->py, entries);
-   entries += PlaceTables(p->pz, entries);
-   int rc = SetFftSmem(p->logH, p->logGY, p->logGZ);
+   int rc = InitTables(p.get());
    if (rc != ISCU_OK)
       return rc;
    const uint32_t nzA = std::max(nz, kz), nyA = std::max(ny, ky);
-   ISCU_CK(p->tw.Reserve(p->G * sizeof(float2)));
-   ISCU_CK(p->twg.Reserve(std::max(entries, 1) * sizeof(float2)));
    ISCU_CK(p->A.Reserve(static_cast<size_t>(nzA) * p->NK * nyA * sizeof(float2)));
    ISCU_CK(p->B.Reserve(static_cast<size_t>(nzA) * p->NK * p->GY * sizeof(float2)));
    ISCU_CK(p->Kh.Reserve(static_cast<size_t>(p->GZ) * p->NK * p->GY * sizeof(float2)));
-   TwiddleKernel<<<(p->G + 255) / 256, 256, 0, ctx->stream>>>(static_cast<int>(p->G), p->tw.as<float2>());
-   ISCU_CK_LAUNCH(ctx, "TwiddleKernel");
-   for (const LinePlan* P : {&p->px, &p->py, &p->pz})
-      for (int g = 0; g < P->groups; ++g)
-         if (P->tw[g] >= 0)
-         {
-            const int M = 1 << (LogQ(*P, g) + P->r[g]);
-            GroupTwiddleKernel<<<(M + 255) / 256, 256, 0, ctx->stream>>>(LogQ(*P, g), P->r[g],
-                                                                          p->twg.as<float2>() + P->tw[g]);
-            ISCU_CK_LAUNCH(ctx, "GroupTwiddleKernel");
-         }
    // The PSF's spectrum: its own x and y passes (kx x ky x kz valid), then the forward z transform of all GZ planes.
    DevBuf dPsf;
    const size_t psfBytes = static_cast<size_t>(kx) * ky * kz * sizeof(float);
@@ -1658,6 +1772,251 @@ int iscu_wf_plan_from_kernel(iscu_ctx* ctx, int32_t slot, int32_t upscale, doubl
    p->fovH = fov_h;
    p->up = static_cast<uint32_t>(up);
    *out = p.release();
+   return ISCU_OK;
+}
+
+int iscu_wf_job_create(iscu_ctx* ctx, uint64_t budget_bytes, iscu_wf_job** out)
+{
+   if (!ctx || !out)
+      return Fail(ISCU_ERR_ARG, "null argument");
+   *out = nullptr;
+   std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+   ClearError();
+   std::unique_ptr<iscu_wf_job> j(new iscu_wf_job());
+   j->ctx = ctx;
+   size_t freeB = 0, total = 0;
+   ISCU_CK(cudaMemGetInfo(&freeB, &total));
+   j->budget = budget_bytes ? static_cast<size_t>(budget_bytes) : total / 4;
+   *out = j.release();
+   return ISCU_OK;
+}
+
+void iscu_wf_job_destroy(iscu_wf_job* job)
+{
+   if (!job)
+      return;
+   cudaStreamSynchronize(job->ctx->stream);
+   delete job;
+}
+
+int iscu_wf_job_has_plane(iscu_wf_job* job, uint64_t geometry, uint64_t key)
+{
+   if (!job)
+      return 0;
+   std::lock_guard<std::recursive_mutex> lock(job->ctx->mu);
+   if (!job->haveGeometry || job->geometry != geometry)
+      return 0;
+   return std::find(job->planeKeys.begin(), job->planeKeys.end(), key) != job->planeKeys.end() ? 1 : 0;
+}
+
+int iscu_wf_job_fits(iscu_wf_job* job, uint64_t geometry, uint32_t nx_fft, uint32_t ny_fft, uint64_t planes)
+{
+   (void)geometry;
+   if (!job)
+      return 0;
+   const double per = (nx_fft / 2.0 + 1.0) * ny_fft * sizeof(float2);
+   return per * static_cast<double>(planes) <= static_cast<double>(job->budget) ? 1 : 0;
+}
+
+int iscu_wf_job_images(iscu_wf_job* job, const iscu_wf_job_desc* d, float* const* images)
+{
+   if (!job || !d || (d->n_channels && (!images || !d->channel_start)))
+      return Fail(ISCU_ERR_ARG, "null argument");
+   const uint32_t NX = d->nx_fft, NY = d->ny_fft;
+   if (NX < 16 || NY < 16 || NX > 2048 || NY > 2048 || (NX & (NX - 1)) || (NY & (NY - 1)))
+      return Fail(ISCU_ERR_ARG, "widefield job: FFT sizes powers of two in 16..2048");
+   if (d->nx == 0 || d->ny == 0 || d->nx > NX || d->ny > NY || d->cw == 0 || d->ch == 0 ||
+       d->fov_x0 + d->cw > NX || d->fov_y0 + d->ch > NY)
+      return Fail(ISCU_ERR_ARG, "widefield job: the dye grid and the FOV window must lie inside the FFT grid");
+   iscu_ctx* ctx = job->ctx;
+   std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+   ClearError();
+   // A new geometry (or transform size) drops every resident spectrum.
+   if (!job->plan || job->plan->GX != NX || job->plan->GY != NY || !job->haveGeometry || job->geometry != d->geometry)
+   {
+      if (!job->plan || job->plan->GX != NX || job->plan->GY != NY)
+      {
+         std::unique_ptr<iscu_wf_plan> p(new iscu_wf_plan());
+         p->ctx = ctx;
+         p->GX = NX;
+         p->GY = NY;
+         p->GZ = 4;
+         const int rc = InitTables(p.get());
+         if (rc != ISCU_OK)
+            return rc;
+         job->plan = std::move(p);
+      }
+      job->planeKeys.clear();
+      job->kernelPs.clear();
+      job->geometry = d->geometry;
+      job->haveGeometry = true;
+   }
+   iscu_wf_plan* P = job->plan.get();
+   const size_t spec = job->Spec(), specBytes = spec * sizeof(float2);
+   auto growSlots = [&](DevBuf& buf, size_t& cap, size_t need) -> int {
+      if (need <= cap)
+         return ISCU_OK;
+      size_t want = std::max(need, cap * 2 + 8);
+      DevBuf grown;
+      ISCU_CK(grown.Reserve(want * specBytes));
+      if (cap)
+         ISCU_CK(cudaMemcpyAsync(grown.p, buf.p, cap * specBytes, cudaMemcpyDeviceToDevice, ctx->stream));
+      ISCU_CK(cudaStreamSynchronize(ctx->stream));
+      std::swap(buf.p, grown.p);
+      std::swap(buf.bytes, grown.bytes);
+      cap = want;
+      return ISCU_OK;
+   };
+   // Kernel spectra not yet resident: RealFft2d's layout in, the transforms' layout kept.
+   for (uint32_t i = 0; i < d->n_kernels; ++i)
+   {
+      const iscu_wf_job_kernel& k = d->kernels[i];
+      if (std::find(job->kernelPs.begin(), job->kernelPs.end(), k.p) != job->kernelPs.end())
+         continue;
+      if (!k.spec)
+         return Fail(ISCU_ERR_ARG, "widefield job: a kernel without its spectrum");
+      int rc = growSlots(job->kernels, job->kernelCap, job->kernelPs.size() + 1);
+      if (rc != ISCU_OK)
+         return rc;
+      ISCU_CK(job->stage.Reserve(specBytes));
+      ISCU_CK(cudaMemcpyAsync(job->stage.p, k.spec, specBytes, cudaMemcpyHostToDevice, ctx->stream));
+      JobKernelLayoutKernel<<<static_cast<unsigned>((spec + 255) / 256), 256, 0, ctx->stream>>>(
+         job->stage.as<float2>(), static_cast<int>(P->NK), static_cast<int>(NY), P->logGY,
+         job->kernels.as<float2>() + job->kernelPs.size() * spec);
+      ISCU_CK_LAUNCH(ctx, "JobKernelLayoutKernel");
+      ISCU_CK(cudaStreamSynchronize(ctx->stream));   // the stage is reused by the next kernel
+      job->kernelPs.push_back(k.p);
+   }
+   // New plane spectra: the sparse cells made dense, then the forward x and y passes straight into their slots.
+   std::vector<uint32_t> starts(1, 0);
+   std::vector<uint32_t> cellsH;
+   std::vector<float> valuesH;
+   std::vector<uint64_t> newKeys;
+   for (uint32_t q = 0; q < d->n_planes; ++q)
+   {
+      const iscu_wf_job_plane& pl = d->planes[q];
+      if (std::find(job->planeKeys.begin(), job->planeKeys.end(), pl.key) != job->planeKeys.end() ||
+          std::find(newKeys.begin(), newKeys.end(), pl.key) != newKeys.end())
+         continue;
+      for (uint32_t i = 0; i < pl.count; ++i)
+         if (pl.cells[i] >= static_cast<uint64_t>(d->nx) * d->ny)
+            return Fail(ISCU_ERR_ARG, "widefield job: a plane cell outside the dye grid");
+      cellsH.insert(cellsH.end(), pl.cells, pl.cells + pl.count);
+      valuesH.insert(valuesH.end(), pl.values, pl.values + pl.count);
+      starts.push_back(static_cast<uint32_t>(cellsH.size()));
+      newKeys.push_back(pl.key);
+   }
+   const uint32_t nNew = static_cast<uint32_t>(newKeys.size());
+   if (nNew)
+   {
+      const size_t base = job->planeKeys.size();
+      if ((base + nNew) * specBytes > job->budget)
+         return Fail(ISCU_ERR_LIMIT, "widefield job: the plane spectra pass the job's device budget");
+      int rc = growSlots(job->planes, job->planeCap, base + nNew);
+      if (rc != ISCU_OK)
+         return rc;
+      const size_t planeCells = static_cast<size_t>(d->nx) * d->ny;
+      ISCU_CK(job->dense.Reserve(nNew * planeCells * sizeof(float)));
+      ISCU_CK(cudaMemsetAsync(job->dense.p, 0, nNew * planeCells * sizeof(float), ctx->stream));
+      ISCU_CK(job->cells.Reserve(std::max<size_t>(1, cellsH.size()) * sizeof(uint32_t)));
+      ISCU_CK(job->values.Reserve(std::max<size_t>(1, valuesH.size()) * sizeof(float)));
+      ISCU_CK(job->starts.Reserve(starts.size() * sizeof(uint32_t)));
+      ISCU_CK(cudaMemcpyAsync(job->cells.p, cellsH.data(), cellsH.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                              ctx->stream));
+      ISCU_CK(cudaMemcpyAsync(job->values.p, valuesH.data(), valuesH.size() * sizeof(float), cudaMemcpyHostToDevice,
+                              ctx->stream));
+      ISCU_CK(cudaMemcpyAsync(job->starts.p, starts.data(), starts.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                              ctx->stream));
+      JobScatterKernel<<<dim3(32, nNew), 256, 0, ctx->stream>>>(job->cells.as<uint32_t>(), job->values.as<float>(),
+                                                               job->starts.as<uint32_t>(), nNew, planeCells,
+                                                               job->dense.as<float>());
+      ISCU_CK_LAUNCH(ctx, "JobScatterKernel");
+      const Dims dp = MakeDims(P, d->nx, d->ny, nNew);
+      ISCU_CK(job->A.Reserve(static_cast<size_t>(nNew) * P->NK * d->ny * sizeof(float2)));
+      rc = ForwardXY(P, job->dense.as<float>(), dp, job->A.as<float2>(), job->planes.as<float2>() + base * spec);
+      if (rc != ISCU_OK)
+         return rc;
+      ISCU_CK(cudaStreamSynchronize(ctx->stream));   // the host staging vectors go out of scope
+      job->planeKeys.insert(job->planeKeys.end(), newKeys.begin(), newKeys.end());
+   }
+   const uint32_t nc = d->n_channels;
+   if (nc == 0)
+      return ISCU_OK;
+   // The channels' deps as slots.
+   std::vector<JobDep> deps;
+   std::vector<uint32_t> chan(1, 0);
+   for (uint32_t c = 0; c < nc; ++c)
+   {
+      for (uint32_t j = d->channel_start[c]; j < d->channel_start[c + 1]; ++j)
+      {
+         const iscu_wf_job_dep& e = d->deps[j];
+         const auto pk = std::find(job->planeKeys.begin(), job->planeKeys.end(), e.key);
+         const auto k0 = std::find(job->kernelPs.begin(), job->kernelPs.end(), e.p0);
+         const auto k1 = std::find(job->kernelPs.begin(), job->kernelPs.end(), e.two ? e.p1 : e.p0);
+         if (pk == job->planeKeys.end() || k0 == job->kernelPs.end() || k1 == job->kernelPs.end())
+            return Fail(ISCU_ERR_STATE, "widefield job: a dep names a plane or kernel that is not resident");
+         deps.push_back({static_cast<uint32_t>(pk - job->planeKeys.begin()),
+                         static_cast<uint32_t>(k0 - job->kernelPs.begin()),
+                         static_cast<uint32_t>(k1 - job->kernelPs.begin()), e.w0, e.two ? e.w1 : 0.0f,
+                         e.two ? 1 : 0});
+      }
+      chan.push_back(static_cast<uint32_t>(deps.size()));
+   }
+   // ApplyShiftRamp's factors (DriftShift.cpp:24-48), tabulated as the reference tabulates them.
+   const bool ramp = d->frac_x != 0.0 || d->frac_y != 0.0;
+   const uint32_t W = NX / 2 + 1;
+   std::vector<double2> px(W), py(NY);
+   const double kPi = 3.14159265358979323846;
+   for (uint32_t kx = 0; kx < W; ++kx)
+   {
+      const double a = 2.0 * kPi * kx * d->frac_x / NX;
+      px[kx] = kx == NX / 2 ? make_double2(std::cos(a), 0.0) : make_double2(std::cos(a), std::sin(a));
+   }
+   for (uint32_t ky = 0; ky < NY; ++ky)
+   {
+      const long kys = ky <= NY / 2 ? static_cast<long>(ky) : static_cast<long>(ky) - static_cast<long>(NY);
+      const double a = 2.0 * kPi * kys * d->frac_y / NY;
+      py[ky] = ky == NY / 2 ? make_double2(std::cos(a), 0.0) : make_double2(std::cos(a), std::sin(a));
+   }
+   ISCU_CK(job->deps.Reserve(std::max<size_t>(1, deps.size()) * sizeof(JobDep)));
+   ISCU_CK(job->starts.Reserve(chan.size() * sizeof(uint32_t)));
+   ISCU_CK(job->rampX.Reserve(W * sizeof(double2)));
+   ISCU_CK(job->rampY.Reserve(NY * sizeof(double2)));
+   ISCU_CK(cudaMemcpyAsync(job->deps.p, deps.data(), deps.size() * sizeof(JobDep), cudaMemcpyHostToDevice,
+                           ctx->stream));
+   ISCU_CK(cudaMemcpyAsync(job->starts.p, chan.data(), chan.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                           ctx->stream));
+   ISCU_CK(cudaMemcpyAsync(job->rampX.p, px.data(), W * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
+   ISCU_CK(cudaMemcpyAsync(job->rampY.p, py.data(), NY * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
+   ISCU_CK(job->B.Reserve(nc * specBytes));
+   JobMacKernel<<<static_cast<unsigned>((spec + 255) / 256), 256, 0, ctx->stream>>>(
+      job->planes.as<float2>(), job->kernels.as<float2>(), job->deps.as<JobDep>(), job->starts.as<uint32_t>(), nc,
+      job->rampX.as<double2>(), job->rampY.as<double2>(), ramp ? 1 : 0, static_cast<int>(P->NK),
+      static_cast<int>(NY), P->logGY, job->B.as<float2>());
+   ISCU_CK_LAUNCH(ctx, "JobMacKernel");
+   // The inverse: rows [fov_y0, + ch) then columns [fov_x0, + cw), scaled 1 / (NX NY) (RealFft2d::Inverse), no clamp.
+   const Dims di = MakeDims(P, d->cw, d->ch, nc);
+   ISCU_CK(job->A.Reserve(static_cast<size_t>(nc) * P->NK * d->ch * sizeof(float2)));
+   const float2* twg = P->twg.as<float2>();
+   const int BK = YLines(di.py);
+   ISCU_WF_Y_CODELETS(di.logGY, (YInverseKernel<K><<<dim3((di.NK + BK - 1) / BK, di.nzv), kThreads,
+                                                     BK * RowBytes(di.py), ctx->stream>>>(
+                                    job->B.as<float2>(), di, BK, static_cast<int>(d->fov_y0), twg,
+                                    job->A.as<float2>())));
+   ISCU_CK_LAUNCH(ctx, "YInverseKernel");
+   const size_t frame = static_cast<size_t>(d->cw) * d->ch;
+   ISCU_CK(job->images.Reserve(nc * frame * sizeof(float)));
+   const int BY = XLines(di.H);
+   const float scale = static_cast<float>(1.0 / (static_cast<double>(NX) * NY));
+   ISCU_WF_X_CODELETS(di.logH, (XInverseKernel<K><<<dim3((di.nyv + BY - 1) / BY, di.nzv), kThreads,
+                                                    XSmem(di.H, BY), ctx->stream>>>(
+                                   job->A.as<float2>(), di, BY, Log2(BY), static_cast<int>(d->fov_x0), scale, 0.0f,
+                                   0, P->tw.as<float2>(), twg, job->images.as<float>())));
+   ISCU_CK_LAUNCH(ctx, "XInverseKernel");
+   for (uint32_t c = 0; c < nc; ++c)
+      ISCU_CK(cudaMemcpyAsync(images[c], job->images.as<float>() + c * frame, frame * sizeof(float),
+                              cudaMemcpyDeviceToHost, ctx->stream));
+   ISCU_CK(cudaStreamSynchronize(ctx->stream));
    return ISCU_OK;
 }
 
