@@ -180,9 +180,10 @@ int iscu_psf_plan_run(iscu_psf_plan* plan, const uint32_t* set_of_psf, const dou
  * synchronization a cudaFree implies. Its temporaries (set parameters, PSF items, pupil tables, DFT matrices) live in
  * one statically sized device array of ISCU_NOALLOC_SCRATCH_BYTES that every GPU loading libiscu.so holds until exit;
  * the call itself allocates nothing on the device. Limits: at most ISCU_NOALLOC_MAX_SETS sets and
- * ISCU_NOALLOC_MAX_PSF PSFs, pupil samples M <= 128, plane size P <= 129 with (M*M + P*M)*8 <= 227 KB (one CTA's
- * shared memory: at M = 128, P <= 99), and the layout within the array (sets, items, M*M*24 bytes of tables and
- * 2*P*M*8 bytes of DFT matrices per set) must fit; beyond: ISCU_ERR_LIMIT, before any copy or launch.
+ * ISCU_NOALLOC_MAX_PSF PSFs, pupil samples M <= 128, plane size P <= 129 with (M*M + P*M)*8 bytes beside the FP32
+ * chirp-Z kernel's static shared memory within one CTA's limit (227 KB on a B200: at M = 128, P <= 98), and the
+ * layout within the array (sets, items, M*M*24 bytes of tables and 2*P*M*8 bytes of DFT matrices per set) must fit;
+ * beyond: ISCU_ERR_LIMIT, before any copy or launch.
  * The first call on a device looks up the array's device address (cudaGetSymbolAddress), so make that first call
  * before any stream capture. All calls share the array: calls whose work overlaps on the GPU (other threads or
  * contexts) race. Returns when the planes are in out_dev. */

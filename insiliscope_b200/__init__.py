@@ -5,11 +5,11 @@ The compute lives in libiscu.so (CUDA kernels + C ABI, include/iscu.h); this pac
 from .engine import (BLINK_EVENT_DTYPE, CZT_FP32, CZT_TF32X3, DYE_DTYPE, EMITTER_DTYPE, EVENT_STRIDE, FRAME_DTYPE,
                      GPU_SPLAT_EMITTER_DTYPE, INTERP_CUBIC, INTERP_LINEAR, INTERP_NEAREST, LABEL_DNA_PAINT,
                      LABEL_DSTORM, LABEL_PALM, LABEL_WIDEFIELD, BinnedRenderer, CameraParams, Engine, IscuError,
-                     PsfParams, PsfPlan, RenderGraph, TiffWriter, WidefieldPlan, WidefieldShift, frames_table,
+                     PsfParams, PsfPlan, RenderGraph, TiffWriter, WidefieldJob, WidefieldPlan, WidefieldShift, frames_table,
                      generate_camera_maps)
 
 __all__ = ["Engine", "CameraParams", "PsfParams", "PsfPlan", "RenderGraph", "IscuError", "WidefieldPlan", "BinnedRenderer",
-           "TiffWriter", "WidefieldShift",
+           "TiffWriter", "WidefieldShift", "WidefieldJob",
            "generate_camera_maps",
            "frames_table",
            "EMITTER_DTYPE", "FRAME_DTYPE", "GPU_SPLAT_EMITTER_DTYPE", "BLINK_EVENT_DTYPE", "CZT_FP32", "CZT_TF32X3",

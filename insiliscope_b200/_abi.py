@@ -46,6 +46,29 @@ class Camera(C.Structure):
     ]
 
 
+class WfJobKernel(C.Structure):
+    _fields_ = [("p", C.c_int32), ("reserved", C.c_int32), ("spec", C.c_void_p)]
+
+
+class WfJobPlane(C.Structure):
+    _fields_ = [("key", C.c_uint64), ("cells", C.c_void_p), ("values", C.c_void_p), ("count", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+
+class WfJobDep(C.Structure):
+    _fields_ = [("key", C.c_uint64), ("p0", C.c_int32), ("p1", C.c_int32), ("w0", C.c_float), ("w1", C.c_float),
+                ("two", C.c_int32), ("reserved", C.c_int32)]
+
+
+class WfJobDesc(C.Structure):
+    _fields_ = [("nx_fft", C.c_uint32), ("ny_fft", C.c_uint32), ("nx", C.c_uint32), ("ny", C.c_uint32),
+                ("fov_x0", C.c_uint32), ("fov_y0", C.c_uint32), ("cw", C.c_uint32), ("ch", C.c_uint32),
+                ("frac_x", C.c_double), ("frac_y", C.c_double), ("geometry", C.c_uint64),
+                ("kernels", C.c_void_p), ("n_kernels", C.c_uint32), ("n_planes", C.c_uint32),
+                ("planes", C.c_void_p), ("deps", C.c_void_p), ("channel_start", C.c_void_p),
+                ("n_channels", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 class PsfRequest(C.Structure):
     _fields_ = [
         ("wavelength_nm", C.c_double),

@@ -9,7 +9,9 @@
 // this header is compiled with --fmad=false, as the reference is with -ffp-contract=off (core/CMakeLists.txt:41);
 // (2) IEEE float64 sqrt and division (always correctly rounded in CUDA); (3) CUDA's float64 log/exp/cos, which, like
 // glibc's, are within an ulp: an integer draw can differ only when its argument sits within ~1e-16 of a count
-// boundary.
+// boundary. A normal draw that only feeds a rounding (DrawGauss) is first tried in float32: the count it gives is
+// taken only when no rounding boundary lies within the float32 form's error bound of it, so every count is the one
+// the float64 form gives.
 #pragma once
 
 #include <cstdint>
@@ -99,13 +101,62 @@ __device__ __forceinline__ double CounterGauss(CounterRng& u)
    return r * cos(6.283185307179586 * u.Uniform());
 }
 
-// Knuth inversion up to mean 60, the rounded normal beyond; 1000-iteration cap (SMLMCounterRng.h:102-118).
+// A Box-Muller normal whose value matters only through a rounding to an integer (the read noise of an ADU, the
+// rounded normal of a large-mean Poisson draw): the stream's next two uniforms, drawn as CounterGauss draws them
+// (radius first, angle second), and gf, the same formula in float32. The uniforms are 24-bit values, exact in float;
+// logf and cospif are within 1 ulp and sqrtf is correctly rounded (CUDA's documented bounds), so with |g| <= 5.8
+// (u1 >= 2^-24) |gf - g| stays below 2e-6 -- kGaussFastErr is 5x that, covering bounds up to 4 ulp.
+constexpr double kGaussFastErr = 1e-5;
+
+struct GaussDraw
+{
+   double u1, u2;
+   float gf;
+};
+
+__device__ __forceinline__ GaussDraw DrawGauss(CounterRng& u)
+{
+   GaussDraw d;
+   d.u1 = u.Uniform();
+   d.u2 = u.Uniform();
+   d.gf = sqrtf(-2.0f * logf(static_cast<float>(d.u1))) * cospif(2.0f * static_cast<float>(d.u2));
+   return d;
+}
+
+// CounterGauss's value of a draw, with its operations in its order.
+__device__ __forceinline__ double GaussExact(const GaussDraw& d)
+{
+   const double r = sqrt(-2.0 * log(d.u1));
+   return r * cos(6.283185307179586 * d.u2);
+}
+
+// floor(v + 0.5) for a v known only to within m of vf: true (and the value) when no rounding boundary n + 0.5 lies
+// within m of vf, so that every v in [vf - m, vf + m] rounds alike.
+__device__ __forceinline__ bool RoundsSurely(double vf, double m, double& out)
+{
+   const double t = vf + 0.5, f = floor(t);
+   if (t - f > m && f + 1.0 - t > m)
+   {
+      out = f;
+      return true;
+   }
+   return false;
+}
+
+// Knuth inversion up to mean 60, the rounded normal beyond; 1000-iteration cap (SMLMCounterRng.h:102-118). The
+// rounded normal floor(l + sqrt(l) g + 0.5) is decided from the float32 normal when no rounding boundary is within
+// sqrt(l) kGaussFastErr of it, else from CounterGauss's float64 value of the same uniforms: the same count either way.
 __device__ __forceinline__ double CounterPoisson(double l, CounterRng& u)
 {
    if (l > 60.0)
    {
       const double s = sqrt(l);
-      const double g = CounterGauss(u);
+      const GaussDraw d = DrawGauss(u);
+      double r;
+      // (l > 60: l + s g >= sqrt(l) (sqrt(l) - 5.8) > 0, so the fmax never acts on a count decided here)
+      if (RoundsSurely(l + s * static_cast<double>(d.gf), s * kGaussFastErr + 1e-9 * l, r) && r >= 1.0)
+         return r;
+      const double g = GaussExact(d);
       return fmax(0.0, floor(l + s * g + 0.5));
    }
    if (!(l > 0.0))

@@ -24,15 +24,28 @@ __device__ __forceinline__ uint16_t NoisePixel(float photonValue, uint32_t i, co
       const double readE = (st.readNoise ? static_cast<double>(st.readNoise[i]) : cam.readNoise) / cam.emGain;
       const double gain = st.gain ? static_cast<double>(st.gain[i]) : cam.gain;
       const double offset = st.offset ? static_cast<double>(st.offset[i]) : 0.0;
-      const double g = CounterGauss(u);
-      const double adu = floor(offset + (out + readE * g) / gain + 0.5);
+      // the rounding (before the clamp) from the float32 normal when no boundary is within |readE / gain|
+      // kGaussFastErr of it, else from the float64 one
+      const GaussDraw d = DrawGauss(u);
+      const double af = offset + (out + readE * static_cast<double>(d.gf)) / gain;
+      double adu;
+      if (!RoundsSurely(af, fabs(readE / gain) * kGaussFastErr + 1e-9 * (1.0 + fabs(af)), adu))
+         adu = floor(offset + (out + readE * GaussExact(d)) / gain + 0.5);
       return static_cast<uint16_t>(adu < 0.0 ? 0.0 : (adu > cam.maxAdu ? cam.maxAdu : adu));
    }
    const double ne = CounterPoisson(photons * cam.qe + cam.dark, u);
    const double readNoise = st.readNoise ? static_cast<double>(st.readNoise[i]) : cam.readNoise;
    const double gain = st.gain ? static_cast<double>(st.gain[i]) : cam.gain;
    const double offset = st.offset ? static_cast<double>(st.offset[i]) : 0.0;
-   const double g = CounterGauss(u);
+   const GaussDraw d = DrawGauss(u);
+   // The ADU from the float32 normal when it is sure: inside (0, 65535) and no rounding boundary within
+   // |readNoise / gain| kGaussFastErr of it (the float64 operations' own rounding, ~1e-13, inside the 1e-9 term).
+   const double af = offset + (ne + readNoise * static_cast<double>(d.gf)) / gain;
+   const double m = fabs(readNoise / gain) * kGaussFastErr + 1e-9 * (1.0 + fabs(af));
+   double r;
+   if (af > m && af < 65535.0 - m && RoundsSurely(af, m, r))
+      return static_cast<uint16_t>(r);
+   const double g = GaussExact(d);
    double adu = offset + (ne + readNoise * g) / gain;
    adu = adu < 0.0 ? 0.0 : (adu > 65535.0 ? 65535.0 : adu);
    return static_cast<uint16_t>(floor(adu + 0.5));

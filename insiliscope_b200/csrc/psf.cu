@@ -597,6 +597,22 @@ int LaunchCztFp32(iscu_ctx* ctx, const SetParams* dSets, const double3* dTab, co
    return ISCU_OK;
 }
 
+int CheckFp32CztSmem(iscu_ctx* ctx, int M, int P, size_t* smem)
+{
+   *smem = (static_cast<size_t>(M) * M + static_cast<size_t>(P) * M) * sizeof(float2);
+   cudaFuncAttributes fa;
+   ISCU_CK(cudaFuncGetAttributes(&fa, CztFp32Kernel));
+   int optin = 0;
+   ISCU_CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+   if (*smem + fa.sharedSizeBytes > static_cast<size_t>(optin))
+      return Fail(ISCU_ERR_LIMIT, "psf library (fp32): the pupil and row pass need (M*M + P*M)*8 = " +
+                                     std::to_string(*smem) + " bytes of shared memory beside the kernel's " +
+                                     std::to_string(fa.sharedSizeBytes) + ", over the device's " +
+                                     std::to_string(optin) + " per block (M = " + std::to_string(M) + ", P = " +
+                                     std::to_string(P) + ")");
+   return ISCU_OK;
+}
+
 // The plain FP32 pipeline (tables, DFT matrices, chirp-Z) on buffers the caller provides.
 int LaunchPsfPipelineFp32(iscu_ctx* ctx, const SetParams* dSets, const PsfItem* dItems, double3* dTab, float2* dA,
                           float2* dAt, uint32_t nSets, uint32_t nPsf, int M, int P, int normalize, float* out)
@@ -605,9 +621,10 @@ int LaunchPsfPipelineFp32(iscu_ctx* ctx, const SetParams* dSets, const PsfItem* 
    ISCU_CK_LAUNCH(ctx, "PupilTablesKernel");
    DftMatrixKernel<<<dim3((P * M + 255) / 256, nSets), 256, 0, ctx->stream>>>(dSets, M, P, dA, dAt);
    ISCU_CK_LAUNCH(ctx, "DftMatrixKernel");
-   const size_t smem = (static_cast<size_t>(M) * M + static_cast<size_t>(P) * M) * sizeof(float2);
-   if (smem > 227 * 1024)
-      return Fail(ISCU_ERR_LIMIT, "psf library (fp32): pupil and row pass exceed shared memory");
+   size_t smem = 0;
+   const int rc = CheckFp32CztSmem(ctx, M, P, &smem);
+   if (rc != ISCU_OK)
+      return rc;
    ISCU_CK(cudaFuncSetAttribute(CztFp32Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
    CztFp32Kernel<<<nPsf, kCztThreads, smem, ctx->stream>>>(dSets, dTab, dA, dAt, dItems, M, P, normalize, out);
    ISCU_CK_LAUNCH(ctx, "CztFp32Kernel");

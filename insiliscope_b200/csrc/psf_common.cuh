@@ -81,6 +81,10 @@ int LaunchCztFp32(iscu_ctx* ctx, const SetParams* dSets, const double3* dTab, co
 
 int PrepareSetParams(const iscu_psf_request* sets, uint32_t nSets, int32_t size, uint32_t maxSets, SetParams* out,
                      int* M, int* P);
+// ISCU_OK when the FP32 chirp-Z kernel's dynamic shared memory -- the pupil (M x M) and the row pass (P x M), complex
+// float -- fits beside its static shared memory in one CTA of the context's device (the per-block opt-in limit);
+// ISCU_ERR_LIMIT (naming the bytes) otherwise. *smem: the dynamic bytes.
+int CheckFp32CztSmem(iscu_ctx* ctx, int M, int P, size_t* smem);
 int LaunchPsfPipelineFp32(iscu_ctx* ctx, const SetParams* dSets, const PsfItem* dItems, double3* dTab, float2* dA,
                           float2* dAt, uint32_t nSets, uint32_t nPsf, int M, int P, int normalize, float* out);
 

@@ -116,10 +116,10 @@ extern "C" int iscu_psf_library_noalloc_dev(iscu_ctx* ctx, const iscu_psf_reques
       return Fail(ISCU_ERR_LIMIT, "psf library (no allocation): pupil samples at most 128 and plane size at most "
                                   "129, asked for M = " + std::to_string(M) + ", P = " + std::to_string(P));
    // The FP32 chirp-Z kernel holds the pupil (M x M) and the row pass (P x M) complex in one CTA's shared memory.
-   const size_t smem = (static_cast<size_t>(M) * M + static_cast<size_t>(P) * M) * sizeof(float2);
-   if (smem > 227 * 1024)
-      return Fail(ISCU_ERR_LIMIT, "psf library (no allocation): (M*M + P*M)*8 bytes of shared memory exceed 227 KB, "
-                                  "asked for M = " + std::to_string(M) + ", P = " + std::to_string(P));
+   size_t smem = 0;
+   rc = CheckFp32CztSmem(ctx, M, P, &smem);
+   if (rc != ISCU_OK)
+      return rc;
    // The layout inside the scratch array.
    const size_t oSets = 0;
    const size_t oSetOf = oSets + Align256(n_sets * sizeof(SetParams));

@@ -32,7 +32,10 @@ namespace iscu {
 namespace {
 
 constexpr int kE = 64;          // emitters per contribution work item
-constexpr int kMaxCT = 640;     // contribution CTA size bound
+// Contribution CTAs: at most 224 computing threads and a staging warp, four per SM (64 registers: the 16 float64 taps
+// in registers without spills), so one CTA's per-item barrier leaves the FP64 pipe to the other three.
+constexpr int kMaxCT = 224;     // contribution CTA size bound
+constexpr int kContribPerSm = 4;
 constexpr int kGT = 256;        // gather CTA size (one thread per pixel of the tile)
 constexpr int kGChunk = 256;    // gather staging chunk
 
@@ -402,7 +405,7 @@ __device__ __forceinline__ void FetchItem(const ContribArgs& a, int* info)
 
 // blockDim.x = computing threads + one staging warp: while the others compute item i, the last warp fetches item
 // i + 1 and stages its emitters into the other buffer.
-__global__ void __launch_bounds__(kMaxCT + 32, 1) ContribKernel(ContribArgs a)
+__global__ void __launch_bounds__(kMaxCT + 32, kContribPerSm) ContribKernel(ContribArgs a)
 {
    __shared__ CStage sE[2][kE];
    __shared__ int sInfo[2][4];

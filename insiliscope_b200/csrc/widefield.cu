@@ -1707,8 +1707,8 @@ int iscu_wf_plan_from_kernel(iscu_ctx* ctx, int32_t slot, int32_t upscale, doubl
    *out = nullptr;
    if (slot < 0 || slot >= ISCU_MAX_KERNELS)
       return Fail(ISCU_ERR_ARG, "kernel slot out of range (0..3)");
-   if (nx < 2 || ny < 1 || nz < 1 || nx % 2 != 0)
-      return Fail(ISCU_ERR_ARG, "widefield plan: nx even >= 2, ny and nz >= 1");
+   if (nx < 1 || ny < 1 || nz < 1)
+      return Fail(ISCU_ERR_ARG, "widefield plan: nx, ny and nz >= 1");
    if (!(pixel_um > 0.0) || !(kernel_cap_um > 0.0) || !(plane_nm > 0.0))
       return Fail(ISCU_ERR_ARG, "widefield plan: pixel size, kernel cap and plane thickness must be > 0");
    const uint64_t up = upscale < 1 ? 1u : static_cast<uint64_t>(upscale);
@@ -1845,6 +1845,10 @@ int iscu_wf_job_images(iscu_wf_job* job, const iscu_wf_job_desc* d, float* const
          if (rc != ISCU_OK)
             return rc;
          job->plan = std::move(p);
+         // the slots were sized for the old transform's spectra
+         job->planes.Free();
+         job->kernels.Free();
+         job->planeCap = job->kernelCap = 0;
       }
       job->planeKeys.clear();
       job->kernelPs.clear();

@@ -827,6 +827,66 @@ class WidefieldPlan:
         self._pending_io.pop(int(io_slot), None)
 
 
+class WidefieldJob:
+    """iscu_wf_job: the GPU side of a widefield scene's focus work (sim::WidefieldAccelerator) -- plane spectra
+    resident by key, kernel spectra by plane index, within one geometry value."""
+
+    def __init__(self, engine: Engine, budget_bytes=0):
+        self.engine = engine
+        self.lib = engine.lib
+        h = C.c_void_p()
+        check(self.lib.iscu_wf_job_create(engine.h, int(budget_bytes), C.byref(h)))
+        self.h = h
+        engine._plans.add(self)
+
+    def close(self):
+        if self.h:
+            if self.engine.h:
+                self.lib.iscu_wf_job_destroy(self.h)
+            self.h = None
+
+    def has_plane(self, geometry, key):
+        return self.lib.iscu_wf_job_has_plane(self.h, int(geometry), int(key)) == 1
+
+    def fits(self, geometry, nx_fft, ny_fft, planes):
+        return self.lib.iscu_wf_job_fits(self.h, int(geometry), nx_fft, ny_fft, int(planes)) == 1
+
+    def images(self, nx_fft, ny_fft, grid, fov, frac, geometry, kernels, planes, channels):
+        """kernels: {p: complex64 (ny_fft, nx_fft/2 + 1) spectrum, RealFft2d's = numpy rfft2's layout}; planes: {key:
+        (cells uint32, values float32)} (cells row-major in the nx x ny grid); channels: lists of deps (key, p0, p1,
+        w0, w1) with p1 None for one kernel. Returns (n_channels, ch, cw) float32 images."""
+        from ._abi import WfJobDep, WfJobDesc, WfJobKernel, WfJobPlane
+        nx, ny = grid
+        x0, y0, cw, ch = fov
+        keep = []
+        ks = (WfJobKernel * max(1, len(kernels)))()
+        for i, (p, spec) in enumerate(kernels.items()):
+            a = np.ascontiguousarray(spec, np.complex64)
+            keep.append(a)
+            ks[i].p, ks[i].spec = int(p), a.ctypes.data
+        ps = (WfJobPlane * max(1, len(planes)))()
+        for i, (key, (cells, values)) in enumerate(planes.items()):
+            c_ = np.ascontiguousarray(cells, np.uint32)
+            v_ = np.ascontiguousarray(values, np.float32)
+            keep += [c_, v_]
+            ps[i].key, ps[i].cells, ps[i].values, ps[i].count = int(key), c_.ctypes.data, v_.ctypes.data, len(c_)
+        flat = [d for ch_ in channels for d in ch_]
+        ds = (WfJobDep * max(1, len(flat)))()
+        for i, (key, p0, p1, w0, w1) in enumerate(flat):
+            ds[i].key, ds[i].p0, ds[i].w0 = int(key), int(p0), float(w0)
+            two = p1 is not None
+            ds[i].p1, ds[i].w1, ds[i].two = (int(p1) if two else int(p0)), (float(w1) if two else 0.0), int(two)
+        start = np.concatenate([[0], np.cumsum([len(c_) for c_ in channels])]).astype(np.uint32)
+        d = WfJobDesc(nx_fft=nx_fft, ny_fft=ny_fft, nx=nx, ny=ny, fov_x0=x0, fov_y0=y0, cw=cw, ch=ch,
+                      frac_x=float(frac[0]), frac_y=float(frac[1]), geometry=int(geometry), kernels=C.cast(ks, C.c_void_p),
+                      n_kernels=len(kernels), n_planes=len(planes), planes=C.cast(ps, C.c_void_p),
+                      deps=C.cast(ds, C.c_void_p), channel_start=start.ctypes.data, n_channels=len(channels))
+        out = np.zeros((len(channels), ch, cw), np.float32)
+        ptrs = (C.c_void_p * max(1, len(channels)))(*[out[c].ctypes.data for c in range(len(channels))])
+        check(self.lib.iscu_wf_job_images(self.h, C.byref(d), ptrs))
+        return out
+
+
 class WidefieldShift:
     """iscu_wf_shift: frames of a drifting widefield sample from its channels' spectra on an nx x ny grid
     (RenderShiftedImages)."""

@@ -35,13 +35,18 @@ void Report(const std::string& name, bool ok, const std::string& detail)
       ++failures;
 }
 
+// max |a - b| / max |b|; infinite when a holds a NaN or the sizes differ.
 double MaxRel(const std::vector<float>& a, const std::vector<float>& b)
 {
+   if (a.size() != b.size())
+      return HUGE_VAL;
    double m = 0.0, d = 0.0;
-   for (size_t i = 0; i < a.size() && i < b.size(); ++i)
+   for (size_t i = 0; i < a.size(); ++i)
    {
+      const double e = std::fabs(static_cast<double>(a[i]) - b[i]);
+      if (!(e <= d))
+         d = std::isnan(e) ? HUGE_VAL : e;
       m = std::max(m, std::fabs(static_cast<double>(b[i])));
-      d = std::max(d, std::fabs(static_cast<double>(a[i]) - b[i]));
    }
    return m > 0.0 ? d / m : d;
 }
@@ -184,18 +189,26 @@ void Accel(iscu_sim::WidefieldAcceleratorCuda& accel, const SceneCase& c)
       return;
    }
    const bool used = gpu.UsingAccelerator() && gpu.GpuError().empty();
-   double e1 = 0.0, e2 = 0.0;
+   const size_t cells = static_cast<size_t>(c.W) * c.upscale * c.H * c.upscale;
+   double e1 = 0.0, e2 = 0.0, wantMax = 0.0, gotMax = 0.0;
+   bool sizes = true;
    for (size_t f = 0; f < foci.size(); ++f)
    {
+      sizes = sizes && want[f].persistent.size() == cells && got[f].persistent.size() == cells &&
+              again[f].persistent.size() == cells;
       e1 = std::max(e1, MaxRel(got[f].persistent, want[f].persistent));
       e2 = std::max(e2, MaxRel(again[f].persistent, want[f].persistent));
+      for (float v : want[f].persistent)
+         wantMax = std::max(wantMax, std::fabs(static_cast<double>(v)));
+      for (float v : got[f].persistent)
+         gotMax = std::max(gotMax, std::fabs(static_cast<double>(v)));
    }
-   char buf[200];
-   std::snprintf(buf, sizeof(buf), "accelerated=%d rel=%.3e resident_rel=%.3e foci=%zu fft=%ux%u cells=%ux%u",
-                 used ? 1 : 0, e1, e2, foci.size(), cpu.FftSizeX(), cpu.FftSizeY(), g.nx, g.ny);
-   Report("accel_" + c.name, used && e1 <= 1e-5 && e2 <= 1e-5 && want[0].persistent.size() == c.W * c.upscale *
-                                                                                             c.H * c.upscale,
-          buf);
+   char buf[260];
+   std::snprintf(buf, sizeof(buf), "accelerated=%d sizes=%d rel=%.3e resident_rel=%.3e want_max=%.4g got_max=%.4g "
+                 "foci=%zu fft=%ux%u cells=%ux%u",
+                 used ? 1 : 0, sizes ? 1 : 0, e1, e2, wantMax, gotMax, foci.size(), cpu.FftSizeX(), cpu.FftSizeY(),
+                 g.nx, g.ny);
+   Report("accel_" + c.name, used && sizes && wantMax > 0.0 && e1 <= 1e-5 && e2 <= 1e-5, buf);
 }
 
 } // namespace

@@ -138,8 +138,8 @@ def test_large_pupil_psf_vs_oracle(engine, oracle):
         assert np.abs(got[i] - want[i]).max() <= TOL * want[i].max(), i
 
 
-@pytest.mark.parametrize("vol_shape,psf_shape,grid", [((24, 200, 160), (12, 100, 120), (512, 512, 64)),
-                                                      ((130, 20, 24), (127, 9, 11), (64, 32, 256))])
+@pytest.mark.parametrize("vol_shape,psf_shape,grid", [((40, 400, 400), (24, 200, 200), (512, 512, 64)),
+                                                      ((130, 20, 40), (127, 9, 11), (64, 32, 256))])
 def test_codelet_lengths_vs_oracle(engine, vol_shape, psf_shape, grid):
     """Grids whose transform lengths run the compiled-in codelets other than the full-size ones (x half length 256,
     y 512, z 64; z 256) against the float64 oracle."""

@@ -68,7 +68,8 @@ def test_noalloc_rejects_sizes_beyond_its_array(engine):
 def test_noalloc_checks_its_output_and_shared_memory(engine):
     """An output too small, of the wrong type or on the host is refused before the call; a pupil and plane whose
     chirp-Z does not fit one CTA's shared memory (M = 128, P = 100) is refused with ISCU_ERR_LIMIT before any copy
-    or launch; the largest plane that fits at M = 128 (P = 99) equals the allocating entry point."""
+    or launch; the largest plane that fits at M = 128 beside the kernel's static shared memory (P = 98) equals the
+    allocating entry point."""
     import torch
     rng = np.random.default_rng(5)
     sets = _sets(rng, (600.0,))
@@ -82,9 +83,9 @@ def test_noalloc_checks_its_output_and_shared_memory(engine):
         engine.psf_library_noalloc_dev(sets, [0, 0], [0.0, 100.0], out, size=100)
     assert e.value.code == _abi.ISCU_ERR_LIMIT and "shared memory" in str(e.value)
     dz = rng.uniform(-500.0, 500.0, 3)
-    want = engine.psf_library_dev(sets, [0, 0, 0], dz, size=99, normalize=True, method=CZT_FP32)
-    out = torch.full((3, 99, 99), float("nan"), dtype=torch.float32, device="cuda")
-    got = engine.psf_library_noalloc_dev(sets, [0, 0, 0], dz, out, size=99, normalize=True)
+    want = engine.psf_library_dev(sets, [0, 0, 0], dz, size=98, normalize=True, method=CZT_FP32)
+    out = torch.full((3, 98, 98), float("nan"), dtype=torch.float32, device="cuda")
+    got = engine.psf_library_noalloc_dev(sets, [0, 0, 0], dz, out, size=98, normalize=True)
     torch.cuda.synchronize()
     g, w = got.cpu().numpy(), want.cpu().numpy()
     assert np.isfinite(g).all() and _max_rel(g, w) <= TOL
