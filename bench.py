@@ -101,12 +101,12 @@ def measured_peaks():
 # DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the dominant kernels, from one ncu
 # capture each; the summaries with their commands are the named files.
 NCU_TRAFFIC = {
-    ("smlm", "GatherTilesKernel"): (139518208, "profiles/GatherTilesKernel_smlm_dstorm.md"),
-    ("smlm", "ContribKernel"): (93568768, "profiles/ContribKernel_smlm_dstorm.md"),
+    ("smlm", "GatherTilesKernel"): (138334464, "profiles/GatherTilesKernel_smlm_dstorm.md"),
+    ("smlm", "ContribKernel"): (96654336, "profiles/ContribKernel_smlm_dstorm.md"),
     ("psflib", "CztTf32x3Kernel"): (52487168, "profiles/CztTf32x3Kernel_psf_library.md"),
     ("two-colour", "GatherTilesKernel"): (2182043649, "profiles/GatherTilesKernel_two_colour.md"),
-    ("widefield", "WfNoiseKernel"): (73977088, "profiles/widefield_cells_launches.md"),
-    ("widefield", "ZKernel<convolve>"): (1045289728, "profiles/widefield_cells_launches.md"),
+    ("widefield", "WfNoiseKernel"): (73900000, "profiles/widefield_cells_launches.md"),
+    ("widefield", "ZKernel<convolve>"): (1046200000, "profiles/widefield_cells_launches.md"),
     ("wfshift", "ShiftColumnsKernel+ShiftRowsKernel"): (636056576, "profiles/shift_frames_launches.md"),
 }
 

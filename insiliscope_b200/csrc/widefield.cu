@@ -1765,7 +1765,8 @@ int iscu_wf_plan_from_kernel(iscu_ctx* ctx, int32_t slot, int32_t upscale, doubl
    rc = MakePlan(ctx, nx, ny, nz, dVol.as<float>(), true, D, D, kz, p);
    if (rc != ISCU_OK)
       return rc;
-   p->camera = true;
+   // a window that is the whole grid at one cell per pixel needs no binning pass: the frames are the grid's cells
+   p->camera = !(fov_x0 == 0 && fov_y0 == 0 && fov_w == nx && fov_h == ny && up == 1);
    p->fovX0 = fov_x0;
    p->fovY0 = fov_y0;
    p->fovW = fov_w;
