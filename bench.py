@@ -592,13 +592,14 @@ class WidefieldWorkload:
 
 class PsfLibraryWorkload:
     """The batched PSF library: 4,096 PSFs (64 z x 4 wavelengths x 16 Noll 4-15 aberration sets), each a 128 x 128
-    pupil (float64 OPD/chirp phases) chirp-Z'd to 64 x 64 as two complex products on the tensor cores (TF32 x 3,
-    float32 accumulation in TMEM), |E|^2, sum-1 planes. One step = the whole library. The plain FP32 GPU form (SIMT
-    complex products in shared memory) is timed beside it."""
+    pupil (float64 OPD/chirp phases) chirp-Z'd to 64 x 64 as two complex products on the tensor cores (FP16 x 3 split
+    operands, float32 accumulation in TMEM, the DFT operand resident in shared memory per request set), |E|^2, sum-1
+    planes. One step = the whole library. The TF32 x 3 tensor-core form and the plain FP32 GPU form (SIMT complex
+    products in shared memory) are timed beside it."""
     name = ("psf library 4096 x (128^2 pupil -> 64^2, NA 1.45, 520/580/670/750 nm, Noll 4-15 ~ N(0, 0.05 wave rms), "
-            "64 z at 25 nm), chirp-Z as TF32x3 tcgen05 GEMMs")
+            "64 z at 25 nm), chirp-Z as FP16x3 tcgen05 GEMMs")
     metric = "PSFs/s"
-    dtype = "tf32x3"
+    dtype = "f16x3"
     roofline_kind = "tensor"
     cpu_kind = "reference"
     frames_per_step_cpu = 130
@@ -614,13 +615,14 @@ class PsfLibraryWorkload:
 
     def setup(self, device: int):
         import torch
-        from insiliscope_b200 import CZT_FP32, CZT_TF32X3, Engine, PsfPlan
+        from insiliscope_b200 import CZT_F16X3, CZT_FP32, CZT_TF32X3, Engine, PsfPlan
         L = self.lib
         self.eng = eng = Engine(device)
         t0 = time.perf_counter()
-        self.plan = PsfPlan(eng, L.sets, size=L.size, method=CZT_TF32X3)
+        self.plan = PsfPlan(eng, L.sets, size=L.size, method=CZT_F16X3)
         self.psf_build_ms = (time.perf_counter() - t0) * 1e3
         self.plan32 = PsfPlan(eng, L.sets, size=L.size, method=CZT_FP32)
+        self.plan_tf32 = PsfPlan(eng, L.sets, size=L.size, method=CZT_TF32X3)
         n = len(L.set_of_psf)
         dev = f"cuda:{device}"
         self.d_set = torch.from_numpy(L.set_of_psf.view(np.int32)).to(dev)
@@ -665,16 +667,17 @@ class PsfLibraryWorkload:
     def dominant(self):
         self.plan.check()
         ms = self.time_plan(self.plan)
-        return "CztTf32x3Kernel", self.flops_per_launch(), ms, {"tf32x3_ms": round(ms, 4)}
+        return "CztF16x3Kernel", self.flops_per_launch(), ms, {"f16x3_ms": round(ms, 4)}
 
     def plain_form(self, step_ms):
         """The precision pattern against the plain FP32 form on this GPU: the same library through the SIMT float32
         chirp-Z (both products in shared memory, FP32 FMA)."""
-        tc, fp32 = self.time_plan(self.plan), self.time_plan(self.plan32)
-        return {"tf32x3_ms": round(tc, 4), "plain_fp32_ms": round(fp32, 4), "speedup_vs_plain": round(fp32 / tc, 3)}
+        tc, tf32, fp32 = self.time_plan(self.plan), self.time_plan(self.plan_tf32), self.time_plan(self.plan32)
+        return {"f16x3_ms": round(tc, 4), "tf32x3_ms": round(tf32, 4), "plain_fp32_ms": round(fp32, 4),
+                "speedup_vs_plain": round(fp32 / tc, 3), "speedup_vs_tf32x3": round(tf32 / tc, 3)}
 
     def accuracy(self):
-        """Every PSF of the library (the device's TF32 x 3 planes) against the float64 oracle: per PSF
+        """Every PSF of the library (the device's FP16 x 3 planes) against the float64 oracle: per PSF
         max |I - I64| / max I64 and ||I - I64|| / ||I64||, worst and median over the 4,096."""
         from concurrent.futures import ThreadPoolExecutor
         from oracle.oracle import Oracle
@@ -702,7 +705,7 @@ class PsfLibraryWorkload:
         return self.frames_per_step * self.lib.size ** 2 * 4
 
     def kernel_name(self):
-        return "CztTf32x3Kernel"
+        return "CztF16x3Kernel"
 
     # -------------------------------------------------- the reference's CPU PSF on the host cores
     def cpu_cores(self):
@@ -1664,8 +1667,8 @@ def measure_ours(w, args, world, rank, local, steps, warmup, cpu=True):
                          ("alg_flops_per_launch" if tensor else "alg_bytes_per_launch"): kbytes, "launch_ms": kms},
             "gpu_launches": launches, "clocks": clk.summary()}
     if breakdown and tensor:
-        line["roofline"]["peak_note"] = ("measured dense bf16 cuBLAS peak; the kernel issues TF32 MMAs (nominal TF32 "
-                                         "dense rate is half of bf16) and 3 of them per product (hi*hi, hi*lo, lo*hi)")
+        line["roofline"]["peak_note"] = ("measured dense bf16 cuBLAS peak; the kernel issues FP16 MMAs (the bf16 "
+                                         "rate) and 3 of them per product (hi*hi, hi*lo, lo*hi)")
         line["roofline"]["issued_tflops"] = 3 * achieved
     elif breakdown:
         line["roofline"]["pass_ms"] = breakdown.get("pass_ms", breakdown)

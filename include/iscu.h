@@ -48,8 +48,10 @@ enum iscu_interp { ISCU_INTERP_NEAREST = 0, ISCU_INTERP_LINEAR = 1, ISCU_INTERP_
 /* Which chirp-Z product a PSF build uses. */
 enum iscu_czt_method {
    ISCU_CZT_FP32 = 0,   /* the plain FP32 form: SIMT complex matmuls in shared memory */
-   ISCU_CZT_TF32X3 = 1  /* split precision on the tensor cores: hi/lo TF32 operands, three tcgen05 MMAs per product,
+   ISCU_CZT_TF32X3 = 1, /* split precision on the tensor cores: hi/lo TF32 operands, three tcgen05 MMAs per product,
                            FP32 accumulation in tensor memory */
+   ISCU_CZT_F16X3 = 2   /* the same with hi/lo FP16 operands (exact power-of-two scales keep them in range): twice
+                           the inputs per MMA, the DFT operand resident in shared memory per request set */
 };
 
 typedef struct iscu_ctx iscu_ctx;
@@ -155,10 +157,10 @@ int iscu_psf_library_dev(iscu_ctx* ctx, const iscu_psf_request* sets, uint32_t n
                          float* out_dev);
 
 /* A PSF library plan: the per-set work of ComputeZernikePsfPlanes (pupil tables, DFT matrices, and for
- * ISCU_CZT_TF32X3 the split stacked operand) done once for `sets` at plane size `size` (0: the first request's), then
- * runs of any number of PSFs (set index + defocus each). The memo of ComputePsfKernelCache
- * (PsfGeneratorBridge.h:317-364) keeps kernel stacks the same way. ISCU_CZT_TF32X3 needs M <= 128 (a multiple of 16)
- * and planes of at most 64 x 64. */
+ * the split methods the split stacked operand) done once for `sets` at plane size `size` (0: the first request's),
+ * then runs of any number of PSFs (set index + defocus each). The memo of ComputePsfKernelCache
+ * (PsfGeneratorBridge.h:317-364) keeps kernel stacks the same way. ISCU_CZT_TF32X3 and ISCU_CZT_F16X3 need M <= 128
+ * (a multiple of 16) and planes of at most 64 x 64. */
 typedef struct iscu_psf_plan iscu_psf_plan;
 int iscu_psf_plan_create(iscu_ctx* ctx, const iscu_psf_request* sets, uint32_t n_sets, int32_t size, int32_t method,
                          iscu_psf_plan** out);

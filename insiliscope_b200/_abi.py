@@ -20,7 +20,7 @@ ISCU_ERR_NODEV = 6
 ISCU_ERR_IO = 7
 
 INTERP_NEAREST, INTERP_LINEAR, INTERP_CUBIC = 0, 1, 2
-CZT_FP32, CZT_TF32X3 = 0, 1
+CZT_FP32, CZT_TF32X3, CZT_F16X3 = 0, 1, 2
 MAX_KERNELS = 4
 
 u8p = C.POINTER(C.c_uint8)

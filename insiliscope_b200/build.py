@@ -30,6 +30,7 @@ UNITS = {
     "nll.cu": [],
     "psf.cu": [],
     "psf_tc.cu": [],
+    "psf_tc16.cu": [],
     "psf_noalloc.cu": [],
     "psf_plan.cu": [],
     "widefield.cu": ["--fmad=false"],

@@ -342,7 +342,7 @@ int iscu_psf_library_dev(iscu_ctx* ctx, const iscu_psf_request* sets, uint32_t n
 {
    if (!ctx || (n_psf && (!sets || !set_of_psf || !defocus_nm || !out_dev)))
       return Fail(ISCU_ERR_ARG, "null argument");
-   if (method != ISCU_CZT_FP32 && method != ISCU_CZT_TF32X3)
+   if (method != ISCU_CZT_FP32 && method != ISCU_CZT_TF32X3 && method != ISCU_CZT_F16X3)
       return Fail(ISCU_ERR_ARG, "unknown chirp-Z method");
    if (size < 0 || size > 1024)
       return Fail(ISCU_ERR_ARG, "plane size out of range (0..1024)");

@@ -522,10 +522,10 @@ int BuildPsfLibrary(iscu_ctx* ctx, const iscu_psf_request* sets, uint32_t nSets,
    DftMatrixKernel<<<dim3((P * M + 255) / 256, nSets), 256, 0, ctx->stream>>>(dSets.as<SetParams>(), M, P,
                                                                               dA.as<float2>(), dAt.as<float2>());
    ISCU_CK_LAUNCH(ctx, "DftMatrixKernel");
-   if (method == ISCU_CZT_TF32X3)
+   if (method == ISCU_CZT_TF32X3 || method == ISCU_CZT_F16X3)
    {
-      const int rc = LaunchCztTf32x3(ctx, dSets.as<SetParams>(), dTab.as<double3>(), dA.as<float2>(), nSets,
-                                     dItems.as<PsfItem>(), nPsf, M, P, normalize, out);
+      const int rc = LaunchCztSplit(ctx, method, dSets.as<SetParams>(), dTab.as<double3>(), dA.as<float2>(), nSets,
+                                    dItems.as<PsfItem>(), nPsf, M, P, normalize, out);
       if (rc != ISCU_OK)
          return rc;
    }

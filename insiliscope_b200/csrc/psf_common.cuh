@@ -1,4 +1,5 @@
-// Shared by the PSF kernels (psf.cu: plain FP32 form; psf_tc.cu: tensor-core TF32 split form).
+// Shared by the PSF kernels (psf.cu: plain FP32 form; psf_tc.cu and psf_tc16.cu: the tensor-core TF32 and FP16
+// split forms).
 #pragma once
 
 #include "iscu_internal.h"
@@ -64,15 +65,23 @@ __device__ __forceinline__ double BlockSumDouble(double v, double* red)
    return t;
 }
 
-int LaunchCztTf32x3(iscu_ctx* ctx, const SetParams* sets, const double3* tables, const float2* A, uint32_t nSets,
-                    const PsfItem* items, uint32_t nPsf, int M, int P, int normalize, float* out);
+// The split-precision chirp-Z (method ISCU_CZT_TF32X3 or ISCU_CZT_F16X3) for one library: builds the method's
+// per-set data, runs, waits and reports a tensor-core wait that ran out.
+int LaunchCztSplit(iscu_ctx* ctx, int method, const SetParams* sets, const double3* tables, const float2* A,
+                   uint32_t nSets, const PsfItem* items, uint32_t nPsf, int M, int P, int normalize, float* out);
 bool Tf32x3Supports(int M, int P);
-// The split-precision kernel's per-set data (the DFT operand's K-block images and the pupil phase tables) in one
-// buffer.
+bool F16x3Supports(int M, int P);
+// The split-precision kernels' per-set data in one buffer: the DFT operand's K-block images in the method's layout
+// (SplitImageBytes), then the pupil phase tables.
 int BuildAhat(iscu_ctx* ctx, const float2* A, const SetParams* sets, const double3* tables, int nSets, int M, int P,
-              DevBuf& ahat);
+              int method, DevBuf& ahat);
+size_t SplitImageBytes(int method, int nSets);
+size_t AhatF16Bytes(int nSets);
+int BuildAhatF16Images(iscu_ctx* ctx, const float2* A, int nSets, int M, int P, unsigned char* out);
 int LaunchCztTf32x3Core(iscu_ctx* ctx, const SetParams* sets, const float* ahat, int nSets, const PsfItem* items,
                         uint32_t nPsf, int M, int P, int normalize, float* out, int* dErr);
+int LaunchCztF16x3Core(iscu_ctx* ctx, const SetParams* sets, const unsigned char* ahat, int nSets,
+                       const PsfItem* items, uint32_t nPsf, int M, int P, int normalize, float* out, int* dErr);
 
 int LaunchPsfTables(iscu_ctx* ctx, const SetParams* dSets, uint32_t nSets, int M, int P, double3* dTab, float2* dA,
                     float2* dAt);

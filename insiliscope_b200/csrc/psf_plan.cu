@@ -52,6 +52,9 @@ int RunDev(iscu_psf_plan* p, const uint32_t* setOf, const double* defocusNm, uin
    PlanItemsKernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(p->sets.as<SetParams>(), setOf, defocusNm, n, p->nSets,
                                                              p->items.as<PsfItem>(), p->err.as<int>());
    ISCU_CK_LAUNCH(ctx, "PlanItemsKernel");
+   if (p->method == ISCU_CZT_F16X3)
+      return LaunchCztF16x3Core(ctx, p->sets.as<SetParams>(), p->ahat.as<unsigned char>(), static_cast<int>(p->nSets),
+                                p->items.as<PsfItem>(), n, p->M, p->P, normalize, out, p->err.as<int>());
    if (p->method == ISCU_CZT_TF32X3)
       return LaunchCztTf32x3Core(ctx, p->sets.as<SetParams>(), p->ahat.as<float>(), static_cast<int>(p->nSets),
                                  p->items.as<PsfItem>(), n, p->M, p->P, normalize, out, p->err.as<int>());
@@ -84,7 +87,7 @@ int iscu_psf_plan_create(iscu_ctx* ctx, const iscu_psf_request* sets, uint32_t n
    if (!ctx || !sets || !out || n_sets == 0)
       return Fail(ISCU_ERR_ARG, "null argument or no sets");
    *out = nullptr;
-   if (method != ISCU_CZT_FP32 && method != ISCU_CZT_TF32X3)
+   if (method != ISCU_CZT_FP32 && method != ISCU_CZT_TF32X3 && method != ISCU_CZT_F16X3)
       return Fail(ISCU_ERR_ARG, "unknown chirp-Z method");
    if (size < 0 || size > 1024)
       return Fail(ISCU_ERR_ARG, "plane size out of range (0..1024)");
@@ -98,9 +101,11 @@ int iscu_psf_plan_create(iscu_ctx* ctx, const iscu_psf_request* sets, uint32_t n
    int rc = PrepareSetParams(sets, n_sets, size, n_sets, hs.data(), &p->M, &p->P);
    if (rc != ISCU_OK)
       return rc;
-   if (method == ISCU_CZT_TF32X3 && !Tf32x3Supports(p->M, p->P))
-      return Fail(ISCU_ERR_ARG, "tf32x3 chirp-Z: needs pupil samples M <= 128 (a multiple of 16) and planes of at "
-                                "most 64 x 64");
+   if ((method == ISCU_CZT_TF32X3 && !Tf32x3Supports(p->M, p->P)) ||
+       (method == ISCU_CZT_F16X3 && !F16x3Supports(p->M, p->P)))
+      return Fail(ISCU_ERR_ARG, std::string(method == ISCU_CZT_F16X3 ? "f16x3" : "tf32x3") +
+                                   " chirp-Z: needs pupil samples M <= 128 (a multiple of 16) and planes of at most "
+                                   "64 x 64");
    const size_t M = p->M, P = p->P;
    ISCU_CK(p->sets.Reserve(n_sets * sizeof(SetParams)));
    ISCU_CK(p->tab.Reserve(n_sets * M * M * sizeof(double3)));
@@ -112,9 +117,9 @@ int iscu_psf_plan_create(iscu_ctx* ctx, const iscu_psf_request* sets, uint32_t n
                         p->At.as<float2>());
    if (rc != ISCU_OK)
       return rc;
-   if (method == ISCU_CZT_TF32X3 &&
+   if (method != ISCU_CZT_FP32 &&
        (rc = BuildAhat(ctx, p->A.as<float2>(), p->sets.as<SetParams>(), p->tab.as<double3>(),
-                       static_cast<int>(n_sets), p->M, p->P, p->ahat)) != ISCU_OK)
+                       static_cast<int>(n_sets), p->M, p->P, method, p->ahat)) != ISCU_OK)
       return rc;
    ISCU_CK(cudaStreamSynchronize(ctx->stream));
    *out = p.release();

@@ -24,6 +24,7 @@
 
 #include "iscu_internal.h"
 #include "psf_common.cuh"
+#include "tcgen05.cuh"
 
 #include <algorithm>
 #include <vector>
@@ -32,15 +33,13 @@ namespace iscu {
 
 namespace {
 
+using namespace tc;
+
 constexpr int kThreads = 512;
 constexpr int kRows = 128;             // UMMA M (2P rows, padded)
 constexpr int kBlockBytes = 128 * 128; // one operand K block: 128 rows x 32 TF32 (128 B per row)
 
 // ------------------------------------------------------------------------------------------ PTX helpers
-__device__ __forceinline__ uint32_t SmemAddr(const void* p)
-{
-   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
 
 // TF32 rounding (to nearest, ties away from zero: cvt.rna.tf32.f32) on the integer pipe: adding half a TF32 unit in
 // the last place to the magnitude bits and clearing the 13 bits TF32 drops rounds the magnitude half away from zero,
@@ -58,27 +57,6 @@ __device__ __forceinline__ void Split(float x, float& hi, float& lo)
    lo = x - hi;
 }
 
-__device__ __forceinline__ void MbarInit(uint64_t* bar, uint32_t count)
-{
-   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(SmemAddr(bar)), "r"(count));
-}
-
-__device__ __forceinline__ void FenceProxyAsync() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void TcFenceBefore() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void TcFenceAfter() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-// Shared-memory matrix descriptor: canonical K-major, 128-byte swizzle, 8-row groups 1024 bytes apart.
-__device__ __forceinline__ uint64_t SmemDesc(uint32_t addr)
-{
-   uint64_t d = 0;
-   d |= static_cast<uint64_t>((addr >> 4) & 0x3FFFu);          // start address
-   d |= static_cast<uint64_t>(1u) << 16;                       // leading byte offset (unused for this layout)
-   d |= static_cast<uint64_t>(1024u >> 4) << 32;               // stride byte offset: 8-row group pitch
-   d |= static_cast<uint64_t>(1u) << 46;                       // descriptor version (sm_100)
-   d |= static_cast<uint64_t>(2u) << 61;                       // layout: 128-byte swizzle
-   return d;
-}
-
 // Instruction descriptor, kind::tf32: D float32, A and B TF32, both K-major, M x N.
 __host__ __device__ constexpr uint32_t InstrDesc(int M, int N)
 {
@@ -91,31 +69,6 @@ __device__ __forceinline__ void Mma(uint32_t dTmem, uint64_t aDesc, uint64_t bDe
    asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
                 " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(dTmem),
                 "l"(aDesc), "l"(bDesc), "r"(idesc), "r"(accum));
-}
-
-__device__ __forceinline__ void Commit(uint64_t* bar)
-{
-   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(SmemAddr(bar))
-                : "memory");
-}
-
-// 32 consecutive TMEM columns of this warp's 32 lanes into v[0..31] (thread = lane).
-__device__ __forceinline__ void TmemLoad32(uint32_t taddr, float* v)
-{
-   uint32_t r[32];
-   asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
-                "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
-                "[%32];"
-                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
-                  "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
-                  "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
-                  "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-                : "r"(taddr));
-   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-   for (int i = 0; i < 32; ++i)
-      v[i] = __uint_as_float(r[i]);
 }
 
 // Byte offset of element (row, col) (col: TF32 index 0..31 within the K block) in a swizzled K block.
@@ -171,53 +124,6 @@ __global__ void PhaseTableKernel(const SetParams* __restrict__ sets, const doubl
                                                     : make_double2(sets[s].k0 * t.x + t.z, t.y);
 }
 
-// The pupil phasor of one sample from the phase table: the float64 phase x = base + a opd3F, reduced mod 2 pi as
-// x - 2 pi n with n = rint(x / 2 pi) (formed by adding and taking away 1.5 2^52, exact for |x / 2 pi| < 2^51) and
-// 2 pi's float64 value (its remaining 2.4e-16 times n is far below float32's resolution for these phases), then the
-// float32 sine and cosine of the reduced phase by the special-function unit (absolute error ~4e-7 over [-pi, pi]).
-// Branch-free, so a thread's samples interleave: outside the aperture (opd3F < 0) the entry (0, -1) gives a finite
-// phase, zeroed at the end.
-__device__ __forceinline__ float2 TablePhasor(double2 t, double a)
-{
-   const double x = fma(a, t.y, t.x);
-   const double kRound = 6755399441055744.0;   // 1.5 2^52
-   const double n = fma(x, 0.15915494309189533577, kRound) - kRound;
-   const float r = static_cast<float>(fma(-n, 6.283185307179586232, x));
-   float sn, cs;
-   __sincosf(r, &sn, &cs);
-   const bool in = t.y >= 0.0;
-   return make_float2(in ? cs : 0.f, in ? sn : 0.f);
-}
-
-// ------------------------------------------------------------------------------------------ async copies
-__device__ __forceinline__ void MbarExpectTx(uint64_t* bar, uint32_t bytes)
-{
-   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(SmemAddr(bar)), "r"(bytes)
-                : "memory");
-}
-
-// A bulk copy global -> this CTA's shared memory (no multicast), completing `bytes` on the mbarrier.
-__device__ __forceinline__ void BulkLoad(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
-{
-   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   SmemAddr(dst)),
-                "l"(src), "r"(bytes), "r"(SmemAddr(bar))
-                : "memory");
-}
-
-// 4 consecutive TMEM columns of this warp's 32 lanes into v[0..3].
-__device__ __forceinline__ void TmemLoad4(uint32_t taddr, float* v)
-{
-   uint32_t r[4];
-   asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
-                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                : "r"(taddr));
-   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-   for (int i = 0; i < 4; ++i)
-      v[i] = __uint_as_float(r[i]);
-}
-
 // ------------------------------------------------------------------------------------------ the fused kernel
 struct TcParams
 {
@@ -249,7 +155,6 @@ constexpr int kItemRounds = (kItemsPerBlock + kProducerThreads - 1) / kProducerT
 __device__ __forceinline__ int ProducerIndex(int warp) { return warp - 5 - (warp >= 9) - (warp >= 13); }
 constexpr int kTmemRow = 0;                        // T of PSF j: columns [128 (j % 2), +128)
 constexpr int kTmemCol = 256;                      // E of PSF j: columns [256 + 64 (j % 2), +64)
-constexpr uint64_t kWaitNs = 4000000000ull;        // a wait gives up after 4 s
 constexpr int kSetCache = 96;                      // PSFs whose set and defocus factor are staged in shared memory
 
 struct Shared
@@ -267,65 +172,6 @@ struct Shared
 };
 constexpr size_t kSmemBytes = static_cast<size_t>(kAStages + kRowStages) * kStageBytes +
                               static_cast<size_t>(kColStages) * kColStageBytes + sizeof(Shared) + 1024;
-
-__device__ __forceinline__ uint64_t GlobalNs()
-{
-   uint64_t t;
-   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-   return t;
-}
-
-// Waits for the phase of the given parity to complete. false after kWaitNs, or (err non-null) once *err is set.
-// backoff: after a few polls the thread sleeps between polls, leaving its scheduler's issue slots to the warps that
-// share it (the MMA thread polls without it: its waits are on the critical path).
-__device__ __forceinline__ bool MbarWait(uint64_t* bar, uint32_t parity, const volatile int* err, bool backoff = true)
-{
-   const uint32_t a = SmemAddr(bar);
-   uint64_t t0 = 0;
-   for (unsigned it = 0;; ++it)
-   {
-      uint32_t done;
-      asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-                   : "=r"(done)
-                   : "r"(a), "r"(parity)
-                   : "memory");
-      if (done)
-         return true;
-      if (backoff && it >= 2)
-         __nanosleep(it < 16 ? 32 : 128);
-      if ((it & 15) == 15)
-      {
-         if (err && *err)
-            return false;
-         const uint64_t now = GlobalNs();
-         if (t0 == 0)
-            t0 = now;
-         else if (now - t0 > kWaitNs)
-            return false;
-      }
-   }
-}
-
-__device__ __forceinline__ void MbarArrive(uint64_t* bar)
-{
-   asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(SmemAddr(bar)) : "memory");
-}
-
-// 16 consecutive TMEM columns of this warp's 32 lanes into v[0..15].
-__device__ __forceinline__ void TmemLoad16(uint32_t taddr, float* v)
-{
-   uint32_t r[16];
-   asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-                "%14, %15}, [%16];"
-                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
-                  "=r"(r[15])
-                : "r"(taddr));
-   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-   for (int i = 0; i < 16; ++i)
-      v[i] = __uint_as_float(r[i]);
-}
 
 // Per CTA, persistent over a contiguous run of PSFs (neighbours in the item list usually share their request set),
 // warp-specialized; the roles meet only at mbarriers:
@@ -745,18 +591,35 @@ size_t AhatBytes(int nSets) { return static_cast<size_t>(nSets) * 8 * kStageByte
 
 static_assert(kSmemBytes <= 227 * 1024, "the chirp-Z kernel's shared memory");
 
-int BuildAhat(iscu_ctx* ctx, const float2* A, const SetParams* sets, const double3* tables, int nSets, int M, int P,
-              DevBuf& ahat)
+size_t SplitImageBytes(int method, int nSets)
 {
-   if (!Tf32x3Supports(M, P))
-      return Fail(ISCU_ERR_ARG, "tf32x3 chirp-Z: needs pupil samples M <= 128 (a multiple of 16) and planes of at "
-                                "most 64 x 64 (else use the fp32 method)");
+   return method == ISCU_CZT_F16X3 ? AhatF16Bytes(nSets) : AhatBytes(nSets);
+}
+
+int BuildAhat(iscu_ctx* ctx, const float2* A, const SetParams* sets, const double3* tables, int nSets, int M, int P,
+              int method, DevBuf& ahat)
+{
+   const bool f16 = method == ISCU_CZT_F16X3;
+   if (f16 ? !F16x3Supports(M, P) : !Tf32x3Supports(M, P))
+      return Fail(ISCU_ERR_ARG, std::string(f16 ? "f16x3" : "tf32x3") +
+                                   " chirp-Z: needs pupil samples M <= 128 (a multiple of 16) and planes of at most "
+                                   "64 x 64 (else use the fp32 method)");
    // the K-block images, then the phase tables
-   ISCU_CK(ahat.Reserve(AhatBytes(nSets) + static_cast<size_t>(nSets) * M * M * sizeof(double2)));
-   AhatKernel<<<dim3((8 * kRows * 32 + 255) / 256, nSets), 256, 0, ctx->stream>>>(A, M, P, ahat.as<float>());
-   ISCU_CK_LAUNCH(ctx, "AhatKernel");
+   const size_t images = SplitImageBytes(method, nSets);
+   ISCU_CK(ahat.Reserve(images + static_cast<size_t>(nSets) * M * M * sizeof(double2)));
+   if (f16)
+   {
+      const int rc = BuildAhatF16Images(ctx, A, nSets, M, P, ahat.as<unsigned char>());
+      if (rc != ISCU_OK)
+         return rc;
+   }
+   else
+   {
+      AhatKernel<<<dim3((8 * kRows * 32 + 255) / 256, nSets), 256, 0, ctx->stream>>>(A, M, P, ahat.as<float>());
+      ISCU_CK_LAUNCH(ctx, "AhatKernel");
+   }
    PhaseTableKernel<<<dim3((M * M + 255) / 256, nSets), 256, 0, ctx->stream>>>(
-      sets, tables, M * M, reinterpret_cast<double2*>(ahat.as<char>() + AhatBytes(nSets)));
+      sets, tables, M * M, reinterpret_cast<double2*>(ahat.as<char>() + images));
    ISCU_CK_LAUNCH(ctx, "PhaseTableKernel");
    return ISCU_OK;
 }
@@ -783,24 +646,27 @@ int LaunchCztTf32x3Core(iscu_ctx* ctx, const SetParams* sets, const float* ahat,
    return ISCU_OK;
 }
 
-int LaunchCztTf32x3(iscu_ctx* ctx, const SetParams* sets, const double3* tables, const float2* A, uint32_t nSets,
-                    const PsfItem* items, uint32_t nPsf, int M, int P, int normalize, float* out)
+int LaunchCztSplit(iscu_ctx* ctx, int method, const SetParams* sets, const double3* tables, const float2* A,
+                   uint32_t nSets, const PsfItem* items, uint32_t nPsf, int M, int P, int normalize, float* out)
 {
    DevBuf dAhat, dErr;
-   int rc = BuildAhat(ctx, A, sets, tables, static_cast<int>(nSets), M, P, dAhat);
+   int rc = BuildAhat(ctx, A, sets, tables, static_cast<int>(nSets), M, P, method, dAhat);
    if (rc != ISCU_OK)
       return rc;
    ISCU_CK(dErr.Reserve(sizeof(int)));
    ISCU_CK(cudaMemsetAsync(dErr.p, 0, sizeof(int), ctx->stream));
-   rc = LaunchCztTf32x3Core(ctx, sets, dAhat.as<float>(), static_cast<int>(nSets), items, nPsf, M, P, normalize, out,
-                            dErr.as<int>());
+   rc = method == ISCU_CZT_F16X3
+           ? LaunchCztF16x3Core(ctx, sets, dAhat.as<unsigned char>(), static_cast<int>(nSets), items, nPsf, M, P,
+                                normalize, out, dErr.as<int>())
+           : LaunchCztTf32x3Core(ctx, sets, dAhat.as<float>(), static_cast<int>(nSets), items, nPsf, M, P, normalize,
+                                 out, dErr.as<int>());
    if (rc != ISCU_OK)
       return rc;
    int err = 0;
    ISCU_CK(cudaMemcpyAsync(&err, dErr.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
    ISCU_CK(cudaStreamSynchronize(ctx->stream));
    if (err)
-      return Fail(ISCU_ERR_TIMEOUT, "tf32x3 chirp-Z: a tensor-core completion wait ran out");
+      return Fail(ISCU_ERR_TIMEOUT, "split-precision chirp-Z: a tensor-core completion wait ran out");
    return ISCU_OK;
 }
 

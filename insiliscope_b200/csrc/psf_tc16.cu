@@ -1,0 +1,607 @@
+// Split-precision chirp-Z on the 5th-generation tensor cores with FP16 operands: the PSF library's two complex
+// products as FP16 x 3 real GEMMs (tcgen05 kind::f16, float32 accumulation in tensor memory), the DFT operand resident
+// in shared memory.
+//
+// The products and the stacked operand are the TF32 x 3 kernel's (psf_tc.cu): row pass T = A U, column pass
+// E^T = A T^T, Ahat = [[Ar, -Ai], [Ai, Ar]], rows interleaved in groups of 16 (row r = 32 g + 16 h + i is output
+// p = 16 g + i, part h) so one warp's 32 TMEM lanes hold 16 outputs' real and imaginary parts. A K block is one row of
+// a 128-byte swizzle atom, 64 FP16: 32 input indices as [16 real, 16 imaginary, 16 real, 16 imaginary] (column c is
+// input q = 32 kb + 16 (c >> 5) + (c & 15), part (c >> 4) & 1). A K step (16 FP16, one MMA) is one of those groups;
+// the steps whose inputs lie at or past M are skipped.
+//
+// FP16 x 3: every operand x is split into hi = fp16(x) and lo = fp16(x - hi), both rounded to nearest (x - hi is
+// exact in float32); a product is hi*hi + hi*lo + lo*hi. With 11-bit significands |x - hi - lo| <= 2^-22 |x| and
+// the dropped lo*lo is <= 2^-22 |a b|, half the TF32 split's error (its lo is truncated to TF32 by the tensor
+// cores). FP16's narrow range is kept by exact power-of-two scales: the DFT operand and the pupil phasors (|x| <= 1)
+// enter times 2^12, so a part falls below FP16's normal range only where it is under 2^-26 of the unit; the row-pass
+// result T (|T| <= M <= 128, accumulated as 2^24 T) is scaled by 2^-16 to 2^8 T (<= 32,768) before its split, and E
+// (2^20 E in TMEM) by 2^-20 before |E|^2.
+//
+// Against the TF32 form: a K step does twice the inputs for the same shared-memory bytes (64.5 cycles per
+// M128 N128 step either way, shared-memory bound at N = 64), so the MMAs take half the time; and the DFT operand
+// (both parts, 2M inputs: 128 KB at M = 128) is loaded once per run of PSFs that share a request set instead of
+// streamed per K block, which takes the two passes out of lockstep. A set change waits until both passes of the
+// previous set are done with the operand.
+
+#include "iscu_internal.h"
+#include "psf_common.cuh"
+#include "tcgen05.cuh"
+
+#include <cuda_fp16.h>
+
+#include <algorithm>
+
+namespace iscu {
+
+namespace {
+
+using namespace tc;
+
+constexpr int kThreads = 512;
+constexpr int kRows = 128;                        // UMMA M (2P rows, padded)
+constexpr int kImgBytes = 128 * 128;              // one operand image: 128 rows x 64 FP16 (128 B per row)
+constexpr int kKbBytes = 2 * kImgBytes;           // a K block: its hi and lo images
+constexpr int kMaxKb = 4;                         // K = 2M <= 256
+constexpr int kABytes = kMaxKb * kKbBytes;        // the resident DFT operand: 128 KB
+constexpr int kRowStages = 2;                     // row-pass B blocks (pupil phasors)
+constexpr int kColStages = 2;                     // column-pass B blocks (T, split)
+constexpr int kColImgBytes = 64 * 128;            // a column-pass B image: 64 rows x 64 FP16
+constexpr int kColStageBytes = 2 * kColImgBytes;
+constexpr float kScaleOp = 4096.0f;               // 2^12: the DFT operand and the pupil phasors
+constexpr float kScaleT = 1.0f / 65536.0f;        // 2^-16: 2^24 T -> 2^8 T
+constexpr float kScaleE = 1.0f / 1048576.0f;      // 2^-20: 2^20 E -> E
+
+// Warp roles. Warps share an SM sub-partition (scheduler) when equal mod 4.
+constexpr int kDrainWarps = 4;                    // warps 0-3, one per TMEM lane quadrant
+constexpr int kRowMmaWarp = 4;                    // lane 0: the DFT operand copies and the row-pass MMAs
+constexpr int kColMmaWarp = 8;                    // lane 0: the column-pass MMAs
+constexpr int kProducerWarps = 10;                // warps 5-7 and 9-15 make the pupil phasors
+constexpr int kProducerThreads = 32 * kProducerWarps;
+constexpr int kItemsPerBlock = 512;               // (pupil column, 8 pupil rows) items of one row-pass K block
+constexpr int kTmemRow = 0;                       // T of PSF j: columns [128 (j % 2), +128)
+constexpr int kTmemCol = 256;                     // E of PSF j: columns [256 + 64 (j % 2), +64)
+constexpr int kSetCache = 96;                     // PSFs whose set and defocus factor are staged in shared memory
+
+static_assert(kItemsPerBlock <= 2 * kProducerThreads, "a producer thread makes at most two items per K block");
+
+// A producer warp's index 0..9 (warps 5-7, 9-15).
+__device__ __forceinline__ int ProducerIndex(int warp) { return warp - 5 - (warp > kColMmaWarp ? 1 : 0); }
+
+// Instruction descriptor, kind::f16: D float32, A and B FP16, both K-major, M x N.
+__host__ __device__ constexpr uint32_t InstrDescF16(int M, int N)
+{
+   return (1u << 4) | (static_cast<uint32_t>(N >> 3) << 17) | (static_cast<uint32_t>(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void MmaF16(uint32_t dTmem, uint64_t aDesc, uint64_t bDesc, uint32_t idesc,
+                                       uint32_t accum)
+{
+   asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(dTmem),
+                "l"(aDesc), "l"(bDesc), "r"(idesc), "r"(accum));
+}
+
+// Byte offset of FP16 element (row, col) (col 0..63 within the K block) in a 128-byte-swizzled image.
+__host__ __device__ __forceinline__ uint32_t SwOff16(int row, int col)
+{
+   return static_cast<uint32_t>((row >> 3) * 1024 + (row & 7) * 128 + ((((col >> 3) ^ (row & 7)) & 7) << 4) +
+                                ((col & 7) << 1));
+}
+
+// (a, b) -> hi = fp16x2(a, b) and lo = fp16x2(a - hi.a, b - hi.b), rounded to nearest; a in the low half.
+__device__ __forceinline__ void SplitH2(float a, float b, uint32_t& hi, uint32_t& lo)
+{
+   const __half2 h = __floats2half2_rn(a, b);
+   const float2 f = __half22float2(h);
+   const __half2 l = __floats2half2_rn(a - f.x, b - f.y);
+   hi = *reinterpret_cast<const uint32_t*>(&h);
+   lo = *reinterpret_cast<const uint32_t*>(&l);
+}
+
+__device__ __forceinline__ void StoreShared16(unsigned char* p, uint32_t a, uint32_t b, uint32_t c, uint32_t d)
+{
+   *reinterpret_cast<uint4*>(p) = make_uint4(a, b, c, d);
+}
+
+// ------------------------------------------------------------------------------------------ the stacked operand
+// Ahat for one set, times 2^12 and split, in K-block order and in the shared-memory image the MMA reads:
+// [kb][hi, lo][16 KB image of 128 rows x 64 FP16]. Rows beyond 2P and inputs at or past M are zero.
+__global__ void AhatF16Kernel(const float2* __restrict__ A, int M, int P, unsigned char* __restrict__ out)
+{
+   const int s = blockIdx.y;
+   const int e = blockIdx.x * blockDim.x + threadIdx.x;   // (kb, row, column pair)
+   if (e >= kMaxKb * kRows * 32)
+      return;
+   const int kb = e / (kRows * 32), row = (e / 32) % kRows, c = 2 * (e % 32);
+   const int p = 16 * (row >> 5) + (row & 15), h = (row >> 4) & 1;
+   float v[2];
+#pragma unroll
+   for (int t = 0; t < 2; ++t)
+   {
+      const int col = c + t, hp = (col >> 4) & 1, q = 32 * kb + 16 * (col >> 5) + (col & 15);
+      v[t] = 0.f;
+      if (p < P && q < M)
+      {
+         const float2 a = A[(static_cast<size_t>(s) * P + p) * M + q];
+         // [[Ar, -Ai], [Ai, Ar]]: output part h, input part hp
+         v[t] = (h == 0 ? (hp == 0 ? a.x : -a.y) : (hp == 0 ? a.y : a.x)) * kScaleOp;
+      }
+   }
+   uint32_t hi, lo;
+   SplitH2(v[0], v[1], hi, lo);
+   unsigned char* base = out + (static_cast<size_t>(s) * kMaxKb + kb) * kKbBytes;
+   *reinterpret_cast<uint32_t*>(base + SwOff16(row, c)) = hi;
+   *reinterpret_cast<uint32_t*>(base + kImgBytes + SwOff16(row, c)) = lo;
+}
+
+// ------------------------------------------------------------------------------------------ the fused kernel
+struct Tc16Params
+{
+   const SetParams* sets;
+   const double2* phase;       // [set][M * M] (base, opd3F)
+   const unsigned char* ahat;  // [set][kMaxKb][hi, lo] images
+   const PsfItem* items;
+   float* out;
+   int* error;
+   int nPsf, M, P, normalize;
+};
+
+struct Shared16
+{
+   uint64_t aFull, aFree;
+   uint64_t rowFull[kRowStages], rowEmpty[kRowStages];
+   uint64_t colFull[kColStages], colEmpty[kColStages];
+   uint64_t rowDone[2], colDone[2], tFree[2], eFree[2], red[2];
+   uint64_t final[2];
+   double sum[2][kDrainWarps];
+   double aDef[kSetCache];   // k0 ni (ti - ti0) of the CTA's j-th PSF, j < kSetCache
+   int set[kSetCache];       // its set
+   uint32_t tmemSlot;
+   int err;
+};
+constexpr size_t kSmemBytes = static_cast<size_t>(kABytes) + static_cast<size_t>(kRowStages) * kKbBytes +
+                              static_cast<size_t>(kColStages) * kColStageBytes + sizeof(Shared16) + 1024;
+static_assert(kSmemBytes <= 227 * 1024, "the FP16 chirp-Z kernel's shared memory");
+
+// Per CTA, persistent over a contiguous run of PSFs, warp-specialized; the roles meet only at mbarriers:
+//   producers (warps 5-7, 9-15): per row-pass K block the pupil phasors of 32 pupil rows (float64 phase reduced mod
+//     2 pi, float32 sine and cosine, times 2^12, FP16 hi/lo split) into a row-B stage -> rowFull; the phase-table
+//     entries of a thread's next item are in flight while it computes the current one;
+//   the row-pass thread (warp 4, lane 0): at the first PSF of each run of one set, once both passes of the previous
+//     set are done with the operand (aFree), the set's DFT operand by bulk copy (aFull); then per PSF its row pass
+//     R(j), K block by K block as the producers fill the stages, into T's TMEM buffer j % 2 (free again when the
+//     drain warps have taken T(j - 2): tFree); commits free the stages and mark the pass done (rowDone);
+//   the column-pass thread (warp 8, lane 0): per PSF its column pass C(j) as the drain warps fill the col-B stages,
+//     into E's TMEM buffer j % 2 (eFree), commits colEmpty / colDone; the last PSF of a set's run commits aFree;
+//   drain warps (0-3, one TMEM lane quadrant each): T of PSF j from TMEM, times 2^-16, split, into col-B stages ->
+//     colFull (then tFree); then E of PSF j: times 2^-20, |E|^2, the plane sum, the normalized plane (eFree).
+// R(j + 1) runs beside C(j) on the tensor pipe. Every wait is bounded (kWaitNs) and also ends when another role has
+// failed (Shared16::err); a failed CTA stops issuing, waits for its copies and MMAs in flight, frees TMEM and reports
+// through prm.error.
+__global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
+{
+   extern __shared__ __align__(1024) unsigned char smemRaw[];
+   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
+   unsigned char* sA = smem;                                  // [kMaxKb] x 32 KB, resident per set
+   unsigned char* sRowB = sA + kABytes;                       // [kRowStages] x 32 KB
+   unsigned char* sColB = sRowB + kRowStages * kKbBytes;      // [kColStages] x 16 KB
+   Shared16* sh = reinterpret_cast<Shared16*>(sColB + kColStages * kColStageBytes);
+   volatile int* err = &sh->err;
+
+   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+   const int M = prm.M, P = prm.P, nKb = (M + 31) / 32;
+   // this CTA's PSFs: psf0 .. psf0 + nLocal - 1
+   const int perCta = prm.nPsf / static_cast<int>(gridDim.x), extra = prm.nPsf % static_cast<int>(gridDim.x);
+   const int cta = static_cast<int>(blockIdx.x);
+   const int psf0 = cta * perCta + min(cta, extra), nLocal = perCta + (cta < extra ? 1 : 0);
+
+   if (warp == 0)
+   {
+      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(SmemAddr(&sh->tmemSlot)),
+                   "r"(512));
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+   }
+   if (tid == 0)
+   {
+      MbarInit(&sh->aFull, 1);
+      MbarInit(&sh->aFree, 2);   // the row-pass and the column-pass threads, once per set run
+      for (int s = 0; s < kRowStages; ++s)
+      {
+         MbarInit(&sh->rowFull[s], kProducerWarps);
+         MbarInit(&sh->rowEmpty[s], 1);
+      }
+      for (int s = 0; s < kColStages; ++s)
+      {
+         MbarInit(&sh->colFull[s], kDrainWarps);
+         MbarInit(&sh->colEmpty[s], 1);
+      }
+      for (int s = 0; s < 2; ++s)
+      {
+         MbarInit(&sh->rowDone[s], 1);
+         MbarInit(&sh->colDone[s], 1);
+         MbarInit(&sh->tFree[s], kDrainWarps);
+         MbarInit(&sh->eFree[s], kDrainWarps);
+         MbarInit(&sh->red[s], kDrainWarps);
+      }
+      MbarInit(&sh->final[0], 1);
+      MbarInit(&sh->final[1], 1);
+      sh->err = 0;
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+   }
+   for (int j = tid; j < nLocal && j < kSetCache; j += kThreads)
+   {
+      const PsfItem it = prm.items[psf0 + j];
+      sh->set[j] = it.set;
+      sh->aDef[j] = prm.sets[it.set].k0 * prm.sets[it.set].ni * it.dtiM;
+   }
+   TcFenceBefore();
+   __syncthreads();
+   TcFenceAfter();
+   const uint32_t tmem = sh->tmemSlot;
+   bool ok = true;
+   auto setOf = [&](int j) { return j < kSetCache ? sh->set[j] : prm.items[psf0 + j].set; };
+   auto firstOfSet = [&](int j) { return j == 0 || setOf(j) != setOf(j - 1); };
+   auto lastOfSet = [&](int j) { return j == nLocal - 1 || setOf(j + 1) != setOf(j); };
+
+   if (warp > kRowMmaWarp && warp != kColMmaWarp)
+   {
+      // ---------------------------------------------------------------- producers: row-pass B blocks
+      // Item r (0, 1) of K block kb: pupil column m = item & 127 and pupil rows n0 .. n0 + 7, n0 = 32 kb + 8 (item >>
+      // 7), item = ptid + r kProducerThreads.
+      const int ptid = 32 * ProducerIndex(warp) + lane;
+      const int nR = ptid + kProducerThreads < kItemsPerBlock ? 2 : 1;
+      auto load = [&](const double2* tab, int kb, int r, double2* dst) {
+         const int item = ptid + r * kProducerThreads, m = item & 127, n0 = 32 * kb + 8 * (item >> 7);
+         const bool in = m < M && n0 < M;
+#pragma unroll
+         for (int c = 0; c < 8; ++c)
+            dst[c] = in ? tab[static_cast<size_t>(n0 + c) * M + m] : make_double2(0.0, -1.0);
+      };
+      // the defocus factor of PSF j (staged in shared memory for j < kSetCache)
+      auto aDefOf = [&](int j) {
+         if (j < kSetCache)
+            return sh->aDef[j];
+         const PsfItem it = prm.items[psf0 + j];
+         return prm.sets[it.set].k0 * prm.sets[it.set].ni * it.dtiM;
+      };
+      auto tabOf = [&](int j) { return prm.phase + static_cast<size_t>(setOf(j)) * M * M; };
+      double2 nxt[8];
+      if (nLocal > 0)
+         load(tabOf(0), 0, 0, nxt);
+      uint32_t rowCount = 0;
+      for (int j = 0; j < nLocal && ok; ++j)
+      {
+         const double aDef = aDefOf(j);
+         const double2* tab = tabOf(j);
+         for (int kb = 0; kb < nKb; ++kb, ++rowCount)
+         {
+            const int rs = static_cast<int>(rowCount % kRowStages);
+            ok = __all_sync(0xffffffffu, MbarWait(&sh->rowEmpty[rs], ((rowCount / kRowStages) & 1u) ^ 1u, err));
+            if (!ok)
+               break;
+            unsigned char* b = sRowB + rs * kKbBytes;
+#pragma unroll
+            for (int r = 0; r < 2; ++r)
+            {
+               if (r >= nR)
+                  break;
+               double2 cur[8];
+#pragma unroll
+               for (int c = 0; c < 8; ++c)
+                  cur[c] = nxt[c];
+               // the next item's table entries while this one computes
+               if (r + 1 < nR)
+                  load(tab, kb, r + 1, nxt);
+               else if (kb + 1 < nKb)
+                  load(tab, kb + 1, 0, nxt);
+               else if (j + 1 < nLocal)
+                  load(tabOf(j + 1), 0, 0, nxt);
+               const int item = ptid + r * kProducerThreads, m = item & 127, l = 8 * (item >> 7);
+               if (m < M && 32 * kb + l < M)   // pupil columns >= M are not read (N = M); K steps >= M are skipped
+               {
+                  uint32_t rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+                  for (int c = 0; c < 4; ++c)
+                  {
+                     const float2 u0 = TablePhasor(cur[2 * c], aDef), u1 = TablePhasor(cur[2 * c + 1], aDef);
+                     SplitH2(u0.x * kScaleOp, u1.x * kScaleOp, rh[c], rl[c]);
+                     SplitH2(u0.y * kScaleOp, u1.y * kScaleOp, ih[c], il[c]);
+                  }
+                  // B[m][c0 + i]: the real part of pupil row n0 + i; B[m][c0 + 16 + i]: the imaginary part
+                  const int c0 = 32 * (l >> 4) + (l & 15);
+                  StoreShared16(b + SwOff16(m, c0), rh[0], rh[1], rh[2], rh[3]);
+                  StoreShared16(b + SwOff16(m, c0 + 16), ih[0], ih[1], ih[2], ih[3]);
+                  StoreShared16(b + kImgBytes + SwOff16(m, c0), rl[0], rl[1], rl[2], rl[3]);
+                  StoreShared16(b + kImgBytes + SwOff16(m, c0 + 16), il[0], il[1], il[2], il[3]);
+               }
+            }
+            FenceProxyAsync();
+            __syncwarp();
+            if (lane == 0)
+               MbarArrive(&sh->rowFull[rs]);
+         }
+      }
+   }
+   else if (warp == kRowMmaWarp)
+   {
+      // ---------------------------------------------------------------- the DFT operand and the row passes
+      if (lane == 0 && nLocal > 0)
+      {
+         const uint32_t idesc = InstrDescF16(kRows, M);
+         uint32_t count = 0, loads = 0;
+         for (int j = 0; j < nLocal && ok; ++j)
+         {
+            if (firstOfSet(j))
+            {
+               if (loads > 0)   // both passes of the previous set are done with the operand
+                  ok = MbarWait(&sh->aFree, (loads - 1) & 1u, err, false);
+               if (!ok)
+                  break;
+               MbarExpectTx(&sh->aFull, static_cast<uint32_t>(nKb * kKbBytes));
+               const unsigned char* src = prm.ahat + static_cast<size_t>(setOf(j)) * kABytes;
+               for (int kb = 0; kb < nKb; ++kb)
+                  BulkLoad(sA + kb * kKbBytes, src + kb * kKbBytes, kKbBytes, &sh->aFull);
+               ++loads;
+               ok = MbarWait(&sh->aFull, (loads - 1) & 1u, err, false);
+               if (!ok)
+                  break;
+            }
+            const uint32_t use = static_cast<uint32_t>(j >> 1) & 1u;
+            ok = MbarWait(&sh->tFree[j & 1], use ^ 1u, err, false);   // T(j - 2) has left the buffer
+            const uint32_t d = tmem + kTmemRow + 128u * static_cast<uint32_t>(j & 1);
+            for (int kb = 0; kb < nKb && ok; ++kb, ++count)
+            {
+               const int rs = static_cast<int>(count % kRowStages);
+               ok = MbarWait(&sh->rowFull[rs], (count / kRowStages) & 1u, err, false);
+               if (!ok)
+                  break;
+               TcFenceAfter();
+               const uint32_t aH = SmemAddr(sA + kb * kKbBytes), aL = aH + kImgBytes;
+               const uint32_t bH = SmemAddr(sRowB + rs * kKbBytes), bL = bH + kImgBytes;
+#pragma unroll
+               for (int kk = 0; kk < 4; ++kk)
+               {
+                  if (32 * kb + 16 * (kk >> 1) >= M)
+                     continue;
+                  const uint32_t off = kk * 32;   // 16 FP16 = 32 bytes along K
+                  MmaF16(d, SmemDesc(aH + off), SmemDesc(bH + off), idesc, (kb == 0 && kk == 0) ? 0u : 1u);
+                  MmaF16(d, SmemDesc(aH + off), SmemDesc(bL + off), idesc, 1u);
+                  MmaF16(d, SmemDesc(aL + off), SmemDesc(bH + off), idesc, 1u);
+               }
+               Commit(&sh->rowEmpty[rs]);
+            }
+            if (!ok)
+               break;
+            Commit(&sh->rowDone[j & 1]);
+            if (lastOfSet(j))
+               Commit(&sh->aFree);
+         }
+         if (!ok)
+         {
+            *err = 1;
+            if (loads > 0)   // the copies in flight land before the CTA frees its memory
+               MbarWait(&sh->aFull, (loads - 1) & 1u, nullptr);
+            Commit(&sh->final[0]);   // this thread's MMAs in flight finish before the CTA frees its TMEM
+            MbarWait(&sh->final[0], 0u, nullptr);
+         }
+      }
+   }
+   else if (warp == kColMmaWarp)
+   {
+      // ---------------------------------------------------------------- the column passes
+      if (lane == 0 && nLocal > 0)
+      {
+         const uint32_t idesc = InstrDescF16(kRows, 64);
+         uint32_t count = 0, runs = 0;
+         for (int j = 0; j < nLocal && ok; ++j)
+         {
+            if (firstOfSet(j))
+            {
+               ok = MbarWait(&sh->aFull, runs & 1u, err, false);   // this set's operand has landed
+               ++runs;
+               if (!ok)
+                  break;
+            }
+            const uint32_t use = static_cast<uint32_t>(j >> 1) & 1u;
+            ok = MbarWait(&sh->eFree[j & 1], use ^ 1u, err, false);   // E(j - 2) has left the buffer
+            const uint32_t d = tmem + kTmemCol + 64u * static_cast<uint32_t>(j & 1);
+            for (int kb = 0; kb < nKb && ok; ++kb, ++count)
+            {
+               const int cs = static_cast<int>(count % kColStages);
+               ok = MbarWait(&sh->colFull[cs], (count / kColStages) & 1u, err, false);
+               if (!ok)
+                  break;
+               TcFenceAfter();
+               const uint32_t aH = SmemAddr(sA + kb * kKbBytes), aL = aH + kImgBytes;
+               const uint32_t bH = SmemAddr(sColB + cs * kColStageBytes), bL = bH + kColImgBytes;
+#pragma unroll
+               for (int kk = 0; kk < 4; ++kk)
+               {
+                  if (32 * kb + 16 * (kk >> 1) >= M)
+                     continue;
+                  const uint32_t off = kk * 32;
+                  MmaF16(d, SmemDesc(aH + off), SmemDesc(bH + off), idesc, (kb == 0 && kk == 0) ? 0u : 1u);
+                  MmaF16(d, SmemDesc(aH + off), SmemDesc(bL + off), idesc, 1u);
+                  MmaF16(d, SmemDesc(aL + off), SmemDesc(bH + off), idesc, 1u);
+               }
+               Commit(&sh->colEmpty[cs]);
+            }
+            if (!ok)
+               break;
+            Commit(&sh->colDone[j & 1]);
+            if (lastOfSet(j))
+               Commit(&sh->aFree);
+         }
+         if (!ok)
+         {
+            *err = 1;
+            Commit(&sh->final[1]);
+            MbarWait(&sh->final[1], 0u, nullptr);
+         }
+      }
+   }
+   else if (warp < kDrainWarps)
+   {
+      // ---------------------------------------------------------------- drain warps
+      // TMEM lane r = 32 w + 16 h + i of T holds row y = 16 w + i, part h (columns: the pupil column m); of E, output
+      // x = 16 w + i, part h (columns: y).
+      const int h = (lane >> 4) & 1, y = 16 * warp + (lane & 15), x = y;
+      const uint32_t quad = static_cast<uint32_t>(32 * warp) << 16;
+      uint32_t colCount = 0;
+      for (int j = 0; j < nLocal && ok; ++j)
+      {
+         const uint32_t use = static_cast<uint32_t>(j >> 1) & 1u;
+         ok = __all_sync(0xffffffffu, MbarWait(&sh->rowDone[j & 1], use, err));
+         if (!ok)
+            break;
+         TcFenceAfter();
+         for (int kb = 0; kb < nKb; ++kb, ++colCount)
+         {
+            const int cs = static_cast<int>(colCount % kColStages);
+            ok = __all_sync(0xffffffffu, MbarWait(&sh->colEmpty[cs], ((colCount / kColStages) & 1u) ^ 1u, err));
+            if (!ok)
+               break;
+            float v[32];
+            TmemLoad32(tmem + quad + kTmemRow + 128u * static_cast<uint32_t>(j & 1) + 32u * kb, v);
+            uint32_t hi[16], lo[16];
+#pragma unroll
+            for (int c = 0; c < 16; ++c)
+               SplitH2(y < P ? v[2 * c] * kScaleT : 0.f, y < P ? v[2 * c + 1] * kScaleT : 0.f, hi[c], lo[c]);
+            // B[y][16 h + i] = part h of T[y][32 kb + i], B[y][32 + 16 h + i] = part h of T[y][32 kb + 16 + i]
+            unsigned char* b = sColB + cs * kColStageBytes;
+#pragma unroll
+            for (int g = 0; g < 4; ++g)
+            {
+               const int col = 32 * (g >> 1) + 16 * h + 8 * (g & 1);
+               StoreShared16(b + SwOff16(y, col), hi[4 * g], hi[4 * g + 1], hi[4 * g + 2], hi[4 * g + 3]);
+               StoreShared16(b + kColImgBytes + SwOff16(y, col), lo[4 * g], lo[4 * g + 1], lo[4 * g + 2],
+                             lo[4 * g + 3]);
+            }
+            FenceProxyAsync();
+            __syncwarp();
+            if (lane == 0)
+               MbarArrive(&sh->colFull[cs]);
+         }
+         if (!ok)
+            break;
+         TcFenceBefore();
+         __syncwarp();
+         if (lane == 0)
+            MbarArrive(&sh->tFree[j & 1]);
+         // ------------------------------------------------ |E|^2, the plane sum, the normalized plane
+         ok = __all_sync(0xffffffffu, MbarWait(&sh->colDone[j & 1], use, err));
+         if (!ok)
+            break;
+         TcFenceAfter();
+         float I[64];
+         float part[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};   // eight float partial sums of 8 values each
+#pragma unroll
+         for (int c0 = 0; c0 < 64; c0 += 32)
+         {
+            float vv[32];
+            TmemLoad32(tmem + quad + kTmemCol + 64u * static_cast<uint32_t>(j & 1) + c0, vv);
+#pragma unroll
+            for (int c = 0; c < 32; ++c)
+            {
+               const float me = vv[c] * kScaleE;
+               const float o = __shfl_xor_sync(0xffffffffu, me, 16);
+               const float e = me * me + o * o;
+               I[c0 + c] = e;
+               if (c0 + c < P)
+                  part[(c0 + c) >> 3] += e;
+            }
+         }
+         double local = 0.0;
+         if (lane < 16 && x < P)
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+               local += static_cast<double>(part[k]);
+         TcFenceBefore();
+         __syncwarp();
+         if (lane == 0)
+            MbarArrive(&sh->eFree[j & 1]);
+         double total = 0.0;
+         if (prm.normalize)
+         {
+            for (int o = 16; o > 0; o >>= 1)
+               local += __shfl_xor_sync(0xffffffffu, local, o);
+            if (lane == 0)
+            {
+               sh->sum[j & 1][warp] = local;
+               MbarArrive(&sh->red[j & 1]);
+            }
+            ok = __all_sync(0xffffffffu, MbarWait(&sh->red[j & 1], use, err));
+            if (!ok)
+               break;
+            const volatile double* s = sh->sum[j & 1];
+            total = s[0] + s[1] + s[2] + s[3];
+         }
+         // lanes 0-15 store rows y < 32 of column x, lanes 16-31 rows y >= 32; the plane times 1 / sum
+         if (x < P)
+         {
+            float* plane = prm.out + static_cast<size_t>(psf0 + j) * P * P;
+            const float scale = (prm.normalize && total > 0.0) ? static_cast<float>(1.0 / total) : 1.0f;
+            const int y0 = 32 * h;
+#pragma unroll
+            for (int c = 0; c < 32; ++c)
+            {
+               const int yy = y0 + c;
+               const float e = h ? I[32 + c] : I[c];
+               if (yy < P)
+                  plane[static_cast<size_t>(yy) * P + x] = e * scale;
+            }
+         }
+      }
+   }
+   if (!ok)
+      *err = 1;
+   TcFenceBefore();
+   __syncthreads();
+   TcFenceAfter();
+   if (tid == 0 && *err)
+      atomicExch(prm.error, 1);
+   if (warp == 0)
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+}
+
+} // namespace
+
+bool F16x3Supports(int M, int P) { return M <= 128 && M % 16 == 0 && P <= 64 && P >= 1; }
+
+size_t AhatF16Bytes(int nSets) { return static_cast<size_t>(nSets) * kABytes; }
+
+int BuildAhatF16Images(iscu_ctx* ctx, const float2* A, int nSets, int M, int P, unsigned char* out)
+{
+   AhatF16Kernel<<<dim3((kMaxKb * kRows * 32 + 255) / 256, nSets), 256, 0, ctx->stream>>>(A, M, P, out);
+   ISCU_CK_LAUNCH(ctx, "AhatF16Kernel");
+   return ISCU_OK;
+}
+
+int LaunchCztF16x3Core(iscu_ctx* ctx, const SetParams* sets, const unsigned char* ahat, int nSets,
+                       const PsfItem* items, uint32_t nPsf, int M, int P, int normalize, float* out, int* dErr)
+{
+   if (!F16x3Supports(M, P))
+      return Fail(ISCU_ERR_ARG, "f16x3 chirp-Z: needs pupil samples M <= 128 (a multiple of 16) and planes of at "
+                                "most 64 x 64");
+   if (nPsf == 0)
+      return ISCU_OK;
+   const size_t smem = kSmemBytes;
+   ISCU_CK(cudaFuncSetAttribute(CztF16x3Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+   Tc16Params prm;
+   prm.sets = sets;
+   prm.phase = reinterpret_cast<const double2*>(ahat + AhatF16Bytes(nSets));
+   prm.ahat = ahat;
+   prm.items = items;
+   prm.out = out;
+   prm.error = dErr;
+   prm.nPsf = static_cast<int>(nPsf);
+   prm.M = M;
+   prm.P = P;
+   prm.normalize = normalize;
+   const int grid = static_cast<int>(std::min<uint32_t>(nPsf, static_cast<uint32_t>(ctx->smCount)));
+   CztF16x3Kernel<<<grid, kThreads, smem, ctx->stream>>>(prm);
+   ISCU_CK_LAUNCH(ctx, "CztF16x3Kernel");
+   return ISCU_OK;
+}
+
+} // namespace iscu

@@ -12,7 +12,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _abi
-from ._abi import (CZT_FP32, CZT_TF32X3, INTERP_CUBIC, INTERP_LINEAR, INTERP_NEAREST, Camera, IscuError, PsfRequest,
+from ._abi import (CZT_FP32, CZT_TF32X3, CZT_F16X3, INTERP_CUBIC, INTERP_LINEAR, INTERP_NEAREST, Camera, IscuError, PsfRequest,
                    check, load)
 
 EMITTER_DTYPE = np.dtype([("x_px", "<f8"), ("y_px", "<f8"), ("photons", "<f8"), ("plane", "<i4"),
@@ -1096,5 +1096,5 @@ def frames_table(counts, frame_ids=None, bg_scales=None):
 
 
 __all__ = ["Engine", "CameraParams", "PsfParams", "IscuError", "generate_camera_maps", "frames_table",
-           "EMITTER_DTYPE", "FRAME_DTYPE", "GPU_SPLAT_EMITTER_DTYPE", "BLINK_EVENT_DTYPE", "CZT_FP32", "CZT_TF32X3",
+           "EMITTER_DTYPE", "FRAME_DTYPE", "GPU_SPLAT_EMITTER_DTYPE", "BLINK_EVENT_DTYPE", "CZT_FP32", "CZT_TF32X3", "CZT_F16X3",
            "INTERP_NEAREST", "INTERP_LINEAR", "INTERP_CUBIC"]

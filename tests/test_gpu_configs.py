@@ -19,7 +19,7 @@ import numpy as np
 import pytest
 import torch
 
-from insiliscope_b200 import CZT_TF32X3, PsfPlan
+from insiliscope_b200 import CZT_F16X3, CZT_TF32X3, PsfPlan
 
 pytestmark = pytest.mark.gpu
 
@@ -145,15 +145,17 @@ def _passes(engine, config):
         engine.set_render_config(0)
 
 
-def test_c2_whole_library_within_1e5(engine, oracle):
-    """Every PSF of the 4,096-PSF library from the TF32 x 3 tensor-core chirp-Z within 1e-5 of the float64 oracle."""
+@pytest.mark.parametrize("method", [CZT_TF32X3, CZT_F16X3])
+def test_c2_whole_library_within_1e5(engine, oracle, method):
+    """Every PSF of the 4,096-PSF library from the split-precision tensor-core chirp-Z (TF32 x 3, FP16 x 3) within 1e-5
+    of the float64 oracle."""
     from insiliscope_b200.workloads import psf_library
     L = psf_library(seed=42)
-    plan = PsfPlan(engine, L.sets, size=L.size, method=CZT_TF32X3)
+    plan = PsfPlan(engine, L.sets, size=L.size, method=method)
     got = plan.run(L.set_of_psf, L.defocus_nm)
     assert got.shape == (4096, 64, 64)
     err, l2 = library_errors(oracle, L, got)
-    print(f"C2 4096 PSFs: max |I - I64| / max I64 worst {err.max():.3e}, median {np.median(err):.3e}; "
+    print(f"C2 4096 PSFs, method {method}: max |I - I64| / max I64 worst {err.max():.3e}, median {np.median(err):.3e}; "
           f"rel L2 worst {l2.max():.3e}")
     assert err.max() <= 1e-5
 

@@ -6,7 +6,7 @@ import os
 import numpy as np
 import pytest
 
-from insiliscope_b200 import CZT_FP32, CZT_TF32X3, INTERP_CUBIC, PsfParams
+from insiliscope_b200 import CZT_F16X3, CZT_FP32, CZT_TF32X3, INTERP_CUBIC, PsfParams
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-5
@@ -33,7 +33,7 @@ def test_fixture_planes(engine, golden_dir, method):
             assert np.argmax(got[z]) == np.argmax(want[z])
 
 
-@pytest.mark.parametrize("method", [CZT_FP32, CZT_TF32X3])
+@pytest.mark.parametrize("method", [CZT_FP32, CZT_TF32X3, CZT_F16X3])
 def test_library_vs_oracle(engine, oracle, method):
     """The library config's shape (M = 128 pupil -> 64 x 64 at 4x oversampling) with Noll 4-15 aberrations, four
     wavelengths, defocus across +-800 nm, plus a double-helix and a deep, index-mismatched set."""
@@ -74,10 +74,11 @@ def test_kernel_build_vs_reference(engine, reference, method):
     assert np.abs(sums - k.block_sums()).max() <= TOL * k.block_sums().max()
 
 
+@pytest.mark.parametrize("method", [CZT_TF32X3, CZT_F16X3])
 @pytest.mark.parametrize("M,P,nz", [(96, 48, 5), (128, 64, 40), (64, 33, 3), (112, 64, 300)])
-def test_tf32x3_shapes_vs_oracle(engine, oracle, M, P, nz):
-    """The tensor-core path on padded shapes (2P < 128 rows, 2M < 256 K) and more PSFs than SMs (the persistent
-    loop), against the float64 oracle, plane by plane."""
+def test_split_shapes_vs_oracle(engine, oracle, M, P, nz, method):
+    """The tensor-core paths on padded shapes (2P < 128 rows, 2M < 256 K; M = 112 leaves the FP16 form's last K block
+    half empty) and more PSFs than SMs (the persistent loop), against the float64 oracle, plane by plane."""
     rng = np.random.default_rng(M + P)
     z = np.zeros(28)
     z[3:15] = rng.normal(0.0, 0.08, 12)
@@ -85,15 +86,17 @@ def test_tf32x3_shapes_vs_oracle(engine, oracle, M, P, nz):
                     nz=3, z_step_nm=25.0, pupil_samples=M, zernike=list(z))
     dz = rng.uniform(-700.0, 700.0, nz)
     got = engine.psf_library_dev([req], np.zeros(nz, np.uint32), dz, size=P, normalize=True,
-                                 method=CZT_TF32X3).cpu().numpy()
+                                 method=method).cpu().numpy()
     idx = list(range(0, nz, max(1, nz // 6)))
     want = oracle.psf_planes(req, dz[idx] * 1e-9, size=P, normalize=True)
     for j, i in enumerate(idx):
         assert np.abs(got[i] - want[j]).max() <= TOL * want[j].max(), i
 
 
-def test_tf32x3_matches_fp32(engine):
-    """The two chirp-Z forms agree (both within 1e-5 of float64) on a library of 4 sets, two of them double helix."""
+@pytest.mark.parametrize("method", [CZT_TF32X3, CZT_F16X3])
+def test_split_matches_fp32(engine, method):
+    """The split forms agree with the plain one (all within 1e-5 of float64) on a library of 4 sets, two of them double
+    helix, in random order (a set change at most PSFs: the FP16 form reloads its resident DFT operand there)."""
     rng = np.random.default_rng(77)
     sets = [PsfParams(wavelength_nm=wl, na=1.45, pixel_size_nm=100.0, oversampling=4, kernel_half_width_px=8, nz=3,
                       pupil_samples=128, double_helix=dh) for wl, dh in ((520.0, False), (580.0, True),
@@ -101,11 +104,11 @@ def test_tf32x3_matches_fp32(engine):
     set_of = rng.integers(0, 4, 512).astype(np.uint32)
     dz = rng.uniform(-800.0, 800.0, 512)
     a = engine.psf_library_dev(sets, set_of, dz, size=64, method=CZT_FP32).cpu().numpy()
-    b = engine.psf_library_dev(sets, set_of, dz, size=64, method=CZT_TF32X3).cpu().numpy()
+    b = engine.psf_library_dev(sets, set_of, dz, size=64, method=method).cpu().numpy()
     assert np.abs(a - b).max() <= 2 * TOL * a.max()
 
 
-@pytest.mark.parametrize("method", [CZT_FP32, CZT_TF32X3])
+@pytest.mark.parametrize("method", [CZT_FP32, CZT_TF32X3, CZT_F16X3])
 def test_plan_matches_library(engine, method):
     """A PSF plan (per-set work once, device-resident runs) gives the one-shot library call's planes, bit for bit."""
     import torch
