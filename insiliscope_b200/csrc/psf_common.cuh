@@ -72,12 +72,13 @@ int LaunchCztSplit(iscu_ctx* ctx, int method, const SetParams* sets, const doubl
 bool Tf32x3Supports(int M, int P);
 bool F16x3Supports(int M, int P);
 // The split-precision kernels' per-set data in one buffer: the DFT operand's K-block images in the method's layout
-// (SplitImageBytes), then the pupil phase tables.
+// (SplitImageBytes), then the pupil phase tables (TF32: float64 radians; FP16: float32 revolutions).
 int BuildAhat(iscu_ctx* ctx, const float2* A, const SetParams* sets, const double3* tables, int nSets, int M, int P,
               int method, DevBuf& ahat);
 size_t SplitImageBytes(int method, int nSets);
 size_t AhatF16Bytes(int nSets);
-int BuildAhatF16Images(iscu_ctx* ctx, const float2* A, int nSets, int M, int P, unsigned char* out);
+int BuildAhatF16(iscu_ctx* ctx, const float2* A, const SetParams* sets, const double3* tables, int nSets, int M,
+                 int P, unsigned char* out);
 int LaunchCztTf32x3Core(iscu_ctx* ctx, const SetParams* sets, const float* ahat, int nSets, const PsfItem* items,
                         uint32_t nPsf, int M, int P, int normalize, float* out, int* dErr);
 int LaunchCztF16x3Core(iscu_ctx* ctx, const SetParams* sets, const unsigned char* ahat, int nSets,

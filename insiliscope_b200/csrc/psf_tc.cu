@@ -604,20 +604,13 @@ int BuildAhat(iscu_ctx* ctx, const float2* A, const SetParams* sets, const doubl
       return Fail(ISCU_ERR_ARG, std::string(f16 ? "f16x3" : "tf32x3") +
                                    " chirp-Z: needs pupil samples M <= 128 (a multiple of 16) and planes of at most "
                                    "64 x 64 (else use the fp32 method)");
-   // the K-block images, then the phase tables
+   // the K-block images, then the phase tables (FP16 form: float2 in revolutions; TF32 form: double2 in radians)
    const size_t images = SplitImageBytes(method, nSets);
-   ISCU_CK(ahat.Reserve(images + static_cast<size_t>(nSets) * M * M * sizeof(double2)));
+   ISCU_CK(ahat.Reserve(images + static_cast<size_t>(nSets) * M * M * (f16 ? sizeof(float2) : sizeof(double2))));
    if (f16)
-   {
-      const int rc = BuildAhatF16Images(ctx, A, nSets, M, P, ahat.as<unsigned char>());
-      if (rc != ISCU_OK)
-         return rc;
-   }
-   else
-   {
-      AhatKernel<<<dim3((8 * kRows * 32 + 255) / 256, nSets), 256, 0, ctx->stream>>>(A, M, P, ahat.as<float>());
-      ISCU_CK_LAUNCH(ctx, "AhatKernel");
-   }
+      return BuildAhatF16(ctx, A, sets, tables, nSets, M, P, ahat.as<unsigned char>());
+   AhatKernel<<<dim3((8 * kRows * 32 + 255) / 256, nSets), 256, 0, ctx->stream>>>(A, M, P, ahat.as<float>());
+   ISCU_CK_LAUNCH(ctx, "AhatKernel");
    PhaseTableKernel<<<dim3((M * M + 255) / 256, nSets), 256, 0, ctx->stream>>>(
       sets, tables, M * M, reinterpret_cast<double2*>(ahat.as<char>() + images));
    ISCU_CK_LAUNCH(ctx, "PhaseTableKernel");

@@ -17,6 +17,13 @@
 // result T (|T| <= M <= 128, accumulated as 2^24 T) is scaled by 2^-16 to 2^8 T (<= 32,768) before its split, and E
 // (2^20 E in TMEM) by 2^-20 before |E|^2.
 //
+// The pupil phasors come from a per-set float32 table in revolutions: (tx, ty) = ((base mod 2 pi) / 2 pi, opd3F /
+// 2 pi), reduced in float64 when the table is built, so a PSF's phase is x = a ty + tx revolutions (a = k0 ni dti, one
+// float32 multiply-add; |x| < 4 at these defocus ranges, so its rounding is < 2.4e-7 revolutions, 1.5e-6 rad), reduced
+// exactly as x - rint(x) and turned into sine and cosine by the special-function unit. Those per-sample phase errors
+// are independent, so their effect on a plane, a sum over ~10^4 samples, stays orders of magnitude below float32
+// resolution of its peak; the float64 form of the TF32 kernel costs twice the table bytes and a float64 chain.
+//
 // Against the TF32 form: a K step does twice the inputs for the same shared-memory bytes (64.5 cycles per
 // M128 N128 step either way, shared-memory bound at N = 64), so the MMAs take half the time; and the DFT operand
 // (both parts, 2M inputs: 128 KB at M = 128) is loaded once per run of PSFs that share a request set instead of
@@ -134,11 +141,41 @@ __global__ void AhatF16Kernel(const float2* __restrict__ A, int M, int P, unsign
    *reinterpret_cast<uint32_t*>(base + kImgBytes + SwOff16(row, c)) = lo;
 }
 
+// The phase table in revolutions: per set and sample (tx, ty) = ((k0 opd1 + zernike + mask) mod 2 pi, opd3F) / 2 pi
+// (ZernikePsf.cpp:240-248), the reduction in float64; (0, -1) outside the aperture (opd3F < 0).
+__global__ void RevTableKernel(const SetParams* __restrict__ sets, const double3* __restrict__ tables, int MM,
+                               float2* __restrict__ out)
+{
+   const int s = blockIdx.y;
+   const int m = blockIdx.x * blockDim.x + threadIdx.x;
+   if (m >= MM)
+      return;
+   const double3 t = tables[static_cast<size_t>(s) * MM + m];
+   const double kInvTwoPi = 0.15915494309189533577;
+   const double b = ReduceTwoPi(sets[s].k0 * t.x + t.z) * kInvTwoPi;
+   out[static_cast<size_t>(s) * MM + m] = t.y < 0.0 ? make_float2(0.f, -1.f)
+                                                    : make_float2(static_cast<float>(b), static_cast<float>(t.y * kInvTwoPi));
+}
+
+// One pupil phasor from the revolution table, times amp inside the aperture (0 outside): x = a ty + tx, r = x - rint(x)
+// (rint by adding and taking away 1.5 2^23, exact for |x| < 2^22; r in [-1/2, 1/2] exactly), then the float32 sine and
+// cosine of 2 pi r (absolute error ~4e-7 over [-pi, pi]).
+__device__ __forceinline__ float2 RevPhasor(float2 t, float a, float amp)
+{
+   const float kRound = 12582912.0f;   // 1.5 2^23
+   const float x = fmaf(a, t.y, t.x);
+   const float n = (x + kRound) - kRound;
+   float sn, cs;
+   __sincosf(6.28318530718f * (x - n), &sn, &cs);
+   const float s = t.y >= 0.f ? amp : 0.f;
+   return make_float2(cs * s, sn * s);
+}
+
 // ------------------------------------------------------------------------------------------ the fused kernel
 struct Tc16Params
 {
    const SetParams* sets;
-   const double2* phase;       // [set][M * M] (base, opd3F)
+   const float2* phase;        // [set][M * M] (tx, ty) revolutions
    const unsigned char* ahat;  // [set][kMaxKb][hi, lo] images
    const PsfItem* items;
    float* out;
@@ -154,7 +191,7 @@ struct Shared16
    uint64_t rowDone[2], colDone[2], tFree[2], eFree[2], red[2];
    uint64_t final[2];
    double sum[2][kDrainWarps];
-   double aDef[kSetCache];   // k0 ni (ti - ti0) of the CTA's j-th PSF, j < kSetCache
+   float aDef[kSetCache];    // k0 ni (ti - ti0) of the CTA's j-th PSF, j < kSetCache (ty carries the 1 / 2 pi)
    int set[kSetCache];       // its set
    uint32_t tmemSlot;
    int err;
@@ -164,9 +201,9 @@ constexpr size_t kSmemBytes = static_cast<size_t>(kABytes) + static_cast<size_t>
 static_assert(kSmemBytes <= 227 * 1024, "the FP16 chirp-Z kernel's shared memory");
 
 // Per CTA, persistent over a contiguous run of PSFs, warp-specialized; the roles meet only at mbarriers:
-//   producers (warps 5-7, 9-15): per row-pass K block the pupil phasors of 32 pupil rows (float64 phase reduced mod
-//     2 pi, float32 sine and cosine, times 2^12, FP16 hi/lo split) into a row-B stage -> rowFull; the phase-table
-//     entries of a thread's next item are in flight while it computes the current one;
+//   producers (warps 5-7, 9-15): per row-pass K block the pupil phasors of 32 pupil rows (float32 phase in
+//     revolutions reduced exactly, float32 sine and cosine, times 2^12, FP16 hi/lo split) into a row-B stage ->
+//     rowFull; the phase-table entries of a thread's next item are in flight while it computes the current one;
 //   the row-pass thread (warp 4, lane 0): at the first PSF of each run of one set, once both passes of the previous
 //     set are done with the operand (aFree), the set's DFT operand by bulk copy (aFull); then per PSF its row pass
 //     R(j), K block by K block as the producers fill the stages, into T's TMEM buffer j % 2 (free again when the
@@ -232,7 +269,7 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
    {
       const PsfItem it = prm.items[psf0 + j];
       sh->set[j] = it.set;
-      sh->aDef[j] = prm.sets[it.set].k0 * prm.sets[it.set].ni * it.dtiM;
+      sh->aDef[j] = static_cast<float>(prm.sets[it.set].k0 * prm.sets[it.set].ni * it.dtiM);
    }
    TcFenceBefore();
    __syncthreads();
@@ -250,29 +287,30 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
       // 7), item = ptid + r kProducerThreads.
       const int ptid = 32 * ProducerIndex(warp) + lane;
       const int nR = ptid + kProducerThreads < kItemsPerBlock ? 2 : 1;
-      auto load = [&](const double2* tab, int kb, int r, double2* dst) {
+      auto load = [&](const float2* tab, int kb, int r, float2* dst) {
          const int item = ptid + r * kProducerThreads, m = item & 127, n0 = 32 * kb + 8 * (item >> 7);
          const bool in = m < M && n0 < M;
+         const float2* t = tab + n0 * M + m;
 #pragma unroll
          for (int c = 0; c < 8; ++c)
-            dst[c] = in ? tab[static_cast<size_t>(n0 + c) * M + m] : make_double2(0.0, -1.0);
+            dst[c] = in ? t[c * M] : make_float2(0.f, -1.f);
       };
       // the defocus factor of PSF j (staged in shared memory for j < kSetCache)
       auto aDefOf = [&](int j) {
          if (j < kSetCache)
             return sh->aDef[j];
          const PsfItem it = prm.items[psf0 + j];
-         return prm.sets[it.set].k0 * prm.sets[it.set].ni * it.dtiM;
+         return static_cast<float>(prm.sets[it.set].k0 * prm.sets[it.set].ni * it.dtiM);
       };
       auto tabOf = [&](int j) { return prm.phase + static_cast<size_t>(setOf(j)) * M * M; };
-      double2 nxt[8];
+      float2 nxt[8];
       if (nLocal > 0)
          load(tabOf(0), 0, 0, nxt);
       uint32_t rowCount = 0;
       for (int j = 0; j < nLocal && ok; ++j)
       {
-         const double aDef = aDefOf(j);
-         const double2* tab = tabOf(j);
+         const float aDef = aDefOf(j);
+         const float2* tab = tabOf(j);
          for (int kb = 0; kb < nKb; ++kb, ++rowCount)
          {
             const int rs = static_cast<int>(rowCount % kRowStages);
@@ -285,7 +323,7 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
             {
                if (r >= nR)
                   break;
-               double2 cur[8];
+               float2 cur[8];
 #pragma unroll
                for (int c = 0; c < 8; ++c)
                   cur[c] = nxt[c];
@@ -303,9 +341,10 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
 #pragma unroll
                   for (int c = 0; c < 4; ++c)
                   {
-                     const float2 u0 = TablePhasor(cur[2 * c], aDef), u1 = TablePhasor(cur[2 * c + 1], aDef);
-                     SplitH2(u0.x * kScaleOp, u1.x * kScaleOp, rh[c], rl[c]);
-                     SplitH2(u0.y * kScaleOp, u1.y * kScaleOp, ih[c], il[c]);
+                     const float2 u0 = RevPhasor(cur[2 * c], aDef, kScaleOp);
+                     const float2 u1 = RevPhasor(cur[2 * c + 1], aDef, kScaleOp);
+                     SplitH2(u0.x, u1.x, rh[c], rl[c]);
+                     SplitH2(u0.y, u1.y, ih[c], il[c]);
                   }
                   // B[m][c0 + i]: the real part of pupil row n0 + i; B[m][c0 + 16 + i]: the imaginary part
                   const int c0 = 32 * (l >> 4) + (l & 15);
@@ -570,10 +609,14 @@ bool F16x3Supports(int M, int P) { return M <= 128 && M % 16 == 0 && P <= 64 && 
 
 size_t AhatF16Bytes(int nSets) { return static_cast<size_t>(nSets) * kABytes; }
 
-int BuildAhatF16Images(iscu_ctx* ctx, const float2* A, int nSets, int M, int P, unsigned char* out)
+int BuildAhatF16(iscu_ctx* ctx, const float2* A, const SetParams* sets, const double3* tables, int nSets, int M,
+                 int P, unsigned char* out)
 {
    AhatF16Kernel<<<dim3((kMaxKb * kRows * 32 + 255) / 256, nSets), 256, 0, ctx->stream>>>(A, M, P, out);
    ISCU_CK_LAUNCH(ctx, "AhatF16Kernel");
+   RevTableKernel<<<dim3((M * M + 255) / 256, nSets), 256, 0, ctx->stream>>>(
+      sets, tables, M * M, reinterpret_cast<float2*>(out + AhatF16Bytes(nSets)));
+   ISCU_CK_LAUNCH(ctx, "RevTableKernel");
    return ISCU_OK;
 }
 
@@ -589,7 +632,7 @@ int LaunchCztF16x3Core(iscu_ctx* ctx, const SetParams* sets, const unsigned char
    ISCU_CK(cudaFuncSetAttribute(CztF16x3Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
    Tc16Params prm;
    prm.sets = sets;
-   prm.phase = reinterpret_cast<const double2*>(ahat + AhatF16Bytes(nSets));
+   prm.phase = reinterpret_cast<const float2*>(ahat + AhatF16Bytes(nSets));
    prm.ahat = ahat;
    prm.items = items;
    prm.out = out;
