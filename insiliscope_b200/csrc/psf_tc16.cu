@@ -1,6 +1,6 @@
 // Split-precision chirp-Z on the 5th-generation tensor cores with FP16 operands: the PSF library's two complex
 // products as FP16 x 3 real GEMMs (tcgen05 kind::f16, float32 accumulation in tensor memory), the DFT operand resident
-// in shared memory.
+// in tensor memory.
 //
 // The products and the stacked operand are the TF32 x 3 kernel's (psf_tc.cu): row pass T = A U, column pass
 // E^T = A T^T, Ahat = [[Ar, -Ai], [Ai, Ar]], rows interleaved in groups of 16 (row r = 32 g + 16 h + i is output
@@ -14,8 +14,9 @@
 // the dropped lo*lo is <= 2^-22 |a b|, half the TF32 split's error (its lo is truncated to TF32 by the tensor
 // cores). FP16's narrow range is kept by exact power-of-two scales: the DFT operand and the pupil phasors (|x| <= 1)
 // enter times 2^12, so a part falls below FP16's normal range only where it is under 2^-26 of the unit; the row-pass
-// result T (|T| <= M <= 128, accumulated as 2^24 T) is scaled by 2^-16 to 2^8 T (<= 32,768) before its split, and E
-// (2^20 E in TMEM) by 2^-20 before |E|^2.
+// result T (|T| <= M <= 128, accumulated as 2^24 T) is scaled by 2^-16 to 2^8 T (<= 32,768) before its split; E is
+// 2^20 E in TMEM (|2^20 E| <= 2^34), so |2^20 E|^2 <= 2^68 stays finite in float32 and the sum-1 normalization
+// cancels the 2^40 (an unnormalized plane is multiplied by 2^-40, exactly).
 //
 // The pupil phasors come from a per-set float32 table in revolutions: (tx, ty) = ((base mod 2 pi) / 2 pi, opd3F /
 // 2 pi), reduced in float64 when the table is built, so a PSF's phase is x = a ty + tx revolutions (a = k0 ni dti, one
@@ -24,11 +25,14 @@
 // are independent, so their effect on a plane, a sum over ~10^4 samples, stays orders of magnitude below float32
 // resolution of its peak; the float64 form of the TF32 kernel costs twice the table bytes and a float64 chain.
 //
-// Against the TF32 form: a K step does twice the inputs for the same shared-memory bytes (64.5 cycles per
-// M128 N128 step either way, shared-memory bound at N = 64), so the MMAs take half the time; and the DFT operand
-// (both parts, 2M inputs: 128 KB at M = 128) is loaded once per run of PSFs that share a request set instead of
-// streamed per K block, which takes the two passes out of lockstep. A set change waits until both passes of the
-// previous set are done with the operand.
+// Against the TF32 form: a K step does twice the inputs, so the MMAs take half the time; and the DFT operand (both
+// parts, 2M inputs: 128 KB at M = 128) is loaded once per run of PSFs that share a request set, into tensor memory
+// (256 of the 512 columns), instead of streamed through shared memory per K block. An MMA then reads only its B
+// operand from shared memory (4 KB per row-pass step, 2 KB per column-pass step, where an A operand in shared memory
+// doubled that and made the N = 64 column pass shared-memory bound), the two passes run out of lockstep, and shared
+// memory holds four row-pass and four column-pass stages. A set change waits until both passes of the previous set
+// are done with the operand (the drain warps, which load it, have by then taken the previous PSF's E). The other
+// 256 columns hold T of the current PSF (128) and E of two PSFs (2 x 64).
 
 #include "iscu_internal.h"
 #include "psf_common.cuh"
@@ -46,27 +50,29 @@ using namespace tc;
 
 constexpr int kThreads = 512;
 constexpr int kRows = 128;                        // UMMA M (2P rows, padded)
-constexpr int kImgBytes = 128 * 128;              // one operand image: 128 rows x 64 FP16 (128 B per row)
-constexpr int kKbBytes = 2 * kImgBytes;           // a K block: its hi and lo images
-constexpr int kMaxKb = 4;                         // K = 2M <= 256
-constexpr int kABytes = kMaxKb * kKbBytes;        // the resident DFT operand: 128 KB
-constexpr int kRowStages = 2;                     // row-pass B blocks (pupil phasors)
-constexpr int kColStages = 2;                     // column-pass B blocks (T, split)
+constexpr int kImgBytes = 128 * 128;              // one B operand image: 128 rows x 64 FP16 (128 B per row)
+constexpr int kKbBytes = 2 * kImgBytes;           // a row-pass B block: its hi and lo images
+constexpr int kACols = 128;                       // TMEM columns of one part of the DFT operand (256 FP16 per row)
+constexpr int kAImageBytes = 2 * kRows * kACols * 4;   // the DFT operand of one set, both parts: 128 KB
+constexpr int kRowStages = 4;                     // row-pass B blocks (pupil phasors)
+constexpr int kColStages = 4;                     // column-pass B blocks (T, split): a whole PSF's at M = 128
 constexpr int kColImgBytes = 64 * 128;            // a column-pass B image: 64 rows x 64 FP16
 constexpr int kColStageBytes = 2 * kColImgBytes;
 constexpr float kScaleOp = 4096.0f;               // 2^12: the DFT operand and the pupil phasors
 constexpr float kScaleT = 1.0f / 65536.0f;        // 2^-16: 2^24 T -> 2^8 T
-constexpr float kScaleE = 1.0f / 1048576.0f;      // 2^-20: 2^20 E -> E
+constexpr float kScaleI = 0x1p-40f;               // 2^-40: |2^20 E|^2 -> |E|^2 (unnormalized planes)
 
 // Warp roles. Warps share an SM sub-partition (scheduler) when equal mod 4.
 constexpr int kDrainWarps = 4;                    // warps 0-3, one per TMEM lane quadrant
-constexpr int kRowMmaWarp = 4;                    // lane 0: the DFT operand copies and the row-pass MMAs
+constexpr int kRowMmaWarp = 4;                    // lane 0: the row-pass MMAs
 constexpr int kColMmaWarp = 8;                    // lane 0: the column-pass MMAs
 constexpr int kProducerWarps = 10;                // warps 5-7 and 9-15 make the pupil phasors
 constexpr int kProducerThreads = 32 * kProducerWarps;
 constexpr int kItemsPerBlock = 512;               // (pupil column, 8 pupil rows) items of one row-pass K block
-constexpr int kTmemRow = 0;                       // T of PSF j: columns [128 (j % 2), +128)
-constexpr int kTmemCol = 256;                     // E of PSF j: columns [256 + 64 (j % 2), +64)
+constexpr int kTmemAHi = 0;                       // the DFT operand's hi part: columns [0, 128)
+constexpr int kTmemALo = 128;                     // its lo part: columns [128, 256)
+constexpr int kTmemRow = 256;                     // T of the current PSF: columns [256, 384)
+constexpr int kTmemCol = 384;                     // E of PSF j: columns [384 + 64 (j % 2), +64)
 constexpr int kSetCache = 96;                     // PSFs whose set and defocus factor are staged in shared memory
 
 static_assert(kItemsPerBlock <= 2 * kProducerThreads, "a producer thread makes at most two items per K block");
@@ -80,12 +86,13 @@ __host__ __device__ constexpr uint32_t InstrDescF16(int M, int N)
    return (1u << 4) | (static_cast<uint32_t>(N >> 3) << 17) | (static_cast<uint32_t>(M >> 4) << 24);
 }
 
-__device__ __forceinline__ void MmaF16(uint32_t dTmem, uint64_t aDesc, uint64_t bDesc, uint32_t idesc,
-                                       uint32_t accum)
+// D (TMEM) += A (TMEM, 8 columns: 16 FP16 per row) x B (shared memory descriptor); accum 0 overwrites D.
+__device__ __forceinline__ void MmaF16Ts(uint32_t dTmem, uint32_t aTmem, uint64_t bDesc, uint32_t idesc,
+                                         uint32_t accum)
 {
    asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-                " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(dTmem),
-                "l"(aDesc), "l"(bDesc), "r"(idesc), "r"(accum));
+                " tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n}\n" ::"r"(dTmem),
+                "r"(aTmem), "l"(bDesc), "r"(idesc), "r"(accum));
 }
 
 // Byte offset of FP16 element (row, col) (col 0..63 within the K block) in a 128-byte-swizzled image.
@@ -111,21 +118,25 @@ __device__ __forceinline__ void StoreShared16(unsigned char* p, uint32_t a, uint
 }
 
 // ------------------------------------------------------------------------------------------ the stacked operand
-// Ahat for one set, times 2^12 and split, in K-block order and in the shared-memory image the MMA reads:
-// [kb][hi, lo][16 KB image of 128 rows x 64 FP16]. Rows beyond 2P and inputs at or past M are zero.
-__global__ void AhatF16Kernel(const float2* __restrict__ A, int M, int P, unsigned char* __restrict__ out)
+// Ahat for one set, times 2^12 and split, in the order the drain warps move it into tensor memory: [part hi, lo]
+// [column group g = 0..31][row r][4 columns], so that a warp's 32 rows of a column group are 512 consecutive bytes.
+// Column c of row r holds K elements 2c and 2c + 1 (the even one in the low half); K element k = 64 kb + c' is input
+// q = 32 kb + 16 (c' >> 5) + (c' & 15), part (c' >> 4) & 1, the order of the B operands' K blocks. Rows beyond 2P and
+// inputs at or past M are zero.
+__global__ void AhatTmemKernel(const float2* __restrict__ A, int M, int P, uint32_t* __restrict__ out)
 {
    const int s = blockIdx.y;
-   const int e = blockIdx.x * blockDim.x + threadIdx.x;   // (kb, row, column pair)
-   if (e >= kMaxKb * kRows * 32)
+   const int e = blockIdx.x * blockDim.x + threadIdx.x;   // (row, column)
+   if (e >= kRows * kACols)
       return;
-   const int kb = e / (kRows * 32), row = (e / 32) % kRows, c = 2 * (e % 32);
+   const int row = e / kACols, col = e % kACols;
    const int p = 16 * (row >> 5) + (row & 15), h = (row >> 4) & 1;
    float v[2];
 #pragma unroll
    for (int t = 0; t < 2; ++t)
    {
-      const int col = c + t, hp = (col >> 4) & 1, q = 32 * kb + 16 * (col >> 5) + (col & 15);
+      const int k = 2 * col + t, kb = k >> 6, c = k & 63;
+      const int hp = (c >> 4) & 1, q = 32 * kb + 16 * (c >> 5) + (c & 15);
       v[t] = 0.f;
       if (p < P && q < M)
       {
@@ -136,9 +147,10 @@ __global__ void AhatF16Kernel(const float2* __restrict__ A, int M, int P, unsign
    }
    uint32_t hi, lo;
    SplitH2(v[0], v[1], hi, lo);
-   unsigned char* base = out + (static_cast<size_t>(s) * kMaxKb + kb) * kKbBytes;
-   *reinterpret_cast<uint32_t*>(base + SwOff16(row, c)) = hi;
-   *reinterpret_cast<uint32_t*>(base + kImgBytes + SwOff16(row, c)) = lo;
+   uint32_t* base = out + static_cast<size_t>(s) * (kAImageBytes / 4);
+   const size_t idx = (static_cast<size_t>(col >> 2) * kRows + row) * 4 + (col & 3);
+   base[idx] = hi;
+   base[kRows * kACols + idx] = lo;
 }
 
 // The phase table in revolutions: per set and sample (tx, ty) = ((k0 opd1 + zernike + mask) mod 2 pi, opd3F) / 2 pi
@@ -176,7 +188,7 @@ struct Tc16Params
 {
    const SetParams* sets;
    const float2* phase;        // [set][M * M] (tx, ty) revolutions
-   const unsigned char* ahat;  // [set][kMaxKb][hi, lo] images
+   const unsigned char* ahat;  // [set] DFT operand images in tensor-memory order (AhatTmemKernel)
    const PsfItem* items;
    float* out;
    int* error;
@@ -185,10 +197,11 @@ struct Tc16Params
 
 struct Shared16
 {
-   uint64_t aFull, aFree;
+   uint64_t aFull;
    uint64_t rowFull[kRowStages], rowEmpty[kRowStages];
    uint64_t colFull[kColStages], colEmpty[kColStages];
-   uint64_t rowDone[2], colDone[2], tFree[2], eFree[2], red[2];
+   uint64_t rowDone, tFree;
+   uint64_t colDone[2], eFree[2], red[2];
    uint64_t final[2];
    double sum[2][kDrainWarps];
    float aDef[kSetCache];    // k0 ni (ti - ti0) of the CTA's j-th PSF, j < kSetCache (ty carries the 1 / 2 pi)
@@ -196,7 +209,7 @@ struct Shared16
    uint32_t tmemSlot;
    int err;
 };
-constexpr size_t kSmemBytes = static_cast<size_t>(kABytes) + static_cast<size_t>(kRowStages) * kKbBytes +
+constexpr size_t kSmemBytes = static_cast<size_t>(kRowStages) * kKbBytes +
                               static_cast<size_t>(kColStages) * kColStageBytes + sizeof(Shared16) + 1024;
 static_assert(kSmemBytes <= 227 * 1024, "the FP16 chirp-Z kernel's shared memory");
 
@@ -204,23 +217,23 @@ static_assert(kSmemBytes <= 227 * 1024, "the FP16 chirp-Z kernel's shared memory
 //   producers (warps 5-7, 9-15): per row-pass K block the pupil phasors of 32 pupil rows (float32 phase in
 //     revolutions reduced exactly, float32 sine and cosine, times 2^12, FP16 hi/lo split) into a row-B stage ->
 //     rowFull; the phase-table entries of a thread's next item are in flight while it computes the current one;
-//   the row-pass thread (warp 4, lane 0): at the first PSF of each run of one set, once both passes of the previous
-//     set are done with the operand (aFree), the set's DFT operand by bulk copy (aFull); then per PSF its row pass
-//     R(j), K block by K block as the producers fill the stages, into T's TMEM buffer j % 2 (free again when the
-//     drain warps have taken T(j - 2): tFree); commits free the stages and mark the pass done (rowDone);
-//   the column-pass thread (warp 8, lane 0): per PSF its column pass C(j) as the drain warps fill the col-B stages,
-//     into E's TMEM buffer j % 2 (eFree), commits colEmpty / colDone; the last PSF of a set's run commits aFree;
+//   the row-pass thread (warp 4, lane 0): per PSF its row pass R(j), K block by K block as the producers fill the
+//     stages, into T's columns once the drain warps have taken T(j - 1) (tFree), with the set's DFT operand from TMEM
+//     (aFull at the first PSF of each run of one set); commits free the stages and mark the pass done (rowDone);
+//   the column-pass thread (warp 8, lane 0): per PSF its column pass C(j) into E's buffer j % 2 once E(j - 2) has
+//     been taken (eFree), K block by K block as the drain warps fill the col-B stages; commits colEmpty / colDone;
 //   drain warps (0-3, one TMEM lane quadrant each): T of PSF j from TMEM, times 2^-16, split, into col-B stages ->
-//     colFull (then tFree); then E of PSF j: times 2^-20, |E|^2, the plane sum, the normalized plane (eFree).
+//     colFull (then tFree); then E of PSF j: |E|^2, the plane sum, the normalized plane (eFree). At the
+//     first PSF of each set's run (E of the previous PSF taken: both passes of every earlier PSF complete) the set's
+//     DFT operand from global memory into TMEM (aFull).
 // R(j + 1) runs beside C(j) on the tensor pipe. Every wait is bounded (kWaitNs) and also ends when another role has
-// failed (Shared16::err); a failed CTA stops issuing, waits for its copies and MMAs in flight, frees TMEM and reports
-// through prm.error.
+// failed (Shared16::err); a failed CTA stops issuing, waits for its MMAs in flight, frees TMEM and reports through
+// prm.error.
 __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
 {
    extern __shared__ __align__(1024) unsigned char smemRaw[];
    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
-   unsigned char* sA = smem;                                  // [kMaxKb] x 32 KB, resident per set
-   unsigned char* sRowB = sA + kABytes;                       // [kRowStages] x 32 KB
+   unsigned char* sRowB = smem;                               // [kRowStages] x 32 KB
    unsigned char* sColB = sRowB + kRowStages * kKbBytes;      // [kColStages] x 16 KB
    Shared16* sh = reinterpret_cast<Shared16*>(sColB + kColStages * kColStageBytes);
    volatile int* err = &sh->err;
@@ -240,8 +253,7 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
    }
    if (tid == 0)
    {
-      MbarInit(&sh->aFull, 1);
-      MbarInit(&sh->aFree, 2);   // the row-pass and the column-pass threads, once per set run
+      MbarInit(&sh->aFull, kDrainWarps);   // once per set run
       for (int s = 0; s < kRowStages; ++s)
       {
          MbarInit(&sh->rowFull[s], kProducerWarps);
@@ -252,11 +264,11 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
          MbarInit(&sh->colFull[s], kDrainWarps);
          MbarInit(&sh->colEmpty[s], 1);
       }
+      MbarInit(&sh->rowDone, 1);
+      MbarInit(&sh->tFree, kDrainWarps);
       for (int s = 0; s < 2; ++s)
       {
-         MbarInit(&sh->rowDone[s], 1);
          MbarInit(&sh->colDone[s], 1);
-         MbarInit(&sh->tFree[s], kDrainWarps);
          MbarInit(&sh->eFree[s], kDrainWarps);
          MbarInit(&sh->red[s], kDrainWarps);
       }
@@ -278,7 +290,6 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
    bool ok = true;
    auto setOf = [&](int j) { return j < kSetCache ? sh->set[j] : prm.items[psf0 + j].set; };
    auto firstOfSet = [&](int j) { return j == 0 || setOf(j) != setOf(j - 1); };
-   auto lastOfSet = [&](int j) { return j == nLocal - 1 || setOf(j + 1) != setOf(j); };
 
    if (warp > kRowMmaWarp && warp != kColMmaWarp)
    {
@@ -363,31 +374,23 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
    }
    else if (warp == kRowMmaWarp)
    {
-      // ---------------------------------------------------------------- the DFT operand and the row passes
+      // ---------------------------------------------------------------- the row passes
       if (lane == 0 && nLocal > 0)
       {
          const uint32_t idesc = InstrDescF16(kRows, M);
-         uint32_t count = 0, loads = 0;
+         uint32_t count = 0, runs = 0;
          for (int j = 0; j < nLocal && ok; ++j)
          {
             if (firstOfSet(j))
             {
-               if (loads > 0)   // both passes of the previous set are done with the operand
-                  ok = MbarWait(&sh->aFree, (loads - 1) & 1u, err, false);
-               if (!ok)
-                  break;
-               MbarExpectTx(&sh->aFull, static_cast<uint32_t>(nKb * kKbBytes));
-               const unsigned char* src = prm.ahat + static_cast<size_t>(setOf(j)) * kABytes;
-               for (int kb = 0; kb < nKb; ++kb)
-                  BulkLoad(sA + kb * kKbBytes, src + kb * kKbBytes, kKbBytes, &sh->aFull);
-               ++loads;
-               ok = MbarWait(&sh->aFull, (loads - 1) & 1u, err, false);
+               ok = MbarWait(&sh->aFull, runs & 1u, err, false);   // this set's operand is in TMEM
+               ++runs;
                if (!ok)
                   break;
             }
-            const uint32_t use = static_cast<uint32_t>(j >> 1) & 1u;
-            ok = MbarWait(&sh->tFree[j & 1], use ^ 1u, err, false);   // T(j - 2) has left the buffer
-            const uint32_t d = tmem + kTmemRow + 128u * static_cast<uint32_t>(j & 1);
+            if (j > 0)   // T(j - 1) has left TMEM
+               ok = MbarWait(&sh->tFree, static_cast<uint32_t>(j - 1) & 1u, err, false);
+            const uint32_t d = tmem + kTmemRow;
             for (int kb = 0; kb < nKb && ok; ++kb, ++count)
             {
                const int rs = static_cast<int>(count % kRowStages);
@@ -395,7 +398,6 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
                if (!ok)
                   break;
                TcFenceAfter();
-               const uint32_t aH = SmemAddr(sA + kb * kKbBytes), aL = aH + kImgBytes;
                const uint32_t bH = SmemAddr(sRowB + rs * kKbBytes), bL = bH + kImgBytes;
 #pragma unroll
                for (int kk = 0; kk < 4; ++kk)
@@ -403,23 +405,20 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
                   if (32 * kb + 16 * (kk >> 1) >= M)
                      continue;
                   const uint32_t off = kk * 32;   // 16 FP16 = 32 bytes along K
-                  MmaF16(d, SmemDesc(aH + off), SmemDesc(bH + off), idesc, (kb == 0 && kk == 0) ? 0u : 1u);
-                  MmaF16(d, SmemDesc(aH + off), SmemDesc(bL + off), idesc, 1u);
-                  MmaF16(d, SmemDesc(aL + off), SmemDesc(bH + off), idesc, 1u);
+                  const uint32_t aH = tmem + kTmemAHi + 8u * (4 * kb + kk), aL = aH + (kTmemALo - kTmemAHi);
+                  MmaF16Ts(d, aH, SmemDesc(bH + off), idesc, (kb == 0 && kk == 0) ? 0u : 1u);
+                  MmaF16Ts(d, aH, SmemDesc(bL + off), idesc, 1u);
+                  MmaF16Ts(d, aL, SmemDesc(bH + off), idesc, 1u);
                }
                Commit(&sh->rowEmpty[rs]);
             }
             if (!ok)
                break;
-            Commit(&sh->rowDone[j & 1]);
-            if (lastOfSet(j))
-               Commit(&sh->aFree);
+            Commit(&sh->rowDone);
          }
          if (!ok)
          {
             *err = 1;
-            if (loads > 0)   // the copies in flight land before the CTA frees its memory
-               MbarWait(&sh->aFull, (loads - 1) & 1u, nullptr);
             Commit(&sh->final[0]);   // this thread's MMAs in flight finish before the CTA frees its TMEM
             MbarWait(&sh->final[0], 0u, nullptr);
          }
@@ -451,7 +450,6 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
                if (!ok)
                   break;
                TcFenceAfter();
-               const uint32_t aH = SmemAddr(sA + kb * kKbBytes), aL = aH + kImgBytes;
                const uint32_t bH = SmemAddr(sColB + cs * kColStageBytes), bL = bH + kColImgBytes;
 #pragma unroll
                for (int kk = 0; kk < 4; ++kk)
@@ -459,17 +457,16 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
                   if (32 * kb + 16 * (kk >> 1) >= M)
                      continue;
                   const uint32_t off = kk * 32;
-                  MmaF16(d, SmemDesc(aH + off), SmemDesc(bH + off), idesc, (kb == 0 && kk == 0) ? 0u : 1u);
-                  MmaF16(d, SmemDesc(aH + off), SmemDesc(bL + off), idesc, 1u);
-                  MmaF16(d, SmemDesc(aL + off), SmemDesc(bH + off), idesc, 1u);
+                  const uint32_t aH = tmem + kTmemAHi + 8u * (4 * kb + kk), aL = aH + (kTmemALo - kTmemAHi);
+                  MmaF16Ts(d, aH, SmemDesc(bH + off), idesc, (kb == 0 && kk == 0) ? 0u : 1u);
+                  MmaF16Ts(d, aH, SmemDesc(bL + off), idesc, 1u);
+                  MmaF16Ts(d, aL, SmemDesc(bH + off), idesc, 1u);
                }
                Commit(&sh->colEmpty[cs]);
             }
             if (!ok)
                break;
             Commit(&sh->colDone[j & 1]);
-            if (lastOfSet(j))
-               Commit(&sh->aFree);
          }
          if (!ok)
          {
@@ -486,26 +483,49 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
       // x = 16 w + i, part h (columns: y).
       const int h = (lane >> 4) & 1, y = 16 * warp + (lane & 15), x = y;
       const uint32_t quad = static_cast<uint32_t>(32 * warp) << 16;
+      // The DFT operand of a set into this warp's 32 TMEM lanes (rows 32 w + lane), both parts, 32 columns per store.
+      auto loadOperand = [&](int set) {
+         const uint4* src = reinterpret_cast<const uint4*>(prm.ahat + static_cast<size_t>(set) * kAImageBytes);
+         const int r = 32 * warp + lane;
+#pragma unroll 1
+         for (int part = 0; part < 2; ++part)
+#pragma unroll 1
+            for (int c0 = 0; c0 < kACols; c0 += 32)
+            {
+               uint32_t v[32];
+#pragma unroll
+               for (int g = 0; g < 8; ++g)
+               {
+                  const uint4 q = src[static_cast<size_t>(part * (kACols / 4) + c0 / 4 + g) * kRows + r];
+                  v[4 * g] = q.x;
+                  v[4 * g + 1] = q.y;
+                  v[4 * g + 2] = q.z;
+                  v[4 * g + 3] = q.w;
+               }
+               TmemStore32(tmem + quad + (part ? kTmemALo : kTmemAHi) + c0, v);
+            }
+         TmemWaitStore();
+      };
+      // T(j): wait for its row pass, then K block by K block from TMEM into the col-B stages; tFree when all is taken.
+      // The drain's waits spin without sleeping: its warps are on the critical path of both passes.
+      const float tScale = y < P ? kScaleT : 0.f;
       uint32_t colCount = 0;
-      for (int j = 0; j < nLocal && ok; ++j)
-      {
-         const uint32_t use = static_cast<uint32_t>(j >> 1) & 1u;
-         ok = __all_sync(0xffffffffu, MbarWait(&sh->rowDone[j & 1], use, err));
-         if (!ok)
-            break;
+      auto drainT = [&](int j) -> bool {
+         if (!__all_sync(0xffffffffu, MbarWait(&sh->rowDone, static_cast<uint32_t>(j) & 1u, err, false)))
+            return false;
          TcFenceAfter();
          for (int kb = 0; kb < nKb; ++kb, ++colCount)
          {
             const int cs = static_cast<int>(colCount % kColStages);
-            ok = __all_sync(0xffffffffu, MbarWait(&sh->colEmpty[cs], ((colCount / kColStages) & 1u) ^ 1u, err));
-            if (!ok)
-               break;
+            if (!__all_sync(0xffffffffu,
+                            MbarWait(&sh->colEmpty[cs], ((colCount / kColStages) & 1u) ^ 1u, err, false)))
+               return false;
             float v[32];
-            TmemLoad32(tmem + quad + kTmemRow + 128u * static_cast<uint32_t>(j & 1) + 32u * kb, v);
+            TmemLoad32(tmem + quad + kTmemRow + 32u * kb, v);
             uint32_t hi[16], lo[16];
 #pragma unroll
-            for (int c = 0; c < 16; ++c)
-               SplitH2(y < P ? v[2 * c] * kScaleT : 0.f, y < P ? v[2 * c + 1] * kScaleT : 0.f, hi[c], lo[c]);
+            for (int c = 0; c < 16; ++c)   // rows y >= P of T are exact zeros (so are those of the DFT operand)
+               SplitH2(v[2 * c] * tScale, v[2 * c + 1] * tScale, hi[c], lo[c]);
             // B[y][16 h + i] = part h of T[y][32 kb + i], B[y][32 + 16 h + i] = part h of T[y][32 kb + 16 + i]
             unsigned char* b = sColB + cs * kColStageBytes;
 #pragma unroll
@@ -521,16 +541,17 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
             if (lane == 0)
                MbarArrive(&sh->colFull[cs]);
          }
-         if (!ok)
-            break;
          TcFenceBefore();
          __syncwarp();
          if (lane == 0)
-            MbarArrive(&sh->tFree[j & 1]);
-         // ------------------------------------------------ |E|^2, the plane sum, the normalized plane
-         ok = __all_sync(0xffffffffu, MbarWait(&sh->colDone[j & 1], use, err));
-         if (!ok)
-            break;
+            MbarArrive(&sh->tFree);
+         return true;
+      };
+      // E(j): wait for its column pass, |E|^2, the plane sum, the normalized plane; eFree once E is in registers.
+      auto drainE = [&](int j) -> bool {
+         const uint32_t use = static_cast<uint32_t>(j >> 1) & 1u;
+         if (!__all_sync(0xffffffffu, MbarWait(&sh->colDone[j & 1], use, err, false)))
+            return false;
          TcFenceAfter();
          float I[64];
          float part[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};   // eight float partial sums of 8 values each
@@ -540,9 +561,9 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
             float vv[32];
             TmemLoad32(tmem + quad + kTmemCol + 64u * static_cast<uint32_t>(j & 1) + c0, vv);
 #pragma unroll
-            for (int c = 0; c < 32; ++c)
+            for (int c = 0; c < 32; ++c)   // |2^20 E|^2 = 2^40 |E|^2; the 2^-40 goes into the final scale
             {
-               const float me = vv[c] * kScaleE;
+               const float me = vv[c];
                const float o = __shfl_xor_sync(0xffffffffu, me, 16);
                const float e = me * me + o * o;
                I[c0 + c] = e;
@@ -569,18 +590,18 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
                sh->sum[j & 1][warp] = local;
                MbarArrive(&sh->red[j & 1]);
             }
-            ok = __all_sync(0xffffffffu, MbarWait(&sh->red[j & 1], use, err));
-            if (!ok)
-               break;
+            if (!__all_sync(0xffffffffu, MbarWait(&sh->red[j & 1], use, err, false)))
+               return false;
             const volatile double* s = sh->sum[j & 1];
             total = s[0] + s[1] + s[2] + s[3];
          }
-         // lanes 0-15 store rows y < 32 of column x, lanes 16-31 rows y >= 32; the plane times 1 / sum
+         // lanes 0-15 hold rows y < 32 of column x, lanes 16-31 rows y >= 32; the plane times 1 / sum (the float
+         // product is within an ulp or two of the float64 quotient)
+         float* plane = prm.out + static_cast<size_t>(psf0 + j) * P * P;
+         const float scale = (prm.normalize && total > 0.0) ? static_cast<float>(1.0 / total) : kScaleI;
+         const int y0 = 32 * h;
          if (x < P)
          {
-            float* plane = prm.out + static_cast<size_t>(psf0 + j) * P * P;
-            const float scale = (prm.normalize && total > 0.0) ? static_cast<float>(1.0 / total) : 1.0f;
-            const int y0 = 32 * h;
 #pragma unroll
             for (int c = 0; c < 32; ++c)
             {
@@ -590,6 +611,22 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
                   plane[static_cast<size_t>(yy) * P + x] = e * scale;
             }
          }
+         return true;
+      };
+      // T(j), then E(j): the column pass of PSF j follows the T drain K block by K block, and the row pass of PSF
+      // j + 1 starts once T(j) is taken. At a set change E of every earlier PSF has been taken, so both passes are
+      // complete and no MMA reads the operand being replaced.
+      for (int j = 0; j < nLocal && ok; ++j)
+      {
+         if (firstOfSet(j))
+         {
+            loadOperand(setOf(j));
+            TcFenceBefore();
+            __syncwarp();
+            if (lane == 0)
+               MbarArrive(&sh->aFull);
+         }
+         ok = drainT(j) && drainE(j);
       }
    }
    if (!ok)
@@ -607,13 +644,14 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
 
 bool F16x3Supports(int M, int P) { return M <= 128 && M % 16 == 0 && P <= 64 && P >= 1; }
 
-size_t AhatF16Bytes(int nSets) { return static_cast<size_t>(nSets) * kABytes; }
+size_t AhatF16Bytes(int nSets) { return static_cast<size_t>(nSets) * kAImageBytes; }
 
 int BuildAhatF16(iscu_ctx* ctx, const float2* A, const SetParams* sets, const double3* tables, int nSets, int M,
                  int P, unsigned char* out)
 {
-   AhatF16Kernel<<<dim3((kMaxKb * kRows * 32 + 255) / 256, nSets), 256, 0, ctx->stream>>>(A, M, P, out);
-   ISCU_CK_LAUNCH(ctx, "AhatF16Kernel");
+   AhatTmemKernel<<<dim3((kRows * kACols + 255) / 256, nSets), 256, 0, ctx->stream>>>(A, M, P,
+                                                                                  reinterpret_cast<uint32_t*>(out));
+   ISCU_CK_LAUNCH(ctx, "AhatTmemKernel");
    RevTableKernel<<<dim3((M * M + 255) / 256, nSets), 256, 0, ctx->stream>>>(
       sets, tables, M * M, reinterpret_cast<float2*>(out + AhatF16Bytes(nSets)));
    ISCU_CK_LAUNCH(ctx, "RevTableKernel");
