@@ -153,20 +153,6 @@ __device__ __forceinline__ void TmemLoad16(uint32_t taddr, float* v)
       v[i] = __uint_as_float(r[i]);
 }
 
-// A bulk copy of `bytes` from this CTA's shared memory to global memory (both 16-byte aligned, bytes a multiple of
-// 16), in the issuing thread's current bulk group; BulkStoreCommit closes the group.
-__device__ __forceinline__ void BulkStore(void* dst, const void* src, uint32_t bytes)
-{
-   asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(SmemAddr(src)),
-                "r"(bytes)
-                : "memory");
-}
-__device__ __forceinline__ void BulkStoreCommit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-// Waits until the issuing thread's bulk groups have finished reading their shared memory.
-__device__ __forceinline__ void BulkStoreWaitRead() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
-// Waits until the issuing thread's bulk groups are complete.
-__device__ __forceinline__ void BulkStoreWait() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-
 // v[0..31] into 32 consecutive TMEM columns of this warp's 32 lanes (thread = lane); the caller waits with
 // TmemWaitStore before another thread may rely on them.
 __device__ __forceinline__ void TmemStore32(uint32_t taddr, const uint32_t* v)
