@@ -259,7 +259,8 @@ class Engine:
 
     # -------------------------------------------------------------------------------------------- PSF
     def psf_library_dev(self, sets, set_of_psf, defocus_nm, size=0, normalize=True, method=CZT_FP32, out=None):
-        """A PSF library (n, P, P) float32 CUDA tensor; see iscu_psf_library_dev."""
+        """A PSF library (n, P, P) float32 CUDA tensor; see iscu_psf_library_dev. method: CZT_FP32 (any size),
+        CZT_F16X3 or CZT_TF32X3 (the tensor-core forms: pupil samples M <= 128, a multiple of 16, planes <= 64 x 64)."""
         import torch
         reqs = (PsfRequest * len(sets))(*[s.c() for s in sets])
         so = np.ascontiguousarray(set_of_psf, dtype=np.uint32)
@@ -661,7 +662,8 @@ class RenderGraph:
 
 
 class PsfPlan:
-    """iscu_psf_plan: the per-set PSF work done once; runs over (set index, defocus nm) lists."""
+    """iscu_psf_plan: the per-set PSF work done once; runs over (set index, defocus nm) lists. method as for
+    Engine.psf_library_dev."""
 
     def __init__(self, engine: Engine, sets, size=0, method=CZT_FP32):
         self.engine = engine
