@@ -114,6 +114,25 @@ def _ptr(a) -> C.c_void_p:
     return C.c_void_p(a.data_ptr())   # torch tensor
 
 
+def _require_tensor(t, name: str, dtypes, device, min_numel: int):
+    """ValueError unless t is a contiguous torch tensor of one of `dtypes` (torch dtypes) with at least min_numel
+    elements, on CUDA device `device` (None: in host memory), so the library never writes past a caller's buffer."""
+    import torch
+    where = f"cuda:{device}" if device is not None else "the host"
+    ok = (isinstance(t, torch.Tensor) and t.dtype in dtypes and t.is_contiguous() and t.numel() >= min_numel and
+          (t.is_cuda and t.device.index == device if device is not None else not t.is_cuda))
+    if not ok:
+        names = " or ".join(str(d).replace("torch.", "") for d in dtypes)
+        raise ValueError(f"{name} must be a contiguous {names} tensor on {where} with at least {min_numel} elements")
+
+
+def _require_array(a, name: str, dtype, min_size: int):
+    """ValueError unless a is a C-contiguous numpy array of dtype with at least min_size elements."""
+    if not (isinstance(a, np.ndarray) and a.dtype == dtype and a.flags.c_contiguous and a.size >= min_size):
+        raise ValueError(f"{name} must be a C-contiguous {np.dtype(dtype).name} array with at least {min_size} "
+                         "elements")
+
+
 def _n_records(a) -> int:
     """EMITTER_DTYPE records in a device (torch, any dtype viewed as bytes) or host emitter buffer."""
     if a is None:
@@ -265,9 +284,12 @@ class Engine:
         reqs = (PsfRequest * len(sets))(*[s.c() for s in sets])
         so = np.ascontiguousarray(set_of_psf, dtype=np.uint32)
         dz = np.ascontiguousarray(defocus_nm, dtype=np.float64)
+        if len(dz) != len(so):
+            raise ValueError(f"defocus_nm has {len(dz)} entries, set_of_psf {len(so)}")
         P = size if size > 0 else sets[0].geometry()[0]
         if out is None:
             out = torch.empty((len(so), P, P), dtype=torch.float32, device=f"cuda:{self.device}")
+        _require_tensor(out, "out", (torch.float32,), self.device, len(so) * P * P)
         check(self.lib.iscu_psf_library_dev(self.h, reqs, len(sets), _ptr(so), _ptr(dz), len(so), size,
                                             int(normalize), method, _ptr(out)))
         return out
@@ -282,10 +304,7 @@ class Engine:
         if len(dz) != len(so):
             raise ValueError(f"defocus_nm has {len(dz)} entries, set_of_psf {len(so)}")
         P = size if size > 0 else sets[0].geometry()[0]
-        if not (isinstance(out, torch.Tensor) and out.dtype == torch.float32 and out.is_cuda
-                and out.device.index == self.device and out.is_contiguous() and out.numel() >= len(so) * P * P):
-            raise ValueError(f"out must be a contiguous float32 tensor on cuda:{self.device} with at least "
-                             f"{len(so)} x {P} x {P} elements")
+        _require_tensor(out, "out", (torch.float32,), self.device, len(so) * P * P)
         check(self.lib.iscu_psf_library_noalloc_dev(self.h, reqs, len(sets), _ptr(so), _ptr(dz), len(so), size,
                                                     int(normalize), _ptr(out)))
         return out
@@ -691,7 +710,12 @@ class PsfPlan:
 
     def run_dev(self, set_of_dev, defocus_nm_dev, out_dev, normalize=True, sync=True):
         """set_of_dev: int32/uint32 CUDA tensor, defocus_nm_dev: float64 CUDA tensor, out_dev: (n, P, P) float32."""
+        import torch
         n = int(set_of_dev.numel())
+        dev = self.engine.device
+        _require_tensor(set_of_dev, "set_of_dev", (torch.int32, torch.uint32), dev, n)
+        _require_tensor(defocus_nm_dev, "defocus_nm_dev", (torch.float64,), dev, n)
+        _require_tensor(out_dev, "out_dev", (torch.float32,), dev, n * self.P * self.P)
         self.engine._before(sync)
         check(self.lib.iscu_psf_plan_run_dev(self.h, _ptr(set_of_dev), _ptr(defocus_nm_dev), n, int(normalize),
                                              _ptr(out_dev)))
@@ -705,8 +729,11 @@ class PsfPlan:
     def run(self, set_of, defocus_nm, normalize=True, out=None):
         so = np.ascontiguousarray(set_of, dtype=np.uint32)
         dz = np.ascontiguousarray(defocus_nm, dtype=np.float64)
+        if len(dz) != len(so):
+            raise ValueError(f"defocus_nm has {len(dz)} entries, set_of {len(so)}")
         if out is None:
             out = np.empty((len(so), self.P, self.P), np.float32)
+        _require_array(out, "out", np.float32, len(so) * self.P * self.P)
         check(self.lib.iscu_psf_plan_run(self.h, _ptr(so), _ptr(dz), len(so), int(normalize), _ptr(out)))
         return out
 

@@ -17,7 +17,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from ._abi import NllSpec as _NllSpecC
-from .engine import Engine, IscuError, _ptr, check
+from .engine import Engine, IscuError, _ptr, _require_tensor, check
 
 
 @dataclass
@@ -71,7 +71,25 @@ class NllModel:
     def run_dev(self, params, frame, bg, zern, counts, nll, err, g_params=None, g_bg=None, g_zern=None, mu=None,
                 sync=True):
         """iscu_nll_eval_dev on prepared CUDA tensors (params (n, 4) float32, frame int32, bg float32, counts float32,
-        nll 1 float64, err 1 int32; the gradient outputs when g_params is given); zern a float64 numpy array."""
+        nll 1 float64, err 1 int32; the gradient outputs when g_params is given); zern a float64 numpy array. Every
+        buffer is checked (dtype, device, contiguity, size) before the call, so none is read or written past."""
+        import torch
+        n, nf, R, dev = int(params.shape[0]), int(bg.shape[0]), self.spec.roi, self.engine.device
+        if not (isinstance(zern, np.ndarray) and zern.dtype == np.float64 and zern.flags.c_contiguous
+                and zern.size == self.n_zern):
+            raise ValueError(f"zern must be a C-contiguous float64 array of {self.n_zern} coefficients")
+        _require_tensor(params, "params", (torch.float32,), dev, 4 * n)
+        _require_tensor(frame, "frame", (torch.int32,), dev, n)
+        _require_tensor(bg, "bg", (torch.float32,), dev, nf)
+        _require_tensor(counts, "counts", (torch.float32,), dev, n * R * R)
+        _require_tensor(nll, "nll", (torch.float64,), dev, 1)
+        _require_tensor(err, "err", (torch.int32,), dev, 1)
+        if mu is not None:
+            _require_tensor(mu, "mu", (torch.float32,), dev, n * R * R)
+        if g_params is not None:
+            _require_tensor(g_params, "g_params", (torch.float32,), dev, 4 * n)
+            _require_tensor(g_bg, "g_bg", (torch.float64,), dev, nf)
+            _require_tensor(g_zern, "g_zern", (torch.float64,), dev, self.n_zern)
         self.engine._before(sync)
         check(self.lib.iscu_nll_eval_dev(self.h, params.shape[0], _ptr(params), _ptr(frame), bg.shape[0], _ptr(bg),
                                          zern.ctypes.data_as(C.POINTER(C.c_double)), _ptr(counts), _ptr(mu),
@@ -90,7 +108,11 @@ class NllModel:
         counts = counts.to(torch.float32).contiguous()
         z = np.ascontiguousarray(np.asarray(zern.detach().cpu() if hasattr(zern, "detach") else zern,
                                             dtype=np.float64))
-        n, nf = params.shape[0], bg.shape[0]
+        n, nf, R = params.shape[0], bg.shape[0], self.spec.roi
+        if params.numel() != 4 * n or frame.numel() != n or counts.numel() != n * R * R or z.size != self.n_zern:
+            raise ValueError(f"expected params (n, 4), frame (n,), counts (n, {R}, {R}) and {self.n_zern} Zernike "
+                             f"coefficients; got {tuple(params.shape)}, {tuple(frame.shape)}, {tuple(counts.shape)}, "
+                             f"{z.size}")
         nll = torch.zeros(1, dtype=torch.float64, device=dev)
         err = torch.zeros(1, dtype=torch.int32, device=dev)
         mu = torch.empty_like(counts) if want_mu else None
