@@ -228,4 +228,58 @@ __device__ __forceinline__ double CounterGamma(double k, CounterRng& u)
    return d;
 }
 
+// CounterGamma's draw with its decisions taken in float32 where each is sure: every iteration's normal from
+// DrawGauss (within kGaussFastErr of CounterGauss's value of the same uniforms), then the sign of t = 1 + c x, the
+// squeeze w < 1 - 0.0331 x^4 and the logarithmic test log w < x^2 / 2 + d (1 - v + log v), each taken only when no
+// normal within that error could decide it the other way. The draws are CounterGamma's, in its order, so the stream
+// ends where CounterGamma leaves it. true: out = d v within outErr of CounterGamma's value. false: a decision was in
+// doubt (about one iteration in 10^4); the caller draws again from its saved stream with CounterGamma. Taking the
+// logarithmic test here too matters: the squeeze alone fails for ~10 % of draws (E[0.0331 x^4] = 0.1), which would
+// send nearly every warp down the float64 path as well.
+__device__ __forceinline__ bool GammaSure(double k, CounterRng& u, double& out, double& outErr)
+{
+   const double d = k - 1.0 / 3.0, c = 1.0 / sqrt(9.0 * d);
+   const double e = kGaussFastErr, dt = c * e;
+   for (int it = 0; it < 1000; ++it)
+   {
+      const GaussDraw g = DrawGauss(u);
+      const double x = static_cast<double>(g.gf), t = 1.0 + c * x;
+      if (t + dt <= 0.0)   // t <= 0 for every normal within e of x: CounterGamma draws again
+         continue;
+      if (!(t - dt > 0.0))
+         return false;
+      const double tt = t + dt, v = t * t * t, dv = 3.0 * tt * tt * dt + 1e-15 * v;
+      const double w = u.Uniform();
+      const double ax = fabs(x) + e;
+      const double s = 1.0 - 0.0331 * x * x * x * x, ds = 4.0 * 0.0331 * ax * ax * ax * e + 1e-12;
+      if (w < s - ds)
+      {
+         out = d * v;
+         outErr = d * dv + 1e-12 * out;
+         return true;
+      }
+      if (!(w >= s + ds))
+         return false;
+      // log w: w is a 24-bit value, exact in float, and logf is within 1 ulp (bounded here at 4). log v from logf of
+      // v's float value (relative rounding 2^-24, so 6e-8 in the logarithm). The normal's error reaches the right side
+      // through x^2 / 2 (at most (|x| + e) e) and through v (d (1 - v + log v) / dv = 1 / v - 1, bounded with slack).
+      const double lw = static_cast<double>(logf(static_cast<float>(w)));
+      const double lv = static_cast<double>(logf(static_cast<float>(v)));
+      const double rhs = 0.5 * x * x + d * (1.0 - v + lv);
+      const double m = 4.8e-7 * fabs(lw) + ax * e + d * ((fabs(1.0 / v - 1.0) + dv / v) * dv + 6e-8 + 4.8e-7 * fabs(lv)) +
+                       1e-12 * (1.0 + d);
+      if (lw < rhs - m)
+      {
+         out = d * v;
+         outErr = d * dv + 1e-12 * out;
+         return true;
+      }
+      if (!(lw > rhs + m))
+         return false;
+   }
+   out = d;
+   outErr = 0.0;
+   return true;
+}
+
 } // namespace iscu

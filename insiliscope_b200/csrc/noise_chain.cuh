@@ -20,17 +20,39 @@ __device__ __forceinline__ uint16_t NoisePixel(float photonValue, uint32_t i, co
    if (cam.emccd)
    {
       const double ne = CounterPoisson(photons * cam.qe + cam.dark + cam.cic, u);
-      const double out = ne > 0.0 ? CounterGamma(ne, u) : 0.0;
       const double readE = (st.readNoise ? static_cast<double>(st.readNoise[i]) : cam.readNoise) / cam.emGain;
       const double gain = st.gain ? static_cast<double>(st.gain[i]) : cam.gain;
       const double offset = st.offset ? static_cast<double>(st.offset[i]) : 0.0;
-      // the rounding (before the clamp) from the float32 normal when no boundary is within |readE / gain|
-      // kGaussFastErr of it, else from the float64 one
-      const GaussDraw d = DrawGauss(u);
+      // The register's Gamma with float32 decisions (GammaSure), else CounterGamma from the saved stream; then the
+      // rounding (before the clamp) from the float32 read-noise normal when no boundary is within the bound of both
+      // float32 errors, else the Gamma (if it was not exact) and the normal again in float64 from the saved stream.
+      const CounterRng saved = u;
+      double out = 0.0, outErr = 0.0;
+      bool exact = true;
+      if (ne > 0.0)
+      {
+         exact = !GammaSure(ne, u, out, outErr);
+         if (exact)
+         {
+            u = saved;
+            out = CounterGamma(ne, u);
+            outErr = 0.0;
+         }
+      }
+      GaussDraw d = DrawGauss(u);
       const double af = offset + (out + readE * static_cast<double>(d.gf)) / gain;
+      const double m = (outErr + fabs(readE) * kGaussFastErr) / fabs(gain) + 1e-9 * (1.0 + fabs(af));
       double adu;
-      if (!RoundsSurely(af, fabs(readE / gain) * kGaussFastErr + 1e-9 * (1.0 + fabs(af)), adu))
+      if (!RoundsSurely(af, m, adu))
+      {
+         if (!exact)
+         {
+            u = saved;
+            out = CounterGamma(ne, u);
+            d = DrawGauss(u);
+         }
          adu = floor(offset + (out + readE * GaussExact(d)) / gain + 0.5);
+      }
       return static_cast<uint16_t>(adu < 0.0 ? 0.0 : (adu > cam.maxAdu ? cam.maxAdu : adu));
    }
    const double ne = CounterPoisson(photons * cam.qe + cam.dark, u);
