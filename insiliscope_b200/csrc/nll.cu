@@ -147,26 +147,31 @@ struct NllArgs
 struct NllSmem
 {
    float2 A[kP][kM];
+   float2 At[kM][kP];     // A transposed: the first product reads it along rows (conflict-free) instead of down A's
+                          // columns (16 lanes 256 bytes apart, one bank)
    float2 U[kM][kM];
    float2 T[kM][kP];
    float2 E[kP][kP];
    float dphi[kM * kM];
+   double dphiSum[kM * kM];   // the CTA's emitters' dNLL/dphi, summed in float64, for the Zernike gradient
    double red[kThreads / 32];
 };
 
 template <bool kGrad>
-__global__ void __launch_bounds__(kThreads) NllKernel(NllArgs a)
+__global__ void __launch_bounds__(kThreads, 2) NllKernel(NllArgs a)
 {
    extern __shared__ __align__(16) unsigned char smemRaw[];
    NllSmem& s = *reinterpret_cast<NllSmem*>(smemRaw);
    const int tid = threadIdx.x;
    for (int i = tid; i < kP * kM; i += kThreads)
+   {
       s.A[i / kM][i % kM] = a.A[i];
-   // the Zernike gradient: warp w accumulates modes j = w, w + 8, ... across the CTA's emitters
-   double gz[kMaxJ / (kThreads / 32)];
-#pragma unroll
-   for (int q = 0; q < kMaxJ / (kThreads / 32); ++q)
-      gz[q] = 0.0;
+      s.At[i % kM][i / kM] = a.A[i];
+   }
+   // the Zernike gradient is linear in dNLL/dphi: the CTA sums dphi over its emitters (float64, each sample by one
+   // thread) and projects the sum onto the modes once, at the end
+   for (int m = tid; m < kM * kM; m += kThreads)
+      s.dphiSum[m] = 0.0;
    double nllAcc = 0.0;
    const int R = a.R, os = a.os, RR = R * R;
    __syncthreads();
@@ -191,7 +196,7 @@ __global__ void __launch_bounds__(kThreads) NllKernel(NllArgs a)
       }
       __syncthreads();
       // 2. T = U A^T (32 x 64), 3. E = A T (64 x 64)
-      SmemGemm<kM, kP, kM>([&](int r, int k) { return s.U[r][k]; }, [&](int k, int c) { return s.A[c][k]; },
+      SmemGemm<kM, kP, kM>([&](int r, int k) { return s.U[r][k]; }, [&](int k, int c) { return s.At[k][c]; },
                            [&](int r, int c, float2 v) { s.T[r][c] = v; });
       __syncthreads();
       SmemGemm<kP, kP, kM>([&](int r, int k) { return s.A[r][k]; }, [&](int k, int c) { return s.T[k][c]; },
@@ -263,6 +268,7 @@ __global__ void __launch_bounds__(kThreads) NllKernel(NllArgs a)
          gx -= d * sm.x;
          gy -= d * sm.y;
          gzd += d * sm.z;
+         s.dphiSum[m] += d;
       }
       gx = BlockSum(gx, s.red);
       gy = BlockSum(gy, s.red);
@@ -270,21 +276,6 @@ __global__ void __launch_bounds__(kThreads) NllKernel(NllArgs a)
       if (tid == 0)
          a.gParams[e] = make_float4(static_cast<float>(gx), static_cast<float>(gy), static_cast<float>(gzd),
                                     static_cast<float>(gN));
-      {
-         const int lane = tid & 31, warp = tid >> 5;
-#pragma unroll
-         for (int q = 0; q < kMaxJ / (kThreads / 32); ++q)
-         {
-            const int j = warp + q * (kThreads / 32);
-            if (j >= a.J)
-               break;
-            const double* Zj = a.basis + static_cast<size_t>(j) * kM * kM;
-            double acc = 0.0;
-            for (int m = lane; m < kM * kM; m += 32)
-               acc += static_cast<double>(s.dphi[m]) * Zj[m];
-            gz[q] += acc;
-         }
-      }
       __syncthreads();
    }
    // the CTA's sums
@@ -293,14 +284,15 @@ __global__ void __launch_bounds__(kThreads) NllKernel(NllArgs a)
       atomicAdd(a.nll, nllCta);
    if (kGrad)
    {
+      // warp w projects the summed dphi onto modes j = w, w + 8, ...
+      __syncthreads();
       const int lane = tid & 31, warp = tid >> 5;
-#pragma unroll
-      for (int q = 0; q < kMaxJ / (kThreads / 32); ++q)
+      for (int j = warp; j < a.J; j += kThreads / 32)
       {
-         const int j = warp + q * (kThreads / 32);
-         if (j >= a.J)
-            break;
-         double v = gz[q];
+         const double* Zj = a.basis + static_cast<size_t>(j) * kM * kM;
+         double v = 0.0;
+         for (int m = lane; m < kM * kM; m += 32)
+            v += s.dphiSum[m] * Zj[m];
 #pragma unroll
          for (int d = 16; d > 0; d >>= 1)
             v += __shfl_xor_sync(0xffffffffu, v, d);
