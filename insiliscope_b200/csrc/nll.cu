@@ -92,6 +92,34 @@ __device__ __forceinline__ void SmemGemm(LF L, RF R, EF epi)
          epi(ty + 16 * i, tx + 16 * j, acc[i][j]);
 }
 
+// Sums of NV float64 values over the CTA in one exchange, each in BlockSum's order (every thread calls it; every
+// thread gets the sums). red: NV x (kThreads / 32) doubles.
+template <int NV>
+__device__ __forceinline__ void BlockSums(double (&v)[NV], double* red)
+{
+#pragma unroll
+   for (int q = 0; q < NV; ++q)
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1)
+         v[q] += __shfl_xor_sync(0xffffffffu, v[q], d);
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   __syncthreads();
+   if (lane == 0)
+#pragma unroll
+      for (int q = 0; q < NV; ++q)
+         red[q * (kThreads / 32) + warp] = v[q];
+   __syncthreads();
+#pragma unroll
+   for (int q = 0; q < NV; ++q)
+   {
+      double t = 0.0;
+#pragma unroll
+      for (int w = 0; w < kThreads / 32; ++w)
+         t += red[q * (kThreads / 32) + w];
+      v[q] = t;
+   }
+}
+
 // Sum over the CTA in float64 (every thread calls it; the result is returned to every thread).
 __device__ __forceinline__ double BlockSum(double v, double* red)
 {
@@ -154,7 +182,7 @@ struct NllSmem
    float2 E[kP][kP];
    float dphi[kM * kM];
    double dphiSum[kM * kM];   // the CTA's emitters' dNLL/dphi, summed in float64, for the Zernike gradient
-   double red[kThreads / 32];
+   double red[3 * (kThreads / 32)];
 };
 
 template <bool kGrad>
@@ -241,8 +269,10 @@ __global__ void __launch_bounds__(kThreads, 2) NllKernel(NllArgs a)
          __syncthreads();
          continue;
       }
-      gN = BlockSum(gN, s.red);
-      gB = BlockSum(gB, s.red);
+      double nb[2] = {gN, gB};   // one exchange for both sums
+      BlockSums<2>(nb, s.red);
+      gN = nb[0];
+      gB = nb[1];
       if (tid == 0 && frameOk)
          atomicAdd(&a.gBg[f], gB);
       __syncthreads();
@@ -270,9 +300,11 @@ __global__ void __launch_bounds__(kThreads, 2) NllKernel(NllArgs a)
          gzd += d * sm.z;
          s.dphiSum[m] += d;
       }
-      gx = BlockSum(gx, s.red);
-      gy = BlockSum(gy, s.red);
-      gzd = BlockSum(gzd, s.red);
+      double xyz[3] = {gx, gy, gzd};
+      BlockSums<3>(xyz, s.red);
+      gx = xyz[0];
+      gy = xyz[1];
+      gzd = xyz[2];
       if (tid == 0)
          a.gParams[e] = make_float4(static_cast<float>(gx), static_cast<float>(gy), static_cast<float>(gzd),
                                     static_cast<float>(gN));
