@@ -33,6 +33,35 @@ def test_fixture_planes(engine, golden_dir, method):
             assert np.argmax(got[z]) == np.argmax(want[z])
 
 
+@pytest.mark.parametrize("method", [CZT_TF32X3, CZT_F16X3])
+def test_split_unnormalized_vs_oracle(engine, oracle, method):
+    """Unnormalized planes (|E|^2 itself, no sum-1 division) from the tensor-core forms: the FP16 form's operands and
+    accumulators carry exact power-of-two scales that only the normalization would otherwise cancel."""
+    req = PsfParams(wavelength_nm=670.0, na=1.45, pixel_size_nm=100.0, oversampling=4, kernel_half_width_px=8, nz=3,
+                    pupil_samples=128)
+    dz = np.array([-600.0, 0.0, 450.0])
+    got = engine.psf_library_dev([req], [0, 0, 0], dz, size=64, normalize=False, method=method).cpu().numpy()
+    want = oracle.psf_planes(req, dz * 1e-9, size=64, normalize=False)
+    assert _max_rel(got, want) <= TOL
+
+
+@pytest.mark.parametrize("method", [CZT_TF32X3, CZT_F16X3])
+def test_split_beyond_staged_items(engine, method):
+    """More than 96 PSFs per CTA (the tensor-core kernels stage the first 96 items' sets and defocus factors in shared
+    memory and read the rest from global memory), three request sets in random order (a set change at most PSFs),
+    against the plain FP32 form."""
+    rng = np.random.default_rng(11)
+    sets = [PsfParams(wavelength_nm=wl, na=1.4, pixel_size_nm=100.0, oversampling=2, kernel_half_width_px=8, nz=3,
+                      pupil_samples=64) for wl in (520.0, 600.0, 700.0)]
+    n = 15000
+    set_of = rng.integers(0, 3, n).astype(np.uint32)
+    dz = rng.uniform(-600.0, 600.0, n)
+    a = engine.psf_library_dev(sets, set_of, dz, size=33, method=CZT_FP32).cpu().numpy()
+    b = engine.psf_library_dev(sets, set_of, dz, size=33, method=method).cpu().numpy()
+    err = np.abs(a - b).max(axis=(1, 2)) / a.max(axis=(1, 2))
+    assert err.max() <= 2 * TOL, (int(err.argmax()), float(err.max()))
+
+
 @pytest.mark.parametrize("method", [CZT_FP32, CZT_TF32X3, CZT_F16X3])
 def test_library_vs_oracle(engine, oracle, method):
     """The library config's shape (M = 128 pupil -> 64 x 64 at 4x oversampling) with Noll 4-15 aberrations, four
