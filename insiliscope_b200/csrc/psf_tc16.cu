@@ -48,7 +48,7 @@ namespace {
 
 using namespace tc;
 
-constexpr int kThreads = 512;
+constexpr int kThreads = 640;
 constexpr int kRows = 128;                        // UMMA M (2P rows, padded)
 constexpr int kImgBytes = 128 * 128;              // one B operand image: 128 rows x 64 FP16 (128 B per row)
 constexpr int kKbBytes = 2 * kImgBytes;           // a row-pass B block: its hi and lo images
@@ -62,11 +62,12 @@ constexpr float kScaleOp = 4096.0f;               // 2^12: the DFT operand and t
 constexpr float kScaleT = 1.0f / 65536.0f;        // 2^-16: 2^24 T -> 2^8 T
 constexpr float kScaleI = 0x1p-40f;               // 2^-40: |2^20 E|^2 -> |E|^2 (unnormalized planes)
 
-// Warp roles. Warps share an SM sub-partition (scheduler) when equal mod 4.
-constexpr int kDrainWarps = 4;                    // warps 0-3, one per TMEM lane quadrant
-constexpr int kRowMmaWarp = 4;                    // lane 0: the row-pass MMAs
-constexpr int kColMmaWarp = 8;                    // lane 0: the column-pass MMAs
-constexpr int kProducerWarps = 10;                // warps 5-7 and 9-15 make the pupil phasors
+// Warp roles. Warps share an SM sub-partition (scheduler) when equal mod 4, and warp w reaches TMEM lanes
+// [32 (w % 4), +32) only.
+constexpr int kDrainWarps = 8;                    // warps 0-7: two per TMEM lane quadrant, each half the columns
+constexpr int kRowMmaWarp = 8;                    // lane 0: the row-pass MMAs
+constexpr int kColMmaWarp = 12;                   // lane 0: the column-pass MMAs
+constexpr int kProducerWarps = 10;                // warps 9-11 and 13-19 make the pupil phasors
 constexpr int kProducerThreads = 32 * kProducerWarps;
 constexpr int kItemsPerBlock = 512;               // (pupil column, 8 pupil rows) items of one row-pass K block
 constexpr int kTmemAHi = 0;                       // the DFT operand's hi part: columns [0, 128)
@@ -77,8 +78,8 @@ constexpr int kSetCache = 96;                     // PSFs whose set and defocus 
 
 static_assert(kItemsPerBlock <= 2 * kProducerThreads, "a producer thread makes at most two items per K block");
 
-// A producer warp's index 0..9 (warps 5-7, 9-15).
-__device__ __forceinline__ int ProducerIndex(int warp) { return warp - 5 - (warp > kColMmaWarp ? 1 : 0); }
+// A producer warp's index 0..9 (warps 9-11, 13-19).
+__device__ __forceinline__ int ProducerIndex(int warp) { return warp - 9 - (warp > kColMmaWarp ? 1 : 0); }
 
 // Instruction descriptor, kind::f16: D float32, A and B FP16, both K-major, M x N.
 __host__ __device__ constexpr uint32_t InstrDescF16(int M, int N)
@@ -214,18 +215,18 @@ constexpr size_t kSmemBytes = static_cast<size_t>(kRowStages) * kKbBytes +
 static_assert(kSmemBytes <= 227 * 1024, "the FP16 chirp-Z kernel's shared memory");
 
 // Per CTA, persistent over a contiguous run of PSFs, warp-specialized; the roles meet only at mbarriers:
-//   producers (warps 5-7, 9-15): per row-pass K block the pupil phasors of 32 pupil rows (float32 phase in
+//   producers (warps 9-11, 13-19): per row-pass K block the pupil phasors of 32 pupil rows (float32 phase in
 //     revolutions reduced exactly, float32 sine and cosine, times 2^12, FP16 hi/lo split) into a row-B stage ->
 //     rowFull; the phase-table entries of a thread's next item are in flight while it computes the current one;
-//   the row-pass thread (warp 4, lane 0): per PSF its row pass R(j), K block by K block as the producers fill the
+//   the row-pass thread (warp 8, lane 0): per PSF its row pass R(j), K block by K block as the producers fill the
 //     stages, into T's columns once the drain warps have taken T(j - 1) (tFree), with the set's DFT operand from TMEM
 //     (aFull at the first PSF of each run of one set); commits free the stages and mark the pass done (rowDone);
-//   the column-pass thread (warp 8, lane 0): per PSF its column pass C(j) into E's buffer j % 2 once E(j - 2) has
+//   the column-pass thread (warp 12, lane 0): per PSF its column pass C(j) into E's buffer j % 2 once E(j - 2) has
 //     been taken (eFree), K block by K block as the drain warps fill the col-B stages; commits colEmpty / colDone;
-//   drain warps (0-3, one TMEM lane quadrant each): T of PSF j from TMEM, times 2^-16, split, into col-B stages ->
-//     colFull (then tFree); then E of PSF j: |E|^2, the plane sum, the normalized plane (eFree). At the
-//     first PSF of each set's run (E of the previous PSF taken: both passes of every earlier PSF complete) the set's
-//     DFT operand from global memory into TMEM (aFull).
+//   drain warps (0-7, two per TMEM lane quadrant, each half of every block's columns): T of PSF j from TMEM, times
+//     2^-16, split, into col-B stages -> colFull (then tFree); then E of PSF j: |E|^2, the plane sum, the normalized
+//     plane (eFree). At the first PSF of each set's run (E of the previous PSF taken: both passes of every earlier
+//     PSF complete) the set's DFT operand from global memory into TMEM (aFull).
 // R(j + 1) runs beside C(j) on the tensor pipe. Every wait is bounded (kWaitNs) and also ends when another role has
 // failed (Shared16::err); a failed CTA stops issuing, waits for its MMAs in flight, frees TMEM and reports through
 // prm.error.
@@ -479,35 +480,39 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
    else if (warp < kDrainWarps)
    {
       // ---------------------------------------------------------------- drain warps
-      // TMEM lane r = 32 w + 16 h + i of T holds row y = 16 w + i, part h (columns: the pupil column m); of E, output
-      // x = 16 w + i, part h (columns: y).
-      const int h = (lane >> 4) & 1, y = 16 * warp + (lane & 15), x = y;
-      const uint32_t quad = static_cast<uint32_t>(32 * warp) << 16;
-      // The DFT operand of a set into this warp's 32 TMEM lanes (rows 32 w + lane), both parts, 32 columns per store.
+      // Warp w drains TMEM lane quadrant q = w % 4, columns half w / 4 of each block. TMEM lane r = 32 q + 16 h + i of
+      // T holds row y = 16 q + i, part h (columns: the pupil column m); of E, output x = 16 q + i, part h (columns:
+      // y).
+      const int q = warp & 3, half = warp >> 2;
+      const int h = (lane >> 4) & 1, y = 16 * q + (lane & 15), x = y;
+      const uint32_t quad = static_cast<uint32_t>(32 * q) << 16;
+      // The DFT operand of a set into this quadrant's 32 TMEM lanes (rows 32 q + lane): both parts, this warp's half
+      // of the columns, 32 columns per store.
       auto loadOperand = [&](int set) {
          const uint4* src = reinterpret_cast<const uint4*>(prm.ahat + static_cast<size_t>(set) * kAImageBytes);
-         const int r = 32 * warp + lane;
+         const int r = 32 * q + lane;
 #pragma unroll 1
          for (int part = 0; part < 2; ++part)
 #pragma unroll 1
-            for (int c0 = 0; c0 < kACols; c0 += 32)
+            for (int c0 = half * (kACols / 2); c0 < (half + 1) * (kACols / 2); c0 += 32)
             {
                uint32_t v[32];
 #pragma unroll
                for (int g = 0; g < 8; ++g)
                {
-                  const uint4 q = src[static_cast<size_t>(part * (kACols / 4) + c0 / 4 + g) * kRows + r];
-                  v[4 * g] = q.x;
-                  v[4 * g + 1] = q.y;
-                  v[4 * g + 2] = q.z;
-                  v[4 * g + 3] = q.w;
+                  const uint4 w4 = src[static_cast<size_t>(part * (kACols / 4) + c0 / 4 + g) * kRows + r];
+                  v[4 * g] = w4.x;
+                  v[4 * g + 1] = w4.y;
+                  v[4 * g + 2] = w4.z;
+                  v[4 * g + 3] = w4.w;
                }
                TmemStore32(tmem + quad + (part ? kTmemALo : kTmemAHi) + c0, v);
             }
          TmemWaitStore();
       };
-      // T(j): wait for its row pass, then K block by K block from TMEM into the col-B stages; tFree when all is taken.
-      // The drain's waits spin without sleeping: its warps are on the critical path of both passes.
+      // T(j): wait for its row pass, then K block by K block from TMEM into the col-B stages (this warp: pupil
+      // columns 32 kb + 16 half .. + 15); tFree when all is taken. The drain's waits spin without sleeping: its warps
+      // are on the critical path of both passes.
       const float tScale = y < P ? kScaleT : 0.f;
       uint32_t colCount = 0;
       auto drainT = [&](int j) -> bool {
@@ -520,18 +525,18 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
             if (!__all_sync(0xffffffffu,
                             MbarWait(&sh->colEmpty[cs], ((colCount / kColStages) & 1u) ^ 1u, err, false)))
                return false;
-            float v[32];
-            TmemLoad32(tmem + quad + kTmemRow + 32u * kb, v);
-            uint32_t hi[16], lo[16];
+            float v[16];
+            TmemLoad16(tmem + quad + kTmemRow + 32u * kb + 16u * half, v);
+            uint32_t hi[8], lo[8];
 #pragma unroll
-            for (int c = 0; c < 16; ++c)   // rows y >= P of T are exact zeros (so are those of the DFT operand)
+            for (int c = 0; c < 8; ++c)   // rows y >= P of T are exact zeros (so are those of the DFT operand)
                SplitH2(v[2 * c] * tScale, v[2 * c + 1] * tScale, hi[c], lo[c]);
-            // B[y][16 h + i] = part h of T[y][32 kb + i], B[y][32 + 16 h + i] = part h of T[y][32 kb + 16 + i]
+            // B[y][32 half + 16 h + i] = part h of T[y][32 kb + 16 half + i]
             unsigned char* b = sColB + cs * kColStageBytes;
 #pragma unroll
-            for (int g = 0; g < 4; ++g)
+            for (int g = 0; g < 2; ++g)
             {
-               const int col = 32 * (g >> 1) + 16 * h + 8 * (g & 1);
+               const int col = 32 * half + 16 * h + 8 * g;
                StoreShared16(b + SwOff16(y, col), hi[4 * g], hi[4 * g + 1], hi[4 * g + 2], hi[4 * g + 3]);
                StoreShared16(b + kColImgBytes + SwOff16(y, col), lo[4 * g], lo[4 * g + 1], lo[4 * g + 2],
                              lo[4 * g + 3]);
@@ -547,34 +552,33 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
             MbarArrive(&sh->tFree);
          return true;
       };
-      // E(j): wait for its column pass, |E|^2, the plane sum, the normalized plane; eFree once E is in registers.
+      // E(j) (this warp: y = 32 half .. + 31): wait for its column pass, |E|^2, the plane sum, the normalized plane;
+      // eFree once E is in registers.
       auto drainE = [&](int j) -> bool {
          const uint32_t use = static_cast<uint32_t>(j >> 1) & 1u;
          if (!__all_sync(0xffffffffu, MbarWait(&sh->colDone[j & 1], use, err, false)))
             return false;
          TcFenceAfter();
-         float I[64];
-         float part[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};   // eight float partial sums of 8 values each
-#pragma unroll
-         for (int c0 = 0; c0 < 64; c0 += 32)
+         float I[32];
+         float part[4] = {0.f, 0.f, 0.f, 0.f};   // four float partial sums of 8 values each
          {
             float vv[32];
-            TmemLoad32(tmem + quad + kTmemCol + 64u * static_cast<uint32_t>(j & 1) + c0, vv);
+            TmemLoad32(tmem + quad + kTmemCol + 64u * static_cast<uint32_t>(j & 1) + 32u * half, vv);
 #pragma unroll
             for (int c = 0; c < 32; ++c)   // |2^20 E|^2 = 2^40 |E|^2; the 2^-40 goes into the final scale
             {
                const float me = vv[c];
                const float o = __shfl_xor_sync(0xffffffffu, me, 16);
                const float e = me * me + o * o;
-               I[c0 + c] = e;
-               if (c0 + c < P)
-                  part[(c0 + c) >> 3] += e;
+               I[c] = e;
+               if (32 * half + c < P)
+                  part[c >> 3] += e;
             }
          }
          double local = 0.0;
          if (lane < 16 && x < P)
 #pragma unroll
-            for (int k = 0; k < 8; ++k)
+            for (int k = 0; k < 4; ++k)
                local += static_cast<double>(part[k]);
          TcFenceBefore();
          __syncwarp();
@@ -592,21 +596,23 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
             }
             if (!__all_sync(0xffffffffu, MbarWait(&sh->red[j & 1], use, err, false)))
                return false;
-            const volatile double* s = sh->sum[j & 1];
-            total = s[0] + s[1] + s[2] + s[3];
+            const volatile double* sm = sh->sum[j & 1];
+#pragma unroll
+            for (int w = 0; w < kDrainWarps; ++w)
+               total += sm[w];
          }
-         // lanes 0-15 hold rows y < 32 of column x, lanes 16-31 rows y >= 32; the plane times 1 / sum (the float
-         // product is within an ulp or two of the float64 quotient)
+         // lanes 0-15 store rows y = 32 half .. + 15 of column x, lanes 16-31 rows 32 half + 16 .. + 31; the plane
+         // times 1 / sum (the float product is within an ulp or two of the float64 quotient)
          float* plane = prm.out + static_cast<size_t>(psf0 + j) * P * P;
          const float scale = (prm.normalize && total > 0.0) ? static_cast<float>(1.0 / total) : kScaleI;
-         const int y0 = 32 * h;
+         const int y0 = 32 * half + 16 * h;
          if (x < P)
          {
 #pragma unroll
-            for (int c = 0; c < 32; ++c)
+            for (int c = 0; c < 16; ++c)
             {
                const int yy = y0 + c;
-               const float e = h ? I[32 + c] : I[c];
+               const float e = h ? I[16 + c] : I[c];
                if (yy < P)
                   plane[static_cast<size_t>(yy) * P + x] = e * scale;
             }
