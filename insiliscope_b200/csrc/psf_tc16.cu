@@ -224,9 +224,9 @@ static_assert(kSmemBytes <= 227 * 1024, "the FP16 chirp-Z kernel's shared memory
 //   the column-pass thread (warp 12, lane 0): per PSF its column pass C(j) into E's buffer j % 2 once E(j - 2) has
 //     been taken (eFree), K block by K block as the drain warps fill the col-B stages; commits colEmpty / colDone;
 //   drain warps (0-7, two per TMEM lane quadrant, each half of every block's columns): T of PSF j from TMEM, times
-//     2^-16, split, into col-B stages -> colFull (then tFree); then E of PSF j: |E|^2, the plane sum, the normalized
-//     plane (eFree). At the first PSF of each set's run (E of the previous PSF taken: both passes of every earlier
-//     PSF complete) the set's DFT operand from global memory into TMEM (aFull).
+//     2^-16, split, into col-B stages -> colFull (then tFree); then E of PSF j - 1: |E|^2, the plane sum, the
+//     normalized plane (eFree). At the first PSF of each set's run, once E of the previous PSF is taken (both passes of
+//     every earlier PSF complete), the set's DFT operand from global memory into TMEM (aFull).
 // R(j + 1) runs beside C(j) on the tensor pipe. Every wait is bounded (kWaitNs) and also ends when another role has
 // failed (Shared16::err); a failed CTA stops issuing, waits for its MMAs in flight, frees TMEM and reports through
 // prm.error.
@@ -619,21 +619,31 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
          }
          return true;
       };
-      // T(j), then E(j): the column pass of PSF j follows the T drain K block by K block, and the row pass of PSF
-      // j + 1 starts once T(j) is taken. At a set change E of every earlier PSF has been taken, so both passes are
-      // complete and no MMA reads the operand being replaced.
+      // T(j), then E(j - 1): the column pass of PSF j follows the T drain K block by K block and the row pass of PSF
+      // j + 1 starts once T(j) is taken, while these warps take E(j - 1), whose column pass has had all of R(j) to
+      // finish (E(j) right after T(j) would wait for C(j)). At a set change E(j - 1) is taken first: then both passes of
+      // every earlier PSF are complete and no MMA reads the operand being replaced.
+      int eNext = 0;   // the next PSF whose E is taken
       for (int j = 0; j < nLocal && ok; ++j)
       {
          if (firstOfSet(j))
          {
+            while (ok && eNext < j)
+               ok = drainE(eNext++);
+            if (!ok)
+               break;
             loadOperand(setOf(j));
             TcFenceBefore();
             __syncwarp();
             if (lane == 0)
                MbarArrive(&sh->aFull);
          }
-         ok = drainT(j) && drainE(j);
+         ok = drainT(j);
+         if (ok && eNext < j)
+            ok = drainE(eNext++);
       }
+      while (ok && eNext < nLocal)
+         ok = drainE(eNext++);
    }
    if (!ok)
       *err = 1;
