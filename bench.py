@@ -104,7 +104,7 @@ NCU_TRAFFIC = {
     ("smlm", "GatherTilesKernel"): (138334464, "profiles/GatherTilesKernel_smlm_dstorm.md"),
     ("smlm", "ContribKernel"): (96654336, "profiles/ContribKernel_smlm_dstorm.md"),
     ("psflib", "CztTf32x3Kernel"): (52487168, "profiles/CztTf32x3Kernel_psf_library.md"),
-    ("psflib", "CztF16x3Kernel"): (30515968, "profiles/CztF16x3Kernel_psf_library.md"),
+    ("psflib", "CztF16x3Kernel"): (28717824, "profiles/CztF16x3Kernel_psf_library.md"),
     ("two-colour", "GatherTilesKernel"): (2182043649, "profiles/GatherTilesKernel_two_colour.md"),
     ("widefield", "WfNoiseKernel"): (73900000, "profiles/widefield_cells_launches.md"),
     ("widefield", "ZKernel<convolve>"): (1046200000, "profiles/widefield_cells_launches.md"),
