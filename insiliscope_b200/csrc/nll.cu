@@ -41,6 +41,7 @@ namespace iscu {
 namespace {
 
 constexpr int kM = 32, kP = 64, kThreads = 256, kMaxJ = 32;
+constexpr int kPre = 4;   // observed counts a thread loads ahead (ROIs up to 32 x 32 pixels)
 
 __device__ __forceinline__ float2 Cmul(float2 a, float2 b)
 {
@@ -212,6 +213,14 @@ __global__ void __launch_bounds__(kThreads, 2) NllKernel(NllArgs a)
          atomicExch(a.err, 1);
       const double b = frameOk ? static_cast<double>(a.bg[f]) : 0.0;
       const double x = pr.x, y = pr.y, z = pr.z, N = pr.w;
+      // the observed counts of this thread's pixels p = tid + 256 q, loaded now so that their latency passes under
+      // the pupil and the forward products (ROIs of up to 32 x 32 pixels: at most four a thread)
+      const float* k = a.counts + static_cast<size_t>(e) * RR;
+      const bool pre = RR <= kPre * kThreads;
+      float kpre[kPre];
+#pragma unroll
+      for (int q = 0; q < kPre; ++q)
+         kpre[q] = pre && tid + q * kThreads < RR ? k[tid + q * kThreads] : 0.f;
       // 1. the pupil
       for (int m = tid; m < kM * kM; m += kThreads)
       {
@@ -232,9 +241,7 @@ __global__ void __launch_bounds__(kThreads, 2) NllKernel(NllArgs a)
       __syncthreads();
       // 4. expected counts and the likelihood; the gradient weights into E
       double part = 0.0, gN = 0.0, gB = 0.0;
-      const float* k = a.counts + static_cast<size_t>(e) * RR;
-      for (int p = tid; p < RR; p += kThreads)
-      {
+      auto pixel = [&](int p, float kf) {
          const int i = p / R, j = p % R;
          float sum = 0.f;
          for (int ty = 0; ty < os; ++ty)
@@ -245,7 +252,7 @@ __global__ void __launch_bounds__(kThreads, 2) NllKernel(NllArgs a)
             }
          const double psf = a.kappa * static_cast<double>(sum);
          const double mu = N * psf + b;
-         const double kk = static_cast<double>(k[p]);
+         const double kk = static_cast<double>(kf);
          part += mu - kk * log(mu);
          if (a.mu)
             a.mu[static_cast<size_t>(e) * RR + p] = static_cast<float>(mu);
@@ -262,7 +269,17 @@ __global__ void __launch_bounds__(kThreads, 2) NllKernel(NllArgs a)
                   v = make_float2(G * v.x, G * v.y);
                }
          }
+      };
+      if (pre)
+      {
+#pragma unroll
+         for (int q = 0; q < kPre; ++q)
+            if (tid + q * kThreads < RR)
+               pixel(tid + q * kThreads, kpre[q]);
       }
+      else
+         for (int p = tid; p < RR; p += kThreads)
+            pixel(p, k[p]);
       nllAcc += part;
       if (!kGrad)
       {
