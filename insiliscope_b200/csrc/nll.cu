@@ -270,7 +270,54 @@ __global__ void __launch_bounds__(kThreads, 2) NllKernel(NllArgs a)
                }
          }
       };
-      if (pre)
+      if (RR == kPre * kThreads)
+      {
+         // Every thread has kPre pixels (32 x 32 ROIs): the same operations as `pixel`, in stages across its pixels so
+         // that their float64 chains (the logarithm, the quotient) run side by side; each sum takes its terms in the
+         // same order, so the results are the pixel-by-pixel form's.
+         double psf[kPre], mu[kPre], lg[kPre], w[kPre];
+#pragma unroll
+         for (int q = 0; q < kPre; ++q)
+         {
+            const int p = tid + q * kThreads, i = p / R, j = p % R;
+            float sum = 0.f;
+            for (int ty = 0; ty < os; ++ty)
+               for (int tx = 0; tx < os; ++tx)
+               {
+                  const float2 v = s.E[i * os + ty][j * os + tx];
+                  sum = fmaf(v.x, v.x, fmaf(v.y, v.y, sum));
+               }
+            psf[q] = a.kappa * static_cast<double>(sum);
+            mu[q] = N * psf[q] + b;
+         }
+#pragma unroll
+         for (int q = 0; q < kPre; ++q)
+            lg[q] = log(mu[q]);
+#pragma unroll
+         for (int q = 0; q < kPre; ++q)
+            w[q] = 1.0 - static_cast<double>(kpre[q]) / mu[q];
+#pragma unroll
+         for (int q = 0; q < kPre; ++q)
+         {
+            const int p = tid + q * kThreads, i = p / R, j = p % R;
+            part += mu[q] - static_cast<double>(kpre[q]) * lg[q];
+            if (a.mu)
+               a.mu[static_cast<size_t>(e) * RR + p] = static_cast<float>(mu[q]);
+            if (kGrad)
+            {
+               gN += w[q] * psf[q];
+               gB += w[q];
+               const float G = static_cast<float>(w[q] * N * a.kappa);
+               for (int ty = 0; ty < os; ++ty)
+                  for (int tx = 0; tx < os; ++tx)
+                  {
+                     float2& v = s.E[i * os + ty][j * os + tx];
+                     v = make_float2(G * v.x, G * v.y);
+                  }
+            }
+         }
+      }
+      else if (pre)
       {
 #pragma unroll
          for (int q = 0; q < kPre; ++q)
