@@ -298,9 +298,13 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
       // Item r (0, 1) of K block kb: pupil column m = item & 127 and pupil rows n0 .. n0 + 7, n0 = 32 kb + 8 (item >>
       // 7), item = ptid + r kProducerThreads.
       const int ptid = 32 * ProducerIndex(warp) + lane;
-      const int nR = ptid + kProducerThreads < kItemsPerBlock ? 2 : 1;
-      auto load = [&](const float2* tab, int kb, int r, float2* dst) {
-         const int item = ptid + r * kProducerThreads, m = item & 127, n0 = 32 * kb + 8 * (item >> 7);
+      // A block's 512 items over 320 threads: 192 threads make two, 128 one. Which do is rotated by 64 threads (two
+      // warps, so a warp's count stays uniform) from one K block to the next: over any five blocks every thread
+      // makes eight items, 1.6 a block, where a fixed split would give some threads two every block.
+      auto slotOf = [&](uint32_t rc) { return (ptid + static_cast<int>(rc % 5u) * 64) % kProducerThreads; };
+      auto countOf = [&](uint32_t rc) { return slotOf(rc) + kProducerThreads < kItemsPerBlock ? 2 : 1; };
+      auto load = [&](const float2* tab, int kb, int item, float2* dst) {
+         const int m = item & 127, n0 = 32 * kb + 8 * (item >> 7);
          const bool in = m < M && n0 < M;
          const float2* t = tab + n0 * M + m;
 #pragma unroll
@@ -317,7 +321,7 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
       auto tabOf = [&](int j) { return prm.phase + static_cast<size_t>(setOf(j)) * M * M; };
       float2 nxt[8];
       if (nLocal > 0)
-         load(tabOf(0), 0, 0, nxt);
+         load(tabOf(0), 0, slotOf(0), nxt);
       uint32_t rowCount = 0;
       for (int j = 0; j < nLocal && ok; ++j)
       {
@@ -330,6 +334,7 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
             if (!ok)
                break;
             unsigned char* b = sRowB + rs * kKbBytes;
+            const int slot = slotOf(rowCount), nR = countOf(rowCount);
 #pragma unroll
             for (int r = 0; r < 2; ++r)
             {
@@ -341,12 +346,12 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
                   cur[c] = nxt[c];
                // the next item's table entries while this one computes
                if (r + 1 < nR)
-                  load(tab, kb, r + 1, nxt);
+                  load(tab, kb, slot + kProducerThreads, nxt);
                else if (kb + 1 < nKb)
-                  load(tab, kb + 1, 0, nxt);
+                  load(tab, kb + 1, slotOf(rowCount + 1), nxt);
                else if (j + 1 < nLocal)
-                  load(tabOf(j + 1), 0, 0, nxt);
-               const int item = ptid + r * kProducerThreads, m = item & 127, l = 8 * (item >> 7);
+                  load(tabOf(j + 1), 0, slotOf(rowCount + 1), nxt);
+               const int item = slot + r * kProducerThreads, m = item & 127, l = 8 * (item >> 7);
                if (m < M && 32 * kb + l < M)   // pupil columns >= M are not read (N = M); K steps >= M are skipped
                {
                   uint32_t rh[4], rl[4], ih[4], il[4];
