@@ -136,11 +136,15 @@ __global__ void ContribSetupKernel(SetupArgs a)
 }
 
 // ------------------------------------------------------------------------------------------------ 2. offsets
-// One CTA of 1024 threads: start[k] = exclusive sum of count, itemStart[k] = exclusive sum of the keys' work items
-// (ceil(count / kE) emitter chunks x the slot's pixel blocks); itemStart[nKeys] and ctr[0] = the total; ctr[1] = 0.
+// One CTA of 1024 threads, kScanPer consecutive keys a thread per pass of 4,096 keys (one round trip for the counts):
+// start[k] = exclusive sum of count, itemStart[k] = exclusive sum of the keys' work items (ceil(count / kE) emitter
+// chunks x the slot's pixel blocks), itemKey[i] = k for each of key k's items; itemStart[nKeys] and ctr[0] = the
+// total; ctr[1] = 0.
+constexpr int kScanPer = 4;
 __global__ void __launch_bounds__(1024) ContribScanKernel(KeyMap km, const uint32_t* __restrict__ count,
                                                           uint32_t* __restrict__ start, uint32_t* __restrict__ cursor,
-                                                          uint32_t* __restrict__ itemStart, uint32_t* __restrict__ ctr)
+                                                          uint32_t* __restrict__ itemStart,
+                                                          uint32_t* __restrict__ itemKey, uint32_t* __restrict__ ctr)
 {
    const int nKeys = km.base[ISCU_MAX_KERNELS];
    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -149,16 +153,21 @@ __global__ void __launch_bounds__(1024) ContribScanKernel(KeyMap km, const uint3
    if (threadIdx.x == 0)
       carry[0] = carry[1] = 0;
    __syncthreads();
-   for (int k0 = 0; k0 < nKeys; k0 += 1024)
+   for (int k0 = 0; k0 < nKeys; k0 += 1024 * kScanPer)
    {
-      const int k = k0 + static_cast<int>(threadIdx.x);
-      uint32_t c = 0, it = 0;
-      if (k < nKeys)
+      const int kb = k0 + static_cast<int>(threadIdx.x) * kScanPer;
+      uint32_t c[kScanPer], it[kScanPer], tc = 0, ti = 0;
+#pragma unroll
+      for (int j = 0; j < kScanPer; ++j)
+         c[j] = kb + j < nKeys ? count[kb + j] : 0u;
+#pragma unroll
+      for (int j = 0; j < kScanPer; ++j)
       {
-         c = count[k];
-         it = c ? ((c + kE - 1) / kE) * static_cast<uint32_t>(km.pbs[SlotOfKey(km, k)]) : 0u;
+         it[j] = c[j] ? ((c[j] + kE - 1) / kE) * static_cast<uint32_t>(km.pbs[SlotOfKey(km, kb + j)]) : 0u;
+         tc += c[j];
+         ti += it[j];
       }
-      uint32_t xc = c, xi = it;   // inclusive warp scans
+      uint32_t xc = tc, xi = ti;   // inclusive warp scans of the threads' totals
 #pragma unroll
       for (int d = 1; d < 32; d <<= 1)
       {
@@ -192,19 +201,28 @@ __global__ void __launch_bounds__(1024) ContribScanKernel(KeyMap km, const uint3
          sw[1][lane] = v;
       }
       __syncthreads();
-      const uint32_t exc = carry[0] + (warp ? sw[0][warp - 1] : 0u) + xc - c;
-      const uint32_t exi = carry[1] + (warp ? sw[1][warp - 1] : 0u) + xi - it;
-      if (k < nKeys)
+      uint32_t ec = carry[0] + (warp ? sw[0][warp - 1] : 0u) + xc - tc;
+      uint32_t ei = carry[1] + (warp ? sw[1][warp - 1] : 0u) + xi - ti;
+#pragma unroll
+      for (int j = 0; j < kScanPer; ++j)
       {
-         start[k] = exc;
-         cursor[k] = exc;
-         itemStart[k] = exi;
+         const int k = kb + j;
+         if (k < nKeys)
+         {
+            start[k] = ec;
+            cursor[k] = ec;
+            itemStart[k] = ei;
+            for (uint32_t q = 0; q < it[j]; ++q)
+               itemKey[ei + q] = static_cast<uint32_t>(k);
+         }
+         ec += c[j];
+         ei += it[j];
       }
       __syncthreads();
       if (threadIdx.x == 1023)
       {
-         carry[0] = exc + c;
-         carry[1] = exi + it;
+         carry[0] = ec;
+         carry[1] = ei;
       }
       __syncthreads();
    }
@@ -256,16 +274,6 @@ __global__ void ContribScatterKernel(uint32_t n, const SplatRec* __restrict__ re
    s.by = r.by;
    s.plane = r.plane;
    stage[base + __popc(peers & ((1u << lane) - 1u))] = s;
-}
-
-// itemKey[i] = the key of work item i.
-__global__ void ContribItemKeysKernel(int nKeys, const uint32_t* __restrict__ itemStart, uint32_t* __restrict__ itemKey)
-{
-   const int k = blockIdx.x * blockDim.x + threadIdx.x;
-   if (k >= nKeys)
-      return;
-   for (uint32_t i = itemStart[k]; i < itemStart[k + 1]; ++i)
-      itemKey[i] = static_cast<uint32_t>(k);
 }
 
 // ------------------------------------------------------------------------------------------------ 4. contributions
@@ -784,14 +792,13 @@ int LaunchContribRender(iscu_ctx* ctx, int tileConfig, const iscu_emitter* ems, 
       ISCU_CK_LAUNCH(ctx, "ContribSetupKernel");
       if (nKeys > 0)
       {
-         ContribScanKernel<<<1, 1024, 0, ctx->stream>>>(km, count, start, cursor, itemStart, sc.ctr.as<uint32_t>());
+         ContribScanKernel<<<1, 1024, 0, ctx->stream>>>(km, count, start, cursor, itemStart, itemKey,
+                                                        sc.ctr.as<uint32_t>());
          ISCU_CK_LAUNCH(ctx, "ContribScanKernel");
          ContribScatterKernel<<<(nEm + 255) / 256, 256, 0, ctx->stream>>>(nEm, sc.rec.as<SplatRec>(),
                                                                            sc.grec.as<int4>(), cursor,
                                                                            sc.list.as<CStage>());
          ISCU_CK_LAUNCH(ctx, "ContribScatterKernel");
-         ContribItemKeysKernel<<<(nKeys + 255) / 256, 256, 0, ctx->stream>>>(nKeys, itemStart, itemKey);
-         ISCU_CK_LAUNCH(ctx, "ContribItemKeysKernel");
          if (marks)
             ISCU_CK(cudaEventRecord(marks[1], ctx->stream));
          ContribArgs ca{km, K, count, start, itemStart, itemKey, sc.list.as<CStage>(), sc.ctr.as<uint32_t>(),

@@ -91,6 +91,29 @@ def test_forms_match_reference(engine, reference, setup):
         engine.set_render_config(0)
 
 
+@pytest.mark.parametrize("emccd", [False, True])
+def test_two_pass_noise_without_photons(engine, reference, setup, emccd):
+    """The two-pass forms when the caller keeps no photon frames (the tiles' photon values in scratch ahead of the
+    pooled noise chain), on an sCMOS and an EMCCD camera: the reference's frames bit for bit."""
+    kernels, (off, gain, rn), _ = setup
+    cam = CameraParams(quantum_efficiency=0.9, dark_electrons=0.02, gain=2.2 if not emccd else 4.0, read_noise_e=1.5,
+                       emccd=emccd, em_gain=150.0, cic_electrons=0.003)
+    rng = np.random.default_rng(41)
+    ev, bucket = _movie(rng)
+    ems, frames = _batch(engine, ev, bucket)
+    seed = 99
+    _, _, want_adu = reference.render_movie_groups(kernels, ev, 0, F, W, H, PX, PER_BLINK, BG, cam, off, gain, rn,
+                                                   seed)
+    try:
+        for config in range(12, engine.RENDER_CONFIGS):
+            engine.set_render_config(config)
+            ph, adu = engine.render_frames(ems, frames, cam, seed, want_photons=False)
+            assert ph is None
+            assert np.array_equal(adu, want_adu), config
+    finally:
+        engine.set_render_config(0)
+
+
 def test_autotune_and_graph(engine, reference, setup):
     kernels, (off, gain, rn), cam = setup
     rng = np.random.default_rng(77)
