@@ -230,6 +230,7 @@ static_assert(kSmemBytes <= 227 * 1024, "the FP16 chirp-Z kernel's shared memory
 // R(j + 1) runs beside C(j) on the tensor pipe. Every wait is bounded (kWaitNs) and also ends when another role has
 // failed (Shared16::err); a failed CTA stops issuing, waits for its MMAs in flight, frees TMEM and reports through
 // prm.error.
+template <int kM, int kP>
 __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
 {
    extern __shared__ __align__(1024) unsigned char smemRaw[];
@@ -240,7 +241,8 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
    volatile int* err = &sh->err;
 
    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-   const int M = prm.M, P = prm.P, nKb = (M + 31) / 32;
+   // kM, kP > 0: the shape compiled in (the library's 128 -> 64); 0: the request's
+   const int M = kM > 0 ? kM : prm.M, P = kP > 0 ? kP : prm.P, nKb = (M + 31) / 32;
    // this CTA's PSFs: psf0 .. psf0 + nLocal - 1
    const int perCta = prm.nPsf / static_cast<int>(gridDim.x), extra = prm.nPsf % static_cast<int>(gridDim.x);
    const int cta = static_cast<int>(blockIdx.x);
@@ -296,13 +298,14 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
    {
       // ---------------------------------------------------------------- producers: row-pass B blocks
       // Item r (0, 1) of K block kb: pupil column m = item & 127 and pupil rows n0 .. n0 + 7, n0 = 32 kb + 8 (item >>
-      // 7), item = ptid + r kProducerThreads.
+      // 7), item = slot + r kProducerThreads with slot = (ptid + rot) mod kProducerThreads.
       const int ptid = 32 * ProducerIndex(warp) + lane;
       // A block's 512 items over 320 threads: 192 threads make two, 128 one. Which do is rotated by 64 threads (two
       // warps, so a warp's count stays uniform) from one K block to the next: over any five blocks every thread
-      // makes eight items, 1.6 a block, where a fixed split would give some threads two every block.
-      auto slotOf = [&](uint32_t rc) { return (ptid + static_cast<int>(rc % 5u) * 64) % kProducerThreads; };
-      auto countOf = [&](uint32_t rc) { return slotOf(rc) + kProducerThreads < kItemsPerBlock ? 2 : 1; };
+      // makes eight items, 1.6 a block, where a fixed split would give some threads two every block. rot = 64 (block
+      // count mod 5), stepped with the blocks rather than divided out.
+      auto slotAt = [&](int rot) { return ptid + rot >= kProducerThreads ? ptid + rot - kProducerThreads : ptid + rot; };
+      auto nextRot = [](int rot) { return rot == kProducerThreads - 64 ? 0 : rot + 64; };
       auto load = [&](const float2* tab, int kb, int item, float2* dst) {
          const int m = item & 127, n0 = 32 * kb + 8 * (item >> 7);
          const bool in = m < M && n0 < M;
@@ -321,20 +324,21 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
       auto tabOf = [&](int j) { return prm.phase + static_cast<size_t>(setOf(j)) * M * M; };
       float2 nxt[8];
       if (nLocal > 0)
-         load(tabOf(0), 0, slotOf(0), nxt);
+         load(tabOf(0), 0, slotAt(0), nxt);
       uint32_t rowCount = 0;
+      int rot = 0;   // (rowCount % 5) 64
       for (int j = 0; j < nLocal && ok; ++j)
       {
          const float aDef = aDefOf(j);
          const float2* tab = tabOf(j);
-         for (int kb = 0; kb < nKb; ++kb, ++rowCount)
+         for (int kb = 0; kb < nKb; ++kb, ++rowCount, rot = nextRot(rot))
          {
             const int rs = static_cast<int>(rowCount % kRowStages);
             ok = __all_sync(0xffffffffu, MbarWait(&sh->rowEmpty[rs], ((rowCount / kRowStages) & 1u) ^ 1u, err));
             if (!ok)
                break;
             unsigned char* b = sRowB + rs * kKbBytes;
-            const int slot = slotOf(rowCount), nR = countOf(rowCount);
+            const int slot = slotAt(rot), nR = slot + kProducerThreads < kItemsPerBlock ? 2 : 1;
 #pragma unroll
             for (int r = 0; r < 2; ++r)
             {
@@ -348,9 +352,9 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
                if (r + 1 < nR)
                   load(tab, kb, slot + kProducerThreads, nxt);
                else if (kb + 1 < nKb)
-                  load(tab, kb + 1, slotOf(rowCount + 1), nxt);
+                  load(tab, kb + 1, slotAt(nextRot(rot)), nxt);
                else if (j + 1 < nLocal)
-                  load(tabOf(j + 1), 0, slotOf(rowCount + 1), nxt);
+                  load(tabOf(j + 1), 0, slotAt(nextRot(rot)), nxt);
                const int item = slot + r * kProducerThreads, m = item & 127, l = 8 * (item >> 7);
                if (m < M && 32 * kb + l < M)   // pupil columns >= M are not read (N = M); K steps >= M are skipped
                {
@@ -688,7 +692,9 @@ int LaunchCztF16x3Core(iscu_ctx* ctx, const SetParams* sets, const unsigned char
    if (nPsf == 0)
       return ISCU_OK;
    const size_t smem = kSmemBytes;
-   ISCU_CK(cudaFuncSetAttribute(CztF16x3Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+   const bool fixed = M == 128 && P == 64;
+   auto kernel = fixed ? CztF16x3Kernel<128, 64> : CztF16x3Kernel<0, 0>;
+   ISCU_CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
    Tc16Params prm;
    prm.sets = sets;
    prm.phase = reinterpret_cast<const float2*>(ahat + AhatF16Bytes(nSets));
@@ -701,7 +707,7 @@ int LaunchCztF16x3Core(iscu_ctx* ctx, const SetParams* sets, const unsigned char
    prm.P = P;
    prm.normalize = normalize;
    const int grid = static_cast<int>(std::min<uint32_t>(nPsf, static_cast<uint32_t>(ctx->smCount)));
-   CztF16x3Kernel<<<grid, kThreads, smem, ctx->stream>>>(prm);
+   kernel<<<grid, kThreads, smem, ctx->stream>>>(prm);
    ISCU_CK_LAUNCH(ctx, "CztF16x3Kernel");
    return ISCU_OK;
 }
