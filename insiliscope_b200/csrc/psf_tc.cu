@@ -604,7 +604,8 @@ int BuildAhat(iscu_ctx* ctx, const float2* A, const SetParams* sets, const doubl
       return Fail(ISCU_ERR_ARG, std::string(f16 ? "f16x3" : "tf32x3") +
                                    " chirp-Z: needs pupil samples M <= 128 (a multiple of 16) and planes of at most "
                                    "64 x 64 (else use the fp32 method)");
-   // the K-block images, then the phase tables (FP16 form: float2 in revolutions; TF32 form: double2 in radians)
+   // the K-block images, then the phase tables (FP16 form: (tx, tx, ty, ty) float4 per pair of pupil rows, in
+   // revolutions, the size of a float2 per sample; TF32 form: double2 in radians)
    const size_t images = SplitImageBytes(method, nSets);
    ISCU_CK(ahat.Reserve(images + static_cast<size_t>(nSets) * M * M * (f16 ? sizeof(float2) : sizeof(double2))));
    if (f16)

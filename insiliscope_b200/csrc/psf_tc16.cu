@@ -155,40 +155,101 @@ __global__ void AhatTmemKernel(const float2* __restrict__ A, int M, int P, uint3
 }
 
 // The phase table in revolutions: per set and sample (tx, ty) = ((k0 opd1 + zernike + mask) mod 2 pi, opd3F) / 2 pi
-// (ZernikePsf.cpp:240-248), the reduction in float64; (0, -1) outside the aperture (opd3F < 0).
-__global__ void RevTableKernel(const SetParams* __restrict__ sets, const double3* __restrict__ tables, int MM,
-                               float2* __restrict__ out)
+// (ZernikePsf.cpp:240-248), the reduction in float64; (0, -1) outside the aperture (opd3F < 0). Laid out by pairs of
+// pupil rows, [set][n / 2][m] float4 = (tx of rows n, n + 1; ty of rows n, n + 1), so that one 16-byte load gives
+// a producer two samples' (tx, ty) already paired for the two-lane float instructions (M is even).
+__global__ void RevTableKernel(const SetParams* __restrict__ sets, const double3* __restrict__ tables, int M,
+                               float* __restrict__ out)
 {
    const int s = blockIdx.y;
-   const int m = blockIdx.x * blockDim.x + threadIdx.x;
-   if (m >= MM)
+   const int i = blockIdx.x * blockDim.x + threadIdx.x, MM = M * M;
+   if (i >= MM)
       return;
-   const double3 t = tables[static_cast<size_t>(s) * MM + m];
+   const int n = i / M, m = i - n * M;
+   const double3 t = tables[static_cast<size_t>(s) * MM + i];
    const double kInvTwoPi = 0.15915494309189533577;
    const double b = ReduceTwoPi(sets[s].k0 * t.x + t.z) * kInvTwoPi;
-   out[static_cast<size_t>(s) * MM + m] = t.y < 0.0 ? make_float2(0.f, -1.f)
-                                                    : make_float2(static_cast<float>(b), static_cast<float>(t.y * kInvTwoPi));
+   // set s holds M / 2 row pairs of M float4 (2 MM floats, the float2 table's size)
+   float* o = out + ((static_cast<size_t>(s) * (M / 2) + static_cast<size_t>(n >> 1)) * M + m) * 4 + (n & 1);
+   o[0] = t.y < 0.0 ? 0.f : static_cast<float>(b);
+   o[2] = t.y < 0.0 ? -1.f : static_cast<float>(t.y * kInvTwoPi);
 }
 
-// One pupil phasor from the revolution table, times amp inside the aperture (0 outside): x = a ty + tx, r = x - rint(x)
-// (rint by adding and taking away 1.5 2^23, exact for |x| < 2^22; r in [-1/2, 1/2] exactly), then the float32 sine and
-// cosine of 2 pi r (absolute error ~4e-7 over [-pi, pi]).
-__device__ __forceinline__ float2 RevPhasor(float2 t, float a, float amp)
+// Two float lanes in one 64-bit register for the sm_100 two-lane float instructions (each lane rounds as the
+// one-lane instruction does).
+__device__ __forceinline__ uint64_t Pack2(float a, float b)
 {
-   const float kRound = 12582912.0f;   // 1.5 2^23
-   const float x = fmaf(a, t.y, t.x);
-   const float n = (x + kRound) - kRound;
-   float sn, cs;
-   __sincosf(6.28318530718f * (x - n), &sn, &cs);
-   const float s = t.y >= 0.f ? amp : 0.f;
-   return make_float2(cs * s, sn * s);
+   uint64_t r;
+   asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+   return r;
+}
+__device__ __forceinline__ float2 Unpack2(uint64_t v)
+{
+   float2 r;
+   asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+   return r;
+}
+__device__ __forceinline__ uint64_t Fma2(uint64_t a, uint64_t b, uint64_t c)
+{
+   uint64_t d;
+   asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+   return d;
+}
+__device__ __forceinline__ uint64_t Add2(uint64_t a, uint64_t b)
+{
+   uint64_t d;
+   asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+   return d;
+}
+__device__ __forceinline__ uint64_t Sub2(uint64_t a, uint64_t b)
+{
+   uint64_t d;
+   asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+   return d;
+}
+__device__ __forceinline__ uint64_t Mul2(uint64_t a, uint64_t b)
+{
+   uint64_t d;
+   asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+   return d;
+}
+
+// Two pupil phasors from the revolution table, times amp inside the aperture (0 outside): x = a ty + tx, r = x -
+// rint(x) (rint by adding and taking away 1.5 2^23, exact for |x| < 2^22; r in [-1/2, 1/2] exactly), then the float32
+// sine and cosine of 2 pi r (absolute error ~4e-7 over [-pi, pi]). The two samples t = (tx0, tx1, ty0, ty1) go through
+// two-lane instructions, each lane rounding as the one-lane form would: re = (cs0 s0, cs1 s1), im = (sn0 s0, sn1 s1).
+__device__ __forceinline__ void RevPhasor2(float4 t, uint64_t a2, float amp, uint64_t& re, uint64_t& im)
+{
+   const uint64_t kRound2 = 0x4B4000004B400000ull;      // (1.5 2^23, 1.5 2^23)
+   const uint64_t kTwoPi2 = 0x40C90FDB40C90FDBull;      // (6.28318530718f, 6.28318530718f)
+   const uint64_t x = Fma2(a2, Pack2(t.z, t.w), Pack2(t.x, t.y));
+   const uint64_t n = Sub2(Add2(x, kRound2), kRound2);
+   const float2 r = Unpack2(Mul2(kTwoPi2, Sub2(x, n)));
+   float sn0, cs0, sn1, cs1;
+   __sincosf(r.x, &sn0, &cs0);
+   __sincosf(r.y, &sn1, &cs1);
+   const uint64_t s = Pack2(t.z >= 0.f ? amp : 0.f, t.w >= 0.f ? amp : 0.f);
+   re = Mul2(Pack2(cs0, cs1), s);
+   im = Mul2(Pack2(sn0, sn1), s);
+}
+
+// SplitH2 of a two-lane value, the residual in one two-lane subtraction.
+__device__ __forceinline__ void SplitH2P(uint64_t v, uint32_t& hi, uint32_t& lo)
+{
+   const float2 ab = Unpack2(v);
+   const __half2 h = __floats2half2_rn(ab.x, ab.y);
+   const float2 f = __half22float2(h);
+   const float2 d = Unpack2(Sub2(v, Pack2(f.x, f.y)));
+   const __half2 l = __floats2half2_rn(d.x, d.y);
+   hi = *reinterpret_cast<const uint32_t*>(&h);
+   lo = *reinterpret_cast<const uint32_t*>(&l);
 }
 
 // ------------------------------------------------------------------------------------------ the fused kernel
 struct Tc16Params
 {
    const SetParams* sets;
-   const float2* phase;        // [set][M * M] (tx, ty) revolutions
+   const float4* phase;        // [set][M / 2][M] (tx, tx, ty, ty) of two pupil rows, revolutions
    const unsigned char* ahat;  // [set] DFT operand images in tensor-memory order (AhatTmemKernel)
    const PsfItem* items;
    float* out;
@@ -306,13 +367,13 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
       // count mod 5), stepped with the blocks rather than divided out.
       auto slotAt = [&](int rot) { return ptid + rot >= kProducerThreads ? ptid + rot - kProducerThreads : ptid + rot; };
       auto nextRot = [](int rot) { return rot == kProducerThreads - 64 ? 0 : rot + 64; };
-      auto load = [&](const float2* tab, int kb, int item, float2* dst) {
+      auto load = [&](const float4* tab, int kb, int item, float4* dst) {
          const int m = item & 127, n0 = 32 * kb + 8 * (item >> 7);
          const bool in = m < M && n0 < M;
-         const float2* t = tab + n0 * M + m;
+         const float4* t = tab + (n0 >> 1) * M + m;
 #pragma unroll
-         for (int c = 0; c < 8; ++c)
-            dst[c] = in ? t[c * M] : make_float2(0.f, -1.f);
+         for (int c = 0; c < 4; ++c)
+            dst[c] = in ? t[c * M] : make_float4(0.f, 0.f, -1.f, -1.f);
       };
       // the defocus factor of PSF j (staged in shared memory for j < kSetCache)
       auto aDefOf = [&](int j) {
@@ -321,8 +382,8 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
          const PsfItem it = prm.items[psf0 + j];
          return static_cast<float>(prm.sets[it.set].k0 * prm.sets[it.set].ni * it.dtiM);
       };
-      auto tabOf = [&](int j) { return prm.phase + static_cast<size_t>(setOf(j)) * M * M; };
-      float2 nxt[8];
+      auto tabOf = [&](int j) { return prm.phase + static_cast<size_t>(setOf(j)) * (M / 2) * M; };
+      float4 nxt[4];
       if (nLocal > 0)
          load(tabOf(0), 0, slotAt(0), nxt);
       uint32_t rowCount = 0;
@@ -330,7 +391,8 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
       for (int j = 0; j < nLocal && ok; ++j)
       {
          const float aDef = aDefOf(j);
-         const float2* tab = tabOf(j);
+         const uint64_t aDef2 = Pack2(aDef, aDef);
+         const float4* tab = tabOf(j);
          for (int kb = 0; kb < nKb; ++kb, ++rowCount, rot = nextRot(rot))
          {
             const int rs = static_cast<int>(rowCount % kRowStages);
@@ -344,9 +406,9 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
             {
                if (r >= nR)
                   break;
-               float2 cur[8];
+               float4 cur[4];
 #pragma unroll
-               for (int c = 0; c < 8; ++c)
+               for (int c = 0; c < 4; ++c)
                   cur[c] = nxt[c];
                // the next item's table entries while this one computes
                if (r + 1 < nR)
@@ -362,10 +424,10 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
 #pragma unroll
                   for (int c = 0; c < 4; ++c)
                   {
-                     const float2 u0 = RevPhasor(cur[2 * c], aDef, kScaleOp);
-                     const float2 u1 = RevPhasor(cur[2 * c + 1], aDef, kScaleOp);
-                     SplitH2(u0.x, u1.x, rh[c], rl[c]);
-                     SplitH2(u0.y, u1.y, ih[c], il[c]);
+                     uint64_t re, im;   // rows n0 + 2c, n0 + 2c + 1
+                     RevPhasor2(cur[c], aDef2, kScaleOp, re, im);
+                     SplitH2P(re, rh[c], rl[c]);
+                     SplitH2P(im, ih[c], il[c]);
                   }
                   // B[m][c0 + i]: the real part of pupil row n0 + i; B[m][c0 + 16 + i]: the imaginary part
                   const int c0 = 32 * (l >> 4) + (l & 15);
@@ -678,7 +740,7 @@ int BuildAhatF16(iscu_ctx* ctx, const float2* A, const SetParams* sets, const do
                                                                                   reinterpret_cast<uint32_t*>(out));
    ISCU_CK_LAUNCH(ctx, "AhatTmemKernel");
    RevTableKernel<<<dim3((M * M + 255) / 256, nSets), 256, 0, ctx->stream>>>(
-      sets, tables, M * M, reinterpret_cast<float2*>(out + AhatF16Bytes(nSets)));
+      sets, tables, M, reinterpret_cast<float*>(out + AhatF16Bytes(nSets)));
    ISCU_CK_LAUNCH(ctx, "RevTableKernel");
    return ISCU_OK;
 }
@@ -697,7 +759,7 @@ int LaunchCztF16x3Core(iscu_ctx* ctx, const SetParams* sets, const unsigned char
    ISCU_CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
    Tc16Params prm;
    prm.sets = sets;
-   prm.phase = reinterpret_cast<const float2*>(ahat + AhatF16Bytes(nSets));
+   prm.phase = reinterpret_cast<const float4*>(ahat + AhatF16Bytes(nSets));
    prm.ahat = ahat;
    prm.items = items;
    prm.out = out;
