@@ -585,6 +585,7 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
       // columns 32 kb + 16 half .. + 15); tFree when all is taken. The drain's waits spin without sleeping: its warps
       // are on the critical path of both passes.
       const float tScale = y < P ? kScaleT : 0.f;
+      const uint64_t tScale2 = Pack2(tScale, tScale);
       uint32_t colCount = 0;
       auto drainT = [&](int j) -> bool {
          if (!__all_sync(0xffffffffu, MbarWait(&sh->rowDone, static_cast<uint32_t>(j) & 1u, err, false)))
@@ -601,7 +602,7 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
             uint32_t hi[8], lo[8];
 #pragma unroll
             for (int c = 0; c < 8; ++c)   // rows y >= P of T are exact zeros (so are those of the DFT operand)
-               SplitH2(v[2 * c] * tScale, v[2 * c + 1] * tScale, hi[c], lo[c]);
+               SplitH2P(Mul2(Pack2(v[2 * c], v[2 * c + 1]), tScale2), hi[c], lo[c]);
             // B[y][32 half + 16 h + i] = part h of T[y][32 kb + 16 half + i]
             unsigned char* b = sColB + cs * kColStageBytes;
 #pragma unroll
@@ -630,27 +631,34 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
          if (!__all_sync(0xffffffffu, MbarWait(&sh->colDone[j & 1], use, err, false)))
             return false;
          TcFenceAfter();
-         float I[32];
-         float part[4] = {0.f, 0.f, 0.f, 0.f};   // four float partial sums of 8 values each
+         uint64_t I2[16];   // |E|^2 of columns (2c, 2c + 1)
+         uint64_t part2[4] = {0ull, 0ull, 0ull, 0ull};   // four two-lane float partial sums of 8 values each
          {
             float vv[32];
             TmemLoad32(tmem + quad + kTmemCol + 64u * static_cast<uint32_t>(j & 1) + 32u * half, vv);
 #pragma unroll
-            for (int c = 0; c < 32; ++c)   // |2^20 E|^2 = 2^40 |E|^2; the 2^-40 goes into the final scale
+            for (int c = 0; c < 16; ++c)   // |2^20 E|^2 = 2^40 |E|^2; the 2^-40 goes into the final scale
             {
-               const float me = vv[c];
-               const float o = __shfl_xor_sync(0xffffffffu, me, 16);
-               const float e = me * me + o * o;
-               I[c] = e;
-               if (32 * half + c < P)
-                  part[c >> 3] += e;
+               const uint64_t me = Pack2(vv[2 * c], vv[2 * c + 1]);
+               const uint64_t o = Pack2(__shfl_xor_sync(0xffffffffu, vv[2 * c], 16),
+                                        __shfl_xor_sync(0xffffffffu, vv[2 * c + 1], 16));
+               const uint64_t e = Fma2(me, me, Mul2(o, o));
+               I2[c] = e;
+               const int col = 32 * half + 2 * c;   // planes' rows y < P are summed
+               if (col + 1 < P)
+                  part2[c >> 2] = Add2(part2[c >> 2], e);
+               else if (col < P)
+                  part2[c >> 2] = Add2(part2[c >> 2], Pack2(Unpack2(e).x, 0.f));
             }
          }
          double local = 0.0;
          if (lane < 16 && x < P)
 #pragma unroll
             for (int k = 0; k < 4; ++k)
-               local += static_cast<double>(part[k]);
+            {
+               const float2 p = Unpack2(part2[k]);
+               local += static_cast<double>(p.x + p.y);
+            }
          TcFenceBefore();
          __syncwarp();
          if (lane == 0)
@@ -677,15 +685,18 @@ __global__ void __launch_bounds__(kThreads, 1) CztF16x3Kernel(Tc16Params prm)
          float* plane = prm.out + static_cast<size_t>(psf0 + j) * P * P;
          const float scale = (prm.normalize && total > 0.0) ? static_cast<float>(1.0 / total) : kScaleI;
          const int y0 = 32 * half + 16 * h;
+         const uint64_t scale2 = Pack2(scale, scale);
          if (x < P)
          {
 #pragma unroll
-            for (int c = 0; c < 16; ++c)
+            for (int c = 0; c < 8; ++c)
             {
-               const int yy = y0 + c;
-               const float e = h ? I[16 + c] : I[c];
+               const float2 e = Unpack2(Mul2(h ? I2[8 + c] : I2[c], scale2));
+               const int yy = y0 + 2 * c;
                if (yy < P)
-                  plane[static_cast<size_t>(yy) * P + x] = e * scale;
+                  plane[static_cast<size_t>(yy) * P + x] = e.x;
+               if (yy + 1 < P)
+                  plane[static_cast<size_t>(yy + 1) * P + x] = e.y;
             }
          }
          return true;
