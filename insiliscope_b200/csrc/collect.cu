@@ -5,7 +5,8 @@
 //
 // Order matters (a frame's emitters are splatted in event order), so the batch is compacted in three launches:
 // a CTA per frame counts the events it keeps, one CTA turns the counts into the frame table, and a CTA per frame
-// writes its emitters at its table offset, ranks inside a chunk from warp ballots.
+// writes its emitters at its table offset, ranks inside a chunk from warp ballots. The event render, which reads a
+// frame's emitters only through its table entry, takes them uncompacted in one launch (CollectGappedKernel).
 //
 // Compiled with --fmad=false, as the host code is compiled with -ffp-contract=off.
 
@@ -272,13 +273,93 @@ __global__ void __launch_bounds__(kCT) CollectWriteKernel(CollectArgs a)
    }
 }
 
+// The event render's collection in one launch: a CTA per frame writes its kept emitters, in event order, at the start
+// of the frame's own candidate slots [bucketStart[f] - bucketStart[0], bucketStart[f + 1] - bucketStart[0]), fills the
+// rest of those slots with zero-photon records (every render form skips them), and writes its frame table entry; the
+// total kept goes to nOut by atomics. The render reads a frame's emitters from its table entry, so the gaps change no
+// addition: the frames are the compacted batch's, bit for bit.
+__global__ void __launch_bounds__(kCT) CollectGappedKernel(CollectArgs a)
+{
+   const uint32_t f = blockIdx.x;
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   __shared__ uint32_t sWarp[kCT / 32];
+   uint32_t j0, j1;
+   Bucket(a, f, j0, j1);
+   const uint32_t first = j0 - a.bucketStart[0], end = j1 - a.bucketStart[0];
+   uint32_t pos = first;
+   unsigned long long clampedSum = 0;
+   for (uint32_t c = j0; c < j1; c += kCT)
+   {
+      const uint32_t j = c + threadIdx.x;
+      bool keep = false, cl = false;
+      iscu_emitter em;
+      uint32_t idx = 0;
+      if (j < j1)
+      {
+         keep = EmitterOf(a, f, j, em, cl, idx);
+         clampedSum += cl ? 1ull : 0ull;
+      }
+      const unsigned ballot = __ballot_sync(0xffffffffu, keep);
+      if (lane == 0)
+         sWarp[warp] = __popc(ballot);
+      __syncthreads();
+      uint32_t base = 0, total = 0;
+#pragma unroll
+      for (int w = 0; w < kCT / 32; ++w)
+      {
+         base += w < warp ? sWarp[w] : 0u;
+         total += sWarp[w];
+      }
+      if (keep)
+      {
+         const uint32_t o = pos + base + __popc(ballot & ((1u << lane) - 1u));
+         if (o < a.maxOut)
+         {
+            a.out[o] = em;
+            if (a.eventIndex)
+               a.eventIndex[o] = idx;
+         }
+      }
+      pos += total;
+      __syncthreads();
+   }
+   iscu_emitter none;
+   none.x_px = 0.0;
+   none.y_px = 0.0;
+   none.photons = 0.0;
+   none.plane = 0;
+   none.reserved = 0;
+   for (uint32_t o = pos + threadIdx.x; o < end && o < a.maxOut; o += kCT)
+      a.out[o] = none;
+   if (threadIdx.x == 0)
+   {
+      iscu_frame fr;
+      fr.em_start = first;
+      fr.em_count = pos - first;
+      fr.frame = static_cast<uint32_t>(a.frame0 + f);
+      fr.reserved = 0;
+      fr.bg_scale = a.bgScale ? a.bgScale[f] : 1.0;
+      a.frames[f] = fr;
+      if (pos > first)
+         atomicAdd(a.nOut, pos - first);
+   }
+   if (a.nClamped)
+   {
+      for (int d = 16; d > 0; d >>= 1)
+         clampedSum += __shfl_down_sync(0xffffffffu, clampedSum, d);
+      if (lane == 0 && clampedSum)
+         atomicAdd(a.nClamped, clampedSum);
+   }
+}
+
 } // namespace
 
 int LaunchCollect(iscu_ctx* ctx, int32_t slot, const iscu_blink_event* events, uint32_t nEvents,
                   const uint32_t* bucketIndex, const uint32_t* bucketStart, int64_t frame0, uint32_t nFrames,
                   double pixelNm, double perBlink, const double* driftX, const double* driftY, const double* globalZ,
                   const double* bgScale, const float* illum, double minPhotons, iscu_emitter* out,
-                  uint32_t* eventIndex, uint32_t maxOut, iscu_frame* frames, uint32_t* nOut, int64_t* nClamped)
+                  uint32_t* eventIndex, uint32_t maxOut, iscu_frame* frames, uint32_t* nOut, int64_t* nClamped,
+                  bool gapped)
 {
    if (nFrames == 0)
    {
@@ -318,6 +399,13 @@ int LaunchCollect(iscu_ctx* ctx, int32_t slot, const iscu_blink_event* events, u
    a.keptPerFrame = ctx->dCollect.as<uint32_t>();
    a.nOut = nOut;
    a.nClamped = reinterpret_cast<unsigned long long*>(nClamped);
+   if (gapped)
+   {
+      // nOut is zeroed by the caller (the event render clears its counts with the upload)
+      CollectGappedKernel<<<nFrames, kCT, 0, ctx->stream>>>(a);
+      ISCU_CK_LAUNCH(ctx, "CollectGappedKernel");
+      return ISCU_OK;
+   }
    CollectCountKernel<<<nFrames, kCT, 0, ctx->stream>>>(a);
    ISCU_CK_LAUNCH(ctx, "CollectCountKernel");
    CollectTableKernel<<<1, 1024, 0, ctx->stream>>>(a);
@@ -422,7 +510,7 @@ int EnqueueRenderEvents(iscu_ctx* ctx, EventIo& io, int32_t slot, const iscu_bli
                              pixelNm, perBlink, devPerFrame[0], devPerFrame[1], devPerFrame[2], devPerFrame[3],
                              useIllum && ctx->haveIllum ? ctx->illum.as<float>() : nullptr, minPhotons,
                              io.emitters.as<iscu_emitter>(), nullptr, nCand, io.frames.as<iscu_frame>(), dN,
-                             dClamped);
+                             dClamped, true);
       if (rc != ISCU_OK)
          return rc;
       CameraView cv;

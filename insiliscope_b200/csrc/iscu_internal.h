@@ -258,12 +258,15 @@ int LaunchNoiseFrames(iscu_ctx* ctx, const float* photons, uint32_t nFrames, con
                       const CameraView& cam, uint32_t seed, uint16_t* adu);
 // CollectFrameEmitters for a batch on the device (collect.cu): out gets the kept emitters (at most maxOut written;
 // eventIndex, nullable, their events' indices),
-// frames the table, *nOut the count kept (may pass maxOut), *nClamped += the clamped z planes (nullable).
+// frames the table, *nOut the count kept (may pass maxOut), *nClamped += the clamped z planes (nullable). gapped: frame
+// f's emitters at the start of its candidate slots (bucketStart[f] - bucketStart[0] on), the rest of the slots
+// zero-photon records, in one launch; *nOut must be zero beforehand.
 int LaunchCollect(iscu_ctx* ctx, int32_t slot, const iscu_blink_event* events, uint32_t nEvents,
                   const uint32_t* bucketIndex, const uint32_t* bucketStart, int64_t frame0, uint32_t nFrames,
                   double pixelNm, double perBlink, const double* driftX, const double* driftY, const double* globalZ,
                   const double* bgScale, const float* illum, double minPhotons, iscu_emitter* out,
-                  uint32_t* eventIndex, uint32_t maxOut, iscu_frame* frames, uint32_t* nOut, int64_t* nClamped);
+                  uint32_t* eventIndex, uint32_t maxOut, iscu_frame* frames, uint32_t* nOut, int64_t* nClamped,
+                  bool gapped = false);
 // The render's timing marks of the current call (nullptr when timing is off or the stream is capturing): 4 events.
 cudaEvent_t* RenderMarks(iscu_ctx* ctx);
 // Emitter runs of the frames beyond nEmitters are cut at nEmitters.
