@@ -5,7 +5,7 @@
 
 Workload `smlm` (the plain dSTORM SMLM render): one step renders a 200-frame 128 x 128 sCMOS movie -- every frame's
 background, ~160 Catmull-Rom PSF splats and the sCMOS noise chain -- from emitter records resident in HBM
-(`value`), and end to end from host blink events to host ADU frames through the C ABI (`e2e`: emitter collection,
+(`value`: the autotuned render form, replayed from a CUDA graph of the batch), and end to end from host blink events to host ADU frames through the C ABI (`e2e`: emitter collection,
 host->device copy, render, device->host copy). Frames shard across ranks (weak scaling: each rank renders its own
 200 frames; no collective on the data path). L2 is flushed (a 256 MB write) before every timed step.
 
@@ -198,12 +198,19 @@ class SmlmWorkload:
         self.stream = eng.torch_stream()
         self.frames_per_step = mv.frames
         self.n_emitters = len(self.ems)
+        # one step replays the batch's render (the form above) captured in a CUDA graph
+        from insiliscope_b200 import RenderGraph
+        self.graph = RenderGraph(eng, self.d_em, self.d_fr, mv.frames, mv.camera, mv.noise_seed, None, self.d_adu)
 
     slot = 0
 
-    def device_step(self):
+    def direct_step(self):
+        """The render launched directly (no graph): the pass timing and the plain-form comparison use it."""
         self.eng.render_frames_dev(self.d_em, self.d_fr, self.mv.frames, self.mv.camera, self.mv.noise_seed,
                                    None, self.d_adu, sync=False)
+
+    def device_step(self):
+        self.graph.launch(sync=False)
 
     def e2e_step(self):
         """Host blink events (page-locked) -> host ADU frames (page-locked) in one C-ABI call: H2D of the events,
@@ -232,13 +239,17 @@ class SmlmWorkload:
         return self.h_events.nbytes + self.h_bucket.nbytes, self.h_adu.nbytes
 
     def timing(self, on):
-        self.eng.set_render_timing(on)
+        pass   # graph replays carry no timing marks: dominant() times three direct renders
 
     def dominant(self):
-        """The render's passes, CUDA events inside the library over the timed steps: the slowest, with the movie's
-        algorithmic bytes (movie_bytes) as the bytes it is judged by; each pass's own traffic as this design moves
-        it (pass_bytes: the two-pass forms' contribution buffer included) in the breakdown."""
+        """The render's passes, CUDA events inside the library over three direct renders: the slowest, with the
+        movie's algorithmic bytes (movie_bytes) as the bytes it is judged by; each pass's own traffic as this design
+        moves it (pass_bytes: the two-pass forms' contribution buffer included) in the breakdown."""
+        self.eng.set_render_timing(True)
+        for _ in range(3):
+            self.direct_step()
         ms, calls = self.eng.render_pass_times()
+        self.eng.set_render_timing(False)
         name = max(ms, key=ms.get)
         kernel = {"grouping": "ContribSetup/Scan/Scatter", "contributions": "ContribKernel",
                   "tiles": "GatherTilesKernel" if self.form[4] == 2 else "RenderTilesKernel"}[name]
@@ -252,7 +263,7 @@ class SmlmWorkload:
         if graph is None:
             self.eng.set_render_config(form)
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        step = graph.launch if graph is not None else SmlmWorkload.device_step.__get__(self)
+        step = graph.launch if graph is not None else self.direct_step
         with torch.cuda.stream(self.stream):
             step() if graph is None else step(sync=False)
             s.record(self.stream)
@@ -275,6 +286,7 @@ class SmlmWorkload:
                "grid_form": grid, "grid_ms": round(self.time_render(grid), 4),
                "plain_form": 0, "plain_ms": round(self.time_render(0), 4)}
         self.eng.set_render_config(auto)
+        out["graph_replay_ms"] = round(self.time_render(None, graph=self.graph), 4)
         out["speedup_vs_plain"] = round(out["plain_ms"] / step_ms, 3)
         return out
 
@@ -320,7 +332,7 @@ class SmlmWorkload:
                                 "passes": 2 if self.form[4] == 2 else 1, "autotuned_config": self.autotuned,
                                 "autotune_ms_per_form": [round(x, 4) for x in self.autotune_ms]},
                 "mean_emitters_per_frame": self.n_emitters / self.mv.frames,
-                "max_emitters_per_frame": int(self.frames["em_count"].max())}
+                "max_emitters_per_frame": int(self.frames["em_count"].max()), "cuda_graph": True}
 
     def alg_bytes_per_launch(self):
         return self.movie_bytes()
@@ -374,37 +386,6 @@ class TwoColourWorkload(SmlmWorkload):
 
     def psfs(self):
         return self.mv.psfs
-
-    def setup(self, device: int, form=None):
-        from insiliscope_b200 import RenderGraph
-        super().setup(device, form)
-        mv = self.mv
-        self.graph = RenderGraph(self.eng, self.d_em, self.d_fr, mv.frames, mv.camera, mv.noise_seed, None,
-                                 self.d_adu)
-
-    def device_step(self):
-        self.graph.launch(sync=False)
-
-    def timing(self, on):
-        pass   # graph replays carry no timing marks: dominant() times three direct renders
-
-    def dominant(self):
-        self.eng.set_render_timing(True)
-        for _ in range(3):
-            SmlmWorkload.device_step(self)
-        out = SmlmWorkload.dominant(self)
-        self.eng.set_render_timing(False)
-        return out
-
-    def config_extra(self):
-        d = super().config_extra()
-        d["cuda_graph"] = True
-        return d
-
-    def plain_form(self, step_ms):
-        out = SmlmWorkload.plain_form(self, step_ms)
-        out["graph_replay_ms"] = round(self.time_render(None, graph=self.graph), 4)
-        return out
 
     cpu_sample = ("the movie's last 256 frames per step (25 % of its emitters, its heaviest frame among them): per "
                   "frame the reference's RenderPhotonImage for channel 0, then for channel 1 accumulating onto it "

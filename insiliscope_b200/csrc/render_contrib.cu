@@ -32,10 +32,12 @@ namespace iscu {
 namespace {
 
 constexpr int kE = 64;          // emitters per contribution work item
-// Contribution CTAs: at most 224 computing threads and a staging warp, four per SM (64 registers: the 16 float64 taps
-// in registers without spills), so one CTA's per-item barrier leaves the FP64 pipe to the other three.
-constexpr int kMaxCT = 224;     // contribution CTA size bound
-constexpr int kContribPerSm = 4;
+// Contribution CTAs: at most 384 computing threads and a staging warp, two per SM (72 registers: the 16 float64 taps
+// in registers without spills). A 33 x 33 square is three pixel blocks, so a group's per-item work (its taps from L2,
+// its geometry, the barrier) is paid three times rather than five as with 224-thread CTAs four to an SM, while the
+// other CTA keeps the FP64 pipe busy through one CTA's barrier.
+constexpr int kMaxCT = 384;
+constexpr int kContribPerSm = 2;
 constexpr int kGT = 256;        // gather CTA size (one thread per pixel of the tile)
 constexpr int kGChunk = 256;    // gather staging chunk
 
