@@ -7,6 +7,7 @@
 #include "iscu_internal.h"
 #include "psf_common.cuh"
 
+#include <algorithm>
 #include <vector>
 
 struct iscu_psf_plan
@@ -42,13 +43,15 @@ __global__ void PlanItemsKernel(const SetParams* __restrict__ sets, const uint32
    items[i].pad = 0;
 }
 
-int RunDev(iscu_psf_plan* p, const uint32_t* setOf, const double* defocusNm, uint32_t n, int normalize, float* out)
+int RunDev(iscu_psf_plan* p, const uint32_t* setOf, const double* defocusNm, uint32_t n, int normalize, float* out,
+           bool clearError = true)
 {
    iscu_ctx* ctx = p->ctx;
    if (n == 0)
       return ISCU_OK;
    ISCU_CK(p->items.Reserve(static_cast<size_t>(n) * sizeof(PsfItem)));
-   ISCU_CK(cudaMemsetAsync(p->err.p, 0, sizeof(int), ctx->stream));
+   if (clearError)
+      ISCU_CK(cudaMemsetAsync(p->err.p, 0, sizeof(int), ctx->stream));
    PlanItemsKernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(p->sets.as<SetParams>(), setOf, defocusNm, n, p->nSets,
                                                              p->items.as<PsfItem>(), p->err.as<int>());
    ISCU_CK_LAUNCH(ctx, "PlanItemsKernel");
@@ -174,17 +177,47 @@ int iscu_psf_plan_run(iscu_psf_plan* plan, const uint32_t* set_of_psf, const dou
    ClearError();
    if (n_psf == 0)
       return ISCU_OK;
-   const size_t planeBytes = static_cast<size_t>(plan->P) * plan->P * sizeof(float);
+   const size_t planeFloats = static_cast<size_t>(plan->P) * plan->P, planeBytes = planeFloats * sizeof(float);
    ISCU_CK(plan->setOf.Reserve(n_psf * sizeof(uint32_t)));
    ISCU_CK(plan->defocus.Reserve(n_psf * sizeof(double)));
    ISCU_CK(plan->out.Reserve(n_psf * planeBytes));
    ISCU_CK(cudaMemcpyAsync(plan->setOf.p, set_of_psf, n_psf * sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
    ISCU_CK(cudaMemcpyAsync(plan->defocus.p, defocus_nm, n_psf * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-   int rc = RunDev(plan, plan->setOf.as<uint32_t>(), plan->defocus.as<double>(), n_psf, normalize,
-                   plan->out.as<float>());
-   if (rc != ISCU_OK)
-      return rc;
-   ISCU_CK(cudaMemcpyAsync(out, plan->out.p, n_psf * planeBytes, cudaMemcpyDeviceToHost, ctx->stream));
+   // A large library runs in kRunChunks launches, each chunk's planes copied back on the download stream while the
+   // next chunk computes: the copy (PCIe) is the longer part, and a PSF's planes do not depend on the others'.
+   constexpr uint32_t kRunChunks = 4, kChunkMin = 2048;
+   const uint32_t chunks = n_psf >= kChunkMin ? kRunChunks : 1u;
+   const uint32_t per = (n_psf + chunks - 1) / chunks;
+   if (!ctx->download)
+      ISCU_CK(cudaStreamCreateWithFlags(&ctx->download, cudaStreamNonBlocking));
+   struct Events
+   {
+      cudaEvent_t e[kRunChunks] = {};
+      ~Events()
+      {
+         for (cudaEvent_t x : e)
+            if (x)
+               cudaEventDestroy(x);
+      }
+   } ev;
+   ISCU_CK(cudaMemsetAsync(plan->err.p, 0, sizeof(int), ctx->stream));
+   for (uint32_t c = 0, c0 = 0; c0 < n_psf; ++c, c0 += per)
+   {
+      const uint32_t nc = std::min(per, n_psf - c0);
+      const int rc = RunDev(plan, plan->setOf.as<uint32_t>() + c0, plan->defocus.as<double>() + c0, nc, normalize,
+                            plan->out.as<float>() + c0 * planeFloats, false);
+      if (rc != ISCU_OK)
+      {
+         cudaStreamSynchronize(ctx->download);
+         return rc;
+      }
+      ISCU_CK(cudaEventCreateWithFlags(&ev.e[c], cudaEventDisableTiming));
+      ISCU_CK(cudaEventRecord(ev.e[c], ctx->stream));
+      ISCU_CK(cudaStreamWaitEvent(ctx->download, ev.e[c], 0));
+      ISCU_CK(cudaMemcpyAsync(out + c0 * planeFloats, plan->out.as<float>() + c0 * planeFloats, nc * planeBytes,
+                              cudaMemcpyDeviceToHost, ctx->download));
+   }
+   ISCU_CK(cudaStreamSynchronize(ctx->download));
    return Check(plan);
 }
 

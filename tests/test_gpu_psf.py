@@ -158,3 +158,27 @@ def test_plan_matches_library(engine, method):
     with pytest.raises(IscuError):
         plan.run(bad, L.defocus_nm)
     plan.close()
+
+
+@pytest.mark.parametrize("method", [CZT_F16X3, CZT_FP32])
+def test_plan_run_in_chunks_matches_device_run(engine, method):
+    """A library large enough (2,100 PSFs) that the host-buffer run splits it into launches whose planes are copied
+    back while the next launch computes (sizes that do not divide evenly): the planes equal the device run's bit for
+    bit, and a bad set index in the last chunk is still reported."""
+    import torch
+    from insiliscope_b200 import IscuError, PsfPlan
+    from insiliscope_b200.workloads import psf_library
+    L = psf_library(seed=9, n_z=35, n_aberr=15)
+    assert len(L.set_of_psf) == 2100
+    plan = PsfPlan(engine, L.sets, size=L.size, method=method)
+    d_set = torch.from_numpy(L.set_of_psf.view(np.int32)).cuda()
+    d_dz = torch.from_numpy(L.defocus_nm).cuda()
+    out = torch.empty((len(L.set_of_psf), L.size, L.size), dtype=torch.float32, device="cuda")
+    want = plan.run_dev(d_set, d_dz, out).cpu().numpy()
+    got = plan.run(L.set_of_psf, L.defocus_nm)
+    assert np.array_equal(got, want)
+    bad = L.set_of_psf.copy()
+    bad[-1] = 10_000
+    with pytest.raises(IscuError):
+        plan.run(bad, L.defocus_nm)
+    plan.close()
