@@ -172,7 +172,8 @@ int iscu_psf_plan_info(iscu_psf_plan* plan, int32_t* size, int32_t* pupil_sample
 int iscu_psf_plan_run_dev(iscu_psf_plan* plan, const uint32_t* set_of_psf_dev, const double* defocus_nm_dev,
                           uint32_t n_psf, int32_t normalize, float* out_dev);
 int iscu_psf_plan_check(iscu_psf_plan* plan);
-/* The same from host arrays into host memory (the copies are part of the call). */
+/* The same from host arrays into host memory (the copies are part of the call; from 2,048 PSFs on, the library runs in
+ * four launches and each one's planes come back while the next computes, which pays with page-locked out). */
 int iscu_psf_plan_run(iscu_psf_plan* plan, const uint32_t* set_of_psf, const double* defocus_nm, uint32_t n_psf,
                       int32_t normalize, float* out);
 
