@@ -184,9 +184,13 @@ void iscu_destroy(iscu_ctx* ctx)
    for (cudaEvent_t e : ctx->renderMarks)
       cudaEventDestroy(e);
    for (iscu::EventIo& io : ctx->eventIo)
+   {
       for (cudaEvent_t e : {io.uploaded, io.rendered, io.downloaded})
          if (e)
             cudaEventDestroy(e);
+      if (io.launches)
+         cudaGraphExecDestroy(io.launches);
+   }
    for (cudaEvent_t e : ctx->fileCopied)
       if (e)
          cudaEventDestroy(e);

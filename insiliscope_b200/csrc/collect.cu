@@ -501,26 +501,69 @@ int EnqueueRenderEvents(iscu_ctx* ctx, EventIo& io, int32_t slot, const iscu_bli
    ISCU_CK(cudaMemsetAsync(io.counts.p, 0, 16, up));
    ISCU_CK(cudaEventRecord(io.uploaded, up));
 
-   // collection, render and noise on the context's stream, after the upload and after everything enqueued before
+   // collection, render and noise on the context's stream, after the upload and after everything enqueued before.
+   // They are captured into a graph and replayed through the slot's executable (updated in place from each batch's
+   // capture, made again when the launches' shape changes): the same kernels with fewer gaps between them. What the
+   // launches would allocate is reserved first, since a capture may not allocate.
    cudaStream_t s = ctx->stream;
    ISCU_CK(cudaStreamWaitEvent(s, io.uploaded, 0));
    if (nFrames)
    {
+      CameraView cv;
+      if (cam)
+         cv = MakeCameraView(*cam);
+      ISCU_CK(ctx->dCollect.Reserve(static_cast<size_t>(nFrames) * sizeof(uint32_t)));
+      ISCU_CK(ctx->dOrder.Reserve(OrderBytes(nFrames)));
+      if (ctx->renderConfig >= 12)
+      {
+         const int rr = ReserveContrib(ctx, nCand, ctx->contrib);
+         if (rr == ISCU_ERR_LIMIT)
+            ClearError();   // the render falls back to the one-pass form of the same tile
+         else if (rr != ISCU_OK)
+            return rr;
+      }
+      ISCU_CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       int rc = LaunchCollect(ctx, slot, io.events.as<iscu_blink_event>(), nEvents, dIdx, dBs, frame0, nFrames,
                              pixelNm, perBlink, devPerFrame[0], devPerFrame[1], devPerFrame[2], devPerFrame[3],
                              useIllum && ctx->haveIllum ? ctx->illum.as<float>() : nullptr, minPhotons,
                              io.emitters.as<iscu_emitter>(), nullptr, nCand, io.frames.as<iscu_frame>(), dN,
                              dClamped, true);
-      if (rc != ISCU_OK)
-         return rc;
-      CameraView cv;
-      if (cam)
-         cv = MakeCameraView(*cam);
-      rc = LaunchRenderFrames(ctx, io.emitters.as<iscu_emitter>(), nCand, io.frames.as<iscu_frame>(), nFrames,
-                              cam ? &cv : nullptr, seed, photons ? io.photons.as<float>() : nullptr,
-                              adu ? io.adu.as<uint16_t>() : nullptr);
-      if (rc != ISCU_OK)
-         return rc;
+      if (rc == ISCU_OK)
+         rc = LaunchRenderFrames(ctx, io.emitters.as<iscu_emitter>(), nCand, io.frames.as<iscu_frame>(), nFrames,
+                                 cam ? &cv : nullptr, seed, photons ? io.photons.as<float>() : nullptr,
+                                 adu ? io.adu.as<uint16_t>() : nullptr);
+      cudaGraph_t graph = nullptr;
+      const cudaError_t ec = cudaStreamEndCapture(s, &graph);
+      if (rc != ISCU_OK || ec != cudaSuccess)
+      {
+         if (graph)
+            cudaGraphDestroy(graph);
+         if (rc != ISCU_OK)
+            return rc;
+         ISCU_CK(ec);
+      }
+      bool updated = false;
+      if (io.launches)
+      {
+         cudaGraphExecUpdateResultInfo info;
+         updated = cudaGraphExecUpdate(io.launches, graph, &info) == cudaSuccess;
+         if (!updated)
+         {
+            cudaGetLastError();   // a refused update leaves no sticky error; the executable is made again
+            cudaGraphExecDestroy(io.launches);
+            io.launches = nullptr;
+         }
+      }
+      cudaError_t ei = cudaSuccess;
+      if (!updated)
+         ei = cudaGraphInstantiate(&io.launches, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ei != cudaSuccess)
+      {
+         io.launches = nullptr;
+         ISCU_CK(ei);
+      }
+      ISCU_CK(cudaGraphLaunch(io.launches, s));
    }
    ISCU_CK(cudaEventRecord(io.rendered, s));
 

@@ -190,6 +190,7 @@ struct EventIo
    DevBuf events, buckets, emitters, frames, counts, photons, adu;
    PinnedBuf hostCounts;           // {n kept (uint32 in a uint64), n clamped (int64)}
    cudaEvent_t uploaded = nullptr, rendered = nullptr, downloaded = nullptr;
+   cudaGraphExec_t launches = nullptr;   // the batch's collection and render, re-captured and updated per batch
 };
 
 } // namespace iscu
