@@ -33,6 +33,11 @@
 // memory holds four row-pass and four column-pass stages. A set change waits until both passes of the previous set
 // are done with the operand (the drain warps, which load it, have by then taken the previous PSF's E). The other
 // 256 columns hold T of the current PSF (128) and E of two PSFs (2 x 64).
+//
+// Instruction count is what the warps spend their time on, so the library's shape (a 128-sample pupil to 64 x 64) is
+// compiled in as its own instantiation, the phase table is laid out by pairs of pupil rows, and the producers' phase,
+// reduction and split residual and the drain's scaling, |E|^2, sums and normalization use the sm_100 two-lane float
+// instructions (fma/add/sub/mul.rn.f32x2; each lane rounds as the one-lane instruction would).
 
 #include "iscu_internal.h"
 #include "psf_common.cuh"
