@@ -484,10 +484,10 @@ __global__ void __launch_bounds__(kMaxCT + 32, kContribPerSm) ContribKernel(Cont
 // ------------------------------------------------------------------------------------------------ 5. gather
 struct GStage
 {
-   const int16_t* lo;   // halo cut of the emitter's plane, by dy + cr; null: the whole square
+   const float* centre;   // the emitter's contributions at its square's centre pixel: contrib + g S + cr side + cr
+   const int16_t* lo;     // halo cut of the emitter's plane, by dy + cr; null: the whole square
    const int16_t* hi;
-   uint32_t g;
-   int x0, y0, cr, side, pad;
+   int x0, y0, cr, side;
 };
 
 struct GatherArgs
@@ -524,11 +524,11 @@ __device__ __forceinline__ int GatherStage(const GatherArgs& a, uint32_t start, 
          const KernelView& kv = a.K.k[gr.z];
          const int cr = kv.camRad;
          keep = gr.x + cr >= tx0 && gr.x - cr <= tx1 && gr.y + cr >= ty0 && gr.y - cr <= ty1;
-         s.g = g;
          s.x0 = gr.x;
          s.y0 = gr.y;
          s.cr = cr;
          s.side = 2 * cr + 1;
+         s.centre = a.contrib + static_cast<size_t>(g) * a.S + static_cast<size_t>(cr) * s.side + cr;
          s.lo = kv.spanLo ? kv.spanLo + gr.w * s.side : nullptr;
          s.hi = kv.spanHi ? kv.spanHi + gr.w * s.side : nullptr;
       }
@@ -578,11 +578,12 @@ __device__ __forceinline__ int GatherWarpList(const GStage* sG, int kept, int wx
 __device__ __forceinline__ bool GatherCovers(const GStage& e, const GatherArgs& a, int X, int Y, const float*& src)
 {
    const int dx = X - e.x0, dy = Y - e.y0, cr = e.cr;
-   if (dx < -cr || dx > cr || dy < -cr || dy > cr)
+   const unsigned w = static_cast<unsigned>(2 * cr);   // |dx|, |dy| <= cr as one unsigned compare each
+   if (static_cast<unsigned>(dx + cr) > w || static_cast<unsigned>(dy + cr) > w)
       return false;
    if (e.lo && (dx < e.lo[dy + cr] || dx > e.hi[dy + cr]))
       return false;
-   src = a.contrib + static_cast<size_t>(e.g) * a.S + (dy + cr) * e.side + (dx + cr);
+   src = e.centre + dy * e.side + dx;
    return true;
 }
 
