@@ -485,9 +485,10 @@ __global__ void __launch_bounds__(kMaxCT + 32, kContribPerSm) ContribKernel(Cont
 struct GStage
 {
    const float* centre;   // the emitter's contributions at its square's centre pixel: contrib + g S + cr side + cr
+   int x0, y0;            // (the first 16 bytes: what every pixel's test and address read)
+   int cr, side;
    const int16_t* lo;     // halo cut of the emitter's plane, by dy + cr; null: the whole square
    const int16_t* hi;
-   int x0, y0, cr, side;
 };
 
 struct GatherArgs
@@ -510,7 +511,7 @@ struct GatherArgs
 
 // Stages one chunk of a frame's emitters whose square reaches the tile, in list order. Every thread calls it.
 __device__ __forceinline__ int GatherStage(const GatherArgs& a, uint32_t start, uint32_t count, int tx0, int ty0,
-                                           int tx1, int ty1, GStage* sG, int* sWarp)
+                                           int tx1, int ty1, GStage* sG, int* sWarp, bool& anyHalo)
 {
    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
    bool keep = false;
@@ -536,7 +537,7 @@ __device__ __forceinline__ int GatherStage(const GatherArgs& a, uint32_t start, 
    const unsigned ballot = __ballot_sync(0xffffffffu, keep);
    if (lane == 0)
       sWarp[warp] = __popc(ballot);
-   __syncthreads();
+   anyHalo = __syncthreads_or(keep && s.lo != nullptr) != 0;
    int base = 0, total = 0;
 #pragma unroll
    for (int w = 0; w < kGT / 32; ++w)
@@ -575,16 +576,47 @@ __device__ __forceinline__ int GatherWarpList(const GStage* sG, int kept, int wx
 }
 
 // Whether the emitter's square and halo cut cover pixel (X, Y); the contribution's address if so.
-__device__ __forceinline__ bool GatherCovers(const GStage& e, const GatherArgs& a, int X, int Y, const float*& src)
+template <bool kHalo>
+__device__ __forceinline__ bool GatherCovers(const GStage& e, int X, int Y, const float*& src)
 {
    const int dx = X - e.x0, dy = Y - e.y0, cr = e.cr;
    const unsigned w = static_cast<unsigned>(2 * cr);   // |dx|, |dy| <= cr as one unsigned compare each
    if (static_cast<unsigned>(dx + cr) > w || static_cast<unsigned>(dy + cr) > w)
       return false;
-   if (e.lo && (dx < e.lo[dy + cr] || dx > e.hi[dy + cr]))
+   if (kHalo && e.lo && (dx < e.lo[dy + cr] || dx > e.hi[dy + cr]))
       return false;
    src = e.centre + dy * e.side + dx;
    return true;
+}
+
+// A pixel's adds of the warp list's contributions, in list order, four loads in flight.
+template <bool kHalo>
+__device__ __forceinline__ float GatherAdds(const GStage* sG, const uint16_t* list, int n, int X, int Y, float acc)
+{
+   int m = 0;
+   for (; m + 4 <= n; m += 4)
+   {
+      float v[4];
+      bool in[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+      {
+         const float* src = nullptr;
+         in[u] = GatherCovers<kHalo>(sG[list[m + u]], X, Y, src);
+         v[u] = in[u] ? __ldg(src) : 0.0f;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+         if (in[u])
+            acc += v[u];
+   }
+   for (; m < n; ++m)
+   {
+      const float* src = nullptr;
+      if (GatherCovers<kHalo>(sG[list[m]], X, Y, src))
+         acc += __ldg(src);
+   }
+   return acc;
 }
 
 // Six CTAs per SM (40 registers; the noise chain spills a little): the gather's loads and the Knuth loops are latency-
@@ -637,32 +669,12 @@ __global__ void __launch_bounds__(kGT, 6) GatherTilesKernel(GatherArgs a)
       for (uint32_t e0 = 0; e0 < emCount; e0 += kGChunk)
       {
          const uint32_t cnt = min(static_cast<uint32_t>(kGChunk), emCount - e0);
-         const int kept = GatherStage(a, fr.em_start + e0, cnt, tx0, ty0, tx1, ty1, sG, sWarp);
+         bool anyHalo = false;
+         const int kept = GatherStage(a, fr.em_start + e0, cnt, tx0, ty0, tx1, ty1, sG, sWarp, anyHalo);
          const int n = GatherWarpList(sG, kept, wx0, wx0 + wcw - 1, wy0, wy0 + wrh - 1, list);
-         // four loads in flight, their adds in list order
-         int m = 0;
-         for (; m + 4 <= n; m += 4)
-         {
-            float v[4];
-            bool in[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-            {
-               const float* src = nullptr;
-               in[u] = inside && GatherCovers(sG[list[m + u]], a, X, Y, src);
-               v[u] = in[u] ? __ldg(src) : 0.0f;
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-               if (in[u])
-                  acc += v[u];
-         }
-         for (; m < n; ++m)
-         {
-            const float* src = nullptr;
-            if (inside && GatherCovers(sG[list[m]], a, X, Y, src))
-               acc += __ldg(src);
-         }
+         // the chunk's adds in list order; the halo test only where a staged emitter has a cut (the same for the CTA)
+         if (inside)
+            acc = anyHalo ? GatherAdds<true>(sG, list, n, X, Y, acc) : GatherAdds<false>(sG, list, n, X, Y, acc);
          __syncthreads();
       }
       if (inside)
